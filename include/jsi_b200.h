@@ -1,0 +1,169 @@
+/* jsi_b200 — B200-native NURBS minimum-distance and surface-surface
+ * intersection query path, C ABI.
+ *
+ * This is the drop-in boundary for the query path of JSI_CAD_NEXT VERSION5.
+ * Each entry point names the reference interface it replaces (paths relative
+ * to JSI_CAD_NEXT_VERSION5/).  All calls return an int status (JSI_OK = 0,
+ * negative = error class); nothing exits the process.  Pointers are plain
+ * host pointers unless stated otherwise; no CUDA or C++ types cross the ABI.
+ *
+ * Threading: a context owns one CUDA stream and one device arena; calls on the
+ * same context are serialised by an internal mutex.  Use one context per
+ * host thread for concurrency.
+ */
+#ifndef JSI_B200_H
+#define JSI_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JSI_B200_ABI_VERSION 1
+#define JSI_MAX_ROUNDS 16
+#define JSI_RECORD_SIZE 18 /* ONE_UV_SIZE, include/jsi_cad.hpp:45 */
+
+typedef enum {
+  JSI_OK = 0,
+  JSI_ERR_INVALID = -1,     /* bad argument (null pointer, nuv < 2, k < 1, ...) */
+  JSI_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  JSI_ERR_NOMEM = -3,       /* device arena or HBM budget exhausted */
+  JSI_ERR_CAPACITY = -4,    /* a result did not fit the caller's buffer or an internal list */
+  JSI_ERR_SURFACE = -5,     /* malformed surface header / data */
+  JSI_ERR_TIMEOUT = -6,     /* a bounded device wait gave up */
+  JSI_ERR_UNSUPPORTED = -7, /* option not available in this build */
+  JSI_ERR_NO_DEVICE = -8    /* no CUDA device / extension not usable */
+} jsi_status;
+
+/* Arithmetic form of a query.
+ *  V5_FP32      - VERSION5's FP32 arithmetic reproduced operation for
+ *                 operation: same k-th value, same candidate sets.
+ *  FP64         - the same algorithm entirely in FP64 (plain form).
+ *  FP32_SCREEN  - FP32 evaluation / boxes / screening with every box widened
+ *                 by a rigorous rounding-error bound, FP64 knot spans, basis
+ *                 and rational division, FP64 re-check of the screened
+ *                 candidates; results equal the FP64 form's. */
+typedef enum { JSI_PREC_V5_FP32 = 0, JSI_PREC_FP64 = 1, JSI_PREC_FP32_SCREEN = 2 } jsi_precision;
+
+typedef struct jsi_context jsi_context;
+typedef int jsi_surface_id;
+
+typedef struct {
+  int device;                          /* CUDA device ordinal */
+  unsigned long long arena_bytes;      /* device arena of the context; 0 = 2 GiB */
+  unsigned long long hbm_budget_bytes; /* cap on arena + resident surfaces; 0 = 120 GiB */
+} jsi_config;
+
+/* Replaces init_cad() / deinit_cad() (src/common/common.cu:35-61): the
+ * 4 GiB host bump workspace becomes a device arena owned by the context. */
+int jsi_create(const jsi_config *cfg, jsi_context **out);
+int jsi_destroy(jsi_context *ctx);
+
+const char *jsi_status_string(int status);
+/* Text of the last error recorded on ctx (empty string if none). */
+const char *jsi_last_error(const jsi_context *ctx);
+int jsi_abi_version(void);
+
+/* Copies one surface in EGADS layout (ivec[7] + data, include/nurbs_data.hpp:1-10,
+ * decoded as in src/evaluation/evaluation.cu:239-257) to device memory and
+ * keeps it resident until released.  Replaces the caller-side
+ * allocate_from_workspace + cadMemcpy of ivec/data
+ * (examples/intersection_example.cu:50-57). */
+int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, int ndata, jsi_surface_id *out);
+int jsi_surface_release(jsi_context *ctx, jsi_surface_id id);
+/* Resident surface bytes on the device. */
+int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out);
+
+/* One query side: EvalAndConstructTask (include/jsi_cad.hpp:11-23) with the
+ * surface named by a resident id instead of raw device pointers. */
+typedef struct {
+  jsi_surface_id surface;
+  float ustart, vstart, ustop, vstop;
+  int nuv;  /* first-round sampling width */
+  int side; /* eval_task_side: 1 or 2 */
+} jsi_task;
+
+/* --- minimum distance ---------------------------------------------------
+ * Replaces float minimum_distance(const EvalAndConstructTask&,
+ * const EvalAndConstructTask&) (include/jsi_cad.hpp:31,
+ * src/distance_analysis/distance_analysis.cu:356-506).  Defaults equal the
+ * reference statics (:33-36): k = 8, rounds = 4, refinement nuv = 16. */
+typedef struct {
+  int nuv_refine; /* next_nuv */
+  int k;          /* k_of_topk, 1..1024 */
+  int rounds;     /* max_layers, 1..JSI_MAX_ROUNDS */
+  int precision;  /* jsi_precision */
+  int newton;     /* 1: FP64 Newton refinement of the closest points from the final candidates */
+} jsi_dist_params;
+
+typedef struct {
+  float v5_value;   /* what minimum_distance returns: sqrt of the last round's k-th d2 */
+  double distance;  /* FP64 forms: sqrt of the last round's k-th d2 in FP64; V5_FP32: v5_value */
+  double newton_distance;     /* refined true distance (newton = 1), else -1 */
+  double uv1[2], uv2[2];      /* closest parameters (newton = 1) */
+  double point1[3], point2[3];
+  int rounds_run;
+  int npairs[JSI_MAX_ROUNDS];        /* pairs kept per round (min(k, #pairs)) */
+  double kth_d2[JSI_MAX_ROUNDS];     /* k-th squared centre distance per round */
+  long long pair_tests[JSI_MAX_ROUNDS];  /* cell-pair distance tests executed per round */
+  long long candidates[JSI_MAX_ROUNDS];  /* pairs that passed the screen, before selection */
+  /* Optional trace (caller-owned, may be null): the kept (slot, i, j)
+   * triples of every round, round r at trace_pairs[(r*k + q)*3 ...]. */
+  int *trace_pairs;
+  long long trace_cap; /* capacity in triples; needs rounds*k */
+  float device_ms;     /* device time of the query (CUDA events) */
+} jsi_dist_result;
+
+void jsi_dist_params_default(jsi_dist_params *p);
+int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
+                     jsi_dist_result *out);
+
+/* --- surface-surface intersection ----------------------------------------
+ * Replaces void intersection(EvalAndConstructTask, EvalAndConstructTask)
+ * (include/jsi_cad.hpp:33, src/intersection/intersection.cu:338-475).  The
+ * reference keeps its refinement width in a file static that the halving rule
+ * mutates across calls (:36, :370); here it is a per-call parameter. */
+typedef struct {
+  int nuv_refine;      /* global_nuv at call start (16) */
+  int use_k;           /* CAD_INTERSECT_USE_K: curvature padding on (1) / off (0) */
+  int rounds;          /* 6 */
+  int halve_threshold; /* 512 */
+  int min_nuv;         /* 4 */
+  int precision;       /* jsi_precision */
+} jsi_inter_params;
+
+typedef struct {
+  int rounds_run;
+  long long counts[JSI_MAX_ROUNDS];     /* overlap pairs per round ("Round r: overlap pairs = N") */
+  long long pair_tests[JSI_MAX_ROUNDS]; /* cell-pair box tests executed per round */
+  long long regions1[JSI_MAX_ROUNDS];   /* unique side-1 regions evaluated per round */
+  long long regions2[JSI_MAX_ROUNDS];
+  double pad[2];                        /* round-1 curvature paddings of side 1 / side 2 */
+  /* Optional trace (caller-owned, may be null): every round's (slot, i, j)
+   * triples concatenated in round order; trace_written counts all pairs
+   * (also those beyond trace_cap). */
+  int *trace_pairs;
+  long long trace_cap;
+  long long trace_written;
+  float device_ms;
+} jsi_inter_result;
+
+void jsi_inter_params_default(jsi_inter_params *p);
+int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_inter_params *params,
+                  jsi_inter_result *out);
+
+/* --- grid evaluation -----------------------------------------------------
+ * Replaces evalWithCuda(int*, float*, int, float, float, float, float, int,
+ * float*) (include/jsi_cad.hpp:46, src/evaluation/evaluation.cu:391-405):
+ * nuv x nuv records of 18 floats (P, Pu, Pv, Puu, Puv, Pvv), sample
+ * (idx, idy) at (ustep*idx + ustart, vstep*idy + vstart), record at
+ * (idx + idy*nuv)*18.  results is a host pointer. */
+int jsi_eval_grid(jsi_context *ctx, const int ivec[7], const float *data, int ndata, float ustep, float vstep,
+                  float ustart, float vstart, int nuv, float *results);
+/* The same grid in FP64 (data promoted from float). */
+int jsi_eval_grid_f64(jsi_context *ctx, const int ivec[7], const float *data, int ndata, double ustep,
+                      double vstep, double ustart, double vstart, int nuv, double *results);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JSI_B200_H */

@@ -1,0 +1,119 @@
+"""ctypes declarations of the C ABI in include/jsi_b200.h.
+
+The shared library is loaded from the package directory; there is no
+fallback: if libjsi_b200.so is missing or cannot be loaded, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libjsi_b200.so"
+
+MAX_ROUNDS = 16
+RECORD_SIZE = 18
+
+JSI_OK = 0
+STATUS_NAMES = {
+    0: "JSI_OK", -1: "JSI_ERR_INVALID", -2: "JSI_ERR_CUDA", -3: "JSI_ERR_NOMEM", -4: "JSI_ERR_CAPACITY",
+    -5: "JSI_ERR_SURFACE", -6: "JSI_ERR_TIMEOUT", -7: "JSI_ERR_UNSUPPORTED", -8: "JSI_ERR_NO_DEVICE",
+}
+
+PREC_V5_FP32 = 0
+PREC_FP64 = 1
+PREC_FP32_SCREEN = 2
+PRECISIONS = {"v5_fp32": PREC_V5_FP32, "fp64": PREC_FP64, "fp32_screen": PREC_FP32_SCREEN}
+
+# Every symbol include/jsi_b200.h declares.
+EXPORTED = [
+    "jsi_abi_version", "jsi_status_string", "jsi_last_error", "jsi_create", "jsi_destroy",
+    "jsi_surface_upload", "jsi_surface_release", "jsi_resident_bytes", "jsi_dist_params_default",
+    "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
+]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("arena_bytes", ctypes.c_ulonglong),
+                ("hbm_budget_bytes", ctypes.c_ulonglong)]
+
+
+class Task(ctypes.Structure):
+    _fields_ = [("surface", ctypes.c_int), ("ustart", ctypes.c_float), ("vstart", ctypes.c_float),
+                ("ustop", ctypes.c_float), ("vstop", ctypes.c_float), ("nuv", ctypes.c_int), ("side", ctypes.c_int)]
+
+
+class DistParams(ctypes.Structure):
+    _fields_ = [("nuv_refine", ctypes.c_int), ("k", ctypes.c_int), ("rounds", ctypes.c_int),
+                ("precision", ctypes.c_int), ("newton", ctypes.c_int)]
+
+
+class DistResult(ctypes.Structure):
+    _fields_ = [("v5_value", ctypes.c_float), ("distance", ctypes.c_double), ("newton_distance", ctypes.c_double),
+                ("uv1", ctypes.c_double * 2), ("uv2", ctypes.c_double * 2), ("point1", ctypes.c_double * 3),
+                ("point2", ctypes.c_double * 3), ("rounds_run", ctypes.c_int), ("npairs", ctypes.c_int * MAX_ROUNDS),
+                ("kth_d2", ctypes.c_double * MAX_ROUNDS), ("pair_tests", ctypes.c_longlong * MAX_ROUNDS),
+                ("candidates", ctypes.c_longlong * MAX_ROUNDS), ("trace_pairs", ctypes.POINTER(ctypes.c_int)),
+                ("trace_cap", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+
+
+class InterParams(ctypes.Structure):
+    _fields_ = [("nuv_refine", ctypes.c_int), ("use_k", ctypes.c_int), ("rounds", ctypes.c_int),
+                ("halve_threshold", ctypes.c_int), ("min_nuv", ctypes.c_int), ("precision", ctypes.c_int)]
+
+
+class InterResult(ctypes.Structure):
+    _fields_ = [("rounds_run", ctypes.c_int), ("counts", ctypes.c_longlong * MAX_ROUNDS),
+                ("pair_tests", ctypes.c_longlong * MAX_ROUNDS), ("regions1", ctypes.c_longlong * MAX_ROUNDS),
+                ("regions2", ctypes.c_longlong * MAX_ROUNDS), ("pad", ctypes.c_double * 2),
+                ("trace_pairs", ctypes.POINTER(ctypes.c_int)), ("trace_cap", ctypes.c_longlong),
+                ("trace_written", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+
+
+_lib = None
+
+
+def load(path: Path | str | None = None) -> ctypes.CDLL:
+    """Load libjsi_b200.so and declare its signatures (raises if absent)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m jsi_cad_next_versions_b200.build` "
+                           "(there is no CPU fallback)")
+    L = ctypes.CDLL(str(p))
+    P = ctypes.c_void_p
+    I = ctypes.c_int
+    L.jsi_abi_version.restype = I
+    L.jsi_status_string.argtypes = [I]
+    L.jsi_status_string.restype = ctypes.c_char_p
+    L.jsi_last_error.argtypes = [P]
+    L.jsi_last_error.restype = ctypes.c_char_p
+    L.jsi_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(P)]
+    L.jsi_create.restype = I
+    L.jsi_destroy.argtypes = [P]
+    L.jsi_destroy.restype = I
+    L.jsi_surface_upload.argtypes = [P, P, P, I, ctypes.POINTER(I)]
+    L.jsi_surface_upload.restype = I
+    L.jsi_surface_release.argtypes = [P, I]
+    L.jsi_surface_release.restype = I
+    L.jsi_resident_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.jsi_resident_bytes.restype = I
+    L.jsi_dist_params_default.argtypes = [ctypes.POINTER(DistParams)]
+    L.jsi_dist_params_default.restype = None
+    L.jsi_min_distance.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),
+                                   ctypes.POINTER(DistResult)]
+    L.jsi_min_distance.restype = I
+    L.jsi_inter_params_default.argtypes = [ctypes.POINTER(InterParams)]
+    L.jsi_inter_params_default.restype = None
+    L.jsi_intersect.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(InterParams),
+                                ctypes.POINTER(InterResult)]
+    L.jsi_intersect.restype = I
+    L.jsi_eval_grid.argtypes = [P, P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, I, P]
+    L.jsi_eval_grid.restype = I
+    L.jsi_eval_grid_f64.argtypes = [P, P, P, I, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, I, P]
+    L.jsi_eval_grid_f64.restype = I
+    if path is None:
+        _lib = L
+    return L

@@ -1,0 +1,278 @@
+"""Python host mirror of the VERSION5 query API over the C ABI.
+
+Two layers:
+
+* ``Context`` - explicit context (device, arena, resident surfaces) with
+  ``upload``, ``min_distance``, ``intersect`` and ``eval_grid``.
+* The reference's own names (include/jsi_cad.hpp:11-46): ``init_cad``,
+  ``deinit_cad``, ``EvalAndConstructTask``, ``minimum_distance``,
+  ``intersection`` and ``evalWithCuda``, bound to a module-level default
+  context, so code written against the reference reads the same.
+
+Errors raise ``JsiError`` carrying the C status; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as C
+
+
+class JsiError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{C.STATUS_NAMES.get(status, status)}: {message}")
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class DistanceResult:
+    v5_value: float
+    distance: float
+    newton_distance: float
+    uv1: tuple
+    uv2: tuple
+    point1: tuple
+    point2: tuple
+    rounds: int
+    npairs: np.ndarray
+    kth_d2: np.ndarray
+    pair_tests: np.ndarray
+    candidates: np.ndarray
+    device_ms: float
+    pairs: list = field(default_factory=list)  # per round (n, 3) int32 (slot, i, j) if traced
+
+
+@dataclass
+class IntersectionResult:
+    rounds: int
+    counts: np.ndarray
+    pair_tests: np.ndarray
+    regions1: np.ndarray
+    regions2: np.ndarray
+    pad: tuple
+    device_ms: float
+    pairs: list = field(default_factory=list)  # per round (n, 3) int32 if traced
+
+
+class Context:
+    """A device context: one stream, one arena, resident surfaces."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = C.load()
+        cfg = C.Config(device, arena_bytes, hbm_budget_bytes)
+        h = ctypes.c_void_p()
+        st = self.lib.jsi_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != C.JSI_OK:
+            raise JsiError(st, "jsi_create failed")
+        self.handle = h
+        self._surfaces = {}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.jsi_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != C.JSI_OK:
+            msg = self.lib.jsi_last_error(self.handle)
+            raise JsiError(st, msg.decode() if msg else "")
+
+    # -- surfaces ---------------------------------------------------------
+    def upload(self, surface=None, *, ivec=None, data=None) -> int:
+        """Upload a surface (``synth.Surface`` or ivec/data arrays); returns its id."""
+        if surface is not None:
+            ivec, data = surface.ivec, surface.data
+        iv = np.ascontiguousarray(ivec, dtype=np.int32)
+        da = np.ascontiguousarray(data, dtype=np.float32)
+        sid = ctypes.c_int(0)
+        self._check(self.lib.jsi_surface_upload(self.handle, _p(iv), _p(da), int(da.shape[0]), ctypes.byref(sid)))
+        return sid.value
+
+    def release(self, sid: int):
+        self._check(self.lib.jsi_surface_release(self.handle, sid))
+
+    def resident_bytes(self) -> int:
+        v = ctypes.c_ulonglong(0)
+        self._check(self.lib.jsi_resident_bytes(self.handle, ctypes.byref(v)))
+        return v.value
+
+    # -- queries ----------------------------------------------------------
+    @staticmethod
+    def task(sid: int, rect, nuv: int, side: int) -> C.Task:
+        return C.Task(sid, float(rect[0]), float(rect[1]), float(rect[2]), float(rect[3]), int(nuv), int(side))
+
+    def min_distance(self, a: C.Task, b: C.Task, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
+                     precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False) -> DistanceResult:
+        prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p = C.DistParams(nuv_refine, k, rounds, prec, 1 if newton else 0)
+        r = C.DistResult()
+        buf = None
+        if trace:
+            buf = np.full(rounds * k * 3, -1, dtype=np.int32)
+            r.trace_pairs = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            r.trace_cap = rounds * k
+        self._check(self.lib.jsi_min_distance(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
+                                              ctypes.byref(r)))
+        n = r.rounds_run
+        npairs = np.array(r.npairs[:n], dtype=np.int64)
+        pairs = []
+        if trace:
+            for q in range(n):
+                pairs.append(buf[q * k * 3:(q * k + int(npairs[q])) * 3].reshape(-1, 3).copy())
+        return DistanceResult(
+            v5_value=float(np.float32(r.v5_value)), distance=r.distance, newton_distance=r.newton_distance,
+            uv1=tuple(r.uv1), uv2=tuple(r.uv2), point1=tuple(r.point1), point2=tuple(r.point2), rounds=n,
+            npairs=npairs, kth_d2=np.array(r.kth_d2[:n]), pair_tests=np.array(r.pair_tests[:n], dtype=np.int64),
+            candidates=np.array(r.candidates[:n], dtype=np.int64), device_ms=r.device_ms, pairs=pairs)
+
+    def intersect(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
+                  halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",
+                  trace: bool = False, trace_cap: int = 1 << 24) -> IntersectionResult:
+        prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec)
+        r = C.InterResult()
+        buf = None
+        if trace:
+            buf = np.full(trace_cap * 3, -1, dtype=np.int32)
+            r.trace_pairs = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            r.trace_cap = trace_cap
+        self._check(self.lib.jsi_intersect(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
+                                           ctypes.byref(r)))
+        n = r.rounds_run
+        counts = np.array(r.counts[:n], dtype=np.int64)
+        pairs = []
+        if trace:
+            off = 0
+            for c in counts:
+                c = int(c)
+                pairs.append(buf[off * 3:(off + c) * 3].reshape(-1, 3).copy() if off + c <= trace_cap else None)
+                off += c
+        return IntersectionResult(
+            rounds=n, counts=counts, pair_tests=np.array(r.pair_tests[:n], dtype=np.int64),
+            regions1=np.array(r.regions1[:n], dtype=np.int64), regions2=np.array(r.regions2[:n], dtype=np.int64),
+            pad=(r.pad[0], r.pad[1]), device_ms=r.device_ms, pairs=pairs)
+
+    def eval_grid(self, ivec, data, ustep, vstep, ustart, vstart, nuv, dtype=np.float32) -> np.ndarray:
+        iv = np.ascontiguousarray(ivec, dtype=np.int32)
+        da = np.ascontiguousarray(data, dtype=np.float32)
+        out = np.zeros(nuv * nuv * C.RECORD_SIZE, dtype=dtype)
+        if dtype == np.float32:
+            st = self.lib.jsi_eval_grid(self.handle, _p(iv), _p(da), int(da.shape[0]), float(np.float32(ustep)),
+                                        float(np.float32(vstep)), float(np.float32(ustart)),
+                                        float(np.float32(vstart)), nuv, _p(out))
+        else:
+            st = self.lib.jsi_eval_grid_f64(self.handle, _p(iv), _p(da), int(da.shape[0]), float(ustep),
+                                            float(vstep), float(ustart), float(vstart), nuv, _p(out))
+        self._check(st)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's names over a default context
+# ---------------------------------------------------------------------------
+
+_default: Context | None = None
+
+default_global_dist_nuv = 512     # include/jsi_cad.hpp:35
+default_global_intersect_nuv = 16  # include/jsi_cad.hpp:36
+ONE_UV_SIZE = C.RECORD_SIZE        # include/jsi_cad.hpp:45
+
+
+def init_cad(device: int = 0):
+    """init_cad() (common.cu:35-49): creates the default device context."""
+    global _default
+    if _default is None:
+        _default = Context(device)
+    return _default
+
+
+def deinit_cad():
+    """deinit_cad() (common.cu:51-61): releases the default context."""
+    global _default
+    if _default is not None:
+        _default.close()
+        _default = None
+
+
+def _ctx() -> Context:
+    if _default is None:
+        raise JsiError(-1, "init_cad() has not been called")
+    return _default
+
+
+@dataclass
+class EvalAndConstructTask:
+    """include/jsi_cad.hpp:11-23, with host arrays in place of d_ivec / d_data."""
+
+    d_ivec: np.ndarray
+    d_data: np.ndarray
+    d_ndata: int
+    ustart: float
+    vstart: float
+    ustop: float
+    vstop: float
+    nuv: int
+    eval_task_side: int
+
+
+def _upload_task(ctx: Context, t: EvalAndConstructTask):
+    sid = ctx.upload(ivec=t.d_ivec, data=np.asarray(t.d_data)[: t.d_ndata])
+    return Context.task(sid, (t.ustart, t.vstart, t.ustop, t.vstop), t.nuv, t.eval_task_side), sid
+
+
+def minimum_distance(t1: EvalAndConstructTask, t2: EvalAndConstructTask, **kw) -> float:
+    """float minimum_distance(t1, t2) (distance_analysis.cu:356-506)."""
+    ctx = _ctx()
+    a, sa = _upload_task(ctx, t1)
+    b, sb = _upload_task(ctx, t2)
+    try:
+        return ctx.min_distance(a, b, **kw).v5_value
+    finally:
+        ctx.release(sa)
+        ctx.release(sb)
+
+
+def intersection(t1: EvalAndConstructTask, t2: EvalAndConstructTask, verbose: bool = False, **kw):
+    """void intersection(t1, t2) (intersection.cu:338-475).  The reference only
+    prints "Round r: overlap pairs = N"; this returns the per-round counts
+    (and prints them when verbose)."""
+    ctx = _ctx()
+    a, sa = _upload_task(ctx, t1)
+    b, sb = _upload_task(ctx, t2)
+    try:
+        res = ctx.intersect(a, b, **kw)
+    finally:
+        ctx.release(sa)
+        ctx.release(sb)
+    if verbose:
+        for r, c in enumerate(res.counts, 1):
+            print(f"Round {r}: overlap pairs = {int(c)}")
+    return res.counts
+
+
+def evalWithCuda(ivec, data, ndata, ustep, vstep, ustart, vstart, nuv, results=None):
+    """evalWithCuda (evaluation.cu:391-405): nuv*nuv records of 18 floats."""
+    out = _ctx().eval_grid(ivec, np.asarray(data)[:ndata], ustep, vstep, ustart, vstart, nuv)
+    if results is not None:
+        results[: out.shape[0]] = out
+        return results
+    return out

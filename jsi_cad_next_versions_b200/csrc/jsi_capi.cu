@@ -1,0 +1,840 @@
+// Host orchestration and C ABI of libjsi_b200.
+//
+// One context = one CUDA stream + one device arena (a chain of cudaMalloc'd
+// blocks reused across queries, rewound at the start of each query: the
+// B200 counterpart of the reference's 4 GiB bump workspace,
+// src/common/common.cu:17-33) + the resident surfaces.
+//
+// A query runs its refinement rounds on the device; the host reads one small
+// stats record per round (pair count, unique-region counts) to size the next
+// round, exactly where the reference's round loop decides
+// (distance_analysis.cu:375-392, intersection.cu:359-370).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "jsi_b200.h"
+#include "jsi_internal.h"
+
+using namespace jsi;
+
+namespace {
+
+struct CudaError {
+  cudaError_t err;
+  const char *what;
+  int line;
+};
+
+#define JSI_CUDA(call)                                 \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) throw CudaError{e_, #call, __LINE__}; \
+  } while (0)
+
+struct StatusError {
+  int status;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int status, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw StatusError{status, buf};
+}
+
+// Device arena: blocks are kept across queries and rewound by reset().
+class Arena {
+ public:
+  Arena() = default;
+  Arena(const Arena &) = delete;
+  Arena &operator=(const Arena &) = delete;
+  ~Arena() {
+    for (auto &b : blocks_) cudaFree(b.base);
+  }
+  void configure(size_t block_bytes, size_t budget) {
+    block_bytes_ = block_bytes;
+    budget_ = budget;
+  }
+  void reset() {
+    for (auto &b : blocks_) b.used = 0;
+    cur_ = 0;
+  }
+  void *alloc(size_t bytes) {
+    bytes = (bytes + 255) & ~static_cast<size_t>(255);
+    if (bytes == 0) bytes = 256;
+    while (cur_ < blocks_.size()) {
+      Block &b = blocks_[cur_];
+      if (b.used + bytes <= b.size) {
+        void *p = b.base + b.used;
+        b.used += bytes;
+        return p;
+      }
+      ++cur_;
+    }
+    const size_t sz = std::max(block_bytes_, bytes);
+    if (total_ + sz > budget_) fail(JSI_ERR_NOMEM, "device arena budget exhausted (%zu + %zu > %zu bytes)", total_, sz, budget_);
+    char *p = nullptr;
+    if (cudaMalloc(&p, sz) != cudaSuccess) {
+      cudaGetLastError();
+      fail(JSI_ERR_NOMEM, "cudaMalloc of %zu bytes failed", sz);
+    }
+    blocks_.push_back({p, sz, bytes});
+    total_ += sz;
+    cur_ = blocks_.size() - 1;
+    return p;
+  }
+  template <typename U>
+  U *get(size_t n) {
+    return static_cast<U *>(alloc(n * sizeof(U)));
+  }
+  size_t total() const { return total_; }
+
+ private:
+  struct Block {
+    char *base;
+    size_t size;
+    size_t used;
+  };
+  std::vector<Block> blocks_;
+  size_t cur_ = 0;
+  size_t block_bytes_ = size_t(2) << 30;
+  size_t budget_ = size_t(120) << 30;
+  size_t total_ = 0;
+};
+
+struct SurfaceRec {
+  int ivec[7];
+  int zero, rat, du, dv;
+  float *U32 = nullptr, *V32 = nullptr;
+  double *U64 = nullptr, *V64 = nullptr;
+  Vec4<float> *cpw32 = nullptr;
+  Vec4<double> *cpw64 = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct jsi_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Arena arena;
+  std::mutex mu;
+  std::string last_error;
+  std::map<int, SurfaceRec> surfaces;
+  int next_id = 1;
+  size_t budget = size_t(120) << 30;
+  size_t resident = 0;
+  ScreenStats *d_stats = nullptr;
+  ScreenStats *h_stats = nullptr;
+};
+
+namespace {
+
+int record(jsi_context *ctx, int status, const std::string &msg) {
+  if (ctx) ctx->last_error = msg;
+  return status;
+}
+
+template <typename Fn>
+int guarded(jsi_context *ctx, Fn &&fn) {
+  try {
+    return fn();
+  } catch (const StatusError &e) {
+    return record(ctx, e.status, e.msg);
+  } catch (const CudaError &e) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at line %d", static_cast<int>(e.err),
+             cudaGetErrorString(e.err), e.what, e.line);
+    return record(ctx, JSI_ERR_CUDA, buf);
+  } catch (const std::bad_alloc &) {
+    return record(ctx, JSI_ERR_NOMEM, "host allocation failed");
+  }
+}
+
+template <typename T>
+SurfView<T> view(const SurfaceRec &s);
+template <>
+SurfView<float> view<float>(const SurfaceRec &s) {
+  SurfView<float> v;
+  v.degu = s.ivec[1];
+  v.ncpu = s.ivec[2];
+  v.nku = s.ivec[3];
+  v.degv = s.ivec[4];
+  v.ncpv = s.ivec[5];
+  v.nkv = s.ivec[6];
+  v.rat = s.rat;
+  v.zero = s.zero;
+  v.du = s.du;
+  v.dv = s.dv;
+  v.U = s.U32;
+  v.V = s.V32;
+  v.cpw = s.cpw32;
+  return v;
+}
+template <>
+SurfView<double> view<double>(const SurfaceRec &s) {
+  SurfView<double> v;
+  v.degu = s.ivec[1];
+  v.ncpu = s.ivec[2];
+  v.nku = s.ivec[3];
+  v.degv = s.ivec[4];
+  v.ncpv = s.ivec[5];
+  v.nkv = s.ivec[6];
+  v.rat = s.rat;
+  v.zero = s.zero;
+  v.du = s.du;
+  v.dv = s.dv;
+  v.U = s.U64;
+  v.V = s.V64;
+  v.cpw = s.cpw64;
+  return v;
+}
+
+int p1_of(const SurfaceRec &s) { return std::max(s.ivec[1], s.ivec[4]) + 1; }
+
+// Header validation.  Degrees >= 25 and non-flat surfaces with flags bits 2|3
+// are accepted and evaluate to zero records, as the reference does
+// (evaluation.cu:271-272).
+void check_surface(const int ivec[7], const float *data, int ndata) {
+  if (!ivec || !data) fail(JSI_ERR_INVALID, "null surface pointer");
+  const int degu = ivec[1], ncpu = ivec[2], nku = ivec[3], degv = ivec[4], ncpv = ivec[5], nkv = ivec[6];
+  if (degu < 0 || degv < 0 || ncpu < 1 || ncpv < 1) fail(JSI_ERR_SURFACE, "bad degree / control net size");
+  if (ncpu < degu + 1 || ncpv < degv + 1) fail(JSI_ERR_SURFACE, "control net smaller than degree + 1");
+  if (nku != ncpu + degu + 1 || nkv != ncpv + degv + 1) fail(JSI_ERR_SURFACE, "knot count != nCP + degree + 1");
+  const long long ncp = static_cast<long long>(ncpu) * ncpv;
+  const long long need = nku + nkv + 3 * ncp + ((ivec[0] & 2) ? ncp : 0);
+  if (ndata < need) fail(JSI_ERR_SURFACE, "ndata %d < %lld required by the header", ndata, need);
+}
+
+SurfaceRec upload_surface(jsi_context *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
+  check_surface(ivec, data, ndata);
+  SurfaceRec s;
+  std::memcpy(s.ivec, ivec, sizeof(s.ivec));
+  const int flags = ivec[0];
+  s.rat = (flags & 2) ? 1 : 0;
+  s.zero = ((!(flags & 1)) && (flags & 12)) || ivec[1] >= kMaxDeg || ivec[4] >= kMaxDeg;
+  s.du = std::min(2, ivec[1]);
+  s.dv = std::min(2, ivec[4]);
+  const int nku = ivec[3], nkv = ivec[6];
+  const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
+  const float *cp = data + nku + nkv;
+  std::vector<Vec4<float>> c32(ncp);
+  std::vector<Vec4<double>> c64(ncp);
+  std::vector<double> u64(data, data + nku), v64(data + nku, data + nku + nkv);
+  for (size_t q = 0; q < ncp; ++q) {
+    const float w = s.rat ? cp[3 * ncp + q] : 1.0f;
+    c32[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
+    c64[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
+  }
+  s.bytes = nku * 12 + nkv * 12 + ncp * (sizeof(Vec4<float>) + sizeof(Vec4<double>));
+  auto dalloc = [&](size_t bytes) -> void * {
+    if (arena) return arena->alloc(bytes);
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      fail(JSI_ERR_NOMEM, "cudaMalloc for a surface failed");
+    }
+    return p;
+  };
+  s.U32 = static_cast<float *>(dalloc(nku * sizeof(float)));
+  s.V32 = static_cast<float *>(dalloc(nkv * sizeof(float)));
+  s.U64 = static_cast<double *>(dalloc(nku * sizeof(double)));
+  s.V64 = static_cast<double *>(dalloc(nkv * sizeof(double)));
+  s.cpw32 = static_cast<Vec4<float> *>(dalloc(ncp * sizeof(Vec4<float>)));
+  s.cpw64 = static_cast<Vec4<double> *>(dalloc(ncp * sizeof(Vec4<double>)));
+  cudaStream_t st = ctx->stream;
+  JSI_CUDA(cudaMemcpyAsync(s.U32, data, nku * sizeof(float), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(s.V32, data + nku, nkv * sizeof(float), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(s.U64, u64.data(), nku * sizeof(double), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(s.V64, v64.data(), nkv * sizeof(double), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(s.cpw32, c32.data(), ncp * sizeof(Vec4<float>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(s.cpw64, c64.data(), ncp * sizeof(Vec4<double>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaStreamSynchronize(st));
+  return s;
+}
+
+void free_surface(SurfaceRec &s) {
+  cudaFree(s.U32);
+  cudaFree(s.V32);
+  cudaFree(s.U64);
+  cudaFree(s.V64);
+  cudaFree(s.cpw32);
+  cudaFree(s.cpw64);
+}
+
+const SurfaceRec &get_surface(jsi_context *ctx, jsi_surface_id id) {
+  auto it = ctx->surfaces.find(id);
+  if (it == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
+  return it->second;
+}
+
+// Allocates one side's per-round arrays for nreg regions.
+template <typename T>
+SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, RegionRec<T> *regions) {
+  SideRound<T> s{};
+  s.g = g;
+  s.nreg = nreg;
+  s.regions = regions ? regions : ar.get<RegionRec<T>>(nreg);
+  s.spans = ar.get<int>(static_cast<size_t>(nreg) * 2 * g.nuv);
+  s.basis = ar.get<T>(static_cast<size_t>(nreg) * 2 * g.nuv * 3 * g.p1max);
+  s.samples = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv);
+  s.kmax = ar.get<unsigned long long>(static_cast<size_t>(nreg) * 3);
+  s.pad = ar.get<T>(nreg);
+  s.center = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.cpr);
+  s.half = intersect ? ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.cpr) : nullptr;
+  s.tlo = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
+  s.thi = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
+  s.thmax = intersect ? ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles) : nullptr;
+  return s;
+}
+
+// Evaluation + cell + tile build of one side (run_evaluation_and_construction_task,
+// distance_analysis.cu:88-116 / intersection.cu:175-219).
+template <typename T>
+void build_side(jsi_context *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect, bool use_k, T span_u0,
+                T span_v0) {
+  cudaStream_t st = ctx->stream;
+  const bool need_k = intersect && use_k;
+  launch_basis(v, s, st);
+  if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
+  launch_samples(v, s, need_k, st);
+  launch_pad(s, need_k, span_u0, span_v0, st);
+  launch_cells(s, intersect, st);
+  launch_tiles(s, st);
+  JSI_CUDA(cudaGetLastError());
+}
+
+void reset_stats(jsi_context *ctx) {
+  ScreenStats z{};
+  z.tau_bits = 0x7f800000u;
+  *ctx->h_stats = z;
+  JSI_CUDA(cudaMemcpyAsync(ctx->d_stats, ctx->h_stats, sizeof(ScreenStats), cudaMemcpyHostToDevice, ctx->stream));
+}
+
+void pull_stats(jsi_context *ctx) {
+  JSI_CUDA(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(ScreenStats), cudaMemcpyDeviceToHost, ctx->stream));
+  JSI_CUDA(cudaStreamSynchronize(ctx->stream));
+  JSI_CUDA(cudaGetLastError());
+}
+
+int bit_width(unsigned long long x) {
+  int b = 0;
+  while (x) {
+    ++b;
+    x >>= 1;
+  }
+  return b;
+}
+
+template <typename T>
+void check_task(const jsi_task *t) {
+  if (!t) fail(JSI_ERR_INVALID, "null task");
+  if (t->nuv < 2 || t->nuv > 4096) fail(JSI_ERR_INVALID, "task nuv %d outside [2, 4096]", t->nuv);
+}
+
+constexpr unsigned long long kMaxTilePairs = 1ull << 27;
+
+// ---------------------------------------------------------------------------
+// minimum_distance
+// ---------------------------------------------------------------------------
+template <typename T>
+void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_dist_params *p,
+                  jsi_dist_result *out) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  const SurfaceRec &sa = get_surface(ctx, ta->surface);
+  const SurfaceRec &sb = get_surface(ctx, tb->surface);
+  const SurfView<T> va = view<T>(sa), vb = view<T>(sb);
+  const int k = p->k;
+  RegionRec<T> roots[2] = {{T(ta->ustart), T(ta->vstart), T(ta->ustop), T(ta->vstop)},
+                           {T(tb->ustart), T(tb->vstart), T(tb->ustop), T(tb->vstop)}};
+  RegionRec<T> *dreg = ar.get<RegionRec<T>>(2);
+  int *dmap = ar.get<int>(2);
+  const int zeros[2] = {0, 0};
+  JSI_CUDA(cudaMemcpyAsync(dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  SideRound<T> A = make_side<T>(ar, make_geom(ta->nuv, p1_of(sa)), 1, false, dreg);
+  SideRound<T> B = make_side<T>(ar, make_geom(tb->nuv, p1_of(sb)), 1, false, dreg + 1);
+  const int *map1 = dmap, *map2 = dmap + 1;
+  int nslots = 1;
+  DistCand<T> *top = ar.get<DistCand<T>>(kMaxK);
+  std::vector<DistCand<T>> htop(kMaxK);
+  int round = 0;
+  for (round = 1; round <= p->rounds; ++round) {
+    build_side(ctx, va, A, false, false, T(1), T(1));
+    build_side(ctx, vb, B, false, false, T(1), T(1));
+    const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
+    if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+    unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+    unsigned long long cand_cap = 1ull << 20;
+    DistCand<T> *cand = ar.get<DistCand<T>>(cand_cap);
+    reset_stats(ctx);
+    launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, st);
+    launch_dist_cull(A, B, map1, map2, nslots, surv, tile_pairs, ctx->d_stats, st);
+    pull_stats(ctx);
+    const unsigned long long nsurv = ctx->h_stats->survivors;
+    for (int attempt = 0;; ++attempt) {
+      launch_dist_leaf(A, B, map1, map2, nslots, surv, nsurv, k, cand, cand_cap, ctx->d_stats, st);
+      launch_dist_select(cand, cand_cap, k, top, ctx->d_stats, st);
+      pull_stats(ctx);
+      ScreenStats &hs = *ctx->h_stats;
+      if (hs.candidates <= cand_cap && hs.status == 0) break;
+      if (attempt >= 4) fail(JSI_ERR_CAPACITY, "distance candidates did not fit after %d passes", attempt + 1);
+      // The leaf pass tightened tau: rerun it with the tighter bound.
+      if (hs.candidates > cand_cap) {
+        cand_cap = std::min<unsigned long long>(hs.candidates, 1ull << 26);
+        cand = ar.get<DistCand<T>>(cand_cap);
+      }
+      hs.candidates = 0;
+      hs.pair_tests = 0;
+      hs.status = 0;
+      JSI_CUDA(cudaMemcpyAsync(ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+    }
+    const ScreenStats hs = *ctx->h_stats;
+    const int n = hs.nsel;
+    out->npairs[round - 1] = n;
+    out->pair_tests[round - 1] = static_cast<long long>(hs.pair_tests);
+    out->candidates[round - 1] = static_cast<long long>(hs.candidates);
+    if (n > 0) {
+      JSI_CUDA(cudaMemcpyAsync(htop.data(), top, sizeof(DistCand<T>) * n, cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(cudaStreamSynchronize(st));
+      out->kth_d2[round - 1] = static_cast<double>(htop[n - 1].d2);
+      if (out->trace_pairs && static_cast<long long>(round) * k <= out->trace_cap) {
+        for (int q = 0; q < n; ++q) {
+          int *tp = out->trace_pairs + (static_cast<long long>(round - 1) * k + q) * 3;
+          tp[0] = htop[q].slot;
+          tp[1] = htop[q].i;
+          tp[2] = htop[q].j;
+        }
+      }
+    } else {
+      out->kth_d2[round - 1] = 0.0;
+    }
+    out->rounds_run = round;
+    if (n == 0 || round == p->rounds) {
+      const T kth = n > 0 ? htop[n - 1].d2 : T(0);
+      const T root = std::sqrt(kth);
+      out->v5_value = static_cast<float>(root);
+      out->distance = static_cast<double>(root);
+      break;
+    }
+    // Next round (nuv = next_nuv after round 1, distance_analysis.cu:389).
+    RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
+    int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
+    launch_dist_next(top, ctx->d_stats, A, B, map1, map2, p->nuv_refine, next1, next2, nmap1, nmap2, st);
+    pull_stats(ctx);
+    const int r1 = ctx->h_stats->nreg1, r2 = ctx->h_stats->nreg2;
+    A = make_side<T>(ar, make_geom(p->nuv_refine, p1_of(sa)), r1, false, next1);
+    B = make_side<T>(ar, make_geom(p->nuv_refine, p1_of(sb)), r2, false, next2);
+    map1 = nmap1;
+    map2 = nmap2;
+    nslots = n;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// intersection
+// ---------------------------------------------------------------------------
+template <typename T>
+void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
+                      jsi_inter_result *out) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  const SurfaceRec &sa = get_surface(ctx, ta->surface);
+  const SurfaceRec &sb = get_surface(ctx, tb->surface);
+  const SurfView<T> va = view<T>(sa), vb = view<T>(sb);
+  const bool use_k = p->use_k != 0;
+  // Initial spans per side (intersection.cu:344-347).
+  const T tiny = sizeof(T) == 4 ? T(1.0e-12f) : T(1.0e-12);
+  T span_u[3] = {T(1), T(1), T(1)}, span_v[3] = {T(1), T(1), T(1)};
+  span_u[1] = std::max(std::fabs(T(ta->ustop) - T(ta->ustart)), tiny);
+  span_v[1] = std::max(std::fabs(T(ta->vstop) - T(ta->vstart)), tiny);
+  span_u[2] = std::max(std::fabs(T(tb->ustop) - T(tb->ustart)), tiny);
+  span_v[2] = std::max(std::fabs(T(tb->vstop) - T(tb->vstart)), tiny);
+  const int side_a = ta->side == 2 ? 2 : 1, side_b = tb->side == 2 ? 2 : 1;
+
+  RegionRec<T> roots[2] = {{T(ta->ustart), T(ta->vstart), T(ta->ustop), T(ta->vstop)},
+                           {T(tb->ustart), T(tb->vstart), T(tb->ustop), T(tb->vstop)}};
+  RegionRec<T> *dreg = ar.get<RegionRec<T>>(2);
+  int *dmap = ar.get<int>(2);
+  const int zeros[2] = {0, 0};
+  JSI_CUDA(cudaMemcpyAsync(dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(cudaMemcpyAsync(dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  SideRound<T> A = make_side<T>(ar, make_geom(ta->nuv, p1_of(sa)), 1, true, dreg);
+  SideRound<T> B = make_side<T>(ar, make_geom(tb->nuv, p1_of(sb)), 1, true, dreg + 1);
+  const int *map1 = dmap, *map2 = dmap + 1;
+  long long nslots = 1;
+  int nuv = p->nuv_refine;
+  long long written = 0;
+  std::vector<unsigned long long> hkeys;
+  for (int round = 1; round <= p->rounds; ++round) {
+    const int sau = round == 1 ? side_a : 1, sbu = round == 1 ? side_b : 2;
+    build_side(ctx, va, A, true, use_k, span_u[sau], span_v[sau]);
+    build_side(ctx, vb, B, true, use_k, span_u[sbu], span_v[sbu]);
+    if (round == 1) {
+      T pads[2];
+      JSI_CUDA(cudaMemcpyAsync(&pads[0], A.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(cudaMemcpyAsync(&pads[1], B.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(cudaStreamSynchronize(st));
+      out->pad[0] = static_cast<double>(pads[0]);
+      out->pad[1] = static_cast<double>(pads[1]);
+    }
+    const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
+    if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+    const int ij_bits = std::max(1, bit_width(static_cast<unsigned long long>(
+                                            std::max(A.g.W * A.g.W, B.g.W * B.g.W) - 1)));
+    const int slot_bits = std::max(1, bit_width(static_cast<unsigned long long>(nslots - 1)));
+    if (2 * ij_bits + slot_bits > 64) fail(JSI_ERR_CAPACITY, "pair key does not fit 64 bits");
+    unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+    reset_stats(ctx);
+    launch_inter_cull(A, B, map1, map2, static_cast<int>(nslots), surv, tile_pairs, ctx->d_stats, st);
+    pull_stats(ctx);
+    const unsigned long long nsurv = ctx->h_stats->survivors;
+    unsigned long long key_cap = std::max<unsigned long long>(1ull << 16, std::min<unsigned long long>(nsurv * 64, 1ull << 24));
+    unsigned long long *keys = ar.get<unsigned long long>(key_cap);
+    for (int attempt = 0;; ++attempt) {
+      launch_inter_leaf(A, B, map1, map2, surv, nsurv, ij_bits, keys, key_cap, ctx->d_stats, st);
+      pull_stats(ctx);
+      ScreenStats &hs = *ctx->h_stats;
+      if (hs.candidates <= key_cap) break;
+      if (attempt >= 1) fail(JSI_ERR_CAPACITY, "overlap list overflow");
+      key_cap = hs.candidates;
+      keys = ar.get<unsigned long long>(key_cap);
+      hs.candidates = 0;
+      hs.pair_tests = 0;
+      JSI_CUDA(cudaMemcpyAsync(ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+    }
+    const long long n = static_cast<long long>(ctx->h_stats->candidates);
+    out->counts[round - 1] = n;
+    out->pair_tests[round - 1] = static_cast<long long>(ctx->h_stats->pair_tests);
+    out->regions1[round - 1] = A.nreg;
+    out->regions2[round - 1] = B.nreg;
+    out->rounds_run = round;
+    unsigned long long *sorted = keys;
+    if (n > 1) {
+      // (slot, i, j) order: slots concatenated in slot order, i-major, j ascending
+      // (intersection.cu:299-306).
+      const int end_bit = 2 * ij_bits + slot_bits;
+      unsigned long long *alt = ar.get<unsigned long long>(n);
+      size_t tmp_bytes = 0;
+      cub::DoubleBuffer<unsigned long long> db(keys, alt);
+      JSI_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
+      void *tmp = ar.alloc(tmp_bytes);
+      JSI_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
+      sorted = db.Current();
+    }
+    if (out->trace_pairs && n > 0) {
+      hkeys.resize(n);
+      JSI_CUDA(cudaMemcpyAsync(hkeys.data(), sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(cudaStreamSynchronize(st));
+      const unsigned long long mij = (1ull << ij_bits) - 1ull;
+      for (long long q = 0; q < n; ++q) {
+        if (written + q < out->trace_cap) {
+          int *tp = out->trace_pairs + (written + q) * 3;
+          tp[0] = static_cast<int>(hkeys[q] >> (2 * ij_bits));
+          tp[1] = static_cast<int>((hkeys[q] >> ij_bits) & mij);
+          tp[2] = static_cast<int>(hkeys[q] & mij);
+        }
+      }
+    }
+    written += n;
+    if (round == p->rounds || n == 0) break;
+    if (n > p->halve_threshold && nuv > p->min_nuv) nuv /= 2;  // intersection.cu:370
+    if (n > (1ll << 31) - 1) fail(JSI_ERR_CAPACITY, "too many pairs for the next round");
+    // Pair-preserving jobs and (slot, cell) dedup per side on the device.
+    unsigned long long *key2 = ar.get<unsigned long long>(n), *key2s = ar.get<unsigned long long>(n);
+    int *idx = ar.get<int>(n), *idxs = ar.get<int>(n);
+    unsigned *flag1 = ar.get<unsigned>(n), *ex1 = ar.get<unsigned>(n), *flag2 = ar.get<unsigned>(n),
+             *ex2 = ar.get<unsigned>(n);
+    launch_inter_prep(sorted, n, ij_bits, key2, idx, flag1, st);
+    size_t tb1 = 0, tb2 = 0, tb3 = 0;
+    JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb1, flag1, ex1, static_cast<int>(n), st));
+    JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key2, key2s, idx, idxs, static_cast<int>(n), 0,
+                                             ij_bits + slot_bits, st));
+    JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, flag2, ex2, static_cast<int>(n), st));
+    void *tmp = ar.alloc(std::max(tb1, std::max(tb2, tb3)));
+    size_t tbs = std::max(tb1, std::max(tb2, tb3));
+    JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag1, ex1, static_cast<int>(n), st));
+    tbs = std::max(tb1, std::max(tb2, tb3));
+    JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tbs, key2, key2s, idx, idxs, static_cast<int>(n), 0,
+                                             ij_bits + slot_bits, st));
+    launch_flag_runs(key2s, n, flag2, st);
+    tbs = std::max(tb1, std::max(tb2, tb3));
+    JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag2, ex2, static_cast<int>(n), st));
+    RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
+    int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
+    launch_inter_side1(sorted, n, ij_bits, flag1, ex1, A, map1, next1, nmap1, st);
+    launch_inter_side2(key2s, idxs, n, ij_bits, flag2, ex2, B, map2, next2, nmap2, st);
+    unsigned tail[4];
+    JSI_CUDA(cudaMemcpyAsync(&tail[0], ex1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(cudaMemcpyAsync(&tail[1], flag1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(cudaMemcpyAsync(&tail[2], ex2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(cudaMemcpyAsync(&tail[3], flag2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(cudaStreamSynchronize(st));
+    JSI_CUDA(cudaGetLastError());
+    const int r1 = static_cast<int>(tail[0] + tail[1]), r2 = static_cast<int>(tail[2] + tail[3]);
+    A = make_side<T>(ar, make_geom(nuv, p1_of(sa)), r1, true, next1);
+    B = make_side<T>(ar, make_geom(nuv, p1_of(sb)), r2, true, next2);
+    map1 = nmap1;
+    map2 = nmap2;
+    nslots = n;
+  }
+  out->trace_written = written;
+}
+
+void check_precision(int prec) {
+  if (prec != JSI_PREC_V5_FP32 && prec != JSI_PREC_FP64 && prec != JSI_PREC_FP32_SCREEN)
+    fail(JSI_ERR_INVALID, "unknown precision %d", prec);
+  if (prec == JSI_PREC_FP32_SCREEN) fail(JSI_ERR_UNSUPPORTED, "FP32-screen form not built yet");
+}
+
+}  // namespace
+
+extern "C" {
+
+int jsi_abi_version(void) { return JSI_B200_ABI_VERSION; }
+
+const char *jsi_status_string(int status) {
+  switch (status) {
+    case JSI_OK: return "ok";
+    case JSI_ERR_INVALID: return "invalid argument";
+    case JSI_ERR_CUDA: return "CUDA error";
+    case JSI_ERR_NOMEM: return "out of device memory / budget";
+    case JSI_ERR_CAPACITY: return "capacity exceeded";
+    case JSI_ERR_SURFACE: return "malformed surface";
+    case JSI_ERR_TIMEOUT: return "device wait timed out";
+    case JSI_ERR_UNSUPPORTED: return "unsupported";
+    case JSI_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char *jsi_last_error(const jsi_context *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int jsi_create(const jsi_config *cfg, jsi_context **out) {
+  if (!out) return JSI_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return JSI_ERR_NO_DEVICE;
+  }
+  const int dev = cfg ? cfg->device : 0;
+  if (dev < 0 || dev >= ndev) return JSI_ERR_INVALID;
+  jsi_context *ctx = new (std::nothrow) jsi_context();
+  if (!ctx) return JSI_ERR_NOMEM;
+  ctx->device = dev;
+  const size_t arena = (cfg && cfg->arena_bytes) ? cfg->arena_bytes : (size_t(2) << 30);
+  ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (size_t(120) << 30);
+  ctx->arena.configure(arena, ctx->budget);
+  const int st = guarded(ctx, [&]() {
+    JSI_CUDA(cudaSetDevice(dev));
+    JSI_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    JSI_CUDA(cudaEventCreate(&ctx->ev0));
+    JSI_CUDA(cudaEventCreate(&ctx->ev1));
+    JSI_CUDA(cudaMalloc(&ctx->d_stats, sizeof(ScreenStats)));
+    JSI_CUDA(cudaMallocHost(&ctx->h_stats, sizeof(ScreenStats)));
+    return JSI_OK;
+  });
+  if (st != JSI_OK) {
+    jsi_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return JSI_OK;
+}
+
+int jsi_destroy(jsi_context *ctx) {
+  if (!ctx) return JSI_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &kv : ctx->surfaces) free_surface(kv.second);
+  ctx->surfaces.clear();
+  if (ctx->d_stats) cudaFree(ctx->d_stats);
+  if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return JSI_OK;
+}
+
+int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, int ndata, jsi_surface_id *out) {
+  if (!ctx || !out) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    JSI_CUDA(cudaSetDevice(ctx->device));
+    check_surface(ivec, data, ndata);
+    SurfaceRec s = upload_surface(ctx, ivec, data, ndata, nullptr);
+    if (ctx->resident + s.bytes + ctx->arena.total() > ctx->budget) {
+      free_surface(s);
+      fail(JSI_ERR_NOMEM, "HBM budget exhausted by resident surfaces");
+    }
+    ctx->resident += s.bytes;
+    const int id = ctx->next_id++;
+    ctx->surfaces[id] = s;
+    *out = id;
+    return JSI_OK;
+  });
+}
+
+int jsi_surface_release(jsi_context *ctx, jsi_surface_id id) {
+  if (!ctx) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->surfaces.find(id);
+  if (it == ctx->surfaces.end()) return record(ctx, JSI_ERR_INVALID, "unknown surface id");
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->resident -= it->second.bytes;
+  free_surface(it->second);
+  ctx->surfaces.erase(it);
+  return JSI_OK;
+}
+
+int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out) {
+  if (!ctx || !out) return JSI_ERR_INVALID;
+  *out = ctx->resident;
+  return JSI_OK;
+}
+
+void jsi_dist_params_default(jsi_dist_params *p) {
+  if (!p) return;
+  p->nuv_refine = 16;
+  p->k = 8;
+  p->rounds = 4;
+  p->precision = JSI_PREC_V5_FP32;
+  p->newton = 0;
+}
+
+void jsi_inter_params_default(jsi_inter_params *p) {
+  if (!p) return;
+  p->nuv_refine = 16;
+  p->use_k = 1;
+  p->rounds = 6;
+  p->halve_threshold = 512;
+  p->min_nuv = 4;
+  p->precision = JSI_PREC_V5_FP32;
+}
+
+int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
+                     jsi_dist_result *out) {
+  if (!ctx || !a || !b || !out) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    jsi_dist_params p;
+    jsi_dist_params_default(&p);
+    if (params) p = *params;
+    if (p.k < 1 || p.k > kMaxK) fail(JSI_ERR_INVALID, "k = %d outside [1, %d]", p.k, kMaxK);
+    if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
+    if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
+    check_precision(p.precision);
+    if (p.newton) fail(JSI_ERR_UNSUPPORTED, "Newton refinement not built yet");
+    check_task<float>(a);
+    check_task<float>(b);
+    int *tp = out->trace_pairs;
+    const long long tc = out->trace_cap;
+    std::memset(out, 0, sizeof(*out));
+    out->trace_pairs = tp;
+    out->trace_cap = tc;
+    out->newton_distance = -1.0;
+    JSI_CUDA(cudaSetDevice(ctx->device));
+    ctx->arena.reset();
+    JSI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (p.precision == JSI_PREC_V5_FP32)
+      run_distance<float>(ctx, a, b, &p, out);
+    else
+      run_distance<double>(ctx, a, b, &p, out);
+    JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    JSI_CUDA(cudaEventSynchronize(ctx->ev1));
+    JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
+    return JSI_OK;
+  });
+}
+
+int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_inter_params *params,
+                  jsi_inter_result *out) {
+  if (!ctx || !a || !b || !out) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    jsi_inter_params p;
+    jsi_inter_params_default(&p);
+    if (params) p = *params;
+    if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
+    if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
+    if (p.min_nuv < 2) fail(JSI_ERR_INVALID, "min_nuv = %d", p.min_nuv);
+    check_precision(p.precision);
+    check_task<float>(a);
+    check_task<float>(b);
+    int *tp = out->trace_pairs;
+    const long long tc = out->trace_cap;
+    std::memset(out, 0, sizeof(*out));
+    out->trace_pairs = tp;
+    out->trace_cap = tc;
+    JSI_CUDA(cudaSetDevice(ctx->device));
+    ctx->arena.reset();
+    JSI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (p.precision == JSI_PREC_V5_FP32)
+      run_intersection<float>(ctx, a, b, &p, out);
+    else
+      run_intersection<double>(ctx, a, b, &p, out);
+    JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    JSI_CUDA(cudaEventSynchronize(ctx->ev1));
+    JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
+    return JSI_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+template <typename T>
+int eval_grid_impl(jsi_context *ctx, const int ivec[7], const float *data, int ndata, T ustep, T vstep, T ustart,
+                   T vstart, int nuv, T *results) {
+  if (!ctx || !results) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    if (nuv < 1 || nuv > 8192) fail(JSI_ERR_INVALID, "nuv = %d", nuv);
+    JSI_CUDA(cudaSetDevice(ctx->device));
+    ctx->arena.reset();
+    SurfaceRec s = upload_surface(ctx, ivec, data, ndata, &ctx->arena);
+    const size_t n = static_cast<size_t>(nuv) * nuv * 18;
+    T *d = ctx->arena.get<T>(n);
+    launch_records(view<T>(s), ustep, vstep, ustart, vstart, nuv, d, ctx->stream);
+    JSI_CUDA(cudaGetLastError());
+    JSI_CUDA(cudaMemcpyAsync(results, d, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    JSI_CUDA(cudaStreamSynchronize(ctx->stream));
+    return JSI_OK;
+  });
+}
+}  // namespace
+
+extern "C" {
+
+int jsi_eval_grid(jsi_context *ctx, const int ivec[7], const float *data, int ndata, float ustep, float vstep,
+                  float ustart, float vstart, int nuv, float *results) {
+  return eval_grid_impl<float>(ctx, ivec, data, ndata, ustep, vstep, ustart, vstart, nuv, results);
+}
+
+int jsi_eval_grid_f64(jsi_context *ctx, const int ivec[7], const float *data, int ndata, double ustep,
+                      double vstep, double ustart, double vstart, int nuv, double *results) {
+  return eval_grid_impl<double>(ctx, ivec, data, ndata, ustep, vstep, ustart, vstart, nuv, results);
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// Internal declarations shared by the kernels and the host orchestration.
+//
+// Layout in HBM (per round, per side):
+//   regions  RegionRec<T>[R]              parameter rectangle of each unique region
+//   spans    int[R][2][nuv]               knot span of every grid line (u lines, then v lines)
+//   basis    T[R][2][nuv][3][p1max]       basis values and 1st/2nd derivatives per line
+//   samples  T4[R][nuv*nuv]               P of every sample (x, y, z, 0), u fastest
+//   kmax     ordered bits[R][3]           max |Puu|, |Puv|, |Pvv| over the grid (curvature padding)
+//   cells    T4 centre[R][cpr], T4 half[R][cpr]
+//            tile-major: cpr = ntiles*te*te; tile (ty, tx) holds cells
+//            iv in [ty*te, ty*te+te), iu in [tx*te, tx*te+te) clipped to W
+//   tiles    T4 lo[R][ntiles], T4 hi[R][ntiles], T4 hmax[R][ntiles]
+// Cell id (the reference's bbox id) = iv * W + iu with W = nuv - 1.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace jsi {
+
+constexpr int kMaxDeg = 25;   // degrees >= kMaxDeg evaluate to zero records (evaluation.cu:13,272)
+constexpr int kMaxTile = 8;   // tile edge in cells
+constexpr int kMaxK = 1024;   // largest top-k supported
+constexpr int kSelectCap = 4096;  // entries the top-k select can sort on chip
+
+template <typename T>
+struct alignas(4 * sizeof(T) > 16 ? 16 : 4 * sizeof(T)) Vec4 {
+  T x, y, z, w;
+};
+
+// Surface as the kernels see it.  cpw = control points with weight,
+// (x, y, z, w) per point, u fastest; w = 1 for non-rational surfaces.
+template <typename T>
+struct SurfView {
+  int degu, degv, ncpu, ncpv, nku, nkv;
+  int rat;   // rational
+  int zero;  // every record is zero (evaluation.cu:271-272)
+  int du, dv;
+  const T *U;
+  const T *V;
+  const Vec4<T> *cpw;
+};
+
+template <typename T>
+struct RegionRec {
+  T u0, v0, u1, v1;
+};
+
+// Sampling geometry shared by all regions of one side in one round.
+struct Geom {
+  int nuv;    // samples per direction
+  int W;      // cells per direction
+  int te;     // tile edge
+  int tw;     // tiles per direction
+  int ntiles; // tw * tw
+  int cpr;    // padded cells per region = ntiles * te * te
+  int p1max;  // basis stride (max degree + 1)
+};
+
+inline Geom make_geom(int nuv, int p1max) {
+  Geom g;
+  g.nuv = nuv;
+  g.W = nuv - 1;
+  g.te = g.W < kMaxTile ? g.W : kMaxTile;
+  if (g.te < 1) g.te = 1;
+  g.tw = (g.W + g.te - 1) / g.te;
+  g.ntiles = g.tw * g.tw;
+  g.cpr = g.ntiles * g.te * g.te;
+  g.p1max = p1max;
+  return g;
+}
+
+// One side's data of one round.
+template <typename T>
+struct SideRound {
+  Geom g;
+  int nreg;
+  RegionRec<T> *regions;
+  int *spans;
+  T *basis;
+  Vec4<T> *samples;
+  unsigned long long *kmax;  // 3 per region, ordered bits of non-negative T
+  T *pad;                    // curvature padding per region
+  Vec4<T> *center;
+  Vec4<T> *half;
+  Vec4<T> *tlo;
+  Vec4<T> *thi;
+  Vec4<T> *thmax;
+};
+
+// Candidate of the distance screen.
+template <typename T>
+struct DistCand {
+  T d2;
+  int slot, i, j;
+};
+
+// Counters one screening round accumulates on the device.
+struct ScreenStats {
+  unsigned long long tile_pairs;    // tile pairs examined
+  unsigned long long survivors;     // tile pairs that passed the bound
+  unsigned long long pair_tests;    // cell pairs tested
+  unsigned long long candidates;    // cell pairs that passed the screen
+  unsigned int tau_bits;            // float bits of the current distance threshold
+  int status;                       // 0 ok, otherwise a jsi_status
+  int nsel;                         // pairs kept by the select
+  int nreg1, nreg2;                 // unique regions built for the next round
+  int pad_;
+};
+
+// ---- launchers (jsi_kernels.cu) ----
+template <typename T>
+void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st);
+template <typename T>
+void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st);
+template <typename T>
+void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaStream_t st);
+template <typename T>
+void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st);
+template <typename T>
+void launch_tiles(const SideRound<T> &sr, cudaStream_t st);
+template <typename T>
+void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st);
+
+template <typename T>
+void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                     int k, ScreenStats *stats, cudaStream_t st);
+template <typename T>
+void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                      unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st);
+template <typename T>
+void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                      const unsigned long long *surv, unsigned long long nsurv, int k, DistCand<T> *cand,
+                      unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st);
+template <typename T>
+void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
+                        ScreenStats *stats, cudaStream_t st);
+template <typename T>
+void launch_dist_next(const DistCand<T> *top, ScreenStats *stats, const SideRound<T> &a, const SideRound<T> &b,
+                      const int *map1, const int *map2, int nuv_next, RegionRec<T> *next1, RegionRec<T> *next2,
+                      int *nmap1, int *nmap2, cudaStream_t st);
+
+template <typename T>
+void launch_inter_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                       unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st);
+template <typename T>
+void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                       const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
+                       unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st);
+// Dedup of the next round's regions from sorted (slot, i, j) keys.
+void launch_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2, int *idx,
+                       unsigned *flag1, cudaStream_t st);
+void launch_flag_runs(const unsigned long long *sorted, long long n, unsigned *flags, cudaStream_t st);
+template <typename T>
+void launch_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
+                        const unsigned *ex1, const SideRound<T> &cur, const int *map1, RegionRec<T> *next,
+                        int *nmap1, cudaStream_t st);
+template <typename T>
+void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
+                        const unsigned *flag2, const unsigned *ex2, const SideRound<T> &cur, const int *map2,
+                        RegionRec<T> *next, int *nmap2, cudaStream_t st);
+
+}  // namespace jsi

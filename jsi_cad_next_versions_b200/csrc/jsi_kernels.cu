@@ -1,0 +1,1239 @@
+// sm_100a kernels of the NURBS distance / intersection query path.
+//
+// Every kernel is a template over the arithmetic type T (float for the
+// VERSION5-FP32 form, double for the plain FP64 form).  The library is built
+// with --fmad=false so that each written product and sum is rounded on its
+// own, in the operation order of the reference (JSI_CAD_NEXT_VERSION5); the
+// FP32 results are therefore bit-identical to the reference's x86 build.
+//
+// Work decomposition (B200: 148 SMs, 32-wide warps):
+//   k_basis     one thread per (region, direction, grid line)
+//   k_samples   one thread per (region, sample)
+//   k_cells     one thread per (region, padded tile-major cell)
+//   k_tiles     one thread per (region, tile)
+//   distance    k_dist_tau -> k_dist_cull -> k_dist_leaf -> k_dist_select -> k_dist_next
+//   intersect   k_inter_cull -> k_inter_leaf -> (device radix sort) -> k_inter_* dedup
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+
+#include "jsi_internal.h"
+
+namespace jsi {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T>
+__device__ __forceinline__ T tmin(T a, T b) {  // std::min
+  return (b < a) ? b : a;
+}
+template <typename T>
+__device__ __forceinline__ T tmax(T a, T b) {  // std::max
+  return (a < b) ? b : a;
+}
+
+__device__ __forceinline__ unsigned long long ordered_bits(float x) { return __float_as_uint(x); }
+__device__ __forceinline__ unsigned long long ordered_bits(double x) {
+  return static_cast<unsigned long long>(__double_as_longlong(x));
+}
+template <typename T>
+__device__ __forceinline__ T from_ordered(unsigned long long b);
+template <>
+__device__ __forceinline__ float from_ordered<float>(unsigned long long b) {
+  return __uint_as_float(static_cast<unsigned>(b));
+}
+template <>
+__device__ __forceinline__ double from_ordered<double>(unsigned long long b) {
+  return __longlong_as_double(static_cast<long long>(b));
+}
+
+// Upper bound of a non-negative value as float bits (for the shared threshold).
+__device__ __forceinline__ unsigned tau_bits_up(float x) { return __float_as_uint(x); }
+__device__ __forceinline__ unsigned tau_bits_up(double x) { return __float_as_uint(__double2float_ru(x)); }
+
+template <typename T>
+__device__ __forceinline__ T tau_value(unsigned bits) {
+  return static_cast<T>(__uint_as_float(bits));
+}
+
+// Warp-aggregated append: returns the slot of this lane or -1.
+__device__ __forceinline__ long long warp_append(bool pred, unsigned long long *counter) {
+  const unsigned mask = __ballot_sync(kFull, pred);
+  if (mask == 0) return -1;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(counter, static_cast<unsigned long long>(__popc(mask)));
+  base = __shfl_sync(kFull, base, leader);
+  if (!pred) return -1;
+  return static_cast<long long>(base + __popc(mask & ((1u << lane) - 1u)));
+}
+
+// ---------------------------------------------------------------------------
+// Knot spans and basis functions
+// ---------------------------------------------------------------------------
+
+// Knot-span binary search (evaluation.cu:152-166).
+template <typename T>
+__device__ int find_span(int nk, int p, T u, const T *knots) {
+  if (u <= knots[p]) return p;
+  const int n = nk - p - 1;
+  if (u >= knots[n]) return n - 1;
+  int lo = p, hi = n;
+  int mid = (lo + hi) / 2;
+  // The search interval halves every step; the bound only guards against
+  // non-monotone knot data (NaN).
+  for (int guard = 0; guard < 64 && (u < knots[mid] || u >= knots[mid + 1]); ++guard) {
+    if (u < knots[mid])
+      hi = mid;
+    else
+      lo = mid;
+    mid = (lo + hi) / 2;
+  }
+  return mid;
+}
+
+// Non-zero basis functions and derivatives up to order nd: the published
+// algorithm A2.3 (Piegl & Tiller, The NURBS Book), in the operation order of
+// evaluation.cu:168-219.  MAXP bounds the degree + 1 held in registers /
+// local memory.
+template <typename T, int MAXP>
+__device__ void basis_ders(int span, int p, T u, const T *knots, int nd, T *out, int stride) {
+  T ndu[MAXP][MAXP];
+  T left[MAXP], right[MAXP];
+  T a[2][MAXP];
+  ndu[0][0] = T(1);
+  for (int j = 1; j <= p; ++j) {
+    left[j] = u - knots[span + 1 - j];
+    right[j] = knots[span + j] - u;
+    T saved = T(0);
+    for (int r = 0; r < j; ++r) {
+      ndu[j][r] = right[r + 1] + left[j - r];
+      const T tmp = ndu[r][j - 1] / ndu[j][r];
+      ndu[r][j] = saved + right[r + 1] * tmp;
+      saved = left[j - r] * tmp;
+    }
+    ndu[j][j] = saved;
+  }
+  for (int j = 0; j <= p; ++j) out[j] = ndu[j][p];
+  for (int k = 1; k <= 2; ++k)
+    for (int j = 0; j <= p; ++j) out[k * stride + j] = T(0);
+  for (int r = 0; r <= p; ++r) {
+    int s1 = 0, s2 = 1;
+    a[0][0] = T(1);
+    for (int k = 1; k <= nd; ++k) {
+      T d = T(0);
+      const int rk = r - k, pk = p - k;
+      if (r >= k) {
+        a[s2][0] = a[s1][0] / ndu[pk + 1][rk];
+        d = a[s2][0] * ndu[rk][pk];
+      }
+      const int j1 = (rk >= -1) ? 1 : -rk;
+      const int j2 = (r - 1 <= pk) ? k - 1 : p - r;
+      for (int j = j1; j <= j2; ++j) {
+        a[s2][j] = (a[s1][j] - a[s1][j - 1]) / ndu[pk + 1][rk + j];
+        d += a[s2][j] * ndu[rk + j][pk];
+      }
+      if (r <= pk) {
+        a[s2][k] = -a[s1][k - 1] / ndu[pk + 1][r];
+        d += a[s2][k] * ndu[r][pk];
+      }
+      out[k * stride + r] = d;
+      const int t = s1;
+      s1 = s2;
+      s2 = t;
+    }
+  }
+  int fac = p;
+  for (int k = 1; k <= nd; ++k) {
+    for (int j = 0; j <= p; ++j) out[k * stride + j] *= static_cast<T>(fac);
+    fac *= p - k;
+  }
+}
+
+template <typename T, int MAXP>
+__global__ void k_basis(SurfView<T> s, const RegionRec<T> *regions, int nreg, int nuv, int p1max, int *spans,
+                        T *basis) {
+  const long long total = static_cast<long long>(nreg) * 2 * nuv;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int q = static_cast<int>(t % nuv);
+    const int dir = static_cast<int>((t / nuv) % 2);
+    const int r = static_cast<int>(t / (2LL * nuv));
+    const RegionRec<T> reg = regions[r];
+    const T lo = dir ? reg.v0 : reg.u0;
+    const T hi = dir ? reg.v1 : reg.u1;
+    // ustep = (ustop - ustart) / nuv; u = ustep * idx + ustart
+    // (distance_analysis.cu:92-93, evaluation.cu:366).
+    const T step = (hi - lo) / static_cast<T>(nuv);
+    const T x = step * static_cast<T>(q) + lo;
+    const int p = dir ? s.degv : s.degu;
+    const int nk = dir ? s.nkv : s.nku;
+    const T *knots = dir ? s.V : s.U;
+    const int nd = dir ? s.dv : s.du;
+    T *out = basis + t * 3 * p1max;
+    if (s.zero) {
+      spans[t] = p;
+      for (int j = 0; j < 3 * p1max; ++j) out[j] = T(0);
+      continue;
+    }
+    const int span = find_span(nk, p, x, knots);
+    spans[t] = span;
+    basis_ders<T, MAXP>(span, p, x, knots, nd, out, p1max);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Sample evaluation (evaluation.cu:259-356)
+// ---------------------------------------------------------------------------
+
+// Sum over the (q+1) x (p+1) window: for every row r, a u-direction sum over
+// the columns, then the v-direction sum over the rows, as the reference
+// orders it.  Non-rational: 3 channels.
+template <typename T>
+__device__ __forceinline__ void contract3(const SurfView<T> &s, int cu0, int cv0, const T *Nu, const T *Nv, T acc[3]) {
+  acc[0] = acc[1] = acc[2] = T(0);
+  for (int r = 0; r <= s.degv; ++r) {
+    T row0 = T(0), row1 = T(0), row2 = T(0);
+    const Vec4<T> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + r) + cu0;
+    for (int c = 0; c <= s.degu; ++c) {
+      const Vec4<T> q = cp[c];
+      const T n = Nu[c];
+      row0 += n * q.x;
+      row1 += n * q.y;
+      row2 += n * q.z;
+    }
+    const T m = Nv[r];
+    acc[0] += m * row0;
+    acc[1] += m * row1;
+    acc[2] += m * row2;
+  }
+}
+
+// Rational: homogeneous 4 channels, row terms (N * w) * coordinate.
+template <typename T>
+__device__ __forceinline__ void contract4(const SurfView<T> &s, int cu0, int cv0, const T *Nu, const T *Nv, T acc[4]) {
+  acc[0] = acc[1] = acc[2] = acc[3] = T(0);
+  for (int r = 0; r <= s.degv; ++r) {
+    T row0 = T(0), row1 = T(0), row2 = T(0), row3 = T(0);
+    const Vec4<T> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + r) + cu0;
+    for (int c = 0; c <= s.degu; ++c) {
+      const Vec4<T> q = cp[c];
+      const T nw = Nu[c] * q.w;
+      row0 += nw * q.x;
+      row1 += nw * q.y;
+      row2 += nw * q.z;
+      row3 += nw;
+    }
+    const T m = Nv[r];
+    acc[0] += m * row0;
+    acc[1] += m * row1;
+    acc[2] += m * row2;
+    acc[3] += m * row3;
+  }
+}
+
+// Homogeneous -> Euclidean up to order 2 (evaluation.cu:77-130 with
+// dim = 3, der_count = 2, stride = 4).  h: P, Pu, Pv, Puu, Puv, Pvv x 4.
+template <typename T>
+__device__ __forceinline__ void quotient2(T h[24]) {
+  const T inv = T(1) / h[3];
+#pragma unroll
+  for (int q = 0; q < 24; ++q) h[q] *= inv;
+  const T ws = -h[7], wt = -h[11];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h[4 + c] += ws * h[c];
+    h[8 + c] += wt * h[c];
+  }
+  const T wss = -h[15], wst = -h[19], wtt = -h[23];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T F = h[c], Fs = h[4 + c], Ft = h[8 + c];
+    h[12 + c] += wss * F + T(2) * ws * Fs;
+    h[16 + c] += wst * F + wt * Fs + ws * Ft;
+    h[20 + c] += wtt * F + T(2) * wt * Ft;
+  }
+}
+
+// Full 18-value record of one sample.
+template <typename T>
+__device__ void eval_record(const SurfView<T> &s, int spanu, const T *Nu, int spanv, const T *Nv, int p1, T out[18]) {
+#pragma unroll
+  for (int q = 0; q < 18; ++q) out[q] = T(0);
+  if (s.zero) return;
+  const int cu0 = spanu - s.degu, cv0 = spanv - s.degv;
+  // (k, l) = derivative order in (u, v); record slots P, Pu, Pv, Puu, Puv, Pvv.
+  const int ku[6] = {0, 1, 0, 2, 1, 0};
+  const int lv[6] = {0, 0, 1, 0, 1, 2};
+  if (!s.rat) {
+    for (int m = 0; m < 6; ++m) {
+      if (ku[m] > s.du || lv[m] > s.dv) continue;
+      T acc[3];
+      contract3(s, cu0, cv0, Nu + ku[m] * p1, Nv + lv[m] * p1, acc);
+      out[3 * m] = acc[0];
+      out[3 * m + 1] = acc[1];
+      out[3 * m + 2] = acc[2];
+    }
+    return;
+  }
+  T h[24];
+#pragma unroll
+  for (int q = 0; q < 24; ++q) h[q] = T(0);
+  for (int m = 0; m < 6; ++m) {
+    if (ku[m] > s.du || lv[m] > s.dv) continue;
+    T acc[4];
+    contract4(s, cu0, cv0, Nu + ku[m] * p1, Nv + lv[m] * p1, acc);
+    h[4 * m] = acc[0];
+    h[4 * m + 1] = acc[1];
+    h[4 * m + 2] = acc[2];
+    h[4 * m + 3] = acc[3];
+  }
+  quotient2(h);
+  for (int m = 0; m < 6; ++m)
+    for (int c = 0; c < 3; ++c) out[3 * m + c] = h[4 * m + c];
+}
+
+// Position only (bit-identical to the P of the full record).
+template <typename T>
+__device__ __forceinline__ void eval_point(const SurfView<T> &s, int spanu, const T *Nu, int spanv, const T *Nv,
+                                           T P[3]) {
+  P[0] = P[1] = P[2] = T(0);
+  if (s.zero) return;
+  const int cu0 = spanu - s.degu, cv0 = spanv - s.degv;
+  if (!s.rat) {
+    contract3(s, cu0, cv0, Nu, Nv, P);
+    return;
+  }
+  T acc[4];
+  contract4(s, cu0, cv0, Nu, Nv, acc);
+  const T inv = T(1) / acc[3];
+  P[0] = acc[0] * inv;
+  P[1] = acc[1] * inv;
+  P[2] = acc[2] * inv;
+}
+
+template <typename T>
+__device__ __forceinline__ void atomic_max_bits(unsigned long long *addr, T v) {
+  atomicMax(addr, ordered_bits(v));
+}
+
+template <typename T>
+__global__ void k_samples(SurfView<T> s, SideRound<T> sr, int need_k) {
+  const Geom g = sr.g;
+  const int nuv = g.nuv;
+  const long long per = static_cast<long long>(nuv) * nuv;
+  const long long total = per * sr.nreg;
+  const int p1 = g.p1max;
+  for (long long base = blockIdx.x * static_cast<long long>(blockDim.x); base < total;
+       base += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long t = base + threadIdx.x;
+    const bool live = t < total;
+    int r = 0;
+    T kuu = T(0), kuv = T(0), kvv = T(0);
+    if (live) {
+      r = static_cast<int>(t / per);
+      const int q = static_cast<int>(t % per);
+      const int idx = q % nuv, idy = q / nuv;
+      const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
+      const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
+      const T *Nu = sr.basis + lu * 3 * p1;
+      const T *Nv = sr.basis + lv * 3 * p1;
+      const int spanu = sr.spans[lu], spanv = sr.spans[lv];
+      Vec4<T> out;
+      if (need_k) {
+        T rec[18];
+        eval_record(s, spanu, Nu, spanv, Nv, p1, rec);
+        out.x = rec[0];
+        out.y = rec[1];
+        out.z = rec[2];
+        // max-abs component of Puu, Puv, Pvv (common.cu:155-161)
+        kuu = tmax(fabs(rec[9]), tmax(fabs(rec[10]), fabs(rec[11])));
+        kuv = tmax(fabs(rec[12]), tmax(fabs(rec[13]), fabs(rec[14])));
+        kvv = tmax(fabs(rec[15]), tmax(fabs(rec[16]), fabs(rec[17])));
+      } else {
+        T P[3];
+        eval_point(s, spanu, Nu, spanv, Nv, P);
+        out.x = P[0];
+        out.y = P[1];
+        out.z = P[2];
+      }
+      out.w = T(0);
+      sr.samples[t] = out;
+    }
+    if (need_k) {
+      // Max is exact and order-free: reduce within the warp when every lane
+      // sits in the same region, otherwise per lane.
+      const int r0 = __shfl_sync(kFull, r, 0);
+      const bool uniform = __all_sync(kFull, (!live) || r == r0);
+      if (uniform) {
+        for (int o = 16; o > 0; o >>= 1) {
+          kuu = tmax(kuu, __shfl_xor_sync(kFull, kuu, o));
+          kuv = tmax(kuv, __shfl_xor_sync(kFull, kuv, o));
+          kvv = tmax(kvv, __shfl_xor_sync(kFull, kvv, o));
+        }
+        if ((threadIdx.x & 31) == 0 && __any_sync(1u, true)) {
+          atomic_max_bits(&sr.kmax[3 * r0 + 0], kuu);
+          atomic_max_bits(&sr.kmax[3 * r0 + 1], kuv);
+          atomic_max_bits(&sr.kmax[3 * r0 + 2], kvv);
+        }
+      } else if (live) {
+        atomic_max_bits(&sr.kmax[3 * r + 0], kuu);
+        atomic_max_bits(&sr.kmax[3 * r + 1], kuv);
+        atomic_max_bits(&sr.kmax[3 * r + 2], kvv);
+      }
+    }
+  }
+}
+
+// Curvature padding per region (common.cu:149-172, intersection.cu:187-205).
+template <typename T>
+__global__ void k_pad(SideRound<T> sr, int use_k, T span_u0, T span_v0) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= sr.nreg) return;
+  T pad = T(0);
+  if (use_k) {
+    const T muu = from_ordered<T>(sr.kmax[3 * r + 0]);
+    const T muv = from_ordered<T>(sr.kmax[3 * r + 1]);
+    const T mvv = from_ordered<T>(sr.kmax[3 * r + 2]);
+    const int n = sr.g.nuv;
+    const int side = n > 1 ? n - 1 : 1;
+    const T ss = static_cast<T>(side * side);
+    const T raw = (muu / ss + T(2) * muv / ss + mvv / ss) / T(8);
+    const RegionRec<T> reg = sr.regions[r];
+    const T us = fabs(reg.u1 - reg.u0) / span_u0;
+    const T vs = fabs(reg.v1 - reg.v0) / span_v0;
+    const T ps = tmax(us, vs);
+    pad = raw * ps * ps;
+    if (!isfinite(pad) || pad < T(0)) pad = T(0);
+  }
+  sr.pad[r] = pad;
+}
+
+// Cell boxes from 4 corner samples, tile-major (distance_analysis.cu:45-86,
+// intersection.cu:106-148).  Half spans are stored without the padding; the
+// screen forms radius = half + pad exactly as the reference does.
+template <typename T>
+__global__ void k_cells(SideRound<T> sr, int intersect) {
+  const Geom g = sr.g;
+  const long long total = static_cast<long long>(sr.nreg) * g.cpr;
+  const int te2 = g.te * g.te;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(t / g.cpr);
+    const int c = static_cast<int>(t % g.cpr);
+    const int tile = c / te2, local = c % te2;
+    const int iv = (tile / g.tw) * g.te + local / g.te;
+    const int iu = (tile % g.tw) * g.te + local % g.te;
+    Vec4<T> cen{T(0), T(0), T(0), T(0)}, hal{T(0), T(0), T(0), T(0)};
+    if (iv < g.W && iu < g.W) {
+      const Vec4<T> *S = sr.samples + static_cast<long long>(r) * g.nuv * g.nuv;
+      const Vec4<T> p0 = S[iv * g.nuv + iu];
+      const Vec4<T> p1 = S[iv * g.nuv + iu + 1];
+      const Vec4<T> p2 = S[(iv + 1) * g.nuv + iu];
+      const Vec4<T> p3 = S[(iv + 1) * g.nuv + iu + 1];
+      const T lx = tmin(p0.x, tmin(p1.x, tmin(p2.x, p3.x)));
+      const T ly = tmin(p0.y, tmin(p1.y, tmin(p2.y, p3.y)));
+      const T lz = tmin(p0.z, tmin(p1.z, tmin(p2.z, p3.z)));
+      const T hx = tmax(p0.x, tmax(p1.x, tmax(p2.x, p3.x)));
+      const T hy = tmax(p0.y, tmax(p1.y, tmax(p2.y, p3.y)));
+      const T hz = tmax(p0.z, tmax(p1.z, tmax(p2.z, p3.z)));
+      if (intersect) {
+        cen.x = (lx + hx) / T(2);
+        cen.y = (ly + hy) / T(2);
+        cen.z = (lz + hz) / T(2);
+      } else {
+        cen.x = (lx - T(0) + hx + T(0)) / T(2);
+        cen.y = (ly - T(0) + hy + T(0)) / T(2);
+        cen.z = (lz - T(0) + hz + T(0)) / T(2);
+      }
+      hal.x = (hx - lx) / T(2);
+      hal.y = (hy - ly) / T(2);
+      hal.z = (hz - lz) / T(2);
+    }
+    sr.center[t] = cen;
+    if (intersect) sr.half[t] = hal;
+  }
+}
+
+// Tile bounds: range of the centres and max half span of every tile.
+template <typename T>
+__global__ void k_tiles(SideRound<T> sr) {
+  const Geom g = sr.g;
+  const long long total = static_cast<long long>(sr.nreg) * g.ntiles;
+  const int te2 = g.te * g.te;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int tile = static_cast<int>(t % g.ntiles);
+    const int ty = tile / g.tw, tx = tile % g.tw;
+    const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
+    const Vec4<T> *C = sr.center + t * te2;
+    const Vec4<T> *H = sr.half ? sr.half + t * te2 : nullptr;
+    Vec4<T> lo{T(0), T(0), T(0), T(0)}, hi{T(0), T(0), T(0), T(0)}, hm{T(0), T(0), T(0), T(0)};
+    bool first = true;
+    for (int a = 0; a < nv; ++a) {
+      for (int b = 0; b < nu; ++b) {
+        const Vec4<T> c = C[a * g.te + b];
+        if (first) {
+          lo = c;
+          hi = c;
+          first = false;
+        } else {
+          lo.x = tmin(lo.x, c.x);
+          lo.y = tmin(lo.y, c.y);
+          lo.z = tmin(lo.z, c.z);
+          hi.x = tmax(hi.x, c.x);
+          hi.y = tmax(hi.y, c.y);
+          hi.z = tmax(hi.z, c.z);
+        }
+        if (H) {
+          const Vec4<T> h = H[a * g.te + b];
+          hm.x = tmax(hm.x, h.x);
+          hm.y = tmax(hm.y, h.y);
+          hm.z = tmax(hm.z, h.z);
+        }
+      }
+    }
+    sr.tlo[t] = lo;
+    sr.thi[t] = hi;
+    if (sr.thmax) sr.thmax[t] = hm;
+  }
+}
+
+template <typename T>
+__global__ void k_records(SurfView<T> s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out) {
+  // Full-record grid for the evalWithCuda entry point; basis per sample.
+  const long long total = static_cast<long long>(nuv) * nuv;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int idx = static_cast<int>(t % nuv), idy = static_cast<int>(t / nuv);
+    const T u = ustep * static_cast<T>(idx) + ustart;
+    const T v = vstep * static_cast<T>(idy) + vstart;
+    T Nu[3 * kMaxDeg], Nv[3 * kMaxDeg];
+    T rec[18];
+    int spanu = s.degu, spanv = s.degv;
+    if (!s.zero) {
+      spanu = find_span(s.nku, s.degu, u, s.U);
+      basis_ders<T, kMaxDeg>(spanu, s.degu, u, s.U, s.du, Nu, kMaxDeg);
+      spanv = find_span(s.nkv, s.degv, v, s.V);
+      basis_ders<T, kMaxDeg>(spanv, s.degv, v, s.V, s.dv, Nv, kMaxDeg);
+    }
+    eval_record(s, spanu, Nu, spanv, Nv, kMaxDeg, rec);
+    T *o = out + t * 18;
+    for (int q = 0; q < 18; ++q) o[q] = rec[q];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Screening helpers
+// ---------------------------------------------------------------------------
+
+struct PairDecode {
+  int slot, t1, t2;
+};
+
+__device__ __forceinline__ PairDecode decode_pair(unsigned long long q, int nt1, int nt2) {
+  const unsigned long long per = static_cast<unsigned long long>(nt1) * nt2;
+  PairDecode d;
+  d.slot = static_cast<int>(q / per);
+  const unsigned long long rem = q % per;
+  d.t1 = static_cast<int>(rem / nt2);
+  d.t2 = static_cast<int>(rem % nt2);
+  return d;
+}
+
+// Squared centre distance, distance_analysis.cu:202-207.
+template <typename T>
+__device__ __forceinline__ T center_d2(const Vec4<T> &a, const Vec4<T> &b) {
+  const T dx = a.x - b.x;
+  const T dy = a.y - b.y;
+  const T dz = a.z - b.z;
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// Gap between two centre ranges on one axis; rounding is monotone, so the
+// rounded gap never exceeds the rounded |c1 - c2| of any member pair.
+template <typename T>
+__device__ __forceinline__ T axis_gap(T lo1, T hi1, T lo2, T hi2) {
+  const T g1 = lo2 - hi1;
+  const T g2 = lo1 - hi2;
+  return tmax(tmax(g1, g2), T(0));
+}
+
+// Lower bound of every rounded d2 between members of two tiles.
+template <typename T>
+__device__ __forceinline__ T tile_lb(const Vec4<T> &lo1, const Vec4<T> &hi1, const Vec4<T> &lo2, const Vec4<T> &hi2) {
+  const T gx = axis_gap(lo1.x, hi1.x, lo2.x, hi2.x);
+  const T gy = axis_gap(lo1.y, hi1.y, lo2.y, hi2.y);
+  const T gz = axis_gap(lo1.z, hi1.z, lo2.z, hi2.z);
+  return gx * gx + gy * gy + gz * gz;
+}
+
+__device__ __forceinline__ int tile_extent(int t, int tw, int te, int W, int axis_v) {
+  const int c = axis_v ? t / tw : t % tw;
+  return min(te, W - c * te);
+}
+
+// Bitonic sort of n (power of two) unsigned keys in shared memory, ascending.
+__device__ void bitonic_u32(unsigned *a, int n) {
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const unsigned x = a[i], y = a[j];
+          if ((x > y) == up) {
+            a[i] = y;
+            a[j] = x;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Block-wide: k-th smallest of the per-thread minima (distinct pairs), as a
+// valid upper bound of the k-th smallest d2 over all pairs, folded into tau.
+__device__ void fold_tau(unsigned my_bits, int k, unsigned *tau, unsigned *sh) {
+  const int n = blockDim.x;  // power of two
+  sh[threadIdx.x] = my_bits;
+  bitonic_u32(sh, n);
+  if (threadIdx.x == 0 && k <= n) {
+    const unsigned b = sh[k - 1];
+    if (b != 0x7f800000u) atomicMin(tau, b);
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Distance screening
+// ---------------------------------------------------------------------------
+
+// Threshold seed: representative cell pair (the centre cells of both tiles)
+// of every tile pair; each block folds the k-th smallest of its per-thread
+// minima into tau.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_dist_tau(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
+                                                   int nslots, int k, ScreenStats *stats, int per_thread) {
+  __shared__ unsigned sh[1024];
+  const Geom g1 = a.g, g2 = b.g;
+  const unsigned long long total = static_cast<unsigned long long>(nslots) * g1.ntiles * g2.ntiles;
+  const unsigned long long chunk = static_cast<unsigned long long>(blockDim.x) * per_thread;
+  const unsigned long long start = blockIdx.x * chunk;
+  float best = __uint_as_float(0x7f800000u);
+  for (int it = 0; it < per_thread; ++it) {
+    const unsigned long long q = start + static_cast<unsigned long long>(it) * blockDim.x + threadIdx.x;
+    if (q >= total) break;
+    const PairDecode d = decode_pair(q, g1.ntiles, g2.ntiles);
+    const int r1 = map1[d.slot], r2 = map2[d.slot];
+    const int nv1 = tile_extent(d.t1, g1.tw, g1.te, g1.W, 1), nu1 = tile_extent(d.t1, g1.tw, g1.te, g1.W, 0);
+    const int nv2 = tile_extent(d.t2, g2.tw, g2.te, g2.W, 1), nu2 = tile_extent(d.t2, g2.tw, g2.te, g2.W, 0);
+    const int l1 = (nv1 / 2) * g1.te + nu1 / 2, l2 = (nv2 / 2) * g2.te + nu2 / 2;
+    const Vec4<T> c1 = a.center[(static_cast<long long>(r1) * g1.ntiles + d.t1) * g1.te * g1.te + l1];
+    const Vec4<T> c2 = b.center[(static_cast<long long>(r2) * g2.ntiles + d.t2) * g2.te * g2.te + l2];
+    const T d2 = center_d2(c1, c2);
+    const float up = __uint_as_float(tau_bits_up(d2));
+    best = fminf(best, up);
+  }
+  fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+}
+
+template <typename T>
+__global__ void k_dist_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
+                            unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats) {
+  const Geom g1 = a.g, g2 = b.g;
+  const unsigned long long total = static_cast<unsigned long long>(nslots) * g1.ntiles * g2.ntiles;
+  const T tau = tau_value<T>(stats->tau_bits);
+  for (unsigned long long base = blockIdx.x * static_cast<unsigned long long>(blockDim.x); base < total;
+       base += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long q = base + threadIdx.x;
+    bool keep = false;
+    if (q < total) {
+      const PairDecode d = decode_pair(q, g1.ntiles, g2.ntiles);
+      const long long i1 = static_cast<long long>(map1[d.slot]) * g1.ntiles + d.t1;
+      const long long i2 = static_cast<long long>(map2[d.slot]) * g2.ntiles + d.t2;
+      const T lb = tile_lb(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
+      keep = lb <= tau;
+    }
+    const long long pos = warp_append(keep, &stats->survivors);
+    if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap) surv[pos] = q;
+  }
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&stats->tile_pairs, total);
+}
+
+// All cell pairs of the surviving tile pairs: d2 <= tau is a candidate.
+template <typename T>
+__global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
+                                                   const unsigned long long *surv, unsigned long long nsurv, int k,
+                                                   DistCand<T> *cand, unsigned long long cand_cap,
+                                                   ScreenStats *stats) {
+  __shared__ Vec4<T> s1[kMaxTile * kMaxTile], s2[kMaxTile * kMaxTile];
+  __shared__ unsigned sh[256];
+  const Geom g1 = a.g, g2 = b.g;
+  const int te1 = g1.te, te2 = g2.te;
+  const int n1 = te1 * te1, n2 = te2 * te2;
+  unsigned long long tests = 0;
+  float best = __uint_as_float(0x7f800000u);
+  for (unsigned long long w = blockIdx.x; w < nsurv; w += gridDim.x) {
+    const PairDecode d = decode_pair(surv[w], g1.ntiles, g2.ntiles);
+    const long long base1 = (static_cast<long long>(map1[d.slot]) * g1.ntiles + d.t1) * n1;
+    const long long base2 = (static_cast<long long>(map2[d.slot]) * g2.ntiles + d.t2) * n2;
+    __syncthreads();
+    for (int q = threadIdx.x; q < n1; q += blockDim.x) s1[q] = a.center[base1 + q];
+    for (int q = threadIdx.x; q < n2; q += blockDim.x) s2[q] = b.center[base2 + q];
+    __syncthreads();
+    const T tau = tau_value<T>(*reinterpret_cast<volatile unsigned *>(&stats->tau_bits));
+    const int nv1 = tile_extent(d.t1, g1.tw, te1, g1.W, 1), nu1 = tile_extent(d.t1, g1.tw, te1, g1.W, 0);
+    const int nv2 = tile_extent(d.t2, g2.tw, te2, g2.W, 1), nu2 = tile_extent(d.t2, g2.tw, te2, g2.W, 0);
+    const int ty1 = d.t1 / g1.tw, tx1 = d.t1 % g1.tw, ty2 = d.t2 / g2.tw, tx2 = d.t2 % g2.tw;
+    const int npair = n1 * n2;
+    for (int p0 = 0; p0 < npair; p0 += blockDim.x) {
+      const int p = p0 + threadIdx.x;
+      bool hit = false;
+      T d2 = T(0);
+      int ci = 0, cj = 0;
+      if (p < npair) {
+        const int l1 = p / n2, l2 = p % n2;
+        const int a1 = l1 / te1, b1 = l1 % te1, a2 = l2 / te2, b2 = l2 % te2;
+        if (a1 < nv1 && b1 < nu1 && a2 < nv2 && b2 < nu2) {
+          ++tests;
+          d2 = center_d2(s1[l1], s2[l2]);
+          best = fminf(best, __uint_as_float(tau_bits_up(d2)));
+          hit = d2 <= tau;
+          ci = (ty1 * te1 + a1) * g1.W + tx1 * te1 + b1;
+          cj = (ty2 * te2 + a2) * g2.W + tx2 * te2 + b2;
+        }
+      }
+      const long long pos = warp_append(hit, &stats->candidates);
+      if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap) {
+        DistCand<T> c;
+        c.d2 = d2;
+        c.slot = d.slot;
+        c.i = ci;
+        c.j = cj;
+        cand[pos] = c;
+      }
+    }
+  }
+  atomicAdd(&stats->pair_tests, tests);
+  fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+}
+
+// Total order of the top-k (distance_analysis.cu:226-231).
+template <typename T>
+__device__ __forceinline__ bool cand_less(const DistCand<T> &x, const DistCand<T> &y) {
+  if (x.d2 != y.d2) return x.d2 < y.d2;
+  if (x.slot != y.slot) return x.slot < y.slot;
+  if (x.i != y.i) return x.i < y.i;
+  return x.j < y.j;
+}
+
+// Exact k smallest candidates under the total order, one block of 1024.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k,
+                                                      DistCand<T> *out, ScreenStats *stats) {
+  extern __shared__ unsigned char smem_raw[];
+  DistCand<T> *buf = reinterpret_cast<DistCand<T> *>(smem_raw);
+  __shared__ unsigned hist[256];
+  __shared__ unsigned long long s_prefix, s_mask;
+  __shared__ int s_need, s_count;
+  const unsigned long long total = stats->candidates;
+  if (total > cand_cap) {
+    if (threadIdx.x == 0) stats->status = -4;
+    return;
+  }
+  const int m = static_cast<int>(total);
+  constexpr int kBits = sizeof(T) * 8;
+  unsigned long long kth_bits = ~0ull;
+  if (m > k) {
+    // MSD radix select of the k-th smallest d2 (non-negative: bits are ordered).
+    if (threadIdx.x == 0) {
+      s_prefix = 0;
+      s_mask = 0;
+      s_need = k;
+    }
+    for (int shift = kBits - 8; shift >= 0; shift -= 8) {
+      for (int q = threadIdx.x; q < 256; q += blockDim.x) hist[q] = 0;
+      __syncthreads();
+      const unsigned long long prefix = s_prefix, mask = s_mask;
+      for (int e = threadIdx.x; e < m; e += blockDim.x) {
+        const unsigned long long bits = ordered_bits(cand[e].d2);
+        if ((bits & mask) == prefix) atomicAdd(&hist[(bits >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int need = s_need;
+        int dgt = 0;
+        for (; dgt < 256; ++dgt) {
+          if (static_cast<int>(hist[dgt]) >= need) break;
+          need -= hist[dgt];
+        }
+        s_need = need;
+        s_prefix = prefix | (static_cast<unsigned long long>(dgt) << shift);
+        s_mask = mask | (255ull << shift);
+      }
+      __syncthreads();
+    }
+    kth_bits = s_prefix;
+  }
+  if (threadIdx.x == 0) s_count = 0;
+  __syncthreads();
+  for (int e = threadIdx.x; e < m; e += blockDim.x) {
+    const DistCand<T> c = cand[e];
+    if (ordered_bits(c.d2) <= kth_bits) {
+      const int pos = atomicAdd(&s_count, 1);
+      if (pos < kSelectCap) buf[pos] = c;
+    }
+  }
+  __syncthreads();
+  const int cnt = s_count;
+  if (cnt > kSelectCap) {
+    if (threadIdx.x == 0) stats->status = -4;
+    return;
+  }
+  int n2 = 1;
+  while (n2 < cnt) n2 <<= 1;
+  for (int e = cnt + threadIdx.x; e < n2; e += blockDim.x) {
+    DistCand<T> c;
+    c.d2 = from_ordered<T>(sizeof(T) == 4 ? 0x7f800000ull : 0x7ff0000000000000ull);
+    c.slot = INT_MAX;
+    c.i = INT_MAX;
+    c.j = INT_MAX;
+    buf[e] = c;
+  }
+  for (int size = 2; size <= n2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const DistCand<T> x = buf[i], y = buf[j];
+          if (cand_less(y, x) == up) {
+            buf[i] = y;
+            buf[j] = x;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const int keep = cnt < k ? cnt : k;
+  for (int e = threadIdx.x; e < keep; e += blockDim.x) out[e] = buf[e];
+  if (threadIdx.x == 0) stats->nsel = keep;
+}
+
+// Child rectangle of cell bbox of a region sampled at nuv_parent:
+// make_dist_refine_task / make_intersect_refine_task
+// (distance_analysis.cu:340-354, intersection.cu:311-325).
+template <typename T>
+__device__ __forceinline__ RegionRec<T> child_rect(const RegionRec<T> &p, int nuv_parent, int bbox) {
+  const T ustep = (p.u1 - p.u0) / static_cast<T>(nuv_parent);
+  const T vstep = (p.v1 - p.v0) / static_cast<T>(nuv_parent);
+  const int w = nuv_parent - 1;
+  const int x = bbox % w, y = bbox / w;
+  RegionRec<T> c;
+  c.u0 = p.u0 + ustep * static_cast<T>(x);
+  c.u1 = c.u0 + ustep;
+  c.v0 = p.v0 + vstep * static_cast<T>(y);
+  c.v1 = c.v0 + vstep;
+  return c;
+}
+
+// Pair-preserving refinement jobs with (slot, cell) dedup per side
+// (distance_analysis.cu:399-491): one block.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_dist_next(const DistCand<T> *top, ScreenStats *stats, SideRound<T> a,
+                                                    SideRound<T> b, const int *map1, const int *map2, int nuv_next,
+                                                    RegionRec<T> *next1, RegionRec<T> *next2, int *nmap1, int *nmap2) {
+  __shared__ int first1[kMaxK], first2[kMaxK];
+  __shared__ int uid1[kMaxK], uid2[kMaxK];
+  const int n = stats->nsel;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const DistCand<T> c = top[e];
+    int f1 = 1, f2 = 1;
+    for (int q = 0; q < e; ++q) {
+      const DistCand<T> o = top[q];
+      if (o.slot == c.slot && o.i == c.i) f1 = 0;
+      if (o.slot == c.slot && o.j == c.j) f2 = 0;
+    }
+    first1[e] = f1;
+    first2[e] = f2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int c1 = 0, c2 = 0;
+    for (int e = 0; e < n; ++e) {
+      uid1[e] = first1[e] ? c1++ : -1;
+      uid2[e] = first2[e] ? c2++ : -1;
+    }
+    stats->nreg1 = c1;
+    stats->nreg2 = c2;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const DistCand<T> c = top[e];
+    int u1 = uid1[e], u2 = uid2[e];
+    if (u1 < 0) {
+      for (int q = 0; q < e; ++q)
+        if (top[q].slot == c.slot && top[q].i == c.i) {
+          u1 = uid1[q];
+          break;
+        }
+    } else {
+      next1[u1] = child_rect(a.regions[map1[c.slot]], a.g.nuv, c.i);
+    }
+    if (u2 < 0) {
+      for (int q = 0; q < e; ++q)
+        if (top[q].slot == c.slot && top[q].j == c.j) {
+          u2 = uid2[q];
+          break;
+        }
+    } else {
+      next2[u2] = child_rect(b.regions[map2[c.slot]], b.g.nuv, c.j);
+    }
+    nmap1[e] = u1;
+    nmap2[e] = u2;
+  }
+  (void)nuv_next;
+}
+
+// ---------------------------------------------------------------------------
+// Intersection screening
+// ---------------------------------------------------------------------------
+
+// A tile pair is skipped only when, on some axis, the rounded gap between the
+// centre ranges reaches the rounded sum of the largest padded radii: then no
+// member pair passes the strict test of intersection.cu:60-62.
+template <typename T>
+__global__ void k_inter_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
+                             unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats) {
+  const Geom g1 = a.g, g2 = b.g;
+  const unsigned long long total = static_cast<unsigned long long>(nslots) * g1.ntiles * g2.ntiles;
+  for (unsigned long long base = blockIdx.x * static_cast<unsigned long long>(blockDim.x); base < total;
+       base += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long q = base + threadIdx.x;
+    bool keep = false;
+    if (q < total) {
+      const PairDecode d = decode_pair(q, g1.ntiles, g2.ntiles);
+      const int r1 = map1[d.slot], r2 = map2[d.slot];
+      const long long i1 = static_cast<long long>(r1) * g1.ntiles + d.t1;
+      const long long i2 = static_cast<long long>(r2) * g2.ntiles + d.t2;
+      const Vec4<T> lo1 = a.tlo[i1], hi1 = a.thi[i1], h1 = a.thmax[i1];
+      const Vec4<T> lo2 = b.tlo[i2], hi2 = b.thi[i2], h2 = b.thmax[i2];
+      const T p1 = a.pad[r1], p2 = b.pad[r2];
+      const bool sx = axis_gap(lo1.x, hi1.x, lo2.x, hi2.x) >= (h1.x + p1) + (h2.x + p2);
+      const bool sy = axis_gap(lo1.y, hi1.y, lo2.y, hi2.y) >= (h1.y + p1) + (h2.y + p2);
+      const bool sz = axis_gap(lo1.z, hi1.z, lo2.z, hi2.z) >= (h1.z + p1) + (h2.z + p2);
+      keep = !(sx || sy || sz);
+    }
+    const long long pos = warp_append(keep, &stats->survivors);
+    if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap) surv[pos] = q;
+  }
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&stats->tile_pairs, total);
+}
+
+// Strict per-axis overlap of every cell pair of the surviving tile pairs
+// (intersection.cu:46-63); hits are appended as (slot, i, j) sort keys.
+template <typename T>
+__global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T> b, const int *map1,
+                                                    const int *map2, const unsigned long long *surv,
+                                                    unsigned long long nsurv, int ij_bits, unsigned long long *keys,
+                                                    unsigned long long key_cap, ScreenStats *stats) {
+  __shared__ Vec4<T> c1s[kMaxTile * kMaxTile], c2s[kMaxTile * kMaxTile];
+  __shared__ Vec4<T> r1s[kMaxTile * kMaxTile], r2s[kMaxTile * kMaxTile];
+  const Geom g1 = a.g, g2 = b.g;
+  const int te1 = g1.te, te2 = g2.te;
+  const int n1 = te1 * te1, n2 = te2 * te2;
+  unsigned long long tests = 0;
+  for (unsigned long long w = blockIdx.x; w < nsurv; w += gridDim.x) {
+    const PairDecode d = decode_pair(surv[w], g1.ntiles, g2.ntiles);
+    const int r1 = map1[d.slot], r2 = map2[d.slot];
+    const long long base1 = (static_cast<long long>(r1) * g1.ntiles + d.t1) * n1;
+    const long long base2 = (static_cast<long long>(r2) * g2.ntiles + d.t2) * n2;
+    const T p1 = a.pad[r1], p2 = b.pad[r2];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n1; q += blockDim.x) {
+      c1s[q] = a.center[base1 + q];
+      Vec4<T> h = a.half[base1 + q];
+      h.x = h.x + p1;  // radius = x_span / 2 + curvature_padding
+      h.y = h.y + p1;
+      h.z = h.z + p1;
+      r1s[q] = h;
+    }
+    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+      c2s[q] = b.center[base2 + q];
+      Vec4<T> h = b.half[base2 + q];
+      h.x = h.x + p2;
+      h.y = h.y + p2;
+      h.z = h.z + p2;
+      r2s[q] = h;
+    }
+    __syncthreads();
+    const int nv1 = tile_extent(d.t1, g1.tw, te1, g1.W, 1), nu1 = tile_extent(d.t1, g1.tw, te1, g1.W, 0);
+    const int nv2 = tile_extent(d.t2, g2.tw, te2, g2.W, 1), nu2 = tile_extent(d.t2, g2.tw, te2, g2.W, 0);
+    const int ty1 = d.t1 / g1.tw, tx1 = d.t1 % g1.tw, ty2 = d.t2 / g2.tw, tx2 = d.t2 % g2.tw;
+    const int npair = n1 * n2;
+    for (int p0 = 0; p0 < npair; p0 += blockDim.x) {
+      const int p = p0 + threadIdx.x;
+      bool hit = false;
+      unsigned long long key = 0;
+      if (p < npair) {
+        const int l1 = p / n2, l2 = p % n2;
+        const int a1 = l1 / te1, b1 = l1 % te1, a2 = l2 / te2, b2 = l2 % te2;
+        if (a1 < nv1 && b1 < nu1 && a2 < nv2 && b2 < nu2) {
+          ++tests;
+          const Vec4<T> c1 = c1s[l1], c2 = c2s[l2], q1 = r1s[l1], q2 = r2s[l2];
+          hit = fabs(c1.x - c2.x) < (q1.x + q2.x) && fabs(c1.y - c2.y) < (q1.y + q2.y) &&
+                fabs(c1.z - c2.z) < (q1.z + q2.z);
+          const unsigned long long ci = static_cast<unsigned long long>((ty1 * te1 + a1) * g1.W + tx1 * te1 + b1);
+          const unsigned long long cj = static_cast<unsigned long long>((ty2 * te2 + a2) * g2.W + tx2 * te2 + b2);
+          key = (static_cast<unsigned long long>(d.slot) << (2 * ij_bits)) | (ci << ij_bits) | cj;
+        }
+      }
+      const long long pos = warp_append(hit, &stats->candidates);
+      if (pos >= 0 && static_cast<unsigned long long>(pos) < key_cap) keys[pos] = key;
+    }
+  }
+  atomicAdd(&stats->pair_tests, tests);
+}
+
+__global__ void k_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2,
+                             int *idx, unsigned *flag1) {
+  const unsigned long long mij = (1ull << ij_bits) - 1ull;
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long k = keys[q];
+    const unsigned long long slot = k >> (2 * ij_bits);
+    key2[q] = (slot << ij_bits) | (k & mij);
+    idx[q] = static_cast<int>(q);
+    flag1[q] = (q == 0 || (keys[q - 1] >> ij_bits) != (k >> ij_bits)) ? 1u : 0u;
+  }
+}
+
+__global__ void k_flag_runs(const unsigned long long *sorted, long long n, unsigned *flags) {
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x)
+    flags[q] = (q == 0 || sorted[q - 1] != sorted[q]) ? 1u : 0u;
+}
+
+// Side 1: pair q (sorted by (slot, i, j)) -> region id ex1[q] + flag1[q] - 1.
+template <typename T>
+__global__ void k_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
+                              const unsigned *ex1, SideRound<T> cur, const int *map1, RegionRec<T> *next,
+                              int *nmap1) {
+  const unsigned long long mij = (1ull << ij_bits) - 1ull;
+  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n;
+       q += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int id = static_cast<int>(ex1[q] + flag1[q]) - 1;
+    nmap1[q] = id;
+    if (flag1[q]) {
+      const unsigned long long k = keys[q];
+      const int slot = static_cast<int>(k >> (2 * ij_bits));
+      const int i = static_cast<int>((k >> ij_bits) & mij);
+      next[id] = child_rect(cur.regions[map1[slot]], cur.g.nuv, i);
+    }
+  }
+}
+
+// Side 2: sorted (slot, j) keys with their pair index.
+template <typename T>
+__global__ void k_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
+                              const unsigned *flag2, const unsigned *ex2, SideRound<T> cur, const int *map2,
+                              RegionRec<T> *next, int *nmap2) {
+  const unsigned long long mij = (1ull << ij_bits) - 1ull;
+  for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < n;
+       p += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int id = static_cast<int>(ex2[p] + flag2[p]) - 1;
+    nmap2[idxs[p]] = id;
+    if (flag2[p]) {
+      const unsigned long long k = key2s[p];
+      const int slot = static_cast<int>(k >> ij_bits);
+      const int j = static_cast<int>(k & mij);
+      next[id] = child_rect(cur.regions[map2[slot]], cur.g.nuv, j);
+    }
+  }
+}
+
+inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > max_blocks) g = max_blocks;
+  return static_cast<int>(g);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+
+template <typename T>
+void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st) {
+  const long long n = static_cast<long long>(sr.nreg) * 2 * sr.g.nuv;
+  const int maxdeg = s.degu > s.degv ? s.degu : s.degv;
+  if (maxdeg < 8)
+    k_basis<T, 9><<<grid_for(n, 128), 128, 0, st>>>(s, sr.regions, sr.nreg, sr.g.nuv, sr.g.p1max, sr.spans,
+                                                     sr.basis);
+  else
+    k_basis<T, kMaxDeg + 1><<<grid_for(n, 64), 64, 0, st>>>(s, sr.regions, sr.nreg, sr.g.nuv, sr.g.p1max,
+                                                             sr.spans, sr.basis);
+}
+
+template <typename T>
+void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st) {
+  const long long n = static_cast<long long>(sr.nreg) * sr.g.nuv * sr.g.nuv;
+  k_samples<T><<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, sr, need_k ? 1 : 0);
+}
+
+template <typename T>
+void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaStream_t st) {
+  k_pad<T><<<(sr.nreg + 127) / 128, 128, 0, st>>>(sr, use_k ? 1 : 0, span_u0, span_v0);
+}
+
+template <typename T>
+void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st) {
+  const long long n = static_cast<long long>(sr.nreg) * sr.g.cpr;
+  k_cells<T><<<grid_for(n, 256, 148 * 32), 256, 0, st>>>(sr, intersect ? 1 : 0);
+}
+
+template <typename T>
+void launch_tiles(const SideRound<T> &sr, cudaStream_t st) {
+  const long long n = static_cast<long long>(sr.nreg) * sr.g.ntiles;
+  k_tiles<T><<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(sr);
+}
+
+template <typename T>
+void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st) {
+  const long long n = static_cast<long long>(nuv) * nuv;
+  k_records<T><<<grid_for(n, 64, 148 * 32), 64, 0, st>>>(s, ustep, vstep, ustart, vstart, nuv, out);
+}
+
+template <typename T>
+void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                     int k, ScreenStats *stats, cudaStream_t st) {
+  const unsigned long long total = static_cast<unsigned long long>(nslots) * a.g.ntiles * b.g.ntiles;
+  const int per_thread = 4;
+  const unsigned long long chunk = 1024ull * per_thread;
+  unsigned long long blocks = (total + chunk - 1) / chunk;
+  if (blocks < 1) blocks = 1;
+  k_dist_tau<T><<<static_cast<unsigned>(blocks), 1024, 0, st>>>(a, b, map1, map2, nslots, k, stats, per_thread);
+}
+
+template <typename T>
+void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                      unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st) {
+  const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
+  k_dist_cull<T><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats);
+}
+
+template <typename T>
+void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                      const unsigned long long *surv, unsigned long long nsurv, int k, DistCand<T> *cand,
+                      unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st) {
+  (void)nslots;
+  if (nsurv == 0) return;
+  const int blocks = static_cast<int>(nsurv < 148ull * 8 ? nsurv : 148ull * 8);
+  k_dist_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, k, cand, cand_cap, stats);
+}
+
+template <typename T>
+void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
+                        ScreenStats *stats, cudaStream_t st) {
+  const size_t smem = sizeof(DistCand<T>) * kSelectCap;
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_dist_select<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    configured = true;
+  }
+  k_dist_select<T><<<1, 1024, smem, st>>>(cand, cand_cap, k, out, stats);
+}
+
+template <typename T>
+void launch_dist_next(const DistCand<T> *top, ScreenStats *stats, const SideRound<T> &a, const SideRound<T> &b,
+                      const int *map1, const int *map2, int nuv_next, RegionRec<T> *next1, RegionRec<T> *next2,
+                      int *nmap1, int *nmap2, cudaStream_t st) {
+  k_dist_next<T><<<1, 1024, 0, st>>>(top, stats, a, b, map1, map2, nuv_next, next1, next2, nmap1, nmap2);
+}
+
+template <typename T>
+void launch_inter_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                       unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st) {
+  const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
+  k_inter_cull<T><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats);
+}
+
+template <typename T>
+void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                       const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
+                       unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st) {
+  if (nsurv == 0) return;
+  const int blocks = static_cast<int>(nsurv < 148ull * 8 ? nsurv : 148ull * 8);
+  k_inter_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats);
+}
+
+void launch_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2, int *idx,
+                       unsigned *flag1, cudaStream_t st) {
+  k_inter_prep<<<grid_for(n, 256), 256, 0, st>>>(keys, n, ij_bits, key2, idx, flag1);
+}
+
+void launch_flag_runs(const unsigned long long *sorted, long long n, unsigned *flags, cudaStream_t st) {
+  k_flag_runs<<<grid_for(n, 256), 256, 0, st>>>(sorted, n, flags);
+}
+
+template <typename T>
+void launch_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
+                        const unsigned *ex1, const SideRound<T> &cur, const int *map1, RegionRec<T> *next,
+                        int *nmap1, cudaStream_t st) {
+  k_inter_side1<T><<<grid_for(n, 256), 256, 0, st>>>(keys, n, ij_bits, flag1, ex1, cur, map1, next, nmap1);
+}
+
+template <typename T>
+void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
+                        const unsigned *flag2, const unsigned *ex2, const SideRound<T> &cur, const int *map2,
+                        RegionRec<T> *next, int *nmap2, cudaStream_t st) {
+  k_inter_side2<T><<<grid_for(n, 256), 256, 0, st>>>(key2s, idxs, n, ij_bits, flag2, ex2, cur, map2, next, nmap2);
+}
+
+#define JSI_INSTANTIATE(T)                                                                                        \
+  template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t);                         \
+  template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t);                 \
+  template void launch_pad<T>(const SideRound<T> &, bool, T, T, cudaStream_t);                                    \
+  template void launch_cells<T>(const SideRound<T> &, bool, cudaStream_t);                                        \
+  template void launch_tiles<T>(const SideRound<T> &, cudaStream_t);                                              \
+  template void launch_records<T>(const SurfView<T> &, T, T, T, T, int, T *, cudaStream_t);                       \
+  template void launch_dist_tau<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, int, \
+                                   ScreenStats *, cudaStream_t);                                                  \
+  template void launch_dist_cull<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,    \
+                                    unsigned long long *, unsigned long long, ScreenStats *, cudaStream_t);       \
+  template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,    \
+                                    const unsigned long long *, unsigned long long, int, DistCand<T> *,           \
+                                    unsigned long long, ScreenStats *, cudaStream_t);                             \
+  template void launch_dist_select<T>(const DistCand<T> *, unsigned long long, int, DistCand<T> *, ScreenStats *, \
+                                      cudaStream_t);                                                              \
+  template void launch_dist_next<T>(const DistCand<T> *, ScreenStats *, const SideRound<T> &,                     \
+                                    const SideRound<T> &, const int *, const int *, int, RegionRec<T> *,          \
+                                    RegionRec<T> *, int *, int *, cudaStream_t);                                  \
+  template void launch_inter_cull<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,   \
+                                     unsigned long long *, unsigned long long, ScreenStats *, cudaStream_t);      \
+  template void launch_inter_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,        \
+                                     const unsigned long long *, unsigned long long, int, unsigned long long *,   \
+                                     unsigned long long, ScreenStats *, cudaStream_t);                            \
+  template void launch_inter_side1<T>(const unsigned long long *, long long, int, const unsigned *,               \
+                                      const unsigned *, const SideRound<T> &, const int *, RegionRec<T> *, int *, \
+                                      cudaStream_t);                                                              \
+  template void launch_inter_side2<T>(const unsigned long long *, const int *, long long, int, const unsigned *,  \
+                                      const unsigned *, const SideRound<T> &, const int *, RegionRec<T> *, int *, \
+                                      cudaStream_t);
+
+JSI_INSTANTIATE(float)
+JSI_INSTANTIATE(double)
+
+}  // namespace jsi

@@ -1,0 +1,74 @@
+"""C-ABI library checks that need no GPU: it loads, exports every symbol
+include/jsi_b200.h declares, and fails loudly (no CPU fallback) without a
+device."""
+from __future__ import annotations
+
+import ctypes
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared_symbols():
+    text = (ROOT / "include" / "jsi_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(jsi_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    from jsi_cad_next_versions_b200 import _capi
+    assert sorted(_capi.EXPORTED) == _declared_symbols()
+
+
+def test_library_exports_every_declared_symbol():
+    from jsi_cad_next_versions_b200 import _capi
+    lib = ctypes.CDLL(str(_capi.LIB_PATH))
+    missing = [s for s in _declared_symbols() if not hasattr(lib, s)]
+    assert not missing
+
+
+def test_library_is_sm100a_build():
+    data = (ROOT / "jsi_cad_next_versions_b200" / "libjsi_b200.so").read_bytes()
+    assert b"sm_100a" in data
+
+
+def test_status_strings_and_abi():
+    from jsi_cad_next_versions_b200 import _capi
+    lib = _capi.load()
+    assert lib.jsi_abi_version() == 1
+    assert lib.jsi_status_string(0) == b"ok"
+    assert lib.jsi_status_string(-4) == b"capacity exceeded"
+
+
+def test_defaults_match_reference_statics():
+    """k_of_topk=8, max_layers=4, next_nuv=16 (distance_analysis.cu:33-36);
+    global_nuv=16, 6 rounds, halve above 512 down to 4 (intersection.cu:36,368-370)."""
+    from jsi_cad_next_versions_b200 import _capi
+    lib = _capi.load()
+    d = _capi.DistParams()
+    lib.jsi_dist_params_default(ctypes.byref(d))
+    assert (d.nuv_refine, d.k, d.rounds, d.precision, d.newton) == (16, 8, 4, 0, 0)
+    i = _capi.InterParams()
+    lib.jsi_inter_params_default(ctypes.byref(i))
+    assert (i.nuv_refine, i.use_k, i.rounds, i.halve_threshold, i.min_nuv, i.precision) == (16, 1, 6, 512, 4, 0)
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import jsi_cad_next_versions_b200 as J
+    with pytest.raises(J.JsiError) as e:
+        J.Context(0)
+    assert e.value.status == -8
+
+
+def test_null_arguments_rejected():
+    from jsi_cad_next_versions_b200 import _capi
+    lib = _capi.load()
+    assert lib.jsi_create(None, None) == -1
+    assert lib.jsi_destroy(None) == -1
+    assert lib.jsi_min_distance(None, None, None, None, None) == -1
+    assert lib.jsi_intersect(None, None, None, None, None) == -1

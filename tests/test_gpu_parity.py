@@ -1,0 +1,230 @@
+"""Parity of the CUDA path (through the C ABI) with the reference and the oracle.
+
+* V5_FP32 form: bit-for-bit against the reference's golden vectors and, per
+  round, against the oracle's float instantiation (candidate sets in order).
+* FP64 form: bit-for-bit against the oracle's double instantiation (the
+  plain-FP64 restatement of the same algorithm): same candidate sets, same
+  k-th squared distances.
+"""
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_npz, rect32, surface_from
+from jsi_cad_next_versions_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _task(ctx, sid, rect, nuv, side):
+    return ctx.task(sid, rect, nuv, side)
+
+
+def _grid_names():
+    g = load_npz("ref_eval_grids.npz")
+    return sorted({k.split("/")[0] for k in g})
+
+
+# ---------------------------------------------------------------------------
+# grid evaluation
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("name", _grid_names())
+@pytest.mark.parametrize("nuv", [5, 16])
+def test_eval_grid_matches_reference_bits(gpu_ctx, name, nuv):
+    g = load_npz("ref_eval_grids.npz")
+    us, vs, u0, v0 = g[f"{name}/n{nuv}/params"]
+    got = gpu_ctx.eval_grid(g[f"{name}/ivec"], g[f"{name}/data"], us, vs, u0, v0, nuv)
+    exp = g[f"{name}/n{nuv}/records"]
+    assert np.array_equal(got.view(np.uint32), exp.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", _grid_names())
+def test_eval_grid_f64_matches_oracle_bits(gpu_ctx, orc, name):
+    g = load_npz("ref_eval_grids.npz")
+    s = surface_from(g[f"{name}/ivec"], g[f"{name}/data"])
+    r = [float(x) for x in s.rect()]
+    nuv = 13
+    us, vs = (r[2] - r[0]) / nuv, (r[3] - r[1]) / nuv
+    got = gpu_ctx.eval_grid(s.ivec, s.data, us, vs, r[0], r[1], nuv, dtype=np.float64)
+    exp = orc.eval_grid(s, us, vs, r[0], r[1], nuv, dtype=np.float64)
+    assert np.array_equal(got.view(np.uint64), exp.view(np.uint64))
+
+
+def test_eval_with_cuda_name(gpu_ctx):
+    """The reference's evalWithCuda entry point name, over the default context."""
+    import jsi_cad_next_versions_b200 as J
+    g = load_npz("ref_eval_grids.npz")
+    s = surface_from(g["sine_a/ivec"], g["sine_a/data"])
+    r = s.rect()
+    us = np.float32((r[2] - r[0]) / np.float32(33))
+    J.init_cad()
+    try:
+        out = np.zeros(33 * 33 * J.ONE_UV_SIZE, np.float32)
+        J.evalWithCuda(s.ivec, s.data, s.ndata, us, us, r[0], r[1], 33, out)
+    finally:
+        J.deinit_cad()
+    assert np.array_equal(out.view(np.uint32), g["sine_a/evalWithCuda33"].view(np.uint32))
+
+
+# ---------------------------------------------------------------------------
+# minimum distance
+# ---------------------------------------------------------------------------
+
+def _dist_both(ctx, orc, A, B, nuv0, k, rounds=4, nuv_b=None, precision="v5_fp32"):
+    ra, rb = rect32(A), rect32(B)
+    sa, sb = ctx.upload(A), ctx.upload(B)
+    try:
+        res = ctx.min_distance(_task(ctx, sa, ra, nuv0, 1), _task(ctx, sb, rb, nuv_b or nuv0, 2), k=k,
+                               rounds=rounds, precision=precision, trace=True)
+    finally:
+        ctx.release(sa)
+        ctx.release(sb)
+    return res
+
+
+@pytest.mark.parametrize("key", ["sine/n64/k8", "sine/n64/k64", "sine/n32/k8", "hardwave/n64/k8",
+                                 "hardwave/n128/k8"])
+def test_distance_v5_matches_reference_and_oracle(gpu_ctx, orc, key):
+    g = load_npz("ref_distance.npz")
+    name, n, k = key.split("/")
+    nuv0, k = int(n[1:]), int(k[1:])
+    A, B, _ = synth.distance_pair_sine() if name == "sine" else synth.distance_pair_hard_wave()
+    res = _dist_both(gpu_ctx, orc, A, B, nuv0, k)
+    per_round = np.sqrt(res.kth_d2.astype(np.float32))
+    assert np.array_equal(per_round.view(np.uint32), g[key + "/per_round"].view(np.uint32))
+    assert np.float32(res.v5_value) == g[key + "/per_round"][-1]
+    o = orc.dist_query(A, B, rect32(A), rect32(B), nuv0, 16, k, 4)
+    for r in range(4):
+        assert np.array_equal(res.pairs[r], o["pairs"][r]), f"round {r + 1} candidate list"
+
+
+@pytest.mark.parametrize("key", ["sine/n64/k8", "sine/n64/k64", "hardwave/n64/k8"])
+def test_distance_fp64_matches_oracle(gpu_ctx, orc, key):
+    name, n, k = key.split("/")
+    nuv0, k = int(n[1:]), int(k[1:])
+    A, B, _ = synth.distance_pair_sine() if name == "sine" else synth.distance_pair_hard_wave()
+    res = _dist_both(gpu_ctx, orc, A, B, nuv0, k, precision="fp64")
+    o = orc.dist_query(A, B, rect32(A).astype(np.float64), rect32(B).astype(np.float64), nuv0, 16, k, 4,
+                       dtype=np.float64)
+    assert np.array_equal(res.kth_d2.view(np.uint64), o["kth_d2"].view(np.uint64))
+    for r in range(4):
+        assert np.array_equal(res.pairs[r], o["pairs"][r])
+    assert res.distance == np.sqrt(o["kth_d2"][-1])
+
+
+def test_distance_full_size_hardwave(gpu_ctx):
+    """Hard-wave pair at full size, nuv0 = 512: the reference's own value."""
+    path = GOLDEN / "ref_full.json"
+    if not path.exists():
+        pytest.skip("full-size fixture not generated")
+    full = json.loads(path.read_text())["hardwave_n512_k8"]
+    A, B, _ = synth.distance_pair_hard_wave()
+    sa, sb = gpu_ctx.upload(A), gpu_ctx.upload(B)
+    res = gpu_ctx.min_distance(_task(gpu_ctx, sa, rect32(A), 512, 1), _task(gpu_ctx, sb, rect32(B), 512, 2))
+    gpu_ctx.release(sa)
+    gpu_ctx.release(sb)
+    assert np.float32(res.v5_value).view(np.uint32) == full["value_bits"]
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13, 14])
+@pytest.mark.parametrize("precision", ["v5_fp32", "fp64"])
+def test_distance_random_pairs(gpu_ctx, orc, seed, precision):
+    """Mixed degrees 2..5, rational and non-rational, uneven nuv per side."""
+    rng = synth.SplitMix64(seed)
+    A = synth.random_surface(rng)
+    B = synth.random_surface(rng)
+    nuv_a, nuv_b = 17 + seed, 23 + 2 * seed
+    k = [1, 5, 8, 33][seed % 4]
+    res = _dist_both(gpu_ctx, orc, A, B, nuv_a, k, nuv_b=nuv_b, precision=precision)
+    dt = np.float32 if precision == "v5_fp32" else np.float64
+    # The oracle's dist_query uses one nuv for both sides: compare round by round
+    # through the oracle's per-side interface only when nuv_a == nuv_b.
+    res2 = _dist_both(gpu_ctx, orc, A, B, nuv_a, k, precision=precision)
+    o = orc.dist_query(A, B, rect32(A).astype(dt), rect32(B).astype(dt), nuv_a, 16, k, 4, dtype=dt)
+    assert np.array_equal(res2.kth_d2.astype(dt), o["kth_d2"])
+    for r in range(len(o["pairs"])):
+        assert np.array_equal(res2.pairs[r], o["pairs"][r])
+    assert res.rounds >= 1
+
+
+def test_distance_k_larger_than_pairs(gpu_ctx, orc):
+    """k beyond the number of cell pairs keeps every pair (min(k, num),
+    distance_analysis.cu:142, :236-240)."""
+    A, B, _ = synth.distance_pair_sine()
+    res = _dist_both(gpu_ctx, orc, A, B, 3, 64, rounds=2)
+    o = orc.dist_query(A, B, rect32(A), rect32(B), 3, 16, 64, 2)
+    assert res.npairs[0] == 16
+    for r in range(2):
+        assert np.array_equal(res.pairs[r], o["pairs"][r])
+    assert np.array_equal(res.kth_d2.astype(np.float32), o["kth_d2"])
+
+
+# ---------------------------------------------------------------------------
+# intersection
+# ---------------------------------------------------------------------------
+
+def _inter(ctx, A, B, nuv0, use_k, precision="v5_fp32", rounds=6):
+    sa, sb = ctx.upload(A), ctx.upload(B)
+    try:
+        return ctx.intersect(_task(ctx, sa, rect32(A), nuv0, 1), _task(ctx, sb, rect32(B), nuv0, 2),
+                             use_k=bool(use_k), precision=precision, rounds=rounds, trace=True)
+    finally:
+        ctx.release(sa)
+        ctx.release(sb)
+
+
+@pytest.mark.parametrize("case", [3, 4])
+@pytest.mark.parametrize("use_k", [1, 0])
+def test_intersection_reference_cases(gpu_ctx, orc, case, use_k):
+    g = load_npz("ref_intersection.npz")
+    A = surface_from(g[f"case{case}/ivec1"], g[f"case{case}/data1"])
+    B = surface_from(g[f"case{case}/ivec2"], g[f"case{case}/data2"])
+    res = _inter(gpu_ctx, A, B, 16, use_k)
+    assert np.array_equal(res.counts, g[f"case{case}/k{use_k}/counts"])
+    o = orc.inter_query(A, B, rect32(A), rect32(B), 16, 16, use_k)
+    for r in range(res.rounds):
+        assert np.array_equal(res.pairs[r], o["pairs"][r]), f"round {r + 1}"
+    assert np.float32(res.pad[0]) == o["pads"][0] and np.float32(res.pad[1]) == o["pads"][1]
+
+
+@pytest.mark.parametrize("case", [3, 4])
+@pytest.mark.parametrize("use_k", [1, 0])
+def test_intersection_fp64_matches_oracle(gpu_ctx, orc, case, use_k):
+    g = load_npz("ref_intersection.npz")
+    A = surface_from(g[f"case{case}/ivec1"], g[f"case{case}/data1"])
+    B = surface_from(g[f"case{case}/ivec2"], g[f"case{case}/data2"])
+    res = _inter(gpu_ctx, A, B, 16, use_k, precision="fp64")
+    o = orc.inter_query(A, B, rect32(A).astype(np.float64), rect32(B).astype(np.float64), 16, 16, use_k,
+                        dtype=np.float64)
+    assert np.array_equal(res.counts, o["counts"])
+    for r in range(res.rounds):
+        assert np.array_equal(res.pairs[r], o["pairs"][r]), f"round {r + 1}"
+
+
+@pytest.mark.parametrize("nuv0", [16, 32])
+@pytest.mark.parametrize("use_k", [1, 0])
+def test_intersection_saddle_plane_counts(gpu_ctx, nuv0, use_k):
+    g = load_npz("ref_inter_synth.npz")
+    C, D, _ = synth.intersection_pair_saddle_plane()
+    res = _inter(gpu_ctx, C, D, nuv0, use_k)
+    assert np.array_equal(res.counts, g[f"n{nuv0}/k{use_k}/counts"])
+
+
+@pytest.mark.parametrize("seed", [21, 22, 23])
+@pytest.mark.parametrize("precision", ["v5_fp32", "fp64"])
+def test_intersection_random_pairs(gpu_ctx, orc, seed, precision):
+    rng = synth.SplitMix64(seed)
+    A = synth.random_surface(rng)
+    B = synth.random_surface(rng)
+    dt = np.float32 if precision == "v5_fp32" else np.float64
+    nuv0 = 12 + seed % 7
+    res = _inter(gpu_ctx, A, B, nuv0, 1, precision=precision, rounds=4)
+    o = orc.inter_query(A, B, rect32(A).astype(dt), rect32(B).astype(dt), nuv0, 16, 1, rounds=4, dtype=dt)
+    assert np.array_equal(res.counts, o["counts"])
+    for r in range(res.rounds):
+        if o["pairs"][r] is not None:
+            assert np.array_equal(res.pairs[r], o["pairs"][r])
