@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Throughput of the hard-wave minimum-distance query on B200.
+
+Workload (one step = one batch): ``--batch`` hard-wave query pairs, each two
+bicubic 64x64 B-spline patches (A: z = 0.05 sin(20 pi x) cos(20 pi y) +
+N(0, 1e-3); B: the field phase-shifted by pi, lifted by 0.1; seeded
+synthetic surfaces, a distinct seed pair per query), first round nuv = 512,
+three refinement rounds at nuv = 16, k = 8: minimum_distance of the reference
+(JSI_CAD_NEXT_VERSION5/src/distance_analysis/distance_analysis.cu:356-506).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* ``value``  queries/s with the surfaces resident in HBM, CUDA events on the
+             library's own stream, L2 flushed (256 MiB write) between steps.
+* ``e2e``    the same metric through the C ABI with host buffers: upload of
+             both surfaces, the query, the result read-back, release.
+* ``roofline`` the dominant kernel, its algorithmic work per launch over its
+             CUDA-event duration measured in the timed region.
+* ``cpu_baseline`` the reference itself (oracle/_ref, built from its sources)
+             on this host's cores, one full query.
+Multi-GPU: one process per GPU (torchrun); each rank runs its own batch
+(independent queries: weak scaling, no data-path collective); the step time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "queries/s + p50/p99 latency: FP32-screen vs plain FP64 on B200 at ≤1e-9 rel err"
+WORKLOAD = "hard-wave 64x64 bicubic pair, minimum distance, nuv0=512 + 3 rounds nuv=16, k=8"
+NUV0, NUV_REFINE, K, ROUNDS = 512, 16, 8, 4
+FORMS = ("fp64", "v5_fp32")  # headline form first
+
+# Algorithmic work of the screening kernels, per unit (FMA = 2 flops):
+#  dist_leaf: one cell-pair centre distance = 3 sub + 3 mul + 2 add = 8 flops,
+#             reading 2 cell centres from shared memory (tile staged once);
+#  dist_cull: one tile-pair box bound = 6 sub + 3 max + 3 mul + 2 add = 14 flops,
+#             reading 4 Vec4 tile bounds (64 B FP32 / 128 B FP64).
+FLOPS_PER_PAIR_TEST = 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--batch", type=int, default=16, help="queries per step")
+    ap.add_argument("--nuv0", type=int, default=NUV0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default=",".join(FORMS))
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_pairs(batch: int, rank: int):
+    from jsi_cad_next_versions_b200 import synth
+    pairs = []
+    for q in range(batch):
+        seed = 1000 + 2 * (rank * batch + q)
+        A, B, _ = synth.distance_pair_hard_wave(seed_a=seed, seed_b=seed + 1)
+        pairs.append((A, B))
+    return pairs
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.text = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.text, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.text, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "text", "") or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(nuv0: int):
+    """The reference (oracle/_ref) on this host: one full query, all cores."""
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    import oracle
+    from jsi_cad_next_versions_b200 import synth
+    if not oracle.Reference.available():
+        return None
+    R = oracle.Reference()
+    A, B, _ = synth.distance_pair_hard_wave()
+    ra, rb = np.array(A.rect(), np.float32), np.array(B.rect(), np.float32)
+    t0 = time.perf_counter()
+    v = R.minimum_distance(A, B, ra, rb, nuv0, NUV_REFINE, K, ROUNDS)
+    el = time.perf_counter() - t0
+    return {"value": 1.0 / el, "unit": "queries/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
+            "sample": f"1 full query (hard-wave seeds 3/4, nuv0={nuv0}) through the reference's minimum_distance, "
+                      f"{el:.2f} s, result {float(v):.9g}"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    import oracle
+    if not oracle.Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libjsi_v5_ref.so was not built (needs "
+                                                              "the reference checkout at build time)"}))
+        return
+    from jsi_cad_next_versions_b200 import synth
+    R = oracle.Reference()
+    A, B, _ = synth.distance_pair_hard_wave()
+    ra, rb = np.array(A.rect(), np.float32), np.array(B.rect(), np.float32)
+    # Each step is one full query (a bounded sample of the batch); the CPU has
+    # no device warm-up, so one untimed query suffices.
+    for _ in range(min(args.warmup, 1)):
+        R.minimum_distance(A, B, ra, rb, args.nuv0, NUV_REFINE, K, ROUNDS)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        R.minimum_distance(A, B, ra, rb, args.nuv0, NUV_REFINE, K, ROUNDS)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = args.steps / total
+    lat = sorted(t * 1e3 for t in times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "queries_per_step": 1, "nuv0": args.nuv0, "cores": int(os.environ["OMP_NUM_THREADS"])},
+        "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                         "kind": "reference", "sample": "one full query per step through minimum_distance"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def percentile(v, q):
+    v = sorted(v)
+    if not v:
+        return None
+    return v[min(len(v) - 1, int(q * len(v)))]
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    import jsi_cad_next_versions_b200 as J
+
+    ctx = J.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    pairs = make_pairs(args.batch, rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    forms = [f for f in args.forms.split(",") if f]
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    # ---------------- device throughput, surfaces resident -----------------
+    ids = [(ctx.upload(A), ctx.upload(B)) for A, B in pairs]
+    tasks = [(ctx.task(a, np.array(A.rect(), np.float32), args.nuv0, 1),
+              ctx.task(b, np.array(B.rect(), np.float32), args.nuv0, 2)) for (a, b), (A, B) in zip(ids, pairs)]
+    ref_values = {}
+    for form in forms:
+        def step():
+            lats = []
+            for ta, tb in tasks:
+                r = ctx.min_distance(ta, tb, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
+                lats.append(r.device_ms)
+            return lats, r
+        for _ in range(args.warmup):
+            step()
+        ctx.kernel_timing(True)
+        launches0 = ctx.launch_count()
+        step_ms, lats = [], []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                barrier()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                l, last = step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                barrier()
+                step_ms.append(max_over_ranks(e0.elapsed_time(e1)))
+                lats += l
+        launches = ctx.launch_count() - launches0
+        ktimes = ctx.kernel_times()
+        ctx.kernel_timing(False)
+        total_ms = sum(step_ms)
+        results[form] = {
+            "value": world * args.batch * args.steps / (total_ms / 1e3), "ms_per_step": total_ms / args.steps,
+            "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99), "clocks": clk.summary(),
+            "gpu_launches": launches, "kernels": ktimes, "last": last}
+        ref_values[form] = last.v5_value if form == "v5_fp32" else last.distance
+
+    # ---------------- end to end through the C ABI, host buffers -----------
+    form = forms[0]
+    h0, d0 = ctx.transfer_bytes()
+    for (a, b) in ids:
+        ctx.release(a)
+        ctx.release(b)
+
+    def e2e_step():
+        for A, B in pairs:
+            sa, sb = ctx.upload(A), ctx.upload(B)
+            ctx.min_distance(ctx.task(sa, np.array(A.rect(), np.float32), args.nuv0, 1),
+                             ctx.task(sb, np.array(B.rect(), np.float32), args.nuv0, 2), k=K, rounds=ROUNDS,
+                             nuv_refine=NUV_REFINE, precision=form)
+            ctx.release(sa)
+            ctx.release(sb)
+    for _ in range(args.warmup):
+        e2e_step()
+    h0, d0 = ctx.transfer_bytes()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms.append(max_over_ranks(e0.elapsed_time(e1)))
+    h1, d1 = ctx.transfer_bytes()
+    e2e = {"value": world * args.batch * args.steps / (sum(e2e_ms) / 1e3), "unit": "queries/s",
+           "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps,
+           "form": form}
+
+    if rank != 0:
+        ctx.close()
+        if pg:
+            pg.destroy_process_group()
+        return
+
+    head = results[forms[0]]
+    # ---------------- roofline of the dominant kernel ----------------------
+    kt = head["kernels"]
+    dom = max(kt.items(), key=lambda kv: kv[1][0])[0] if kt else None
+    roof = None
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    last = head["last"]
+    if dom:
+        ms, n = kt[dom]
+        avg_s = ms / max(n, 1) / 1e3
+        if dom == "dist_leaf":
+            # executed cell-pair tests of the step / leaf launches
+            tests = int(sum(last.pair_tests)) * args.batch
+            launches_per_step = n / args.steps
+            flops = FLOPS_PER_PAIR_TEST * tests / max(launches_per_step, 1)
+            fp_peak = 74.4 if forms[0] != "fp64" else 37.2
+            roof = {"bound": "fp32" if forms[0] != "fp64" else "fp64", "kernel": dom,
+                    "achieved": flops / avg_s / 1e12, "peak": fp_peak, "unit": "TFLOP/s",
+                    "frac": flops / avg_s / 1e12 / fp_peak, "traffic": None,
+                    "peak_source": "nominal CUDA-core peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz; FP64 half)"}
+        else:
+            roof = {"kernel": dom, "avg_ms": avg_s * 1e3}
+    cpu = None if args.no_cpu_baseline else cpu_baseline(args.nuv0)
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if forms[0] == "fp64" else "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": forms[0], "queries_per_step_per_gpu": args.batch,
+                   "nuv0": args.nuv0, "l2": "flushed (256 MiB write) between steps", "parallelism": f"dp{world}"},
+        "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"]},
+        "forms": {f: {"queries_per_s": r["value"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+                      "result": ref_values[f]} for f, r in results.items()},
+        "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": head["clocks"],
+        "gpu_launches": head["gpu_launches"],
+        "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
+    }
+    print(json.dumps(line))
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -73,6 +73,23 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id);
 /* Resident surface bytes on the device. */
 int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out);
 
+/* --- instrumentation (no counterpart in the reference; its CAD_TIMING /
+ * CAD_PROFILE hooks, src/common/profiler.hpp:11-41, time on the host) ---- */
+/* The context's CUDA stream (a cudaStream_t) so callers can time it with
+ * their own CUDA events. */
+int jsi_context_stream(jsi_context *ctx, void **stream);
+/* Cumulative host->device and device->host bytes the context has copied. */
+int jsi_transfer_bytes(const jsi_context *ctx, unsigned long long *h2d, unsigned long long *d2h);
+/* Cumulative number of kernels this library has launched (all contexts). */
+int jsi_launch_count(unsigned long long *out);
+/* Per-kernel timing: while enabled, every kernel launch of the context is
+ * bracketed by CUDA events on its stream.  Enabling or disabling resets the
+ * totals.  jsi_kernel_time reads the total milliseconds and launch count of
+ * one kernel name; jsi_kernel_names lists the names seen (comma separated). */
+int jsi_kernel_timing(jsi_context *ctx, int enable);
+int jsi_kernel_time(jsi_context *ctx, const char *name, double *total_ms, long long *launches);
+const char *jsi_kernel_names(jsi_context *ctx);
+
 /* One query side: EvalAndConstructTask (include/jsi_cad.hpp:11-23) with the
  * surface named by a resident id instead of raw device pointers. */
 typedef struct {

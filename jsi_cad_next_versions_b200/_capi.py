@@ -27,7 +27,9 @@ PRECISIONS = {"v5_fp32": PREC_V5_FP32, "fp64": PREC_FP64, "fp32_screen": PREC_FP
 # Every symbol include/jsi_b200.h declares.
 EXPORTED = [
     "jsi_abi_version", "jsi_status_string", "jsi_last_error", "jsi_create", "jsi_destroy",
-    "jsi_surface_upload", "jsi_surface_release", "jsi_resident_bytes", "jsi_dist_params_default",
+    "jsi_surface_upload", "jsi_surface_release", "jsi_resident_bytes", "jsi_context_stream",
+    "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_names",
+    "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
 ]
 
@@ -99,6 +101,19 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_surface_release.restype = I
     L.jsi_resident_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong)]
     L.jsi_resident_bytes.restype = I
+    L.jsi_context_stream.argtypes = [P, ctypes.POINTER(P)]
+    L.jsi_context_stream.restype = I
+    L.jsi_transfer_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
+    L.jsi_transfer_bytes.restype = I
+    L.jsi_launch_count.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
+    L.jsi_launch_count.restype = I
+    L.jsi_kernel_timing.argtypes = [P, I]
+    L.jsi_kernel_timing.restype = I
+    L.jsi_kernel_time.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_longlong)]
+    L.jsi_kernel_time.restype = I
+    L.jsi_kernel_names.argtypes = [P]
+    L.jsi_kernel_names.restype = ctypes.c_char_p
     L.jsi_dist_params_default.argtypes = [ctypes.POINTER(DistParams)]
     L.jsi_dist_params_default.restype = None
     L.jsi_min_distance.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),

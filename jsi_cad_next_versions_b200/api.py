@@ -115,6 +115,37 @@ class Context:
         self._check(self.lib.jsi_resident_bytes(self.handle, ctypes.byref(v)))
         return v.value
 
+    # -- instrumentation --------------------------------------------------
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for external CUDA events)."""
+        v = ctypes.c_void_p()
+        self._check(self.lib.jsi_context_stream(self.handle, ctypes.byref(v)))
+        return v.value or 0
+
+    def transfer_bytes(self):
+        h2d, d2h = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+        self._check(self.lib.jsi_transfer_bytes(self.handle, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return h2d.value, d2h.value
+
+    def kernel_timing(self, enable: bool):
+        """Bracket every kernel launch with CUDA events (resets the totals)."""
+        self._check(self.lib.jsi_kernel_timing(self.handle, 1 if enable else 0))
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (total ms, launches)} since kernel_timing(True)."""
+        names = self.lib.jsi_kernel_names(self.handle).decode()
+        out = {}
+        for n in filter(None, names.split(",")):
+            ms, cnt = ctypes.c_double(0), ctypes.c_longlong(0)
+            self._check(self.lib.jsi_kernel_time(self.handle, n.encode(), ctypes.byref(ms), ctypes.byref(cnt)))
+            out[n] = (ms.value, cnt.value)
+        return out
+
+    def launch_count(self) -> int:
+        v = ctypes.c_ulonglong(0)
+        self._check(self.lib.jsi_launch_count(ctypes.byref(v)))
+        return v.value
+
     # -- queries ----------------------------------------------------------
     @staticmethod
     def task(sid: int, rect, nuv: int, side: int) -> C.Task:

@@ -143,6 +143,14 @@ struct jsi_context {
   size_t resident = 0;
   ScreenStats *d_stats = nullptr;
   ScreenStats *h_stats = nullptr;
+  unsigned long long h2d_bytes = 0, d2h_bytes = 0;
+  // Optional per-kernel timing: CUDA events recorded on the context stream
+  // around every launch, resolved at the next host sync.
+  bool timing = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  std::map<std::string, std::pair<double, long long>> kernel_ms;
+  std::string kernel_names;
 };
 
 namespace {
@@ -166,6 +174,14 @@ int guarded(jsi_context *ctx, Fn &&fn) {
   } catch (const std::bad_alloc &) {
     return record(ctx, JSI_ERR_NOMEM, "host allocation failed");
   }
+}
+
+// cudaMemcpyAsync that also counts the bytes crossing PCIe / C2C.
+cudaError_t copy_async(jsi_context *ctx, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
+                       cudaStream_t st) {
+  if (kind == cudaMemcpyHostToDevice) ctx->h2d_bytes += bytes;
+  if (kind == cudaMemcpyDeviceToHost) ctx->d2h_bytes += bytes;
+  return cudaMemcpyAsync(dst, src, bytes, kind, st);
 }
 
 template <typename T>
@@ -260,12 +276,12 @@ SurfaceRec upload_surface(jsi_context *ctx, const int ivec[7], const float *data
   s.cpw32 = static_cast<Vec4<float> *>(dalloc(ncp * sizeof(Vec4<float>)));
   s.cpw64 = static_cast<Vec4<double> *>(dalloc(ncp * sizeof(Vec4<double>)));
   cudaStream_t st = ctx->stream;
-  JSI_CUDA(cudaMemcpyAsync(s.U32, data, nku * sizeof(float), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(s.V32, data + nku, nkv * sizeof(float), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(s.U64, u64.data(), nku * sizeof(double), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(s.V64, v64.data(), nkv * sizeof(double), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(s.cpw32, c32.data(), ncp * sizeof(Vec4<float>), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(s.cpw64, c64.data(), ncp * sizeof(Vec4<double>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, s.U32, data, nku * sizeof(float), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, s.V32, data + nku, nkv * sizeof(float), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, s.U64, u64.data(), nku * sizeof(double), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, s.V64, v64.data(), nkv * sizeof(double), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, s.cpw32, c32.data(), ncp * sizeof(Vec4<float>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, s.cpw64, c64.data(), ncp * sizeof(Vec4<double>), cudaMemcpyHostToDevice, st));
   JSI_CUDA(cudaStreamSynchronize(st));
   return s;
 }
@@ -312,26 +328,66 @@ void build_side(jsi_context *ctx, const SurfView<T> &v, SideRound<T> &s, bool in
                 T span_v0) {
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
-  launch_basis(v, s, st);
+  timed(ctx, "basis", [&] { launch_basis(v, s, st); });
   if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
-  launch_samples(v, s, need_k, st);
-  launch_pad(s, need_k, span_u0, span_v0, st);
-  launch_cells(s, intersect, st);
-  launch_tiles(s, st);
+  timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); });
+  timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
+  timed(ctx, "cells", [&] { launch_cells(s, intersect, st); });
+  timed(ctx, "tiles", [&] { launch_tiles(s, st); });
   JSI_CUDA(cudaGetLastError());
+}
+
+cudaEvent_t take_event(jsi_context *ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  JSI_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+// Resolves recorded kernel timings; call after the stream has synchronised.
+void resolve_timing(jsi_context *ctx) {
+  for (auto &p : ctx->pending) {
+    float ms = 0.0f;
+    JSI_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+    auto &acc = ctx->kernel_ms[p.first];
+    acc.first += ms;
+    acc.second += 1;
+    ctx->event_pool.push_back(p.second.first);
+    ctx->event_pool.push_back(p.second.second);
+  }
+  ctx->pending.clear();
+}
+
+// Runs one launcher, bracketed by events when timing is on.
+template <typename Fn>
+void timed(jsi_context *ctx, const char *name, Fn &&fn) {
+  if (!ctx->timing) {
+    fn();
+    return;
+  }
+  cudaEvent_t a = take_event(ctx), b = take_event(ctx);
+  JSI_CUDA(cudaEventRecord(a, ctx->stream));
+  fn();
+  JSI_CUDA(cudaEventRecord(b, ctx->stream));
+  ctx->pending.push_back({name, {a, b}});
 }
 
 void reset_stats(jsi_context *ctx) {
   ScreenStats z{};
   z.tau_bits = 0x7f800000u;
   *ctx->h_stats = z;
-  JSI_CUDA(cudaMemcpyAsync(ctx->d_stats, ctx->h_stats, sizeof(ScreenStats), cudaMemcpyHostToDevice, ctx->stream));
+  JSI_CUDA(copy_async(ctx, ctx->d_stats, ctx->h_stats, sizeof(ScreenStats), cudaMemcpyHostToDevice, ctx->stream));
 }
 
 void pull_stats(jsi_context *ctx) {
-  JSI_CUDA(cudaMemcpyAsync(ctx->h_stats, ctx->d_stats, sizeof(ScreenStats), cudaMemcpyDeviceToHost, ctx->stream));
+  JSI_CUDA(copy_async(ctx, ctx->h_stats, ctx->d_stats, sizeof(ScreenStats), cudaMemcpyDeviceToHost, ctx->stream));
   JSI_CUDA(cudaStreamSynchronize(ctx->stream));
   JSI_CUDA(cudaGetLastError());
+  if (ctx->timing) resolve_timing(ctx);
 }
 
 int bit_width(unsigned long long x) {
@@ -368,8 +424,8 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
   RegionRec<T> *dreg = ar.get<RegionRec<T>>(2);
   int *dmap = ar.get<int>(2);
   const int zeros[2] = {0, 0};
-  JSI_CUDA(cudaMemcpyAsync(dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
   SideRound<T> A = make_side<T>(ar, make_geom(ta->nuv, p1_of(sa)), 1, false, dreg);
   SideRound<T> B = make_side<T>(ar, make_geom(tb->nuv, p1_of(sb)), 1, false, dreg + 1);
   const int *map1 = dmap, *map2 = dmap + 1;
@@ -386,13 +442,13 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
     unsigned long long cand_cap = 1ull << 20;
     DistCand<T> *cand = ar.get<DistCand<T>>(cand_cap);
     reset_stats(ctx);
-    launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, st);
-    launch_dist_cull(A, B, map1, map2, nslots, surv, tile_pairs, ctx->d_stats, st);
+    timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, st); });
+    timed(ctx, "dist_cull", [&] { launch_dist_cull(A, B, map1, map2, nslots, surv, tile_pairs, ctx->d_stats, st); });
     pull_stats(ctx);
     const unsigned long long nsurv = ctx->h_stats->survivors;
     for (int attempt = 0;; ++attempt) {
-      launch_dist_leaf(A, B, map1, map2, nslots, surv, nsurv, k, cand, cand_cap, ctx->d_stats, st);
-      launch_dist_select(cand, cand_cap, k, top, ctx->d_stats, st);
+      timed(ctx, "dist_leaf", [&] { launch_dist_leaf(A, B, map1, map2, nslots, surv, nsurv, k, cand, cand_cap, ctx->d_stats, st); });
+      timed(ctx, "dist_select", [&] { launch_dist_select(cand, cand_cap, k, top, ctx->d_stats, st); });
       pull_stats(ctx);
       ScreenStats &hs = *ctx->h_stats;
       if (hs.candidates <= cand_cap && hs.status == 0) break;
@@ -405,7 +461,7 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
       hs.candidates = 0;
       hs.pair_tests = 0;
       hs.status = 0;
-      JSI_CUDA(cudaMemcpyAsync(ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+      JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
     }
     const ScreenStats hs = *ctx->h_stats;
     const int n = hs.nsel;
@@ -413,7 +469,7 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
     out->pair_tests[round - 1] = static_cast<long long>(hs.pair_tests);
     out->candidates[round - 1] = static_cast<long long>(hs.candidates);
     if (n > 0) {
-      JSI_CUDA(cudaMemcpyAsync(htop.data(), top, sizeof(DistCand<T>) * n, cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(copy_async(ctx, htop.data(), top, sizeof(DistCand<T>) * n, cudaMemcpyDeviceToHost, st));
       JSI_CUDA(cudaStreamSynchronize(st));
       out->kth_d2[round - 1] = static_cast<double>(htop[n - 1].d2);
       if (out->trace_pairs && static_cast<long long>(round) * k <= out->trace_cap) {
@@ -438,7 +494,7 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
     // Next round (nuv = next_nuv after round 1, distance_analysis.cu:389).
     RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
     int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
-    launch_dist_next(top, ctx->d_stats, A, B, map1, map2, p->nuv_refine, next1, next2, nmap1, nmap2, st);
+    timed(ctx, "dist_next", [&] { launch_dist_next(top, ctx->d_stats, A, B, map1, map2, p->nuv_refine, next1, next2, nmap1, nmap2, st); });
     pull_stats(ctx);
     const int r1 = ctx->h_stats->nreg1, r2 = ctx->h_stats->nreg2;
     A = make_side<T>(ar, make_geom(p->nuv_refine, p1_of(sa)), r1, false, next1);
@@ -475,8 +531,8 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
   RegionRec<T> *dreg = ar.get<RegionRec<T>>(2);
   int *dmap = ar.get<int>(2);
   const int zeros[2] = {0, 0};
-  JSI_CUDA(cudaMemcpyAsync(dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(cudaMemcpyAsync(dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
   SideRound<T> A = make_side<T>(ar, make_geom(ta->nuv, p1_of(sa)), 1, true, dreg);
   SideRound<T> B = make_side<T>(ar, make_geom(tb->nuv, p1_of(sb)), 1, true, dreg + 1);
   const int *map1 = dmap, *map2 = dmap + 1;
@@ -490,8 +546,8 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
     build_side(ctx, vb, B, true, use_k, span_u[sbu], span_v[sbu]);
     if (round == 1) {
       T pads[2];
-      JSI_CUDA(cudaMemcpyAsync(&pads[0], A.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
-      JSI_CUDA(cudaMemcpyAsync(&pads[1], B.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(copy_async(ctx, &pads[0], A.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(copy_async(ctx, &pads[1], B.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
       JSI_CUDA(cudaStreamSynchronize(st));
       out->pad[0] = static_cast<double>(pads[0]);
       out->pad[1] = static_cast<double>(pads[1]);
@@ -504,13 +560,13 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
     if (2 * ij_bits + slot_bits > 64) fail(JSI_ERR_CAPACITY, "pair key does not fit 64 bits");
     unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
     reset_stats(ctx);
-    launch_inter_cull(A, B, map1, map2, static_cast<int>(nslots), surv, tile_pairs, ctx->d_stats, st);
+    timed(ctx, "inter_cull", [&] { launch_inter_cull(A, B, map1, map2, static_cast<int>(nslots), surv, tile_pairs, ctx->d_stats, st); });
     pull_stats(ctx);
     const unsigned long long nsurv = ctx->h_stats->survivors;
     unsigned long long key_cap = std::max<unsigned long long>(1ull << 16, std::min<unsigned long long>(nsurv * 64, 1ull << 24));
     unsigned long long *keys = ar.get<unsigned long long>(key_cap);
     for (int attempt = 0;; ++attempt) {
-      launch_inter_leaf(A, B, map1, map2, surv, nsurv, ij_bits, keys, key_cap, ctx->d_stats, st);
+      timed(ctx, "inter_leaf", [&] { launch_inter_leaf(A, B, map1, map2, surv, nsurv, ij_bits, keys, key_cap, ctx->d_stats, st); });
       pull_stats(ctx);
       ScreenStats &hs = *ctx->h_stats;
       if (hs.candidates <= key_cap) break;
@@ -519,7 +575,7 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
       keys = ar.get<unsigned long long>(key_cap);
       hs.candidates = 0;
       hs.pair_tests = 0;
-      JSI_CUDA(cudaMemcpyAsync(ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+      JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
     }
     const long long n = static_cast<long long>(ctx->h_stats->candidates);
     out->counts[round - 1] = n;
@@ -537,12 +593,14 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
       cub::DoubleBuffer<unsigned long long> db(keys, alt);
       JSI_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
       void *tmp = ar.alloc(tmp_bytes);
-      JSI_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
+      timed(ctx, "sort_pairs", [&] {
+        JSI_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
+      });
       sorted = db.Current();
     }
     if (out->trace_pairs && n > 0) {
       hkeys.resize(n);
-      JSI_CUDA(cudaMemcpyAsync(hkeys.data(), sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(copy_async(ctx, hkeys.data(), sorted, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
       JSI_CUDA(cudaStreamSynchronize(st));
       const unsigned long long mij = (1ull << ij_bits) - 1ull;
       for (long long q = 0; q < n; ++q) {
@@ -563,7 +621,7 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
     int *idx = ar.get<int>(n), *idxs = ar.get<int>(n);
     unsigned *flag1 = ar.get<unsigned>(n), *ex1 = ar.get<unsigned>(n), *flag2 = ar.get<unsigned>(n),
              *ex2 = ar.get<unsigned>(n);
-    launch_inter_prep(sorted, n, ij_bits, key2, idx, flag1, st);
+    timed(ctx, "inter_prep", [&] { launch_inter_prep(sorted, n, ij_bits, key2, idx, flag1, st); });
     size_t tb1 = 0, tb2 = 0, tb3 = 0;
     JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb1, flag1, ex1, static_cast<int>(n), st));
     JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key2, key2s, idx, idxs, static_cast<int>(n), 0,
@@ -575,18 +633,18 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
     tbs = std::max(tb1, std::max(tb2, tb3));
     JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tbs, key2, key2s, idx, idxs, static_cast<int>(n), 0,
                                              ij_bits + slot_bits, st));
-    launch_flag_runs(key2s, n, flag2, st);
+    timed(ctx, "flag_runs", [&] { launch_flag_runs(key2s, n, flag2, st); });
     tbs = std::max(tb1, std::max(tb2, tb3));
     JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag2, ex2, static_cast<int>(n), st));
     RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
     int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
-    launch_inter_side1(sorted, n, ij_bits, flag1, ex1, A, map1, next1, nmap1, st);
-    launch_inter_side2(key2s, idxs, n, ij_bits, flag2, ex2, B, map2, next2, nmap2, st);
+    timed(ctx, "inter_side1", [&] { launch_inter_side1(sorted, n, ij_bits, flag1, ex1, A, map1, next1, nmap1, st); });
+    timed(ctx, "inter_side2", [&] { launch_inter_side2(key2s, idxs, n, ij_bits, flag2, ex2, B, map2, next2, nmap2, st); });
     unsigned tail[4];
-    JSI_CUDA(cudaMemcpyAsync(&tail[0], ex1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(cudaMemcpyAsync(&tail[1], flag1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(cudaMemcpyAsync(&tail[2], ex2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(cudaMemcpyAsync(&tail[3], flag2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(copy_async(ctx, &tail[0], ex1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(copy_async(ctx, &tail[1], flag1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(copy_async(ctx, &tail[2], ex2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(copy_async(ctx, &tail[3], flag2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     JSI_CUDA(cudaStreamSynchronize(st));
     JSI_CUDA(cudaGetLastError());
     const int r1 = static_cast<int>(tail[0] + tail[1]), r2 = static_cast<int>(tail[2] + tail[3]);
@@ -669,6 +727,11 @@ int jsi_destroy(jsi_context *ctx) {
   ctx->surfaces.clear();
   if (ctx->d_stats) cudaFree(ctx->d_stats);
   if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+  for (auto &p : ctx->pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -711,6 +774,54 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id) {
 int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out) {
   if (!ctx || !out) return JSI_ERR_INVALID;
   *out = ctx->resident;
+  return JSI_OK;
+}
+
+int jsi_context_stream(jsi_context *ctx, void **stream) {
+  if (!ctx || !stream) return JSI_ERR_INVALID;
+  *stream = static_cast<void *>(ctx->stream);
+  return JSI_OK;
+}
+
+int jsi_transfer_bytes(const jsi_context *ctx, unsigned long long *h2d, unsigned long long *d2h) {
+  if (!ctx || !h2d || !d2h) return JSI_ERR_INVALID;
+  *h2d = ctx->h2d_bytes;
+  *d2h = ctx->d2h_bytes;
+  return JSI_OK;
+}
+
+int jsi_kernel_timing(jsi_context *ctx, int enable) {
+  if (!ctx) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->timing = enable != 0;
+  ctx->kernel_ms.clear();
+  ctx->pending.clear();
+  return JSI_OK;
+}
+
+int jsi_kernel_time(jsi_context *ctx, const char *name, double *total_ms, long long *launches) {
+  if (!ctx || !name || !total_ms || !launches) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->kernel_ms.find(name);
+  *total_ms = it == ctx->kernel_ms.end() ? 0.0 : it->second.first;
+  *launches = it == ctx->kernel_ms.end() ? 0 : it->second.second;
+  return JSI_OK;
+}
+
+const char *jsi_kernel_names(jsi_context *ctx) {
+  if (!ctx) return "";
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->kernel_names.clear();
+  for (auto &kv : ctx->kernel_ms) {
+    if (!ctx->kernel_names.empty()) ctx->kernel_names += ",";
+    ctx->kernel_names += kv.first;
+  }
+  return ctx->kernel_names.c_str();
+}
+
+int jsi_launch_count(unsigned long long *out) {
+  if (!out) return JSI_ERR_INVALID;
+  *out = jsi::launch_count();
   return JSI_OK;
 }
 
@@ -764,6 +875,7 @@ int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, con
     JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     JSI_CUDA(cudaEventSynchronize(ctx->ev1));
     JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
+    if (ctx->timing) resolve_timing(ctx);
     return JSI_OK;
   });
 }
@@ -797,6 +909,7 @@ int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const 
     JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     JSI_CUDA(cudaEventSynchronize(ctx->ev1));
     JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
+    if (ctx->timing) resolve_timing(ctx);
     return JSI_OK;
   });
 }
@@ -818,7 +931,7 @@ int eval_grid_impl(jsi_context *ctx, const int ivec[7], const float *data, int n
     T *d = ctx->arena.get<T>(n);
     launch_records(view<T>(s), ustep, vstep, ustart, vstart, nuv, d, ctx->stream);
     JSI_CUDA(cudaGetLastError());
-    JSI_CUDA(cudaMemcpyAsync(results, d, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    JSI_CUDA(copy_async(ctx, results, d, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
     JSI_CUDA(cudaStreamSynchronize(ctx->stream));
     return JSI_OK;
   });

@@ -111,6 +111,7 @@ struct ScreenStats {
 };
 
 // ---- launchers (jsi_kernels.cu) ----
+unsigned long long launch_count();  // kernels launched so far (all contexts)
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st);
 template <typename T>

@@ -15,6 +15,7 @@
 //   intersect   k_inter_cull -> k_inter_leaf -> (device radix sort) -> k_inter_* dedup
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cfloat>
 #include <climits>
 #include <cstdint>
@@ -1069,7 +1070,13 @@ inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
   return static_cast<int>(g);
 }
 
+std::atomic<unsigned long long> g_launches{0};
+
+inline void counted(int n = 1) { g_launches.fetch_add(static_cast<unsigned long long>(n), std::memory_order_relaxed); }
+
 }  // namespace
+
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------------------
 // Launchers
@@ -1077,6 +1084,7 @@ inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
 
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(sr.nreg) * 2 * sr.g.nuv;
   const int maxdeg = s.degu > s.degv ? s.degu : s.degv;
   if (maxdeg < 8)
@@ -1089,29 +1097,34 @@ void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st)
 
 template <typename T>
 void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(sr.nreg) * sr.g.nuv * sr.g.nuv;
   k_samples<T><<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, sr, need_k ? 1 : 0);
 }
 
 template <typename T>
 void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaStream_t st) {
+  counted();
   k_pad<T><<<(sr.nreg + 127) / 128, 128, 0, st>>>(sr, use_k ? 1 : 0, span_u0, span_v0);
 }
 
 template <typename T>
 void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(sr.nreg) * sr.g.cpr;
   k_cells<T><<<grid_for(n, 256, 148 * 32), 256, 0, st>>>(sr, intersect ? 1 : 0);
 }
 
 template <typename T>
 void launch_tiles(const SideRound<T> &sr, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(sr.nreg) * sr.g.ntiles;
   k_tiles<T><<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(sr);
 }
 
 template <typename T>
 void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(nuv) * nuv;
   k_records<T><<<grid_for(n, 64, 148 * 32), 64, 0, st>>>(s, ustep, vstep, ustart, vstart, nuv, out);
 }
@@ -1119,6 +1132,7 @@ void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, 
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                      int k, ScreenStats *stats, cudaStream_t st) {
+  counted();
   const unsigned long long total = static_cast<unsigned long long>(nslots) * a.g.ntiles * b.g.ntiles;
   const int per_thread = 4;
   const unsigned long long chunk = 1024ull * per_thread;
@@ -1130,6 +1144,7 @@ void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *ma
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                       unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
   k_dist_cull<T><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats);
 }
@@ -1138,6 +1153,7 @@ template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                       const unsigned long long *surv, unsigned long long nsurv, int k, DistCand<T> *cand,
                       unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st) {
+  counted();
   (void)nslots;
   if (nsurv == 0) return;
   const int blocks = static_cast<int>(nsurv < 148ull * 8 ? nsurv : 148ull * 8);
@@ -1147,6 +1163,7 @@ void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *m
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
                         ScreenStats *stats, cudaStream_t st) {
+  counted();
   const size_t smem = sizeof(DistCand<T>) * kSelectCap;
   static bool configured = false;
   if (!configured) {
@@ -1160,12 +1177,14 @@ template <typename T>
 void launch_dist_next(const DistCand<T> *top, ScreenStats *stats, const SideRound<T> &a, const SideRound<T> &b,
                       const int *map1, const int *map2, int nuv_next, RegionRec<T> *next1, RegionRec<T> *next2,
                       int *nmap1, int *nmap2, cudaStream_t st) {
+  counted();
   k_dist_next<T><<<1, 1024, 0, st>>>(top, stats, a, b, map1, map2, nuv_next, next1, next2, nmap1, nmap2);
 }
 
 template <typename T>
 void launch_inter_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                        unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st) {
+  counted();
   const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
   k_inter_cull<T><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats);
 }
@@ -1174,6 +1193,7 @@ template <typename T>
 void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                        const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
                        unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st) {
+  counted();
   if (nsurv == 0) return;
   const int blocks = static_cast<int>(nsurv < 148ull * 8 ? nsurv : 148ull * 8);
   k_inter_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats);
@@ -1181,10 +1201,12 @@ void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *
 
 void launch_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2, int *idx,
                        unsigned *flag1, cudaStream_t st) {
+  counted();
   k_inter_prep<<<grid_for(n, 256), 256, 0, st>>>(keys, n, ij_bits, key2, idx, flag1);
 }
 
 void launch_flag_runs(const unsigned long long *sorted, long long n, unsigned *flags, cudaStream_t st) {
+  counted();
   k_flag_runs<<<grid_for(n, 256), 256, 0, st>>>(sorted, n, flags);
 }
 
@@ -1192,6 +1214,7 @@ template <typename T>
 void launch_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
                         const unsigned *ex1, const SideRound<T> &cur, const int *map1, RegionRec<T> *next,
                         int *nmap1, cudaStream_t st) {
+  counted();
   k_inter_side1<T><<<grid_for(n, 256), 256, 0, st>>>(keys, n, ij_bits, flag1, ex1, cur, map1, next, nmap1);
 }
 
@@ -1199,6 +1222,7 @@ template <typename T>
 void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
                         const unsigned *flag2, const unsigned *ex2, const SideRound<T> &cur, const int *map2,
                         RegionRec<T> *next, int *nmap2, cudaStream_t st) {
+  counted();
   k_inter_side2<T><<<grid_for(n, 256), 256, 0, st>>>(key2s, idxs, n, ij_bits, flag2, ex2, cur, map2, next, nmap2);
 }
 
