@@ -228,3 +228,18 @@ def test_intersection_random_pairs(gpu_ctx, orc, seed, precision):
     for r in range(res.rounds):
         if o["pairs"][r] is not None:
             assert np.array_equal(res.pairs[r], o["pairs"][r])
+
+
+@pytest.mark.parametrize("case", [1, 2])
+def test_intersection_degree11_reference_inputs(gpu_ctx, ref, orc, case):
+    """The reference's own degree-11 inputs (345x356 control points), read
+    from the compiled reference data when oracle/_ref is present."""
+    ia, da = ref.face(f"inter_case{case}_obj1")
+    ib, db = ref.face(f"inter_case{case}_obj2")
+    A, B = surface_from(ia, da), surface_from(ib, db)
+    res = _inter(gpu_ctx, A, B, 16, 1)
+    o = orc.inter_query(A, B, rect32(A), rect32(B), 16, 16, 1, pair_cap=1 << 20)
+    assert np.array_equal(res.counts, o["counts"])
+    for r in range(res.rounds):
+        if o["pairs"][r] is not None:
+            assert np.array_equal(res.pairs[r], o["pairs"][r])
