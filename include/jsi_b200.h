@@ -180,6 +180,21 @@ int jsi_eval_grid(jsi_context *ctx, const int ivec[7], const float *data, int nd
 int jsi_eval_grid_f64(jsi_context *ctx, const int ivec[7], const float *data, int ndata, double ustep,
                       double vstep, double ustart, double vstart, int nuv, double *results);
 
+/* The FP32 grid of jsi_eval_grid without a context and without allocating
+ * any device memory, for callers that cannot call cudaMalloc (a host
+ * application whose memory pool owns the whole device, or a loop that cannot
+ * take cudaMalloc's implicit synchronisation).  It has no counterpart in the
+ * reference.  Works on the current device; every device buffer lives in one
+ * fixed 32 MiB __device__ array that each GPU loading this code keeps until
+ * exit.  Knots, the control net (16 bytes per point) and the nuv*nuv*18 float
+ * records, each rounded up to 256 bytes, must fit in it, else
+ * JSI_ERR_CAPACITY.  The first call on a device sets up the array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the array: calls whose device work overlaps race; serialise
+ * them. */
+int jsi_eval_grid_noalloc(const int ivec[7], const float *data, int ndata, float ustep, float vstep, float ustart,
+                          float vstart, int nuv, float *results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,7 @@ EXPORTED = [
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_names",
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
+    "jsi_eval_grid_noalloc",
 ]
 
 
@@ -129,6 +130,9 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_eval_grid_f64.argtypes = [P, P, P, I, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, I, P]
     L.jsi_eval_grid_f64.restype = I
+    L.jsi_eval_grid_noalloc.argtypes = [P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                        I, P]
+    L.jsi_eval_grid_noalloc.restype = I
     if path is None:
         _lib = L
     return L

@@ -16,7 +16,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libjsi_b200.so"
-SOURCES = ["jsi_kernels.cu", "jsi_capi.cu"]
+SOURCES = ["jsi_kernels.cu", "jsi_capi.cu", "jsi_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: products and sums round separately, in the written order, so
 # the FP32 form reproduces the reference's x86 results bit for bit.  Explicit
