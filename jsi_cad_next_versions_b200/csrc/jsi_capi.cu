@@ -331,9 +331,8 @@ void build_side(jsi_context *ctx, const SurfView<T> &v, SideRound<T> &s, bool in
   timed(ctx, "basis", [&] { launch_basis(v, s, st); });
   if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
   timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); });
-  timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
+  if (intersect) timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
   timed(ctx, "cells", [&] { launch_cells(s, intersect, st); });
-  timed(ctx, "tiles", [&] { launch_tiles(s, st); });
   JSI_CUDA(cudaGetLastError());
 }
 
@@ -439,15 +438,38 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
     const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
     if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
     unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+    unsigned *surv_lb = ar.get<unsigned>(tile_pairs);
     unsigned long long cand_cap = 1ull << 20;
     DistCand<T> *cand = ar.get<DistCand<T>>(cand_cap);
     reset_stats(ctx);
     timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, st); });
-    timed(ctx, "dist_cull", [&] { launch_dist_cull(A, B, map1, map2, nslots, surv, tile_pairs, ctx->d_stats, st); });
+    timed(ctx, "dist_cull", [&] {
+      launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, st);
+    });
     pull_stats(ctx);
     const unsigned long long nsurv = ctx->h_stats->survivors;
+    // Leaf order: ascending lower bound, so that the first tile pairs tighten
+    // tau and the rest stop early (exactness does not depend on the order).
+    const unsigned long long *leaf_surv = surv;
+    const unsigned *leaf_lb = nullptr;
+    if (nsurv > 2048) {
+      unsigned long long *surv_alt = ar.get<unsigned long long>(nsurv);
+      unsigned *lb_alt = ar.get<unsigned>(nsurv);
+      cub::DoubleBuffer<unsigned> kb(surv_lb, lb_alt);
+      cub::DoubleBuffer<unsigned long long> vb(surv, surv_alt);
+      size_t tmp_bytes = 0;
+      JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, static_cast<int>(nsurv), 0, 32, st));
+      void *tmp = ar.alloc(tmp_bytes);
+      timed(ctx, "sort_tiles", [&] {
+        JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kb, vb, static_cast<int>(nsurv), 0, 32, st));
+      });
+      leaf_surv = vb.Current();
+      leaf_lb = kb.Current();
+    }
     for (int attempt = 0;; ++attempt) {
-      timed(ctx, "dist_leaf", [&] { launch_dist_leaf(A, B, map1, map2, nslots, surv, nsurv, k, cand, cand_cap, ctx->d_stats, st); });
+      timed(ctx, "dist_leaf", [&] {
+        launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, nsurv, k, cand, cand_cap, ctx->d_stats, st);
+      });
       timed(ctx, "dist_select", [&] { launch_dist_select(cand, cand_cap, k, top, ctx->d_stats, st); });
       pull_stats(ctx);
       ScreenStats &hs = *ctx->h_stats;
@@ -461,6 +483,7 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
       hs.candidates = 0;
       hs.pair_tests = 0;
       hs.status = 0;
+      hs.work = 0;
       JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
     }
     const ScreenStats hs = *ctx->h_stats;
@@ -575,6 +598,7 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
       keys = ar.get<unsigned long long>(key_cap);
       hs.candidates = 0;
       hs.pair_tests = 0;
+      hs.work = 0;
       JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
     }
     const long long n = static_cast<long long>(ctx->h_stats->candidates);

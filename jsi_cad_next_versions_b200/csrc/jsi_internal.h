@@ -108,7 +108,13 @@ struct ScreenStats {
   int nsel;                         // pairs kept by the select
   int nreg1, nreg2;                 // unique regions built for the next round
   int pad_;
+  unsigned long long work;          // work counter of the persistent leaf kernels
 };
+
+// A surviving tile pair: (row = slot * ntiles1 + t1) << 32 | t2.
+__host__ __device__ inline unsigned long long pack_tile_pair(unsigned row, unsigned t2) {
+  return (static_cast<unsigned long long>(row) << 32) | t2;
+}
 
 // ---- launchers (jsi_kernels.cu) ----
 unsigned long long launch_count();  // kernels launched so far (all contexts)
@@ -121,8 +127,6 @@ void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaSt
 template <typename T>
 void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st);
 template <typename T>
-void launch_tiles(const SideRound<T> &sr, cudaStream_t st);
-template <typename T>
 void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st);
 
 template <typename T>
@@ -130,11 +134,13 @@ void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *ma
                      int k, ScreenStats *stats, cudaStream_t st);
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                      unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st);
+                      unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
+                      cudaStream_t st);
+// surv_lb may be null (no early exit); when given, surv must be sorted by it.
 template <typename T>
-void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                      const unsigned long long *surv, unsigned long long nsurv, int k, DistCand<T> *cand,
-                      unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st);
+void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                      const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
+                      DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st);
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
                         ScreenStats *stats, cudaStream_t st);

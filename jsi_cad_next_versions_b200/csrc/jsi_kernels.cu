@@ -9,8 +9,7 @@
 // Work decomposition (B200: 148 SMs, 32-wide warps):
 //   k_basis     one thread per (region, direction, grid line)
 //   k_samples   one thread per (region, sample)
-//   k_cells     one thread per (region, padded tile-major cell)
-//   k_tiles     one thread per (region, tile)
+//   k_cells     one warp per (region, tile): cells and the tile's bounds
 //   distance    k_dist_tau -> k_dist_cull -> k_dist_leaf -> k_dist_select -> k_dist_next
 //   intersect   k_inter_cull -> k_inter_leaf -> (device radix sort) -> k_inter_* dedup
 #include <cuda_runtime.h>
@@ -415,93 +414,93 @@ __global__ void k_pad(SideRound<T> sr, int use_k, T span_u0, T span_v0) {
   sr.pad[r] = pad;
 }
 
+template <typename T>
+__device__ __forceinline__ T pos_inf();
+template <>
+__device__ __forceinline__ float pos_inf<float>() {
+  return __uint_as_float(0x7f800000u);
+}
+template <>
+__device__ __forceinline__ double pos_inf<double>() {
+  return __longlong_as_double(0x7ff0000000000000ll);
+}
+
 // Cell boxes from 4 corner samples, tile-major (distance_analysis.cu:45-86,
-// intersection.cu:106-148).  Half spans are stored without the padding; the
-// screen forms radius = half + pad exactly as the reference does.
+// intersection.cu:106-148), one warp per tile (<= 64 cells, 2 per lane); the
+// same warp reduces the tile's centre range and largest half span.  Half spans
+// are stored without the padding; the screen forms radius = half + pad exactly
+// as the reference does.
 template <typename T>
 __global__ void k_cells(SideRound<T> sr, int intersect) {
   const Geom g = sr.g;
-  const long long total = static_cast<long long>(sr.nreg) * g.cpr;
+  const int lane = threadIdx.x & 31;
+  const long long ntile_total = static_cast<long long>(sr.nreg) * g.ntiles;
   const int te2 = g.te * g.te;
-  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
-       t += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int r = static_cast<int>(t / g.cpr);
-    const int c = static_cast<int>(t % g.cpr);
-    const int tile = c / te2, local = c % te2;
-    const int iv = (tile / g.tw) * g.te + local / g.te;
-    const int iu = (tile % g.tw) * g.te + local % g.te;
-    Vec4<T> cen{T(0), T(0), T(0), T(0)}, hal{T(0), T(0), T(0), T(0)};
-    if (iv < g.W && iu < g.W) {
-      const Vec4<T> *S = sr.samples + static_cast<long long>(r) * g.nuv * g.nuv;
-      const Vec4<T> p0 = S[iv * g.nuv + iu];
-      const Vec4<T> p1 = S[iv * g.nuv + iu + 1];
-      const Vec4<T> p2 = S[(iv + 1) * g.nuv + iu];
-      const Vec4<T> p3 = S[(iv + 1) * g.nuv + iu + 1];
-      const T lx = tmin(p0.x, tmin(p1.x, tmin(p2.x, p3.x)));
-      const T ly = tmin(p0.y, tmin(p1.y, tmin(p2.y, p3.y)));
-      const T lz = tmin(p0.z, tmin(p1.z, tmin(p2.z, p3.z)));
-      const T hx = tmax(p0.x, tmax(p1.x, tmax(p2.x, p3.x)));
-      const T hy = tmax(p0.y, tmax(p1.y, tmax(p2.y, p3.y)));
-      const T hz = tmax(p0.z, tmax(p1.z, tmax(p2.z, p3.z)));
-      if (intersect) {
-        cen.x = (lx + hx) / T(2);
-        cen.y = (ly + hy) / T(2);
-        cen.z = (lz + hz) / T(2);
-      } else {
-        cen.x = (lx - T(0) + hx + T(0)) / T(2);
-        cen.y = (ly - T(0) + hy + T(0)) / T(2);
-        cen.z = (lz - T(0) + hz + T(0)) / T(2);
-      }
-      hal.x = (hx - lx) / T(2);
-      hal.y = (hy - ly) / T(2);
-      hal.z = (hz - lz) / T(2);
-    }
-    sr.center[t] = cen;
-    if (intersect) sr.half[t] = hal;
-  }
-}
-
-// Tile bounds: range of the centres and max half span of every tile.
-template <typename T>
-__global__ void k_tiles(SideRound<T> sr) {
-  const Geom g = sr.g;
-  const long long total = static_cast<long long>(sr.nreg) * g.ntiles;
-  const int te2 = g.te * g.te;
-  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
-       t += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int tile = static_cast<int>(t % g.ntiles);
-    const int ty = tile / g.tw, tx = tile % g.tw;
+  const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  for (long long t = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; t < ntile_total;
+       t += nwarps) {
+    const int r = static_cast<int>(t / g.ntiles);
+    const int tile = static_cast<int>(t - static_cast<long long>(r) * g.ntiles);
+    const int ty = tile / g.tw, tx = tile - (tile / g.tw) * g.tw;
     const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
-    const Vec4<T> *C = sr.center + t * te2;
-    const Vec4<T> *H = sr.half ? sr.half + t * te2 : nullptr;
-    Vec4<T> lo{T(0), T(0), T(0), T(0)}, hi{T(0), T(0), T(0), T(0)}, hm{T(0), T(0), T(0), T(0)};
-    bool first = true;
-    for (int a = 0; a < nv; ++a) {
-      for (int b = 0; b < nu; ++b) {
-        const Vec4<T> c = C[a * g.te + b];
-        if (first) {
-          lo = c;
-          hi = c;
-          first = false;
+    const Vec4<T> *S = sr.samples + static_cast<long long>(r) * g.nuv * g.nuv;
+    T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
+    T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
+    T hm[3] = {T(0), T(0), T(0)};
+    for (int local = lane; local < te2; local += 32) {
+      const int a = local / g.te, b = local - (local / g.te) * g.te;
+      Vec4<T> cen{T(0), T(0), T(0), T(0)}, hal{T(0), T(0), T(0), T(0)};
+      if (a < nv && b < nu) {
+        const int iv = ty * g.te + a, iu = tx * g.te + b;
+        const Vec4<T> p0 = S[iv * g.nuv + iu];
+        const Vec4<T> p1 = S[iv * g.nuv + iu + 1];
+        const Vec4<T> p2 = S[(iv + 1) * g.nuv + iu];
+        const Vec4<T> p3 = S[(iv + 1) * g.nuv + iu + 1];
+        const T lx = tmin(p0.x, tmin(p1.x, tmin(p2.x, p3.x)));
+        const T ly = tmin(p0.y, tmin(p1.y, tmin(p2.y, p3.y)));
+        const T lz = tmin(p0.z, tmin(p1.z, tmin(p2.z, p3.z)));
+        const T hx = tmax(p0.x, tmax(p1.x, tmax(p2.x, p3.x)));
+        const T hy = tmax(p0.y, tmax(p1.y, tmax(p2.y, p3.y)));
+        const T hz = tmax(p0.z, tmax(p1.z, tmax(p2.z, p3.z)));
+        if (intersect) {
+          cen.x = (lx + hx) / T(2);
+          cen.y = (ly + hy) / T(2);
+          cen.z = (lz + hz) / T(2);
         } else {
-          lo.x = tmin(lo.x, c.x);
-          lo.y = tmin(lo.y, c.y);
-          lo.z = tmin(lo.z, c.z);
-          hi.x = tmax(hi.x, c.x);
-          hi.y = tmax(hi.y, c.y);
-          hi.z = tmax(hi.z, c.z);
+          cen.x = (lx - T(0) + hx + T(0)) / T(2);
+          cen.y = (ly - T(0) + hy + T(0)) / T(2);
+          cen.z = (lz - T(0) + hz + T(0)) / T(2);
         }
-        if (H) {
-          const Vec4<T> h = H[a * g.te + b];
-          hm.x = tmax(hm.x, h.x);
-          hm.y = tmax(hm.y, h.y);
-          hm.z = tmax(hm.z, h.z);
-        }
+        hal.x = (hx - lx) / T(2);
+        hal.y = (hy - ly) / T(2);
+        hal.z = (hz - lz) / T(2);
+        lo[0] = tmin(lo[0], cen.x);
+        lo[1] = tmin(lo[1], cen.y);
+        lo[2] = tmin(lo[2], cen.z);
+        hi[0] = tmax(hi[0], cen.x);
+        hi[1] = tmax(hi[1], cen.y);
+        hi[2] = tmax(hi[2], cen.z);
+        hm[0] = tmax(hm[0], hal.x);
+        hm[1] = tmax(hm[1], hal.y);
+        hm[2] = tmax(hm[2], hal.z);
+      }
+      sr.center[t * te2 + local] = cen;
+      if (intersect) sr.half[t * te2 + local] = hal;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = tmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+        hi[c] = tmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+        hm[c] = tmax(hm[c], __shfl_xor_sync(kFull, hm[c], o));
       }
     }
-    sr.tlo[t] = lo;
-    sr.thi[t] = hi;
-    if (sr.thmax) sr.thmax[t] = hm;
+    if (lane == 0) {
+      sr.tlo[t] = Vec4<T>{lo[0], lo[1], lo[2], T(0)};
+      sr.thi[t] = Vec4<T>{hi[0], hi[1], hi[2], T(0)};
+      if (sr.thmax) sr.thmax[t] = Vec4<T>{hm[0], hm[1], hm[2], T(0)};
+    }
   }
 }
 
@@ -533,20 +532,6 @@ __global__ void k_records(SurfView<T> s, T ustep, T vstep, T ustart, T vstart, i
 // Screening helpers
 // ---------------------------------------------------------------------------
 
-struct PairDecode {
-  int slot, t1, t2;
-};
-
-__device__ __forceinline__ PairDecode decode_pair(unsigned long long q, int nt1, int nt2) {
-  const unsigned long long per = static_cast<unsigned long long>(nt1) * nt2;
-  PairDecode d;
-  d.slot = static_cast<int>(q / per);
-  const unsigned long long rem = q % per;
-  d.t1 = static_cast<int>(rem / nt2);
-  d.t2 = static_cast<int>(rem % nt2);
-  return d;
-}
-
 // Squared centre distance, distance_analysis.cu:202-207.
 template <typename T>
 __device__ __forceinline__ T center_d2(const Vec4<T> &a, const Vec4<T> &b) {
@@ -574,10 +559,6 @@ __device__ __forceinline__ T tile_lb(const Vec4<T> &lo1, const Vec4<T> &hi1, con
   return gx * gx + gy * gy + gz * gz;
 }
 
-__device__ __forceinline__ int tile_extent(int t, int tw, int te, int W, int axis_v) {
-  const int c = axis_v ? t / tw : t % tw;
-  return min(te, W - c * te);
-}
 
 // Bitonic sort of n (power of two) unsigned keys in shared memory, ascending.
 __device__ void bitonic_u32(unsigned *a, int n) {
@@ -617,114 +598,160 @@ __device__ void fold_tau(unsigned my_bits, int k, unsigned *tau, unsigned *sh) {
 // Distance screening
 // ---------------------------------------------------------------------------
 
-// Threshold seed: representative cell pair (the centre cells of both tiles)
-// of every tile pair; each block folds the k-th smallest of its per-thread
-// minima into tau.
+// Representative cell of a tile: its middle cell (always valid).
+__device__ __forceinline__ int tile_rep(int t, const Geom &g) {
+  const int ty = t / g.tw, tx = t - (t / g.tw) * g.tw;
+  const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
+  return (nv / 2) * g.te + nu / 2;
+}
+
+// Lower bound as float bits, rounded down (ordering key of the survivors).
+__device__ __forceinline__ unsigned lb_bits_down(float x) { return __float_as_uint(x); }
+__device__ __forceinline__ unsigned lb_bits_down(double x) { return __float_as_uint(__double2float_rd(x)); }
+
+// Ascending bitonic sort of one value per lane; returns the value of lane q.
+__device__ __forceinline__ unsigned warp_sorted_at(unsigned v, int q) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const unsigned o = __shfl_xor_sync(kFull, v, stride);
+      const bool asc = (lane & size) == 0 || size == 32;
+      const bool low = (lane & stride) == 0;
+      v = (low == asc) ? min(v, o) : max(v, o);
+    }
+  }
+  return __shfl_sync(kFull, v, q);
+}
+
+// Threshold seed: the representative cell pair (middle cells) of every tile
+// pair.  Rows (slot, t1) are spread over blocks, t2 over threads; each block
+// folds the k-th smallest of its per-thread minima into tau.
 template <typename T>
-__global__ void __launch_bounds__(1024) k_dist_tau(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
-                                                   int nslots, int k, ScreenStats *stats, int per_thread) {
-  __shared__ unsigned sh[1024];
+__global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b, const int *map1,
+                                                  const int *map2, int nslots, int k, ScreenStats *stats) {
+  __shared__ unsigned sh[256];
   const Geom g1 = a.g, g2 = b.g;
-  const unsigned long long total = static_cast<unsigned long long>(nslots) * g1.ntiles * g2.ntiles;
-  const unsigned long long chunk = static_cast<unsigned long long>(blockDim.x) * per_thread;
-  const unsigned long long start = blockIdx.x * chunk;
+  const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
+  const int nrows = nslots * g1.ntiles;
   float best = __uint_as_float(0x7f800000u);
-  for (int it = 0; it < per_thread; ++it) {
-    const unsigned long long q = start + static_cast<unsigned long long>(it) * blockDim.x + threadIdx.x;
-    if (q >= total) break;
-    const PairDecode d = decode_pair(q, g1.ntiles, g2.ntiles);
-    const int r1 = map1[d.slot], r2 = map2[d.slot];
-    const int nv1 = tile_extent(d.t1, g1.tw, g1.te, g1.W, 1), nu1 = tile_extent(d.t1, g1.tw, g1.te, g1.W, 0);
-    const int nv2 = tile_extent(d.t2, g2.tw, g2.te, g2.W, 1), nu2 = tile_extent(d.t2, g2.tw, g2.te, g2.W, 0);
-    const int l1 = (nv1 / 2) * g1.te + nu1 / 2, l2 = (nv2 / 2) * g2.te + nu2 / 2;
-    const Vec4<T> c1 = a.center[(static_cast<long long>(r1) * g1.ntiles + d.t1) * g1.te * g1.te + l1];
-    const Vec4<T> c2 = b.center[(static_cast<long long>(r2) * g2.ntiles + d.t2) * g2.te * g2.te + l2];
-    const T d2 = center_d2(c1, c2);
-    const float up = __uint_as_float(tau_bits_up(d2));
-    best = fminf(best, up);
+  for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+    const Vec4<T> c1 = a.center[(static_cast<long long>(map1[slot]) * g1.ntiles + t1) * n1 + tile_rep(t1, g1)];
+    const long long base2 = static_cast<long long>(map2[slot]) * g2.ntiles;
+    for (int t2 = threadIdx.x; t2 < g2.ntiles; t2 += blockDim.x) {
+      const Vec4<T> c2 = b.center[(base2 + t2) * n2 + tile_rep(t2, g2)];
+      best = fminf(best, __uint_as_float(tau_bits_up(center_d2(c1, c2))));
+    }
   }
   fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
 }
 
+// Tile pairs whose box-gap bound does not exceed tau survive, with the bound
+// (float, rounded down) as the key the leaf is ordered by.
 template <typename T>
 __global__ void k_dist_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
-                            unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats) {
+                            unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap,
+                            ScreenStats *stats) {
   const Geom g1 = a.g, g2 = b.g;
-  const unsigned long long total = static_cast<unsigned long long>(nslots) * g1.ntiles * g2.ntiles;
+  const int nrows = nslots * g1.ntiles;
   const T tau = tau_value<T>(stats->tau_bits);
-  for (unsigned long long base = blockIdx.x * static_cast<unsigned long long>(blockDim.x); base < total;
-       base += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
-    const unsigned long long q = base + threadIdx.x;
-    bool keep = false;
-    if (q < total) {
-      const PairDecode d = decode_pair(q, g1.ntiles, g2.ntiles);
-      const long long i1 = static_cast<long long>(map1[d.slot]) * g1.ntiles + d.t1;
-      const long long i2 = static_cast<long long>(map2[d.slot]) * g2.ntiles + d.t2;
-      const T lb = tile_lb(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
-      keep = lb <= tau;
+  for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+    const long long i1 = static_cast<long long>(map1[slot]) * g1.ntiles + t1;
+    const Vec4<T> lo1 = a.tlo[i1], hi1 = a.thi[i1];
+    const long long base2 = static_cast<long long>(map2[slot]) * g2.ntiles;
+    for (int t0 = 0; t0 < g2.ntiles; t0 += blockDim.x) {
+      const int t2 = t0 + threadIdx.x;
+      bool keep = false;
+      T lb = T(0);
+      if (t2 < g2.ntiles) {
+        lb = tile_lb(lo1, hi1, b.tlo[base2 + t2], b.thi[base2 + t2]);
+        keep = lb <= tau;
+      }
+      const long long pos = warp_append(keep, &stats->survivors);
+      if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap) {
+        surv[pos] = pack_tile_pair(static_cast<unsigned>(row), static_cast<unsigned>(t2));
+        if (surv_lb) surv_lb[pos] = lb_bits_down(lb);
+      }
     }
-    const long long pos = warp_append(keep, &stats->survivors);
-    if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap) surv[pos] = q;
   }
-  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&stats->tile_pairs, total);
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    atomicAdd(&stats->tile_pairs, static_cast<unsigned long long>(nrows) * g2.ntiles);
 }
 
-// All cell pairs of the surviving tile pairs: d2 <= tau is a candidate.
+// All cell pairs of the surviving tile pairs, one warp per tile pair taken
+// from a work counter: the tile-2 centres sit in registers (cells lane and
+// lane+32), the tile-1 centres are broadcast row by row.  A pair with
+// d2 <= tau is a candidate.  With surv sorted by its lower bound, a warp that
+// meets a bound above tau stops: every later tile pair has a larger bound and
+// tau never grows.  Warps tighten tau with the k-th smallest of their lanes'
+// minima (k <= 32); blocks do the same at exit for larger k.
 template <typename T>
 __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
-                                                   const unsigned long long *surv, unsigned long long nsurv, int k,
-                                                   DistCand<T> *cand, unsigned long long cand_cap,
-                                                   ScreenStats *stats) {
-  __shared__ Vec4<T> s1[kMaxTile * kMaxTile], s2[kMaxTile * kMaxTile];
+                                                   const unsigned long long *surv, const unsigned *surv_lb,
+                                                   unsigned long long nsurv, int k, DistCand<T> *cand,
+                                                   unsigned long long cand_cap, ScreenStats *stats) {
   __shared__ unsigned sh[256];
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
   const int n1 = te1 * te1, n2 = te2 * te2;
+  const int lane = threadIdx.x & 31;
   unsigned long long tests = 0;
-  float best = __uint_as_float(0x7f800000u);
-  for (unsigned long long w = blockIdx.x; w < nsurv; w += gridDim.x) {
-    const PairDecode d = decode_pair(surv[w], g1.ntiles, g2.ntiles);
-    const long long base1 = (static_cast<long long>(map1[d.slot]) * g1.ntiles + d.t1) * n1;
-    const long long base2 = (static_cast<long long>(map2[d.slot]) * g2.ntiles + d.t2) * n2;
-    __syncthreads();
-    for (int q = threadIdx.x; q < n1; q += blockDim.x) s1[q] = a.center[base1 + q];
-    for (int q = threadIdx.x; q < n2; q += blockDim.x) s2[q] = b.center[base2 + q];
-    __syncthreads();
-    const T tau = tau_value<T>(*reinterpret_cast<volatile unsigned *>(&stats->tau_bits));
-    const int nv1 = tile_extent(d.t1, g1.tw, te1, g1.W, 1), nu1 = tile_extent(d.t1, g1.tw, te1, g1.W, 0);
-    const int nv2 = tile_extent(d.t2, g2.tw, te2, g2.W, 1), nu2 = tile_extent(d.t2, g2.tw, te2, g2.W, 0);
-    const int ty1 = d.t1 / g1.tw, tx1 = d.t1 % g1.tw, ty2 = d.t2 / g2.tw, tx2 = d.t2 % g2.tw;
-    const int npair = n1 * n2;
-    for (int p0 = 0; p0 < npair; p0 += blockDim.x) {
-      const int p = p0 + threadIdx.x;
-      bool hit = false;
-      T d2 = T(0);
-      int ci = 0, cj = 0;
-      if (p < npair) {
-        const int l1 = p / n2, l2 = p % n2;
-        const int a1 = l1 / te1, b1 = l1 % te1, a2 = l2 / te2, b2 = l2 % te2;
-        if (a1 < nv1 && b1 < nu1 && a2 < nv2 && b2 < nu2) {
-          ++tests;
-          d2 = center_d2(s1[l1], s2[l2]);
-          best = fminf(best, __uint_as_float(tau_bits_up(d2)));
-          hit = d2 <= tau;
-          ci = (ty1 * te1 + a1) * g1.W + tx1 * te1 + b1;
-          cj = (ty2 * te2 + a2) * g2.W + tx2 * te2 + b2;
+  T best = pos_inf<T>();
+  Vec4<T> far4{pos_inf<T>(), pos_inf<T>(), pos_inf<T>(), T(0)};
+  for (;;) {
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(&stats->work, 1ull);
+    w = __shfl_sync(kFull, w, 0);
+    if (w >= nsurv) break;
+    const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
+    if (surv_lb && __uint_as_float(surv_lb[w]) > __uint_as_float(taub)) break;
+    const T tau = tau_value<T>(taub);
+    const unsigned long long q = surv[w];
+    const int row = static_cast<int>(q >> 32), t2 = static_cast<int>(q & 0xffffffffull);
+    const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+    const long long base1 = (static_cast<long long>(map1[slot]) * g1.ntiles + t1) * n1;
+    const long long base2 = (static_cast<long long>(map2[slot]) * g2.ntiles + t2) * n2;
+    const int ty1 = t1 / g1.tw, tx1 = t1 - ty1 * g1.tw, ty2 = t2 / g2.tw, tx2 = t2 - ty2 * g2.tw;
+    const int nv1 = min(te1, g1.W - ty1 * te1), nu1 = min(te1, g1.W - tx1 * te1);
+    const int nv2 = min(te2, g2.W - ty2 * te2), nu2 = min(te2, g2.W - tx2 * te2);
+    const int ja = lane, jb = lane + 32;
+    const int ja_v = ja / te2, ja_u = ja - ja_v * te2, jb_v = jb / te2, jb_u = jb - jb_v * te2;
+    const bool va = ja < n2 && ja_v < nv2 && ja_u < nu2;
+    const bool vb = jb < n2 && jb_v < nv2 && jb_u < nu2;
+    const Vec4<T> c2a = va ? b.center[base2 + ja] : far4;
+    const Vec4<T> c2b = vb ? b.center[base2 + jb] : far4;
+    const int cja = (ty2 * te2 + ja_v) * g2.W + tx2 * te2 + ja_u;
+    const int cjb = (ty2 * te2 + jb_v) * g2.W + tx2 * te2 + jb_u;
+    for (int a1 = 0; a1 < nv1; ++a1) {
+      for (int b1 = 0; b1 < nu1; ++b1) {
+        const Vec4<T> c1 = a.center[base1 + a1 * te1 + b1];
+        const T da = center_d2(c1, c2a);
+        const T db = center_d2(c1, c2b);
+        best = tmin(best, tmin(da, db));
+        const bool ha = da <= tau, hb = db <= tau;
+        if (__any_sync(kFull, ha || hb)) {
+          const int ci = (ty1 * te1 + a1) * g1.W + tx1 * te1 + b1;
+          long long pos = warp_append(ha, &stats->candidates);
+          if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap) cand[pos] = DistCand<T>{da, slot, ci, cja};
+          pos = warp_append(hb, &stats->candidates);
+          if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap) cand[pos] = DistCand<T>{db, slot, ci, cjb};
         }
       }
-      const long long pos = warp_append(hit, &stats->candidates);
-      if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap) {
-        DistCand<T> c;
-        c.d2 = d2;
-        c.slot = d.slot;
-        c.i = ci;
-        c.j = cj;
-        cand[pos] = c;
+    }
+    if (lane == 0) tests += static_cast<unsigned long long>(nv1 * nu1) * (nv2 * nu2);
+    if (k <= 32) {
+      const unsigned mine = tau_bits_up(best);
+      if (__popc(__ballot_sync(kFull, mine < taub)) >= k) {
+        const unsigned kth = warp_sorted_at(mine, k - 1);
+        if (lane == 0) atomicMin(&stats->tau_bits, kth);
       }
     }
   }
-  atomicAdd(&stats->pair_tests, tests);
-  fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+  if (lane == 0) atomicAdd(&stats->pair_tests, tests);
+  if (k > 32) fold_tau(tau_bits_up(best), k, &stats->tau_bits, sh);
 }
 
 // Total order of the top-k (distance_analysis.cu:226-231).
@@ -917,16 +944,22 @@ template <typename T>
 __global__ void k_inter_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
                              unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats) {
   const Geom g1 = a.g, g2 = b.g;
-  const unsigned long long total = static_cast<unsigned long long>(nslots) * g1.ntiles * g2.ntiles;
-  for (unsigned long long base = blockIdx.x * static_cast<unsigned long long>(blockDim.x); base < total;
-       base += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
-    const unsigned long long q = base + threadIdx.x;
+  const long long nrows = static_cast<long long>(nslots) * g1.ntiles;
+  const int lanes = blockDim.x;
+  // Rows (slot, t1) x t2 flattened so that small tile counts still fill warps.
+  const long long total = nrows * g2.ntiles;
+  for (long long base = blockIdx.x * static_cast<long long>(lanes); base < total;
+       base += static_cast<long long>(gridDim.x) * lanes) {
+    const long long e = base + threadIdx.x;
     bool keep = false;
-    if (q < total) {
-      const PairDecode d = decode_pair(q, g1.ntiles, g2.ntiles);
-      const int r1 = map1[d.slot], r2 = map2[d.slot];
-      const long long i1 = static_cast<long long>(r1) * g1.ntiles + d.t1;
-      const long long i2 = static_cast<long long>(r2) * g2.ntiles + d.t2;
+    int row = 0, t2 = 0;
+    if (e < total) {
+      row = static_cast<int>(e / g2.ntiles);
+      t2 = static_cast<int>(e - static_cast<long long>(row) * g2.ntiles);
+      const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+      const int r1 = map1[slot], r2 = map2[slot];
+      const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
+      const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
       const Vec4<T> lo1 = a.tlo[i1], hi1 = a.thi[i1], h1 = a.thmax[i1];
       const Vec4<T> lo2 = b.tlo[i2], hi2 = b.thi[i2], h2 = b.thmax[i2];
       const T p1 = a.pad[r1], p2 = b.pad[r2];
@@ -936,74 +969,89 @@ __global__ void k_inter_cull(SideRound<T> a, SideRound<T> b, const int *map1, co
       keep = !(sx || sy || sz);
     }
     const long long pos = warp_append(keep, &stats->survivors);
-    if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap) surv[pos] = q;
+    if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap)
+      surv[pos] = pack_tile_pair(static_cast<unsigned>(row), static_cast<unsigned>(t2));
   }
-  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&stats->tile_pairs, total);
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&stats->tile_pairs, static_cast<unsigned long long>(total));
 }
 
 // Strict per-axis overlap of every cell pair of the surviving tile pairs
-// (intersection.cu:46-63); hits are appended as (slot, i, j) sort keys.
+// (intersection.cu:46-63), one warp per tile pair: tile-2 centres and padded
+// radii in registers, tile-1 cells broadcast row by row; hits are appended as
+// (slot, i, j) sort keys.
 template <typename T>
 __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T> b, const int *map1,
                                                     const int *map2, const unsigned long long *surv,
                                                     unsigned long long nsurv, int ij_bits, unsigned long long *keys,
                                                     unsigned long long key_cap, ScreenStats *stats) {
-  __shared__ Vec4<T> c1s[kMaxTile * kMaxTile], c2s[kMaxTile * kMaxTile];
-  __shared__ Vec4<T> r1s[kMaxTile * kMaxTile], r2s[kMaxTile * kMaxTile];
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
   const int n1 = te1 * te1, n2 = te2 * te2;
+  const int lane = threadIdx.x & 31;
   unsigned long long tests = 0;
-  for (unsigned long long w = blockIdx.x; w < nsurv; w += gridDim.x) {
-    const PairDecode d = decode_pair(surv[w], g1.ntiles, g2.ntiles);
-    const int r1 = map1[d.slot], r2 = map2[d.slot];
-    const long long base1 = (static_cast<long long>(r1) * g1.ntiles + d.t1) * n1;
-    const long long base2 = (static_cast<long long>(r2) * g2.ntiles + d.t2) * n2;
+  const Vec4<T> zero4{T(0), T(0), T(0), T(0)};
+  const Vec4<T> neg4{-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>(), T(0)};
+  for (;;) {
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(&stats->work, 1ull);
+    w = __shfl_sync(kFull, w, 0);
+    if (w >= nsurv) break;
+    const unsigned long long q = surv[w];
+    const int row = static_cast<int>(q >> 32), t2 = static_cast<int>(q & 0xffffffffull);
+    const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+    const int r1 = map1[slot], r2 = map2[slot];
+    const long long base1 = (static_cast<long long>(r1) * g1.ntiles + t1) * n1;
+    const long long base2 = (static_cast<long long>(r2) * g2.ntiles + t2) * n2;
     const T p1 = a.pad[r1], p2 = b.pad[r2];
-    __syncthreads();
-    for (int q = threadIdx.x; q < n1; q += blockDim.x) {
-      c1s[q] = a.center[base1 + q];
-      Vec4<T> h = a.half[base1 + q];
-      h.x = h.x + p1;  // radius = x_span / 2 + curvature_padding
-      h.y = h.y + p1;
-      h.z = h.z + p1;
-      r1s[q] = h;
+    const int ty1 = t1 / g1.tw, tx1 = t1 - ty1 * g1.tw, ty2 = t2 / g2.tw, tx2 = t2 - ty2 * g2.tw;
+    const int nv1 = min(te1, g1.W - ty1 * te1), nu1 = min(te1, g1.W - tx1 * te1);
+    const int nv2 = min(te2, g2.W - ty2 * te2), nu2 = min(te2, g2.W - tx2 * te2);
+    const int ja = lane, jb = lane + 32;
+    const int ja_v = ja / te2, ja_u = ja - ja_v * te2, jb_v = jb / te2, jb_u = jb - jb_v * te2;
+    const bool va = ja < n2 && ja_v < nv2 && ja_u < nu2;
+    const bool vb = jb < n2 && jb_v < nv2 && jb_u < nu2;
+    // Invalid lanes get a zero centre and a -inf radius: |dc| < -inf never holds.
+    Vec4<T> c2a = va ? b.center[base2 + ja] : zero4, c2b = vb ? b.center[base2 + jb] : zero4;
+    Vec4<T> r2a = neg4, r2b = neg4;
+    if (va) {
+      r2a = b.half[base2 + ja];
+      r2a.x = r2a.x + p2;  // radius = x_span / 2 + curvature_padding
+      r2a.y = r2a.y + p2;
+      r2a.z = r2a.z + p2;
     }
-    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
-      c2s[q] = b.center[base2 + q];
-      Vec4<T> h = b.half[base2 + q];
-      h.x = h.x + p2;
-      h.y = h.y + p2;
-      h.z = h.z + p2;
-      r2s[q] = h;
+    if (vb) {
+      r2b = b.half[base2 + jb];
+      r2b.x = r2b.x + p2;
+      r2b.y = r2b.y + p2;
+      r2b.z = r2b.z + p2;
     }
-    __syncthreads();
-    const int nv1 = tile_extent(d.t1, g1.tw, te1, g1.W, 1), nu1 = tile_extent(d.t1, g1.tw, te1, g1.W, 0);
-    const int nv2 = tile_extent(d.t2, g2.tw, te2, g2.W, 1), nu2 = tile_extent(d.t2, g2.tw, te2, g2.W, 0);
-    const int ty1 = d.t1 / g1.tw, tx1 = d.t1 % g1.tw, ty2 = d.t2 / g2.tw, tx2 = d.t2 % g2.tw;
-    const int npair = n1 * n2;
-    for (int p0 = 0; p0 < npair; p0 += blockDim.x) {
-      const int p = p0 + threadIdx.x;
-      bool hit = false;
-      unsigned long long key = 0;
-      if (p < npair) {
-        const int l1 = p / n2, l2 = p % n2;
-        const int a1 = l1 / te1, b1 = l1 % te1, a2 = l2 / te2, b2 = l2 % te2;
-        if (a1 < nv1 && b1 < nu1 && a2 < nv2 && b2 < nu2) {
-          ++tests;
-          const Vec4<T> c1 = c1s[l1], c2 = c2s[l2], q1 = r1s[l1], q2 = r2s[l2];
-          hit = fabs(c1.x - c2.x) < (q1.x + q2.x) && fabs(c1.y - c2.y) < (q1.y + q2.y) &&
-                fabs(c1.z - c2.z) < (q1.z + q2.z);
-          const unsigned long long ci = static_cast<unsigned long long>((ty1 * te1 + a1) * g1.W + tx1 * te1 + b1);
-          const unsigned long long cj = static_cast<unsigned long long>((ty2 * te2 + a2) * g2.W + tx2 * te2 + b2);
-          key = (static_cast<unsigned long long>(d.slot) << (2 * ij_bits)) | (ci << ij_bits) | cj;
+    const unsigned long long cja = static_cast<unsigned long long>((ty2 * te2 + ja_v) * g2.W + tx2 * te2 + ja_u);
+    const unsigned long long cjb = static_cast<unsigned long long>((ty2 * te2 + jb_v) * g2.W + tx2 * te2 + jb_u);
+    const unsigned long long slot_key = static_cast<unsigned long long>(slot) << (2 * ij_bits);
+    for (int a1 = 0; a1 < nv1; ++a1) {
+      for (int b1 = 0; b1 < nu1; ++b1) {
+        const Vec4<T> c1 = a.center[base1 + a1 * te1 + b1];
+        Vec4<T> r1 = a.half[base1 + a1 * te1 + b1];
+        r1.x = r1.x + p1;
+        r1.y = r1.y + p1;
+        r1.z = r1.z + p1;
+        const bool ha = fabs(c1.x - c2a.x) < (r1.x + r2a.x) && fabs(c1.y - c2a.y) < (r1.y + r2a.y) &&
+                        fabs(c1.z - c2a.z) < (r1.z + r2a.z);
+        const bool hb = fabs(c1.x - c2b.x) < (r1.x + r2b.x) && fabs(c1.y - c2b.y) < (r1.y + r2b.y) &&
+                        fabs(c1.z - c2b.z) < (r1.z + r2b.z);
+        if (__any_sync(kFull, ha || hb)) {
+          const unsigned long long ci =
+              static_cast<unsigned long long>((ty1 * te1 + a1) * g1.W + tx1 * te1 + b1) << ij_bits;
+          long long pos = warp_append(ha, &stats->candidates);
+          if (pos >= 0 && static_cast<unsigned long long>(pos) < key_cap) keys[pos] = slot_key | ci | cja;
+          pos = warp_append(hb, &stats->candidates);
+          if (pos >= 0 && static_cast<unsigned long long>(pos) < key_cap) keys[pos] = slot_key | ci | cjb;
         }
       }
-      const long long pos = warp_append(hit, &stats->candidates);
-      if (pos >= 0 && static_cast<unsigned long long>(pos) < key_cap) keys[pos] = key;
     }
+    if (lane == 0) tests += static_cast<unsigned long long>(nv1 * nu1) * (nv2 * nu2);
   }
-  atomicAdd(&stats->pair_tests, tests);
+  if (lane == 0) atomicAdd(&stats->pair_tests, tests);
 }
 
 __global__ void k_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2,
@@ -1111,15 +1159,8 @@ void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaSt
 template <typename T>
 void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st) {
   counted();
-  const long long n = static_cast<long long>(sr.nreg) * sr.g.cpr;
-  k_cells<T><<<grid_for(n, 256, 148 * 32), 256, 0, st>>>(sr, intersect ? 1 : 0);
-}
-
-template <typename T>
-void launch_tiles(const SideRound<T> &sr, cudaStream_t st) {
-  counted();
-  const long long n = static_cast<long long>(sr.nreg) * sr.g.ntiles;
-  k_tiles<T><<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(sr);
+  const long long warps = static_cast<long long>(sr.nreg) * sr.g.ntiles;
+  k_cells<T><<<grid_for(warps * 32, 256, 148 * 32), 256, 0, st>>>(sr, intersect ? 1 : 0);
 }
 
 template <typename T>
@@ -1133,31 +1174,30 @@ template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                      int k, ScreenStats *stats, cudaStream_t st) {
   counted();
-  const unsigned long long total = static_cast<unsigned long long>(nslots) * a.g.ntiles * b.g.ntiles;
-  const int per_thread = 4;
-  const unsigned long long chunk = 1024ull * per_thread;
-  unsigned long long blocks = (total + chunk - 1) / chunk;
-  if (blocks < 1) blocks = 1;
-  k_dist_tau<T><<<static_cast<unsigned>(blocks), 1024, 0, st>>>(a, b, map1, map2, nslots, k, stats, per_thread);
+  const int rows = nslots * a.g.ntiles;
+  k_dist_tau<T><<<rows < 148 * 8 ? rows : 148 * 8, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats);
 }
 
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                      unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st) {
+                      unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
+                      cudaStream_t st) {
   counted();
-  const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
-  k_dist_cull<T><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats);
+  const int rows = nslots * a.g.ntiles;
+  const int block = b.g.ntiles >= 256 ? 256 : (b.g.ntiles >= 128 ? 128 : 64);
+  k_dist_cull<T><<<rows < 148 * 16 ? rows : 148 * 16, block, 0, st>>>(a, b, map1, map2, nslots, surv, surv_lb,
+                                                                        surv_cap, stats);
 }
 
 template <typename T>
-void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                      const unsigned long long *surv, unsigned long long nsurv, int k, DistCand<T> *cand,
-                      unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st) {
+void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                      const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
+                      DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st) {
   counted();
-  (void)nslots;
   if (nsurv == 0) return;
-  const int blocks = static_cast<int>(nsurv < 148ull * 8 ? nsurv : 148ull * 8);
-  k_dist_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, k, cand, cand_cap, stats);
+  const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
+  const int blocks = static_cast<int>((warps + 7) / 8);
+  k_dist_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, cand, cand_cap, stats);
 }
 
 template <typename T>
@@ -1195,7 +1235,8 @@ void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *
                        unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st) {
   counted();
   if (nsurv == 0) return;
-  const int blocks = static_cast<int>(nsurv < 148ull * 8 ? nsurv : 148ull * 8);
+  const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
+  const int blocks = static_cast<int>((warps + 7) / 8);
   k_inter_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats);
 }
 
@@ -1231,15 +1272,15 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
   template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t);                 \
   template void launch_pad<T>(const SideRound<T> &, bool, T, T, cudaStream_t);                                    \
   template void launch_cells<T>(const SideRound<T> &, bool, cudaStream_t);                                        \
-  template void launch_tiles<T>(const SideRound<T> &, cudaStream_t);                                              \
   template void launch_records<T>(const SurfView<T> &, T, T, T, T, int, T *, cudaStream_t);                       \
   template void launch_dist_tau<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, int, \
                                    ScreenStats *, cudaStream_t);                                                  \
   template void launch_dist_cull<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,    \
-                                    unsigned long long *, unsigned long long, ScreenStats *, cudaStream_t);       \
-  template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,    \
-                                    const unsigned long long *, unsigned long long, int, DistCand<T> *,           \
-                                    unsigned long long, ScreenStats *, cudaStream_t);                             \
+                                    unsigned long long *, unsigned *, unsigned long long, ScreenStats *,          \
+                                    cudaStream_t);                                                                \
+  template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
+                                    const unsigned long long *, const unsigned *, unsigned long long, int,        \
+                                    DistCand<T> *, unsigned long long, ScreenStats *, cudaStream_t);              \
   template void launch_dist_select<T>(const DistCand<T> *, unsigned long long, int, DistCand<T> *, ScreenStats *, \
                                       cudaStream_t);                                                              \
   template void launch_dist_next<T>(const DistCand<T> *, ScreenStats *, const SideRound<T> &,                     \
