@@ -731,7 +731,8 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
         const T da = center_d2(c1, c2a);
         const T db = center_d2(c1, c2b);
         best = tmin(best, tmin(da, db));
-        const bool ha = da <= tau, hb = db <= tau;
+        // tau is +inf until k pairs are known: padding lanes (d2 = +inf) must not pass.
+        const bool ha = va && da <= tau, hb = vb && db <= tau;
         if (__any_sync(kFull, ha || hb)) {
           const int ci = (ty1 * te1 + a1) * g1.W + tx1 * te1 + b1;
           long long pos = warp_append(ha, &stats->candidates);
