@@ -137,10 +137,12 @@ void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *m
                       unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
                       cudaStream_t st);
 // surv_lb may be null (no early exit); when given, surv must be sorted by it.
+// collect = 0: only tighten tau (no candidates); 1: append pairs with d2 <= tau.
 template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                       const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
-                      DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st);
+                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats,
+                      cudaStream_t st);
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
                         ScreenStats *stats, cudaStream_t st);

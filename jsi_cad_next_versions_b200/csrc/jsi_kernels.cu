@@ -689,9 +689,19 @@ __global__ void k_dist_cull(SideRound<T> a, SideRound<T> b, const int *map1, con
 // tau never grows.  Warps tighten tau with the k-th smallest of their lanes'
 // minima (k <= 32); blocks do the same at exit for larger k.
 template <typename T>
+__device__ __forceinline__ Vec4<T> shfl_vec(const Vec4<T> &v, int src) {
+  Vec4<T> r;
+  r.x = __shfl_sync(kFull, v.x, src);
+  r.y = __shfl_sync(kFull, v.y, src);
+  r.z = __shfl_sync(kFull, v.z, src);
+  r.w = T(0);
+  return r;
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
                                                    const unsigned long long *surv, const unsigned *surv_lb,
-                                                   unsigned long long nsurv, int k, DistCand<T> *cand,
+                                                   unsigned long long nsurv, int k, int collect, DistCand<T> *cand,
                                                    unsigned long long cand_cap, ScreenStats *stats) {
   __shared__ unsigned sh[256];
   const Geom g1 = a.g, g2 = b.g;
@@ -700,7 +710,7 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
   const int lane = threadIdx.x & 31;
   unsigned long long tests = 0;
   T best = pos_inf<T>();
-  Vec4<T> far4{pos_inf<T>(), pos_inf<T>(), pos_inf<T>(), T(0)};
+  const Vec4<T> far4{pos_inf<T>(), pos_inf<T>(), pos_inf<T>(), T(0)};
   for (;;) {
     unsigned long long w = 0;
     if (lane == 0) w = atomicAdd(&stats->work, 1ull);
@@ -723,22 +733,30 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
     const bool vb = jb < n2 && jb_v < nv2 && jb_u < nu2;
     const Vec4<T> c2a = va ? b.center[base2 + ja] : far4;
     const Vec4<T> c2b = vb ? b.center[base2 + jb] : far4;
+    // Tile-1 centres: two per lane, broadcast row by row through shuffles.
+    const Vec4<T> c1a = ja < n1 ? a.center[base1 + ja] : far4;
+    const Vec4<T> c1b = jb < n1 ? a.center[base1 + jb] : far4;
     const int cja = (ty2 * te2 + ja_v) * g2.W + tx2 * te2 + ja_u;
     const int cjb = (ty2 * te2 + jb_v) * g2.W + tx2 * te2 + jb_u;
     for (int a1 = 0; a1 < nv1; ++a1) {
       for (int b1 = 0; b1 < nu1; ++b1) {
-        const Vec4<T> c1 = a.center[base1 + a1 * te1 + b1];
+        const int l1 = a1 * te1 + b1;
+        const Vec4<T> c1 = shfl_vec(l1 < 32 ? c1a : c1b, l1 & 31);
         const T da = center_d2(c1, c2a);
         const T db = center_d2(c1, c2b);
         best = tmin(best, tmin(da, db));
-        // tau is +inf until k pairs are known: padding lanes (d2 = +inf) must not pass.
-        const bool ha = va && da <= tau, hb = vb && db <= tau;
-        if (__any_sync(kFull, ha || hb)) {
-          const int ci = (ty1 * te1 + a1) * g1.W + tx1 * te1 + b1;
-          long long pos = warp_append(ha, &stats->candidates);
-          if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap) cand[pos] = DistCand<T>{da, slot, ci, cja};
-          pos = warp_append(hb, &stats->candidates);
-          if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap) cand[pos] = DistCand<T>{db, slot, ci, cjb};
+        if (collect) {
+          // tau is +inf until k pairs are known: padding lanes (d2 = +inf) must not pass.
+          const bool ha = va && da <= tau, hb = vb && db <= tau;
+          if (__any_sync(kFull, ha || hb)) {
+            const int ci = (ty1 * te1 + a1) * g1.W + tx1 * te1 + b1;
+            long long pos = warp_append(ha, &stats->candidates);
+            if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap)
+              cand[pos] = DistCand<T>{da, slot, ci, cja};
+            pos = warp_append(hb, &stats->candidates);
+            if (pos >= 0 && static_cast<unsigned long long>(pos) < cand_cap)
+              cand[pos] = DistCand<T>{db, slot, ci, cjb};
+          }
         }
       }
     }
@@ -751,7 +769,7 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
       }
     }
   }
-  if (lane == 0) atomicAdd(&stats->pair_tests, tests);
+  if (collect && lane == 0) atomicAdd(&stats->pair_tests, tests);
   if (k > 32) fold_tau(tau_bits_up(best), k, &stats->tau_bits, sh);
 }
 
@@ -779,10 +797,25 @@ __global__ void __launch_bounds__(1024) k_dist_select(const DistCand<T> *cand, u
     return;
   }
   const int m = static_cast<int>(total);
+  // Every pair with d2 <= (true k-th d2) was appended, and the final tau is
+  // >= the true k-th d2: entries above tau can be dropped first.
+  const T tau = tau_value<T>(stats->tau_bits);
+  const unsigned long long tau_b = ordered_bits(tau);
   constexpr int kBits = sizeof(T) * 8;
-  unsigned long long kth_bits = ~0ull;
-  if (m > k) {
-    // MSD radix select of the k-th smallest d2 (non-negative: bits are ordered).
+  if (threadIdx.x == 0) s_count = 0;
+  __syncthreads();
+  for (int e = threadIdx.x; e < m; e += blockDim.x) {
+    const DistCand<T> c = cand[e];
+    if (ordered_bits(c.d2) <= tau_b) {
+      const int pos = atomicAdd(&s_count, 1);
+      if (pos < kSelectCap) buf[pos] = c;
+    }
+  }
+  __syncthreads();
+  int cnt = s_count;
+  if (cnt > kSelectCap) {
+    // MSD radix select of the k-th smallest d2 among the entries <= tau
+    // (non-negative values: the bits are ordered), then keep entries <= it.
     if (threadIdx.x == 0) {
       s_prefix = 0;
       s_mask = 0;
@@ -794,7 +827,7 @@ __global__ void __launch_bounds__(1024) k_dist_select(const DistCand<T> *cand, u
       const unsigned long long prefix = s_prefix, mask = s_mask;
       for (int e = threadIdx.x; e < m; e += blockDim.x) {
         const unsigned long long bits = ordered_bits(cand[e].d2);
-        if ((bits & mask) == prefix) atomicAdd(&hist[(bits >> shift) & 255u], 1u);
+        if (bits <= tau_b && (bits & mask) == prefix) atomicAdd(&hist[(bits >> shift) & 255u], 1u);
       }
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -810,28 +843,28 @@ __global__ void __launch_bounds__(1024) k_dist_select(const DistCand<T> *cand, u
       }
       __syncthreads();
     }
-    kth_bits = s_prefix;
-  }
-  if (threadIdx.x == 0) s_count = 0;
-  __syncthreads();
-  for (int e = threadIdx.x; e < m; e += blockDim.x) {
-    const DistCand<T> c = cand[e];
-    if (ordered_bits(c.d2) <= kth_bits) {
-      const int pos = atomicAdd(&s_count, 1);
-      if (pos < kSelectCap) buf[pos] = c;
+    const unsigned long long kth_bits = s_prefix;
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+      const DistCand<T> c = cand[e];
+      if (ordered_bits(c.d2) <= kth_bits) {
+        const int pos = atomicAdd(&s_count, 1);
+        if (pos < kSelectCap) buf[pos] = c;
+      }
     }
-  }
-  __syncthreads();
-  const int cnt = s_count;
-  if (cnt > kSelectCap) {
-    if (threadIdx.x == 0) stats->status = -4;
-    return;
+    __syncthreads();
+    cnt = s_count;
+    if (cnt > kSelectCap) {
+      if (threadIdx.x == 0) stats->status = -4;
+      return;
+    }
   }
   int n2 = 1;
   while (n2 < cnt) n2 <<= 1;
   for (int e = cnt + threadIdx.x; e < n2; e += blockDim.x) {
     DistCand<T> c;
-    c.d2 = from_ordered<T>(sizeof(T) == 4 ? 0x7f800000ull : 0x7ff0000000000000ull);
+    c.d2 = pos_inf<T>();
     c.slot = INT_MAX;
     c.i = INT_MAX;
     c.j = INT_MAX;
@@ -1193,12 +1226,14 @@ void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *m
 template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                       const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
-                      DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, cudaStream_t st) {
+                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats,
+                      cudaStream_t st) {
   counted();
   if (nsurv == 0) return;
   const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
   const int blocks = static_cast<int>((warps + 7) / 8);
-  k_dist_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, cand, cand_cap, stats);
+  k_dist_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, collect, cand, cand_cap,
+                                          stats);
 }
 
 template <typename T>
@@ -1280,7 +1315,7 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
                                     unsigned long long *, unsigned *, unsigned long long, ScreenStats *,          \
                                     cudaStream_t);                                                                \
   template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
-                                    const unsigned long long *, const unsigned *, unsigned long long, int,        \
+                                    const unsigned long long *, const unsigned *, unsigned long long, int, int,   \
                                     DistCand<T> *, unsigned long long, ScreenStats *, cudaStream_t);              \
   template void launch_dist_select<T>(const DistCand<T> *, unsigned long long, int, DistCand<T> *, ScreenStats *, \
                                       cudaStream_t);                                                              \
