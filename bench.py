@@ -351,6 +351,9 @@ def run_ours(args):
                       "result": ref_values[f]} for f, r in results.items()},
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": head["clocks"],
         "gpu_launches": head["gpu_launches"],
+        "screen": {"pair_tests_per_round": [int(x) for x in last.pair_tests],
+                   "candidates_per_round": [int(x) for x in last.candidates],
+                   "kept_per_round": [int(x) for x in last.npairs]},
         "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
     }
     print(json.dumps(line))

@@ -466,14 +466,19 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
       leaf_surv = vb.Current();
       leaf_lb = kb.Current();
     }
-    if (leaf_lb) {
-      // Tighten tau on the tile pairs with the smallest bounds before any
-      // candidate is collected, so the collecting pass appends few pairs.
-      const unsigned long long head = std::min<unsigned long long>(nsurv, 148ull * 4);
-      timed(ctx, "dist_leaf_tau", [&] {
-        launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, head, k, 0, cand, cand_cap, ctx->d_stats, st);
-      });
-      JSI_CUDA(cudaMemsetAsync(&ctx->d_stats->work, 0, sizeof(unsigned long long), st));
+    {
+      // Tighten tau before any candidate is collected, so that the collecting
+      // pass appends few pairs: exact per-tile-pair k-th (k <= 8) over the
+      // tile pairs with the smallest bounds (all of them when few survive).
+      const unsigned long long head = leaf_lb ? std::min<unsigned long long>(nsurv, 148ull * 4) : nsurv;
+      if (k <= 8) {
+        timed(ctx, "dist_head", [&] { launch_dist_head(A, B, map1, map2, leaf_surv, head, k, ctx->d_stats, st); });
+      } else {
+        timed(ctx, "dist_head", [&] {
+          launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, head, k, 0, cand, cand_cap, ctx->d_stats, st);
+        });
+        JSI_CUDA(cudaMemsetAsync(&ctx->d_stats->work, 0, sizeof(unsigned long long), st));
+      }
     }
     for (int attempt = 0;; ++attempt) {
       timed(ctx, "dist_leaf", [&] {

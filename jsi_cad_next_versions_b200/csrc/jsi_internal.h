@@ -143,6 +143,11 @@ void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *m
                       const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
                       int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats,
                       cudaStream_t st);
+// Exact k-th d2 (k <= 8) of each of the first nhead tile pairs, folded into tau.
+template <typename T>
+void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats,
+                      cudaStream_t st);
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
                         ScreenStats *stats, cudaStream_t st);

@@ -773,6 +773,76 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
   if (k > 32) fold_tau(tau_bits_up(best), k, &stats->tau_bits, sh);
 }
 
+// Threshold pass over the first nhead tile pairs (the ones with the smallest
+// bounds when surv is sorted): one warp per tile pair, each lane keeps the KL
+// smallest d2 of its own pairs in a sorted register list, and the warp merges
+// the 32 lists to the exact k-th smallest d2 of the tile pair (k <= KL), which
+// is a valid upper bound of the global k-th and is folded into tau.
+template <typename T, int KL>
+__global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> b, const int *map1,
+                                                   const int *map2, const unsigned long long *surv,
+                                                   unsigned long long nhead, int k, ScreenStats *stats) {
+  const Geom g1 = a.g, g2 = b.g;
+  const int te1 = g1.te, te2 = g2.te;
+  const int n1 = te1 * te1, n2 = te2 * te2;
+  const int lane = threadIdx.x & 31;
+  const Vec4<T> far4{pos_inf<T>(), pos_inf<T>(), pos_inf<T>(), T(0)};
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  for (unsigned long long w = (blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x) >> 5;
+       w < nhead; w += nwarps) {
+    const unsigned long long q = surv[w];
+    const int row = static_cast<int>(q >> 32), t2 = static_cast<int>(q & 0xffffffffull);
+    const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+    const long long base1 = (static_cast<long long>(map1[slot]) * g1.ntiles + t1) * n1;
+    const long long base2 = (static_cast<long long>(map2[slot]) * g2.ntiles + t2) * n2;
+    const int ty1 = t1 / g1.tw, tx1 = t1 - ty1 * g1.tw, ty2 = t2 / g2.tw, tx2 = t2 - ty2 * g2.tw;
+    const int nv1 = min(te1, g1.W - ty1 * te1), nu1 = min(te1, g1.W - tx1 * te1);
+    const int nv2 = min(te2, g2.W - ty2 * te2), nu2 = min(te2, g2.W - tx2 * te2);
+    const int ja = lane, jb = lane + 32;
+    const int ja_v = ja / te2, ja_u = ja - ja_v * te2, jb_v = jb / te2, jb_u = jb - jb_v * te2;
+    const bool va = ja < n2 && ja_v < nv2 && ja_u < nu2;
+    const bool vb = jb < n2 && jb_v < nv2 && jb_u < nu2;
+    const Vec4<T> c2a = va ? b.center[base2 + ja] : far4;
+    const Vec4<T> c2b = vb ? b.center[base2 + jb] : far4;
+    const Vec4<T> c1a = ja < n1 ? a.center[base1 + ja] : far4;
+    const Vec4<T> c1b = jb < n1 ? a.center[base1 + jb] : far4;
+    T L[KL];
+#pragma unroll
+    for (int q2 = 0; q2 < KL; ++q2) L[q2] = pos_inf<T>();
+    for (int a1 = 0; a1 < nv1; ++a1) {
+      for (int b1 = 0; b1 < nu1; ++b1) {
+        const int l1 = a1 * te1 + b1;
+        const Vec4<T> c1 = shfl_vec(l1 < 32 ? c1a : c1b, l1 & 31);
+        const T d[2] = {center_d2(c1, c2a), center_d2(c1, c2b)};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const T x = d[h];
+          if (x < L[KL - 1]) {
+#pragma unroll
+            for (int q2 = KL - 1; q2 >= 1; --q2) L[q2] = (x < L[q2 - 1]) ? L[q2 - 1] : ((x < L[q2]) ? x : L[q2]);
+            L[0] = (x < L[0]) ? x : L[0];
+          }
+        }
+      }
+    }
+    // k rounds of warp minimum over the list heads; the owner pops its head.
+    T kth = pos_inf<T>();
+    for (int r = 0; r < k; ++r) {
+      T m = L[0];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = tmin(m, __shfl_xor_sync(kFull, m, o));
+      const unsigned owner = __ballot_sync(kFull, L[0] == m);
+      if (lane == __ffs(owner) - 1) {
+#pragma unroll
+        for (int q2 = 0; q2 < KL - 1; ++q2) L[q2] = L[q2 + 1];
+        L[KL - 1] = pos_inf<T>();
+      }
+      kth = m;
+    }
+    if (lane == 0 && kth != pos_inf<T>()) atomicMin(&stats->tau_bits, tau_bits_up(kth));
+  }
+}
+
 // Total order of the top-k (distance_analysis.cu:226-231).
 template <typename T>
 __device__ __forceinline__ bool cand_less(const DistCand<T> &x, const DistCand<T> &y) {
@@ -1237,6 +1307,16 @@ void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *m
 }
 
 template <typename T>
+void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats,
+                      cudaStream_t st) {
+  counted();
+  if (nhead == 0) return;
+  const int blocks = static_cast<int>((nhead + 7) / 8);
+  k_dist_head<T, 8><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats);
+}
+
+template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
                         ScreenStats *stats, cudaStream_t st) {
   counted();
@@ -1317,6 +1397,9 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
   template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
                                     const unsigned long long *, const unsigned *, unsigned long long, int, int,   \
                                     DistCand<T> *, unsigned long long, ScreenStats *, cudaStream_t);              \
+  template void launch_dist_head<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
+                                    const unsigned long long *, unsigned long long, int, ScreenStats *,           \
+                                    cudaStream_t);                                                                \
   template void launch_dist_select<T>(const DistCand<T> *, unsigned long long, int, DistCand<T> *, ScreenStats *, \
                                       cudaStream_t);                                                              \
   template void launch_dist_next<T>(const DistCand<T> *, ScreenStats *, const SideRound<T> &,                     \
