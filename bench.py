@@ -41,7 +41,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "queries/s + p50/p99 latency: FP32-screen vs plain FP64 on B200 at ≤1e-9 rel err"
 WORKLOAD = "hard-wave 64x64 bicubic pair, minimum distance, nuv0=512 + 3 rounds nuv=16, k=8"
 NUV0, NUV_REFINE, K, ROUNDS = 512, 16, 8, 4
-FORMS = ("fp64", "v5_fp32")  # headline form first
+FORMS = ("fp32_screen", "fp64", "v5_fp32")  # headline form first
 
 # Algorithmic work of the screening kernels, per unit (FMA = 2 flops):
 #  dist_leaf: one cell-pair centre distance = 3 sub + 3 mul + 2 add = 8 flops,
@@ -238,11 +238,15 @@ def run_ours(args):
               ctx.task(b, np.array(B.rect(), np.float32), args.nuv0, 2)) for (a, b), (A, B) in zip(ids, pairs)]
     ref_values = {}
     for form in forms:
+        step_distances = []
+
         def step():
             lats = []
+            step_distances.clear()
             for ta, tb in tasks:
                 r = ctx.min_distance(ta, tb, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
                 lats.append(r.device_ms)
+                step_distances.append(r.distance)
             return lats, r
         for _ in range(args.warmup):
             step()
@@ -271,6 +275,7 @@ def run_ours(args):
             "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99), "clocks": clk.summary(),
             "gpu_launches": launches, "kernels": ktimes, "last": last}
         ref_values[form] = last.v5_value if form == "v5_fp32" else last.distance
+        results[form]["distances"] = step_distances
 
     # ---------------- end to end through the C ABI, host buffers -----------
     form = forms[0]
@@ -314,6 +319,11 @@ def run_ours(args):
         return
 
     head = results[forms[0]]
+    rel_err = None
+    if "fp64" in results and forms[0] != "fp64":
+        a = np.array(head["distances"], np.float64)
+        b = np.array(results["fp64"]["distances"], np.float64)
+        rel_err = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
     # ---------------- roofline of the dominant kernel ----------------------
     kt = head["kernels"]
     dom = max(kt.items(), key=lambda kv: kv[1][0])[0] if kt else None
@@ -343,12 +353,14 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": head["value"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if forms[0] == "fp64" else "f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": {"fp64": "f64", "v5_fp32": "f32", "fp32_screen": "f32+f64"}[forms[0]], "data": "synthetic",
         "config": {"workload": WORKLOAD, "form": forms[0], "queries_per_step_per_gpu": args.batch,
                    "nuv0": args.nuv0, "l2": "flushed (256 MiB write) between steps", "parallelism": f"dp{world}"},
         "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"]},
         "forms": {f: {"queries_per_s": r["value"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
                       "result": ref_values[f]} for f, r in results.items()},
+        "rel_err_vs_fp64": rel_err,
+        "speedup_vs_fp64": (head["value"] / results["fp64"]["value"]) if "fp64" in results else None,
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": head["clocks"],
         "gpu_launches": head["gpu_launches"],
         "screen": {"pair_tests_per_round": [int(x) for x in last.pair_tests],

@@ -20,6 +20,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -121,6 +122,9 @@ class Arena {
 struct SurfaceRec {
   int ivec[7];
   int zero, rat, du, dv;
+  double cmax[3] = {0, 0, 0};   // max |control point coordinate|
+  double wcmax[3] = {0, 0, 0};  // max |w * control point coordinate| (rational)
+  double wmin = 1, wmax = 1;    // weight range (rational)
   float *U32 = nullptr, *V32 = nullptr;
   double *U64 = nullptr, *V64 = nullptr;
   Vec4<float> *cpw32 = nullptr;
@@ -254,10 +258,17 @@ SurfaceRec upload_surface(jsi_context *ctx, const int ivec[7], const float *data
   std::vector<Vec4<float>> c32(ncp);
   std::vector<Vec4<double>> c64(ncp);
   std::vector<double> u64(data, data + nku), v64(data + nku, data + nku + nkv);
+  if (s.rat && ncp > 0) s.wmin = s.wmax = cp[3 * ncp];
   for (size_t q = 0; q < ncp; ++q) {
     const float w = s.rat ? cp[3 * ncp + q] : 1.0f;
     c32[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
     c64[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
+    for (int c = 0; c < 3; ++c) {
+      s.cmax[c] = std::max(s.cmax[c], std::fabs(static_cast<double>(cp[3 * q + c])));
+      s.wcmax[c] = std::max(s.wcmax[c], std::fabs(static_cast<double>(w) * cp[3 * q + c]));
+    }
+    s.wmin = std::min(s.wmin, static_cast<double>(w));
+    s.wmax = std::max(s.wmax, static_cast<double>(w));
   }
   s.bytes = nku * 12 + nkv * 12 + ncp * (sizeof(Vec4<float>) + sizeof(Vec4<double>));
   auto dalloc = [&](size_t bytes) -> void * {
@@ -409,104 +420,208 @@ constexpr unsigned long long kMaxTilePairs = 1ull << 27;
 // ---------------------------------------------------------------------------
 // minimum_distance
 // ---------------------------------------------------------------------------
-template <typename T>
+
+// Per-coordinate bound of |c32 - c64| for the cell centres of one surface in
+// the FP32-screen form.  The FP64 form contracts the FP64 basis N64 with the
+// control net in FP64; the screen rounds the same N64 to FP32 and contracts
+// with FMAs.  With gamma_n = n u / (1 - n u) and n = degu + degv + 6 roundings
+// along either chain, both results lie within gamma_n * sum|Nv||Nu||CP| of the
+// exact sum; the B-spline basis is non-negative and sums to 1, so that sum is
+// at most max|CP| per coordinate.  Rational surfaces: the same bound for the
+// homogeneous sums (w CP, w), then the FP64 division.  Centres add one FP32
+// and one FP64 rounding of (lo + hi) / 2.  Margins (x1.01) cover the basis
+// sums deviating from 1 by FP64 rounding.
+void centre_error(const SurfaceRec &s, double ec[3]) {
+  const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+  const double n = s.ivec[1] + s.ivec[4] + 6;
+  const double g = n * u32 / (1 - n * u32) + n * u64 / (1 - n * u64);
+  for (int c = 0; c < 3; ++c) {
+    double ep;
+    if (!s.rat) {
+      ep = g * s.cmax[c] * 1.01;
+    } else {
+      const double ehx = g * s.wcmax[c] * 1.01, ehw = g * s.wmax * 1.01;
+      ep = (ehx + s.cmax[c] * ehw) / (s.wmin - ehw) + 4 * u64 * s.cmax[c] + u32 * s.cmax[c];
+    }
+    ec[c] = (ep + (u32 + u64) * (s.cmax[c] + ep)) * 1.01;
+  }
+}
+
+float screen_error(const SurfaceRec &a, const SurfaceRec &b) {
+  if (a.rat && !(a.wmin > 0)) fail(JSI_ERR_UNSUPPORTED, "FP32 screen needs positive weights");
+  if (b.rat && !(b.wmin > 0)) fail(JSI_ERR_UNSUPPORTED, "FP32 screen needs positive weights");
+  double ea[3], eb[3];
+  centre_error(a, ea);
+  centre_error(b, eb);
+  double ss = 0;
+  for (int c = 0; c < 3; ++c) ss += (ea[c] + eb[c]) * (ea[c] + eb[c]);
+  const double e = std::sqrt(ss) * (1 + 1e-6);
+  return std::nextafter(static_cast<float>(e), INFINITY);
+}
+
+// One screening round of the distance query: exact k smallest cell pairs
+// under (d2, slot, i, j) into top; returns how many were kept.  TC is the
+// precision of the cells; TS that of the selection (TC, or double for the
+// FP32 screen, whose candidates are re-checked in FP64 by `verify`).
+template <typename TC, typename TS, typename Verify>
+int dist_screen_round(jsi_context *ctx, const SideRound<TC> &A, const SideRound<TC> &B, const int *map1,
+                      const int *map2, int nslots, int k, bool screen, float e, DistCand<TS> *top, Verify &&verify,
+                      long long *tests, long long *cands) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
+  if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+  unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+  unsigned *surv_lb = ar.get<unsigned>(tile_pairs);
+  unsigned long long cand_cap = 1ull << 20;
+  DistCand<TC> *cand = ar.get<DistCand<TC>>(cand_cap);
+  reset_stats(ctx);
+  timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); });
+  timed(ctx, "dist_cull", [&] {
+    launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, screen, e, st);
+  });
+  pull_stats(ctx);
+  const unsigned long long nsurv = ctx->h_stats->survivors;
+  // Leaf order: ascending lower bound, so that the first tile pairs tighten
+  // tau and the rest stop early (exactness does not depend on the order).
+  const unsigned long long *leaf_surv = surv;
+  const unsigned *leaf_lb = nullptr;
+  if (nsurv > 2048) {
+    unsigned long long *surv_alt = ar.get<unsigned long long>(nsurv);
+    unsigned *lb_alt = ar.get<unsigned>(nsurv);
+    cub::DoubleBuffer<unsigned> kb(surv_lb, lb_alt);
+    cub::DoubleBuffer<unsigned long long> vb(surv, surv_alt);
+    size_t tmp_bytes = 0;
+    JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, static_cast<int>(nsurv), 0, 32, st));
+    void *tmp = ar.alloc(tmp_bytes);
+    timed(ctx, "sort_tiles", [&] {
+      JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kb, vb, static_cast<int>(nsurv), 0, 32, st));
+    });
+    leaf_surv = vb.Current();
+    leaf_lb = kb.Current();
+  }
+  {
+    // Tighten tau before any candidate is collected, so that the collecting
+    // pass appends few pairs: exact per-tile-pair k-th (k <= 8) over the tile
+    // pairs with the smallest bounds (all of them when few survive).
+    const unsigned long long head = leaf_lb ? std::min<unsigned long long>(nsurv, 148ull * 4) : nsurv;
+    if (k <= 8) {
+      timed(ctx, "dist_head", [&] {
+        launch_dist_head(A, B, map1, map2, leaf_surv, head, k, ctx->d_stats, screen, e, st);
+      });
+    } else {
+      timed(ctx, "dist_head", [&] {
+        launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, head, k, 0, cand, cand_cap, ctx->d_stats, screen, e,
+                         st);
+      });
+      JSI_CUDA(cudaMemsetAsync(&ctx->d_stats->work, 0, sizeof(unsigned long long), st));
+    }
+  }
+  for (int attempt = 0;; ++attempt) {
+    timed(ctx, "dist_leaf", [&] {
+      launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, nsurv, k, 1, cand, cand_cap, ctx->d_stats, screen, e,
+                       st);
+    });
+    bool fits = true;
+    if constexpr (std::is_same<TC, TS>::value) {
+      timed(ctx, "dist_select", [&] { launch_dist_select(cand, cand_cap, k, top, ctx->d_stats, st); });
+    } else {
+      pull_stats(ctx);
+      const unsigned long long m = ctx->h_stats->candidates;
+      fits = m <= cand_cap;
+      if (fits) {
+        DistCand<TS> *checked = ar.get<DistCand<TS>>(std::max<unsigned long long>(m, 1));
+        timed(ctx, "dist_verify", [&] { verify(cand, static_cast<long long>(m), checked); });
+        timed(ctx, "dist_select", [&] { launch_dist_select(checked, m, k, top, ctx->d_stats, st); });
+      }
+    }
+    pull_stats(ctx);
+    ScreenStats &hs = *ctx->h_stats;
+    if (fits && hs.candidates <= cand_cap && hs.status == 0) break;
+    if (attempt >= 4) fail(JSI_ERR_CAPACITY, "distance candidates did not fit after %d passes", attempt + 1);
+    // The leaf pass tightened tau: rerun it with the tighter bound.
+    if (hs.candidates > cand_cap) {
+      cand_cap = std::min<unsigned long long>(hs.candidates, 1ull << 26);
+      cand = ar.get<DistCand<TC>>(cand_cap);
+    }
+    hs.candidates = 0;
+    hs.pair_tests = 0;
+    hs.status = 0;
+    hs.work = 0;
+    JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+  }
+  *tests = static_cast<long long>(ctx->h_stats->pair_tests);
+  *cands = static_cast<long long>(ctx->h_stats->candidates);
+  return ctx->h_stats->nsel;
+}
+
+struct NoVerify {
+  template <typename A, typename B>
+  void operator()(const A *, long long, B *) const {}
+};
+
+// The round loop (distance_analysis.cu:375-492).  TP = precision of the
+// parameter rectangles, basis tables and selection; TC = precision of the
+// samples and cells.  Exact forms: TP = TC.  FP32 screen: TP = double,
+// TC = float, candidates re-checked in FP64.
+template <typename TP, typename TC>
 void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_dist_params *p,
                   jsi_dist_result *out) {
+  constexpr bool kScreen = !std::is_same<TP, TC>::value;
   Arena &ar = ctx->arena;
   cudaStream_t st = ctx->stream;
   const SurfaceRec &sa = get_surface(ctx, ta->surface);
   const SurfaceRec &sb = get_surface(ctx, tb->surface);
-  const SurfView<T> va = view<T>(sa), vb = view<T>(sb);
+  const SurfView<TP> pa = view<TP>(sa), pb = view<TP>(sb);
+  const SurfView<TC> ca = view<TC>(sa), cb = view<TC>(sb);
+  const float e = kScreen ? screen_error(sa, sb) : 0.0f;
   const int k = p->k;
-  RegionRec<T> roots[2] = {{T(ta->ustart), T(ta->vstart), T(ta->ustop), T(ta->vstop)},
-                           {T(tb->ustart), T(tb->vstart), T(tb->ustop), T(tb->vstop)}};
-  RegionRec<T> *dreg = ar.get<RegionRec<T>>(2);
+  RegionRec<TP> roots[2] = {{TP(ta->ustart), TP(ta->vstart), TP(ta->ustop), TP(ta->vstop)},
+                            {TP(tb->ustart), TP(tb->vstart), TP(tb->ustop), TP(tb->vstop)}};
+  RegionRec<TP> *dreg = ar.get<RegionRec<TP>>(2);
   int *dmap = ar.get<int>(2);
   const int zeros[2] = {0, 0};
   JSI_CUDA(copy_async(ctx, dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
   JSI_CUDA(copy_async(ctx, dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
-  SideRound<T> A = make_side<T>(ar, make_geom(ta->nuv, p1_of(sa)), 1, false, dreg);
-  SideRound<T> B = make_side<T>(ar, make_geom(tb->nuv, p1_of(sb)), 1, false, dreg + 1);
+  SideRound<TP> A = make_side<TP>(ar, make_geom(ta->nuv, p1_of(sa)), 1, false, dreg);
+  SideRound<TP> B = make_side<TP>(ar, make_geom(tb->nuv, p1_of(sb)), 1, false, dreg + 1);
   const int *map1 = dmap, *map2 = dmap + 1;
   int nslots = 1;
-  DistCand<T> *top = ar.get<DistCand<T>>(kMaxK);
-  std::vector<DistCand<T>> htop(kMaxK);
-  int round = 0;
-  for (round = 1; round <= p->rounds; ++round) {
-    build_side(ctx, va, A, false, false, T(1), T(1));
-    build_side(ctx, vb, B, false, false, T(1), T(1));
-    const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
-    if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
-    unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
-    unsigned *surv_lb = ar.get<unsigned>(tile_pairs);
-    unsigned long long cand_cap = 1ull << 20;
-    DistCand<T> *cand = ar.get<DistCand<T>>(cand_cap);
-    reset_stats(ctx);
-    timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, st); });
-    timed(ctx, "dist_cull", [&] {
-      launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, st);
-    });
-    pull_stats(ctx);
-    const unsigned long long nsurv = ctx->h_stats->survivors;
-    // Leaf order: ascending lower bound, so that the first tile pairs tighten
-    // tau and the rest stop early (exactness does not depend on the order).
-    const unsigned long long *leaf_surv = surv;
-    const unsigned *leaf_lb = nullptr;
-    if (nsurv > 2048) {
-      unsigned long long *surv_alt = ar.get<unsigned long long>(nsurv);
-      unsigned *lb_alt = ar.get<unsigned>(nsurv);
-      cub::DoubleBuffer<unsigned> kb(surv_lb, lb_alt);
-      cub::DoubleBuffer<unsigned long long> vb(surv, surv_alt);
-      size_t tmp_bytes = 0;
-      JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, static_cast<int>(nsurv), 0, 32, st));
-      void *tmp = ar.alloc(tmp_bytes);
-      timed(ctx, "sort_tiles", [&] {
-        JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kb, vb, static_cast<int>(nsurv), 0, 32, st));
-      });
-      leaf_surv = vb.Current();
-      leaf_lb = kb.Current();
-    }
-    {
-      // Tighten tau before any candidate is collected, so that the collecting
-      // pass appends few pairs: exact per-tile-pair k-th (k <= 8) over the
-      // tile pairs with the smallest bounds (all of them when few survive).
-      const unsigned long long head = leaf_lb ? std::min<unsigned long long>(nsurv, 148ull * 4) : nsurv;
-      if (k <= 8) {
-        timed(ctx, "dist_head", [&] { launch_dist_head(A, B, map1, map2, leaf_surv, head, k, ctx->d_stats, st); });
-      } else {
-        timed(ctx, "dist_head", [&] {
-          launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, head, k, 0, cand, cand_cap, ctx->d_stats, st);
-        });
-        JSI_CUDA(cudaMemsetAsync(&ctx->d_stats->work, 0, sizeof(unsigned long long), st));
+  DistCand<TP> *top = ar.get<DistCand<TP>>(kMaxK);
+  std::vector<DistCand<TP>> htop(kMaxK);
+  for (int round = 1; round <= p->rounds; ++round) {
+    long long tests = 0, cands = 0;
+    int n = 0;
+    if constexpr (!kScreen) {
+      build_side(ctx, pa, A, false, false, TP(1), TP(1));
+      build_side(ctx, pb, B, false, false, TP(1), TP(1));
+      n = dist_screen_round<TP, TP>(ctx, A, B, map1, map2, nslots, k, false, 0.0f, top, NoVerify{}, &tests, &cands);
+    } else {
+      // FP64 rectangles and basis tables, FP32 samples / cells / tiles.
+      SideRound<TC> A32{}, B32{};
+      for (int side = 0; side < 2; ++side) {
+        SideRound<TP> &P = side ? B : A;
+        SideRound<TC> &C = side ? B32 : A32;
+        C.g = P.g;
+        C.nreg = P.nreg;
+        C.samples = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.nuv * P.g.nuv);
+        C.center = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.cpr);
+        C.tlo = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
+        C.thi = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
+        timed(ctx, "basis", [&] { launch_basis(side ? pb : pa, P, st); });
+        timed(ctx, "samples", [&] { launch_samples_screen(side ? cb : ca, P, C, st); });
+        timed(ctx, "cells", [&] { launch_cells(C, false, st); });
       }
+      auto verify = [&](const DistCand<TC> *c, long long m, DistCand<TP> *o) {
+        launch_dist_verify(pa, pb, A, B, map1, map2, c, m, o, st);
+      };
+      n = dist_screen_round<TC, TP>(ctx, A32, B32, map1, map2, nslots, k, true, e, top, verify, &tests, &cands);
     }
-    for (int attempt = 0;; ++attempt) {
-      timed(ctx, "dist_leaf", [&] {
-        launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, nsurv, k, 1, cand, cand_cap, ctx->d_stats, st);
-      });
-      timed(ctx, "dist_select", [&] { launch_dist_select(cand, cand_cap, k, top, ctx->d_stats, st); });
-      pull_stats(ctx);
-      ScreenStats &hs = *ctx->h_stats;
-      if (hs.candidates <= cand_cap && hs.status == 0) break;
-      if (attempt >= 4) fail(JSI_ERR_CAPACITY, "distance candidates did not fit after %d passes", attempt + 1);
-      // The leaf pass tightened tau: rerun it with the tighter bound.
-      if (hs.candidates > cand_cap) {
-        cand_cap = std::min<unsigned long long>(hs.candidates, 1ull << 26);
-        cand = ar.get<DistCand<T>>(cand_cap);
-      }
-      hs.candidates = 0;
-      hs.pair_tests = 0;
-      hs.status = 0;
-      hs.work = 0;
-      JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
-    }
-    const ScreenStats hs = *ctx->h_stats;
-    const int n = hs.nsel;
     out->npairs[round - 1] = n;
-    out->pair_tests[round - 1] = static_cast<long long>(hs.pair_tests);
-    out->candidates[round - 1] = static_cast<long long>(hs.candidates);
+    out->pair_tests[round - 1] = tests;
+    out->candidates[round - 1] = cands;
     if (n > 0) {
-      JSI_CUDA(copy_async(ctx, htop.data(), top, sizeof(DistCand<T>) * n, cudaMemcpyDeviceToHost, st));
+      JSI_CUDA(copy_async(ctx, htop.data(), top, sizeof(DistCand<TP>) * n, cudaMemcpyDeviceToHost, st));
       JSI_CUDA(cudaStreamSynchronize(st));
       out->kth_d2[round - 1] = static_cast<double>(htop[n - 1].d2);
       if (out->trace_pairs && static_cast<long long>(round) * k <= out->trace_cap) {
@@ -522,20 +637,22 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
     }
     out->rounds_run = round;
     if (n == 0 || round == p->rounds) {
-      const T kth = n > 0 ? htop[n - 1].d2 : T(0);
-      const T root = std::sqrt(kth);
+      const TP kth = n > 0 ? htop[n - 1].d2 : TP(0);
+      const TP root = std::sqrt(kth);
       out->v5_value = static_cast<float>(root);
       out->distance = static_cast<double>(root);
       break;
     }
     // Next round (nuv = next_nuv after round 1, distance_analysis.cu:389).
-    RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
+    RegionRec<TP> *next1 = ar.get<RegionRec<TP>>(n), *next2 = ar.get<RegionRec<TP>>(n);
     int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
-    timed(ctx, "dist_next", [&] { launch_dist_next(top, ctx->d_stats, A, B, map1, map2, p->nuv_refine, next1, next2, nmap1, nmap2, st); });
+    timed(ctx, "dist_next", [&] {
+      launch_dist_next(top, ctx->d_stats, A, B, map1, map2, p->nuv_refine, next1, next2, nmap1, nmap2, st);
+    });
     pull_stats(ctx);
     const int r1 = ctx->h_stats->nreg1, r2 = ctx->h_stats->nreg2;
-    A = make_side<T>(ar, make_geom(p->nuv_refine, p1_of(sa)), r1, false, next1);
-    B = make_side<T>(ar, make_geom(p->nuv_refine, p1_of(sb)), r2, false, next2);
+    A = make_side<TP>(ar, make_geom(p->nuv_refine, p1_of(sa)), r1, false, next1);
+    B = make_side<TP>(ar, make_geom(p->nuv_refine, p1_of(sb)), r2, false, next2);
     map1 = nmap1;
     map2 = nmap2;
     nslots = n;
@@ -695,10 +812,10 @@ void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, 
   out->trace_written = written;
 }
 
-void check_precision(int prec) {
+void check_precision(int prec, bool screen_built) {
   if (prec != JSI_PREC_V5_FP32 && prec != JSI_PREC_FP64 && prec != JSI_PREC_FP32_SCREEN)
     fail(JSI_ERR_INVALID, "unknown precision %d", prec);
-  if (prec == JSI_PREC_FP32_SCREEN) fail(JSI_ERR_UNSUPPORTED, "FP32-screen form not built yet");
+  if (prec == JSI_PREC_FP32_SCREEN && !screen_built) fail(JSI_ERR_UNSUPPORTED, "FP32-screen form not built for this query");
 }
 
 }  // namespace
@@ -893,7 +1010,7 @@ int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, con
     if (p.k < 1 || p.k > kMaxK) fail(JSI_ERR_INVALID, "k = %d outside [1, %d]", p.k, kMaxK);
     if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
     if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
-    check_precision(p.precision);
+    check_precision(p.precision, true);
     if (p.newton) fail(JSI_ERR_UNSUPPORTED, "Newton refinement not built yet");
     check_task<float>(a);
     check_task<float>(b);
@@ -907,9 +1024,11 @@ int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, con
     ctx->arena.reset();
     JSI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     if (p.precision == JSI_PREC_V5_FP32)
-      run_distance<float>(ctx, a, b, &p, out);
+      run_distance<float, float>(ctx, a, b, &p, out);
+    else if (p.precision == JSI_PREC_FP64)
+      run_distance<double, double>(ctx, a, b, &p, out);
     else
-      run_distance<double>(ctx, a, b, &p, out);
+      run_distance<double, float>(ctx, a, b, &p, out);
     JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     JSI_CUDA(cudaEventSynchronize(ctx->ev1));
     JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
@@ -929,7 +1048,7 @@ int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const 
     if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
     if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
     if (p.min_nuv < 2) fail(JSI_ERR_INVALID, "min_nuv = %d", p.min_nuv);
-    check_precision(p.precision);
+    check_precision(p.precision, false);
     check_task<float>(a);
     check_task<float>(b);
     int *tp = out->trace_pairs;

@@ -129,25 +129,32 @@ void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st);
 template <typename T>
 void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st);
 
+// screen = true (float only): FP32-screen thresholds with centre-error bound e.
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                     int k, ScreenStats *stats, cudaStream_t st);
+                     int k, ScreenStats *stats, bool screen, float e, cudaStream_t st);
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                       unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
-                      cudaStream_t st);
+                      bool screen, float e, cudaStream_t st);
 // surv_lb may be null (no early exit); when given, surv must be sorted by it.
 // collect = 0: only tighten tau (no candidates); 1: append pairs with d2 <= tau.
 template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                       const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
-                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats,
-                      cudaStream_t st);
+                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, bool screen,
+                      float e, cudaStream_t st);
 // Exact k-th d2 (k <= 8) of each of the first nhead tile pairs, folded into tau.
 template <typename T>
 void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats,
-                      cudaStream_t st);
+                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats, bool screen,
+                      float e, cudaStream_t st);
+// FP32-screen form: FP32 samples from FP64 basis tables; FP64 re-check.
+void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
+                           cudaStream_t st);
+void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
+                        const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,
+                        long long n, DistCand<double> *out, cudaStream_t st);
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
                         ScreenStats *stats, cudaStream_t st);

@@ -18,6 +18,7 @@
 #include <cfloat>
 #include <climits>
 #include <cstdint>
+#include <type_traits>
 
 #include "jsi_internal.h"
 
@@ -609,6 +610,60 @@ __device__ __forceinline__ int tile_rep(int t, const Geom &g) {
 __device__ __forceinline__ unsigned lb_bits_down(float x) { return __float_as_uint(x); }
 __device__ __forceinline__ unsigned lb_bits_down(double x) { return __float_as_uint(__double2float_rd(x)); }
 
+// ---- FP32-screen thresholds ----------------------------------------------
+// In the FP32-screen form every cell centre c32 differs from the FP64 form's
+// c64 by at most a per-coordinate bound; e bounds the Euclidean norm of the
+// summed bounds of both sides (computed on the host, rounded up).  With
+// D = exact distance of two centres and 5u the relative error of a computed
+// squared distance in either precision (2^-20 covers both):
+//   d2_64 <= tau64  =>  d2_32 <= screen_widen(tau64, e)
+//   d2_32 <= v      =>  d2_64 <= screen_ub(v, e)
+// All operations round upward.
+__device__ __forceinline__ float screen_widen(float tau64, float e) {
+  if (!(tau64 < __uint_as_float(0x7f800000u))) return tau64;
+  float sq = __fsqrt_ru(__fmul_ru(tau64, 1.0f + 0x1p-20f));
+  sq = __fadd_ru(sq, e);
+  return __fmul_ru(__fmul_ru(sq, sq), 1.0f + 0x1p-20f);
+}
+__device__ __forceinline__ unsigned screen_ub_bits(float v32, float e) {
+  if (!(v32 < __uint_as_float(0x7f800000u))) return 0x7f800000u;
+  float sq = __fsqrt_ru(__fmul_ru(v32, 1.0f + 0x1p-20f));
+  sq = __fadd_ru(sq, e);
+  return __float_as_uint(__fmul_ru(__fmul_ru(sq, sq), 1.0f + 0x1p-20f));
+}
+
+// Squared distance of two centres: the reference's operation order (exact
+// forms), or FMA-contracted for the FP32 screen (error covered above).
+template <typename T, bool S>
+__device__ __forceinline__ T pair_d2(const Vec4<T> &a, const Vec4<T> &b) {
+  if constexpr (S) {
+    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+  } else {
+    return center_d2(a, b);
+  }
+}
+
+// Threshold value (in the FP64 domain for the screen) of a pair distance.
+template <typename T, bool S>
+__device__ __forceinline__ unsigned thr_bits(T d2, float e) {
+  if constexpr (S) {
+    return screen_ub_bits(d2, e);
+  } else {
+    return tau_bits_up(d2);
+  }
+}
+
+// Compare value (in the FP32 domain for the screen) of the shared threshold.
+template <typename T, bool S>
+__device__ __forceinline__ T thr_compare(unsigned tau_bits, float e) {
+  if constexpr (S) {
+    return screen_widen(__uint_as_float(tau_bits), e);
+  } else {
+    return tau_value<T>(tau_bits);
+  }
+}
+
 // Ascending bitonic sort of one value per lane; returns the value of lane q.
 __device__ __forceinline__ unsigned warp_sorted_at(unsigned v, int q) {
   const int lane = threadIdx.x & 31;
@@ -628,9 +683,9 @@ __device__ __forceinline__ unsigned warp_sorted_at(unsigned v, int q) {
 // Threshold seed: the representative cell pair (middle cells) of every tile
 // pair.  Rows (slot, t1) are spread over blocks, t2 over threads; each block
 // folds the k-th smallest of its per-thread minima into tau.
-template <typename T>
+template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b, const int *map1,
-                                                  const int *map2, int nslots, int k, ScreenStats *stats) {
+                                                  const int *map2, int nslots, int k, ScreenStats *stats, float e) {
   __shared__ unsigned sh[256];
   const Geom g1 = a.g, g2 = b.g;
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
@@ -642,7 +697,7 @@ __global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b
     const long long base2 = static_cast<long long>(map2[slot]) * g2.ntiles;
     for (int t2 = threadIdx.x; t2 < g2.ntiles; t2 += blockDim.x) {
       const Vec4<T> c2 = b.center[(base2 + t2) * n2 + tile_rep(t2, g2)];
-      best = fminf(best, __uint_as_float(tau_bits_up(center_d2(c1, c2))));
+      best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
     }
   }
   fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
@@ -650,13 +705,13 @@ __global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b
 
 // Tile pairs whose box-gap bound does not exceed tau survive, with the bound
 // (float, rounded down) as the key the leaf is ordered by.
-template <typename T>
+template <typename T, bool S>
 __global__ void k_dist_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
                             unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap,
-                            ScreenStats *stats) {
+                            ScreenStats *stats, float e) {
   const Geom g1 = a.g, g2 = b.g;
   const int nrows = nslots * g1.ntiles;
-  const T tau = tau_value<T>(stats->tau_bits);
+  const T tau = thr_compare<T, S>(stats->tau_bits, e);
   for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
     const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
     const long long i1 = static_cast<long long>(map1[slot]) * g1.ntiles + t1;
@@ -668,6 +723,9 @@ __global__ void k_dist_cull(SideRound<T> a, SideRound<T> b, const int *map1, con
       T lb = T(0);
       if (t2 < g2.ntiles) {
         lb = tile_lb(lo1, hi1, b.tlo[base2 + t2], b.thi[base2 + t2]);
+        // The screen's pair distances are FMA-contracted: shave the rounded
+        // bound by 2^-19 (more than the 12u they can differ by).
+        if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
         keep = lb <= tau;
       }
       const long long pos = warp_append(keep, &stats->survivors);
@@ -698,11 +756,11 @@ __device__ __forceinline__ Vec4<T> shfl_vec(const Vec4<T> &v, int src) {
   return r;
 }
 
-template <typename T>
+template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
                                                    const unsigned long long *surv, const unsigned *surv_lb,
                                                    unsigned long long nsurv, int k, int collect, DistCand<T> *cand,
-                                                   unsigned long long cand_cap, ScreenStats *stats) {
+                                                   unsigned long long cand_cap, ScreenStats *stats, float e) {
   __shared__ unsigned sh[256];
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
@@ -717,8 +775,8 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
     w = __shfl_sync(kFull, w, 0);
     if (w >= nsurv) break;
     const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
-    if (surv_lb && __uint_as_float(surv_lb[w]) > __uint_as_float(taub)) break;
-    const T tau = tau_value<T>(taub);
+    const T tau = thr_compare<T, S>(taub, e);
+    if (surv_lb && __uint_as_float(surv_lb[w]) > static_cast<float>(thr_compare<float, S>(taub, e))) break;
     const unsigned long long q = surv[w];
     const int row = static_cast<int>(q >> 32), t2 = static_cast<int>(q & 0xffffffffull);
     const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
@@ -742,8 +800,8 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
       for (int b1 = 0; b1 < nu1; ++b1) {
         const int l1 = a1 * te1 + b1;
         const Vec4<T> c1 = shfl_vec(l1 < 32 ? c1a : c1b, l1 & 31);
-        const T da = center_d2(c1, c2a);
-        const T db = center_d2(c1, c2b);
+        const T da = pair_d2<T, S>(c1, c2a);
+        const T db = pair_d2<T, S>(c1, c2b);
         best = tmin(best, tmin(da, db));
         if (collect) {
           // tau is +inf until k pairs are known: padding lanes (d2 = +inf) must not pass.
@@ -762,7 +820,7 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
     }
     if (lane == 0) tests += static_cast<unsigned long long>(nv1 * nu1) * (nv2 * nu2);
     if (k <= 32) {
-      const unsigned mine = tau_bits_up(best);
+      const unsigned mine = thr_bits<T, S>(best, e);
       if (__popc(__ballot_sync(kFull, mine < taub)) >= k) {
         const unsigned kth = warp_sorted_at(mine, k - 1);
         if (lane == 0) atomicMin(&stats->tau_bits, kth);
@@ -770,7 +828,7 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
     }
   }
   if (collect && lane == 0) atomicAdd(&stats->pair_tests, tests);
-  if (k > 32) fold_tau(tau_bits_up(best), k, &stats->tau_bits, sh);
+  if (k > 32) fold_tau(thr_bits<T, S>(best, e), k, &stats->tau_bits, sh);
 }
 
 // Threshold pass over the first nhead tile pairs (the ones with the smallest
@@ -778,10 +836,10 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
 // smallest d2 of its own pairs in a sorted register list, and the warp merges
 // the 32 lists to the exact k-th smallest d2 of the tile pair (k <= KL), which
 // is a valid upper bound of the global k-th and is folded into tau.
-template <typename T, int KL>
+template <typename T, int KL, bool S>
 __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> b, const int *map1,
                                                    const int *map2, const unsigned long long *surv,
-                                                   unsigned long long nhead, int k, ScreenStats *stats) {
+                                                   unsigned long long nhead, int k, ScreenStats *stats, float e) {
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
   const int n1 = te1 * te1, n2 = te2 * te2;
@@ -813,7 +871,7 @@ __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> 
       for (int b1 = 0; b1 < nu1; ++b1) {
         const int l1 = a1 * te1 + b1;
         const Vec4<T> c1 = shfl_vec(l1 < 32 ? c1a : c1b, l1 & 31);
-        const T d[2] = {center_d2(c1, c2a), center_d2(c1, c2b)};
+        const T d[2] = {pair_d2<T, S>(c1, c2a), pair_d2<T, S>(c1, c2b)};
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const T x = d[h];
@@ -839,7 +897,7 @@ __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> 
       }
       kth = m;
     }
-    if (lane == 0 && kth != pos_inf<T>()) atomicMin(&stats->tau_bits, tau_bits_up(kth));
+    if (lane == 0 && kth != pos_inf<T>()) atomicMin(&stats->tau_bits, thr_bits<T, S>(kth, e));
   }
 }
 
@@ -1215,6 +1273,109 @@ __global__ void k_inter_side2(const unsigned long long *key2s, const int *idxs, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP32-screen form: FP32 positions from FP64 basis tables, FP64 re-check
+// ---------------------------------------------------------------------------
+
+// P of every sample in FP32: the FP64 basis values (the same tables the FP64
+// form uses) are rounded to FP32 and contracted with FMAs against the FP32
+// control net; rational surfaces divide by the weight in FP64.  The host
+// bounds |P32 - P64| per coordinate from the operation count.
+__global__ void k_samples_screen(SurfView<float> s, SideRound<double> basis_side, SideRound<float> out) {
+  const Geom g = basis_side.g;
+  const int nuv = g.nuv;
+  const long long per = static_cast<long long>(nuv) * nuv;
+  const long long total = per * basis_side.nreg;
+  const int p1 = g.p1max;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(t / per);
+    const int q = static_cast<int>(t - static_cast<long long>(r) * per);
+    const int idx = q % nuv, idy = q / nuv;
+    const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
+    const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
+    const double *Nu = basis_side.basis + lu * 3 * p1;
+    const double *Nv = basis_side.basis + lv * 3 * p1;
+    Vec4<float> P{0.0f, 0.0f, 0.0f, 0.0f};
+    if (!s.zero) {
+      const int cu0 = basis_side.spans[lu] - s.degu, cv0 = basis_side.spans[lv] - s.degv;
+      float ax = 0.0f, ay = 0.0f, az = 0.0f, aw = 0.0f;
+      for (int rr = 0; rr <= s.degv; ++rr) {
+        const Vec4<float> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + rr) + cu0;
+        float rx = 0.0f, ry = 0.0f, rz = 0.0f, rw = 0.0f;
+        for (int c = 0; c <= s.degu; ++c) {
+          const Vec4<float> v = cp[c];
+          float n = __double2float_rn(Nu[c]);
+          if (s.rat) {
+            n = __fmul_rn(n, v.w);
+            rw = __fadd_rn(rw, n);
+          }
+          rx = __fmaf_rn(n, v.x, rx);
+          ry = __fmaf_rn(n, v.y, ry);
+          rz = __fmaf_rn(n, v.z, rz);
+        }
+        const float m = __double2float_rn(Nv[rr]);
+        ax = __fmaf_rn(m, rx, ax);
+        ay = __fmaf_rn(m, ry, ay);
+        az = __fmaf_rn(m, rz, az);
+        aw = __fmaf_rn(m, rw, aw);
+      }
+      if (s.rat) {
+        const double w = static_cast<double>(aw);
+        P.x = __double2float_rn(static_cast<double>(ax) / w);
+        P.y = __double2float_rn(static_cast<double>(ay) / w);
+        P.z = __double2float_rn(static_cast<double>(az) / w);
+      } else {
+        P.x = ax;
+        P.y = ay;
+        P.z = az;
+      }
+    }
+    out.samples[t] = P;
+  }
+}
+
+// FP64 centre of one cell exactly as the FP64 form builds it: P at the four
+// corners from the FP64 basis tables (eval_point), min/max, (lo - 0 + hi + 0)/2.
+__device__ Vec4<double> cell_center64(const SurfView<double> &s, const SideRound<double> &sr, int region, int cell) {
+  const Geom g = sr.g;
+  const int iv = cell / g.W, iu = cell - (cell / g.W) * g.W;
+  const int p1 = g.p1max;
+  double P[4][3];
+#pragma unroll
+  for (int cnr = 0; cnr < 4; ++cnr) {
+    const int idx = iu + (cnr & 1), idy = iv + (cnr >> 1);
+    const long long lu = (static_cast<long long>(region) * 2 + 0) * g.nuv + idx;
+    const long long lv = (static_cast<long long>(region) * 2 + 1) * g.nuv + idy;
+    eval_point(s, sr.spans[lu], sr.basis + lu * 3 * p1, sr.spans[lv], sr.basis + lv * 3 * p1, P[cnr]);
+  }
+  Vec4<double> c;
+  double lo[3], hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = tmin(P[0][d], tmin(P[1][d], tmin(P[2][d], P[3][d])));
+    hi[d] = tmax(P[0][d], tmax(P[1][d], tmax(P[2][d], P[3][d])));
+  }
+  c.x = (lo[0] - 0.0 + hi[0] + 0.0) / 2.0;
+  c.y = (lo[1] - 0.0 + hi[1] + 0.0) / 2.0;
+  c.z = (lo[2] - 0.0 + hi[2] + 0.0) / 2.0;
+  c.w = 0.0;
+  return c;
+}
+
+// Re-check of the screened candidates in FP64: the FP64 form's d2 of each.
+__global__ void k_dist_verify(SurfView<double> sa, SurfView<double> sb, SideRound<double> a, SideRound<double> b,
+                              const int *map1, const int *map2, const DistCand<float> *cand, long long n,
+                              DistCand<double> *out) {
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const DistCand<float> c = cand[e];
+    const Vec4<double> c1 = cell_center64(sa, a, map1[c.slot], c.i);
+    const Vec4<double> c2 = cell_center64(sb, b, map2[c.slot], c.j);
+    out[e] = DistCand<double>{center_d2(c1, c2), c.slot, c.i, c.j};
+  }
+}
+
 inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -1276,44 +1437,70 @@ void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, 
 
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                     int k, ScreenStats *stats, cudaStream_t st) {
+                     int k, ScreenStats *stats, bool screen, float e, cudaStream_t st) {
   counted();
   const int rows = nslots * a.g.ntiles;
-  k_dist_tau<T><<<rows < 148 * 8 ? rows : 148 * 8, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats);
+  const int grid = rows < 148 * 8 ? rows : 148 * 8;
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_tau<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+      return;
+    }
+  }
+  k_dist_tau<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
 }
 
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                       unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
-                      cudaStream_t st) {
+                      bool screen, float e, cudaStream_t st) {
   counted();
   const int rows = nslots * a.g.ntiles;
   const int block = b.g.ntiles >= 256 ? 256 : (b.g.ntiles >= 128 ? 128 : 64);
-  k_dist_cull<T><<<rows < 148 * 16 ? rows : 148 * 16, block, 0, st>>>(a, b, map1, map2, nslots, surv, surv_lb,
-                                                                        surv_cap, stats);
+  const int grid = rows < 148 * 16 ? rows : 148 * 16;
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_cull<float, true><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, surv_lb, surv_cap, stats, e);
+      return;
+    }
+  }
+  k_dist_cull<T, false><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, surv_lb, surv_cap, stats, e);
 }
 
 template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                       const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
-                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats,
-                      cudaStream_t st) {
+                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, bool screen,
+                      float e, cudaStream_t st) {
   counted();
   if (nsurv == 0) return;
   const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
   const int blocks = static_cast<int>((warps + 7) / 8);
-  k_dist_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, collect, cand, cand_cap,
-                                          stats);
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_leaf<float, true><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, collect, cand,
+                                                       cand_cap, stats, e);
+      return;
+    }
+  }
+  k_dist_leaf<T, false><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, collect, cand, cand_cap,
+                                                stats, e);
 }
 
 template <typename T>
 void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats,
-                      cudaStream_t st) {
+                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats, bool screen,
+                      float e, cudaStream_t st) {
   counted();
   if (nhead == 0) return;
   const int blocks = static_cast<int>((nhead + 7) / 8);
-  k_dist_head<T, 8><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats);
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_head<float, 8, true><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats, e);
+      return;
+    }
+  }
+  k_dist_head<T, 8, false><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats, e);
 }
 
 template <typename T>
@@ -1383,6 +1570,21 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
   k_inter_side2<T><<<grid_for(n, 256), 256, 0, st>>>(key2s, idxs, n, ij_bits, flag2, ex2, cur, map2, next, nmap2);
 }
 
+void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
+                           cudaStream_t st) {
+  counted();
+  const long long n = static_cast<long long>(basis_side.nreg) * basis_side.g.nuv * basis_side.g.nuv;
+  k_samples_screen<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, basis_side, out);
+}
+
+void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
+                        const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,
+                        long long n, DistCand<double> *out, cudaStream_t st) {
+  counted();
+  if (n <= 0) return;
+  k_dist_verify<<<grid_for(n, 128), 128, 0, st>>>(sa, sb, a, b, map1, map2, cand, n, out);
+}
+
 #define JSI_INSTANTIATE(T)                                                                                        \
   template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t);                         \
   template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t);                 \
@@ -1390,16 +1592,17 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
   template void launch_cells<T>(const SideRound<T> &, bool, cudaStream_t);                                        \
   template void launch_records<T>(const SurfView<T> &, T, T, T, T, int, T *, cudaStream_t);                       \
   template void launch_dist_tau<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, int, \
-                                   ScreenStats *, cudaStream_t);                                                  \
+                                   ScreenStats *, bool, float, cudaStream_t);                                     \
   template void launch_dist_cull<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,    \
-                                    unsigned long long *, unsigned *, unsigned long long, ScreenStats *,          \
-                                    cudaStream_t);                                                                \
+                                    unsigned long long *, unsigned *, unsigned long long, ScreenStats *, bool,    \
+                                    float, cudaStream_t);                                                         \
   template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
                                     const unsigned long long *, const unsigned *, unsigned long long, int, int,   \
-                                    DistCand<T> *, unsigned long long, ScreenStats *, cudaStream_t);              \
-  template void launch_dist_head<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
-                                    const unsigned long long *, unsigned long long, int, ScreenStats *,           \
+                                    DistCand<T> *, unsigned long long, ScreenStats *, bool, float,               \
                                     cudaStream_t);                                                                \
+  template void launch_dist_head<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
+                                    const unsigned long long *, unsigned long long, int, ScreenStats *, bool,     \
+                                    float, cudaStream_t);                                                         \
   template void launch_dist_select<T>(const DistCand<T> *, unsigned long long, int, DistCand<T> *, ScreenStats *, \
                                       cudaStream_t);                                                              \
   template void launch_dist_next<T>(const DistCand<T> *, ScreenStats *, const SideRound<T> &,                     \

@@ -243,3 +243,54 @@ def test_intersection_degree11_reference_inputs(gpu_ctx, ref, orc, case):
     for r in range(res.rounds):
         if o["pairs"][r] is not None:
             assert np.array_equal(res.pairs[r], o["pairs"][r])
+
+
+# ---------------------------------------------------------------------------
+# FP32-screen form: FP32 evaluation and screening with rigorous bounds, FP64
+# re-check; its candidate lists and k-th distances must equal the FP64 form's.
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("key", ["sine/n64/k8", "sine/n64/k64", "sine/n32/k8", "hardwave/n64/k8",
+                                 "hardwave/n128/k8"])
+def test_distance_screen_equals_fp64(gpu_ctx, orc, key):
+    name, n, k = key.split("/")
+    nuv0, k = int(n[1:]), int(k[1:])
+    A, B, _ = synth.distance_pair_sine() if name == "sine" else synth.distance_pair_hard_wave()
+    scr = _dist_both(gpu_ctx, orc, A, B, nuv0, k, precision="fp32_screen")
+    ref = _dist_both(gpu_ctx, orc, A, B, nuv0, k, precision="fp64")
+    assert np.array_equal(scr.kth_d2.view(np.uint64), ref.kth_d2.view(np.uint64))
+    for r in range(4):
+        assert np.array_equal(scr.pairs[r], ref.pairs[r]), f"round {r + 1}"
+        # the FP32 screen passed a superset of the kept pairs
+        assert scr.candidates[r] >= scr.npairs[r]
+    assert scr.distance == ref.distance
+
+
+@pytest.mark.parametrize("seed", [31, 32, 33, 34, 35, 36])
+def test_distance_screen_random_pairs(gpu_ctx, orc, seed):
+    """Mixed degrees, 30% rational, nuv0 per side, k in {1, 5, 8, 33}."""
+    rng = synth.SplitMix64(seed)
+    A = synth.random_surface(rng)
+    B = synth.random_surface(rng)
+    nuv0 = 20 + 3 * seed % 40
+    k = [1, 5, 8, 33][seed % 4]
+    scr = _dist_both(gpu_ctx, orc, A, B, nuv0, k, precision="fp32_screen")
+    o = orc.dist_query(A, B, rect32(A).astype(np.float64), rect32(B).astype(np.float64), nuv0, 16, k, 4,
+                       dtype=np.float64)
+    assert np.array_equal(scr.kth_d2, o["kth_d2"])
+    for r in range(len(o["pairs"])):
+        assert np.array_equal(scr.pairs[r], o["pairs"][r])
+
+
+def test_distance_screen_full_size(gpu_ctx):
+    """Full-size hard-wave pair (nuv0 = 512): screen form == FP64 form."""
+    A, B, _ = synth.distance_pair_hard_wave()
+    sa, sb = gpu_ctx.upload(A), gpu_ctx.upload(B)
+    ta, tb = _task(gpu_ctx, sa, rect32(A), 512, 1), _task(gpu_ctx, sb, rect32(B), 512, 2)
+    scr = gpu_ctx.min_distance(ta, tb, precision="fp32_screen", trace=True)
+    ref = gpu_ctx.min_distance(ta, tb, precision="fp64", trace=True)
+    gpu_ctx.release(sa)
+    gpu_ctx.release(sb)
+    assert np.array_equal(scr.kth_d2, ref.kth_d2)
+    for r in range(4):
+        assert np.array_equal(scr.pairs[r], ref.pairs[r])
