@@ -592,7 +592,11 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
   for (int round = 1; round <= p->rounds; ++round) {
     long long tests = 0, cands = 0;
     int n = 0;
-    if constexpr (!kScreen) {
+    // The FP32 screen pays where the screen is large: the first round's
+    // (nuv0-1)^4 pairs over cells much wider than the FP32 error bound.
+    // Refinement rounds shrink cells to ~1e-6 of the coordinates, below FP32
+    // resolution, so they run in FP64 (same results either way).
+    if (!kScreen || round > 1) {
       build_side(ctx, pa, A, false, false, TP(1), TP(1));
       build_side(ctx, pb, B, false, false, TP(1), TP(1));
       n = dist_screen_round<TP, TP>(ctx, A, B, map1, map2, nslots, k, false, 0.0f, top, NoVerify{}, &tests, &cands);
