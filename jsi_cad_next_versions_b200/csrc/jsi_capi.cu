@@ -600,7 +600,7 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
       build_side(ctx, pa, A, false, false, TP(1), TP(1));
       build_side(ctx, pb, B, false, false, TP(1), TP(1));
       n = dist_screen_round<TP, TP>(ctx, A, B, map1, map2, nslots, k, false, 0.0f, top, NoVerify{}, &tests, &cands);
-    } else {
+    } else if constexpr (kScreen) {
       // FP64 rectangles and basis tables, FP32 samples / cells / tiles.
       SideRound<TC> A32{}, B32{};
       for (int side = 0; side < 2; ++side) {
