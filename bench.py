@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--nuv0", type=int, default=NUV0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default=",".join(FORMS))
+    ap.add_argument("--lanes", type=int, default=8, help="worker lanes (concurrent queries on the device)")
     return ap.parse_args()
 
 
@@ -214,6 +215,7 @@ def run_ours(args):
     import jsi_cad_next_versions_b200 as J
 
     ctx = J.Context(local)
+    ctx.workers(args.lanes)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     pairs = make_pairs(args.batch, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -241,13 +243,10 @@ def run_ours(args):
         step_distances = []
 
         def step():
-            lats = []
             step_distances.clear()
-            for ta, tb in tasks:
-                r = ctx.min_distance(ta, tb, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
-                lats.append(r.device_ms)
-                step_distances.append(r.distance)
-            return lats, r
+            res, _ = ctx.min_distance_batch(tasks, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
+            step_distances.extend(r.distance for r in res)
+            return [r.device_ms for r in res], res[-1]
         for _ in range(args.warmup):
             step()
         ctx.kernel_timing(True)
@@ -285,11 +284,11 @@ def run_ours(args):
         ctx.release(b)
 
     def e2e_step():
-        for A, B in pairs:
-            sa, sb = ctx.upload(A), ctx.upload(B)
-            ctx.min_distance(ctx.task(sa, np.array(A.rect(), np.float32), args.nuv0, 1),
-                             ctx.task(sb, np.array(B.rect(), np.float32), args.nuv0, 2), k=K, rounds=ROUNDS,
-                             nuv_refine=NUV_REFINE, precision=form)
+        ids2 = [(ctx.upload(A), ctx.upload(B)) for A, B in pairs]
+        tl = [(ctx.task(sa, np.array(A.rect(), np.float32), args.nuv0, 1),
+               ctx.task(sb, np.array(B.rect(), np.float32), args.nuv0, 2)) for (sa, sb), (A, B) in zip(ids2, pairs)]
+        ctx.min_distance_batch(tl, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
+        for sa, sb in ids2:
             ctx.release(sa)
             ctx.release(sb)
     for _ in range(args.warmup):
@@ -355,6 +354,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"fp64": "f64", "v5_fp32": "f32", "fp32_screen": "f32+f64"}[forms[0]], "data": "synthetic",
         "config": {"workload": WORKLOAD, "form": forms[0], "queries_per_step_per_gpu": args.batch,
+                   "lanes": args.lanes,
                    "nuv0": args.nuv0, "l2": "flushed (256 MiB write) between steps", "parallelism": f"dp{world}"},
         "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"]},
         "forms": {f: {"queries_per_s": r["value"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],

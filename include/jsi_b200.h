@@ -168,6 +168,33 @@ void jsi_inter_params_default(jsi_inter_params *p);
 int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_inter_params *params,
                   jsi_inter_result *out);
 
+/* --- queued and batched queries (the serving engine) ----------------------
+ * No counterpart in the reference, whose API runs one query at a time and is
+ * not re-entrant (file statics, intersection.cu:36-39).  jsi_workers starts n
+ * worker lanes (each: a CUDA stream, a device arena of up to lane_bytes, a
+ * host thread); queued queries run on the first free lane in arrival order
+ * and their kernels overlap on the device.  n = 0 stops the pool (only when
+ * nothing is queued).  A surface cannot be released while a queued query
+ * uses it.  Results of a query are bit-identical whichever lane runs it and
+ * whatever runs beside it. */
+typedef long long jsi_ticket;
+int jsi_workers(jsi_context *ctx, int n, unsigned long long lane_bytes);
+/* trace_pairs (may be null) must stay valid until jsi_wait returns. */
+int jsi_submit_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
+                        int *trace_pairs, long long trace_cap, jsi_ticket *out);
+int jsi_submit_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_inter_params *params,
+                         int *trace_pairs, long long trace_cap, jsi_ticket *out);
+/* Waits up to timeout_ms (< 0: no limit) for a ticket; JSI_ERR_TIMEOUT if it
+ * is not done yet (the ticket stays valid), else the query's own status with
+ * its result copied to dist or inter. */
+int jsi_wait(jsi_context *ctx, jsi_ticket ticket, int timeout_ms, jsi_dist_result *dist, jsi_inter_result *inter);
+int jsi_queue_depth(jsi_context *ctx, int *queued, int *running);
+/* n distance queries over the worker lanes; status[q] (may be null) gets each
+ * query's status, device_ms (may be null) the device span of the batch
+ * (CUDA events).  Returns the first error, else JSI_OK. */
+int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
+                           const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms);
+
 /* --- grid evaluation -----------------------------------------------------
  * Replaces evalWithCuda(int*, float*, int, float, float, float, float, int,
  * float*) (include/jsi_cad.hpp:46, src/evaluation/evaluation.cu:391-405):

@@ -31,7 +31,8 @@ EXPORTED = [
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_names",
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
-    "jsi_eval_grid_noalloc",
+    "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
+    "jsi_queue_depth", "jsi_min_distance_batch",
 ]
 
 
@@ -130,6 +131,22 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_eval_grid_f64.argtypes = [P, P, P, I, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, I, P]
     L.jsi_eval_grid_f64.restype = I
+    LL = ctypes.c_longlong
+    L.jsi_workers.argtypes = [P, I, ctypes.c_ulonglong]
+    L.jsi_workers.restype = I
+    L.jsi_submit_distance.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),
+                                      ctypes.POINTER(ctypes.c_int), LL, ctypes.POINTER(LL)]
+    L.jsi_submit_distance.restype = I
+    L.jsi_submit_intersect.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(InterParams),
+                                       ctypes.POINTER(ctypes.c_int), LL, ctypes.POINTER(LL)]
+    L.jsi_submit_intersect.restype = I
+    L.jsi_wait.argtypes = [P, LL, I, ctypes.POINTER(DistResult), ctypes.POINTER(InterResult)]
+    L.jsi_wait.restype = I
+    L.jsi_queue_depth.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
+    L.jsi_queue_depth.restype = I
+    L.jsi_min_distance_batch.argtypes = [P, I, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),
+                                         ctypes.POINTER(DistResult), ctypes.POINTER(I), ctypes.POINTER(ctypes.c_float)]
+    L.jsi_min_distance_batch.restype = I
     L.jsi_eval_grid_noalloc.argtypes = [P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                         I, P]
     L.jsi_eval_grid_noalloc.restype = I

@@ -73,6 +73,7 @@ class Context:
             raise JsiError(st, "jsi_create failed")
         self.handle = h
         self._surfaces = {}
+        self._pending = {}
 
     def close(self):
         if getattr(self, "handle", None):
@@ -151,10 +152,28 @@ class Context:
     def task(sid: int, rect, nuv: int, side: int) -> C.Task:
         return C.Task(sid, float(rect[0]), float(rect[1]), float(rect[2]), float(rect[3]), int(nuv), int(side))
 
+    @staticmethod
+    def _dist_params(k, rounds, nuv_refine, precision, newton):
+        prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        return C.DistParams(nuv_refine, k, rounds, prec, 1 if newton else 0)
+
+    @staticmethod
+    def _dist_result(r: C.DistResult, buf, k: int) -> DistanceResult:
+        n = r.rounds_run
+        npairs = np.array(r.npairs[:n], dtype=np.int64)
+        pairs = []
+        if buf is not None:
+            for q in range(n):
+                pairs.append(buf[q * k * 3:(q * k + int(npairs[q])) * 3].reshape(-1, 3).copy())
+        return DistanceResult(
+            v5_value=float(np.float32(r.v5_value)), distance=r.distance, newton_distance=r.newton_distance,
+            uv1=tuple(r.uv1), uv2=tuple(r.uv2), point1=tuple(r.point1), point2=tuple(r.point2), rounds=n,
+            npairs=npairs, kth_d2=np.array(r.kth_d2[:n]), pair_tests=np.array(r.pair_tests[:n], dtype=np.int64),
+            candidates=np.array(r.candidates[:n], dtype=np.int64), device_ms=r.device_ms, pairs=pairs)
+
     def min_distance(self, a: C.Task, b: C.Task, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
                      precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False) -> DistanceResult:
-        prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
-        p = C.DistParams(nuv_refine, k, rounds, prec, 1 if newton else 0)
+        p = self._dist_params(k, rounds, nuv_refine, precision, newton)
         r = C.DistResult()
         buf = None
         if trace:
@@ -163,17 +182,79 @@ class Context:
             r.trace_cap = rounds * k
         self._check(self.lib.jsi_min_distance(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
                                               ctypes.byref(r)))
-        n = r.rounds_run
-        npairs = np.array(r.npairs[:n], dtype=np.int64)
-        pairs = []
-        if trace:
-            for q in range(n):
-                pairs.append(buf[q * k * 3:(q * k + int(npairs[q])) * 3].reshape(-1, 3).copy())
-        return DistanceResult(
-            v5_value=float(np.float32(r.v5_value)), distance=r.distance, newton_distance=r.newton_distance,
-            uv1=tuple(r.uv1), uv2=tuple(r.uv2), point1=tuple(r.point1), point2=tuple(r.point2), rounds=n,
-            npairs=npairs, kth_d2=np.array(r.kth_d2[:n]), pair_tests=np.array(r.pair_tests[:n], dtype=np.int64),
-            candidates=np.array(r.candidates[:n], dtype=np.int64), device_ms=r.device_ms, pairs=pairs)
+        return self._dist_result(r, buf, k)
+
+    # -- worker lanes: queued / batched queries ----------------------------
+    def workers(self, n: int, lane_bytes: int = 0):
+        """Start n worker lanes (stream + arena + host thread each); 0 stops them."""
+        self._check(self.lib.jsi_workers(self.handle, int(n), int(lane_bytes)))
+
+    def submit_distance(self, a: C.Task, b: C.Task, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
+                        precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False):
+        """Queue a distance query; returns a ticket for wait()."""
+        p = self._dist_params(k, rounds, nuv_refine, precision, newton)
+        buf = np.full(rounds * k * 3, -1, dtype=np.int32) if trace else None
+        t = ctypes.c_longlong(0)
+        ptr = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if trace else None
+        self._check(self.lib.jsi_submit_distance(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
+                                                 ptr, rounds * k if trace else 0, ctypes.byref(t)))
+        self._pending[t.value] = ("d", buf, k, None)
+        return t.value
+
+    def submit_intersect(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
+                         halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",
+                         trace: bool = False, trace_cap: int = 1 << 22):
+        prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec)
+        buf = np.full(trace_cap * 3, -1, dtype=np.int32) if trace else None
+        t = ctypes.c_longlong(0)
+        ptr = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if trace else None
+        self._check(self.lib.jsi_submit_intersect(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
+                                                  ptr, trace_cap if trace else 0, ctypes.byref(t)))
+        self._pending[t.value] = ("i", buf, trace_cap, None)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """Result of a queued query, or None if not done within timeout_ms."""
+        kind, buf, cap, _ = self._pending[ticket]
+        d, i = C.DistResult(), C.InterResult()
+        st = self.lib.jsi_wait(self.handle, ticket, int(timeout_ms), ctypes.byref(d), ctypes.byref(i))
+        if st == -6:
+            return None
+        del self._pending[ticket]
+        self._check(st)
+        if kind == "d":
+            return self._dist_result(d, buf, cap)
+        return self._inter_result(i, buf, cap)
+
+    def queue_depth(self):
+        q, r = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.jsi_queue_depth(self.handle, ctypes.byref(q), ctypes.byref(r)))
+        return q.value, r.value
+
+    def min_distance_batch(self, pairs, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
+                           precision: str | int = "v5_fp32", trace: bool = False):
+        """Distance queries [(task_a, task_b), ...] over the worker lanes.
+        Returns (results, device_ms of the whole batch)."""
+        n = len(pairs)
+        p = self._dist_params(k, rounds, nuv_refine, precision, False)
+        ta = (C.Task * n)(*[x[0] for x in pairs])
+        tb = (C.Task * n)(*[x[1] for x in pairs])
+        res = (C.DistResult * n)()
+        bufs = []
+        for q in range(n):
+            if trace:
+                buf = np.full(rounds * k * 3, -1, dtype=np.int32)
+                res[q].trace_pairs = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+                res[q].trace_cap = rounds * k
+                bufs.append(buf)
+            else:
+                bufs.append(None)
+        status = (ctypes.c_int * n)()
+        ms = ctypes.c_float(0)
+        self._check(self.lib.jsi_min_distance_batch(self.handle, n, ta, tb, ctypes.byref(p), res, status,
+                                                    ctypes.byref(ms)))
+        return [self._dist_result(res[q], bufs[q], k) for q in range(n)], ms.value
 
     def intersect(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                   halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",
@@ -188,10 +269,14 @@ class Context:
             r.trace_cap = trace_cap
         self._check(self.lib.jsi_intersect(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
                                            ctypes.byref(r)))
+        return self._inter_result(r, buf, trace_cap)
+
+    @staticmethod
+    def _inter_result(r: C.InterResult, buf, trace_cap: int) -> IntersectionResult:
         n = r.rounds_run
         counts = np.array(r.counts[:n], dtype=np.int64)
         pairs = []
-        if trace:
+        if buf is not None:
             off = 0
             for c in counts:
                 c = int(c)

@@ -15,11 +15,17 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -104,7 +110,6 @@ class Arena {
   U *get(size_t n) {
     return static_cast<U *>(alloc(n * sizeof(U)));
   }
-  size_t total() const { return total_; }
 
  private:
   struct Block {
@@ -134,27 +139,66 @@ struct SurfaceRec {
 
 }  // namespace
 
-struct jsi_context {
+namespace {
+
+// One execution lane: a CUDA stream with its own device arena, stats record,
+// transfer counters and optional kernel timing.  The context owns a main lane
+// for synchronous calls and worker lanes for queued and batched queries, whose
+// kernels overlap on the device.
+struct Lane {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   Arena arena;
-  std::mutex mu;
-  std::string last_error;
-  std::map<int, SurfaceRec> surfaces;
-  int next_id = 1;
-  size_t budget = size_t(120) << 30;
-  size_t resident = 0;
   ScreenStats *d_stats = nullptr;
   ScreenStats *h_stats = nullptr;
   unsigned long long h2d_bytes = 0, d2h_bytes = 0;
-  // Optional per-kernel timing: CUDA events recorded on the context stream
+  // Optional per-kernel timing: CUDA events recorded on the lane's stream
   // around every launch, resolved at the next host sync.
   bool timing = false;
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   std::map<std::string, std::pair<double, long long>> kernel_ms;
+  const std::map<int, SurfaceRec> *surfaces = nullptr;
+};
+
+// A queued query of the worker pool.
+struct Job {
+  int kind = 0;  // 0 distance, 1 intersection
+  jsi_task a{}, b{};
+  jsi_dist_params dp{};
+  jsi_inter_params ip{};
+  jsi_dist_result dres{};
+  jsi_inter_result ires{};
+  int status = JSI_OK;
+  std::string error;
+  bool done = false;
+};
+
+}  // namespace
+
+struct jsi_context {
+  int device = 0;
+  Lane main;
+  std::mutex mu;  // serialises the main lane and the surface table
+  std::string last_error;
+  std::map<int, SurfaceRec> surfaces;
+  std::map<int, int> surface_refs;  // queued / running jobs per surface
+  int next_id = 1;
+  size_t budget = size_t(120) << 30;
+  size_t lane_bytes = size_t(1) << 30;
+  size_t resident = 0;
   std::string kernel_names;
+  // worker pool
+  std::vector<std::unique_ptr<Lane>> lanes;
+  std::vector<std::thread> threads;
+  std::mutex qmu;
+  std::condition_variable qcv, dcv;
+  std::deque<std::shared_ptr<Job>> queue;
+  std::map<long long, std::shared_ptr<Job>> jobs;
+  long long next_ticket = 1;
+  int busy = 0;
+  bool stopping = false;
 };
 
 namespace {
@@ -181,7 +225,7 @@ int guarded(jsi_context *ctx, Fn &&fn) {
 }
 
 // cudaMemcpyAsync that also counts the bytes crossing PCIe / C2C.
-cudaError_t copy_async(jsi_context *ctx, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
+cudaError_t copy_async(Lane *ctx, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
                        cudaStream_t st) {
   if (kind == cudaMemcpyHostToDevice) ctx->h2d_bytes += bytes;
   if (kind == cudaMemcpyDeviceToHost) ctx->d2h_bytes += bytes;
@@ -243,7 +287,7 @@ void check_surface(const int ivec[7], const float *data, int ndata) {
   if (ndata < need) fail(JSI_ERR_SURFACE, "ndata %d < %lld required by the header", ndata, need);
 }
 
-SurfaceRec upload_surface(jsi_context *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
+SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
   check_surface(ivec, data, ndata);
   SurfaceRec s;
   std::memcpy(s.ivec, ivec, sizeof(s.ivec));
@@ -306,9 +350,9 @@ void free_surface(SurfaceRec &s) {
   cudaFree(s.cpw64);
 }
 
-const SurfaceRec &get_surface(jsi_context *ctx, jsi_surface_id id) {
-  auto it = ctx->surfaces.find(id);
-  if (it == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
+const SurfaceRec &get_surface(Lane *ctx, jsi_surface_id id) {
+  auto it = ctx->surfaces->find(id);
+  if (it == ctx->surfaces->end()) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
   return it->second;
 }
 
@@ -335,7 +379,7 @@ SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, Regio
 // Evaluation + cell + tile build of one side (run_evaluation_and_construction_task,
 // distance_analysis.cu:88-116 / intersection.cu:175-219).
 template <typename T>
-void build_side(jsi_context *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect, bool use_k, T span_u0,
+void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect, bool use_k, T span_u0,
                 T span_v0) {
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
@@ -347,7 +391,7 @@ void build_side(jsi_context *ctx, const SurfView<T> &v, SideRound<T> &s, bool in
   JSI_CUDA(cudaGetLastError());
 }
 
-cudaEvent_t take_event(jsi_context *ctx) {
+cudaEvent_t take_event(Lane *ctx) {
   if (!ctx->event_pool.empty()) {
     cudaEvent_t e = ctx->event_pool.back();
     ctx->event_pool.pop_back();
@@ -359,7 +403,7 @@ cudaEvent_t take_event(jsi_context *ctx) {
 }
 
 // Resolves recorded kernel timings; call after the stream has synchronised.
-void resolve_timing(jsi_context *ctx) {
+void resolve_timing(Lane *ctx) {
   for (auto &p : ctx->pending) {
     float ms = 0.0f;
     JSI_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
@@ -374,7 +418,7 @@ void resolve_timing(jsi_context *ctx) {
 
 // Runs one launcher, bracketed by events when timing is on.
 template <typename Fn>
-void timed(jsi_context *ctx, const char *name, Fn &&fn) {
+void timed(Lane *ctx, const char *name, Fn &&fn) {
   if (!ctx->timing) {
     fn();
     return;
@@ -386,14 +430,14 @@ void timed(jsi_context *ctx, const char *name, Fn &&fn) {
   ctx->pending.push_back({name, {a, b}});
 }
 
-void reset_stats(jsi_context *ctx) {
+void reset_stats(Lane *ctx) {
   ScreenStats z{};
   z.tau_bits = 0x7f800000u;
   *ctx->h_stats = z;
   JSI_CUDA(copy_async(ctx, ctx->d_stats, ctx->h_stats, sizeof(ScreenStats), cudaMemcpyHostToDevice, ctx->stream));
 }
 
-void pull_stats(jsi_context *ctx) {
+void pull_stats(Lane *ctx) {
   JSI_CUDA(copy_async(ctx, ctx->h_stats, ctx->d_stats, sizeof(ScreenStats), cudaMemcpyDeviceToHost, ctx->stream));
   JSI_CUDA(cudaStreamSynchronize(ctx->stream));
   JSI_CUDA(cudaGetLastError());
@@ -464,7 +508,7 @@ float screen_error(const SurfaceRec &a, const SurfaceRec &b) {
 // precision of the cells; TS that of the selection (TC, or double for the
 // FP32 screen, whose candidates are re-checked in FP64 by `verify`).
 template <typename TC, typename TS, typename Verify>
-int dist_screen_round(jsi_context *ctx, const SideRound<TC> &A, const SideRound<TC> &B, const int *map1,
+int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B, const int *map1,
                       const int *map2, int nslots, int k, bool screen, float e, DistCand<TS> *top, Verify &&verify,
                       long long *tests, long long *cands) {
   Arena &ar = ctx->arena;
@@ -565,7 +609,7 @@ struct NoVerify {
 // samples and cells.  Exact forms: TP = TC.  FP32 screen: TP = double,
 // TC = float, candidates re-checked in FP64.
 template <typename TP, typename TC>
-void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_dist_params *p,
+void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_dist_params *p,
                   jsi_dist_result *out) {
   constexpr bool kScreen = !std::is_same<TP, TC>::value;
   Arena &ar = ctx->arena;
@@ -667,7 +711,7 @@ void run_distance(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, cons
 // intersection
 // ---------------------------------------------------------------------------
 template <typename T>
-void run_intersection(jsi_context *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
+void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
                       jsi_inter_result *out) {
   Arena &ar = ctx->arena;
   cudaStream_t st = ctx->stream;
@@ -822,6 +866,198 @@ void check_precision(int prec, bool screen_built) {
   if (prec == JSI_PREC_FP32_SCREEN && !screen_built) fail(JSI_ERR_UNSUPPORTED, "FP32-screen form not built for this query");
 }
 
+// Lane set-up / tear-down.
+void lane_init(Lane &L, int device, size_t block, size_t budget, const std::map<int, SurfaceRec> *surfaces) {
+  L.device = device;
+  L.surfaces = surfaces;
+  L.arena.configure(block, budget);
+  JSI_CUDA(cudaSetDevice(device));
+  JSI_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+  JSI_CUDA(cudaEventCreate(&L.ev0));
+  JSI_CUDA(cudaEventCreate(&L.ev1));
+  JSI_CUDA(cudaMalloc(&L.d_stats, sizeof(ScreenStats)));
+  JSI_CUDA(cudaMallocHost(&L.h_stats, sizeof(ScreenStats)));
+}
+
+void lane_free(Lane &L) {
+  if (L.stream) cudaStreamSynchronize(L.stream);
+  for (auto &p : L.pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  L.pending.clear();
+  for (auto e : L.event_pool) cudaEventDestroy(e);
+  L.event_pool.clear();
+  if (L.d_stats) cudaFree(L.d_stats);
+  if (L.h_stats) cudaFreeHost(L.h_stats);
+  if (L.ev0) cudaEventDestroy(L.ev0);
+  if (L.ev1) cudaEventDestroy(L.ev1);
+  if (L.stream) cudaStreamDestroy(L.stream);
+  L.d_stats = nullptr;
+  L.h_stats = nullptr;
+  L.ev0 = L.ev1 = nullptr;
+  L.stream = nullptr;
+}
+
+void validate_dist(jsi_dist_params &p, const jsi_task *a, const jsi_task *b) {
+  if (p.k < 1 || p.k > kMaxK) fail(JSI_ERR_INVALID, "k = %d outside [1, %d]", p.k, kMaxK);
+  if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
+  if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
+  check_precision(p.precision, true);
+  if (p.newton) fail(JSI_ERR_UNSUPPORTED, "Newton refinement not built yet");
+  check_task<float>(a);
+  check_task<float>(b);
+}
+
+void validate_inter(jsi_inter_params &p, const jsi_task *a, const jsi_task *b) {
+  if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
+  if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
+  if (p.min_nuv < 2) fail(JSI_ERR_INVALID, "min_nuv = %d", p.min_nuv);
+  check_precision(p.precision, false);
+  check_task<float>(a);
+  check_task<float>(b);
+}
+
+// One distance query on one lane (arena rewound, device time in out->device_ms).
+void exec_distance(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_dist_params &p, jsi_dist_result *out) {
+  int *tp = out->trace_pairs;
+  const long long tc = out->trace_cap;
+  std::memset(out, 0, sizeof(*out));
+  out->trace_pairs = tp;
+  out->trace_cap = tc;
+  out->newton_distance = -1.0;
+  JSI_CUDA(cudaSetDevice(L->device));
+  L->arena.reset();
+  JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
+  if (p.precision == JSI_PREC_V5_FP32)
+    run_distance<float, float>(L, a, b, &p, out);
+  else if (p.precision == JSI_PREC_FP64)
+    run_distance<double, double>(L, a, b, &p, out);
+  else
+    run_distance<double, float>(L, a, b, &p, out);
+  JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
+  JSI_CUDA(cudaEventSynchronize(L->ev1));
+  JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
+  if (L->timing) resolve_timing(L);
+}
+
+void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_inter_params &p,
+                       jsi_inter_result *out) {
+  int *tp = out->trace_pairs;
+  const long long tc = out->trace_cap;
+  std::memset(out, 0, sizeof(*out));
+  out->trace_pairs = tp;
+  out->trace_cap = tc;
+  JSI_CUDA(cudaSetDevice(L->device));
+  L->arena.reset();
+  JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
+  if (p.precision == JSI_PREC_V5_FP32)
+    run_intersection<float>(L, a, b, &p, out);
+  else
+    run_intersection<double>(L, a, b, &p, out);
+  JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
+  JSI_CUDA(cudaEventSynchronize(L->ev1));
+  JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
+  if (L->timing) resolve_timing(L);
+}
+
+int run_guarded(std::string &err, const std::function<void()> &fn) {
+  try {
+    fn();
+    return JSI_OK;
+  } catch (const StatusError &e) {
+    err = e.msg;
+    return e.status;
+  } catch (const CudaError &e) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at line %d", static_cast<int>(e.err),
+             cudaGetErrorString(e.err), e.what, e.line);
+    err = buf;
+    return JSI_ERR_CUDA;
+  } catch (const std::bad_alloc &) {
+    err = "host allocation failed";
+    return JSI_ERR_NOMEM;
+  }
+}
+
+void release_refs(jsi_context *ctx, const Job &j) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (int id : {j.a.surface, j.b.surface}) {
+    auto it = ctx->surface_refs.find(id);
+    if (it != ctx->surface_refs.end() && --it->second <= 0) ctx->surface_refs.erase(it);
+  }
+}
+
+// Worker: takes queued queries in arrival order and runs them on its lane.
+void worker_loop(jsi_context *ctx, Lane *L) {
+  cudaSetDevice(L->device);
+  for (;;) {
+    std::shared_ptr<Job> job;
+    {
+      std::unique_lock<std::mutex> lk(ctx->qmu);
+      ctx->qcv.wait(lk, [&] { return ctx->stopping || !ctx->queue.empty(); });
+      if (ctx->queue.empty()) return;  // stopping and drained
+      job = ctx->queue.front();
+      ctx->queue.pop_front();
+      ++ctx->busy;
+    }
+    job->status = run_guarded(job->error, [&] {
+      if (job->kind == 0)
+        exec_distance(L, &job->a, &job->b, job->dp, &job->dres);
+      else
+        exec_intersection(L, &job->a, &job->b, job->ip, &job->ires);
+    });
+    release_refs(ctx, *job);
+    {
+      std::lock_guard<std::mutex> lk(ctx->qmu);
+      job->done = true;
+      --ctx->busy;
+    }
+    ctx->dcv.notify_all();
+  }
+}
+
+void stop_workers(jsi_context *ctx) {
+  {
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    ctx->stopping = true;
+  }
+  ctx->qcv.notify_all();
+  for (auto &t : ctx->threads) t.join();
+  ctx->threads.clear();
+  for (auto &L : ctx->lanes) lane_free(*L);
+  ctx->lanes.clear();
+  ctx->stopping = false;
+}
+
+void start_workers(jsi_context *ctx, int n) {
+  for (int q = 0; q < n; ++q) {
+    auto L = std::make_unique<Lane>();
+    lane_init(*L, ctx->device, std::min(ctx->lane_bytes, size_t(512) << 20), ctx->lane_bytes, &ctx->surfaces);
+    ctx->lanes.push_back(std::move(L));
+  }
+  for (auto &L : ctx->lanes) ctx->threads.emplace_back(worker_loop, ctx, L.get());
+}
+
+long long enqueue(jsi_context *ctx, std::shared_ptr<Job> job) {
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (int id : {job->a.surface, job->b.surface}) {
+      if (!ctx->surfaces.count(id)) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
+      ++ctx->surface_refs[id];
+    }
+  }
+  long long t;
+  {
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    t = ctx->next_ticket++;
+    ctx->jobs[t] = job;
+    ctx->queue.push_back(job);
+  }
+  ctx->qcv.notify_one();
+  return t;
+}
+
 }  // namespace
 
 extern "C" {
@@ -860,14 +1096,8 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
   ctx->device = dev;
   const size_t arena = (cfg && cfg->arena_bytes) ? cfg->arena_bytes : (size_t(2) << 30);
   ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (size_t(120) << 30);
-  ctx->arena.configure(arena, ctx->budget);
   const int st = guarded(ctx, [&]() {
-    JSI_CUDA(cudaSetDevice(dev));
-    JSI_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    JSI_CUDA(cudaEventCreate(&ctx->ev0));
-    JSI_CUDA(cudaEventCreate(&ctx->ev1));
-    JSI_CUDA(cudaMalloc(&ctx->d_stats, sizeof(ScreenStats)));
-    JSI_CUDA(cudaMallocHost(&ctx->h_stats, sizeof(ScreenStats)));
+    lane_init(ctx->main, dev, arena, ctx->budget, &ctx->surfaces);
     return JSI_OK;
   });
   if (st != JSI_OK) {
@@ -881,19 +1111,11 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
 int jsi_destroy(jsi_context *ctx) {
   if (!ctx) return JSI_ERR_INVALID;
   cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  stop_workers(ctx);
+  if (ctx->main.stream) cudaStreamSynchronize(ctx->main.stream);
   for (auto &kv : ctx->surfaces) free_surface(kv.second);
   ctx->surfaces.clear();
-  if (ctx->d_stats) cudaFree(ctx->d_stats);
-  if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
-  for (auto &p : ctx->pending) {
-    cudaEventDestroy(p.second.first);
-    cudaEventDestroy(p.second.second);
-  }
-  for (auto e : ctx->event_pool) cudaEventDestroy(e);
-  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  lane_free(ctx->main);
   delete ctx;
   return JSI_OK;
 }
@@ -904,8 +1126,8 @@ int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, i
   return guarded(ctx, [&]() {
     JSI_CUDA(cudaSetDevice(ctx->device));
     check_surface(ivec, data, ndata);
-    SurfaceRec s = upload_surface(ctx, ivec, data, ndata, nullptr);
-    if (ctx->resident + s.bytes + ctx->arena.total() > ctx->budget) {
+    SurfaceRec s = upload_surface(&ctx->main, ivec, data, ndata, nullptr);
+    if (ctx->resident + s.bytes > ctx->budget) {
       free_surface(s);
       fail(JSI_ERR_NOMEM, "HBM budget exhausted by resident surfaces");
     }
@@ -922,8 +1144,9 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   auto it = ctx->surfaces.find(id);
   if (it == ctx->surfaces.end()) return record(ctx, JSI_ERR_INVALID, "unknown surface id");
+  if (ctx->surface_refs.count(id)) return record(ctx, JSI_ERR_INVALID, "surface is used by a queued query");
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
+  cudaStreamSynchronize(ctx->main.stream);
   ctx->resident -= it->second.bytes;
   free_surface(it->second);
   ctx->surfaces.erase(it);
@@ -938,40 +1161,60 @@ int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out) {
 
 int jsi_context_stream(jsi_context *ctx, void **stream) {
   if (!ctx || !stream) return JSI_ERR_INVALID;
-  *stream = static_cast<void *>(ctx->stream);
+  *stream = static_cast<void *>(ctx->main.stream);
   return JSI_OK;
 }
 
 int jsi_transfer_bytes(const jsi_context *ctx, unsigned long long *h2d, unsigned long long *d2h) {
   if (!ctx || !h2d || !d2h) return JSI_ERR_INVALID;
-  *h2d = ctx->h2d_bytes;
-  *d2h = ctx->d2h_bytes;
+  *h2d = ctx->main.h2d_bytes;
+  *d2h = ctx->main.d2h_bytes;
+  for (auto &L : ctx->lanes) {
+    *h2d += L->h2d_bytes;
+    *d2h += L->d2h_bytes;
+  }
   return JSI_OK;
 }
 
 int jsi_kernel_timing(jsi_context *ctx, int enable) {
   if (!ctx) return JSI_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  ctx->timing = enable != 0;
-  ctx->kernel_ms.clear();
-  ctx->pending.clear();
+  auto set = [&](Lane &L) {
+    L.timing = enable != 0;
+    L.kernel_ms.clear();
+    L.pending.clear();
+  };
+  set(ctx->main);
+  for (auto &L : ctx->lanes) set(*L);
   return JSI_OK;
 }
 
 int jsi_kernel_time(jsi_context *ctx, const char *name, double *total_ms, long long *launches) {
   if (!ctx || !name || !total_ms || !launches) return JSI_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  auto it = ctx->kernel_ms.find(name);
-  *total_ms = it == ctx->kernel_ms.end() ? 0.0 : it->second.first;
-  *launches = it == ctx->kernel_ms.end() ? 0 : it->second.second;
+  *total_ms = 0.0;
+  *launches = 0;
+  auto add = [&](Lane &L) {
+    auto it = L.kernel_ms.find(name);
+    if (it != L.kernel_ms.end()) {
+      *total_ms += it->second.first;
+      *launches += it->second.second;
+    }
+  };
+  add(ctx->main);
+  for (auto &L : ctx->lanes) add(*L);
   return JSI_OK;
 }
 
 const char *jsi_kernel_names(jsi_context *ctx) {
   if (!ctx) return "";
   std::lock_guard<std::mutex> lk(ctx->mu);
+  std::map<std::string, int> names;
+  for (auto &kv : ctx->main.kernel_ms) names[kv.first] = 1;
+  for (auto &L : ctx->lanes)
+    for (auto &kv : L->kernel_ms) names[kv.first] = 1;
   ctx->kernel_names.clear();
-  for (auto &kv : ctx->kernel_ms) {
+  for (auto &kv : names) {
     if (!ctx->kernel_names.empty()) ctx->kernel_names += ",";
     ctx->kernel_names += kv.first;
   }
@@ -1011,32 +1254,8 @@ int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, con
     jsi_dist_params p;
     jsi_dist_params_default(&p);
     if (params) p = *params;
-    if (p.k < 1 || p.k > kMaxK) fail(JSI_ERR_INVALID, "k = %d outside [1, %d]", p.k, kMaxK);
-    if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
-    if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
-    check_precision(p.precision, true);
-    if (p.newton) fail(JSI_ERR_UNSUPPORTED, "Newton refinement not built yet");
-    check_task<float>(a);
-    check_task<float>(b);
-    int *tp = out->trace_pairs;
-    const long long tc = out->trace_cap;
-    std::memset(out, 0, sizeof(*out));
-    out->trace_pairs = tp;
-    out->trace_cap = tc;
-    out->newton_distance = -1.0;
-    JSI_CUDA(cudaSetDevice(ctx->device));
-    ctx->arena.reset();
-    JSI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (p.precision == JSI_PREC_V5_FP32)
-      run_distance<float, float>(ctx, a, b, &p, out);
-    else if (p.precision == JSI_PREC_FP64)
-      run_distance<double, double>(ctx, a, b, &p, out);
-    else
-      run_distance<double, float>(ctx, a, b, &p, out);
-    JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
-    JSI_CUDA(cudaEventSynchronize(ctx->ev1));
-    JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
-    if (ctx->timing) resolve_timing(ctx);
+    validate_dist(p, a, b);
+    exec_distance(&ctx->main, a, b, p, out);
     return JSI_OK;
   });
 }
@@ -1049,30 +1268,142 @@ int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const 
     jsi_inter_params p;
     jsi_inter_params_default(&p);
     if (params) p = *params;
-    if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
-    if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
-    if (p.min_nuv < 2) fail(JSI_ERR_INVALID, "min_nuv = %d", p.min_nuv);
-    check_precision(p.precision, false);
-    check_task<float>(a);
-    check_task<float>(b);
-    int *tp = out->trace_pairs;
-    const long long tc = out->trace_cap;
-    std::memset(out, 0, sizeof(*out));
-    out->trace_pairs = tp;
-    out->trace_cap = tc;
-    JSI_CUDA(cudaSetDevice(ctx->device));
-    ctx->arena.reset();
-    JSI_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (p.precision == JSI_PREC_V5_FP32)
-      run_intersection<float>(ctx, a, b, &p, out);
-    else
-      run_intersection<double>(ctx, a, b, &p, out);
-    JSI_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
-    JSI_CUDA(cudaEventSynchronize(ctx->ev1));
-    JSI_CUDA(cudaEventElapsedTime(&out->device_ms, ctx->ev0, ctx->ev1));
-    if (ctx->timing) resolve_timing(ctx);
+    validate_inter(p, a, b);
+    exec_intersection(&ctx->main, a, b, p, out);
     return JSI_OK;
   });
+}
+
+int jsi_workers(jsi_context *ctx, int n, unsigned long long lane_bytes) {
+  if (!ctx || n < 0 || n > 256) return JSI_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    if (!ctx->queue.empty() || ctx->busy) return record(ctx, JSI_ERR_INVALID, "queries are still queued");
+  }
+  stop_workers(ctx);
+  if (lane_bytes) ctx->lane_bytes = lane_bytes;
+  return guarded(ctx, [&]() {
+    start_workers(ctx, n);
+    return JSI_OK;
+  });
+}
+
+int jsi_submit_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
+                        int *trace_pairs, long long trace_cap, jsi_ticket *out) {
+  if (!ctx || !a || !b || !out) return JSI_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    if (ctx->lanes.empty()) fail(JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
+    auto job = std::make_shared<Job>();
+    job->kind = 0;
+    job->a = *a;
+    job->b = *b;
+    jsi_dist_params_default(&job->dp);
+    if (params) job->dp = *params;
+    validate_dist(job->dp, a, b);
+    job->dres.trace_pairs = trace_pairs;
+    job->dres.trace_cap = trace_cap;
+    *out = enqueue(ctx, job);
+    return JSI_OK;
+  });
+}
+
+int jsi_submit_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_inter_params *params,
+                         int *trace_pairs, long long trace_cap, jsi_ticket *out) {
+  if (!ctx || !a || !b || !out) return JSI_ERR_INVALID;
+  return guarded(ctx, [&]() {
+    if (ctx->lanes.empty()) fail(JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
+    auto job = std::make_shared<Job>();
+    job->kind = 1;
+    job->a = *a;
+    job->b = *b;
+    jsi_inter_params_default(&job->ip);
+    if (params) job->ip = *params;
+    validate_inter(job->ip, a, b);
+    job->ires.trace_pairs = trace_pairs;
+    job->ires.trace_cap = trace_cap;
+    *out = enqueue(ctx, job);
+    return JSI_OK;
+  });
+}
+
+int jsi_wait(jsi_context *ctx, jsi_ticket ticket, int timeout_ms, jsi_dist_result *dist, jsi_inter_result *inter) {
+  if (!ctx) return JSI_ERR_INVALID;
+  std::shared_ptr<Job> job;
+  {
+    std::unique_lock<std::mutex> lk(ctx->qmu);
+    auto it = ctx->jobs.find(ticket);
+    if (it == ctx->jobs.end()) return record(ctx, JSI_ERR_INVALID, "unknown ticket");
+    job = it->second;
+    auto ready = [&] { return job->done; };
+    if (timeout_ms < 0)
+      ctx->dcv.wait(lk, ready);
+    else if (!ctx->dcv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+      return JSI_ERR_TIMEOUT;
+    ctx->jobs.erase(ticket);
+  }
+  if (dist && job->kind == 0) *dist = job->dres;
+  if (inter && job->kind == 1) *inter = job->ires;
+  if (job->status != JSI_OK) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->last_error = job->error;
+  }
+  return job->status;
+}
+
+int jsi_queue_depth(jsi_context *ctx, int *queued, int *running) {
+  if (!ctx || !queued || !running) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->qmu);
+  *queued = static_cast<int>(ctx->queue.size());
+  *running = ctx->busy;
+  return JSI_OK;
+}
+
+int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
+                           const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms) {
+  if (!ctx || n < 0 || (n > 0 && (!a || !b || !out))) return JSI_ERR_INVALID;
+  if (ctx->lanes.empty()) return record(ctx, JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
+  std::vector<jsi_ticket> tickets(n, 0);
+  int first_err = JSI_OK;
+  // Device span of the batch: every lane waits for a start event on the main
+  // stream; the main stream waits for every lane at the end.
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const int st = guarded(ctx, [&]() {
+      JSI_CUDA(cudaSetDevice(ctx->device));
+      JSI_CUDA(cudaEventRecord(ctx->main.ev0, ctx->main.stream));
+      for (auto &L : ctx->lanes) JSI_CUDA(cudaStreamWaitEvent(L->stream, ctx->main.ev0, 0));
+      return JSI_OK;
+    });
+    if (st != JSI_OK) return st;
+  }
+  for (int q = 0; q < n; ++q) {
+    const int st = jsi_submit_distance(ctx, &a[q], &b[q], params, out[q].trace_pairs, out[q].trace_cap, &tickets[q]);
+    if (st != JSI_OK) {
+      if (status) status[q] = st;
+      if (first_err == JSI_OK) first_err = st;
+      tickets[q] = 0;
+    }
+  }
+  for (int q = 0; q < n; ++q) {
+    if (!tickets[q]) continue;
+    const int st = jsi_wait(ctx, tickets[q], -1, &out[q], nullptr);
+    if (status) status[q] = st;
+    if (st != JSI_OK && first_err == JSI_OK) first_err = st;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int st = guarded(ctx, [&]() {
+    for (auto &L : ctx->lanes) {
+      JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
+      JSI_CUDA(cudaStreamWaitEvent(ctx->main.stream, L->ev1, 0));
+    }
+    JSI_CUDA(cudaEventRecord(ctx->main.ev1, ctx->main.stream));
+    JSI_CUDA(cudaEventSynchronize(ctx->main.ev1));
+    float ms = 0.0f;
+    JSI_CUDA(cudaEventElapsedTime(&ms, ctx->main.ev0, ctx->main.ev1));
+    if (device_ms) *device_ms = ms;
+    return JSI_OK;
+  });
+  return first_err != JSI_OK ? first_err : st;
 }
 
 }  // extern "C"
@@ -1085,15 +1416,16 @@ int eval_grid_impl(jsi_context *ctx, const int ivec[7], const float *data, int n
   std::lock_guard<std::mutex> lk(ctx->mu);
   return guarded(ctx, [&]() {
     if (nuv < 1 || nuv > 8192) fail(JSI_ERR_INVALID, "nuv = %d", nuv);
+    Lane *L = &ctx->main;
     JSI_CUDA(cudaSetDevice(ctx->device));
-    ctx->arena.reset();
-    SurfaceRec s = upload_surface(ctx, ivec, data, ndata, &ctx->arena);
+    L->arena.reset();
+    SurfaceRec s = upload_surface(L, ivec, data, ndata, &L->arena);
     const size_t n = static_cast<size_t>(nuv) * nuv * 18;
-    T *d = ctx->arena.get<T>(n);
-    launch_records(view<T>(s), ustep, vstep, ustart, vstart, nuv, d, ctx->stream);
+    T *d = L->arena.get<T>(n);
+    launch_records(view<T>(s), ustep, vstep, ustart, vstart, nuv, d, L->stream);
     JSI_CUDA(cudaGetLastError());
-    JSI_CUDA(copy_async(ctx, results, d, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
-    JSI_CUDA(cudaStreamSynchronize(ctx->stream));
+    JSI_CUDA(copy_async(L, results, d, n * sizeof(T), cudaMemcpyDeviceToHost, L->stream));
+    JSI_CUDA(cudaStreamSynchronize(L->stream));
     return JSI_OK;
   });
 }
