@@ -50,6 +50,43 @@ FORMS = ("fp32_screen", "fp64", "v5_fp32")  # headline form first
 #             reading 4 Vec4 tile bounds (64 B FP32 / 128 B FP64).
 FLOPS_PER_PAIR_TEST = 8
 
+# Algorithmic work per unit of each kernel (jsi_kernel_units), bicubic
+# surfaces: (flops, HBM bytes) with FMA = 2 flops; bytes for FP32 cells
+# (FP64: x2).  samples: P contraction 2*3*(16+4) = 120 flops, one 16 B sample
+# written.  basis: A2.3 for p = 3 with 2 derivatives ~ 100 flops, 3*4 values
+# + span written (52 B).  cells: 24 min/max + 12 add/div ~ 36 flops, one
+# sample read + one centre written (32 B).  dist_tau / dist_cull: one
+# representative distance (8 flops) / one box-gap bound (14 flops) per tile
+# pair, tile data L2-resident (0 B).  dist_leaf / inter_leaf: 8 / 9 flops per
+# executed cell-pair test, operands in registers (0 B).
+UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "dist_tau": (8, 0),
+             "dist_cull": (14, 0), "dist_leaf": (8, 0), "dist_head": (8, 0), "inter_cull": (14, 0),
+             "inter_leaf": (9, 0)}
+NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 74.4: 148 SMs x 128 lanes x FMA x 1.965 GHz
+NOMINAL_FP64_TFLOPS = NOMINAL_FP32_TFLOPS / 2
+
+
+def roofline(kernel, kt, form, peaks):
+    """Roofline record of the dominant kernel from its live CUDA-event time and
+    its work units; HBM bound against the measured copy bandwidth, plus the
+    CUDA-core bound against the nominal FP32/FP64 peak."""
+    ms, launches, units = kt[kernel]
+    avg_s = ms / max(launches, 1) / 1e3
+    flops_u, bytes_u = UNIT_WORK.get(kernel, (0, 0))
+    fp64 = form == "fp64" or (form == "fp32_screen" and kernel in ("basis",))
+    scale = 2 if fp64 else 1
+    per_launch_units = units / max(launches, 1)
+    gbs = per_launch_units * bytes_u * scale / avg_s / 1e9 if avg_s > 0 else 0.0
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    tflops = per_launch_units * flops_u / avg_s / 1e12 if avg_s > 0 else 0.0
+    fp_peak = NOMINAL_FP64_TFLOPS if fp64 else NOMINAL_FP32_TFLOPS
+    return {"bound": "hbm", "kernel": kernel, "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+            "frac": gbs / hbm_peak, "traffic": None,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+            "avg_launch_ms": avg_s * 1e3, "units_per_launch": per_launch_units,
+            "compute": {"achieved": tflops, "peak": fp_peak, "unit": "TFLOP/s", "frac": tflops / fp_peak,
+                        "peak_source": "nominal CUDA-core peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz; FP64 half)"}}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -326,28 +363,12 @@ def run_ours(args):
     # ---------------- roofline of the dominant kernel ----------------------
     kt = head["kernels"]
     dom = max(kt.items(), key=lambda kv: kv[1][0])[0] if kt else None
-    roof = None
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
     except (OSError, ValueError):
         pass
-    last = head["last"]
-    if dom:
-        ms, n = kt[dom]
-        avg_s = ms / max(n, 1) / 1e3
-        if dom == "dist_leaf":
-            # executed cell-pair tests of the step / leaf launches
-            tests = int(sum(last.pair_tests)) * args.batch
-            launches_per_step = n / args.steps
-            flops = FLOPS_PER_PAIR_TEST * tests / max(launches_per_step, 1)
-            fp_peak = 74.4 if forms[0] != "fp64" else 37.2
-            roof = {"bound": "fp32" if forms[0] != "fp64" else "fp64", "kernel": dom,
-                    "achieved": flops / avg_s / 1e12, "peak": fp_peak, "unit": "TFLOP/s",
-                    "frac": flops / avg_s / 1e12 / fp_peak, "traffic": None,
-                    "peak_source": "nominal CUDA-core peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz; FP64 half)"}
-        else:
-            roof = {"kernel": dom, "avg_ms": avg_s * 1e3}
+    roof = roofline(dom, kt, forms[0], peaks) if dom else None
     cpu = None if args.no_cpu_baseline else cpu_baseline(args.nuv0)
     line = {
         "metric": METRIC, "value": head["value"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
@@ -367,6 +388,7 @@ def run_ours(args):
                    "candidates_per_round": [int(x) for x in last.candidates],
                    "kept_per_round": [int(x) for x in last.npairs]},
         "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
+        "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kt.items()},
     }
     print(json.dumps(line))
     ctx.close()

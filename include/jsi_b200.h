@@ -88,6 +88,10 @@ int jsi_launch_count(unsigned long long *out);
  * one kernel name; jsi_kernel_names lists the names seen (comma separated). */
 int jsi_kernel_timing(jsi_context *ctx, int enable);
 int jsi_kernel_time(jsi_context *ctx, const char *name, double *total_ms, long long *launches);
+/* Work units the timed launches of one kernel processed: grid lines (basis),
+ * samples (samples), cells (cells), tile pairs (dist_tau, dist_cull,
+ * inter_cull), executed cell-pair tests (dist_leaf, inter_leaf). */
+int jsi_kernel_units(jsi_context *ctx, const char *name, double *units);
 const char *jsi_kernel_names(jsi_context *ctx);
 
 /* One query side: EvalAndConstructTask (include/jsi_cad.hpp:11-23) with the

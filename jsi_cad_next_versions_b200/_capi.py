@@ -28,7 +28,7 @@ PRECISIONS = {"v5_fp32": PREC_V5_FP32, "fp64": PREC_FP64, "fp32_screen": PREC_FP
 EXPORTED = [
     "jsi_abi_version", "jsi_status_string", "jsi_last_error", "jsi_create", "jsi_destroy",
     "jsi_surface_upload", "jsi_surface_release", "jsi_resident_bytes", "jsi_context_stream",
-    "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_names",
+    "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_units", "jsi_kernel_names",
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
@@ -114,6 +114,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_kernel_time.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_longlong)]
     L.jsi_kernel_time.restype = I
+    L.jsi_kernel_units.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+    L.jsi_kernel_units.restype = I
     L.jsi_kernel_names.argtypes = [P]
     L.jsi_kernel_names.restype = ctypes.c_char_p
     L.jsi_dist_params_default.argtypes = [ctypes.POINTER(DistParams)]

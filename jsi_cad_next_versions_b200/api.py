@@ -133,13 +133,14 @@ class Context:
         self._check(self.lib.jsi_kernel_timing(self.handle, 1 if enable else 0))
 
     def kernel_times(self) -> dict:
-        """{kernel name: (total ms, launches)} since kernel_timing(True)."""
+        """{kernel name: (total ms, launches, work units)} since kernel_timing(True)."""
         names = self.lib.jsi_kernel_names(self.handle).decode()
         out = {}
         for n in filter(None, names.split(",")):
-            ms, cnt = ctypes.c_double(0), ctypes.c_longlong(0)
+            ms, cnt, units = ctypes.c_double(0), ctypes.c_longlong(0), ctypes.c_double(0)
             self._check(self.lib.jsi_kernel_time(self.handle, n.encode(), ctypes.byref(ms), ctypes.byref(cnt)))
-            out[n] = (ms.value, cnt.value)
+            self._check(self.lib.jsi_kernel_units(self.handle, n.encode(), ctypes.byref(units)))
+            out[n] = (ms.value, cnt.value, units.value)
         return out
 
     def launch_count(self) -> int:

@@ -159,6 +159,7 @@ struct Lane {
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   std::map<std::string, std::pair<double, long long>> kernel_ms;
+  std::map<std::string, double> kernel_units;  // work units (samples, tile pairs, pair tests, ...)
   const std::map<int, SurfaceRec> *surfaces = nullptr;
 };
 
@@ -383,11 +384,11 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
                 T span_v0) {
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
-  timed(ctx, "basis", [&] { launch_basis(v, s, st); });
+  timed(ctx, "basis", [&] { launch_basis(v, s, st); }, 2.0 * s.nreg * s.g.nuv);
   if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
-  timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); });
+  timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); }, double(s.nreg) * s.g.nuv * s.g.nuv);
   if (intersect) timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
-  timed(ctx, "cells", [&] { launch_cells(s, intersect, st); });
+  timed(ctx, "cells", [&] { launch_cells(s, intersect, st); }, double(s.nreg) * s.g.W * s.g.W);
   JSI_CUDA(cudaGetLastError());
 }
 
@@ -416,13 +417,19 @@ void resolve_timing(Lane *ctx) {
   ctx->pending.clear();
 }
 
+// Work units of a kernel (for the live roofline); only kept while timing.
+void add_units(Lane *ctx, const char *name, double units) {
+  if (ctx->timing) ctx->kernel_units[name] += units;
+}
+
 // Runs one launcher, bracketed by events when timing is on.
 template <typename Fn>
-void timed(Lane *ctx, const char *name, Fn &&fn) {
+void timed(Lane *ctx, const char *name, Fn &&fn, double units = 0) {
   if (!ctx->timing) {
     fn();
     return;
   }
+  add_units(ctx, name, units);
   cudaEvent_t a = take_event(ctx), b = take_event(ctx);
   JSI_CUDA(cudaEventRecord(a, ctx->stream));
   fn();
@@ -520,10 +527,10 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
   unsigned long long cand_cap = 1ull << 20;
   DistCand<TC> *cand = ar.get<DistCand<TC>>(cand_cap);
   reset_stats(ctx);
-  timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); });
+  timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); }, double(tile_pairs));
   timed(ctx, "dist_cull", [&] {
     launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, screen, e, st);
-  });
+  }, double(tile_pairs));
   pull_stats(ctx);
   const unsigned long long nsurv = ctx->h_stats->survivors;
   // Leaf order: ascending lower bound, so that the first tile pairs tighten
@@ -596,6 +603,7 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
   }
   *tests = static_cast<long long>(ctx->h_stats->pair_tests);
   *cands = static_cast<long long>(ctx->h_stats->candidates);
+  add_units(ctx, "dist_leaf", static_cast<double>(*tests));
   return ctx->h_stats->nsel;
 }
 
@@ -656,9 +664,9 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
         C.center = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.cpr);
         C.tlo = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
         C.thi = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
-        timed(ctx, "basis", [&] { launch_basis(side ? pb : pa, P, st); });
-        timed(ctx, "samples", [&] { launch_samples_screen(side ? cb : ca, P, C, st); });
-        timed(ctx, "cells", [&] { launch_cells(C, false, st); });
+        timed(ctx, "basis", [&] { launch_basis(side ? pb : pa, P, st); }, 2.0 * P.nreg * P.g.nuv);
+        timed(ctx, "samples", [&] { launch_samples_screen(side ? cb : ca, P, C, st); }, double(P.nreg) * P.g.nuv * P.g.nuv);
+        timed(ctx, "cells", [&] { launch_cells(C, false, st); }, double(C.nreg) * C.g.W * C.g.W);
       }
       auto verify = [&](const DistCand<TC> *c, long long m, DistCand<TP> *o) {
         launch_dist_verify(pa, pb, A, B, map1, map2, c, m, o, st);
@@ -781,6 +789,8 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
       JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
     }
     const long long n = static_cast<long long>(ctx->h_stats->candidates);
+    add_units(ctx, "inter_leaf", static_cast<double>(ctx->h_stats->pair_tests));
+    add_units(ctx, "inter_cull", static_cast<double>(tile_pairs));
     out->counts[round - 1] = n;
     out->pair_tests[round - 1] = static_cast<long long>(ctx->h_stats->pair_tests);
     out->regions1[round - 1] = A.nreg;
@@ -1182,6 +1192,7 @@ int jsi_kernel_timing(jsi_context *ctx, int enable) {
   auto set = [&](Lane &L) {
     L.timing = enable != 0;
     L.kernel_ms.clear();
+    L.kernel_units.clear();
     L.pending.clear();
   };
   set(ctx->main);
@@ -1200,6 +1211,19 @@ int jsi_kernel_time(jsi_context *ctx, const char *name, double *total_ms, long l
       *total_ms += it->second.first;
       *launches += it->second.second;
     }
+  };
+  add(ctx->main);
+  for (auto &L : ctx->lanes) add(*L);
+  return JSI_OK;
+}
+
+int jsi_kernel_units(jsi_context *ctx, const char *name, double *units) {
+  if (!ctx || !name || !units) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  *units = 0.0;
+  auto add = [&](Lane &L) {
+    auto it = L.kernel_units.find(name);
+    if (it != L.kernel_units.end()) *units += it->second;
   };
   add(ctx->main);
   for (auto &L : ctx->lanes) add(*L);
