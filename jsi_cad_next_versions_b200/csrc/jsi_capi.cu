@@ -521,16 +521,51 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
   Arena &ar = ctx->arena;
   cudaStream_t st = ctx->stream;
   const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
-  if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
-  unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
-  unsigned *surv_lb = ar.get<unsigned>(tile_pairs);
   unsigned long long cand_cap = 1ull << 20;
   DistCand<TC> *cand = ar.get<DistCand<TC>>(cand_cap);
+  unsigned long long *surv = nullptr;
+  unsigned *surv_lb = nullptr;
   reset_stats(ctx);
-  timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); }, double(tile_pairs));
-  timed(ctx, "dist_cull", [&] {
-    launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, screen, e, st);
-  }, double(tile_pairs));
+  if (A.g.tw > kMaxTile || B.g.tw > kMaxTile) {
+    // Two levels: supertile pairs (8 x 8 tiles each) seed tau and are culled;
+    // only the tile pairs inside surviving supertile pairs are examined.
+    SideRound<TC> As = A, Bs = B;
+    As.stlo = ar.get<Vec4<TC>>(static_cast<size_t>(A.nreg) * A.g.nst);
+    As.sthi = ar.get<Vec4<TC>>(static_cast<size_t>(A.nreg) * A.g.nst);
+    Bs.stlo = ar.get<Vec4<TC>>(static_cast<size_t>(B.nreg) * B.g.nst);
+    Bs.sthi = ar.get<Vec4<TC>>(static_cast<size_t>(B.nreg) * B.g.nst);
+    timed(ctx, "supertiles", [&] {
+      launch_supertiles(As, st);
+      launch_supertiles(Bs, st);
+    }, double(A.nreg) * A.g.nst + double(B.nreg) * B.g.nst);
+    const unsigned long long st_pairs = static_cast<unsigned long long>(nslots) * A.g.nst * B.g.nst;
+    if (st_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu supertile pairs exceed the screen's list", st_pairs);
+    unsigned long long *st_surv = ar.get<unsigned long long>(st_pairs);
+    timed(ctx, "dist_tau", [&] { launch_dist_tau_st(As, Bs, map1, map2, nslots, k, ctx->d_stats, screen, e, st); },
+          double(st_pairs));
+    timed(ctx, "dist_cull", [&] {
+      launch_dist_cull_st(As, Bs, map1, map2, nslots, st_surv, st_pairs, ctx->d_stats, screen, e, st);
+    }, double(st_pairs));
+    pull_stats(ctx);
+    const unsigned long long n_st = ctx->h_stats->st_survivors;
+    const unsigned long long cap = n_st * kMaxTile * kMaxTile * kMaxTile * kMaxTile;
+    if (cap > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", cap);
+    surv = ar.get<unsigned long long>(std::max<unsigned long long>(cap, 1));
+    surv_lb = ar.get<unsigned>(std::max<unsigned long long>(cap, 1));
+    timed(ctx, "dist_expand", [&] {
+      launch_dist_expand(As, Bs, map1, map2, st_surv, n_st, k, 0, surv, surv_lb, cap, ctx->d_stats, screen, e, st);
+      launch_dist_expand(As, Bs, map1, map2, st_surv, n_st, k, 1, surv, surv_lb, cap, ctx->d_stats, screen, e, st);
+    }, 2.0 * double(cap));
+  } else {
+    if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+    surv = ar.get<unsigned long long>(tile_pairs);
+    surv_lb = ar.get<unsigned>(tile_pairs);
+    timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); },
+          double(tile_pairs));
+    timed(ctx, "dist_cull", [&] {
+      launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, screen, e, st);
+    }, double(tile_pairs));
+  }
   pull_stats(ctx);
   const unsigned long long nsurv = ctx->h_stats->survivors;
   // Leaf order: ascending lower bound, so that the first tile pairs tighten

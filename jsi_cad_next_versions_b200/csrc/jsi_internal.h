@@ -57,6 +57,8 @@ struct Geom {
   int ntiles; // tw * tw
   int cpr;    // padded cells per region = ntiles * te * te
   int p1max;  // basis stride (max degree + 1)
+  int stw;    // supertiles (8 x 8 tiles) per direction
+  int nst;    // stw * stw
 };
 
 inline Geom make_geom(int nuv, int p1max) {
@@ -69,6 +71,8 @@ inline Geom make_geom(int nuv, int p1max) {
   g.ntiles = g.tw * g.tw;
   g.cpr = g.ntiles * g.te * g.te;
   g.p1max = p1max;
+  g.stw = (g.tw + kMaxTile - 1) / kMaxTile;
+  g.nst = g.stw * g.stw;
   return g;
 }
 
@@ -88,6 +92,8 @@ struct SideRound {
   Vec4<T> *tlo;
   Vec4<T> *thi;
   Vec4<T> *thmax;
+  Vec4<T> *stlo;  // supertile bounds [R][nst] (built on demand)
+  Vec4<T> *sthi;
 };
 
 // Candidate of the distance screen.
@@ -109,6 +115,7 @@ struct ScreenStats {
   int nreg1, nreg2;                 // unique regions built for the next round
   int pad_;
   unsigned long long work;          // work counter of the persistent leaf kernels
+  unsigned long long st_survivors;  // supertile pairs that passed the bound
 };
 
 // A surviving tile pair: (row = slot * ntiles1 + t1) << 32 | t2.
@@ -144,6 +151,23 @@ void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *m
                       const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
                       int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, bool screen,
                       float e, cudaStream_t st);
+// Supertile level of the distance screen: bounds of 8 x 8 tiles, threshold
+// seed and cull over supertile pairs, expansion of the surviving supertile
+// pairs into tile pairs (threshold pass, then cull with the bound keys).
+template <typename T>
+void launch_supertiles(const SideRound<T> &sr, cudaStream_t st);
+template <typename T>
+void launch_dist_tau_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                        int k, ScreenStats *stats, bool screen, float e, cudaStream_t st);
+template <typename T>
+void launch_dist_cull_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                         unsigned long long *surv, unsigned long long cap, ScreenStats *stats, bool screen, float e,
+                         cudaStream_t st);
+template <typename T>
+void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                        const unsigned long long *st_surv, unsigned long long nst_surv, int k, int cull,
+                        unsigned long long *surv, unsigned *surv_lb, unsigned long long cap, ScreenStats *stats,
+                        bool screen, float e, cudaStream_t st);
 // Exact k-th d2 (k <= 8) of each of the first nhead tile pairs, folded into tau.
 template <typename T>
 void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,

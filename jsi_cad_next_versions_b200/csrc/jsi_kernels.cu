@@ -901,6 +901,155 @@ __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> 
   }
 }
 
+// ---- supertile level ------------------------------------------------------
+
+// Bounds of every supertile (8 x 8 tiles): one warp reduces its <= 64 tiles.
+template <typename T>
+__global__ void k_supertiles(SideRound<T> sr) {
+  const Geom g = sr.g;
+  const int lane = threadIdx.x & 31;
+  const long long total = static_cast<long long>(sr.nreg) * g.nst;
+  const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  for (long long w = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; w < total; w += nwarps) {
+    const int r = static_cast<int>(w / g.nst), st = static_cast<int>(w - static_cast<long long>(r) * g.nst);
+    const int sy = st / g.stw, sx = st - (st / g.stw) * g.stw;
+    T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
+    T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
+    for (int l = lane; l < kMaxTile * kMaxTile; l += 32) {
+      const int ty = sy * kMaxTile + l / kMaxTile, tx = sx * kMaxTile + l % kMaxTile;
+      if (ty < g.tw && tx < g.tw) {
+        const long long t = static_cast<long long>(r) * g.ntiles + ty * g.tw + tx;
+        const Vec4<T> a = sr.tlo[t], b = sr.thi[t];
+        lo[0] = tmin(lo[0], a.x);
+        lo[1] = tmin(lo[1], a.y);
+        lo[2] = tmin(lo[2], a.z);
+        hi[0] = tmax(hi[0], b.x);
+        hi[1] = tmax(hi[1], b.y);
+        hi[2] = tmax(hi[2], b.z);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = tmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+        hi[c] = tmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+      }
+    }
+    if (lane == 0) {
+      sr.stlo[w] = Vec4<T>{lo[0], lo[1], lo[2], T(0)};
+      sr.sthi[w] = Vec4<T>{hi[0], hi[1], hi[2], T(0)};
+    }
+  }
+}
+
+// Representative cell of a supertile: the representative of its middle tile.
+__device__ __forceinline__ long long super_rep(int r, int st, const Geom &g) {
+  const int sy = st / g.stw, sx = st - (st / g.stw) * g.stw;
+  const int nty = min(kMaxTile, g.tw - sy * kMaxTile), ntx = min(kMaxTile, g.tw - sx * kMaxTile);
+  const int t = (sy * kMaxTile + nty / 2) * g.tw + sx * kMaxTile + ntx / 2;
+  return (static_cast<long long>(r) * g.ntiles + t) * (g.te * g.te) + tile_rep(t, g);
+}
+
+template <typename T, bool S>
+__global__ void __launch_bounds__(256) k_dist_tau_st(SideRound<T> a, SideRound<T> b, const int *map1,
+                                                     const int *map2, int nslots, int k, ScreenStats *stats, float e) {
+  __shared__ unsigned sh[256];
+  const Geom g1 = a.g, g2 = b.g;
+  const int nrows = nslots * g1.nst;
+  float best = __uint_as_float(0x7f800000u);
+  for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const int slot = row / g1.nst, s1 = row - slot * g1.nst;
+    const Vec4<T> c1 = a.center[super_rep(map1[slot], s1, g1)];
+    for (int s2 = threadIdx.x; s2 < g2.nst; s2 += blockDim.x) {
+      const Vec4<T> c2 = b.center[super_rep(map2[slot], s2, g2)];
+      best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+    }
+  }
+  fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+}
+
+template <typename T, bool S>
+__global__ void k_dist_cull_st(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
+                               unsigned long long *surv, unsigned long long cap, ScreenStats *stats, float e) {
+  const Geom g1 = a.g, g2 = b.g;
+  const int nrows = nslots * g1.nst;
+  const T tau = thr_compare<T, S>(stats->tau_bits, e);
+  for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const int slot = row / g1.nst, s1 = row - slot * g1.nst;
+    const long long i1 = static_cast<long long>(map1[slot]) * g1.nst + s1;
+    const Vec4<T> lo1 = a.stlo[i1], hi1 = a.sthi[i1];
+    const long long base2 = static_cast<long long>(map2[slot]) * g2.nst;
+    for (int s0 = 0; s0 < g2.nst; s0 += blockDim.x) {
+      const int s2 = s0 + threadIdx.x;
+      bool keep = false;
+      if (s2 < g2.nst) {
+        T lb = tile_lb(lo1, hi1, b.stlo[base2 + s2], b.sthi[base2 + s2]);
+        if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
+        keep = lb <= tau;
+      }
+      const long long pos = warp_append(keep, &stats->st_survivors);
+      if (pos >= 0 && static_cast<unsigned long long>(pos) < cap)
+        surv[pos] = pack_tile_pair(static_cast<unsigned>(row), static_cast<unsigned>(s2));
+    }
+  }
+}
+
+// One block per surviving supertile pair; its <= 64 x 64 child tile pairs.
+// cull = 0: fold the representative distances into tau; cull = 1: append the
+// tile pairs whose bound passes tau, with the bound as sort key (the same
+// format k_dist_cull writes).
+template <typename T, bool S>
+__global__ void __launch_bounds__(256) k_dist_expand(SideRound<T> a, SideRound<T> b, const int *map1,
+                                                     const int *map2, const unsigned long long *st_surv,
+                                                     unsigned long long nst_surv, int k, int cull,
+                                                     unsigned long long *surv, unsigned *surv_lb,
+                                                     unsigned long long cap, ScreenStats *stats, float e) {
+  __shared__ unsigned sh[256];
+  const Geom g1 = a.g, g2 = b.g;
+  const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
+  float best = __uint_as_float(0x7f800000u);
+  const T tau = thr_compare<T, S>(stats->tau_bits, e);
+  for (unsigned long long w = blockIdx.x; w < nst_surv; w += gridDim.x) {
+    const unsigned long long q = st_surv[w];
+    const int row = static_cast<int>(q >> 32), s2 = static_cast<int>(q & 0xffffffffull);
+    const int slot = row / g1.nst, s1 = row - slot * g1.nst;
+    const int r1 = map1[slot], r2 = map2[slot];
+    const int sy1 = s1 / g1.stw, sx1 = s1 - sy1 * g1.stw, sy2 = s2 / g2.stw, sx2 = s2 - sy2 * g2.stw;
+    for (int c0 = 0; c0 < kMaxTile * kMaxTile * kMaxTile * kMaxTile; c0 += blockDim.x) {
+      const int c = c0 + threadIdx.x;
+      const int l1 = c >> 6, l2 = c & 63;
+      const int ty1 = sy1 * kMaxTile + (l1 >> 3), tx1 = sx1 * kMaxTile + (l1 & 7);
+      const int ty2 = sy2 * kMaxTile + (l2 >> 3), tx2 = sx2 * kMaxTile + (l2 & 7);
+      const bool valid = ty1 < g1.tw && tx1 < g1.tw && ty2 < g2.tw && tx2 < g2.tw;
+      const int t1 = ty1 * g1.tw + tx1, t2 = ty2 * g2.tw + tx2;
+      bool keep = false;
+      T lb = T(0);
+      if (valid) {
+        const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
+        const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
+        if (!cull) {
+          const Vec4<T> c1 = a.center[i1 * n1 + tile_rep(t1, g1)];
+          const Vec4<T> c2 = b.center[i2 * n2 + tile_rep(t2, g2)];
+          best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+        } else {
+          lb = tile_lb(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
+          if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
+          keep = lb <= tau;
+        }
+      }
+      if (cull) {
+        const long long pos = warp_append(keep, &stats->survivors);
+        if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) {
+          surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + t1), static_cast<unsigned>(t2));
+          surv_lb[pos] = lb_bits_down(lb);
+        }
+      }
+    }
+  }
+  if (!cull) fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+}
+
 // Total order of the top-k (distance_analysis.cu:226-231).
 template <typename T>
 __device__ __forceinline__ bool cand_less(const DistCand<T> &x, const DistCand<T> &y) {
@@ -1488,6 +1637,64 @@ void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *m
 }
 
 template <typename T>
+void launch_supertiles(const SideRound<T> &sr, cudaStream_t st) {
+  counted();
+  const long long warps = static_cast<long long>(sr.nreg) * sr.g.nst;
+  k_supertiles<T><<<grid_for(warps * 32, 256, 148 * 32), 256, 0, st>>>(sr);
+}
+
+template <typename T>
+void launch_dist_tau_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                        int k, ScreenStats *stats, bool screen, float e, cudaStream_t st) {
+  counted();
+  const int rows = nslots * a.g.nst;
+  const int grid = rows < 148 * 8 ? rows : 148 * 8;
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_tau_st<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+      return;
+    }
+  }
+  k_dist_tau_st<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+}
+
+template <typename T>
+void launch_dist_cull_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
+                         unsigned long long *surv, unsigned long long cap, ScreenStats *stats, bool screen, float e,
+                         cudaStream_t st) {
+  counted();
+  const int rows = nslots * a.g.nst;
+  const int grid = rows < 148 * 16 ? rows : 148 * 16;
+  const int block = b.g.nst >= 256 ? 256 : (b.g.nst >= 128 ? 128 : 64);
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_cull_st<float, true><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, cap, stats, e);
+      return;
+    }
+  }
+  k_dist_cull_st<T, false><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, cap, stats, e);
+}
+
+template <typename T>
+void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
+                        const unsigned long long *st_surv, unsigned long long nst_surv, int k, int cull,
+                        unsigned long long *surv, unsigned *surv_lb, unsigned long long cap, ScreenStats *stats,
+                        bool screen, float e, cudaStream_t st) {
+  counted();
+  if (nst_surv == 0) return;
+  const int grid = static_cast<int>(nst_surv < 148ull * 8 ? nst_surv : 148ull * 8);
+  if constexpr (std::is_same<T, float>::value) {
+    if (screen) {
+      k_dist_expand<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, k, cull, surv, surv_lb,
+                                                        cap, stats, e);
+      return;
+    }
+  }
+  k_dist_expand<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, k, cull, surv, surv_lb, cap,
+                                                 stats, e);
+}
+
+template <typename T>
 void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                       const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats, bool screen,
                       float e, cudaStream_t st) {
@@ -1600,6 +1807,16 @@ void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, 
                                     const unsigned long long *, const unsigned *, unsigned long long, int, int,   \
                                     DistCand<T> *, unsigned long long, ScreenStats *, bool, float,               \
                                     cudaStream_t);                                                                \
+  template void launch_supertiles<T>(const SideRound<T> &, cudaStream_t);                                         \
+  template void launch_dist_tau_st<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,  \
+                                      int, ScreenStats *, bool, float, cudaStream_t);                             \
+  template void launch_dist_cull_st<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, \
+                                       unsigned long long *, unsigned long long, ScreenStats *, bool, float,      \
+                                       cudaStream_t);                                                             \
+  template void launch_dist_expand<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,       \
+                                      const unsigned long long *, unsigned long long, int, int,                   \
+                                      unsigned long long *, unsigned *, unsigned long long, ScreenStats *, bool,  \
+                                      float, cudaStream_t);                                                       \
   template void launch_dist_head<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
                                     const unsigned long long *, unsigned long long, int, ScreenStats *, bool,     \
                                     float, cudaStream_t);                                                         \

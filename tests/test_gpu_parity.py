@@ -294,3 +294,24 @@ def test_distance_screen_full_size(gpu_ctx):
     assert np.array_equal(scr.kth_d2, ref.kth_d2)
     for r in range(4):
         assert np.array_equal(scr.pairs[r], ref.pairs[r])
+
+
+def test_distance_4x_scaled_nuv2048(gpu_ctx):
+    """The 4x geometrically scaled hard-wave pair at nuv0 = 2048 (4.19M cells
+    per side, 1.76e13 cell pairs brute force): the FP32-screen form equals the
+    FP64 form round by round, and the V5-FP32 value agrees with FP64 to FP32
+    precision.  (The CPU paths would need hours at this size.)"""
+    A, B, _ = synth.distance_pair_hard_wave(scale=4.0)
+    sa, sb = gpu_ctx.upload(A), gpu_ctx.upload(B)
+    ta, tb = _task(gpu_ctx, sa, rect32(A), 2048, 1), _task(gpu_ctx, sb, rect32(B), 2048, 2)
+    r64 = gpu_ctx.min_distance(ta, tb, precision="fp64", trace=True)
+    scr = gpu_ctx.min_distance(ta, tb, precision="fp32_screen", trace=True)
+    v5 = gpu_ctx.min_distance(ta, tb, precision="v5_fp32", trace=True)
+    gpu_ctx.release(sa)
+    gpu_ctx.release(sb)
+    assert np.array_equal(scr.kth_d2, r64.kth_d2)
+    for r in range(4):
+        assert np.array_equal(scr.pairs[r], r64.pairs[r])
+    assert abs(v5.distance - r64.distance) <= 1e-5 * r64.distance
+    # round 1 examined a tiny fraction of the (2047^2)^2 pairs
+    assert r64.pair_tests[0] < 1e9
