@@ -113,7 +113,7 @@ typedef struct {
   int k;          /* k_of_topk, 1..1024 */
   int rounds;     /* max_layers, 1..JSI_MAX_ROUNDS */
   int precision;  /* jsi_precision */
-  int newton;     /* 1: FP64 Newton refinement of the closest points from the final candidates */
+  int newton;     /* 1: FP64 Levenberg-Marquardt from every final candidate pair to the closest points */
 } jsi_dist_params;
 
 typedef struct {
@@ -150,6 +150,7 @@ typedef struct {
   int halve_threshold; /* 512 */
   int min_nuv;         /* 4 */
   int precision;       /* jsi_precision */
+  int points;          /* 1: refine every final pair to an intersection point (FP64) */
 } jsi_inter_params;
 
 typedef struct {
@@ -165,6 +166,14 @@ typedef struct {
   int *trace_pairs;
   long long trace_cap;
   long long trace_written;
+  /* Optional intersection points (caller-owned, points = 1): 8 doubles per
+   * final pair, in the final round's (slot, i, j) order: x, y, z of the point,
+   * (u, v) on surface 1, (s, t) on surface 2, residual |S1 - S2|; a point is
+   * counted as converged when residual <= 1e-9 (1 + |x| + |y| + |z|). */
+  double *points;
+  long long points_cap;
+  long long points_written;
+  long long points_converged;
   float device_ms;
 } jsi_inter_result;
 

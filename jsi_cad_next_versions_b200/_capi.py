@@ -62,7 +62,8 @@ class DistResult(ctypes.Structure):
 
 class InterParams(ctypes.Structure):
     _fields_ = [("nuv_refine", ctypes.c_int), ("use_k", ctypes.c_int), ("rounds", ctypes.c_int),
-                ("halve_threshold", ctypes.c_int), ("min_nuv", ctypes.c_int), ("precision", ctypes.c_int)]
+                ("halve_threshold", ctypes.c_int), ("min_nuv", ctypes.c_int), ("precision", ctypes.c_int),
+                ("points", ctypes.c_int)]
 
 
 class InterResult(ctypes.Structure):
@@ -70,7 +71,9 @@ class InterResult(ctypes.Structure):
                 ("pair_tests", ctypes.c_longlong * MAX_ROUNDS), ("regions1", ctypes.c_longlong * MAX_ROUNDS),
                 ("regions2", ctypes.c_longlong * MAX_ROUNDS), ("pad", ctypes.c_double * 2),
                 ("trace_pairs", ctypes.POINTER(ctypes.c_int)), ("trace_cap", ctypes.c_longlong),
-                ("trace_written", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+                ("trace_written", ctypes.c_longlong), ("points", ctypes.POINTER(ctypes.c_double)),
+                ("points_cap", ctypes.c_longlong), ("points_written", ctypes.c_longlong),
+                ("points_converged", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
 
 
 _lib = None

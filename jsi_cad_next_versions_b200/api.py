@@ -59,6 +59,8 @@ class IntersectionResult:
     pad: tuple
     device_ms: float
     pairs: list = field(default_factory=list)  # per round (n, 3) int32 if traced
+    points: np.ndarray | None = None  # (n, 8): x, y, z, u, v, s, t, residual
+    points_converged: int = 0
 
 
 class Context:
@@ -206,7 +208,7 @@ class Context:
                          halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",
                          trace: bool = False, trace_cap: int = 1 << 22):
         prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
-        p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec)
+        p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec, 0)
         buf = np.full(trace_cap * 3, -1, dtype=np.int32) if trace else None
         t = ctypes.c_longlong(0)
         ptr = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if trace else None
@@ -259,18 +261,28 @@ class Context:
 
     def intersect(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                   halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",
-                  trace: bool = False, trace_cap: int = 1 << 24) -> IntersectionResult:
+                  trace: bool = False, trace_cap: int = 1 << 24, points: bool = False,
+                  points_cap: int = 1 << 22) -> IntersectionResult:
         prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
-        p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec)
+        p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec, 1 if points else 0)
         r = C.InterResult()
         buf = None
         if trace:
             buf = np.full(trace_cap * 3, -1, dtype=np.int32)
             r.trace_pairs = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
             r.trace_cap = trace_cap
+        pbuf = None
+        if points:
+            pbuf = np.zeros(points_cap * 8, dtype=np.float64)
+            r.points = pbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            r.points_cap = points_cap
         self._check(self.lib.jsi_intersect(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
                                            ctypes.byref(r)))
-        return self._inter_result(r, buf, trace_cap)
+        res = self._inter_result(r, buf, trace_cap)
+        if points:
+            res.points = pbuf[:r.points_written * 8].reshape(-1, 8).copy()
+            res.points_converged = int(r.points_converged)
+        return res
 
     @staticmethod
     def _inter_result(r: C.InterResult, buf, trace_cap: int) -> IntersectionResult:

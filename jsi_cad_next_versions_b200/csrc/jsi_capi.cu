@@ -642,6 +642,52 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
   return ctx->h_stats->nsel;
 }
 
+// Query rectangles as Newton bounds {u0, u1, v0, v1, s0, s1, t0, t1}.
+void newton_domain(const jsi_task *ta, const jsi_task *tb, double dom[8]) {
+  const float r[2][4] = {{ta->ustart, ta->ustop, ta->vstart, ta->vstop}, {tb->ustart, tb->ustop, tb->vstart, tb->vstop}};
+  for (int side = 0; side < 2; ++side)
+    for (int d = 0; d < 2; ++d) {
+      const double a = r[side][2 * d], b = r[side][2 * d + 1];
+      dom[side * 4 + 2 * d] = std::min(a, b);
+      dom[side * 4 + 2 * d + 1] = std::max(a, b);
+    }
+}
+
+// FP64 Levenberg-Marquardt from every final candidate pair; the smallest
+// distance wins (earliest candidate on ties).
+template <typename TP>
+void newton_refine(Lane *ctx, const SurfaceRec &sa, const SurfaceRec &sb, const jsi_task *ta, const jsi_task *tb,
+                   const SideRound<TP> &A, const SideRound<TP> &B, const int *map1, const int *map2,
+                   const DistCand<TP> *top, int n, jsi_dist_result *out) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  double dom[8];
+  newton_domain(ta, tb, dom);
+  double *ddom = ar.get<double>(8);
+  double *dres = ar.get<double>(static_cast<size_t>(n) * 11);
+  JSI_CUDA(copy_async(ctx, ddom, dom, sizeof(dom), cudaMemcpyHostToDevice, st));
+  timed(ctx, "newton", [&] {
+    launch_newton_dist(view<double>(sa), view<double>(sb), A.regions, B.regions, map1, map2, A.g.nuv, B.g.nuv, top,
+                       n, ddom, dres, st);
+  }, double(n));
+  std::vector<double> h(static_cast<size_t>(n) * 11);
+  JSI_CUDA(copy_async(ctx, h.data(), dres, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  JSI_CUDA(cudaStreamSynchronize(st));
+  int best = 0;
+  for (int q = 1; q < n; ++q)
+    if (h[q * 11] < h[best * 11]) best = q;
+  const double *b = h.data() + static_cast<size_t>(best) * 11;
+  out->newton_distance = b[0];
+  out->uv1[0] = b[1];
+  out->uv1[1] = b[2];
+  out->uv2[0] = b[3];
+  out->uv2[1] = b[4];
+  for (int c = 0; c < 3; ++c) {
+    out->point1[c] = b[5 + c];
+    out->point2[c] = b[8 + c];
+  }
+}
+
 struct NoVerify {
   template <typename A, typename B>
   void operator()(const A *, long long, B *) const {}
@@ -732,6 +778,7 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
       const TP root = std::sqrt(kth);
       out->v5_value = static_cast<float>(root);
       out->distance = static_cast<double>(root);
+      if (p->newton && n > 0) newton_refine(ctx, sa, sb, ta, tb, A, B, map1, map2, top, n, out);
       break;
     }
     // Next round (nuv = next_nuv after round 1, distance_analysis.cu:389).
@@ -861,7 +908,34 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
       }
     }
     written += n;
-    if (round == p->rounds || n == 0) break;
+    if (round == p->rounds || n == 0) {
+      if (p->points && n > 0 && out->points) {
+        // Intersection points from every final pair (minimum-norm Gauss-Newton).
+        double dom[8];
+        newton_domain(ta, tb, dom);
+        double *ddom = ar.get<double>(8);
+        double *dres = ar.get<double>(static_cast<size_t>(n) * 8);
+        JSI_CUDA(copy_async(ctx, ddom, dom, sizeof(dom), cudaMemcpyHostToDevice, st));
+        timed(ctx, "newton", [&] {
+          launch_newton_inter(view<double>(sa), view<double>(sb), A.regions, B.regions, map1, map2, A.g.nuv, B.g.nuv,
+                              sorted, n, ij_bits, ddom, dres, st);
+        }, double(n));
+        const long long keep = std::min<long long>(n, out->points_cap);
+        if (keep > 0)
+          JSI_CUDA(copy_async(ctx, out->points, dres, static_cast<size_t>(keep) * 8 * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+        JSI_CUDA(cudaStreamSynchronize(st));
+        out->points_written = keep;
+        long long conv = 0;
+        for (long long q = 0; q < keep; ++q) {
+          const double *pt = out->points + q * 8;
+          const double scale = 1.0 + std::fabs(pt[0]) + std::fabs(pt[1]) + std::fabs(pt[2]);
+          if (pt[7] <= 1e-9 * scale) ++conv;
+        }
+        out->points_converged = conv;
+      }
+      break;
+    }
     if (n > p->halve_threshold && nuv > p->min_nuv) nuv /= 2;  // intersection.cu:370
     if (n > (1ll << 31) - 1) fail(JSI_ERR_CAPACITY, "too many pairs for the next round");
     // Pair-preserving jobs and (slot, cell) dedup per side on the device.
@@ -949,7 +1023,6 @@ void validate_dist(jsi_dist_params &p, const jsi_task *a, const jsi_task *b) {
   if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
   if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
   check_precision(p.precision, true);
-  if (p.newton) fail(JSI_ERR_UNSUPPORTED, "Newton refinement not built yet");
   check_task<float>(a);
   check_task<float>(b);
 }
@@ -990,9 +1063,13 @@ void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_
                        jsi_inter_result *out) {
   int *tp = out->trace_pairs;
   const long long tc = out->trace_cap;
+  double *pts = out->points;
+  const long long pc = out->points_cap;
   std::memset(out, 0, sizeof(*out));
   out->trace_pairs = tp;
   out->trace_cap = tc;
+  out->points = pts;
+  out->points_cap = pc;
   JSI_CUDA(cudaSetDevice(L->device));
   L->arena.reset();
   JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
@@ -1303,6 +1380,7 @@ void jsi_inter_params_default(jsi_inter_params *p) {
   p->halve_threshold = 512;
   p->min_nuv = 4;
   p->precision = JSI_PREC_V5_FP32;
+  p->points = 0;
 }
 
 int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
@@ -1380,6 +1458,8 @@ int jsi_submit_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b,
     validate_inter(job->ip, a, b);
     job->ires.trace_pairs = trace_pairs;
     job->ires.trace_cap = trace_cap;
+    job->ires.points = nullptr;
+    job->ires.points_cap = 0;
     *out = enqueue(ctx, job);
     return JSI_OK;
   });

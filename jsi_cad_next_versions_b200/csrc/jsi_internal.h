@@ -207,4 +207,17 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
                         const unsigned *flag2, const unsigned *ex2, const SideRound<T> &cur, const int *map2,
                         RegionRec<T> *next, int *nmap2, cudaStream_t st);
 
+// FP64 Newton refinement.  dom = {u0, u1, v0, v1, s0, s1, t0, t1} (the query
+// rectangles).  Distance: 11 doubles per candidate (d, u, v, s, t, P1, P2);
+// intersection: 8 doubles per pair (x, y, z, u, v, s, t, residual).
+template <typename TP>
+void launch_newton_dist(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
+                        const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                        const DistCand<TP> *top, int n, const double *dom, double *out, cudaStream_t st);
+template <typename TP>
+void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
+                         const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                         const unsigned long long *keys, long long n, int ij_bits, const double *dom, double *out,
+                         cudaStream_t st);
+
 }  // namespace jsi

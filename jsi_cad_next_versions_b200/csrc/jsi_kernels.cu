@@ -1525,6 +1525,220 @@ __global__ void k_dist_verify(SurfView<double> sa, SurfView<double> sb, SideRoun
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 Newton refinement (closest points, intersection points)
+// ---------------------------------------------------------------------------
+
+// Full 18-value record at an arbitrary (u, v) in FP64.
+__device__ void point_record(const SurfView<double> &s, double u, double v, double rec[18]) {
+  double Nu[3 * (kMaxDeg + 1)], Nv[3 * (kMaxDeg + 1)];
+  int spanu = s.degu, spanv = s.degv;
+  if (!s.zero) {
+    spanu = find_span(s.nku, s.degu, u, s.U);
+    basis_ders<double, kMaxDeg + 1>(spanu, s.degu, u, s.U, s.du, Nu, kMaxDeg + 1);
+    spanv = find_span(s.nkv, s.degv, v, s.V);
+    basis_ders<double, kMaxDeg + 1>(spanv, s.degv, v, s.V, s.dv, Nv, kMaxDeg + 1);
+  }
+  eval_record(s, spanu, Nu, spanv, Nv, kMaxDeg + 1, rec);
+}
+
+__device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+__device__ __forceinline__ double clampd(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// Solves the n x n system M x = r (n <= 4) by Gaussian elimination with
+// partial pivoting; returns false when a pivot vanishes.
+__device__ bool solve_small(double M[4][4], double r[4], int n) {
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    for (int q = c + 1; q < n; ++q)
+      if (fabs(M[q][c]) > fabs(M[piv][c])) piv = q;
+    if (!(fabs(M[piv][c]) > 0.0)) return false;
+    if (piv != c) {
+      for (int q = 0; q < n; ++q) {
+        const double t = M[c][q];
+        M[c][q] = M[piv][q];
+        M[piv][q] = t;
+      }
+      const double t = r[c];
+      r[c] = r[piv];
+      r[piv] = t;
+    }
+    for (int q = c + 1; q < n; ++q) {
+      const double f = M[q][c] / M[c][c];
+      for (int w = c; w < n; ++w) M[q][w] -= f * M[c][w];
+      r[q] -= f * r[c];
+    }
+  }
+  for (int c = n - 1; c >= 0; --c) {
+    double acc = r[c];
+    for (int q = c + 1; q < n; ++q) acc -= M[c][q] * r[q];
+    r[c] = acc / M[c][c];
+  }
+  return true;
+}
+
+// Levenberg-Marquardt on f(u, v, s, t) = |S1(u, v) - S2(s, t)|^2 from the
+// centres of the candidate cells, inside the query rectangles.  Records are
+// P, Pu, Pv, Puu, Puv, Pvv (3 each).  out: d, u, v, s, t, P1[3], P2[3].
+__device__ void newton_distance(const SurfView<double> &sa, const SurfView<double> &sb, const double dom[8],
+                                double x[4], double out[11]) {
+  double r1[18], r2[18];
+  point_record(sa, x[0], x[1], r1);
+  point_record(sb, x[2], x[3], r2);
+  double D[3] = {r1[0] - r2[0], r1[1] - r2[1], r1[2] - r2[2]};
+  double f = dot3(D, D);
+  double lam = 1e-6;
+  for (int it = 0; it < 60; ++it) {
+    const double *S1u = r1 + 3, *S1v = r1 + 6, *S1uu = r1 + 9, *S1uv = r1 + 12, *S1vv = r1 + 15;
+    const double *S2s = r2 + 3, *S2t = r2 + 6, *S2ss = r2 + 9, *S2st = r2 + 12, *S2tt = r2 + 15;
+    double g[4] = {dot3(D, S1u), dot3(D, S1v), -dot3(D, S2s), -dot3(D, S2t)};
+    double H[4][4];
+    H[0][0] = dot3(S1u, S1u) + dot3(D, S1uu);
+    H[0][1] = dot3(S1u, S1v) + dot3(D, S1uv);
+    H[1][1] = dot3(S1v, S1v) + dot3(D, S1vv);
+    H[0][2] = -dot3(S1u, S2s);
+    H[0][3] = -dot3(S1u, S2t);
+    H[1][2] = -dot3(S1v, S2s);
+    H[1][3] = -dot3(S1v, S2t);
+    H[2][2] = dot3(S2s, S2s) - dot3(D, S2ss);
+    H[2][3] = dot3(S2s, S2t) - dot3(D, S2st);
+    H[3][3] = dot3(S2t, S2t) - dot3(D, S2tt);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < a; ++b) H[a][b] = H[b][a];
+    bool moved = false;
+    while (lam < 1e16) {
+      double M[4][4], step[4];
+      for (int a = 0; a < 4; ++a) {
+        for (int b = 0; b < 4; ++b) M[a][b] = H[a][b];
+        M[a][a] += lam * (fabs(H[a][a]) + 1e-30);
+        step[a] = -g[a];
+      }
+      if (!solve_small(M, step, 4)) {
+        lam *= 10.0;
+        continue;
+      }
+      double y[4];
+      for (int a = 0; a < 4; ++a) y[a] = clampd(x[a] + step[a], dom[2 * a], dom[2 * a + 1]);
+      double q1[18], q2[18];
+      point_record(sa, y[0], y[1], q1);
+      point_record(sb, y[2], y[3], q2);
+      const double E[3] = {q1[0] - q2[0], q1[1] - q2[1], q1[2] - q2[2]};
+      const double fy = dot3(E, E);
+      if (fy < f) {
+        double dmax = 0.0;
+        for (int a = 0; a < 4; ++a) {
+          dmax = fmax(dmax, fabs(y[a] - x[a]));
+          x[a] = y[a];
+        }
+        for (int q = 0; q < 18; ++q) {
+          r1[q] = q1[q];
+          r2[q] = q2[q];
+        }
+        D[0] = E[0];
+        D[1] = E[1];
+        D[2] = E[2];
+        f = fy;
+        lam = fmax(lam * 0.1, 1e-12);
+        moved = dmax > 1e-15;
+        break;
+      }
+      lam *= 10.0;
+    }
+    if (!moved) break;
+  }
+  out[0] = sqrt(f);
+  for (int a = 0; a < 4; ++a) out[1 + a] = x[a];
+  for (int c = 0; c < 3; ++c) {
+    out[5 + c] = r1[c];
+    out[8 + c] = r2[c];
+  }
+}
+
+// One thread per final candidate pair: cell centres as the starting point.
+template <typename TP>
+__global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
+                              const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                              const DistCand<TP> *top, int n, const double *dom, double *out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const DistCand<TP> c = top[e];
+  const RegionRec<TP> R1 = reg1[map1[c.slot]], R2 = reg2[map2[c.slot]];
+  const int w1 = nuv1 - 1, w2 = nuv2 - 1;
+  const double du1 = (double(R1.u1) - double(R1.u0)) / nuv1, dv1 = (double(R1.v1) - double(R1.v0)) / nuv1;
+  const double du2 = (double(R2.u1) - double(R2.u0)) / nuv2, dv2 = (double(R2.v1) - double(R2.v0)) / nuv2;
+  double x[4] = {double(R1.u0) + du1 * ((c.i % w1) + 0.5), double(R1.v0) + dv1 * ((c.i / w1) + 0.5),
+                 double(R2.u0) + du2 * ((c.j % w2) + 0.5), double(R2.v0) + dv2 * ((c.j / w2) + 0.5)};
+  double d[8];
+  for (int q = 0; q < 8; ++q) d[q] = dom[q];
+  double o[11];
+  newton_distance(sa, sb, d, x, o);
+  for (int q = 0; q < 11; ++q) out[e * 11 + q] = o[q];
+}
+
+// Minimum-norm Gauss-Newton on S1(u, v) - S2(s, t) = 0 (3 equations, 4
+// unknowns): step = -J^T (J J^T)^-1 D.  out: x, y, z, u, v, s, t, residual.
+__device__ void newton_point(const SurfView<double> &sa, const SurfView<double> &sb, const double dom[8], double x[4],
+                             double out[8]) {
+  double r1[18], r2[18], D[3];
+  for (int it = 0; it < 40; ++it) {
+    point_record(sa, x[0], x[1], r1);
+    point_record(sb, x[2], x[3], r2);
+    for (int c = 0; c < 3; ++c) D[c] = r1[c] - r2[c];
+    const double J[3][4] = {{r1[3], r1[6], -r2[3], -r2[6]},
+                            {r1[4], r1[7], -r2[4], -r2[7]},
+                            {r1[5], r1[8], -r2[5], -r2[8]}};
+    double M[4][4] = {}, y[4] = {D[0], D[1], D[2], 0.0};
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double acc = 0.0;
+        for (int q = 0; q < 4; ++q) acc += J[a][q] * J[b][q];
+        M[a][b] = acc;
+      }
+    if (!solve_small(M, y, 3)) break;
+    double dmax = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const double step = -(J[0][q] * y[0] + J[1][q] * y[1] + J[2][q] * y[2]);
+      const double nx = clampd(x[q] + step, dom[2 * q], dom[2 * q + 1]);
+      dmax = fmax(dmax, fabs(nx - x[q]));
+      x[q] = nx;
+    }
+    if (dmax <= 1e-15) break;
+  }
+  point_record(sa, x[0], x[1], r1);
+  point_record(sb, x[2], x[3], r2);
+  for (int c = 0; c < 3; ++c) {
+    D[c] = r1[c] - r2[c];
+    out[c] = 0.5 * (r1[c] + r2[c]);
+  }
+  for (int q = 0; q < 4; ++q) out[3 + q] = x[q];
+  out[7] = sqrt(dot3(D, D));
+}
+
+template <typename TP>
+__global__ void k_newton_inter(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
+                               const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                               const unsigned long long *keys, long long n, int ij_bits, const double *dom,
+                               double *out) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= n) return;
+  const unsigned long long k = keys[e];
+  const unsigned long long mij = (1ull << ij_bits) - 1ull;
+  const int slot = static_cast<int>(k >> (2 * ij_bits));
+  const int ci = static_cast<int>((k >> ij_bits) & mij), cj = static_cast<int>(k & mij);
+  const RegionRec<TP> R1 = reg1[map1[slot]], R2 = reg2[map2[slot]];
+  const int w1 = nuv1 - 1, w2 = nuv2 - 1;
+  const double du1 = (double(R1.u1) - double(R1.u0)) / nuv1, dv1 = (double(R1.v1) - double(R1.v0)) / nuv1;
+  const double du2 = (double(R2.u1) - double(R2.u0)) / nuv2, dv2 = (double(R2.v1) - double(R2.v0)) / nuv2;
+  double x[4] = {double(R1.u0) + du1 * ((ci % w1) + 0.5), double(R1.v0) + dv1 * ((ci / w1) + 0.5),
+                 double(R2.u0) + du2 * ((cj % w2) + 0.5), double(R2.v0) + dv2 * ((cj / w2) + 0.5)};
+  double d[8];
+  for (int q = 0; q < 8; ++q) d[q] = dom[q];
+  double o[8];
+  newton_point(sa, sb, d, x, o);
+  for (int q = 0; q < 8; ++q) out[e * 8 + q] = o[q];
+}
+
 inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -1792,6 +2006,26 @@ void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, 
   k_dist_verify<<<grid_for(n, 128), 128, 0, st>>>(sa, sb, a, b, map1, map2, cand, n, out);
 }
 
+template <typename TP>
+void launch_newton_dist(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
+                        const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                        const DistCand<TP> *top, int n, const double *dom, double *out, cudaStream_t st) {
+  counted();
+  if (n <= 0) return;
+  k_newton_dist<TP><<<(n + 63) / 64, 64, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, top, n, dom, out);
+}
+
+template <typename TP>
+void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
+                         const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                         const unsigned long long *keys, long long n, int ij_bits, const double *dom, double *out,
+                         cudaStream_t st) {
+  counted();
+  if (n <= 0) return;
+  k_newton_inter<TP><<<static_cast<unsigned>((n + 63) / 64), 64, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2,
+                                                                          keys, n, ij_bits, dom, out);
+}
+
 #define JSI_INSTANTIATE(T)                                                                                        \
   template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t);                         \
   template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t);                 \
@@ -1839,5 +2073,21 @@ void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, 
 
 JSI_INSTANTIATE(float)
 JSI_INSTANTIATE(double)
+
+template void launch_newton_dist<float>(const SurfView<double> &, const SurfView<double> &, const RegionRec<float> *,
+                                        const RegionRec<float> *, const int *, const int *, int, int,
+                                        const DistCand<float> *, int, const double *, double *, cudaStream_t);
+template void launch_newton_dist<double>(const SurfView<double> &, const SurfView<double> &,
+                                         const RegionRec<double> *, const RegionRec<double> *, const int *,
+                                         const int *, int, int, const DistCand<double> *, int, const double *,
+                                         double *, cudaStream_t);
+template void launch_newton_inter<float>(const SurfView<double> &, const SurfView<double> &, const RegionRec<float> *,
+                                         const RegionRec<float> *, const int *, const int *, int, int,
+                                         const unsigned long long *, long long, int, const double *, double *,
+                                         cudaStream_t);
+template void launch_newton_inter<double>(const SurfView<double> &, const SurfView<double> &,
+                                          const RegionRec<double> *, const RegionRec<double> *, const int *,
+                                          const int *, int, int, const unsigned long long *, long long, int,
+                                          const double *, double *, cudaStream_t);
 
 }  // namespace jsi

@@ -60,15 +60,17 @@ class Oracle:
         L.orc_compute_k_f32.restype = _F
         L.orc_compute_k_f64.argtypes = [_P, _I]
         L.orc_compute_k_f64.restype = _D
-        L.orc_dist_query_f32.argtypes = [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P]
+        L.orc_dist_query_f32.argtypes = [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P]
         L.orc_dist_query_f32.restype = _I
-        L.orc_dist_query_f64.argtypes = [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P]
+        L.orc_dist_query_f64.argtypes = [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P]
         L.orc_dist_query_f64.restype = _I
-        qargs = [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _LL, _P, _P, _LL, _P, _P]
+        qargs = [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _LL, _P, _P, _LL, _P, _P, _P, _LL]
         L.orc_inter_query_f32.argtypes = qargs
         L.orc_inter_query_f32.restype = _I
         L.orc_inter_query_f64.argtypes = qargs
         L.orc_inter_query_f64.restype = _I
+        L.orc_newton_distance.argtypes = [_P, _P, _P, _P, _P, _P, _P]
+        L.orc_newton_point.argtypes = [_P, _P, _P, _P, _P, _P, _P]
         L.orc_region_cells_f32.argtypes = [_P, _P, _P, _I, _F, _P, _P]
         L.orc_region_cells_f64.argtypes = [_P, _P, _P, _I, _D, _P, _P]
 
@@ -88,24 +90,28 @@ class Oracle:
         kth = np.zeros(rounds, dtype=dtype)
         npairs = np.zeros(rounds, dtype=np.int32)
         pairs = np.full(rounds * lim * 3, -1, dtype=np.int32)
+        starts = np.zeros(lim * 4, dtype=np.float64)
         conv = _f32 if dtype == np.float32 else _f64
         fn = self.lib.orc_dist_query_f32 if dtype == np.float32 else self.lib.orc_dist_query_f64
         nr = fn(_p(_i32(a.ivec)), _p(_f32(a.data)), _p(conv(rect1)), _p(_i32(b.ivec)), _p(_f32(b.data)),
-                _p(conv(rect2)), nuv0, nuv_refine, k, rounds, _p(kth), _p(npairs), _p(pairs))
+                _p(conv(rect2)), nuv0, nuv_refine, k, rounds, _p(kth), _p(npairs), _p(pairs), _p(starts))
         per_round = [pairs[r * lim * 3:(r * lim + int(npairs[r])) * 3].reshape(-1, 3) for r in range(nr)]
-        return dict(rounds=nr, kth_d2=kth[:nr], npairs=npairs[:nr], pairs=per_round)
+        last = int(npairs[nr - 1]) if nr else 0
+        return dict(rounds=nr, kth_d2=kth[:nr], npairs=npairs[:nr], pairs=per_round,
+                    starts=starts[:last * 4].reshape(-1, 4))
 
     def inter_query(self, a, b, rect1, rect2, nuv0, nuv_refine=16, use_k=1, rounds=6, halve_threshold=512,
-                    min_nuv=4, max_pairs=1 << 26, pair_cap=1 << 22, dtype=np.float32):
+                    min_nuv=4, max_pairs=1 << 26, pair_cap=1 << 22, dtype=np.float32, starts_cap=0):
         counts = np.zeros(rounds, dtype=np.int64)
         pairs = np.zeros(pair_cap * 3, dtype=np.int32)
         written = ctypes.c_longlong(0)
         pads = np.zeros(2, dtype=dtype)
+        starts = np.zeros(starts_cap * 4, dtype=np.float64) if starts_cap else None
         conv = _f32 if dtype == np.float32 else _f64
         fn = self.lib.orc_inter_query_f32 if dtype == np.float32 else self.lib.orc_inter_query_f64
         nr = fn(_p(_i32(a.ivec)), _p(_f32(a.data)), _p(conv(rect1)), _p(_i32(b.ivec)), _p(_f32(b.data)),
                 _p(conv(rect2)), nuv0, nuv_refine, use_k, rounds, halve_threshold, min_nuv, max_pairs,
-                _p(counts), _p(pairs), pair_cap, ctypes.byref(written), _p(pads))
+                _p(counts), _p(pairs), pair_cap, ctypes.byref(written), _p(pads), _p(starts), starts_cap)
         if nr < 0:
             raise RuntimeError("oracle intersection exceeded max_pairs")
         per_round = []
@@ -117,7 +123,23 @@ class Oracle:
             else:
                 per_round.append(None)
             off += c
-        return dict(rounds=nr, counts=counts[:nr], pairs=per_round, pads=pads)
+        out = dict(rounds=nr, counts=counts[:nr], pairs=per_round, pads=pads)
+        if starts_cap:
+            last = min(int(counts[nr - 1]), starts_cap) if nr else 0
+            out["starts"] = starts[:last * 4].reshape(-1, 4)
+        return out
+
+    def newton_distance(self, a, b, dom, x0):
+        out = np.zeros(11, np.float64)
+        self.lib.orc_newton_distance(_p(_i32(a.ivec)), _p(_f32(a.data)), _p(_i32(b.ivec)), _p(_f32(b.data)),
+                                     _p(_f64(dom)), _p(_f64(x0)), _p(out))
+        return out
+
+    def newton_point(self, a, b, dom, x0):
+        out = np.zeros(8, np.float64)
+        self.lib.orc_newton_point(_p(_i32(a.ivec)), _p(_f32(a.data)), _p(_i32(b.ivec)), _p(_f32(b.data)),
+                                  _p(_f64(dom)), _p(_f64(x0)), _p(out))
+        return out
 
     def region_cells(self, surf, rect, nuv, padding=0.0, radii=True, dtype=np.float32):
         n = (nuv - 1) * (nuv - 1) * 3

@@ -434,9 +434,23 @@ Region<T> root_region(const T *rect, int nuv, int side) {
 // minimum_distance round loop, distance_analysis.cu:356-506, with pair
 // preservation (JSI_CAD_PRESERVE_PAIR_RELATION=1) and duplicate-region reuse
 // keyed by (slot, cell) per side (:426-465).
+// Start parameters (u, v, s, t) of a final pair for the Newton refinement:
+// the centres of its two cells, in double.
+template <typename T>
+void cell_start(const Region<T> &r1, int i, const Region<T> &r2, int j, double *x) {
+  const int w1 = r1.nuv - 1, w2 = r2.nuv - 1;
+  const double du1 = (double(r1.u1) - double(r1.u0)) / r1.nuv, dv1 = (double(r1.v1) - double(r1.v0)) / r1.nuv;
+  const double du2 = (double(r2.u1) - double(r2.u0)) / r2.nuv, dv2 = (double(r2.v1) - double(r2.v0)) / r2.nuv;
+  x[0] = double(r1.u0) + du1 * ((i % w1) + 0.5);
+  x[1] = double(r1.v0) + dv1 * ((i / w1) + 0.5);
+  x[2] = double(r2.u0) + du2 * ((j % w2) + 0.5);
+  x[3] = double(r2.v0) + dv2 * ((j / w2) + 0.5);
+}
+
 template <typename T>
 int dist_query(const int *ivec1, const float *data1, const T *rect1, const int *ivec2, const float *data2,
-               const T *rect2, int nuv0, int nuv_refine, int k, int rounds, T *kth_d2, int *npairs, int *pairs_out) {
+               const T *rect2, int nuv0, int nuv_refine, int k, int rounds, T *kth_d2, int *npairs, int *pairs_out,
+               double *starts) {
   const Surface<T> sa = load_surface<T>(ivec1, data1);
   const Surface<T> sb = load_surface<T>(ivec2, data2);
   Spans<T> spans;
@@ -463,7 +477,12 @@ int dist_query(const int *ivec1, const float *data1, const T *rect1, const int *
       pairs_out[(static_cast<size_t>(round - 1) * limit + q) * 3 + 1] = best[q].i;
       pairs_out[(static_cast<size_t>(round - 1) * limit + q) * 3 + 2] = best[q].j;
     }
-    if (best.empty() || round == rounds) break;
+    if (best.empty() || round == rounds) {
+      if (starts)
+        for (size_t q = 0; q < best.size(); ++q)
+          cell_start(*ch1[best[q].slot], best[q].i, *ch2[best[q].slot], best[q].j, starts + 4 * q);
+      break;
+    }
     std::vector<Region<T>> next1, next2;
     std::unordered_map<uint64_t, size_t> idx1, idx2;
     std::vector<size_t> slot1, slot2;
@@ -497,7 +516,7 @@ template <typename T>
 int inter_query(const int *ivec1, const float *data1, const T *rect1, const int *ivec2, const float *data2,
                 const T *rect2, int nuv0, int nuv_refine, int use_k, int rounds, int halve_threshold, int min_nuv,
                 long long max_pairs, long long *counts, int *pairs_out, long long pair_cap, long long *pairs_written,
-                T *pads) {
+                T *pads, double *starts, long long starts_cap) {
   const Surface<T> sa = load_surface<T>(ivec1, data1);
   const Surface<T> sb = load_surface<T>(ivec2, data2);
   Spans<T> spans;
@@ -545,8 +564,12 @@ int inter_query(const int *ivec1, const float *data1, const T *rect1, const int 
       }
       ++written;
     }
-    if (round == rounds) break;
-    if (pairs.empty()) break;
+    if (round == rounds || pairs.empty()) {
+      if (starts)
+        for (size_t q = 0; q < pairs.size() && static_cast<long long>(q) < starts_cap; ++q)
+          cell_start(*ch1[pairs[q].slot], pairs[q].i, *ch2[pairs[q].slot], pairs[q].j, starts + 4 * q);
+      break;
+    }
     if (static_cast<long long>(pairs.size()) > halve_threshold && nuv > min_nuv) nuv /= 2;
     std::vector<Region<T>> next1, next2;
     std::unordered_map<uint64_t, size_t> idx1, idx2;
@@ -592,9 +615,168 @@ void region_cells(const int *ivec, const float *data, const T *rect, int nuv, T 
   if (radii) std::memcpy(radii, r.data(), r.size() * sizeof(T));
 }
 
+// ---------------------------------------------------------------------------
+// FP64 Newton refinement (no counterpart in the reference: it stops at cell
+// centres).  Levenberg-Marquardt on |S1(u,v) - S2(s,t)|^2 and minimum-norm
+// Gauss-Newton on S1 - S2 = 0, both inside the query rectangles.
+// ---------------------------------------------------------------------------
+
+void record_at(const Surface<double> &s, double u, double v, double r[18]) { eval_point(s, u, v, r); }
+
+double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+double clamp(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+// Gaussian elimination with partial pivoting on an n x n system (n <= 4).
+bool gauss_solve(double M[4][4], double r[4], int n) {
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    for (int q = c + 1; q < n; ++q)
+      if (std::fabs(M[q][c]) > std::fabs(M[piv][c])) piv = q;
+    if (!(std::fabs(M[piv][c]) > 0.0)) return false;
+    if (piv != c) {
+      for (int q = 0; q < n; ++q) std::swap(M[c][q], M[piv][q]);
+      std::swap(r[c], r[piv]);
+    }
+    for (int q = c + 1; q < n; ++q) {
+      const double f = M[q][c] / M[c][c];
+      for (int w = c; w < n; ++w) M[q][w] -= f * M[c][w];
+      r[q] -= f * r[c];
+    }
+  }
+  for (int c = n - 1; c >= 0; --c) {
+    double acc = r[c];
+    for (int q = c + 1; q < n; ++q) acc -= M[c][q] * r[q];
+    r[c] = acc / M[c][c];
+  }
+  return true;
+}
+
+void lm_distance(const Surface<double> &sa, const Surface<double> &sb, const double dom[8], double x[4],
+                 double out[11]) {
+  double r1[18], r2[18];
+  record_at(sa, x[0], x[1], r1);
+  record_at(sb, x[2], x[3], r2);
+  double D[3] = {r1[0] - r2[0], r1[1] - r2[1], r1[2] - r2[2]};
+  double f = dot3(D, D);
+  double lam = 1e-6;
+  for (int it = 0; it < 60; ++it) {
+    // half gradient and half Hessian of f (first and second derivatives of both patches)
+    const double g[4] = {dot3(D, r1 + 3), dot3(D, r1 + 6), -dot3(D, r2 + 3), -dot3(D, r2 + 6)};
+    double H[4][4];
+    H[0][0] = dot3(r1 + 3, r1 + 3) + dot3(D, r1 + 9);
+    H[0][1] = dot3(r1 + 3, r1 + 6) + dot3(D, r1 + 12);
+    H[1][1] = dot3(r1 + 6, r1 + 6) + dot3(D, r1 + 15);
+    H[0][2] = -dot3(r1 + 3, r2 + 3);
+    H[0][3] = -dot3(r1 + 3, r2 + 6);
+    H[1][2] = -dot3(r1 + 6, r2 + 3);
+    H[1][3] = -dot3(r1 + 6, r2 + 6);
+    H[2][2] = dot3(r2 + 3, r2 + 3) - dot3(D, r2 + 9);
+    H[2][3] = dot3(r2 + 3, r2 + 6) - dot3(D, r2 + 12);
+    H[3][3] = dot3(r2 + 6, r2 + 6) - dot3(D, r2 + 15);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < a; ++b) H[a][b] = H[b][a];
+    bool moved = false;
+    while (lam < 1e16) {
+      double M[4][4], step[4];
+      for (int a = 0; a < 4; ++a) {
+        for (int b = 0; b < 4; ++b) M[a][b] = H[a][b];
+        M[a][a] += lam * (std::fabs(H[a][a]) + 1e-30);
+        step[a] = -g[a];
+      }
+      if (!gauss_solve(M, step, 4)) {
+        lam *= 10.0;
+        continue;
+      }
+      double y[4];
+      for (int a = 0; a < 4; ++a) y[a] = clamp(x[a] + step[a], dom[2 * a], dom[2 * a + 1]);
+      double q1[18], q2[18];
+      record_at(sa, y[0], y[1], q1);
+      record_at(sb, y[2], y[3], q2);
+      const double E[3] = {q1[0] - q2[0], q1[1] - q2[1], q1[2] - q2[2]};
+      const double fy = dot3(E, E);
+      if (fy < f) {
+        double dmax = 0.0;
+        for (int a = 0; a < 4; ++a) {
+          dmax = std::max(dmax, std::fabs(y[a] - x[a]));
+          x[a] = y[a];
+        }
+        std::memcpy(r1, q1, sizeof(r1));
+        std::memcpy(r2, q2, sizeof(r2));
+        std::memcpy(D, E, sizeof(D));
+        f = fy;
+        lam = std::max(lam * 0.1, 1e-12);
+        moved = dmax > 1e-15;
+        break;
+      }
+      lam *= 10.0;
+    }
+    if (!moved) break;
+  }
+  out[0] = std::sqrt(f);
+  for (int a = 0; a < 4; ++a) out[1 + a] = x[a];
+  for (int c = 0; c < 3; ++c) {
+    out[5 + c] = r1[c];
+    out[8 + c] = r2[c];
+  }
+}
+
+void gn_point(const Surface<double> &sa, const Surface<double> &sb, const double dom[8], double x[4],
+              double out[8]) {
+  double r1[18], r2[18], D[3];
+  for (int it = 0; it < 40; ++it) {
+    record_at(sa, x[0], x[1], r1);
+    record_at(sb, x[2], x[3], r2);
+    for (int c = 0; c < 3; ++c) D[c] = r1[c] - r2[c];
+    // J = [S1u, S1v, -S2s, -S2t] (3 x 4); step = -J^T (J J^T)^-1 D
+    const double J[3][4] = {{r1[3], r1[6], -r2[3], -r2[6]},
+                            {r1[4], r1[7], -r2[4], -r2[7]},
+                            {r1[5], r1[8], -r2[5], -r2[8]}};
+    double M[4][4] = {}, y[4] = {D[0], D[1], D[2], 0.0};
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double acc = 0.0;
+        for (int q = 0; q < 4; ++q) acc += J[a][q] * J[b][q];
+        M[a][b] = acc;
+      }
+    if (!gauss_solve(M, y, 3)) break;
+    double dmax = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const double step = -(J[0][q] * y[0] + J[1][q] * y[1] + J[2][q] * y[2]);
+      const double nx = clamp(x[q] + step, dom[2 * q], dom[2 * q + 1]);
+      dmax = std::max(dmax, std::fabs(nx - x[q]));
+      x[q] = nx;
+    }
+    if (dmax <= 1e-15) break;
+  }
+  record_at(sa, x[0], x[1], r1);
+  record_at(sb, x[2], x[3], r2);
+  for (int c = 0; c < 3; ++c) {
+    D[c] = r1[c] - r2[c];
+    out[c] = 0.5 * (r1[c] + r2[c]);
+  }
+  for (int q = 0; q < 4; ++q) out[3 + q] = x[q];
+  out[7] = std::sqrt(dot3(D, D));
+}
+
 }  // namespace
 
 extern "C" {
+
+void orc_newton_distance(const int *ivec1, const float *data1, const int *ivec2, const float *data2,
+                         const double *dom, const double *x0, double *out) {
+  const Surface<double> sa = load_surface<double>(ivec1, data1), sb = load_surface<double>(ivec2, data2);
+  double x[4] = {x0[0], x0[1], x0[2], x0[3]};
+  lm_distance(sa, sb, dom, x, out);
+}
+
+void orc_newton_point(const int *ivec1, const float *data1, const int *ivec2, const float *data2, const double *dom,
+                      const double *x0, double *out) {
+  const Surface<double> sa = load_surface<double>(ivec1, data1), sb = load_surface<double>(ivec2, data2);
+  double x[4] = {x0[0], x0[1], x0[2], x0[3]};
+  gn_point(sa, sb, dom, x, out);
+}
+
 
 void orc_eval_grid_f32(const int *ivec, const float *data, float ustep, float vstep, float ustart, float vstart,
                        int nuv, float *out) {
@@ -611,32 +793,36 @@ double orc_compute_k_f64(const double *records, int nuv) { return compute_k(reco
 
 int orc_dist_query_f32(const int *ivec1, const float *data1, const float *rect1, const int *ivec2,
                        const float *data2, const float *rect2, int nuv0, int nuv_refine, int k, int rounds,
-                       float *kth_d2, int *npairs, int *pairs) {
+                       float *kth_d2, int *npairs, int *pairs, double *starts) {
   return dist_query<float>(ivec1, data1, rect1, ivec2, data2, rect2, nuv0, nuv_refine, k, rounds, kth_d2, npairs,
-                           pairs);
+                           pairs, starts);
 }
 
 int orc_dist_query_f64(const int *ivec1, const float *data1, const double *rect1, const int *ivec2,
                        const float *data2, const double *rect2, int nuv0, int nuv_refine, int k, int rounds,
-                       double *kth_d2, int *npairs, int *pairs) {
+                       double *kth_d2, int *npairs, int *pairs, double *starts) {
   return dist_query<double>(ivec1, data1, rect1, ivec2, data2, rect2, nuv0, nuv_refine, k, rounds, kth_d2, npairs,
-                            pairs);
+                            pairs, starts);
 }
 
 int orc_inter_query_f32(const int *ivec1, const float *data1, const float *rect1, const int *ivec2,
                         const float *data2, const float *rect2, int nuv0, int nuv_refine, int use_k, int rounds,
                         int halve_threshold, int min_nuv, long long max_pairs, long long *counts, int *pairs,
-                        long long pair_cap, long long *pairs_written, float *pads) {
+                        long long pair_cap, long long *pairs_written, float *pads, double *starts,
+                        long long starts_cap) {
   return inter_query<float>(ivec1, data1, rect1, ivec2, data2, rect2, nuv0, nuv_refine, use_k, rounds,
-                            halve_threshold, min_nuv, max_pairs, counts, pairs, pair_cap, pairs_written, pads);
+                            halve_threshold, min_nuv, max_pairs, counts, pairs, pair_cap, pairs_written, pads, starts,
+                            starts_cap);
 }
 
 int orc_inter_query_f64(const int *ivec1, const float *data1, const double *rect1, const int *ivec2,
                         const float *data2, const double *rect2, int nuv0, int nuv_refine, int use_k, int rounds,
                         int halve_threshold, int min_nuv, long long max_pairs, long long *counts, int *pairs,
-                        long long pair_cap, long long *pairs_written, double *pads) {
+                        long long pair_cap, long long *pairs_written, double *pads, double *starts,
+                        long long starts_cap) {
   return inter_query<double>(ivec1, data1, rect1, ivec2, data2, rect2, nuv0, nuv_refine, use_k, rounds,
-                             halve_threshold, min_nuv, max_pairs, counts, pairs, pair_cap, pairs_written, pads);
+                             halve_threshold, min_nuv, max_pairs, counts, pairs, pair_cap, pairs_written, pads, starts,
+                             starts_cap);
 }
 
 void orc_region_cells_f32(const int *ivec, const float *data, const float *rect, int nuv, float padding,
