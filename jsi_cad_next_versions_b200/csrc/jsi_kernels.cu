@@ -1133,8 +1133,72 @@ __global__ void __launch_bounds__(1024) k_dist_select(const DistCand<T> *cand, u
     __syncthreads();
     cnt = s_count;
     if (cnt > kSelectCap) {
-      if (threadIdx.x == 0) stats->status = -4;
-      return;
+      // Too many exact ties at the k-th d2: among the tied entries, radix
+      // select the needed number by the (slot, i, j) key, most significant
+      // byte first, so the kept set is exactly the first k of the order.
+      if (threadIdx.x == 0) s_count = 0;
+      __syncthreads();
+      for (int e = threadIdx.x; e < m; e += blockDim.x)
+        if (ordered_bits(cand[e].d2) < kth_bits) atomicAdd(&s_count, 1);
+      __syncthreads();
+      const int below = s_count;
+      __shared__ unsigned s_key[3], s_kmask[3];
+      if (threadIdx.x == 0) {
+        s_need = k - below;
+        for (int w = 0; w < 3; ++w) s_key[w] = s_kmask[w] = 0u;
+      }
+      __syncthreads();
+      for (int byte = 11; byte >= 0; --byte) {
+        const int word = 2 - byte / 4, shift = (byte % 4) * 8;  // word 0 = slot, 1 = i, 2 = j
+        for (int q = threadIdx.x; q < 256; q += blockDim.x) hist[q] = 0;
+        __syncthreads();
+        const unsigned k0 = s_key[0], k1 = s_key[1], k2 = s_key[2];
+        const unsigned m0 = s_kmask[0], m1 = s_kmask[1], m2 = s_kmask[2];
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {
+          const DistCand<T> c = cand[e];
+          if (ordered_bits(c.d2) != kth_bits) continue;
+          const unsigned w0 = static_cast<unsigned>(c.slot), w1 = static_cast<unsigned>(c.i),
+                         w2 = static_cast<unsigned>(c.j);
+          if ((w0 & m0) != k0 || (w1 & m1) != k1 || (w2 & m2) != k2) continue;
+          const unsigned wv = word == 0 ? w0 : (word == 1 ? w1 : w2);
+          atomicAdd(&hist[(wv >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          int need = s_need, dgt = 0;
+          for (; dgt < 256; ++dgt) {
+            if (static_cast<int>(hist[dgt]) >= need) break;
+            need -= hist[dgt];
+          }
+          s_need = need;
+          s_key[word] |= static_cast<unsigned>(dgt) << shift;
+          s_kmask[word] |= 255u << shift;
+        }
+        __syncthreads();
+      }
+      const unsigned K0 = s_key[0], K1 = s_key[1], K2 = s_key[2];
+      if (threadIdx.x == 0) s_count = 0;
+      __syncthreads();
+      for (int e = threadIdx.x; e < m; e += blockDim.x) {
+        const DistCand<T> c = cand[e];
+        const unsigned long long b = ordered_bits(c.d2);
+        bool take = b < kth_bits;
+        if (b == kth_bits) {
+          const unsigned w0 = static_cast<unsigned>(c.slot), w1 = static_cast<unsigned>(c.i),
+                         w2 = static_cast<unsigned>(c.j);
+          take = w0 < K0 || (w0 == K0 && (w1 < K1 || (w1 == K1 && w2 <= K2)));
+        }
+        if (take) {
+          const int pos = atomicAdd(&s_count, 1);
+          if (pos < kSelectCap) buf[pos] = c;
+        }
+      }
+      __syncthreads();
+      cnt = s_count;
+      if (cnt > kSelectCap) {
+        if (threadIdx.x == 0) stats->status = -4;
+        return;
+      }
     }
   }
   int n2 = 1;

@@ -315,3 +315,21 @@ def test_distance_4x_scaled_nuv2048(gpu_ctx):
     assert abs(v5.distance - r64.distance) <= 1e-5 * r64.distance
     # round 1 examined a tiny fraction of the (2047^2)^2 pairs
     assert r64.pair_tests[0] < 1e9
+
+
+@pytest.mark.parametrize("precision", ["v5_fp32", "fp64", "fp32_screen"])
+@pytest.mark.parametrize("k", [1, 8, 300])
+def test_distance_heavy_exact_ties(gpu_ctx, orc, precision, k):
+    """Parallel planes on regular grids: thousands of cell pairs share the
+    k-th squared distance exactly; the kept pairs are the first k under the
+    reference's (d2, slot, i, j) order."""
+    X, Y = np.meshgrid(np.linspace(0, 1, 6), np.linspace(0, 1, 5))
+    P0 = synth.make_surface(np.stack([X, Y, 0 * X], -1), 3, 3)
+    X2, Y2 = np.meshgrid(np.linspace(0, 1, 7), np.linspace(0, 1, 6))
+    P1 = synth.make_surface(np.stack([0.9 * X2 + 0.05, 0.8 * Y2 + 0.1, 0 * X2 + 0.5], -1), 3, 2)
+    res = _dist_both(gpu_ctx, orc, P0, P1, 20, k, rounds=2, precision=precision)
+    dt = np.float32 if precision == "v5_fp32" else np.float64
+    o = orc.dist_query(P0, P1, rect32(P0).astype(dt), rect32(P1).astype(dt), 20, 16, k, 2, dtype=dt)
+    for r in range(2):
+        assert np.array_equal(res.pairs[r], o["pairs"][r])
+    assert np.array_equal(res.kth_d2.astype(dt), o["kth_d2"])
