@@ -41,7 +41,9 @@ typedef enum {
  *  FP32_SCREEN  - FP32 evaluation / boxes / screening with every box widened
  *                 by a rigorous rounding-error bound, FP64 knot spans, basis
  *                 and rational division, FP64 re-check of the screened
- *                 candidates; results equal the FP64 form's. */
+ *                 candidates; results equal the FP64 form's.  The
+ *                 intersection query has no FP32 stage (each surviving pair
+ *                 needs its exact FP64 boxes) and runs as FP64. */
 typedef enum { JSI_PREC_V5_FP32 = 0, JSI_PREC_FP64 = 1, JSI_PREC_FP32_SCREEN = 2 } jsi_precision;
 
 typedef struct jsi_context jsi_context;

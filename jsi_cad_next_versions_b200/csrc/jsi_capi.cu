@@ -1031,7 +1031,7 @@ void validate_inter(jsi_inter_params &p, const jsi_task *a, const jsi_task *b) {
   if (p.rounds < 1 || p.rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "rounds = %d", p.rounds);
   if (p.nuv_refine < 2 || p.nuv_refine > 4096) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
   if (p.min_nuv < 2) fail(JSI_ERR_INVALID, "min_nuv = %d", p.min_nuv);
-  check_precision(p.precision, false);
+  check_precision(p.precision, true);
   check_task<float>(a);
   check_task<float>(b);
 }
@@ -1073,6 +1073,10 @@ void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_
   JSI_CUDA(cudaSetDevice(L->device));
   L->arena.reset();
   JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
+  // The intersection query has no FP32 stage: every overlapping pair needs its
+  // exact FP64 boxes (and the FP64 curvature padding of its regions), which
+  // costs what the FP64 evaluation it would replace costs.  FP32_SCREEN
+  // therefore runs the FP64 form.
   if (p.precision == JSI_PREC_V5_FP32)
     run_intersection<float>(L, a, b, &p, out);
   else

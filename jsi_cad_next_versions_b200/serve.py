@@ -1,0 +1,261 @@
+"""Serving loop over the library's worker lanes.
+
+* ``SurfaceCache``  keeps surfaces resident on the device, addressed by id.
+* ``ServingLoop``   takes a stream of timestamped queries (surface ids, kind,
+                    first-round nuv), admits each in arrival order as soon as
+                    its memory estimate fits the budget beside the queries in
+                    flight and a slot is free, and hands it to the C++ worker
+                    pool (``jsi_submit_*``): queries that arrive while others
+                    run on the GPU start as lanes free up, and their kernels
+                    overlap on the device (continuous batching).  Latency is
+                    arrival to completion.
+* ``poisson_queries`` builds a seeded arrival stream.
+
+    python -m jsi_cad_next_versions_b200.serve --surfaces 10000 --queries 4000 \\
+        --rates 1000,10000,100000 --forms fp32_screen,fp64
+
+prints one JSON line per (form, rate): throughput, p50/p99 latency, admitted
+memory peak.  The reference has no serving layer (its API runs one query at a
+time and keeps mutable file statics, intersection.cu:36-39).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import synth
+
+
+@dataclass
+class Query:
+    kind: str          # "distance" or "intersection"
+    a: int             # surface ids in the cache
+    b: int
+    nuv0: int
+    arrival: float     # seconds from the start of the stream
+    result: object = None
+    latency: float = float("nan")
+    status: str = "pending"
+
+
+def query_bytes(kind: str, nuv0: int) -> int:
+    """Device memory estimate of one query (arena high-water mark): round-1
+    samples, cells and tile lists of both sides in FP64 plus refinement rounds;
+    intersection queries also hold per-round pair lists."""
+    base = 2 * nuv0 * nuv0 * 32 * 3 + (8 << 20)
+    return base if kind == "distance" else 4 * base + (64 << 20)
+
+
+class SurfaceCache:
+    """Surfaces resident on the device, addressed by cache index."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.ids: list[int] = []
+        self.rects: list[np.ndarray] = []
+
+    def add(self, surf) -> int:
+        self.ids.append(self.ctx.upload(surf))
+        self.rects.append(np.array(surf.rect(), np.float32))
+        return len(self.ids) - 1
+
+    def __len__(self):
+        return len(self.ids)
+
+    def task(self, idx: int, nuv: int, side: int):
+        return self.ctx.task(self.ids[idx], self.rects[idx], nuv, side)
+
+    def release(self):
+        for sid in self.ids:
+            self.ctx.release(sid)
+        self.ids.clear()
+        self.rects.clear()
+
+
+def poisson_queries(n: int, rate: float, n_surfaces: int, seed: int = 11, nuv_lo: int = 64, nuv_hi: int = 512,
+                    distance_share: float = 0.5) -> list[Query]:
+    """Seeded Poisson arrivals at `rate` queries/s over random surface pairs."""
+    rng = synth.SplitMix64(seed)
+    t = 0.0
+    out = []
+    for _ in range(n):
+        t += -math.log(1.0 - rng.uniform()) / rate
+        a = rng.randint(0, n_surfaces - 1)
+        b = rng.randint(0, n_surfaces - 1)
+        if b == a:
+            b = (a + 1) % n_surfaces
+        kind = "distance" if rng.uniform() < distance_share else "intersection"
+        out.append(Query(kind, a, b, rng.randint(nuv_lo, nuv_hi), t))
+    return out
+
+
+@dataclass
+class ServeStats:
+    queries: int
+    completed: int
+    failed: int
+    wall_s: float
+    throughput: float
+    p50_ms: float
+    p99_ms: float
+    peak_admitted_bytes: int
+    peak_inflight: int
+    latencies_ms: list = field(default_factory=list)
+
+
+class ServingLoop:
+    """Admission by memory budget + continuous batching over worker lanes."""
+
+    def __init__(self, ctx, cache: SurfaceCache, *, lanes: int = 8, budget_bytes: int = 120 << 30,
+                 max_inflight: int | None = None, precision: str = "fp32_screen", k: int = 8,
+                 inter_rounds: int = 6, inter_precision: str | None = None, trace: bool = False):
+        self.ctx = ctx
+        self.cache = cache
+        self.lanes = lanes
+        self.budget = budget_bytes
+        self.max_inflight = max_inflight or 2 * lanes
+        self.precision = precision
+        # The intersection query has no FP32 stage: the
+        # screen form runs it in FP64.
+        self.inter_precision = inter_precision or ("fp64" if precision == "fp32_screen" else precision)
+        self.k = k
+        self.inter_rounds = inter_rounds
+        self.trace = trace
+
+    def _submit(self, q: Query) -> int:
+        ta = self.cache.task(q.a, q.nuv0, 1)
+        tb = self.cache.task(q.b, q.nuv0, 2)
+        if q.kind == "distance":
+            return self.ctx.submit_distance(ta, tb, k=self.k, precision=self.precision, trace=self.trace)
+        return self.ctx.submit_intersect(ta, tb, rounds=self.inter_rounds, precision=self.inter_precision,
+                                         trace=self.trace)
+
+    def run(self, queries: list[Query], *, poll_ms: int = 1) -> ServeStats:
+        self.ctx.workers(self.lanes)
+        pending = deque(queries)
+        inflight: dict[int, tuple[Query, int]] = {}
+        used = 0
+        peak_used = 0
+        peak_inflight = 0
+        t0 = time.perf_counter()
+        done = 0
+        while pending or inflight:
+            now = time.perf_counter() - t0
+            # admit in arrival order: memory budget and free slots permitting
+            while pending and pending[0].arrival <= now and len(inflight) < self.max_inflight:
+                q = pending[0]
+                need = query_bytes(q.kind, q.nuv0)
+                if used + need > self.budget and inflight:
+                    break
+                pending.popleft()
+                try:
+                    t = self._submit(q)
+                except Exception as exc:  # rejected at submission
+                    q.status = f"rejected: {exc}"
+                    done += 1
+                    continue
+                inflight[t] = (q, need)
+                used += need
+                peak_used = max(peak_used, used)
+                peak_inflight = max(peak_inflight, len(inflight))
+            progressed = False
+            for t in list(inflight):
+                q, need = inflight[t]
+                try:
+                    r = self.ctx.wait(t, 0)
+                except Exception as exc:
+                    r = exc
+                if r is None:
+                    continue
+                progressed = True
+                del inflight[t]
+                used -= need
+                q.latency = time.perf_counter() - t0 - q.arrival
+                if isinstance(r, Exception):
+                    q.status = f"failed: {r}"
+                else:
+                    q.result = r
+                    q.status = "ok"
+                done += 1
+            if not progressed:
+                if inflight:
+                    oldest = next(iter(inflight))
+                    r = None
+                    try:
+                        r = self.ctx.wait(oldest, poll_ms)
+                    except Exception as exc:
+                        r = exc
+                    if r is not None:
+                        q, need = inflight.pop(oldest)
+                        used -= need
+                        q.latency = time.perf_counter() - t0 - q.arrival
+                        if isinstance(r, Exception):
+                            q.status = f"failed: {r}"
+                        else:
+                            q.result = r
+                            q.status = "ok"
+                        done += 1
+                elif pending:
+                    time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.001)))
+        wall = time.perf_counter() - t0
+        self.ctx.workers(0)
+        lat = sorted(q.latency * 1e3 for q in queries if q.status == "ok")
+        ok = len(lat)
+
+        def pct(p):
+            return lat[min(len(lat) - 1, int(p * len(lat)))] if lat else float("nan")
+        return ServeStats(queries=len(queries), completed=ok, failed=len(queries) - ok, wall_s=wall,
+                          throughput=ok / wall if wall > 0 else 0.0, p50_ms=pct(0.5), p99_ms=pct(0.99),
+                          peak_admitted_bytes=peak_used, peak_inflight=peak_inflight, latencies_ms=lat)
+
+
+def build_cache(ctx, n: int, seed: int = 7) -> SurfaceCache:
+    """n resident surfaces from the mixed-batch distribution (degrees 2..5,
+    nets 4..64 log-uniform, 30% rational, random-phase height fields)."""
+    rng = synth.SplitMix64(seed)
+    cache = SurfaceCache(ctx)
+    for q in range(n):
+        cache.add(synth.random_surface(rng, name=f"cache{q}"))
+    return cache
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--surfaces", type=int, default=10000)
+    ap.add_argument("--queries", type=int, default=2000)
+    ap.add_argument("--rates", default="1000,10000,100000")
+    ap.add_argument("--forms", default="fp32_screen,fp64")
+    ap.add_argument("--lanes", type=int, default=16)
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--nuv-lo", type=int, default=64)
+    ap.add_argument("--nuv-hi", type=int, default=512)
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+    from .api import Context
+    with Context(args.device) as ctx:
+        t = time.perf_counter()
+        cache = build_cache(ctx, args.surfaces)
+        load_s = time.perf_counter() - t
+        for form in args.forms.split(","):
+            for rate in [float(x) for x in args.rates.split(",")]:
+                qs = poisson_queries(args.queries, rate, len(cache), nuv_lo=args.nuv_lo, nuv_hi=args.nuv_hi)
+                loop = ServingLoop(ctx, cache, lanes=args.lanes, budget_bytes=int(args.budget_gb * (1 << 30)),
+                                   precision=form)
+                st = loop.run(qs)
+                print(json.dumps({
+                    "form": form, "offered_rate": rate, "queries": st.queries, "completed": st.completed,
+                    "failed": st.failed, "throughput_qps": st.throughput, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                    "peak_admitted_gb": st.peak_admitted_bytes / (1 << 30), "peak_inflight": st.peak_inflight,
+                    "lanes": args.lanes, "resident_surfaces": len(cache), "resident_mb": ctx.resident_bytes() / 2**20,
+                    "cache_load_s": load_s, "nuv0_range": [args.nuv_lo, args.nuv_hi]}), flush=True)
+        cache.release()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,126 @@
+"""Serving loop: admission by memory budget and continuous batching.
+
+CPU tests drive the loop with a fake context (no GPU): admission order,
+budget and slot limits, failures.  The GPU test serves a Poisson stream of
+mixed distance / intersection queries and checks that every result equals the
+same query run alone."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+from jsi_cad_next_versions_b200 import serve
+
+
+class FakeCtx:
+    """Stands in for Context: every query 'runs' for a fixed time after
+    submission; wait() returns a marker once that time has passed."""
+
+    def __init__(self, run_s=0.002, fail_every=0):
+        self.run_s = run_s
+        self.fail_every = fail_every
+        self.n = 0
+        self.jobs = {}
+        self.lanes = 0
+        self.order = []
+
+    def workers(self, n, lane_bytes=0):
+        self.lanes = n
+
+    def task(self, sid, rect, nuv, side):
+        return (sid, nuv, side)
+
+    def _submit(self, ta, tb):
+        self.n += 1
+        self.jobs[self.n] = time.perf_counter() + self.run_s
+        self.order.append((ta, tb))
+        return self.n
+
+    def submit_distance(self, ta, tb, **kw):
+        return self._submit(ta, tb)
+
+    def submit_intersect(self, ta, tb, **kw):
+        return self._submit(ta, tb)
+
+    def wait(self, t, timeout_ms=-1):
+        end = self.jobs[t]
+        now = time.perf_counter()
+        if now < end:
+            if timeout_ms == 0:
+                return None
+            time.sleep(min(end - now, timeout_ms / 1e3 if timeout_ms > 0 else end - now))
+            if time.perf_counter() < end:
+                return None
+        del self.jobs[t]
+        if self.fail_every and t % self.fail_every == 0:
+            raise RuntimeError("JSI_ERR_NOMEM: arena budget exhausted")
+        return ("done", t)
+
+
+class FakeCache:
+    def __init__(self, n):
+        self.n = n
+
+    def __len__(self):
+        return self.n
+
+    def task(self, idx, nuv, side):
+        return (idx, nuv, side)
+
+
+def test_admission_respects_budget_and_order():
+    qs = serve.poisson_queries(200, rate=50000.0, n_surfaces=30, seed=3, nuv_lo=64, nuv_hi=128)
+    budget = 3 * serve.query_bytes("intersection", 128)
+    ctx = FakeCtx(run_s=0.001)
+    loop = serve.ServingLoop(ctx, FakeCache(30), lanes=4, budget_bytes=budget, max_inflight=6)
+    st = loop.run(qs)
+    assert st.completed == 200 and st.failed == 0
+    assert st.peak_admitted_bytes <= budget
+    assert st.peak_inflight <= 6
+    # admitted in arrival order
+    assert [o[0][0] for o in ctx.order] == [q.a for q in qs]
+    assert all(q.latency >= 0 for q in qs)
+    assert st.p50_ms <= st.p99_ms
+
+
+def test_failures_are_reported_not_raised():
+    qs = serve.poisson_queries(40, rate=1e5, n_surfaces=10, seed=4)
+    st = serve.ServingLoop(FakeCtx(run_s=0.0005, fail_every=5), FakeCache(10), lanes=2).run(qs)
+    assert st.failed == 8 and st.completed == 32
+    assert sum(q.status.startswith("failed") for q in qs) == 8
+
+
+def test_poisson_stream_is_seeded():
+    a = serve.poisson_queries(50, 1000.0, 20, seed=9)
+    b = serve.poisson_queries(50, 1000.0, 20, seed=9)
+    assert [(q.kind, q.a, q.b, q.nuv0, q.arrival) for q in a] == [(q.kind, q.a, q.b, q.nuv0, q.arrival) for q in b]
+    gaps = np.diff([q.arrival for q in a])
+    assert (gaps > 0).all() and abs(gaps.mean() - 1e-3) < 5e-4
+
+
+@pytest.mark.gpu
+def test_served_results_equal_results_alone():
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        cache = serve.build_cache(ctx, 40, seed=21)
+        qs = serve.poisson_queries(120, rate=5000.0, n_surfaces=len(cache), seed=22, nuv_lo=24, nuv_hi=64)
+        loop = serve.ServingLoop(ctx, cache, lanes=4, precision="fp32_screen", inter_rounds=4, trace=True)
+        st = loop.run(qs)
+        assert st.completed == len(qs), [q.status for q in qs if q.status != "ok"][:3]
+        for q in qs:
+            ta, tb = cache.task(q.a, q.nuv0, 1), cache.task(q.b, q.nuv0, 2)
+            if q.kind == "distance":
+                alone = ctx.min_distance(ta, tb, k=8, precision="fp32_screen", trace=True)
+                assert np.array_equal(q.result.kth_d2, alone.kth_d2)
+                for r in range(alone.rounds):
+                    assert np.array_equal(q.result.pairs[r], alone.pairs[r])
+            else:
+                alone = ctx.intersect(ta, tb, rounds=4, precision="fp64", trace=True)
+                assert np.array_equal(q.result.counts, alone.counts)
+                for r in range(alone.rounds):
+                    if alone.pairs[r] is not None:
+                        assert np.array_equal(q.result.pairs[r], alone.pairs[r])
+        assert st.p50_ms <= st.p99_ms
+        cache.release()
