@@ -186,8 +186,9 @@ int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const 
 /* --- queued and batched queries (the serving engine) ----------------------
  * No counterpart in the reference, whose API runs one query at a time and is
  * not re-entrant (file statics, intersection.cu:36-39).  jsi_workers starts n
- * worker lanes (each: a CUDA stream, a device arena of up to lane_bytes, a
- * host thread); queued queries run on the first free lane in arrival order
+ * worker lanes (each: a CUDA stream, a device arena of up to lane_bytes, or
+ * an equal share of the HBM budget left beside the resident surfaces when
+ * lane_bytes = 0, and a host thread); queued queries run on the first free lane in arrival order
  * and their kernels overlap on the device.  n = 0 stops the pool (only when
  * nothing is queued).  A surface cannot be released while a queued query
  * uses it.  Results of a query are bit-identical whichever lane runs it and

@@ -187,7 +187,7 @@ struct jsi_context {
   std::map<int, int> surface_refs;  // queued / running jobs per surface
   int next_id = 1;
   size_t budget = size_t(120) << 30;
-  size_t lane_bytes = size_t(1) << 30;
+  size_t lane_bytes = 0;  // 0: an equal share of the budget per lane
   size_t resident = 0;
   std::string kernel_names;
   // worker pool
@@ -1157,9 +1157,14 @@ void stop_workers(jsi_context *ctx) {
 }
 
 void start_workers(jsi_context *ctx, int n) {
+  // Each lane may grow its arena (in 512 MiB blocks, only as used) up to its
+  // share of the budget left beside the resident surfaces, or lane_bytes when
+  // the caller set it.
+  const size_t share = n > 0 ? (ctx->budget > ctx->resident ? (ctx->budget - ctx->resident) / n : 0) : 0;
+  const size_t cap = ctx->lane_bytes ? ctx->lane_bytes : share;
   for (int q = 0; q < n; ++q) {
     auto L = std::make_unique<Lane>();
-    lane_init(*L, ctx->device, std::min(ctx->lane_bytes, size_t(512) << 20), ctx->lane_bytes, &ctx->surfaces);
+    lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces);
     ctx->lanes.push_back(std::move(L));
   }
   for (auto &L : ctx->lanes) ctx->threads.emplace_back(worker_loop, ctx, L.get());
@@ -1422,7 +1427,7 @@ int jsi_workers(jsi_context *ctx, int n, unsigned long long lane_bytes) {
     if (!ctx->queue.empty() || ctx->busy) return record(ctx, JSI_ERR_INVALID, "queries are still queued");
   }
   stop_workers(ctx);
-  if (lane_bytes) ctx->lane_bytes = lane_bytes;
+  ctx->lane_bytes = lane_bytes;
   return guarded(ctx, [&]() {
     start_workers(ctx, n);
     return JSI_OK;
