@@ -65,18 +65,21 @@ struct StatusError {
   throw StatusError{status, buf};
 }
 
-// Device arena: blocks are kept across queries and rewound by reset().
+// Device arena: blocks are kept across queries and rewound by reset().  All
+// arenas of a context draw on one shared budget (bytes held across lanes), so
+// a heavy query can grow beyond an even share while the others are small;
+// trim() hands blocks beyond a lane's steady size back after such a query.
 class Arena {
  public:
   Arena() = default;
   Arena(const Arena &) = delete;
   Arena &operator=(const Arena &) = delete;
-  ~Arena() {
-    for (auto &b : blocks_) cudaFree(b.base);
-  }
-  void configure(size_t block_bytes, size_t budget) {
+  ~Arena() { release_all(); }
+  void configure(size_t block_bytes, size_t budget, std::atomic<size_t> *shared = nullptr, size_t shared_cap = 0) {
     block_bytes_ = block_bytes;
     budget_ = budget;
+    shared_ = shared;
+    shared_cap_ = shared_cap;
   }
   void reset() {
     for (auto &b : blocks_) b.used = 0;
@@ -96,9 +99,17 @@ class Arena {
     }
     const size_t sz = std::max(block_bytes_, bytes);
     if (total_ + sz > budget_) fail(JSI_ERR_NOMEM, "device arena budget exhausted (%zu + %zu > %zu bytes)", total_, sz, budget_);
+    if (shared_) {
+      const size_t before = shared_->fetch_add(sz);
+      if (before + sz > shared_cap_) {
+        shared_->fetch_sub(sz);
+        fail(JSI_ERR_NOMEM, "HBM budget of the context exhausted (%zu + %zu > %zu bytes)", before, sz, shared_cap_);
+      }
+    }
     char *p = nullptr;
     if (cudaMalloc(&p, sz) != cudaSuccess) {
       cudaGetLastError();
+      if (shared_) shared_->fetch_sub(sz);
       fail(JSI_ERR_NOMEM, "cudaMalloc of %zu bytes failed", sz);
     }
     blocks_.push_back({p, sz, bytes});
@@ -110,8 +121,29 @@ class Arena {
   U *get(size_t n) {
     return static_cast<U *>(alloc(n * sizeof(U)));
   }
+  size_t held() const { return total_; }
+  // Frees whole blocks from the back until at most keep bytes are held (the
+  // lane's stream must be idle).
+  void trim(size_t keep) {
+    while (!blocks_.empty() && total_ > keep) {
+      Block b = blocks_.back();
+      blocks_.pop_back();
+      cudaFree(b.base);
+      total_ -= b.size;
+      if (shared_) shared_->fetch_sub(b.size);
+    }
+    cur_ = 0;
+  }
 
  private:
+  void release_all() {
+    for (auto &b : blocks_) {
+      cudaFree(b.base);
+      if (shared_) shared_->fetch_sub(b.size);
+    }
+    blocks_.clear();
+    total_ = 0;
+  }
   struct Block {
     char *base;
     size_t size;
@@ -122,6 +154,8 @@ class Arena {
   size_t block_bytes_ = size_t(2) << 30;
   size_t budget_ = size_t(120) << 30;
   size_t total_ = 0;
+  std::atomic<size_t> *shared_ = nullptr;
+  size_t shared_cap_ = 0;
 };
 
 struct SurfaceRec {
@@ -187,7 +221,9 @@ struct jsi_context {
   std::map<int, int> surface_refs;  // queued / running jobs per surface
   int next_id = 1;
   size_t budget = size_t(120) << 30;
-  size_t lane_bytes = 0;  // 0: an equal share of the budget per lane
+  size_t lane_bytes = 0;  // 0: lanes draw on the shared budget
+  std::atomic<size_t> lane_held{0};  // arena bytes held by all worker lanes
+  size_t lane_keep = 0;              // steady arena size a lane keeps after a query
   size_t resident = 0;
   std::string kernel_names;
   // worker pool
@@ -986,10 +1022,11 @@ void check_precision(int prec, bool screen_built) {
 }
 
 // Lane set-up / tear-down.
-void lane_init(Lane &L, int device, size_t block, size_t budget, const std::map<int, SurfaceRec> *surfaces) {
+void lane_init(Lane &L, int device, size_t block, size_t budget, const std::map<int, SurfaceRec> *surfaces,
+               std::atomic<size_t> *shared = nullptr, size_t shared_cap = 0) {
   L.device = device;
   L.surfaces = surfaces;
-  L.arena.configure(block, budget);
+  L.arena.configure(block, budget, shared, shared_cap);
   JSI_CUDA(cudaSetDevice(device));
   JSI_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
   JSI_CUDA(cudaEventCreate(&L.ev0));
@@ -1134,6 +1171,7 @@ void worker_loop(jsi_context *ctx, Lane *L) {
         exec_intersection(L, &job->a, &job->b, job->ip, &job->ires);
     });
     release_refs(ctx, *job);
+    if (L->arena.held() > ctx->lane_keep) L->arena.trim(ctx->lane_keep);
     {
       std::lock_guard<std::mutex> lk(ctx->qmu);
       job->done = true;
@@ -1157,14 +1195,15 @@ void stop_workers(jsi_context *ctx) {
 }
 
 void start_workers(jsi_context *ctx, int n) {
-  // Each lane may grow its arena (in 512 MiB blocks, only as used) up to its
-  // share of the budget left beside the resident surfaces, or lane_bytes when
-  // the caller set it.
-  const size_t share = n > 0 ? (ctx->budget > ctx->resident ? (ctx->budget - ctx->resident) / n : 0) : 0;
-  const size_t cap = ctx->lane_bytes ? ctx->lane_bytes : share;
+  // Lanes grow their arenas in 512 MiB blocks as used, all drawing on the
+  // budget left beside the resident surfaces (or each up to lane_bytes when
+  // the caller set it); after a query a lane keeps at most an even share.
+  const size_t left = ctx->budget > ctx->resident ? ctx->budget - ctx->resident : 0;
+  const size_t cap = ctx->lane_bytes ? ctx->lane_bytes : left;
+  ctx->lane_keep = n > 0 ? std::max<size_t>(size_t(512) << 20, left / n) : 0;
   for (int q = 0; q < n; ++q) {
     auto L = std::make_unique<Lane>();
-    lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces);
+    lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces, &ctx->lane_held, left);
     ctx->lanes.push_back(std::move(L));
   }
   for (auto &L : ctx->lanes) ctx->threads.emplace_back(worker_loop, ctx, L.get());

@@ -248,8 +248,10 @@ def main(argv=None):
                 loop = ServingLoop(ctx, cache, lanes=args.lanes, budget_bytes=int(args.budget_gb * (1 << 30)),
                                    precision=form)
                 st = loop.run(qs)
+                reasons = sorted({q.status for q in qs if q.status != "ok"})[:3]
                 print(json.dumps({
                     "form": form, "offered_rate": rate, "queries": st.queries, "completed": st.completed,
+                    "failure_reasons": reasons,
                     "failed": st.failed, "throughput_qps": st.throughput, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
                     "peak_admitted_gb": st.peak_admitted_bytes / (1 << 30), "peak_inflight": st.peak_inflight,
                     "lanes": args.lanes, "resident_surfaces": len(cache), "resident_mb": ctx.resident_bytes() / 2**20,
