@@ -16,6 +16,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libjsi_b200.so"
+SHIM = PKG / "libjsi_v5_shim.so"
 SOURCES = ["jsi_kernels.cu", "jsi_capi.cu", "jsi_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: products and sums round separately, in the written order, so
@@ -37,8 +38,20 @@ def needs_build() -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
+def build_shim(force: bool = False) -> Path:
+    """libjsi_v5_shim.so: the reference's C++ query API over the C ABI."""
+    src = CSRC / "jsi_v5_shim.cpp"
+    if not force and SHIM.exists() and SHIM.stat().st_mtime >= max(src.stat().st_mtime, LIB.stat().st_mtime):
+        return SHIM
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", f"-I{ROOT / 'include'}", str(src), f"-L{PKG}",
+           "-ljsi_b200", "-Wl,-rpath,$ORIGIN", "-o", str(SHIM)]
+    subprocess.run(cmd, check=True)
+    return SHIM
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
+        build_shim()
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, *FLAGS, "-shared", f"-I{ROOT / 'include'}", f"-I{CSRC}", "-o", str(tmp)]
@@ -48,6 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_shim(force=True)
     return LIB
 
 

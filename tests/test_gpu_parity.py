@@ -333,3 +333,37 @@ def test_distance_heavy_exact_ties(gpu_ctx, orc, precision, k):
     for r in range(2):
         assert np.array_equal(res.pairs[r], o["pairs"][r])
     assert np.array_equal(res.kth_d2.astype(dt), o["kth_d2"])
+
+
+def _run_example(binary, case, use_k):
+    import os
+    import re
+    import subprocess
+    env = dict(os.environ, CAD_INTERSECT_USE_K=str(use_k), OMP_NUM_THREADS="4")
+    out = subprocess.run([str(binary), str(case)], env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    return [int(m.group(2)) for m in re.finditer(r"Round (\d+): overlap pairs = (\d+)", out.stdout)]
+
+
+@pytest.mark.parametrize("case", [3, 4])
+@pytest.mark.parametrize("use_k", [1, 0])
+def test_reference_example_linked_to_b200_library(case, use_k):
+    """The reference's own examples/intersection_example.cu, compiled
+    unchanged and linked against libjsi_v5_shim.so (the reference's C++ API
+    over this library's C ABI), prints the reference's per-round counts."""
+    from conftest import ROOT
+    binary = ROOT / "oracle" / "_ref" / "test_intersect_b200"
+    if not binary.exists():
+        pytest.skip("reference example not built (needs the reference checkout at build time)")
+    g = load_npz("ref_intersection.npz")
+    assert _run_example(binary, case, use_k) == g[f"case{case}/k{use_k}/counts"].tolist()
+
+
+@pytest.mark.parametrize("case", [1, 2])
+def test_reference_example_degree11_linked_to_b200_library(case):
+    from conftest import ROOT
+    b200 = ROOT / "oracle" / "_ref" / "test_intersect_b200"
+    ref = ROOT / "oracle" / "_ref" / "test_intersect_ref"
+    if not (b200.exists() and ref.exists()):
+        pytest.skip("reference example not built")
+    assert _run_example(b200, case, 1) == _run_example(ref, case, 1)
