@@ -109,14 +109,27 @@ def dist_env():
     return rank, world, local
 
 
+def shard_seeds(batch: int, rank: int):
+    """Seed pairs of the queries one rank runs: ranks own disjoint queries
+    (independent units, no data-path collective)."""
+    return [(1000 + 2 * (rank * batch + q), 1001 + 2 * (rank * batch + q)) for q in range(batch)]
+
+
 def make_pairs(batch: int, rank: int):
     from jsi_cad_next_versions_b200 import synth
     pairs = []
-    for q in range(batch):
-        seed = 1000 + 2 * (rank * batch + q)
-        A, B, _ = synth.distance_pair_hard_wave(seed_a=seed, seed_b=seed + 1)
+    for sa, sb in shard_seeds(batch, rank):
+        A, B, _ = synth.distance_pair_hard_wave(seed_a=sa, seed_b=sb)
         pairs.append((A, B))
     return pairs
+
+
+def reduce_max(x: float, dist, device: str) -> float:
+    """Max over ranks of a per-rank device time (the step time of the job)."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 class ClockSampler:
@@ -264,11 +277,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, pg, f"cuda:{local}") if pg else x
 
     results = {}
     # ---------------- device throughput, surfaces resident -----------------
