@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default=",".join(FORMS))
     ap.add_argument("--lanes", type=int, default=8, help="worker lanes (concurrent queries on the device)")
+    ap.add_argument("--chunk", type=int, default=64,
+                    help="queries per lockstep batch on a lane (0: one query per lane job)")
     return ap.parse_args()
 
 
@@ -266,6 +268,7 @@ def run_ours(args):
 
     ctx = J.Context(local)
     ctx.workers(args.lanes)
+    ctx.batch_chunk(args.chunk)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     pairs = make_pairs(args.batch, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -295,7 +298,7 @@ def run_ours(args):
             return [r.device_ms for r in res], res[-1]
         for _ in range(args.warmup):
             step()
-        ctx.kernel_timing(True)
+        reruns0 = ctx.batch_reruns()
         launches0 = ctx.launch_count()
         step_ms, lats = [], []
         with ClockSampler(local) as clk:
@@ -312,13 +315,21 @@ def run_ours(args):
                 step_ms.append(max_over_ranks(e0.elapsed_time(e1)))
                 lats += l
         launches = ctx.launch_count() - launches0
+        reruns = ctx.batch_reruns() - reruns0
+        # Per-kernel breakdown in separate steps (events around every launch
+        # would perturb the timed steps above).
+        ctx.kernel_timing(True)
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            step()
         ktimes = ctx.kernel_times()
         ctx.kernel_timing(False)
         total_ms = sum(step_ms)
         results[form] = {
             "value": world * args.batch * args.steps / (total_ms / 1e3), "ms_per_step": total_ms / args.steps,
             "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99), "clocks": clk.summary(),
-            "gpu_launches": launches, "kernels": ktimes, "last": last}
+            "gpu_launches": launches, "kernels": ktimes, "last": last, "reruns": reruns}
         ref_values[form] = last.v5_value if form == "v5_fp32" else last.distance
         results[form]["distances"] = step_distances
 
@@ -384,7 +395,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"fp64": "f64", "v5_fp32": "f32", "fp32_screen": "f32+f64"}[forms[0]], "data": "synthetic",
         "config": {"workload": WORKLOAD, "form": forms[0], "queries_per_step_per_gpu": args.batch,
-                   "lanes": args.lanes,
+                   "lanes": args.lanes, "chunk": args.chunk,
                    "nuv0": args.nuv0, "l2": "flushed (256 MiB write) between steps", "parallelism": f"dp{world}"},
         "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"]},
         "forms": {f: {"queries_per_s": r["value"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
@@ -393,6 +404,7 @@ def run_ours(args):
         "speedup_vs_fp64": (head["value"] / results["fp64"]["value"]) if "fp64" in results else None,
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": head["clocks"],
         "gpu_launches": head["gpu_launches"],
+        "batch_reruns": head["reruns"],
         "screen": {"pair_tests_per_round": [int(x) for x in last.pair_tests],
                    "candidates_per_round": [int(x) for x in last.candidates],
                    "kept_per_round": [int(x) for x in last.npairs]},

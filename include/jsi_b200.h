@@ -207,9 +207,20 @@ int jsi_wait(jsi_context *ctx, jsi_ticket ticket, int timeout_ms, jsi_dist_resul
 int jsi_queue_depth(jsi_context *ctx, int *queued, int *running);
 /* n distance queries over the worker lanes; status[q] (may be null) gets each
  * query's status, device_ms (may be null) the device span of the batch
- * (CUDA events).  Returns the first error, else JSI_OK. */
+ * (CUDA events).  Returns the first error, else JSI_OK.
+ * With k <= 8 and rounds <= 8, queries of one shape (first-round nuv and
+ * degrees of both sides) run in lockstep batches of up to jsi_batch_chunk
+ * queries per lane: one launch per stage for the whole batch, counts kept on
+ * the device, one copy in and one copy out per batch.  Results are the same
+ * as the per-query path's; a query whose internal lists overflow is re-run
+ * alone.  No reference counterpart (V5 runs one query per call,
+ * distance_analysis.cu:356). */
 int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
                            const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms);
+/* Queries per lockstep batch (default 64; 0: every query runs alone). */
+int jsi_batch_chunk(jsi_context *ctx, int chunk);
+/* Batch items re-run alone after an internal list overflowed (all lanes). */
+int jsi_batch_reruns(jsi_context *ctx, long long *out);
 
 /* --- grid evaluation -----------------------------------------------------
  * Replaces evalWithCuda(int*, float*, int, float, float, float, float, int,

@@ -235,12 +235,24 @@ class Context:
         self._check(self.lib.jsi_queue_depth(self.handle, ctypes.byref(q), ctypes.byref(r)))
         return q.value, r.value
 
+    def batch_chunk(self, chunk: int) -> None:
+        """Queries per lockstep batch of min_distance_batch (0: one query per
+        lane job)."""
+        self._check(self.lib.jsi_batch_chunk(self.handle, int(chunk)))
+
+    def batch_reruns(self) -> int:
+        """Batch items re-run alone after an internal list overflowed."""
+        v = ctypes.c_longlong(0)
+        self._check(self.lib.jsi_batch_reruns(self.handle, ctypes.byref(v)))
+        return v.value
+
     def min_distance_batch(self, pairs, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
-                           precision: str | int = "v5_fp32", trace: bool = False):
-        """Distance queries [(task_a, task_b), ...] over the worker lanes.
+                           precision: str | int = "v5_fp32", trace: bool = False, newton: bool = False):
+        """Distance queries [(task_a, task_b), ...] over the worker lanes
+        (lockstep batches per shape, see batch_chunk).
         Returns (results, device_ms of the whole batch)."""
         n = len(pairs)
-        p = self._dist_params(k, rounds, nuv_refine, precision, False)
+        p = self._dist_params(k, rounds, nuv_refine, precision, newton)
         ta = (C.Task * n)(*[x[0] for x in pairs])
         tb = (C.Task * n)(*[x[1] for x in pairs])
         res = (C.DistResult * n)()

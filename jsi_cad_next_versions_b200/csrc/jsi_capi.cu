@@ -12,11 +12,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -195,16 +197,29 @@ struct Lane {
   std::map<std::string, std::pair<double, long long>> kernel_ms;
   std::map<std::string, double> kernel_units;  // work units (samples, tile pairs, pair tests, ...)
   const std::map<int, SurfaceRec> *surfaces = nullptr;
+  char *h_pin = nullptr;  // pinned staging of batch heads / records
+  size_t h_pin_bytes = 0;
+  long long batch_reruns = 0;  // batch items re-run alone after an overflow
 };
 
-// A queued query of the worker pool.
+// One query of a batch: its tasks, the caller's result slot and its status
+// (JSI_OK, or the error of its solo re-run).
+struct BatchItem {
+  const jsi_task *a = nullptr, *b = nullptr;
+  jsi_dist_result *out = nullptr;
+  int status = JSI_OK;
+  std::string error;
+};
+
+// A queued query (or lockstep batch of distance queries) of the worker pool.
 struct Job {
-  int kind = 0;  // 0 distance, 1 intersection
+  int kind = 0;  // 0 distance, 1 intersection, 2 distance batch (items)
   jsi_task a{}, b{};
   jsi_dist_params dp{};
   jsi_inter_params ip{};
   jsi_dist_result dres{};
   jsi_inter_result ires{};
+  std::vector<BatchItem> items;
   int status = JSI_OK;
   std::string error;
   bool done = false;
@@ -225,6 +240,7 @@ struct jsi_context {
   std::atomic<size_t> lane_held{0};  // arena bytes held by all worker lanes
   size_t lane_keep = 0;              // steady arena size a lane keeps after a query
   size_t resident = 0;
+  int batch_chunk = 64;  // queries per lockstep batch (0: one query per lane job)
   std::string kernel_names;
   // worker pool
   std::vector<std::unique_ptr<Lane>> lanes;
@@ -589,8 +605,10 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
     surv = ar.get<unsigned long long>(std::max<unsigned long long>(cap, 1));
     surv_lb = ar.get<unsigned>(std::max<unsigned long long>(cap, 1));
     timed(ctx, "dist_expand", [&] {
-      launch_dist_expand(As, Bs, map1, map2, st_surv, n_st, k, 0, surv, surv_lb, cap, ctx->d_stats, screen, e, st);
-      launch_dist_expand(As, Bs, map1, map2, st_surv, n_st, k, 1, surv, surv_lb, cap, ctx->d_stats, screen, e, st);
+      launch_dist_expand(As, Bs, map1, map2, st_surv, n_st, n_st, k, 0, surv, surv_lb, cap, ctx->d_stats, screen, e,
+                         st);
+      launch_dist_expand(As, Bs, map1, map2, st_surv, n_st, n_st, k, 1, surv, surv_lb, cap, ctx->d_stats, screen, e,
+                         st);
     }, 2.0 * double(cap));
   } else {
     if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
@@ -629,11 +647,12 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
     const unsigned long long head = leaf_lb ? std::min<unsigned long long>(nsurv, 148ull * 4) : nsurv;
     if (k <= 8) {
       timed(ctx, "dist_head", [&] {
-        launch_dist_head(A, B, map1, map2, leaf_surv, head, k, ctx->d_stats, screen, e, st);
+        launch_dist_head(A, B, map1, map2, leaf_surv, head, head, k, ctx->d_stats, screen, e, st);
       });
     } else {
       timed(ctx, "dist_head", [&] {
-        launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, head, k, 0, cand, cand_cap, ctx->d_stats, screen, e,
+        launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, head, head, leaf_lb != nullptr, k, 0, cand, cand_cap,
+                         ctx->d_stats, screen, e,
                          st);
       });
       JSI_CUDA(cudaMemsetAsync(&ctx->d_stats->work, 0, sizeof(unsigned long long), st));
@@ -641,7 +660,8 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
   }
   for (int attempt = 0;; ++attempt) {
     timed(ctx, "dist_leaf", [&] {
-      launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, nsurv, k, 1, cand, cand_cap, ctx->d_stats, screen, e,
+      launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, nsurv, nsurv, leaf_lb != nullptr, k, 1, cand, cand_cap,
+                       ctx->d_stats, screen, e,
                        st);
     });
     bool fits = true;
@@ -831,6 +851,412 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
     map2 = nmap2;
     nslots = n;
   }
+}
+
+// ---------------------------------------------------------------------------
+// minimum_distance, lockstep batch
+// ---------------------------------------------------------------------------
+//
+// Queries with one shape (first-round nuv and basis stride of both sides, k,
+// rounds, refinement nuv, precision) run together: every stage is one launch
+// over the batch (query = blockIdx.y), every count stays on the device, and
+// the host touches the batch twice (one strided copy of the query heads in,
+// one of the records out).  Each query owns a slab of identical layout; the
+// kernels reach query q's arrays at the query-0 addresses + q * slab bytes.
+// Lists have fixed capacities; a query that overflows one is flagged in its
+// record and re-run alone by run_distance.
+
+// Bump planner over one slab (base = nullptr: sizing pass).
+class SlabPlan {
+ public:
+  explicit SlabPlan(char *base) : base_(base) {}
+  template <typename U>
+  U *get(size_t n) {
+    const size_t bytes = (std::max<size_t>(n * sizeof(U), 1) + 255) & ~static_cast<size_t>(255);
+    U *p = reinterpret_cast<U *>(base_ + off_);
+    off_ += bytes;
+    return p;
+  }
+  size_t size() const { return off_; }
+
+ private:
+  char *base_;
+  size_t off_ = 0;
+};
+
+// What the host writes into each slab before the batch runs.
+template <typename TP>
+struct DistHead {
+  SurfView<double> a64, b64;
+  SurfView<float> a32, b32;
+  double dom[8];
+  RegionRec<TP> roots[2];
+  int maps[2];
+  int pad_[2];
+  ScreenStats stats;
+};
+
+template <typename TP>
+const SurfView<TP> *head_view(const DistHead<TP> *h, int side);
+template <>
+const SurfView<double> *head_view<double>(const DistHead<double> *h, int side) {
+  return side ? &h->b64 : &h->a64;
+}
+template <>
+const SurfView<float> *head_view<float>(const DistHead<float> *h, int side) {
+  return side ? &h->b32 : &h->a32;
+}
+
+template <typename T>
+SideRound<T> slab_side(SlabPlan &sp, const Geom &g, int nreg, RegionRec<T> *regions, const int *dnreg, bool basis,
+                       bool cells, bool super) {
+  SideRound<T> s{};
+  s.g = g;
+  s.nreg = nreg;
+  s.regions = regions;
+  s.dnreg = dnreg;
+  if (basis) {
+    s.spans = sp.get<int>(static_cast<size_t>(nreg) * 2 * g.nuv);
+    s.basis = sp.get<T>(static_cast<size_t>(nreg) * 2 * g.nuv * 3 * g.p1max);
+  }
+  if (cells) {
+    s.samples = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv);
+    s.center = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.cpr);
+    s.tlo = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
+    s.thi = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
+  }
+  if (super) {
+    s.stlo = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nst);
+    s.sthi = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nst);
+  }
+  return s;
+}
+
+// List capacities per query and round: tile pairs after the supertile
+// expansion and screen candidates.  JSI_BATCH_SURV_CAP / JSI_BATCH_CAND_CAP
+// override them (the small values exercise the re-run of overflowed queries).
+struct BatchCaps {
+  unsigned long long surv = 1ull << 16;
+  unsigned long long cand = 1ull << 14;
+};
+
+BatchCaps batch_caps() {
+  BatchCaps c;
+  auto env = [](const char *name, unsigned long long dflt) {
+    const char *v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    const unsigned long long x = std::strtoull(v, nullptr, 10);
+    return std::min<unsigned long long>(std::max<unsigned long long>(x, 1), 1ull << 24);
+  };
+  c.surv = env("JSI_BATCH_SURV_CAP", c.surv);
+  c.cand = env("JSI_BATCH_CAND_CAP", c.cand);
+  return c;
+}
+constexpr unsigned long long kBatchHeadCap = 2048;        // threshold-pass list
+constexpr unsigned kBatchHeadWant = 148 * 4;
+
+// One round's arrays in the slab.  TP sides hold the regions and basis tables
+// (and, in exact rounds, the cells); the FP32 screen's first round keeps its
+// cells in the TC sides.
+template <typename TP, typename TC>
+struct BatchRound {
+  SideRound<TP> A, B;
+  SideRound<TC> A32, B32;
+  const int *map1 = nullptr, *map2 = nullptr;
+  int max_slots = 1;
+  bool super = false;
+  unsigned long long st_cap = 0, surv_cap = 0, cand_cap = 0;
+  unsigned long long *st_surv = nullptr, *surv = nullptr, *head = nullptr;
+  unsigned *surv_lb = nullptr;
+  void *cand = nullptr;  // DistCand of the round's screening precision
+  DistCand<TP> *checked = nullptr;
+  DistCand<TP> *top = nullptr;
+  RegionRec<TP> *next1 = nullptr, *next2 = nullptr;
+  int *nmap1 = nullptr, *nmap2 = nullptr;
+};
+
+template <typename TP, typename TC>
+struct BatchLayout {
+  DistHead<TP> *head = nullptr;
+  DistRecord<TP> *rec = nullptr;
+  std::vector<BatchRound<TP, TC>> rounds;
+  size_t bytes = 0;
+};
+
+template <typename TP, typename TC>
+BatchLayout<TP, TC> plan_batch(char *base, int nuv1, int nuv2, int p1a, int p1b, const jsi_dist_params &p,
+                               const BatchCaps &caps) {
+  constexpr bool kScreen = !std::is_same<TP, TC>::value;
+  SlabPlan sp(base);
+  BatchLayout<TP, TC> L;
+  L.head = sp.get<DistHead<TP>>(1);
+  L.rec = sp.get<DistRecord<TP>>(1);
+  RegionRec<TP> *reg1 = L.head->roots, *reg2 = L.head->roots + 1;
+  const int *map1 = L.head->maps, *map2 = L.head->maps + 1;
+  const int *dn1 = nullptr, *dn2 = nullptr;
+  int nreg = 1;
+  for (int r = 1; r <= p.rounds; ++r) {
+    BatchRound<TP, TC> R;
+    const Geom g1 = make_geom(r == 1 ? nuv1 : p.nuv_refine, p1a);
+    const Geom g2 = make_geom(r == 1 ? nuv2 : p.nuv_refine, p1b);
+    R.super = g1.tw > kMaxTile || g2.tw > kMaxTile;
+    R.max_slots = r == 1 ? 1 : p.k;
+    const bool scr = kScreen && r == 1;
+    R.A = slab_side<TP>(sp, g1, nreg, reg1, dn1, true, !scr, !scr && R.super);
+    R.B = slab_side<TP>(sp, g2, nreg, reg2, dn2, true, !scr, !scr && R.super);
+    if (scr) {
+      R.A32 = slab_side<TC>(sp, g1, nreg, nullptr, dn1, false, true, R.super);
+      R.B32 = slab_side<TC>(sp, g2, nreg, nullptr, dn2, false, true, R.super);
+    }
+    R.map1 = map1;
+    R.map2 = map2;
+    if (R.super) {
+      R.st_cap = static_cast<unsigned long long>(R.max_slots) * g1.nst * g2.nst;
+      R.st_surv = sp.get<unsigned long long>(R.st_cap);
+      R.surv_cap = caps.surv;
+    } else {
+      R.surv_cap = static_cast<unsigned long long>(R.max_slots) * g1.ntiles * g2.ntiles;
+    }
+    R.surv = sp.get<unsigned long long>(R.surv_cap);
+    R.surv_lb = sp.get<unsigned>(R.surv_cap);
+    R.head = sp.get<unsigned long long>(kBatchHeadCap);
+    R.cand_cap = caps.cand;
+    R.cand = sp.get<DistCand<TP>>(R.cand_cap);  // TP is the wider type
+    if (scr) R.checked = sp.get<DistCand<TP>>(R.cand_cap);
+    R.top = sp.get<DistCand<TP>>(p.k);
+    if (r < p.rounds) {
+      R.next1 = sp.get<RegionRec<TP>>(p.k);
+      R.next2 = sp.get<RegionRec<TP>>(p.k);
+      R.nmap1 = sp.get<int>(p.k);
+      R.nmap2 = sp.get<int>(p.k);
+      reg1 = R.next1;
+      reg2 = R.next2;
+      map1 = R.nmap1;
+      map2 = R.nmap2;
+      dn1 = &L.head->stats.nreg1;
+      dn2 = &L.head->stats.nreg2;
+      nreg = p.k;
+    }
+    L.rounds.push_back(R);
+  }
+  L.bytes = sp.size();
+  return L;
+}
+
+// Screening stages of one batched round over sides of precision T.
+template <typename T, typename TP, typename TC>
+void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, const SideRound<T> &Y,
+                  ScreenStats *stats, int k, bool screen, float e, const Batch &bt) {
+  cudaStream_t st = L->stream;
+  const int ns = R.max_slots == 1 ? 1 : -R.max_slots;
+  if (R.super) {
+    timed(L, "supertiles", [&] {
+      launch_supertiles(X, st, bt);
+      launch_supertiles(Y, st, bt);
+    });
+    timed(L, "dist_tau", [&] { launch_dist_tau_st(X, Y, R.map1, R.map2, ns, k, stats, screen, e, st, bt); });
+    timed(L, "dist_cull", [&] {
+      launch_dist_cull_st(X, Y, R.map1, R.map2, ns, R.st_surv, R.st_cap, stats, screen, e, st, bt);
+    });
+    timed(L, "dist_expand", [&] {
+      launch_dist_expand(X, Y, R.map1, R.map2, R.st_surv, kFromDevice, R.st_cap, k, 0, R.surv, R.surv_lb, R.surv_cap,
+                         stats, screen, e, st, bt);
+      launch_dist_expand(X, Y, R.map1, R.map2, R.st_surv, kFromDevice, R.st_cap, k, 1, R.surv, R.surv_lb, R.surv_cap,
+                         stats, screen, e, st, bt);
+    });
+  } else {
+    timed(L, "dist_tau", [&] { launch_dist_tau(X, Y, R.map1, R.map2, ns, k, stats, screen, e, st, bt); });
+    timed(L, "dist_cull", [&] {
+      launch_dist_cull(X, Y, R.map1, R.map2, ns, R.surv, R.surv_lb, R.surv_cap, stats, screen, e, st, bt);
+    });
+  }
+  timed(L, "dist_pick", [&] {
+    launch_dist_pick(R.surv, R.surv_lb, R.surv_cap, R.head, kBatchHeadCap, kBatchHeadWant, stats, st, bt);
+  });
+  timed(L, "dist_head", [&] {
+    launch_dist_head(X, Y, R.map1, R.map2, R.head, kFromDevice, kBatchHeadCap, k, stats, screen, e, st, bt);
+  });
+  timed(L, "dist_leaf", [&] {
+    launch_dist_leaf(X, Y, R.map1, R.map2, R.surv, R.surv_lb, kFromDevice, R.surv_cap, false, k, 1,
+                     static_cast<DistCand<T> *>(R.cand), R.cand_cap, stats, screen, e, st, bt);
+  });
+}
+
+char *lane_pinned(Lane *L, size_t bytes) {
+  if (L->h_pin_bytes < bytes) {
+    JSI_CUDA(cudaStreamSynchronize(L->stream));
+    if (L->h_pin) JSI_CUDA(cudaFreeHost(L->h_pin));
+    L->h_pin = nullptr;
+    L->h_pin_bytes = 0;
+    JSI_CUDA(cudaMallocHost(reinterpret_cast<void **>(&L->h_pin), bytes));
+    L->h_pin_bytes = bytes;
+  }
+  return L->h_pin;
+}
+
+// The lockstep batch (all items share the shape of items[0]); items whose
+// record reports an overflow are re-run alone.  Returns the number re-run.
+template <typename TP, typename TC>
+int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_params &p) {
+  constexpr bool kScreen = !std::is_same<TP, TC>::value;
+  const int n = static_cast<int>(items.size());
+  if (n == 0) return 0;
+  cudaStream_t st = L->stream;
+  const SurfaceRec &s0a = get_surface(L, items[0].a->surface);
+  const SurfaceRec &s0b = get_surface(L, items[0].b->surface);
+  const int nuv1 = items[0].a->nuv, nuv2 = items[0].b->nuv, p1a = p1_of(s0a), p1b = p1_of(s0b);
+  const BatchCaps caps = batch_caps();
+  const BatchLayout<TP, TC> probe = plan_batch<TP, TC>(nullptr, nuv1, nuv2, p1a, p1b, p, caps);
+  const size_t slab = (probe.bytes + 255) & ~static_cast<size_t>(255);
+  char *base = static_cast<char *>(L->arena.alloc(slab * n));
+  const BatchLayout<TP, TC> lay = plan_batch<TP, TC>(base, nuv1, nuv2, p1a, p1b, p, caps);
+  const Batch bt{n, static_cast<long long>(slab)};
+
+  // Heads: surface views, Newton domains, root rectangles, fresh counters.
+  const size_t hsz = sizeof(DistHead<TP>), rsz = sizeof(DistRecord<TP>);
+  char *pin = lane_pinned(L, std::max(hsz, rsz) * n);
+  float e = 0.0f;
+  for (int q = 0; q < n; ++q) {
+    const SurfaceRec &sa = get_surface(L, items[q].a->surface);
+    const SurfaceRec &sb = get_surface(L, items[q].b->surface);
+    if (p1_of(sa) != p1a || p1_of(sb) != p1b || items[q].a->nuv != nuv1 || items[q].b->nuv != nuv2)
+      fail(JSI_ERR_INVALID, "batch items differ in shape");
+    DistHead<TP> h{};
+    h.a64 = view<double>(sa);
+    h.b64 = view<double>(sb);
+    h.a32 = view<float>(sa);
+    h.b32 = view<float>(sb);
+    newton_domain(items[q].a, items[q].b, h.dom);
+    const jsi_task *ta = items[q].a, *tb = items[q].b;
+    h.roots[0] = RegionRec<TP>{TP(ta->ustart), TP(ta->vstart), TP(ta->ustop), TP(ta->vstop)};
+    h.roots[1] = RegionRec<TP>{TP(tb->ustart), TP(tb->vstart), TP(tb->ustop), TP(tb->vstop)};
+    h.stats.tau_bits = 0x7f800000u;
+    h.stats.nslots = 1;
+    std::memcpy(pin + q * hsz, &h, hsz);
+    if (kScreen) e = std::max(e, screen_error(sa, sb));
+  }
+  JSI_CUDA(cudaMemcpy2DAsync(lay.head, slab, pin, hsz, hsz, n, cudaMemcpyHostToDevice, st));
+  L->h2d_bytes += hsz * n;
+
+  ScreenStats *stats = &lay.head->stats;
+  const SurfView<TP> va = view<TP>(s0a), vb = view<TP>(s0b);
+  const int R = p.rounds;
+  for (int r = 1; r <= R; ++r) {
+    const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
+    const bool scr = kScreen && r == 1;
+    timed(L, "basis", [&] {
+      launch_basis(va, Rd.A, st, bt, head_view<TP>(lay.head, 0));
+      launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1));
+    });
+    if (!scr) {
+      timed(L, "samples", [&] {
+        launch_samples(va, Rd.A, false, st, bt, head_view<TP>(lay.head, 0));
+        launch_samples(vb, Rd.B, false, st, bt, head_view<TP>(lay.head, 1));
+      });
+      timed(L, "cells", [&] {
+        launch_cells(Rd.A, false, st, bt);
+        launch_cells(Rd.B, false, st, bt);
+      });
+      batch_screen<TP>(L, Rd, Rd.A, Rd.B, stats, p.k, false, 0.0f, bt);
+      timed(L, "dist_select", [&] {
+        launch_dist_select(static_cast<const DistCand<TP> *>(Rd.cand), Rd.cand_cap, p.k, Rd.top, stats, st, bt);
+      });
+    } else if constexpr (kScreen) {
+      timed(L, "samples", [&] {
+        launch_samples_screen(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
+        launch_samples_screen(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
+      });
+      timed(L, "cells", [&] {
+        launch_cells(Rd.A32, false, st, bt);
+        launch_cells(Rd.B32, false, st, bt);
+      });
+      batch_screen<TC>(L, Rd, Rd.A32, Rd.B32, stats, p.k, true, e, bt);
+      timed(L, "dist_verify", [&] {
+        launch_dist_verify(view<double>(s0a), view<double>(s0b), Rd.A, Rd.B, Rd.map1, Rd.map2,
+                           static_cast<const DistCand<float> *>(Rd.cand), 0, Rd.checked,
+                           st, bt, &lay.head->a64, &lay.head->b64, stats, Rd.cand_cap);
+      });
+      timed(L, "dist_select", [&] { launch_dist_select(Rd.checked, Rd.cand_cap, p.k, Rd.top, stats, st, bt); });
+    }
+    if (r < R) {
+      timed(L, "dist_next", [&] {
+        launch_dist_next(Rd.top, stats, Rd.A, Rd.B, Rd.map1, Rd.map2, p.nuv_refine, Rd.next1, Rd.next2, Rd.nmap1,
+                         Rd.nmap2, st, bt);
+      });
+    }
+    timed(L, "dist_close", [&] {
+      launch_dist_close(stats, Rd.top, lay.rec, r - 1, Rd.surv_cap, Rd.cand_cap, r == R, st, bt);
+    });
+  }
+  if (p.newton) {
+    const BatchRound<TP, TC> &Rd = lay.rounds[R - 1];
+    timed(L, "newton", [&] {
+      launch_newton_dist(view<double>(s0a), view<double>(s0b), Rd.A.regions, Rd.B.regions, Rd.map1, Rd.map2,
+                         Rd.A.g.nuv, Rd.B.g.nuv, Rd.top, p.k, lay.head->dom, lay.rec->newton, st, bt,
+                         &lay.head->a64, &lay.head->b64, stats);
+    });
+  }
+  JSI_CUDA(cudaGetLastError());
+  JSI_CUDA(cudaMemcpy2DAsync(pin, rsz, lay.rec, slab, rsz, n, cudaMemcpyDeviceToHost, st));
+  L->d2h_bytes += rsz * n;
+  JSI_CUDA(cudaStreamSynchronize(st));
+  if (L->timing) resolve_timing(L);
+
+  // Results, in the order and with the meaning run_distance gives them.
+  int rerun = 0;
+  for (int q = 0; q < n; ++q) {
+    const DistRecord<TP> &rec = *reinterpret_cast<const DistRecord<TP> *>(pin + q * rsz);
+    jsi_dist_result *out = items[q].out;
+    bool bad = false;
+    for (int r = 0; r < R && !bad; ++r) {
+      bad = rec.status[r] != 0;
+      if (rec.npairs[r] == 0) break;
+    }
+    if (bad) {
+      items[q].status = -1;  // re-run below
+      ++rerun;
+      continue;
+    }
+    for (int round = 1; round <= R; ++round) {
+      const int np = rec.npairs[round - 1];
+      out->npairs[round - 1] = np;
+      out->pair_tests[round - 1] = rec.tests[round - 1];
+      out->candidates[round - 1] = rec.cands[round - 1];
+      out->kth_d2[round - 1] = np > 0 ? static_cast<double>(rec.top[round - 1][np - 1].d2) : 0.0;
+      if (np > 0 && out->trace_pairs && static_cast<long long>(round) * p.k <= out->trace_cap) {
+        for (int e2 = 0; e2 < np; ++e2) {
+          int *tp = out->trace_pairs + (static_cast<long long>(round - 1) * p.k + e2) * 3;
+          tp[0] = rec.top[round - 1][e2].slot;
+          tp[1] = rec.top[round - 1][e2].i;
+          tp[2] = rec.top[round - 1][e2].j;
+        }
+      }
+      out->rounds_run = round;
+      if (np == 0 || round == R) {
+        const TP kth = np > 0 ? rec.top[round - 1][np - 1].d2 : TP(0);
+        const TP root = std::sqrt(kth);
+        out->v5_value = static_cast<float>(root);
+        out->distance = static_cast<double>(root);
+        if (p.newton && np > 0 && round == R) {
+          int best = 0;
+          for (int e2 = 1; e2 < np; ++e2)
+            if (rec.newton[e2 * 11] < rec.newton[best * 11]) best = e2;
+          const double *b = rec.newton + best * 11;
+          out->newton_distance = b[0];
+          out->uv1[0] = b[1];
+          out->uv1[1] = b[2];
+          out->uv2[0] = b[3];
+          out->uv2[1] = b[4];
+          for (int c = 0; c < 3; ++c) {
+            out->point1[c] = b[5 + c];
+            out->point2[c] = b[8 + c];
+          }
+        }
+        break;
+      }
+    }
+  }
+  return rerun;
 }
 
 // ---------------------------------------------------------------------------
@@ -1046,6 +1472,9 @@ void lane_free(Lane &L) {
   L.event_pool.clear();
   if (L.d_stats) cudaFree(L.d_stats);
   if (L.h_stats) cudaFreeHost(L.h_stats);
+  if (L.h_pin) cudaFreeHost(L.h_pin);
+  L.h_pin = nullptr;
+  L.h_pin_bytes = 0;
   if (L.ev0) cudaEventDestroy(L.ev0);
   if (L.ev1) cudaEventDestroy(L.ev1);
   if (L.stream) cudaStreamDestroy(L.stream);
@@ -1124,6 +1553,44 @@ void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_
   if (L->timing) resolve_timing(L);
 }
 
+int run_guarded(std::string &err, const std::function<void()> &fn);
+
+// A lockstep batch on one lane; every item gets the batch's device time.
+// Items flagged by the batch (a list overflowed) are re-run alone.
+void exec_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_params &p) {
+  JSI_CUDA(cudaSetDevice(L->device));
+  L->arena.reset();
+  for (auto &it : items) {
+    int *tp = it.out->trace_pairs;
+    const long long tc = it.out->trace_cap;
+    std::memset(it.out, 0, sizeof(*it.out));
+    it.out->trace_pairs = tp;
+    it.out->trace_cap = tc;
+    it.out->newton_distance = -1.0;
+    it.status = JSI_OK;
+  }
+  JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
+  int rerun = 0;
+  if (p.precision == JSI_PREC_V5_FP32)
+    rerun = run_distance_batch<float, float>(L, items, p);
+  else if (p.precision == JSI_PREC_FP64)
+    rerun = run_distance_batch<double, double>(L, items, p);
+  else
+    rerun = run_distance_batch<double, float>(L, items, p);
+  JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
+  JSI_CUDA(cudaEventSynchronize(L->ev1));
+  float ms = 0.0f;
+  JSI_CUDA(cudaEventElapsedTime(&ms, L->ev0, L->ev1));
+  L->batch_reruns += rerun;
+  for (auto &it : items) {
+    if (it.status == JSI_OK) {
+      it.out->device_ms = ms;
+      continue;
+    }
+    it.status = run_guarded(it.error, [&] { exec_distance(L, it.a, it.b, p, it.out); });
+  }
+}
+
 int run_guarded(std::string &err, const std::function<void()> &fn) {
   try {
     fn();
@@ -1143,9 +1610,20 @@ int run_guarded(std::string &err, const std::function<void()> &fn) {
   }
 }
 
+std::vector<int> job_surfaces(const Job &j) {
+  if (j.kind != 2) return {j.a.surface, j.b.surface};
+  std::vector<int> ids;
+  ids.reserve(2 * j.items.size());
+  for (const auto &it : j.items) {
+    ids.push_back(it.a->surface);
+    ids.push_back(it.b->surface);
+  }
+  return ids;
+}
+
 void release_refs(jsi_context *ctx, const Job &j) {
   std::lock_guard<std::mutex> lk(ctx->mu);
-  for (int id : {j.a.surface, j.b.surface}) {
+  for (int id : job_surfaces(j)) {
     auto it = ctx->surface_refs.find(id);
     if (it != ctx->surface_refs.end() && --it->second <= 0) ctx->surface_refs.erase(it);
   }
@@ -1167,8 +1645,10 @@ void worker_loop(jsi_context *ctx, Lane *L) {
     job->status = run_guarded(job->error, [&] {
       if (job->kind == 0)
         exec_distance(L, &job->a, &job->b, job->dp, &job->dres);
-      else
+      else if (job->kind == 1)
         exec_intersection(L, &job->a, &job->b, job->ip, &job->ires);
+      else
+        exec_distance_batch(L, job->items, job->dp);
     });
     release_refs(ctx, *job);
     if (L->arena.held() > ctx->lane_keep) L->arena.trim(ctx->lane_keep);
@@ -1212,10 +1692,10 @@ void start_workers(jsi_context *ctx, int n) {
 long long enqueue(jsi_context *ctx, std::shared_ptr<Job> job) {
   {
     std::lock_guard<std::mutex> lk(ctx->mu);
-    for (int id : {job->a.surface, job->b.surface}) {
+    const std::vector<int> ids = job_surfaces(*job);
+    for (int id : ids)
       if (!ctx->surfaces.count(id)) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
-      ++ctx->surface_refs[id];
-    }
+    for (int id : ids) ++ctx->surface_refs[id];
   }
   long long t;
   {
@@ -1545,12 +2025,35 @@ int jsi_queue_depth(jsi_context *ctx, int *queued, int *running) {
   return JSI_OK;
 }
 
+int jsi_batch_chunk(jsi_context *ctx, int chunk) {
+  if (!ctx || chunk < 0 || chunk > 65535) return JSI_ERR_INVALID;
+  ctx->batch_chunk = chunk;
+  return JSI_OK;
+}
+
+int jsi_batch_reruns(jsi_context *ctx, long long *out) {
+  if (!ctx || !out) return JSI_ERR_INVALID;
+  long long t = 0;
+  for (auto &L : ctx->lanes) t += L->batch_reruns;
+  *out = t;
+  return JSI_OK;
+}
+
 int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
                            const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms) {
   if (!ctx || n < 0 || (n > 0 && (!a || !b || !out))) return JSI_ERR_INVALID;
   if (ctx->lanes.empty()) return record(ctx, JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
-  std::vector<jsi_ticket> tickets(n, 0);
+  jsi_dist_params p;
+  jsi_dist_params_default(&p);
+  if (params) p = *params;
+  std::vector<jsi_ticket> tickets;
+  std::vector<std::shared_ptr<Job>> batch_jobs;
+  std::vector<int> solo;  // query index of each ticket of a per-query job (-1: batch job)
   int first_err = JSI_OK;
+  auto set_status = [&](int q, int st) {
+    if (status) status[q] = st;
+    if (st != JSI_OK && first_err == JSI_OK) first_err = st;
+  };
   // Device span of the batch: every lane waits for a start event on the main
   // stream; the main stream waits for every lane at the end.
   {
@@ -1563,19 +2066,88 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
     });
     if (st != JSI_OK) return st;
   }
-  for (int q = 0; q < n; ++q) {
-    const int st = jsi_submit_distance(ctx, &a[q], &b[q], params, out[q].trace_pairs, out[q].trace_cap, &tickets[q]);
-    if (st != JSI_OK) {
-      if (status) status[q] = st;
-      if (first_err == JSI_OK) first_err = st;
-      tickets[q] = 0;
+  const bool lockstep = ctx->batch_chunk > 0 && p.k >= 1 && p.k <= kBatchK && p.rounds >= 1 &&
+                        p.rounds <= kBatchRounds;
+  if (lockstep) {
+    // Group by shape: first-round nuv and basis stride of both sides.
+    std::map<std::array<int, 4>, std::vector<int>> groups;
+    for (int q = 0; q < n; ++q) {
+      std::string err;
+      std::array<int, 4> key{};
+      const int st = run_guarded(err, [&] {
+        validate_dist(p, &a[q], &b[q]);
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto ia = ctx->surfaces.find(a[q].surface), ib = ctx->surfaces.find(b[q].surface);
+        if (ia == ctx->surfaces.end() || ib == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
+        key = {a[q].nuv, b[q].nuv, p1_of(ia->second), p1_of(ib->second)};
+      });
+      if (st != JSI_OK) {
+        set_status(q, st);
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->last_error = err;
+        continue;
+      }
+      groups[key].push_back(q);
+    }
+    const int nl = static_cast<int>(ctx->lanes.size());
+    for (auto &g : groups) {
+      const int m = static_cast<int>(g.second.size());
+      const int per = std::max(1, std::min(ctx->batch_chunk, (m + nl - 1) / nl));
+      for (int s0 = 0; s0 < m; s0 += per) {
+        auto job = std::make_shared<Job>();
+        job->kind = 2;
+        job->dp = p;
+        for (int t = s0; t < std::min(m, s0 + per); ++t) {
+          const int q = g.second[t];
+          BatchItem it;
+          it.a = &a[q];
+          it.b = &b[q];
+          it.out = &out[q];
+          job->items.push_back(it);
+        }
+        jsi_ticket t = 0;
+        const int st = guarded(ctx, [&]() {
+          t = enqueue(ctx, job);
+          return JSI_OK;
+        });
+        if (st != JSI_OK) {
+          for (int u = s0; u < std::min(m, s0 + per); ++u) set_status(g.second[u], st);
+          continue;
+        }
+        tickets.push_back(t);
+        solo.push_back(-1);
+        batch_jobs.push_back(job);
+      }
+    }
+  } else {
+    for (int q = 0; q < n; ++q) {
+      jsi_ticket t = 0;
+      const int st = jsi_submit_distance(ctx, &a[q], &b[q], &p, out[q].trace_pairs, out[q].trace_cap, &t);
+      if (st != JSI_OK) {
+        set_status(q, st);
+        continue;
+      }
+      tickets.push_back(t);
+      solo.push_back(q);
     }
   }
-  for (int q = 0; q < n; ++q) {
-    if (!tickets[q]) continue;
-    const int st = jsi_wait(ctx, tickets[q], -1, &out[q], nullptr);
-    if (status) status[q] = st;
-    if (st != JSI_OK && first_err == JSI_OK) first_err = st;
+  size_t bj = 0;
+  for (size_t w = 0; w < tickets.size(); ++w) {
+    if (solo[w] >= 0) {
+      set_status(solo[w], jsi_wait(ctx, tickets[w], -1, &out[solo[w]], nullptr));
+      continue;
+    }
+    const int st = jsi_wait(ctx, tickets[w], -1, nullptr, nullptr);
+    Job &job = *batch_jobs[bj++];
+    for (auto &it : job.items) {
+      const int q = static_cast<int>(it.out - out);
+      const int sq = st != JSI_OK ? st : it.status;
+      set_status(q, sq);
+      if (sq != JSI_OK && !it.error.empty()) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->last_error = it.error;
+      }
+    }
   }
   std::lock_guard<std::mutex> lk(ctx->mu);
   const int st = guarded(ctx, [&]() {

@@ -94,6 +94,7 @@ struct SideRound {
   Vec4<T> *thmax;
   Vec4<T> *stlo;  // supertile bounds [R][nst] (built on demand)
   Vec4<T> *sthi;
+  const int *dnreg;  // when set: the region count lives on the device (batched rounds)
 };
 
 // Candidate of the distance screen.
@@ -116,6 +117,38 @@ struct ScreenStats {
   int pad_;
   unsigned long long work;          // work counter of the persistent leaf kernels
   unsigned long long st_survivors;  // supertile pairs that passed the bound
+  unsigned long long nhead;         // tile pairs in the threshold pass's list (batched rounds)
+  int nslots;                       // slots of this round (batched rounds)
+  int pad2_;
+};
+
+// Lockstep batch of queries that share one shape: query q runs in
+// blockIdx.y = q and finds every per-query array at the query-0 address plus
+// q * qs bytes (one slab per query, identical layouts).  n = 1, qs = 0 is the
+// single-query launch.
+struct Batch {
+  int n = 1;
+  long long qs = 0;
+};
+
+// Count arguments with this value are read from the device (ScreenStats).
+constexpr unsigned long long kFromDevice = ~0ull;
+
+// Batched distance form: limits and the per-query record it leaves in the
+// query's slab (read back with one strided copy per batch).
+constexpr int kBatchRounds = 8;  // rounds a batched query may run
+constexpr int kBatchK = 8;       // largest k of the batched form
+constexpr int kStatusCapacity = -4;  // JSI_ERR_CAPACITY
+
+template <typename TP>
+struct DistRecord {
+  long long tests[kBatchRounds];
+  long long cands[kBatchRounds];
+  unsigned long long survivors[kBatchRounds];
+  int npairs[kBatchRounds];
+  int status[kBatchRounds];
+  DistCand<TP> top[kBatchRounds][kBatchK];
+  double newton[kBatchK * 11];
 };
 
 // A surviving tile pair: (row = slot * ntiles1 + t1) << 32 | t2.
@@ -124,68 +157,90 @@ __host__ __device__ inline unsigned long long pack_tile_pair(unsigned row, unsig
 }
 
 // ---- launchers (jsi_kernels.cu) ----
+// Every distance-path launcher takes an optional Batch (default: one query).
+// In a batch the per-query arrays sit in slabs qs bytes apart; surfaces come
+// from the slabs through the vdev pointers; counts given as kFromDevice (or a
+// negative slot count -max) are read from each query's ScreenStats, with the
+// host value (or cap) only bounding the grid.
 unsigned long long launch_count();  // kernels launched so far (all contexts)
 template <typename T>
-void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st);
+void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt = Batch{},
+                  const SurfView<T> *vdev = nullptr);
 template <typename T>
-void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st);
+void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st,
+                    const Batch &bt = Batch{}, const SurfView<T> *vdev = nullptr);
 template <typename T>
 void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaStream_t st);
 template <typename T>
-void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st);
+void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st, const Batch &bt = Batch{});
 template <typename T>
 void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st);
 
 // screen = true (float only): FP32-screen thresholds with centre-error bound e.
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                     int k, ScreenStats *stats, bool screen, float e, cudaStream_t st);
+                     int k, ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt = Batch{});
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                       unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
-                      bool screen, float e, cudaStream_t st);
-// surv_lb may be null (no early exit); when given, surv must be sorted by it.
+                      bool screen, float e, cudaStream_t st, const Batch &bt = Batch{});
+// sorted: surv is ordered by surv_lb (a warp stops at the first bound above
+// tau); otherwise tile pairs whose bound exceeds tau are skipped.
 // collect = 0: only tighten tau (no candidates); 1: append pairs with d2 <= tau.
 template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                      const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
-                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, bool screen,
-                      float e, cudaStream_t st);
+                      const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv,
+                      unsigned long long surv_cap, bool sorted, int k, int collect, DistCand<T> *cand,
+                      unsigned long long cand_cap, ScreenStats *stats, bool screen, float e, cudaStream_t st,
+                      const Batch &bt = Batch{});
 // Supertile level of the distance screen: bounds of 8 x 8 tiles, threshold
 // seed and cull over supertile pairs, expansion of the surviving supertile
 // pairs into tile pairs (threshold pass, then cull with the bound keys).
 template <typename T>
-void launch_supertiles(const SideRound<T> &sr, cudaStream_t st);
+void launch_supertiles(const SideRound<T> &sr, cudaStream_t st, const Batch &bt = Batch{});
 template <typename T>
 void launch_dist_tau_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                        int k, ScreenStats *stats, bool screen, float e, cudaStream_t st);
+                        int k, ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt = Batch{});
 template <typename T>
 void launch_dist_cull_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                          unsigned long long *surv, unsigned long long cap, ScreenStats *stats, bool screen, float e,
-                         cudaStream_t st);
+                         cudaStream_t st, const Batch &bt = Batch{});
 template <typename T>
 void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                        const unsigned long long *st_surv, unsigned long long nst_surv, int k, int cull,
-                        unsigned long long *surv, unsigned *surv_lb, unsigned long long cap, ScreenStats *stats,
-                        bool screen, float e, cudaStream_t st);
+                        const unsigned long long *st_surv, unsigned long long nst_surv, unsigned long long st_cap,
+                        int k, int cull, unsigned long long *surv, unsigned *surv_lb, unsigned long long cap,
+                        ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt = Batch{});
 // Exact k-th d2 (k <= 8) of each of the first nhead tile pairs, folded into tau.
 template <typename T>
 void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats, bool screen,
-                      float e, cudaStream_t st);
+                      const unsigned long long *surv, unsigned long long nhead, unsigned long long head_cap, int k,
+                      ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt = Batch{});
 // FP32-screen form: FP32 samples from FP64 basis tables; FP64 re-check.
 void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
-                           cudaStream_t st);
+                           cudaStream_t st, const Batch &bt = Batch{}, const SurfView<float> *vdev = nullptr);
+// stats set: the candidate count is read on the device (capped at cap).
 void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
                         const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,
-                        long long n, DistCand<double> *out, cudaStream_t st);
+                        long long n, DistCand<double> *out, cudaStream_t st, const Batch &bt = Batch{},
+                        const SurfView<double> *va = nullptr, const SurfView<double> *vb = nullptr,
+                        const ScreenStats *stats = nullptr, unsigned long long cap = 0);
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
-                        ScreenStats *stats, cudaStream_t st);
+                        ScreenStats *stats, cudaStream_t st, const Batch &bt = Batch{});
 template <typename T>
 void launch_dist_next(const DistCand<T> *top, ScreenStats *stats, const SideRound<T> &a, const SideRound<T> &b,
                       const int *map1, const int *map2, int nuv_next, RegionRec<T> *next1, RegionRec<T> *next2,
-                      int *nmap1, int *nmap2, cudaStream_t st);
+                      int *nmap1, int *nmap2, cudaStream_t st, const Batch &bt = Batch{});
+// Batched rounds: record a round and restart the counters; choose the
+// threshold-pass list (at most head_cap tile pairs, about `want` with the
+// smallest bounds when more survive).
+template <typename TP>
+void launch_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRecord<TP> *rec, int round,
+                       unsigned long long surv_cap, unsigned long long cand_cap, bool last, cudaStream_t st,
+                       const Batch &bt);
+void launch_dist_pick(const unsigned long long *surv, const unsigned *surv_lb, unsigned long long surv_cap,
+                      unsigned long long *head, unsigned long long head_cap, unsigned want, ScreenStats *stats,
+                      cudaStream_t st, const Batch &bt);
 
 template <typename T>
 void launch_inter_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
@@ -210,10 +265,13 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
 // FP64 Newton refinement.  dom = {u0, u1, v0, v1, s0, s1, t0, t1} (the query
 // rectangles).  Distance: 11 doubles per candidate (d, u, v, s, t, P1, P2);
 // intersection: 8 doubles per pair (x, y, z, u, v, s, t, residual).
+// stats set: the candidate count is the device slot count of the last round.
 template <typename TP>
 void launch_newton_dist(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
                         const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
-                        const DistCand<TP> *top, int n, const double *dom, double *out, cudaStream_t st);
+                        const DistCand<TP> *top, int n, const double *dom, double *out, cudaStream_t st,
+                        const Batch &bt = Batch{}, const SurfView<double> *va = nullptr,
+                        const SurfView<double> *vb = nullptr, const ScreenStats *stats = nullptr);
 template <typename TP>
 void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
                          const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,

@@ -74,6 +74,53 @@ __device__ __forceinline__ long long warp_append(bool pred, unsigned long long *
   return static_cast<long long>(base + __popc(mask & ((1u << lane) - 1u)));
 }
 
+// ---- lockstep batches (see Batch): query = blockIdx.y, slab offset q * qs ----
+__device__ __forceinline__ long long qoff(long long qs) { return static_cast<long long>(blockIdx.y) * qs; }
+
+template <typename P>
+__device__ __forceinline__ P *qsh(P *p, long long off) {
+  return (p && off) ? reinterpret_cast<P *>(reinterpret_cast<uintptr_t>(p) + off) : p;
+}
+
+template <typename T>
+__device__ __forceinline__ SideRound<T> qsh(SideRound<T> s, long long off) {
+  if (!off) return s;
+  s.regions = qsh(s.regions, off);
+  s.spans = qsh(s.spans, off);
+  s.basis = qsh(s.basis, off);
+  s.samples = qsh(s.samples, off);
+  s.kmax = qsh(s.kmax, off);
+  s.pad = qsh(s.pad, off);
+  s.center = qsh(s.center, off);
+  s.half = qsh(s.half, off);
+  s.tlo = qsh(s.tlo, off);
+  s.thi = qsh(s.thi, off);
+  s.thmax = qsh(s.thmax, off);
+  s.stlo = qsh(s.stlo, off);
+  s.sthi = qsh(s.sthi, off);
+  s.dnreg = qsh(s.dnreg, off);
+  return s;
+}
+
+// Region count of a side: on the device in batched refinement rounds.
+template <typename T>
+__device__ __forceinline__ int nreg_of(const SideRound<T> &s) {
+  return s.dnreg ? *s.dnreg : s.nreg;
+}
+
+// Slot count: nslots < 0 means the device count of this round.
+__device__ __forceinline__ int nslots_of(int nslots, const ScreenStats *stats) {
+  return nslots >= 0 ? nslots : stats->nslots;
+}
+
+// A list length given on the host, or (kFromDevice) the device count capped
+// at the list's capacity.
+__device__ __forceinline__ unsigned long long count_of(unsigned long long host, unsigned long long dev,
+                                                       unsigned long long cap) {
+  if (host != kFromDevice) return host;
+  return dev < cap ? dev : cap;
+}
+
 // ---------------------------------------------------------------------------
 // Knot spans and basis functions
 // ---------------------------------------------------------------------------
@@ -157,8 +204,14 @@ __device__ void basis_ders(int span, int p, T u, const T *knots, int nd, T *out,
 }
 
 template <typename T, int MAXP>
-__global__ void k_basis(SurfView<T> s, const RegionRec<T> *regions, int nreg, int nuv, int p1max, int *spans,
-                        T *basis) {
+__global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<T> *regions, int nreg,
+                        const int *dnreg, int nuv, int p1max, int *spans, T *basis, long long qs) {
+  const long long qo = qoff(qs);
+  if (vdev) s = *qsh(vdev, qo);
+  if (dnreg) nreg = *qsh(dnreg, qo);
+  regions = qsh(regions, qo);
+  spans = qsh(spans, qo);
+  basis = qsh(basis, qo);
   const long long total = static_cast<long long>(nreg) * 2 * nuv;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -324,11 +377,14 @@ __device__ __forceinline__ void atomic_max_bits(unsigned long long *addr, T v) {
 }
 
 template <typename T>
-__global__ void k_samples(SurfView<T> s, SideRound<T> sr, int need_k) {
+__global__ void k_samples(SurfView<T> s, const SurfView<T> *vdev, SideRound<T> sr, int need_k, long long qs) {
+  const long long qo = qoff(qs);
+  if (vdev) s = *qsh(vdev, qo);
+  sr = qsh(sr, qo);
   const Geom g = sr.g;
   const int nuv = g.nuv;
   const long long per = static_cast<long long>(nuv) * nuv;
-  const long long total = per * sr.nreg;
+  const long long total = per * nreg_of(sr);
   const int p1 = g.p1max;
   for (long long base = blockIdx.x * static_cast<long long>(blockDim.x); base < total;
        base += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -432,10 +488,11 @@ __device__ __forceinline__ double pos_inf<double>() {
 // are stored without the padding; the screen forms radius = half + pad exactly
 // as the reference does.
 template <typename T>
-__global__ void k_cells(SideRound<T> sr, int intersect) {
+__global__ void k_cells(SideRound<T> sr, int intersect, long long qs) {
+  sr = qsh(sr, qoff(qs));
   const Geom g = sr.g;
   const int lane = threadIdx.x & 31;
-  const long long ntile_total = static_cast<long long>(sr.nreg) * g.ntiles;
+  const long long ntile_total = static_cast<long long>(nreg_of(sr)) * g.ntiles;
   const int te2 = g.te * g.te;
   const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
   for (long long t = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; t < ntile_total;
@@ -685,8 +742,16 @@ __device__ __forceinline__ unsigned warp_sorted_at(unsigned v, int q) {
 // folds the k-th smallest of its per-thread minima into tau.
 template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b, const int *map1,
-                                                  const int *map2, int nslots, int k, ScreenStats *stats, float e) {
+                                                  const int *map2, int nslots, int k, ScreenStats *stats, float e,
+                                                  long long qs) {
   __shared__ unsigned sh[256];
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  nslots = nslots_of(nslots, stats);
   const Geom g1 = a.g, g2 = b.g;
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
   const int nrows = nslots * g1.ntiles;
@@ -708,7 +773,16 @@ __global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b
 template <typename T, bool S>
 __global__ void k_dist_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
                             unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap,
-                            ScreenStats *stats, float e) {
+                            ScreenStats *stats, float e, long long qs) {
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  surv = qsh(surv, qo);
+  surv_lb = qsh(surv_lb, qo);
+  nslots = nslots_of(nslots, stats);
   const Geom g1 = a.g, g2 = b.g;
   const int nrows = nslots * g1.ntiles;
   const T tau = thr_compare<T, S>(stats->tau_bits, e);
@@ -759,9 +833,21 @@ __device__ __forceinline__ Vec4<T> shfl_vec(const Vec4<T> &v, int src) {
 template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2,
                                                    const unsigned long long *surv, const unsigned *surv_lb,
-                                                   unsigned long long nsurv, int k, int collect, DistCand<T> *cand,
-                                                   unsigned long long cand_cap, ScreenStats *stats, float e) {
+                                                   unsigned long long nsurv, unsigned long long surv_cap,
+                                                   int sorted, int k, int collect, DistCand<T> *cand,
+                                                   unsigned long long cand_cap, ScreenStats *stats, float e,
+                                                   long long qs) {
   __shared__ unsigned sh[256];
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  surv = qsh(surv, qo);
+  surv_lb = qsh(surv_lb, qo);
+  cand = qsh(cand, qo);
+  nsurv = count_of(nsurv, stats->survivors, surv_cap);
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
   const int n1 = te1 * te1, n2 = te2 * te2;
@@ -769,14 +855,26 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
   unsigned long long tests = 0;
   T best = pos_inf<T>();
   const Vec4<T> far4{pos_inf<T>(), pos_inf<T>(), pos_inf<T>(), T(0)};
+  // Sorted lists are taken in order from a work counter (a bound above tau
+  // ends the warp); unsorted lists are split statically and skip such pairs.
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long wnext = (blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x) >> 5;
   for (;;) {
     unsigned long long w = 0;
-    if (lane == 0) w = atomicAdd(&stats->work, 1ull);
-    w = __shfl_sync(kFull, w, 0);
+    if (sorted) {
+      if (lane == 0) w = atomicAdd(&stats->work, 1ull);
+      w = __shfl_sync(kFull, w, 0);
+    } else {
+      w = wnext;
+      wnext += nwarps;
+    }
     if (w >= nsurv) break;
     const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
     const T tau = thr_compare<T, S>(taub, e);
-    if (surv_lb && __uint_as_float(surv_lb[w]) > static_cast<float>(thr_compare<float, S>(taub, e))) break;
+    if (surv_lb && __uint_as_float(surv_lb[w]) > static_cast<float>(thr_compare<float, S>(taub, e))) {
+      if (sorted) break;
+      continue;
+    }
     const unsigned long long q = surv[w];
     const int row = static_cast<int>(q >> 32), t2 = static_cast<int>(q & 0xffffffffull);
     const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
@@ -839,7 +937,16 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
 template <typename T, int KL, bool S>
 __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> b, const int *map1,
                                                    const int *map2, const unsigned long long *surv,
-                                                   unsigned long long nhead, int k, ScreenStats *stats, float e) {
+                                                   unsigned long long nhead, int k, ScreenStats *stats, float e,
+                                                   long long qs) {
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  surv = qsh(surv, qo);
+  nhead = count_of(nhead, stats->nhead, stats->nhead);
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
   const int n1 = te1 * te1, n2 = te2 * te2;
@@ -905,10 +1012,11 @@ __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> 
 
 // Bounds of every supertile (8 x 8 tiles): one warp reduces its <= 64 tiles.
 template <typename T>
-__global__ void k_supertiles(SideRound<T> sr) {
+__global__ void k_supertiles(SideRound<T> sr, long long qs) {
+  sr = qsh(sr, qoff(qs));
   const Geom g = sr.g;
   const int lane = threadIdx.x & 31;
-  const long long total = static_cast<long long>(sr.nreg) * g.nst;
+  const long long total = static_cast<long long>(nreg_of(sr)) * g.nst;
   const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
   for (long long w = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; w < total; w += nwarps) {
     const int r = static_cast<int>(w / g.nst), st = static_cast<int>(w - static_cast<long long>(r) * g.nst);
@@ -953,8 +1061,16 @@ __device__ __forceinline__ long long super_rep(int r, int st, const Geom &g) {
 
 template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_tau_st(SideRound<T> a, SideRound<T> b, const int *map1,
-                                                     const int *map2, int nslots, int k, ScreenStats *stats, float e) {
+                                                     const int *map2, int nslots, int k, ScreenStats *stats, float e,
+                                                     long long qs) {
   __shared__ unsigned sh[256];
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  nslots = nslots_of(nslots, stats);
   const Geom g1 = a.g, g2 = b.g;
   const int nrows = nslots * g1.nst;
   float best = __uint_as_float(0x7f800000u);
@@ -971,7 +1087,16 @@ __global__ void __launch_bounds__(256) k_dist_tau_st(SideRound<T> a, SideRound<T
 
 template <typename T, bool S>
 __global__ void k_dist_cull_st(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
-                               unsigned long long *surv, unsigned long long cap, ScreenStats *stats, float e) {
+                               unsigned long long *surv, unsigned long long cap, ScreenStats *stats, float e,
+                               long long qs) {
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  surv = qsh(surv, qo);
+  nslots = nslots_of(nslots, stats);
   const Geom g1 = a.g, g2 = b.g;
   const int nrows = nslots * g1.nst;
   const T tau = thr_compare<T, S>(stats->tau_bits, e);
@@ -995,55 +1120,68 @@ __global__ void k_dist_cull_st(SideRound<T> a, SideRound<T> b, const int *map1, 
   }
 }
 
-// One block per surviving supertile pair; its <= 64 x 64 child tile pairs.
+// Surviving supertile pairs expanded into their <= 64 x 64 child tile pairs,
+// in chunks of 256 child pairs per block iteration (16 chunks per supertile
+// pair, so that a few survivors still spread over many SMs).
 // cull = 0: fold the representative distances into tau; cull = 1: append the
 // tile pairs whose bound passes tau, with the bound as sort key (the same
 // format k_dist_cull writes).
 template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_expand(SideRound<T> a, SideRound<T> b, const int *map1,
                                                      const int *map2, const unsigned long long *st_surv,
-                                                     unsigned long long nst_surv, int k, int cull,
-                                                     unsigned long long *surv, unsigned *surv_lb,
-                                                     unsigned long long cap, ScreenStats *stats, float e) {
+                                                     unsigned long long nst_surv, unsigned long long st_cap, int k,
+                                                     int cull, unsigned long long *surv, unsigned *surv_lb,
+                                                     unsigned long long cap, ScreenStats *stats, float e,
+                                                     long long qs) {
   __shared__ unsigned sh[256];
+  const long long qo = qoff(qs);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  stats = qsh(stats, qo);
+  st_surv = qsh(st_surv, qo);
+  surv = qsh(surv, qo);
+  surv_lb = qsh(surv_lb, qo);
+  nst_surv = count_of(nst_surv, stats->st_survivors, st_cap);
   const Geom g1 = a.g, g2 = b.g;
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
+  constexpr int kChunks = kMaxTile * kMaxTile * kMaxTile * kMaxTile / 256;
   float best = __uint_as_float(0x7f800000u);
   const T tau = thr_compare<T, S>(stats->tau_bits, e);
-  for (unsigned long long w = blockIdx.x; w < nst_surv; w += gridDim.x) {
+  for (unsigned long long it = blockIdx.x; it < nst_surv * kChunks; it += gridDim.x) {
+    const unsigned long long w = it / kChunks;
+    const int c = static_cast<int>(it % kChunks) * 256 + threadIdx.x;
     const unsigned long long q = st_surv[w];
     const int row = static_cast<int>(q >> 32), s2 = static_cast<int>(q & 0xffffffffull);
     const int slot = row / g1.nst, s1 = row - slot * g1.nst;
     const int r1 = map1[slot], r2 = map2[slot];
     const int sy1 = s1 / g1.stw, sx1 = s1 - sy1 * g1.stw, sy2 = s2 / g2.stw, sx2 = s2 - sy2 * g2.stw;
-    for (int c0 = 0; c0 < kMaxTile * kMaxTile * kMaxTile * kMaxTile; c0 += blockDim.x) {
-      const int c = c0 + threadIdx.x;
-      const int l1 = c >> 6, l2 = c & 63;
-      const int ty1 = sy1 * kMaxTile + (l1 >> 3), tx1 = sx1 * kMaxTile + (l1 & 7);
-      const int ty2 = sy2 * kMaxTile + (l2 >> 3), tx2 = sx2 * kMaxTile + (l2 & 7);
-      const bool valid = ty1 < g1.tw && tx1 < g1.tw && ty2 < g2.tw && tx2 < g2.tw;
-      const int t1 = ty1 * g1.tw + tx1, t2 = ty2 * g2.tw + tx2;
-      bool keep = false;
-      T lb = T(0);
-      if (valid) {
-        const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
-        const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
-        if (!cull) {
-          const Vec4<T> c1 = a.center[i1 * n1 + tile_rep(t1, g1)];
-          const Vec4<T> c2 = b.center[i2 * n2 + tile_rep(t2, g2)];
-          best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
-        } else {
-          lb = tile_lb(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
-          if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
-          keep = lb <= tau;
-        }
+    const int l1 = c >> 6, l2 = c & 63;
+    const int ty1 = sy1 * kMaxTile + (l1 >> 3), tx1 = sx1 * kMaxTile + (l1 & 7);
+    const int ty2 = sy2 * kMaxTile + (l2 >> 3), tx2 = sx2 * kMaxTile + (l2 & 7);
+    const bool valid = ty1 < g1.tw && tx1 < g1.tw && ty2 < g2.tw && tx2 < g2.tw;
+    const int t1 = ty1 * g1.tw + tx1, t2 = ty2 * g2.tw + tx2;
+    bool keep = false;
+    T lb = T(0);
+    if (valid) {
+      const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
+      const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
+      if (!cull) {
+        const Vec4<T> c1 = a.center[i1 * n1 + tile_rep(t1, g1)];
+        const Vec4<T> c2 = b.center[i2 * n2 + tile_rep(t2, g2)];
+        best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+      } else {
+        lb = tile_lb(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
+        if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
+        keep = lb <= tau;
       }
-      if (cull) {
-        const long long pos = warp_append(keep, &stats->survivors);
-        if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) {
-          surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + t1), static_cast<unsigned>(t2));
-          surv_lb[pos] = lb_bits_down(lb);
-        }
+    }
+    if (cull) {
+      const long long pos = warp_append(keep, &stats->survivors);
+      if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) {
+        surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + t1), static_cast<unsigned>(t2));
+        surv_lb[pos] = lb_bits_down(lb);
       }
     }
   }
@@ -1062,8 +1200,12 @@ __device__ __forceinline__ bool cand_less(const DistCand<T> &x, const DistCand<T
 // Exact k smallest candidates under the total order, one block of 1024.
 template <typename T>
 __global__ void __launch_bounds__(1024) k_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k,
-                                                      DistCand<T> *out, ScreenStats *stats) {
+                                                      DistCand<T> *out, ScreenStats *stats, long long qs) {
   extern __shared__ unsigned char smem_raw[];
+  const long long qo = qoff(qs);
+  cand = qsh(cand, qo);
+  out = qsh(out, qo);
+  stats = qsh(stats, qo);
   DistCand<T> *buf = reinterpret_cast<DistCand<T> *>(smem_raw);
   __shared__ unsigned hist[256];
   __shared__ unsigned long long s_prefix, s_mask;
@@ -1255,9 +1397,21 @@ __device__ __forceinline__ RegionRec<T> child_rect(const RegionRec<T> &p, int nu
 template <typename T>
 __global__ void __launch_bounds__(1024) k_dist_next(const DistCand<T> *top, ScreenStats *stats, SideRound<T> a,
                                                     SideRound<T> b, const int *map1, const int *map2, int nuv_next,
-                                                    RegionRec<T> *next1, RegionRec<T> *next2, int *nmap1, int *nmap2) {
+                                                    RegionRec<T> *next1, RegionRec<T> *next2, int *nmap1, int *nmap2,
+                                                    long long qs) {
   __shared__ int first1[kMaxK], first2[kMaxK];
   __shared__ int uid1[kMaxK], uid2[kMaxK];
+  const long long qo = qoff(qs);
+  top = qsh(top, qo);
+  stats = qsh(stats, qo);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  next1 = qsh(next1, qo);
+  next2 = qsh(next2, qo);
+  nmap1 = qsh(nmap1, qo);
+  nmap2 = qsh(nmap2, qo);
   const int n = stats->nsel;
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
     const DistCand<T> c = top[e];
@@ -1306,6 +1460,149 @@ __global__ void __launch_bounds__(1024) k_dist_next(const DistCand<T> *top, Scre
     nmap2[e] = u2;
   }
   (void)nuv_next;
+}
+
+// ---- batched distance: round bookkeeping and the threshold-pass list -------
+
+// End of a batched round, one warp per query: the round's counters, status
+// and kept pairs go to the query's record; the kept count becomes the next
+// round's slot count (0 after a failure, which idles the query's later
+// rounds); the counters restart unless this was the last round.
+template <typename TP>
+__global__ void k_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRecord<TP> *rec, int round,
+                             unsigned long long surv_cap, unsigned long long cand_cap, int last, long long qs) {
+  const long long qo = qoff(qs);
+  stats = qsh(stats, qo);
+  top = qsh(top, qo);
+  rec = qsh(rec, qo);
+  const int t = threadIdx.x;
+  int st = stats->status;
+  if (st == 0 && (stats->survivors > surv_cap || stats->candidates > cand_cap)) st = kStatusCapacity;
+  const int n = st == 0 ? stats->nsel : 0;
+  if (t < n && t < kBatchK) rec->top[round][t] = top[t];
+  const unsigned long long tests = stats->pair_tests, cands = stats->candidates, surv = stats->survivors;
+  __syncwarp();
+  if (t == 0) {
+    rec->tests[round] = static_cast<long long>(tests);
+    rec->cands[round] = static_cast<long long>(cands);
+    rec->survivors[round] = surv;
+    rec->npairs[round] = n;
+    rec->status[round] = st;
+    stats->nslots = n;
+    if (!last) {
+      stats->tile_pairs = 0;
+      stats->survivors = 0;
+      stats->pair_tests = 0;
+      stats->candidates = 0;
+      stats->tau_bits = 0x7f800000u;
+      stats->status = 0;
+      stats->nsel = 0;
+      stats->work = 0;
+      stats->st_survivors = 0;
+      stats->nhead = 0;
+    }
+  }
+}
+
+// Block-wide search over 4096 counts for the bin where the running total
+// reaches want: *bin and the count still needed inside it (1024 threads).
+__device__ void find_crossing(const unsigned *hist, unsigned want, unsigned *s_warp, int *s_bin, unsigned *s_need) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const unsigned h0 = hist[4 * t], h1 = hist[4 * t + 1], h2 = hist[4 * t + 2], h3 = hist[4 * t + 3];
+  const unsigned sum = h0 + h1 + h2 + h3;
+  unsigned inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned v = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned w = s_warp[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned v = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += v;
+    }
+    s_warp[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const unsigned before = (warp ? s_warp[warp - 1] : 0u) + inc - sum;
+  if (before < want && before + sum >= want) {
+    unsigned c = before;
+    int b = 4 * t;
+    if (c + h0 < want) {
+      c += h0;
+      ++b;
+      if (c + h1 < want) {
+        c += h1;
+        ++b;
+        if (c + h2 < want) {
+          c += h2;
+          ++b;
+        }
+      }
+    }
+    *s_bin = b;
+    *s_need = want - c;
+  }
+  __syncthreads();
+}
+
+// Threshold-pass list of a batched round, one block of 1024 per query: all
+// surviving tile pairs when at most head_cap survive, else about `want` of
+// them with the smallest bounds (two-level radix select on the bound bits),
+// so the exact per-tile-pair k-th starts from the closest tile pairs.
+__global__ void __launch_bounds__(1024) k_dist_pick(const unsigned long long *surv, const unsigned *surv_lb,
+                                                    unsigned long long surv_cap, unsigned long long *head,
+                                                    unsigned long long head_cap, unsigned want, ScreenStats *stats,
+                                                    long long qs) {
+  __shared__ unsigned hist[4096];
+  __shared__ unsigned s_warp[32], s_need, s_cnt;
+  __shared__ int s_bin;
+  const long long qo = qoff(qs);
+  surv = qsh(surv, qo);
+  surv_lb = qsh(surv_lb, qo);
+  head = qsh(head, qo);
+  stats = qsh(stats, qo);
+  const unsigned long long n = count_of(kFromDevice, stats->survivors, surv_cap);
+  if (n <= head_cap) {
+    for (unsigned long long e = threadIdx.x; e < n; e += blockDim.x) head[e] = surv[e];
+    if (threadIdx.x == 0) stats->nhead = n;
+    return;
+  }
+  for (int b = threadIdx.x; b < 4096; b += blockDim.x) hist[b] = 0;
+  if (threadIdx.x == 0) {
+    s_bin = 4095;
+    s_need = want;
+  }
+  __syncthreads();
+  for (unsigned long long e = threadIdx.x; e < n; e += blockDim.x) atomicAdd(&hist[surv_lb[e] >> 20], 1u);
+  __syncthreads();
+  find_crossing(hist, want, s_warp, &s_bin, &s_need);
+  const unsigned b1 = static_cast<unsigned>(s_bin), need = s_need;
+  for (int b = threadIdx.x; b < 4096; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  for (unsigned long long e = threadIdx.x; e < n; e += blockDim.x) {
+    const unsigned key = surv_lb[e];
+    if ((key >> 20) == b1) atomicAdd(&hist[(key >> 8) & 4095u], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) s_bin = 4095;
+  __syncthreads();
+  find_crossing(hist, need, s_warp, &s_bin, &s_need);
+  const unsigned thr = (b1 << 12) | static_cast<unsigned>(s_bin);
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  for (unsigned long long e = threadIdx.x; e < n; e += blockDim.x) {
+    if ((surv_lb[e] >> 8) <= thr) {
+      const unsigned pos = atomicAdd(&s_cnt, 1u);
+      if (pos < head_cap) head[pos] = surv[e];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) stats->nhead = s_cnt < head_cap ? s_cnt : head_cap;
 }
 
 // ---------------------------------------------------------------------------
@@ -1494,11 +1791,16 @@ __global__ void k_inter_side2(const unsigned long long *key2s, const int *idxs, 
 // form uses) are rounded to FP32 and contracted with FMAs against the FP32
 // control net; rational surfaces divide by the weight in FP64.  The host
 // bounds |P32 - P64| per coordinate from the operation count.
-__global__ void k_samples_screen(SurfView<float> s, SideRound<double> basis_side, SideRound<float> out) {
+__global__ void k_samples_screen(SurfView<float> s, const SurfView<float> *vdev, SideRound<double> basis_side,
+                                 SideRound<float> out, long long qs) {
+  const long long qo = qoff(qs);
+  if (vdev) s = *qsh(vdev, qo);
+  basis_side = qsh(basis_side, qo);
+  out = qsh(out, qo);
   const Geom g = basis_side.g;
   const int nuv = g.nuv;
   const long long per = static_cast<long long>(nuv) * nuv;
-  const long long total = per * basis_side.nreg;
+  const long long total = per * nreg_of(basis_side);
   const int p1 = g.p1max;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -1577,9 +1879,20 @@ __device__ Vec4<double> cell_center64(const SurfView<double> &s, const SideRound
 }
 
 // Re-check of the screened candidates in FP64: the FP64 form's d2 of each.
-__global__ void k_dist_verify(SurfView<double> sa, SurfView<double> sb, SideRound<double> a, SideRound<double> b,
-                              const int *map1, const int *map2, const DistCand<float> *cand, long long n,
-                              DistCand<double> *out) {
+__global__ void k_dist_verify(SurfView<double> sa, SurfView<double> sb, const SurfView<double> *va,
+                              const SurfView<double> *vb, SideRound<double> a, SideRound<double> b, const int *map1,
+                              const int *map2, const DistCand<float> *cand, long long n, unsigned long long cap,
+                              const ScreenStats *stats, DistCand<double> *out, long long qs) {
+  const long long qo = qoff(qs);
+  if (va) sa = *qsh(va, qo);
+  if (vb) sb = *qsh(vb, qo);
+  a = qsh(a, qo);
+  b = qsh(b, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  cand = qsh(cand, qo);
+  out = qsh(out, qo);
+  if (stats) n = static_cast<long long>(count_of(kFromDevice, qsh(stats, qo)->candidates, cap));
   for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < n;
        e += static_cast<long long>(gridDim.x) * blockDim.x) {
     const DistCand<float> c = cand[e];
@@ -1721,9 +2034,21 @@ __device__ void newton_distance(const SurfView<double> &sa, const SurfView<doubl
 
 // One thread per final candidate pair: cell centres as the starting point.
 template <typename TP>
-__global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
-                              const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
-                              const DistCand<TP> *top, int n, const double *dom, double *out) {
+__global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const SurfView<double> *va,
+                              const SurfView<double> *vb, const RegionRec<TP> *reg1, const RegionRec<TP> *reg2,
+                              const int *map1, const int *map2, int nuv1, int nuv2, const DistCand<TP> *top, int n,
+                              const ScreenStats *stats, const double *dom, double *out, long long qs) {
+  const long long qo = qoff(qs);
+  if (va) sa = *qsh(va, qo);
+  if (vb) sb = *qsh(vb, qo);
+  reg1 = qsh(reg1, qo);
+  reg2 = qsh(reg2, qo);
+  map1 = qsh(map1, qo);
+  map2 = qsh(map2, qo);
+  top = qsh(top, qo);
+  dom = qsh(dom, qo);
+  out = qsh(out, qo);
+  if (stats) n = qsh(stats, qo)->nslots;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   const DistCand<TP> c = top[e];
@@ -1822,24 +2147,39 @@ unsigned long long launch_count() { return g_launches.load(std::memory_order_rel
 // Launchers
 // ---------------------------------------------------------------------------
 
+// Blocks per query: the single-query grid, shrunk so that a batch of bt.n
+// queries stays within max_total blocks.
+inline int bgrid(long long want, const Batch &bt, int max_total) {
+  long long g = want < 1 ? 1 : want;
+  const long long per = max_total / (bt.n > 0 ? bt.n : 1);
+  if (g > per) g = per;
+  if (g < 1) g = 1;
+  return static_cast<int>(g);
+}
+
+inline dim3 bdim(int gx, const Batch &bt) { return dim3(static_cast<unsigned>(gx), static_cast<unsigned>(bt.n), 1u); }
+
 template <typename T>
-void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st) {
+void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt,
+                  const SurfView<T> *vdev) {
   counted();
   const long long n = static_cast<long long>(sr.nreg) * 2 * sr.g.nuv;
+  // Degrees are part of a batch's shape: the host view decides the variant.
   const int maxdeg = s.degu > s.degv ? s.degu : s.degv;
   if (maxdeg < 8)
-    k_basis<T, 9><<<grid_for(n, 128), 128, 0, st>>>(s, sr.regions, sr.nreg, sr.g.nuv, sr.g.p1max, sr.spans,
-                                                     sr.basis);
+    k_basis<T, 9><<<bdim(bgrid((n + 127) / 128, bt, 148 * 16), bt), 128, 0, st>>>(
+        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs);
   else
-    k_basis<T, kMaxDeg + 1><<<grid_for(n, 64), 64, 0, st>>>(s, sr.regions, sr.nreg, sr.g.nuv, sr.g.p1max,
-                                                             sr.spans, sr.basis);
+    k_basis<T, kMaxDeg + 1><<<bdim(bgrid((n + 63) / 64, bt, 148 * 16), bt), 64, 0, st>>>(
+        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs);
 }
 
 template <typename T>
-void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st) {
+void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st, const Batch &bt,
+                    const SurfView<T> *vdev) {
   counted();
   const long long n = static_cast<long long>(sr.nreg) * sr.g.nuv * sr.g.nuv;
-  k_samples<T><<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, sr, need_k ? 1 : 0);
+  k_samples<T><<<bdim(bgrid((n + 127) / 128, bt, 148 * 32), bt), 128, 0, st>>>(s, vdev, sr, need_k ? 1 : 0, bt.qs);
 }
 
 template <typename T>
@@ -1849,10 +2189,10 @@ void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaSt
 }
 
 template <typename T>
-void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st) {
+void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st, const Batch &bt) {
   counted();
   const long long warps = static_cast<long long>(sr.nreg) * sr.g.ntiles;
-  k_cells<T><<<grid_for(warps * 32, 256, 148 * 32), 256, 0, st>>>(sr, intersect ? 1 : 0);
+  k_cells<T><<<bdim(bgrid((warps + 7) / 8, bt, 148 * 32), bt), 256, 0, st>>>(sr, intersect ? 1 : 0, bt.qs);
 }
 
 template <typename T>
@@ -1862,135 +2202,146 @@ void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, 
   k_records<T><<<grid_for(n, 64, 148 * 32), 64, 0, st>>>(s, ustep, vstep, ustart, vstart, nuv, out);
 }
 
+// nslots < 0: the slot count is read on the device; the host passes the
+// largest it can be as -(max slots).
+inline int rows_for(int nslots, int per_slot) { return (nslots < 0 ? -nslots : nslots) * per_slot; }
+inline int dev_slots(int nslots) { return nslots < 0 ? -1 : nslots; }
+
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                     int k, ScreenStats *stats, bool screen, float e, cudaStream_t st) {
+                     int k, ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
-  const int rows = nslots * a.g.ntiles;
-  const int grid = rows < 148 * 8 ? rows : 148 * 8;
+  const dim3 grid = bdim(bgrid(rows_for(nslots, a.g.ntiles), bt, 148 * 8), bt);
+  const int ns = dev_slots(nslots);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_tau<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+      k_dist_tau<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, ns, k, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_tau<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+  k_dist_tau<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, ns, k, stats, e, bt.qs);
 }
 
 template <typename T>
 void launch_dist_cull(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                       unsigned long long *surv, unsigned *surv_lb, unsigned long long surv_cap, ScreenStats *stats,
-                      bool screen, float e, cudaStream_t st) {
+                      bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
-  const int rows = nslots * a.g.ntiles;
-  const int block = b.g.ntiles >= 256 ? 256 : (b.g.ntiles >= 128 ? 128 : 64);
-  const int grid = rows < 148 * 16 ? rows : 148 * 16;
+  const int block = b.g.ntiles >= 256 ? 256 : (b.g.ntiles >= 128 ? 128 : (b.g.ntiles >= 64 ? 64 : 32));
+  const dim3 grid = bdim(bgrid(rows_for(nslots, a.g.ntiles), bt, 148 * 16), bt);
+  const int ns = dev_slots(nslots);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_cull<float, true><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, surv_lb, surv_cap, stats, e);
+      k_dist_cull<float, true><<<grid, block, 0, st>>>(a, b, map1, map2, ns, surv, surv_lb, surv_cap, stats, e,
+                                                       bt.qs);
       return;
     }
   }
-  k_dist_cull<T, false><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, surv_lb, surv_cap, stats, e);
+  k_dist_cull<T, false><<<grid, block, 0, st>>>(a, b, map1, map2, ns, surv, surv_lb, surv_cap, stats, e, bt.qs);
 }
 
 template <typename T>
 void launch_dist_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                      const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv, int k,
-                      int collect, DistCand<T> *cand, unsigned long long cand_cap, ScreenStats *stats, bool screen,
-                      float e, cudaStream_t st) {
+                      const unsigned long long *surv, const unsigned *surv_lb, unsigned long long nsurv,
+                      unsigned long long surv_cap, bool sorted, int k, int collect, DistCand<T> *cand,
+                      unsigned long long cand_cap, ScreenStats *stats, bool screen, float e, cudaStream_t st,
+                      const Batch &bt) {
   counted();
   if (nsurv == 0) return;
-  const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
-  const int blocks = static_cast<int>((warps + 7) / 8);
+  const unsigned long long most = nsurv == kFromDevice ? surv_cap : nsurv;
+  const unsigned long long warps = most < 148ull * 64 ? most : 148ull * 64;
+  const dim3 grid = bdim(bgrid(static_cast<long long>((warps + 7) / 8), bt, 148 * 8), bt);
+  const int so = sorted ? 1 : 0;
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_leaf<float, true><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, collect, cand,
-                                                       cand_cap, stats, e);
+      k_dist_leaf<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, surv_cap, so, k, collect,
+                                                     cand, cand_cap, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_leaf<T, false><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, k, collect, cand, cand_cap,
-                                                stats, e);
+  k_dist_leaf<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, surv, surv_lb, nsurv, surv_cap, so, k, collect, cand,
+                                              cand_cap, stats, e, bt.qs);
 }
 
 template <typename T>
-void launch_supertiles(const SideRound<T> &sr, cudaStream_t st) {
+void launch_supertiles(const SideRound<T> &sr, cudaStream_t st, const Batch &bt) {
   counted();
   const long long warps = static_cast<long long>(sr.nreg) * sr.g.nst;
-  k_supertiles<T><<<grid_for(warps * 32, 256, 148 * 32), 256, 0, st>>>(sr);
+  k_supertiles<T><<<bdim(bgrid((warps + 7) / 8, bt, 148 * 32), bt), 256, 0, st>>>(sr, bt.qs);
 }
 
 template <typename T>
 void launch_dist_tau_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
-                        int k, ScreenStats *stats, bool screen, float e, cudaStream_t st) {
+                        int k, ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
-  const int rows = nslots * a.g.nst;
-  const int grid = rows < 148 * 8 ? rows : 148 * 8;
+  const dim3 grid = bdim(bgrid(rows_for(nslots, a.g.nst), bt, 148 * 8), bt);
+  const int ns = dev_slots(nslots);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_tau_st<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+      k_dist_tau_st<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, ns, k, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_tau_st<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, nslots, k, stats, e);
+  k_dist_tau_st<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, ns, k, stats, e, bt.qs);
 }
 
 template <typename T>
 void launch_dist_cull_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                          unsigned long long *surv, unsigned long long cap, ScreenStats *stats, bool screen, float e,
-                         cudaStream_t st) {
+                         cudaStream_t st, const Batch &bt) {
   counted();
-  const int rows = nslots * a.g.nst;
-  const int grid = rows < 148 * 16 ? rows : 148 * 16;
-  const int block = b.g.nst >= 256 ? 256 : (b.g.nst >= 128 ? 128 : 64);
+  const dim3 grid = bdim(bgrid(rows_for(nslots, a.g.nst), bt, 148 * 16), bt);
+  const int block = b.g.nst >= 256 ? 256 : (b.g.nst >= 128 ? 128 : (b.g.nst >= 64 ? 64 : 32));
+  const int ns = dev_slots(nslots);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_cull_st<float, true><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, cap, stats, e);
+      k_dist_cull_st<float, true><<<grid, block, 0, st>>>(a, b, map1, map2, ns, surv, cap, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_cull_st<T, false><<<grid, block, 0, st>>>(a, b, map1, map2, nslots, surv, cap, stats, e);
+  k_dist_cull_st<T, false><<<grid, block, 0, st>>>(a, b, map1, map2, ns, surv, cap, stats, e, bt.qs);
 }
 
 template <typename T>
 void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                        const unsigned long long *st_surv, unsigned long long nst_surv, int k, int cull,
-                        unsigned long long *surv, unsigned *surv_lb, unsigned long long cap, ScreenStats *stats,
-                        bool screen, float e, cudaStream_t st) {
+                        const unsigned long long *st_surv, unsigned long long nst_surv, unsigned long long st_cap,
+                        int k, int cull, unsigned long long *surv, unsigned *surv_lb, unsigned long long cap,
+                        ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
   if (nst_surv == 0) return;
-  const int grid = static_cast<int>(nst_surv < 148ull * 8 ? nst_surv : 148ull * 8);
+  const unsigned long long most = (nst_surv == kFromDevice ? st_cap : nst_surv) * 16ull;
+  const dim3 grid = bdim(bgrid(static_cast<long long>(most < 148ull * 8 ? most : 148ull * 8), bt, 148 * 8), bt);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_expand<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, k, cull, surv, surv_lb,
-                                                        cap, stats, e);
+      k_dist_expand<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, st_cap, k, cull, surv,
+                                                        surv_lb, cap, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_expand<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, k, cull, surv, surv_lb, cap,
-                                                 stats, e);
+  k_dist_expand<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, st_cap, k, cull, surv, surv_lb,
+                                                 cap, stats, e, bt.qs);
 }
 
 template <typename T>
 void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
-                      const unsigned long long *surv, unsigned long long nhead, int k, ScreenStats *stats, bool screen,
-                      float e, cudaStream_t st) {
+                      const unsigned long long *surv, unsigned long long nhead, unsigned long long head_cap, int k,
+                      ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
   if (nhead == 0) return;
-  const int blocks = static_cast<int>((nhead + 7) / 8);
+  const unsigned long long most = nhead == kFromDevice ? head_cap : nhead;
+  const dim3 grid = bdim(bgrid(static_cast<long long>((most + 7) / 8), bt, 148 * 8), bt);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_head<float, 8, true><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats, e);
+      k_dist_head<float, 8, true><<<grid, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_head<T, 8, false><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats, e);
+  k_dist_head<T, 8, false><<<grid, 256, 0, st>>>(a, b, map1, map2, surv, nhead, k, stats, e, bt.qs);
 }
 
 template <typename T>
 void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, int k, DistCand<T> *out,
-                        ScreenStats *stats, cudaStream_t st) {
+                        ScreenStats *stats, cudaStream_t st, const Batch &bt) {
   counted();
   const size_t smem = sizeof(DistCand<T>) * kSelectCap;
   static bool configured = false;
@@ -1998,15 +2349,31 @@ void launch_dist_select(const DistCand<T> *cand, unsigned long long cand_cap, in
     cudaFuncSetAttribute(k_dist_select<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     configured = true;
   }
-  k_dist_select<T><<<1, 1024, smem, st>>>(cand, cand_cap, k, out, stats);
+  k_dist_select<T><<<bdim(1, bt), 1024, smem, st>>>(cand, cand_cap, k, out, stats, bt.qs);
 }
 
 template <typename T>
 void launch_dist_next(const DistCand<T> *top, ScreenStats *stats, const SideRound<T> &a, const SideRound<T> &b,
                       const int *map1, const int *map2, int nuv_next, RegionRec<T> *next1, RegionRec<T> *next2,
-                      int *nmap1, int *nmap2, cudaStream_t st) {
+                      int *nmap1, int *nmap2, cudaStream_t st, const Batch &bt) {
   counted();
-  k_dist_next<T><<<1, 1024, 0, st>>>(top, stats, a, b, map1, map2, nuv_next, next1, next2, nmap1, nmap2);
+  k_dist_next<T><<<bdim(1, bt), 1024, 0, st>>>(top, stats, a, b, map1, map2, nuv_next, next1, next2, nmap1, nmap2,
+                                               bt.qs);
+}
+
+template <typename TP>
+void launch_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRecord<TP> *rec, int round,
+                       unsigned long long surv_cap, unsigned long long cand_cap, bool last, cudaStream_t st,
+                       const Batch &bt) {
+  counted();
+  k_dist_close<TP><<<bdim(1, bt), 32, 0, st>>>(stats, top, rec, round, surv_cap, cand_cap, last ? 1 : 0, bt.qs);
+}
+
+void launch_dist_pick(const unsigned long long *surv, const unsigned *surv_lb, unsigned long long surv_cap,
+                      unsigned long long *head, unsigned long long head_cap, unsigned want, ScreenStats *stats,
+                      cudaStream_t st, const Batch &bt) {
+  counted();
+  k_dist_pick<<<bdim(1, bt), 1024, 0, st>>>(surv, surv_lb, surv_cap, head, head_cap, want, stats, bt.qs);
 }
 
 template <typename T>
@@ -2056,27 +2423,34 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
 }
 
 void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
-                           cudaStream_t st) {
+                           cudaStream_t st, const Batch &bt, const SurfView<float> *vdev) {
   counted();
   const long long n = static_cast<long long>(basis_side.nreg) * basis_side.g.nuv * basis_side.g.nuv;
-  k_samples_screen<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, basis_side, out);
+  k_samples_screen<<<bdim(bgrid((n + 127) / 128, bt, 148 * 32), bt), 128, 0, st>>>(s, vdev, basis_side, out, bt.qs);
 }
 
 void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
                         const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,
-                        long long n, DistCand<double> *out, cudaStream_t st) {
+                        long long n, DistCand<double> *out, cudaStream_t st, const Batch &bt,
+                        const SurfView<double> *va, const SurfView<double> *vb, const ScreenStats *stats,
+                        unsigned long long cap) {
   counted();
-  if (n <= 0) return;
-  k_dist_verify<<<grid_for(n, 128), 128, 0, st>>>(sa, sb, a, b, map1, map2, cand, n, out);
+  if (n <= 0 && !stats) return;
+  const long long most = stats ? static_cast<long long>(cap) : n;
+  k_dist_verify<<<bdim(bgrid((most + 127) / 128, bt, 148 * 16), bt), 128, 0, st>>>(sa, sb, va, vb, a, b, map1, map2,
+                                                                                   cand, n, cap, stats, out, bt.qs);
 }
 
 template <typename TP>
 void launch_newton_dist(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<TP> *reg1,
                         const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
-                        const DistCand<TP> *top, int n, const double *dom, double *out, cudaStream_t st) {
+                        const DistCand<TP> *top, int n, const double *dom, double *out, cudaStream_t st,
+                        const Batch &bt, const SurfView<double> *va, const SurfView<double> *vb,
+                        const ScreenStats *stats) {
   counted();
   if (n <= 0) return;
-  k_newton_dist<TP><<<(n + 63) / 64, 64, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, top, n, dom, out);
+  k_newton_dist<TP><<<bdim((n + 63) / 64, bt), 64, 0, st>>>(sa, sb, va, vb, reg1, reg2, map1, map2, nuv1, nuv2, top, n,
+                                                            stats, dom, out, bt.qs);
 }
 
 template <typename TP>
@@ -2091,38 +2465,42 @@ void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb,
 }
 
 #define JSI_INSTANTIATE(T)                                                                                        \
-  template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t);                         \
-  template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t);                 \
+  template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t, const Batch &,           \
+                                const SurfView<T> *);                                                             \
+  template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t, const Batch &,   \
+                                  const SurfView<T> *);                                                           \
   template void launch_pad<T>(const SideRound<T> &, bool, T, T, cudaStream_t);                                    \
-  template void launch_cells<T>(const SideRound<T> &, bool, cudaStream_t);                                        \
+  template void launch_cells<T>(const SideRound<T> &, bool, cudaStream_t, const Batch &);                         \
   template void launch_records<T>(const SurfView<T> &, T, T, T, T, int, T *, cudaStream_t);                       \
   template void launch_dist_tau<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, int, \
-                                   ScreenStats *, bool, float, cudaStream_t);                                     \
+                                   ScreenStats *, bool, float, cudaStream_t, const Batch &);                      \
   template void launch_dist_cull<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,    \
                                     unsigned long long *, unsigned *, unsigned long long, ScreenStats *, bool,    \
-                                    float, cudaStream_t);                                                         \
+                                    float, cudaStream_t, const Batch &);                                          \
   template void launch_dist_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
-                                    const unsigned long long *, const unsigned *, unsigned long long, int, int,   \
-                                    DistCand<T> *, unsigned long long, ScreenStats *, bool, float,               \
-                                    cudaStream_t);                                                                \
-  template void launch_supertiles<T>(const SideRound<T> &, cudaStream_t);                                         \
+                                    const unsigned long long *, const unsigned *, unsigned long long,             \
+                                    unsigned long long, bool, int, int, DistCand<T> *, unsigned long long,        \
+                                    ScreenStats *, bool, float, cudaStream_t, const Batch &);                     \
+  template void launch_supertiles<T>(const SideRound<T> &, cudaStream_t, const Batch &);                          \
   template void launch_dist_tau_st<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,  \
-                                      int, ScreenStats *, bool, float, cudaStream_t);                             \
+                                      int, ScreenStats *, bool, float, cudaStream_t, const Batch &);              \
   template void launch_dist_cull_st<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, \
                                        unsigned long long *, unsigned long long, ScreenStats *, bool, float,      \
-                                       cudaStream_t);                                                             \
+                                       cudaStream_t, const Batch &);                                              \
   template void launch_dist_expand<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,       \
-                                      const unsigned long long *, unsigned long long, int, int,                   \
-                                      unsigned long long *, unsigned *, unsigned long long, ScreenStats *, bool,  \
-                                      float, cudaStream_t);                                                       \
+                                      const unsigned long long *, unsigned long long, unsigned long long, int,    \
+                                      int, unsigned long long *, unsigned *, unsigned long long, ScreenStats *,   \
+                                      bool, float, cudaStream_t, const Batch &);                                  \
   template void launch_dist_head<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,         \
-                                    const unsigned long long *, unsigned long long, int, ScreenStats *, bool,     \
-                                    float, cudaStream_t);                                                         \
+                                    const unsigned long long *, unsigned long long, unsigned long long, int,      \
+                                    ScreenStats *, bool, float, cudaStream_t, const Batch &);                     \
   template void launch_dist_select<T>(const DistCand<T> *, unsigned long long, int, DistCand<T> *, ScreenStats *, \
-                                      cudaStream_t);                                                              \
+                                      cudaStream_t, const Batch &);                                               \
   template void launch_dist_next<T>(const DistCand<T> *, ScreenStats *, const SideRound<T> &,                     \
                                     const SideRound<T> &, const int *, const int *, int, RegionRec<T> *,          \
-                                    RegionRec<T> *, int *, int *, cudaStream_t);                                  \
+                                    RegionRec<T> *, int *, int *, cudaStream_t, const Batch &);                   \
+  template void launch_dist_close<T>(ScreenStats *, const DistCand<T> *, DistRecord<T> *, int,                    \
+                                     unsigned long long, unsigned long long, bool, cudaStream_t, const Batch &);  \
   template void launch_inter_cull<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int,   \
                                      unsigned long long *, unsigned long long, ScreenStats *, cudaStream_t);      \
   template void launch_inter_leaf<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *,        \
@@ -2140,11 +2518,14 @@ JSI_INSTANTIATE(double)
 
 template void launch_newton_dist<float>(const SurfView<double> &, const SurfView<double> &, const RegionRec<float> *,
                                         const RegionRec<float> *, const int *, const int *, int, int,
-                                        const DistCand<float> *, int, const double *, double *, cudaStream_t);
+                                        const DistCand<float> *, int, const double *, double *, cudaStream_t,
+                                        const Batch &, const SurfView<double> *, const SurfView<double> *,
+                                        const ScreenStats *);
 template void launch_newton_dist<double>(const SurfView<double> &, const SurfView<double> &,
                                          const RegionRec<double> *, const RegionRec<double> *, const int *,
                                          const int *, int, int, const DistCand<double> *, int, const double *,
-                                         double *, cudaStream_t);
+                                         double *, cudaStream_t, const Batch &, const SurfView<double> *,
+                                         const SurfView<double> *, const ScreenStats *);
 template void launch_newton_inter<float>(const SurfView<double> &, const SurfView<double> &, const RegionRec<float> *,
                                          const RegionRec<float> *, const int *, const int *, int, int,
                                          const unsigned long long *, long long, int, const double *, double *,

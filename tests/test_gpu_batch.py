@@ -1,0 +1,166 @@
+"""Lockstep batches of distance queries (one launch per stage for a whole
+batch of same-shape queries): every result equals the same query run alone
+on the per-query path, bit for bit, including the per-round kept pairs, the
+Newton refinement and queries that overflow a batch list and are re-run."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rect32
+from jsi_cad_next_versions_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = ["v5_fp32", "fp64", "fp32_screen"]
+
+
+def _upload_pairs(ctx, pairs, nuv):
+    tasks = []
+    for a, b in pairs:
+        sa, sb = ctx.upload(a), ctx.upload(b)
+        tasks.append((ctx.task(sa, rect32(a), nuv, 1), ctx.task(sb, rect32(b), nuv, 2)))
+    return tasks
+
+
+def _hard_wave_pairs(n, seed0=100):
+    return [synth.distance_pair_hard_wave(seed_a=seed0 + 2 * q, seed_b=seed0 + 2 * q + 1)[:2] for q in range(n)]
+
+
+def _sine_pairs(n, seed0=200):
+    return [synth.distance_pair_sine(seed_a=seed0 + 2 * q, seed_b=seed0 + 2 * q + 1)[:2] for q in range(n)]
+
+
+def _same(r, a, newton=False):
+    """Equal results (pair-test and candidate counts may differ: they depend
+    on the order the screen visits tile pairs in)."""
+    assert r.rounds == a.rounds
+    assert np.array_equal(r.npairs, a.npairs)
+    assert np.array_equal(r.kth_d2, a.kth_d2)
+    for rr in range(a.rounds):
+        assert np.array_equal(r.pairs[rr], a.pairs[rr])
+    assert r.v5_value == a.v5_value
+    assert r.distance == a.distance
+    if newton:
+        assert r.newton_distance == a.newton_distance
+        assert r.uv1 == a.uv1 and r.uv2 == a.uv2
+
+
+def _check_batch(ctx, tasks, *, k=8, rounds=4, precision="fp64", newton=False, lanes=2):
+    alone = [ctx.min_distance(ta, tb, k=k, rounds=rounds, precision=precision, newton=newton, trace=True)
+             for ta, tb in tasks]
+    ctx.workers(lanes)
+    try:
+        batch, ms = ctx.min_distance_batch(tasks, k=k, rounds=rounds, precision=precision, newton=newton,
+                                           trace=True)
+    finally:
+        ctx.workers(0)
+    assert ms > 0
+    for r, a in zip(batch, alone):
+        _same(r, a, newton)
+    return batch
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_batch_supertile_round(precision):
+    """nuv0 = 128: 16 x 16 tiles per side, the two-level (supertile) screen."""
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _hard_wave_pairs(10), 128)
+        _check_batch(ctx, tasks, precision=precision)
+
+
+@pytest.mark.parametrize("precision", PRECISIONS)
+@pytest.mark.parametrize("k,rounds", [(8, 4), (3, 2), (1, 5)])
+def test_batch_single_level_round(precision, k, rounds):
+    """nuv0 = 64: 8 x 8 tiles per side, tile pairs screened directly."""
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _sine_pairs(9), 64)
+        _check_batch(ctx, tasks, k=k, rounds=rounds, precision=precision, lanes=1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_screen"])
+def test_batch_newton(precision):
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _sine_pairs(6, seed0=300), 48)
+        _check_batch(ctx, tasks, precision=precision, newton=True)
+
+
+def test_batch_mixed_shapes_grouped():
+    """Queries of several shapes in one call: grouped per shape, results in
+    the caller's order."""
+    import jsi_cad_next_versions_b200 as J
+    rng = synth.SplitMix64(91)
+    with J.Context(0) as ctx:
+        tasks = []
+        for q in range(12):
+            if q % 3 == 0:
+                a, b = synth.distance_pair_sine(seed_a=400 + q, seed_b=500 + q)[:2]
+                nuv = 64
+            elif q % 3 == 1:
+                a, b = synth.random_surface(rng), synth.random_surface(rng)
+                nuv = 33
+            else:
+                a, b = synth.distance_pair_hard_wave(seed_a=600 + q, seed_b=700 + q)[:2]
+                nuv = 96
+            tasks += _upload_pairs(ctx, [(a, b)], nuv)
+        _check_batch(ctx, tasks, precision="fp64", lanes=3)
+
+
+def test_batch_chunk_zero_runs_per_query():
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _sine_pairs(5, seed0=800), 40)
+        ctx.workers(2)
+        try:
+            lock, _ = ctx.min_distance_batch(tasks, precision="fp32_screen", trace=True)
+            ctx.batch_chunk(0)
+            solo, _ = ctx.min_distance_batch(tasks, precision="fp32_screen", trace=True)
+        finally:
+            ctx.workers(0)
+        for r, a in zip(lock, solo):
+            _same(r, a)
+
+
+@pytest.mark.parametrize("env", ["JSI_BATCH_CAND_CAP", "JSI_BATCH_SURV_CAP"])
+def test_batch_overflow_reruns_alone(env):
+    """A one-entry list overflows in every query (k = 8 needs at least 8
+    candidates, and round 1 keeps more than one tile pair): each query is
+    flagged in its record and re-run alone, with the same results."""
+    import jsi_cad_next_versions_b200 as J
+    os.environ[env] = "1"
+    try:
+        with J.Context(0) as ctx:
+            tasks = _upload_pairs(ctx, _hard_wave_pairs(4, seed0=900), 128)
+            _check_batch(ctx, tasks, precision="fp32_screen", lanes=1)
+    finally:
+        del os.environ[env]
+
+
+def test_batch_overflow_counter():
+    import jsi_cad_next_versions_b200 as J
+    os.environ["JSI_BATCH_CAND_CAP"] = "1"
+    try:
+        with J.Context(0) as ctx:
+            tasks = _upload_pairs(ctx, _hard_wave_pairs(3, seed0=950), 128)
+            ctx.workers(1)
+            try:
+                ctx.min_distance_batch(tasks, precision="fp64")
+                assert ctx.batch_reruns() == len(tasks)
+            finally:
+                ctx.workers(0)
+    finally:
+        del os.environ["JSI_BATCH_CAND_CAP"]
+
+
+def test_batch_full_size_screen():
+    """The headline shape (hard-wave pair, nuv0 = 512) in one batch of 6."""
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _hard_wave_pairs(6, seed0=1000), 512)
+        batch = _check_batch(ctx, tasks, precision="fp32_screen", lanes=1)
+        assert all(r.rounds == 4 for r in batch)
