@@ -418,7 +418,7 @@ SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, Regio
   s.regions = regions ? regions : ar.get<RegionRec<T>>(nreg);
   s.spans = ar.get<int>(static_cast<size_t>(nreg) * 2 * g.nuv);
   s.basis = ar.get<T>(static_cast<size_t>(nreg) * 2 * g.nuv * 3 * g.p1max);
-  s.samples = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv);
+  s.samples = intersect ? ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv) : nullptr;
   s.kmax = ar.get<unsigned long long>(static_cast<size_t>(nreg) * 3);
   s.pad = ar.get<T>(nreg);
   s.center = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.cpr);
@@ -437,6 +437,12 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
   timed(ctx, "basis", [&] { launch_basis(v, s, st); }, 2.0 * s.nreg * s.g.nuv);
+  if (!intersect) {
+    // Distance: centres straight from the basis tables, no sample grid.
+    timed(ctx, "cells", [&] { launch_cells_fused(v, s, s, st); }, double(s.nreg) * s.g.W * s.g.W);
+    JSI_CUDA(cudaGetLastError());
+    return;
+  }
   if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
   timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); }, double(s.nreg) * s.g.nuv * s.g.nuv);
   if (intersect) timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
@@ -797,13 +803,11 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
         SideRound<TC> &C = side ? B32 : A32;
         C.g = P.g;
         C.nreg = P.nreg;
-        C.samples = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.nuv * P.g.nuv);
         C.center = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.cpr);
         C.tlo = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
         C.thi = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
         timed(ctx, "basis", [&] { launch_basis(side ? pb : pa, P, st); }, 2.0 * P.nreg * P.g.nuv);
-        timed(ctx, "samples", [&] { launch_samples_screen(side ? cb : ca, P, C, st); }, double(P.nreg) * P.g.nuv * P.g.nuv);
-        timed(ctx, "cells", [&] { launch_cells(C, false, st); }, double(C.nreg) * C.g.W * C.g.W);
+        timed(ctx, "cells", [&] { launch_cells_fused(side ? cb : ca, P, C, st); }, double(C.nreg) * C.g.W * C.g.W);
       }
       auto verify = [&](const DistCand<TC> *c, long long m, DistCand<TP> *o) {
         launch_dist_verify(pa, pb, A, B, map1, map2, c, m, o, st);
@@ -920,7 +924,6 @@ SideRound<T> slab_side(SlabPlan &sp, const Geom &g, int nreg, RegionRec<T> *regi
     s.basis = sp.get<T>(static_cast<size_t>(nreg) * 2 * g.nuv * 3 * g.p1max);
   }
   if (cells) {
-    s.samples = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv);
     s.center = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.cpr);
     s.tlo = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
     s.thi = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
@@ -953,7 +956,7 @@ BatchCaps batch_caps() {
   return c;
 }
 constexpr unsigned long long kBatchHeadCap = 2048;        // threshold-pass list
-constexpr unsigned kBatchHeadWant = 148 * 4;
+constexpr unsigned kBatchHeadWant = 256;
 
 // One round's arrays in the slab.  TP sides hold the regions and basis tables
 // (and, in exact rounds, the cells); the FP32 screen's first round keeps its
@@ -1149,26 +1152,18 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1));
     });
     if (!scr) {
-      timed(L, "samples", [&] {
-        launch_samples(va, Rd.A, false, st, bt, head_view<TP>(lay.head, 0));
-        launch_samples(vb, Rd.B, false, st, bt, head_view<TP>(lay.head, 1));
-      });
       timed(L, "cells", [&] {
-        launch_cells(Rd.A, false, st, bt);
-        launch_cells(Rd.B, false, st, bt);
+        launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0));
+        launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1));
       });
       batch_screen<TP>(L, Rd, Rd.A, Rd.B, stats, p.k, false, 0.0f, bt);
       timed(L, "dist_select", [&] {
         launch_dist_select(static_cast<const DistCand<TP> *>(Rd.cand), Rd.cand_cap, p.k, Rd.top, stats, st, bt);
       });
     } else if constexpr (kScreen) {
-      timed(L, "samples", [&] {
-        launch_samples_screen(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
-        launch_samples_screen(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
-      });
       timed(L, "cells", [&] {
-        launch_cells(Rd.A32, false, st, bt);
-        launch_cells(Rd.B32, false, st, bt);
+        launch_cells_fused(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
+        launch_cells_fused(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
       });
       batch_screen<TC>(L, Rd, Rd.A32, Rd.B32, stats, p.k, true, e, bt);
       timed(L, "dist_verify", [&] {

@@ -218,6 +218,12 @@ void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *m
 // FP32-screen form: FP32 samples from FP64 basis tables; FP64 re-check.
 void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
                            cudaStream_t st, const Batch &bt = Batch{}, const SurfView<float> *vdev = nullptr);
+// Distance cells straight from the basis tables (no sample grid in HBM):
+// centres and tile ranges of out, bit-identical to launch_samples(_screen) +
+// launch_cells.  TB = basis precision, TC = cell precision.
+template <typename TB, typename TC>
+void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
+                        const Batch &bt = Batch{}, const SurfView<TC> *vdev = nullptr);
 // stats set: the candidate count is read on the device (capped at cap).
 void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
                         const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,

@@ -1121,11 +1121,25 @@ __global__ void k_dist_cull_st(SideRound<T> a, SideRound<T> b, const int *map1, 
 }
 
 // Surviving supertile pairs expanded into their <= 64 x 64 child tile pairs,
-// in chunks of 256 child pairs per block iteration (16 chunks per supertile
-// pair, so that a few survivors still spread over many SMs).
-// cull = 0: fold the representative distances into tau; cull = 1: append the
-// tile pairs whose bound passes tau, with the bound as sort key (the same
-// format k_dist_cull writes).
+// one block per supertile pair.  Each side's child tiles are first tested
+// against the other supertile's box: a tile box lies inside its supertile's
+// box and the rounded gap is monotone, so lb(t1, t2) >= lb(t1, S2) and a tile
+// that fails against the box fails against every tile inside it.  Only the
+// surviving children are crossed.
+// cull = 0: fold the representative distances into tau (each warp folds the
+// k-th of its lanes' minima after every supertile pair, so the pre-filter of
+// the next one already uses the tighter value); cull = 1: append the tile
+// pairs whose bound passes tau, with the bound as sort key (the same format
+// k_dist_cull writes).
+template <typename T, bool S>
+__device__ __forceinline__ T shaved_lb(const Vec4<T> &lo1, const Vec4<T> &hi1, const Vec4<T> &lo2, const Vec4<T> &hi2) {
+  T lb = tile_lb(lo1, hi1, lo2, hi2);
+  // The screen's pair distances are FMA-contracted: shave the rounded bound
+  // by 2^-19 (more than the 12u they can differ by).
+  if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
+  return lb;
+}
+
 template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_expand(SideRound<T> a, SideRound<T> b, const int *map1,
                                                      const int *map2, const unsigned long long *st_surv,
@@ -1134,6 +1148,8 @@ __global__ void __launch_bounds__(256) k_dist_expand(SideRound<T> a, SideRound<T
                                                      unsigned long long cap, ScreenStats *stats, float e,
                                                      long long qs) {
   __shared__ unsigned sh[256];
+  __shared__ int s_t1[kMaxTile * kMaxTile], s_t2[kMaxTile * kMaxTile];
+  __shared__ int s_n1, s_n2;
   const long long qo = qoff(qs);
   a = qsh(a, qo);
   b = qsh(b, qo);
@@ -1146,46 +1162,80 @@ __global__ void __launch_bounds__(256) k_dist_expand(SideRound<T> a, SideRound<T
   nst_surv = count_of(nst_surv, stats->st_survivors, st_cap);
   const Geom g1 = a.g, g2 = b.g;
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
-  constexpr int kChunks = kMaxTile * kMaxTile * kMaxTile * kMaxTile / 256;
+  const int tid = threadIdx.x;
   float best = __uint_as_float(0x7f800000u);
-  const T tau = thr_compare<T, S>(stats->tau_bits, e);
-  for (unsigned long long it = blockIdx.x; it < nst_surv * kChunks; it += gridDim.x) {
-    const unsigned long long w = it / kChunks;
-    const int c = static_cast<int>(it % kChunks) * 256 + threadIdx.x;
+  for (unsigned long long w = blockIdx.x; w < nst_surv; w += gridDim.x) {
     const unsigned long long q = st_surv[w];
     const int row = static_cast<int>(q >> 32), s2 = static_cast<int>(q & 0xffffffffull);
     const int slot = row / g1.nst, s1 = row - slot * g1.nst;
     const int r1 = map1[slot], r2 = map2[slot];
     const int sy1 = s1 / g1.stw, sx1 = s1 - sy1 * g1.stw, sy2 = s2 / g2.stw, sx2 = s2 - sy2 * g2.stw;
-    const int l1 = c >> 6, l2 = c & 63;
-    const int ty1 = sy1 * kMaxTile + (l1 >> 3), tx1 = sx1 * kMaxTile + (l1 & 7);
-    const int ty2 = sy2 * kMaxTile + (l2 >> 3), tx2 = sx2 * kMaxTile + (l2 & 7);
-    const bool valid = ty1 < g1.tw && tx1 < g1.tw && ty2 < g2.tw && tx2 < g2.tw;
-    const int t1 = ty1 * g1.tw + tx1, t2 = ty2 * g2.tw + tx2;
-    bool keep = false;
-    T lb = T(0);
-    if (valid) {
-      const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
-      const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
-      if (!cull) {
-        const Vec4<T> c1 = a.center[i1 * n1 + tile_rep(t1, g1)];
-        const Vec4<T> c2 = b.center[i2 * n2 + tile_rep(t2, g2)];
-        best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+    const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
+    const T tau = thr_compare<T, S>(taub, e);
+    if (tid == 0) {
+      s_n1 = 0;
+      s_n2 = 0;
+    }
+    __syncthreads();
+    if (tid < 2 * kMaxTile * kMaxTile) {
+      const int side = tid >> 6, l = tid & 63;
+      if (side == 0) {
+        const int ty = sy1 * kMaxTile + (l >> 3), tx = sx1 * kMaxTile + (l & 7);
+        if (ty < g1.tw && tx < g1.tw) {
+          const int t = ty * g1.tw + tx;
+          const long long i1 = static_cast<long long>(r1) * g1.ntiles + t;
+          const long long j2 = static_cast<long long>(r2) * g2.nst + s2;
+          if (shaved_lb<T, S>(a.tlo[i1], a.thi[i1], b.stlo[j2], b.sthi[j2]) <= tau) s_t1[atomicAdd(&s_n1, 1)] = t;
+        }
       } else {
-        lb = tile_lb(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
-        if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
-        keep = lb <= tau;
+        const int ty = sy2 * kMaxTile + (l >> 3), tx = sx2 * kMaxTile + (l & 7);
+        if (ty < g2.tw && tx < g2.tw) {
+          const int t = ty * g2.tw + tx;
+          const long long i2 = static_cast<long long>(r2) * g2.ntiles + t;
+          const long long j1 = static_cast<long long>(r1) * g1.nst + s1;
+          if (shaved_lb<T, S>(a.stlo[j1], a.sthi[j1], b.tlo[i2], b.thi[i2]) <= tau) s_t2[atomicAdd(&s_n2, 1)] = t;
+        }
       }
     }
-    if (cull) {
-      const long long pos = warp_append(keep, &stats->survivors);
-      if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) {
-        surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + t1), static_cast<unsigned>(t2));
-        surv_lb[pos] = lb_bits_down(lb);
+    __syncthreads();
+    const int m1 = s_n1, m2 = s_n2, total = m1 * m2;
+    for (int c0 = 0; c0 < total; c0 += blockDim.x) {
+      const int c = c0 + tid;
+      bool keep = false;
+      T lb = T(0);
+      int t1 = 0, t2 = 0;
+      if (c < total) {
+        t1 = s_t1[c / m2];
+        t2 = s_t2[c - (c / m2) * m2];
+        const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
+        const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
+        if (!cull) {
+          const Vec4<T> c1 = a.center[i1 * n1 + tile_rep(t1, g1)];
+          const Vec4<T> c2 = b.center[i2 * n2 + tile_rep(t2, g2)];
+          best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+        } else {
+          lb = shaved_lb<T, S>(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
+          keep = lb <= tau;
+        }
+      }
+      if (cull) {
+        const long long pos = warp_append(keep, &stats->survivors);
+        if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) {
+          surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + t1), static_cast<unsigned>(t2));
+          surv_lb[pos] = lb_bits_down(lb);
+        }
       }
     }
+    if (!cull && k <= 32) {
+      const unsigned mine = __float_as_uint(best);
+      if (__popc(__ballot_sync(kFull, mine < taub)) >= k) {
+        const unsigned kth = warp_sorted_at(mine, k - 1);
+        if ((tid & 31) == 0) atomicMin(&stats->tau_bits, kth);
+      }
+    }
+    __syncthreads();
   }
-  if (!cull) fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+  if (!cull && k > 32) fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
 }
 
 // Total order of the top-k (distance_analysis.cu:226-231).
@@ -1551,9 +1601,10 @@ __device__ void find_crossing(const unsigned *hist, unsigned want, unsigned *s_w
 }
 
 // Threshold-pass list of a batched round, one block of 1024 per query: all
-// surviving tile pairs when at most head_cap survive, else about `want` of
-// them with the smallest bounds (two-level radix select on the bound bits),
-// so the exact per-tile-pair k-th starts from the closest tile pairs.
+// surviving tile pairs when at most `want` survive, else about `want` of them
+// (at most head_cap) with the smallest bounds (two-level radix select on the
+// bound bits), so the exact per-tile-pair k-th comes from the closest tile
+// pairs and the collecting pass meets a tight threshold.
 __global__ void __launch_bounds__(1024) k_dist_pick(const unsigned long long *surv, const unsigned *surv_lb,
                                                     unsigned long long surv_cap, unsigned long long *head,
                                                     unsigned long long head_cap, unsigned want, ScreenStats *stats,
@@ -1567,7 +1618,7 @@ __global__ void __launch_bounds__(1024) k_dist_pick(const unsigned long long *su
   head = qsh(head, qo);
   stats = qsh(stats, qo);
   const unsigned long long n = count_of(kFromDevice, stats->survivors, surv_cap);
-  if (n <= head_cap) {
+  if (n <= want) {
     for (unsigned long long e = threadIdx.x; e < n; e += blockDim.x) head[e] = surv[e];
     if (threadIdx.x == 0) stats->nhead = n;
     return;
@@ -1787,10 +1838,49 @@ __global__ void k_inter_side2(const unsigned long long *key2s, const int *idxs, 
 // FP32-screen form: FP32 positions from FP64 basis tables, FP64 re-check
 // ---------------------------------------------------------------------------
 
-// P of every sample in FP32: the FP64 basis values (the same tables the FP64
+// P of one sample in FP32: the FP64 basis values (the same tables the FP64
 // form uses) are rounded to FP32 and contracted with FMAs against the FP32
 // control net; rational surfaces divide by the weight in FP64.  The host
 // bounds |P32 - P64| per coordinate from the operation count.
+__device__ __forceinline__ Vec4<float> screen_point(const SurfView<float> &s, int spanu, const double *Nu, int spanv,
+                                                    const double *Nv) {
+  Vec4<float> P{0.0f, 0.0f, 0.0f, 0.0f};
+  if (s.zero) return P;
+  const int cu0 = spanu - s.degu, cv0 = spanv - s.degv;
+  float ax = 0.0f, ay = 0.0f, az = 0.0f, aw = 0.0f;
+  for (int rr = 0; rr <= s.degv; ++rr) {
+    const Vec4<float> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + rr) + cu0;
+    float rx = 0.0f, ry = 0.0f, rz = 0.0f, rw = 0.0f;
+    for (int c = 0; c <= s.degu; ++c) {
+      const Vec4<float> v = cp[c];
+      float n = __double2float_rn(Nu[c]);
+      if (s.rat) {
+        n = __fmul_rn(n, v.w);
+        rw = __fadd_rn(rw, n);
+      }
+      rx = __fmaf_rn(n, v.x, rx);
+      ry = __fmaf_rn(n, v.y, ry);
+      rz = __fmaf_rn(n, v.z, rz);
+    }
+    const float m = __double2float_rn(Nv[rr]);
+    ax = __fmaf_rn(m, rx, ax);
+    ay = __fmaf_rn(m, ry, ay);
+    az = __fmaf_rn(m, rz, az);
+    aw = __fmaf_rn(m, rw, aw);
+  }
+  if (s.rat) {
+    const double w = static_cast<double>(aw);
+    P.x = __double2float_rn(static_cast<double>(ax) / w);
+    P.y = __double2float_rn(static_cast<double>(ay) / w);
+    P.z = __double2float_rn(static_cast<double>(az) / w);
+  } else {
+    P.x = ax;
+    P.y = ay;
+    P.z = az;
+  }
+  return P;
+}
+
 __global__ void k_samples_screen(SurfView<float> s, const SurfView<float> *vdev, SideRound<double> basis_side,
                                  SideRound<float> out, long long qs) {
   const long long qo = qoff(qs);
@@ -1809,44 +1899,225 @@ __global__ void k_samples_screen(SurfView<float> s, const SurfView<float> *vdev,
     const int idx = q % nuv, idy = q / nuv;
     const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
     const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
-    const double *Nu = basis_side.basis + lu * 3 * p1;
-    const double *Nv = basis_side.basis + lv * 3 * p1;
-    Vec4<float> P{0.0f, 0.0f, 0.0f, 0.0f};
-    if (!s.zero) {
-      const int cu0 = basis_side.spans[lu] - s.degu, cv0 = basis_side.spans[lv] - s.degv;
-      float ax = 0.0f, ay = 0.0f, az = 0.0f, aw = 0.0f;
-      for (int rr = 0; rr <= s.degv; ++rr) {
-        const Vec4<float> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + rr) + cu0;
-        float rx = 0.0f, ry = 0.0f, rz = 0.0f, rw = 0.0f;
-        for (int c = 0; c <= s.degu; ++c) {
-          const Vec4<float> v = cp[c];
-          float n = __double2float_rn(Nu[c]);
-          if (s.rat) {
-            n = __fmul_rn(n, v.w);
-            rw = __fadd_rn(rw, n);
+    out.samples[t] = screen_point(s, basis_side.spans[lu], basis_side.basis + lu * 3 * p1, basis_side.spans[lv],
+                                  basis_side.basis + lv * 3 * p1);
+  }
+}
+
+// Distance cells without a sample grid in HBM: one warp per tile evaluates
+// the tile's (te + 1)^2 corner samples into shared memory, then forms the
+// tile's cell centres and centre range exactly as k_cells does.
+// TB = precision of the basis tables, TC = of the samples and cells
+// (TB = double, TC = float: the FP32 screen).
+//
+// The samples are evaluated in factored form: all samples of a tile column
+// share the u span and u basis, so the u-direction sum of every control-net
+// row the tile needs is formed once per (row, column) and then combined in v
+// per sample.  Each of those sums and each v accumulation is the same
+// operation sequence as in eval_point / screen_point, so the samples carry
+// the same bits; tiles whose rows exceed the shared-memory table (or degrees
+// above 8, MAXP > 9) take the per-sample path.
+template <typename TB, typename TC, int MAXP>
+__global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfView<TC> *vdev, SideRound<TB> bs,
+                                                     SideRound<TC> out, long long qs) {
+  constexpr int kE = kMaxTile + 1;       // samples per tile edge
+  constexpr int kRows = 16;              // control-net rows of the row-sum table
+  constexpr bool kFactor = MAXP <= 9;
+  constexpr int kNB = kFactor ? MAXP : 1;
+  constexpr int kNR = kFactor ? kRows : 1;
+  using TN = TC;                         // basis values as the contraction uses them
+  constexpr int kW = 4;                  // warps per block (one tile each)
+  __shared__ Vec4<TC> smp[kW][kE * kE];
+  __shared__ Vec4<TC> rsum[kW][kNR][kE];
+  __shared__ TN snu[kW][kE][kNB], snv[kW][kE][kNB];
+  __shared__ int ssu[kW][kE], ssv[kW][kE];
+  const long long qo = qoff(qs);
+  if (vdev) s = *qsh(vdev, qo);
+  bs = qsh(bs, qo);
+  out = qsh(out, qo);
+  const Geom g = out.g;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int te2 = g.te * g.te;
+  const int p1 = g.p1max;
+  Vec4<TC> *S = smp[wib];
+  const long long ntile_total = static_cast<long long>(nreg_of(bs)) * g.ntiles;
+  const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  for (long long t = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; t < ntile_total;
+       t += nwarps) {
+    const int r = static_cast<int>(t / g.ntiles);
+    const int tile = static_cast<int>(t - static_cast<long long>(r) * g.ntiles);
+    const int ty = tile / g.tw, tx = tile - (tile / g.tw) * g.tw;
+    const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
+    const int sw = nu + 1, ns = (nv + 1) * sw;
+    const long long lu0 = (static_cast<long long>(r) * 2 + 0) * g.nuv + tx * g.te;
+    const long long lv0 = (static_cast<long long>(r) * 2 + 1) * g.nuv + ty * g.te;
+    bool factored = false;
+    int rmin = 0;
+    if constexpr (kFactor) {
+      if (!s.zero) {
+        // Spans and basis values of the tile's sample columns (lanes 0..nu)
+        // and rows (lanes 16..16+nv), converted as the contraction uses them.
+        if (lane <= nu) {
+          ssu[wib][lane] = bs.spans[lu0 + lane];
+          const TB *N = bs.basis + (lu0 + lane) * 3 * p1;
+          for (int c = 0; c <= s.degu; ++c) {
+            if constexpr (std::is_same<TB, TC>::value) snu[wib][lane][c] = N[c];
+            else snu[wib][lane][c] = __double2float_rn(N[c]);
           }
-          rx = __fmaf_rn(n, v.x, rx);
-          ry = __fmaf_rn(n, v.y, ry);
-          rz = __fmaf_rn(n, v.z, rz);
         }
-        const float m = __double2float_rn(Nv[rr]);
-        ax = __fmaf_rn(m, rx, ax);
-        ay = __fmaf_rn(m, ry, ay);
-        az = __fmaf_rn(m, rz, az);
-        aw = __fmaf_rn(m, rw, aw);
-      }
-      if (s.rat) {
-        const double w = static_cast<double>(aw);
-        P.x = __double2float_rn(static_cast<double>(ax) / w);
-        P.y = __double2float_rn(static_cast<double>(ay) / w);
-        P.z = __double2float_rn(static_cast<double>(az) / w);
-      } else {
-        P.x = ax;
-        P.y = ay;
-        P.z = az;
+        if (lane >= 16 && lane - 16 <= nv) {
+          const int a = lane - 16;
+          ssv[wib][a] = bs.spans[lv0 + a];
+          const TB *N = bs.basis + (lv0 + a) * 3 * p1;
+          for (int c = 0; c <= s.degv; ++c) {
+            if constexpr (std::is_same<TB, TC>::value) snv[wib][a][c] = N[c];
+            else snv[wib][a][c] = __double2float_rn(N[c]);
+          }
+        }
+        __syncwarp();
+        int lo = INT_MAX, hi = INT_MIN;
+        for (int a = 0; a <= nv; ++a) {
+          lo = min(lo, ssv[wib][a]);
+          hi = max(hi, ssv[wib][a]);
+        }
+        rmin = lo - s.degv;
+        const int nrows = hi - rmin + 1;
+        factored = nrows <= kRows;
+        if (factored) {
+          // u-direction sums of every needed control-net row and column.
+          for (int it = lane; it < nrows * sw; it += 32) {
+            const int R = it / sw, b = it - (it / sw) * sw;
+            const Vec4<TC> *cp = s.cpw + static_cast<long long>(s.ncpu) * (rmin + R) + (ssu[wib][b] - s.degu);
+            const TN *Nu = snu[wib][b];
+            TC r0 = TC(0), r1 = TC(0), r2 = TC(0), r3 = TC(0);
+            for (int c = 0; c <= s.degu; ++c) {
+              const Vec4<TC> q = cp[c];
+              if constexpr (std::is_same<TB, TC>::value) {
+                if (!s.rat) {
+                  const TC n = Nu[c];
+                  r0 += n * q.x;
+                  r1 += n * q.y;
+                  r2 += n * q.z;
+                } else {
+                  const TC nw = Nu[c] * q.w;
+                  r0 += nw * q.x;
+                  r1 += nw * q.y;
+                  r2 += nw * q.z;
+                  r3 += nw;
+                }
+              } else {
+                float n = Nu[c];
+                if (s.rat) {
+                  n = __fmul_rn(n, q.w);
+                  r3 = __fadd_rn(r3, n);
+                }
+                r0 = __fmaf_rn(n, q.x, r0);
+                r1 = __fmaf_rn(n, q.y, r1);
+                r2 = __fmaf_rn(n, q.z, r2);
+              }
+            }
+            rsum[wib][R][b] = Vec4<TC>{r0, r1, r2, r3};
+          }
+          __syncwarp();
+          // v-direction combination per sample.
+          for (int l = lane; l < ns; l += 32) {
+            const int a = l / sw, b = l - (l / sw) * sw;
+            const int R0 = ssv[wib][a] - s.degv - rmin;
+            const TN *Nv = snv[wib][a];
+            TC a0 = TC(0), a1 = TC(0), a2 = TC(0), a3 = TC(0);
+            for (int rr = 0; rr <= s.degv; ++rr) {
+              const Vec4<TC> row = rsum[wib][R0 + rr][b];
+              const TC m = Nv[rr];
+              if constexpr (std::is_same<TB, TC>::value) {
+                a0 += m * row.x;
+                a1 += m * row.y;
+                a2 += m * row.z;
+                a3 += m * row.w;
+              } else {
+                a0 = __fmaf_rn(m, row.x, a0);
+                a1 = __fmaf_rn(m, row.y, a1);
+                a2 = __fmaf_rn(m, row.z, a2);
+                a3 = __fmaf_rn(m, row.w, a3);
+              }
+            }
+            Vec4<TC> P{a0, a1, a2, TC(0)};
+            if (s.rat) {
+              if constexpr (std::is_same<TB, TC>::value) {
+                const TC inv = TC(1) / a3;
+                P.x = a0 * inv;
+                P.y = a1 * inv;
+                P.z = a2 * inv;
+              } else {
+                const double w = static_cast<double>(a3);
+                P.x = __double2float_rn(static_cast<double>(a0) / w);
+                P.y = __double2float_rn(static_cast<double>(a1) / w);
+                P.z = __double2float_rn(static_cast<double>(a2) / w);
+              }
+            }
+            S[l] = P;
+          }
+        }
       }
     }
-    out.samples[t] = P;
+    if (!factored) {
+      for (int l = lane; l < ns; l += 32) {
+        const int a = l / sw, b = l - (l / sw) * sw;
+        const long long lu = lu0 + b, lv = lv0 + a;
+        const TB *Nu = bs.basis + lu * 3 * p1;
+        const TB *Nv = bs.basis + lv * 3 * p1;
+        Vec4<TC> P;
+        if constexpr (std::is_same<TB, TC>::value) {
+          TC q[3];
+          eval_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv, q);
+          P = Vec4<TC>{q[0], q[1], q[2], TC(0)};
+        } else {
+          P = screen_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv);
+        }
+        S[l] = P;
+      }
+    }
+    __syncwarp();
+    TC lo[3] = {pos_inf<TC>(), pos_inf<TC>(), pos_inf<TC>()};
+    TC hi[3] = {-pos_inf<TC>(), -pos_inf<TC>(), -pos_inf<TC>()};
+    for (int local = lane; local < te2; local += 32) {
+      const int a = local / g.te, b = local - (local / g.te) * g.te;
+      Vec4<TC> cen{TC(0), TC(0), TC(0), TC(0)};
+      if (a < nv && b < nu) {
+        const Vec4<TC> p0 = S[a * sw + b];
+        const Vec4<TC> p1v = S[a * sw + b + 1];
+        const Vec4<TC> p2 = S[(a + 1) * sw + b];
+        const Vec4<TC> p3 = S[(a + 1) * sw + b + 1];
+        const TC lx = tmin(p0.x, tmin(p1v.x, tmin(p2.x, p3.x)));
+        const TC ly = tmin(p0.y, tmin(p1v.y, tmin(p2.y, p3.y)));
+        const TC lz = tmin(p0.z, tmin(p1v.z, tmin(p2.z, p3.z)));
+        const TC hx = tmax(p0.x, tmax(p1v.x, tmax(p2.x, p3.x)));
+        const TC hy = tmax(p0.y, tmax(p1v.y, tmax(p2.y, p3.y)));
+        const TC hz = tmax(p0.z, tmax(p1v.z, tmax(p2.z, p3.z)));
+        cen.x = (lx - TC(0) + hx + TC(0)) / TC(2);
+        cen.y = (ly - TC(0) + hy + TC(0)) / TC(2);
+        cen.z = (lz - TC(0) + hz + TC(0)) / TC(2);
+        lo[0] = tmin(lo[0], cen.x);
+        lo[1] = tmin(lo[1], cen.y);
+        lo[2] = tmin(lo[2], cen.z);
+        hi[0] = tmax(hi[0], cen.x);
+        hi[1] = tmax(hi[1], cen.y);
+        hi[2] = tmax(hi[2], cen.z);
+      }
+      out.center[t * te2 + local] = cen;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = tmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+        hi[c] = tmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+      }
+    }
+    if (lane == 0) {
+      out.tlo[t] = Vec4<TC>{lo[0], lo[1], lo[2], TC(0)};
+      out.thi[t] = Vec4<TC>{hi[0], hi[1], hi[2], TC(0)};
+    }
+    __syncwarp();
   }
 }
 
@@ -2309,7 +2580,7 @@ void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int 
                         ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
   if (nst_surv == 0) return;
-  const unsigned long long most = (nst_surv == kFromDevice ? st_cap : nst_surv) * 16ull;
+  const unsigned long long most = nst_surv == kFromDevice ? st_cap : nst_surv;
   const dim3 grid = bdim(bgrid(static_cast<long long>(most < 148ull * 8 ? most : 148ull * 8), bt, 148 * 8), bt);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
@@ -2428,6 +2699,28 @@ void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &ba
   const long long n = static_cast<long long>(basis_side.nreg) * basis_side.g.nuv * basis_side.g.nuv;
   k_samples_screen<<<bdim(bgrid((n + 127) / 128, bt, 148 * 32), bt), 128, 0, st>>>(s, vdev, basis_side, out, bt.qs);
 }
+
+template <typename TB, typename TC>
+void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
+                        const Batch &bt, const SurfView<TC> *vdev) {
+  counted();
+  const long long warps = static_cast<long long>(bs.nreg) * out.g.ntiles;
+  const dim3 grid = bdim(bgrid((warps + 3) / 4, bt, 148 * 64), bt);
+  if (out.g.p1max <= 9)
+    k_cells_fused<TB, TC, 9><<<grid, 128, 0, st>>>(s, vdev, bs, out, bt.qs);
+  else
+    k_cells_fused<TB, TC, kMaxDeg + 1><<<grid, 128, 0, st>>>(s, vdev, bs, out, bt.qs);
+}
+
+template void launch_cells_fused<float, float>(const SurfView<float> &, const SideRound<float> &,
+                                               const SideRound<float> &, cudaStream_t, const Batch &,
+                                               const SurfView<float> *);
+template void launch_cells_fused<double, double>(const SurfView<double> &, const SideRound<double> &,
+                                                 const SideRound<double> &, cudaStream_t, const Batch &,
+                                                 const SurfView<double> *);
+template void launch_cells_fused<double, float>(const SurfView<float> &, const SideRound<double> &,
+                                                const SideRound<float> &, cudaStream_t, const Batch &,
+                                                const SurfView<float> *);
 
 void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
                         const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,
