@@ -59,7 +59,14 @@ FLOPS_PER_PAIR_TEST = 8
 # representative distance (8 flops) / one box-gap bound (14 flops) per tile
 # pair, tile data L2-resident (0 B).  dist_leaf / inter_leaf: 8 / 9 flops per
 # executed cell-pair test, operands in registers (0 B).
-UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "dist_tau": (8, 0),
+# cells_r1: the first round's fused cell build (no sample grid in HBM), per
+# cell: the factored bicubic contraction amortised over a band column
+# (5 net rows x 4 x 3 FMA per column / 8 cells + 4 x 3 FMA per sample, with
+# 9/8 samples per cell) ~ 40 flops, plus 18 min/max + 6 add + 3 halvings for
+# the centre and 6 min/max for the tile range ~ 33 flops: 73 flops; HBM: the
+# 16 B centre written plus 2 x 16 B tile bounds per 64 cells = 16.5 B.
+UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "cells_r1": (73, 16.5),
+             "dist_tau": (8, 0),
              "dist_cull": (14, 0), "dist_leaf": (8, 0), "dist_head": (8, 0), "inter_cull": (14, 0),
              "inter_leaf": (9, 0)}
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 74.4: 148 SMs x 128 lanes x FMA x 1.965 GHz
@@ -94,12 +101,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--batch", type=int, default=16, help="queries per step")
+    ap.add_argument("--batch", type=int, default=512, help="queries per step")
     ap.add_argument("--nuv0", type=int, default=NUV0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default=",".join(FORMS))
-    ap.add_argument("--lanes", type=int, default=8, help="worker lanes (concurrent queries on the device)")
-    ap.add_argument("--chunk", type=int, default=64,
+    ap.add_argument("--lanes", type=int, default=2, help="worker lanes (concurrent batches on the device)")
+    ap.add_argument("--chunk", type=int, default=256,
                     help="queries per lockstep batch on a lane (0: one query per lane job)")
     return ap.parse_args()
 
@@ -340,8 +347,11 @@ def run_ours(args):
         ctx.release(a)
         ctx.release(b)
 
+    flat = [x for pr in pairs for x in pr]
+
     def e2e_step():
-        ids2 = [(ctx.upload(A), ctx.upload(B)) for A, B in pairs]
+        got = ctx.upload_many(flat)
+        ids2 = list(zip(got[0::2], got[1::2]))
         tl = [(ctx.task(sa, np.array(A.rect(), np.float32), args.nuv0, 1),
                ctx.task(sb, np.array(B.rect(), np.float32), args.nuv0, 2)) for (sa, sb), (A, B) in zip(ids2, pairs)]
         ctx.min_distance_batch(tl, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)

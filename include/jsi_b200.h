@@ -69,9 +69,16 @@ int jsi_abi_version(void);
  * decoded as in src/evaluation/evaluation.cu:239-257) to device memory and
  * keeps it resident until released.  Replaces the caller-side
  * allocate_from_workspace + cadMemcpy of ivec/data
- * (examples/intersection_example.cu:50-57). */
+ * (examples/intersection_example.cu:50-57).  The copy is asynchronous (the
+ * data is staged in pinned memory before the call returns); queries issued
+ * afterwards see the surface.  Releases return the device block to the
+ * context's pool without synchronising. */
 int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, int ndata, jsi_surface_id *out);
 int jsi_surface_release(jsi_context *ctx, jsi_surface_id id);
+/* n surfaces in one call: ivecs = n x 7 headers, datas[q] / ndatas[q] the
+ * records; out[q] gets each id (0 for those not uploaded after an error). */
+int jsi_surface_upload_many(jsi_context *ctx, int n, const int *ivecs, const float *const *datas, const int *ndatas,
+                            jsi_surface_id *out);
 /* Resident surface bytes on the device. */
 int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out);
 

@@ -110,6 +110,21 @@ class Context:
         self._check(self.lib.jsi_surface_upload(self.handle, _p(iv), _p(da), int(da.shape[0]), ctypes.byref(sid)))
         return sid.value
 
+    def upload_many(self, surfaces) -> list[int]:
+        """Upload several surfaces in one call; returns their ids."""
+        n = len(surfaces)
+        if n == 0:
+            return []
+        iv = np.ascontiguousarray(np.stack([np.asarray(x.ivec, np.int32) for x in surfaces]), dtype=np.int32)
+        keep = [np.ascontiguousarray(x.data, dtype=np.float32) for x in surfaces]
+        FP = ctypes.POINTER(ctypes.c_float)
+        ptrs = (FP * n)(*[k.ctypes.data_as(FP) for k in keep])
+        nd = (ctypes.c_int * n)(*[int(k.shape[0]) for k in keep])
+        ids = (ctypes.c_int * n)()
+        self._check(self.lib.jsi_surface_upload_many(self.handle, n, iv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                     ptrs, nd, ids))
+        return list(ids)
+
     def release(self, sid: int):
         self._check(self.lib.jsi_surface_release(self.handle, sid))
 

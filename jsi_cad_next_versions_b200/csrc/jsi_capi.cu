@@ -171,7 +171,65 @@ struct SurfaceRec {
   Vec4<float> *cpw32 = nullptr;
   Vec4<double> *cpw64 = nullptr;
   size_t bytes = 0;
+  char *block = nullptr;  // pooled device block of a resident surface
+  size_t block_bytes = 0;
 };
+
+// Device blocks of resident surfaces: power-of-two size classes carved from
+// 64 MiB slabs (blocks above a slab get a slab of their own), recycled
+// through per-class free lists, so uploads and releases allocate nothing in
+// steady state and never synchronise the device.
+class SurfacePool {
+ public:
+  ~SurfacePool() {
+    for (char *p : slabs_) cudaFree(p);
+  }
+  static size_t class_bytes(size_t bytes) {
+    size_t c = 4096;
+    while (c < bytes) c <<= 1;
+    return c;
+  }
+  char *get(size_t bytes) {
+    const size_t c = class_bytes(bytes);
+    auto &fl = free_[c];
+    if (!fl.empty()) {
+      char *p = fl.back();
+      fl.pop_back();
+      return p;
+    }
+    if (c > kSlab) return new_slab(c);
+    if (!cur_ || left_ < c) {
+      cur_ = new_slab(kSlab);
+      left_ = kSlab;
+    }
+    char *p = cur_;
+    cur_ += c;
+    left_ -= c;
+    return p;
+  }
+  void put(char *p, size_t bytes) { free_[class_bytes(bytes)].push_back(p); }
+
+ private:
+  static constexpr size_t kSlab = size_t(64) << 20;
+  char *new_slab(size_t bytes) {
+    char *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      fail(JSI_ERR_NOMEM, "cudaMalloc of %zu bytes for resident surfaces failed", bytes);
+    }
+    slabs_.push_back(p);
+    return p;
+  }
+  std::vector<char *> slabs_;
+  std::map<size_t, std::vector<char *>> free_;
+  char *cur_ = nullptr;
+  size_t left_ = 0;
+};
+
+// Pinned staging of surface uploads: kRingSegs segments used in turn; an
+// event recorded when a segment is left guards its reuse.
+constexpr int kRingSegs = 8;
+constexpr size_t kRingSeg = size_t(8) << 20;
 
 }  // namespace
 
@@ -240,6 +298,12 @@ struct jsi_context {
   std::atomic<size_t> lane_held{0};  // arena bytes held by all worker lanes
   size_t lane_keep = 0;              // steady arena size a lane keeps after a query
   size_t resident = 0;
+  SurfacePool pool;
+  char *ring = nullptr;
+  int ring_cur = 0;
+  size_t ring_off = 0;
+  cudaEvent_t ring_ev[kRingSegs] = {};
+  cudaEvent_t upload_ev = nullptr;  // recorded after every upload (lanes wait on it)
   int batch_chunk = 64;  // queries per lockstep batch (0: one query per lane job)
   std::string kernel_names;
   // worker pool
@@ -340,32 +404,43 @@ void check_surface(const int ivec[7], const float *data, int ndata) {
   if (ndata < need) fail(JSI_ERR_SURFACE, "ndata %d < %lld required by the header", ndata, need);
 }
 
-SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
-  check_surface(ivec, data, ndata);
-  SurfaceRec s;
+// Header fields and the per-surface magnitudes the FP32-screen error bound
+// needs (max |coordinate|, max |w coordinate|, weight range).
+void surface_header(SurfaceRec &s, const int ivec[7], const float *data) {
   std::memcpy(s.ivec, ivec, sizeof(s.ivec));
   const int flags = ivec[0];
   s.rat = (flags & 2) ? 1 : 0;
   s.zero = ((!(flags & 1)) && (flags & 12)) || ivec[1] >= kMaxDeg || ivec[4] >= kMaxDeg;
   s.du = std::min(2, ivec[1]);
   s.dv = std::min(2, ivec[4]);
-  const int nku = ivec[3], nkv = ivec[6];
   const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
-  const float *cp = data + nku + nkv;
-  std::vector<Vec4<float>> c32(ncp);
-  std::vector<Vec4<double>> c64(ncp);
-  std::vector<double> u64(data, data + nku), v64(data + nku, data + nku + nkv);
+  const float *cp = data + ivec[3] + ivec[6];
   if (s.rat && ncp > 0) s.wmin = s.wmax = cp[3 * ncp];
   for (size_t q = 0; q < ncp; ++q) {
     const float w = s.rat ? cp[3 * ncp + q] : 1.0f;
-    c32[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
-    c64[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
     for (int c = 0; c < 3; ++c) {
       s.cmax[c] = std::max(s.cmax[c], std::fabs(static_cast<double>(cp[3 * q + c])));
       s.wcmax[c] = std::max(s.wcmax[c], std::fabs(static_cast<double>(w) * cp[3 * q + c]));
     }
     s.wmin = std::min(s.wmin, static_cast<double>(w));
     s.wmax = std::max(s.wmax, static_cast<double>(w));
+  }
+}
+
+SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
+  check_surface(ivec, data, ndata);
+  SurfaceRec s;
+  surface_header(s, ivec, data);
+  const int nku = ivec[3], nkv = ivec[6];
+  const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
+  const float *cp = data + nku + nkv;
+  std::vector<Vec4<float>> c32(ncp);
+  std::vector<Vec4<double>> c64(ncp);
+  std::vector<double> u64(data, data + nku), v64(data + nku, data + nku + nkv);
+  for (size_t q = 0; q < ncp; ++q) {
+    const float w = s.rat ? cp[3 * ncp + q] : 1.0f;
+    c32[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
+    c64[q] = {cp[3 * q], cp[3 * q + 1], cp[3 * q + 2], w};
   }
   s.bytes = nku * 12 + nkv * 12 + ncp * (sizeof(Vec4<float>) + sizeof(Vec4<double>));
   auto dalloc = [&](size_t bytes) -> void * {
@@ -394,20 +469,68 @@ SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int n
   return s;
 }
 
-void free_surface(SurfaceRec &s) {
-  cudaFree(s.U32);
-  cudaFree(s.V32);
-  cudaFree(s.U64);
-  cudaFree(s.V64);
-  cudaFree(s.cpw32);
-  cudaFree(s.cpw64);
-}
-
 const SurfaceRec &get_surface(Lane *ctx, jsi_surface_id id) {
   auto it = ctx->surfaces->find(id);
   if (it == ctx->surfaces->end()) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
   return it->second;
 }
+
+}  // namespace
+
+namespace {
+
+// Resident upload on the main stream without a host sync: the raw record
+// goes through the pinned ring into the surface's pooled block (where it is
+// also the FP32 knot vectors), a kernel builds the FP64 knots and the nets,
+// and upload_ev marks the point that worker lanes wait for.
+SurfaceRec upload_resident(jsi_context *ctx, const int ivec[7], const float *data, int ndata) {
+  check_surface(ivec, data, ndata);
+  SurfaceRec s;
+  surface_header(s, ivec, data);
+  const int nku = ivec[3], nkv = ivec[6];
+  const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
+  auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t raw_b = al(static_cast<size_t>(ndata) * sizeof(float));
+  const size_t u64_b = al(nku * sizeof(double)), v64_b = al(nkv * sizeof(double));
+  const size_t c32_b = al(ncp * sizeof(Vec4<float>)), c64_b = al(ncp * sizeof(Vec4<double>));
+  const size_t total = raw_b + u64_b + v64_b + c32_b + c64_b;
+  if (ctx->resident + SurfacePool::class_bytes(total) > ctx->budget)
+    fail(JSI_ERR_NOMEM, "HBM budget exhausted by resident surfaces");
+  char *blk = ctx->pool.get(total);
+  s.block = blk;
+  s.block_bytes = total;
+  s.bytes = SurfacePool::class_bytes(total);
+  s.U32 = reinterpret_cast<float *>(blk);
+  s.V32 = s.U32 + nku;
+  s.U64 = reinterpret_cast<double *>(blk + raw_b);
+  s.V64 = reinterpret_cast<double *>(blk + raw_b + u64_b);
+  s.cpw32 = reinterpret_cast<Vec4<float> *>(blk + raw_b + u64_b + v64_b);
+  s.cpw64 = reinterpret_cast<Vec4<double> *>(blk + raw_b + u64_b + v64_b + c32_b);
+  Lane *L = &ctx->main;
+  cudaStream_t st = L->stream;
+  const size_t nbytes = static_cast<size_t>(ndata) * sizeof(float);
+  if (nbytes <= kRingSeg) {
+    if (ctx->ring_off + nbytes > kRingSeg) {
+      JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
+      ctx->ring_cur = (ctx->ring_cur + 1) % kRingSegs;
+      ctx->ring_off = 0;
+      JSI_CUDA(cudaEventSynchronize(ctx->ring_ev[ctx->ring_cur]));
+    }
+    char *stage = ctx->ring + static_cast<size_t>(ctx->ring_cur) * kRingSeg + ctx->ring_off;
+    std::memcpy(stage, data, nbytes);
+    JSI_CUDA(copy_async(L, blk, stage, nbytes, cudaMemcpyHostToDevice, st));
+    ctx->ring_off += (nbytes + 255) & ~static_cast<size_t>(255);
+  } else {
+    // Larger than a ring segment: pageable copy, completed before returning.
+    JSI_CUDA(copy_async(L, blk, data, nbytes, cudaMemcpyHostToDevice, st));
+    JSI_CUDA(cudaStreamSynchronize(st));
+  }
+  launch_surface_prep(s.U32, nku, nkv, static_cast<long long>(ncp), s.rat, s.U64, s.V64, s.cpw32, s.cpw64, st);
+  JSI_CUDA(cudaGetLastError());
+  JSI_CUDA(cudaEventRecord(ctx->upload_ev, st));
+  return s;
+}
+
 
 // Allocates one side's per-round arrays for nreg regions.
 template <typename T>
@@ -956,7 +1079,9 @@ BatchCaps batch_caps() {
   return c;
 }
 constexpr unsigned long long kBatchHeadCap = 2048;        // threshold-pass list
-constexpr unsigned kBatchHeadWant = 256;
+// Threshold-pass list sizes: round 1 (large grids) and refinement rounds.
+constexpr unsigned kBatchHeadWant = 128;
+constexpr unsigned kBatchHeadWantRefine = 32;
 
 // One round's arrays in the slab.  TP sides hold the regions and basis tables
 // (and, in exact rounds, the cells); the FP32 screen's first round keeps its
@@ -1073,9 +1198,8 @@ void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, c
       launch_dist_cull(X, Y, R.map1, R.map2, ns, R.surv, R.surv_lb, R.surv_cap, stats, screen, e, st, bt);
     });
   }
-  timed(L, "dist_pick", [&] {
-    launch_dist_pick(R.surv, R.surv_lb, R.surv_cap, R.head, kBatchHeadCap, kBatchHeadWant, stats, st, bt);
-  });
+  const unsigned want = R.max_slots == 1 ? kBatchHeadWant : kBatchHeadWantRefine;
+  timed(L, "dist_pick", [&] { launch_dist_pick(R.surv, R.surv_lb, R.surv_cap, R.head, kBatchHeadCap, want, stats, st, bt); });
   timed(L, "dist_head", [&] {
     launch_dist_head(X, Y, R.map1, R.map2, R.head, kFromDevice, kBatchHeadCap, k, stats, screen, e, st, bt);
   });
@@ -1151,20 +1275,25 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       launch_basis(va, Rd.A, st, bt, head_view<TP>(lay.head, 0));
       launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1));
     });
+    // Work units of the cell build: cells of both sides (exact in round 1,
+    // where every query has one region per side; the refinement rounds'
+    // region counts live on the device).
+    const double cells_units = r == 1 ? double(n) * (double(Rd.A.g.W) * Rd.A.g.W + double(Rd.B.g.W) * Rd.B.g.W) : 0.0;
+    const char *cells_name = r == 1 ? "cells_r1" : "cells";
     if (!scr) {
-      timed(L, "cells", [&] {
+      timed(L, cells_name, [&] {
         launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0));
         launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1));
-      });
+      }, cells_units);
       batch_screen<TP>(L, Rd, Rd.A, Rd.B, stats, p.k, false, 0.0f, bt);
       timed(L, "dist_select", [&] {
         launch_dist_select(static_cast<const DistCand<TP> *>(Rd.cand), Rd.cand_cap, p.k, Rd.top, stats, st, bt);
       });
     } else if constexpr (kScreen) {
-      timed(L, "cells", [&] {
+      timed(L, cells_name, [&] {
         launch_cells_fused(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
         launch_cells_fused(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
-      });
+      }, cells_units);
       batch_screen<TC>(L, Rd, Rd.A32, Rd.B32, stats, p.k, true, e, bt);
       timed(L, "dist_verify", [&] {
         launch_dist_verify(view<double>(s0a), view<double>(s0b), Rd.A, Rd.B, Rd.map1, Rd.map2,
@@ -1638,6 +1767,10 @@ void worker_loop(jsi_context *ctx, Lane *L) {
       ++ctx->busy;
     }
     job->status = run_guarded(job->error, [&] {
+      {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        JSI_CUDA(cudaStreamWaitEvent(L->stream, ctx->upload_ev, 0));
+      }
       if (job->kind == 0)
         exec_distance(L, &job->a, &job->b, job->dp, &job->dres);
       else if (job->kind == 1)
@@ -1743,6 +1876,13 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
   ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (size_t(120) << 30);
   const int st = guarded(ctx, [&]() {
     lane_init(ctx->main, dev, arena, ctx->budget, &ctx->surfaces);
+    JSI_CUDA(cudaMallocHost(reinterpret_cast<void **>(&ctx->ring), kRingSeg * kRingSegs));
+    for (auto &e : ctx->ring_ev) {
+      JSI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      JSI_CUDA(cudaEventRecord(e, ctx->main.stream));
+    }
+    JSI_CUDA(cudaEventCreateWithFlags(&ctx->upload_ev, cudaEventDisableTiming));
+    JSI_CUDA(cudaEventRecord(ctx->upload_ev, ctx->main.stream));
     return JSI_OK;
   });
   if (st != JSI_OK) {
@@ -1758,8 +1898,11 @@ int jsi_destroy(jsi_context *ctx) {
   cudaSetDevice(ctx->device);
   stop_workers(ctx);
   if (ctx->main.stream) cudaStreamSynchronize(ctx->main.stream);
-  for (auto &kv : ctx->surfaces) free_surface(kv.second);
-  ctx->surfaces.clear();
+  ctx->surfaces.clear();  // pooled blocks go with the pool
+  for (auto &e : ctx->ring_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->upload_ev) cudaEventDestroy(ctx->upload_ev);
+  if (ctx->ring) cudaFreeHost(ctx->ring);
   lane_free(ctx->main);
   delete ctx;
   return JSI_OK;
@@ -1770,12 +1913,7 @@ int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, i
   std::lock_guard<std::mutex> lk(ctx->mu);
   return guarded(ctx, [&]() {
     JSI_CUDA(cudaSetDevice(ctx->device));
-    check_surface(ivec, data, ndata);
-    SurfaceRec s = upload_surface(&ctx->main, ivec, data, ndata, nullptr);
-    if (ctx->resident + s.bytes > ctx->budget) {
-      free_surface(s);
-      fail(JSI_ERR_NOMEM, "HBM budget exhausted by resident surfaces");
-    }
+    SurfaceRec s = upload_resident(ctx, ivec, data, ndata);
     ctx->resident += s.bytes;
     const int id = ctx->next_id++;
     ctx->surfaces[id] = s;
@@ -1790,12 +1928,33 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id) {
   auto it = ctx->surfaces.find(id);
   if (it == ctx->surfaces.end()) return record(ctx, JSI_ERR_INVALID, "unknown surface id");
   if (ctx->surface_refs.count(id)) return record(ctx, JSI_ERR_INVALID, "surface is used by a queued query");
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->main.stream);
+  // No query holds the surface: its block returns to the pool at once (a
+  // later upload into it is ordered after this one's copies on the main
+  // stream).
   ctx->resident -= it->second.bytes;
-  free_surface(it->second);
+  ctx->pool.put(it->second.block, it->second.block_bytes);
   ctx->surfaces.erase(it);
   return JSI_OK;
+}
+
+int jsi_surface_upload_many(jsi_context *ctx, int n, const int *ivecs, const float *const *datas, const int *ndatas,
+                            jsi_surface_id *out) {
+  if (!ctx || n < 0 || (n > 0 && (!ivecs || !datas || !ndatas || !out))) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  int done = 0;
+  const int st = guarded(ctx, [&]() {
+    JSI_CUDA(cudaSetDevice(ctx->device));
+    for (; done < n; ++done) {
+      SurfaceRec s = upload_resident(ctx, ivecs + 7 * done, datas[done], ndatas[done]);
+      ctx->resident += s.bytes;
+      const int id = ctx->next_id++;
+      ctx->surfaces[id] = s;
+      out[done] = id;
+    }
+    return JSI_OK;
+  });
+  for (int q = done; q < n; ++q) out[q] = 0;
+  return st;
 }
 
 int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out) {

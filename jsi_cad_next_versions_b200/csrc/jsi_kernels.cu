@@ -14,6 +14,7 @@
 //   intersect   k_inter_cull -> k_inter_leaf -> (device radix sort) -> k_inter_* dedup
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <climits>
@@ -1141,7 +1142,7 @@ __device__ __forceinline__ T shaved_lb(const Vec4<T> &lo1, const Vec4<T> &hi1, c
 }
 
 template <typename T, bool S>
-__global__ void __launch_bounds__(256) k_dist_expand(SideRound<T> a, SideRound<T> b, const int *map1,
+__global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T> b, const int *map1,
                                                      const int *map2, const unsigned long long *st_surv,
                                                      unsigned long long nst_surv, unsigned long long st_cap, int k,
                                                      int cull, unsigned long long *surv, unsigned *surv_lb,
@@ -2121,6 +2122,238 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
   }
 }
 
+// Distance cells without a sample grid in HBM.  One block per (region, band
+// of te cell rows, chunk of up to 32 tiles along u): the block evaluates the
+// band's (te + 1) x (32 te + 1) corner samples into shared memory, then one
+// warp per tile forms the tile's cell centres and centre range exactly as
+// k_cells does.  TB = precision of the basis tables, TC = of the samples and
+// cells (TB = double, TC = float: the FP32 screen).
+//
+// Samples are evaluated in factored form: a thread owns one sample column
+// (its u span and u basis), forms the u-direction sum of every control-net
+// row the band needs in registers, and combines them in v for each sample
+// row.  Each u sum and each v accumulation is the same operation sequence as
+// in eval_point / screen_point, so the samples carry the same bits.  The
+// kernel is compiled for degrees <= D in both directions (loops of fixed trip
+// count); bands needing more than D + 3 net rows (coarse grids) take the
+// per-sample path.
+constexpr int kBandTiles = 32;
+constexpr int kBandCols = kBandTiles * kMaxTile + 1;
+
+template <typename TC>
+constexpr size_t band_smem() {
+  return sizeof(Vec4<TC>) * (kMaxTile + 1) * kBandCols;
+}
+
+template <typename TB, typename TC, int D>
+__global__ void __launch_bounds__(256) k_cells_band(SurfView<TC> s, const SurfView<TC> *vdev, SideRound<TB> bs,
+                                                    SideRound<TC> out, long long qs) {
+  constexpr int kE = kMaxTile + 1;
+  constexpr int kP = D + 1;          // u basis values held per thread
+  constexpr int kBandRows = D + 3;   // net rows held per thread
+  extern __shared__ __align__(16) unsigned char band_raw[];
+  Vec4<TC> *S = reinterpret_cast<Vec4<TC> *>(band_raw);  // [kE][kBandCols]
+  __shared__ TC snv[kE][kBandRows];
+  __shared__ int ssv[kE];
+  const long long qo = qoff(qs);
+  if (vdev) s = *qsh(vdev, qo);
+  bs = qsh(bs, qo);
+  out = qsh(out, qo);
+  const Geom g = out.g;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int te = g.te, te2 = te * te, p1 = g.p1max;
+  const int nch = (g.tw + kBandTiles - 1) / kBandTiles;
+  const long long nunits = static_cast<long long>(nreg_of(bs)) * g.tw * nch;
+  for (long long unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+    const int r = static_cast<int>(unit / (static_cast<long long>(g.tw) * nch));
+    const int rest = static_cast<int>(unit - static_cast<long long>(r) * g.tw * nch);
+    const int ty = rest / nch, ch = rest - (rest / nch) * nch;
+    const int tx0 = ch * kBandTiles, ntx = min(kBandTiles, g.tw - tx0);
+    const int nv = min(te, g.W - ty * te);
+    const int nuc = min(ntx * te, g.W - tx0 * te);
+    const int ncols = nuc + 1;
+    const long long lu0 = (static_cast<long long>(r) * 2 + 0) * g.nuv + tx0 * te;
+    const long long lv0 = (static_cast<long long>(r) * 2 + 1) * g.nuv + ty * te;
+    const bool fit = !s.zero && s.degu <= D && s.degv <= D;
+    if (fit && tid <= nv) {
+      ssv[tid] = bs.spans[lv0 + tid];
+      const TB *N = bs.basis + (lv0 + tid) * 3 * p1;
+      for (int c = 0; c <= s.degv; ++c) {
+        if constexpr (std::is_same<TB, TC>::value) snv[tid][c] = N[c];
+        else snv[tid][c] = __double2float_rn(N[c]);
+      }
+    }
+    __syncthreads();
+    int rmin = 0, nrows = kBandRows + 1;
+    if (fit) {
+      int lo = INT_MAX, hi = INT_MIN;
+      for (int a = 0; a <= nv; ++a) {
+        lo = min(lo, ssv[a]);
+        hi = max(hi, ssv[a]);
+      }
+      rmin = lo - s.degv;
+      nrows = hi - rmin + 1;
+    }
+    const bool factored = fit && nrows <= kBandRows;
+    for (int col = tid; col < ncols; col += blockDim.x) {
+      const long long lu = lu0 + col;
+      if (factored) {
+        const int su = bs.spans[lu];
+        const TB *Nb = bs.basis + lu * 3 * p1;
+        TC Nu[kP];
+#pragma unroll
+        for (int c = 0; c < kP; ++c) {
+          if (c <= s.degu) {
+            if constexpr (std::is_same<TB, TC>::value) Nu[c] = Nb[c];
+            else Nu[c] = __double2float_rn(Nb[c]);
+          }
+        }
+        TC rs[kBandRows][4];
+#pragma unroll
+        for (int R = 0; R < kBandRows; ++R) {
+          TC r0 = TC(0), r1 = TC(0), r2 = TC(0), r3 = TC(0);
+          if (R < nrows) {
+            const Vec4<TC> *cp = s.cpw + static_cast<long long>(s.ncpu) * (rmin + R) + (su - s.degu);
+#pragma unroll
+            for (int c = 0; c < kP; ++c) {
+              if (c <= s.degu) {
+                const Vec4<TC> q = cp[c];
+                if constexpr (std::is_same<TB, TC>::value) {
+                  if (!s.rat) {
+                    const TC n = Nu[c];
+                    r0 += n * q.x;
+                    r1 += n * q.y;
+                    r2 += n * q.z;
+                  } else {
+                    const TC nw = Nu[c] * q.w;
+                    r0 += nw * q.x;
+                    r1 += nw * q.y;
+                    r2 += nw * q.z;
+                    r3 += nw;
+                  }
+                } else {
+                  float n = Nu[c];
+                  if (s.rat) {
+                    n = __fmul_rn(n, q.w);
+                    r3 = __fadd_rn(r3, n);
+                  }
+                  r0 = __fmaf_rn(n, q.x, r0);
+                  r1 = __fmaf_rn(n, q.y, r1);
+                  r2 = __fmaf_rn(n, q.z, r2);
+                }
+              }
+            }
+          }
+          rs[R][0] = r0;
+          rs[R][1] = r1;
+          rs[R][2] = r2;
+          rs[R][3] = r3;
+        }
+        for (int a = 0; a <= nv; ++a) {
+          const int R0 = ssv[a] - s.degv - rmin;
+          TC a0 = TC(0), a1 = TC(0), a2 = TC(0), a3 = TC(0);
+#pragma unroll
+          for (int R = 0; R < kBandRows; ++R) {
+            if (R >= R0 && R - R0 <= s.degv) {
+              const TC m = snv[a][R - R0];
+              if constexpr (std::is_same<TB, TC>::value) {
+                a0 += m * rs[R][0];
+                a1 += m * rs[R][1];
+                a2 += m * rs[R][2];
+                a3 += m * rs[R][3];
+              } else {
+                a0 = __fmaf_rn(m, rs[R][0], a0);
+                a1 = __fmaf_rn(m, rs[R][1], a1);
+                a2 = __fmaf_rn(m, rs[R][2], a2);
+                a3 = __fmaf_rn(m, rs[R][3], a3);
+              }
+            }
+          }
+          Vec4<TC> P{a0, a1, a2, TC(0)};
+          if (s.rat) {
+            if constexpr (std::is_same<TB, TC>::value) {
+              const TC inv = TC(1) / a3;
+              P.x = a0 * inv;
+              P.y = a1 * inv;
+              P.z = a2 * inv;
+            } else {
+              const double w = static_cast<double>(a3);
+              P.x = __double2float_rn(static_cast<double>(a0) / w);
+              P.y = __double2float_rn(static_cast<double>(a1) / w);
+              P.z = __double2float_rn(static_cast<double>(a2) / w);
+            }
+          }
+          S[a * kBandCols + col] = P;
+        }
+      } else {
+        for (int a = 0; a <= nv; ++a) {
+          const long long lv = lv0 + a;
+          const TB *Nu = bs.basis + lu * 3 * p1;
+          const TB *Nv = bs.basis + lv * 3 * p1;
+          Vec4<TC> P;
+          if constexpr (std::is_same<TB, TC>::value) {
+            TC q[3];
+            eval_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv, q);
+            P = Vec4<TC>{q[0], q[1], q[2], TC(0)};
+          } else {
+            P = screen_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv);
+          }
+          S[a * kBandCols + col] = P;
+        }
+      }
+    }
+    __syncthreads();
+    // Cells, one warp per tile of the chunk (k_cells' arithmetic and layout).
+    for (int j = warp; j < ntx; j += blockDim.x >> 5) {
+      const int tx = tx0 + j;
+      const int nu = min(te, g.W - tx * te);
+      const long long t = static_cast<long long>(r) * g.ntiles + ty * g.tw + tx;
+      TC lo[3] = {pos_inf<TC>(), pos_inf<TC>(), pos_inf<TC>()};
+      TC hi[3] = {-pos_inf<TC>(), -pos_inf<TC>(), -pos_inf<TC>()};
+      for (int local = lane; local < te2; local += 32) {
+        const int a = local / te, b = local - (local / te) * te;
+        Vec4<TC> cen{TC(0), TC(0), TC(0), TC(0)};
+        if (a < nv && b < nu) {
+          const int c0 = j * te + b;
+          const Vec4<TC> p0 = S[a * kBandCols + c0];
+          const Vec4<TC> p1v = S[a * kBandCols + c0 + 1];
+          const Vec4<TC> p2 = S[(a + 1) * kBandCols + c0];
+          const Vec4<TC> p3 = S[(a + 1) * kBandCols + c0 + 1];
+          const TC lx = tmin(p0.x, tmin(p1v.x, tmin(p2.x, p3.x)));
+          const TC ly = tmin(p0.y, tmin(p1v.y, tmin(p2.y, p3.y)));
+          const TC lz = tmin(p0.z, tmin(p1v.z, tmin(p2.z, p3.z)));
+          const TC hx = tmax(p0.x, tmax(p1v.x, tmax(p2.x, p3.x)));
+          const TC hy = tmax(p0.y, tmax(p1v.y, tmax(p2.y, p3.y)));
+          const TC hz = tmax(p0.z, tmax(p1v.z, tmax(p2.z, p3.z)));
+          cen.x = (lx - TC(0) + hx + TC(0)) / TC(2);
+          cen.y = (ly - TC(0) + hy + TC(0)) / TC(2);
+          cen.z = (lz - TC(0) + hz + TC(0)) / TC(2);
+          lo[0] = tmin(lo[0], cen.x);
+          lo[1] = tmin(lo[1], cen.y);
+          lo[2] = tmin(lo[2], cen.z);
+          hi[0] = tmax(hi[0], cen.x);
+          hi[1] = tmax(hi[1], cen.y);
+          hi[2] = tmax(hi[2], cen.z);
+        }
+        out.center[t * te2 + local] = cen;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          lo[c] = tmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+          hi[c] = tmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+        }
+      }
+      if (lane == 0) {
+        out.tlo[t] = Vec4<TC>{lo[0], lo[1], lo[2], TC(0)};
+        out.thi[t] = Vec4<TC>{hi[0], hi[1], hi[2], TC(0)};
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // FP64 centre of one cell exactly as the FP64 form builds it: P at the four
 // corners from the FP64 basis tables (eval_point), min/max, (lo - 0 + hi + 0)/2.
 __device__ Vec4<double> cell_center64(const SurfView<double> &s, const SideRound<double> &sr, int region, int cell) {
@@ -2399,6 +2632,26 @@ __global__ void k_newton_inter(SurfView<double> sa, SurfView<double> sb, const R
   for (int q = 0; q < 8; ++q) out[e * 8 + q] = o[q];
 }
 
+// Resident surface layout from the raw EGADS record (knots, xyz net, weights;
+// include/nurbs_data.hpp:1-10): FP64 knot vectors and the (x, y, z, w) nets
+// in FP32 and FP64 (w = 1 when non-rational).  Exact conversions.
+__global__ void k_surface_prep(const float *raw, int nku, int nkv, long long ncp, int rat, double *U64, double *V64,
+                               Vec4<float> *cpw32, Vec4<double> *cpw64) {
+  const long long n = ncp > nku + nkv ? ncp : nku + nkv;
+  const float *cp = raw + nku + nkv;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    if (t < nku) U64[t] = static_cast<double>(raw[t]);
+    else if (t < nku + nkv) V64[t - nku] = static_cast<double>(raw[t]);
+    if (t < ncp) {
+      const float w = rat ? cp[3 * ncp + t] : 1.0f;
+      const float x = cp[3 * t], y = cp[3 * t + 1], z = cp[3 * t + 2];
+      cpw32[t] = Vec4<float>{x, y, z, w};
+      cpw64[t] = Vec4<double>{x, y, z, w};
+    }
+  }
+}
+
 inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -2580,16 +2833,17 @@ void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int 
                         ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
   if (nst_surv == 0) return;
+  // One 128-thread block per supertile pair (2 x 64 child pre-filter lanes).
   const unsigned long long most = nst_surv == kFromDevice ? st_cap : nst_surv;
-  const dim3 grid = bdim(bgrid(static_cast<long long>(most < 148ull * 8 ? most : 148ull * 8), bt, 148 * 8), bt);
+  const dim3 grid = bdim(bgrid(static_cast<long long>(most < 148ull * 32 ? most : 148ull * 32), bt, 148 * 32), bt);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
-      k_dist_expand<float, true><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, st_cap, k, cull, surv,
+      k_dist_expand<float, true><<<grid, 128, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, st_cap, k, cull, surv,
                                                         surv_lb, cap, stats, e, bt.qs);
       return;
     }
   }
-  k_dist_expand<T, false><<<grid, 256, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, st_cap, k, cull, surv, surv_lb,
+  k_dist_expand<T, false><<<grid, 128, 0, st>>>(a, b, map1, map2, st_surv, nst_surv, st_cap, k, cull, surv, surv_lb,
                                                  cap, stats, e, bt.qs);
 }
 
@@ -2700,13 +2954,35 @@ void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &ba
   k_samples_screen<<<bdim(bgrid((n + 127) / 128, bt, 148 * 32), bt), 128, 0, st>>>(s, vdev, basis_side, out, bt.qs);
 }
 
+void launch_surface_prep(const float *raw, int nku, int nkv, long long ncp, int rat, double *U64, double *V64,
+                         Vec4<float> *cpw32, Vec4<double> *cpw64, cudaStream_t st) {
+  counted();
+  const long long n = std::max<long long>(nku + nkv, ncp);
+  k_surface_prep<<<grid_for(n, 256), 256, 0, st>>>(raw, nku, nkv, ncp, rat, U64, V64, cpw32, cpw64);
+}
+
 template <typename TB, typename TC>
 void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
                         const Batch &bt, const SurfView<TC> *vdev) {
   counted();
-  const long long warps = static_cast<long long>(bs.nreg) * out.g.ntiles;
+  const Geom &g = out.g;
+  if (g.tw >= 16 && s.degu <= 3 && s.degv <= 3) {
+    // Large grids of bicubic-or-lower surfaces (degrees are part of a batch's
+    // shape): whole bands per block.
+    constexpr size_t smem = band_smem<TC>();
+    static bool configured = false;
+    if (!configured) {
+      cudaFuncSetAttribute(k_cells_band<TB, TC, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem));
+      configured = true;
+    }
+    const long long units = static_cast<long long>(bs.nreg) * g.tw * ((g.tw + kBandTiles - 1) / kBandTiles);
+    k_cells_band<TB, TC, 3><<<bdim(bgrid(units, bt, 148 * 16), bt), 256, smem, st>>>(s, vdev, bs, out, bt.qs);
+    return;
+  }
+  const long long warps = static_cast<long long>(bs.nreg) * g.ntiles;
   const dim3 grid = bdim(bgrid((warps + 3) / 4, bt, 148 * 64), bt);
-  if (out.g.p1max <= 9)
+  if (g.p1max <= 9)
     k_cells_fused<TB, TC, 9><<<grid, 128, 0, st>>>(s, vdev, bs, out, bt.qs);
   else
     k_cells_fused<TB, TC, kMaxDeg + 1><<<grid, 128, 0, st>>>(s, vdev, bs, out, bt.qs);

@@ -164,3 +164,37 @@ def test_batch_full_size_screen():
         tasks = _upload_pairs(ctx, _hard_wave_pairs(6, seed0=1000), 512)
         batch = _check_batch(ctx, tasks, precision="fp32_screen", lanes=1)
         assert all(r.rounds == 4 for r in batch)
+
+
+def test_upload_many_release_reuse():
+    """Surfaces uploaded in one call, released, and other surfaces uploaded
+    into the recycled device blocks: every query sees its own surfaces."""
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        first = _hard_wave_pairs(4, seed0=1100)
+        second = _sine_pairs(4, seed0=1200)
+        ids = ctx.upload_many([x for pr in first for x in pr])
+        t1 = [(ctx.task(a, rect32(A), 96, 1), ctx.task(b, rect32(B), 96, 2))
+              for (a, b), (A, B) in zip(zip(ids[0::2], ids[1::2]), first)]
+        r1 = [ctx.min_distance(ta, tb, precision="fp64") for ta, tb in t1]
+        for sid in ids:
+            ctx.release(sid)
+        ids2 = ctx.upload_many([x for pr in second for x in pr])
+        t2 = [(ctx.task(a, rect32(A), 40, 1), ctx.task(b, rect32(B), 40, 2))
+              for (a, b), (A, B) in zip(zip(ids2[0::2], ids2[1::2]), second)]
+        ctx.workers(2)
+        try:
+            batch, _ = ctx.min_distance_batch(t2, precision="fp64")
+        finally:
+            ctx.workers(0)
+        # reference values from a fresh context
+        with J.Context(0) as c2:
+            for (A, B), r in zip(second, batch):
+                ta = c2.task(c2.upload(A), rect32(A), 40, 1)
+                tb = c2.task(c2.upload(B), rect32(B), 40, 2)
+                assert c2.min_distance(ta, tb, precision="fp64").distance == r.distance
+        with J.Context(0) as c3:
+            for (A, B), r in zip(first, r1):
+                ta = c3.task(c3.upload(A), rect32(A), 96, 1)
+                tb = c3.task(c3.upload(B), rect32(B), 96, 2)
+                assert c3.min_distance(ta, tb, precision="fp64").distance == r.distance
