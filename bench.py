@@ -69,6 +69,10 @@ UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "cells
              "dist_tau": (8, 0),
              "dist_cull": (14, 0), "dist_leaf": (8, 0), "dist_head": (8, 0), "inter_cull": (14, 0),
              "inter_leaf": (9, 0)}
+# DRAM traffic per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch / its units), for the form it was captured in:
+# profiles/k_cells_band_hardwave_n512.md (FP32 screen, 128 x 511^2 cells).
+MEASURED_TRAFFIC = {("cells_r1", "fp32_screen"): 15.44}
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 74.4: 148 SMs x 128 lanes x FMA x 1.965 GHz
 NOMINAL_FP64_TFLOPS = NOMINAL_FP32_TFLOPS / 2
 
@@ -87,8 +91,10 @@ def roofline(kernel, kt, form, peaks):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     tflops = per_launch_units * flops_u / avg_s / 1e12 if avg_s > 0 else 0.0
     fp_peak = NOMINAL_FP64_TFLOPS if fp64 else NOMINAL_FP32_TFLOPS
+    tb = MEASURED_TRAFFIC.get((kernel, form))
+    traffic = per_launch_units * tb if tb else None
     return {"bound": "hbm", "kernel": kernel, "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
-            "frac": gbs / hbm_peak, "traffic": None,
+            "frac": gbs / hbm_peak, "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled by units)",
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
             "avg_launch_ms": avg_s * 1e3, "units_per_launch": per_launch_units,
             "compute": {"achieved": tflops, "peak": fp_peak, "unit": "TFLOP/s", "frac": tflops / fp_peak,
@@ -156,7 +162,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
         return self
@@ -303,24 +309,27 @@ def run_ours(args):
             res, _ = ctx.min_distance_batch(tasks, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
             step_distances.extend(r.distance for r in res)
             return [r.device_ms for r in res], res[-1]
+        # Clocks are sampled from the warm-up on (all of it runs under load):
+        # the timed steps alone are shorter than nvidia-smi's start-up.
+        clk = ClockSampler(local)
+        clk.__enter__()
         for _ in range(args.warmup):
             step()
         reruns0 = ctx.batch_reruns()
         launches0 = ctx.launch_count()
         step_ms, lats = [], []
-        with ClockSampler(local) as clk:
-            for _ in range(args.steps):
-                flush.zero_()
-                barrier()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                l, last = step()
-                e1.record(stream)
-                torch.cuda.synchronize()
-                barrier()
-                step_ms.append(max_over_ranks(e0.elapsed_time(e1)))
-                lats += l
+        for _ in range(args.steps):
+            flush.zero_()
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            l, last = step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            step_ms.append(max_over_ranks(e0.elapsed_time(e1)))
+            lats += l
         launches = ctx.launch_count() - launches0
         reruns = ctx.batch_reruns() - reruns0
         # Per-kernel breakdown in separate steps (events around every launch
@@ -332,6 +341,7 @@ def run_ours(args):
             step()
         ktimes = ctx.kernel_times()
         ctx.kernel_timing(False)
+        clk.__exit__(None, None, None)
         total_ms = sum(step_ms)
         results[form] = {
             "value": world * args.batch * args.steps / (total_ms / 1e3), "ms_per_step": total_ms / args.steps,
