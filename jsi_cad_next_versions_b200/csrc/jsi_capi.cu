@@ -299,7 +299,8 @@ struct jsi_context {
   size_t lane_keep = 0;              // steady arena size a lane keeps after a query
   size_t resident = 0;
   SurfacePool pool;
-  char *ring = nullptr;
+  char *ring = nullptr;   // pinned staging
+  char *dring = nullptr;  // its device mirror (records + prep jobs)
   int ring_cur = 0;
   size_t ring_off = 0;
   cudaEvent_t ring_ev[kRingSegs] = {};
@@ -479,11 +480,19 @@ const SurfaceRec &get_surface(Lane *ctx, jsi_surface_id id) {
 
 namespace {
 
-// Resident upload on the main stream without a host sync: the raw record
-// goes through the pinned ring into the surface's pooled block (where it is
-// also the FP32 knot vectors), a kernel builds the FP64 knots and the nets,
-// and upload_ev marks the point that worker lanes wait for.
-SurfaceRec upload_resident(jsi_context *ctx, const int ivec[7], const float *data, int ndata) {
+// Resident uploads on the main stream without a host sync.  Records (and
+// the prep jobs) are packed into the current segment of the pinned ring,
+// copied in one piece to the segment's device mirror, and one prep launch
+// writes every surface's block (record, FP64 knots, nets).  upload_ev marks
+// the point that worker lanes wait for.  A record larger than a segment goes
+// through a temporary device buffer and completes before returning.
+struct PendingSurface {
+  const int *ivec;
+  const float *data;
+  int ndata;
+};
+
+SurfaceRec make_block(jsi_context *ctx, const int ivec[7], const float *data, int ndata, SurfacePrep *job) {
   check_surface(ivec, data, ndata);
   SurfaceRec s;
   surface_header(s, ivec, data);
@@ -506,29 +515,89 @@ SurfaceRec upload_resident(jsi_context *ctx, const int ivec[7], const float *dat
   s.V64 = reinterpret_cast<double *>(blk + raw_b + u64_b);
   s.cpw32 = reinterpret_cast<Vec4<float> *>(blk + raw_b + u64_b + v64_b);
   s.cpw64 = reinterpret_cast<Vec4<double> *>(blk + raw_b + u64_b + v64_b + c32_b);
+  job->src = nullptr;
+  job->raw = s.U32;
+  job->U64 = s.U64;
+  job->V64 = s.V64;
+  job->cpw32 = s.cpw32;
+  job->cpw64 = s.cpw64;
+  job->ndata = ndata;
+  job->ncp = static_cast<long long>(ncp);
+  job->nku = nku;
+  job->nkv = nkv;
+  job->rat = s.rat;
+  job->pad_ = 0;
+  return s;
+}
+
+void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &in, std::vector<SurfaceRec> &out) {
   Lane *L = &ctx->main;
   cudaStream_t st = L->stream;
-  const size_t nbytes = static_cast<size_t>(ndata) * sizeof(float);
-  if (nbytes <= kRingSeg) {
-    if (ctx->ring_off + nbytes > kRingSeg) {
-      JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
-      ctx->ring_cur = (ctx->ring_cur + 1) % kRingSegs;
-      ctx->ring_off = 0;
-      JSI_CUDA(cudaEventSynchronize(ctx->ring_ev[ctx->ring_cur]));
+  auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  auto next_segment = [&]() {
+    JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
+    ctx->ring_cur = (ctx->ring_cur + 1) % kRingSegs;
+    ctx->ring_off = 0;
+    JSI_CUDA(cudaEventSynchronize(ctx->ring_ev[ctx->ring_cur]));
+  };
+  size_t q = 0;
+  while (q < in.size()) {
+    const size_t rec_b = al(static_cast<size_t>(in[q].ndata) * sizeof(float));
+    if (rec_b + al(sizeof(SurfacePrep)) > kRingSeg) {
+      // Larger than a segment: its own device staging, completed here.
+      SurfacePrep job;
+      out.push_back(make_block(ctx, in[q].ivec, in[q].data, in[q].ndata, &job));
+      char *tmp = nullptr;
+      if (cudaMalloc(&tmp, rec_b + al(sizeof(SurfacePrep))) != cudaSuccess) {
+        cudaGetLastError();
+        fail(JSI_ERR_NOMEM, "cudaMalloc of %zu bytes to stage a surface failed", rec_b);
+      }
+      job.src = reinterpret_cast<const float *>(tmp);
+      JSI_CUDA(copy_async(L, tmp, in[q].data, static_cast<size_t>(in[q].ndata) * sizeof(float),
+                          cudaMemcpyHostToDevice, st));
+      JSI_CUDA(copy_async(L, tmp + rec_b, &job, sizeof(job), cudaMemcpyHostToDevice, st));
+      launch_surface_prep(reinterpret_cast<const SurfacePrep *>(tmp + rec_b), 1, std::max<long long>(job.ndata, job.ncp),
+                          st);
+      JSI_CUDA(cudaStreamSynchronize(st));
+      cudaFree(tmp);
+      ++q;
+      continue;
     }
-    char *stage = ctx->ring + static_cast<size_t>(ctx->ring_cur) * kRingSeg + ctx->ring_off;
-    std::memcpy(stage, data, nbytes);
-    JSI_CUDA(copy_async(L, blk, stage, nbytes, cudaMemcpyHostToDevice, st));
-    ctx->ring_off += (nbytes + 255) & ~static_cast<size_t>(255);
-  } else {
-    // Larger than a ring segment: pageable copy, completed before returning.
-    JSI_CUDA(copy_async(L, blk, data, nbytes, cudaMemcpyHostToDevice, st));
-    JSI_CUDA(cudaStreamSynchronize(st));
+    // Pack as many records as fit in the rest of the segment, then the jobs.
+    if (ctx->ring_off + rec_b + al(sizeof(SurfacePrep)) > kRingSeg) next_segment();
+    const size_t seg0 = static_cast<size_t>(ctx->ring_cur) * kRingSeg;
+    size_t off = ctx->ring_off;
+    std::vector<SurfacePrep> jobs;
+    long long most = 0;
+    while (q < in.size()) {
+      const size_t rb = al(static_cast<size_t>(in[q].ndata) * sizeof(float));
+      if (off + rb + al(sizeof(SurfacePrep) * (jobs.size() + 1)) > kRingSeg) break;
+      SurfacePrep job;
+      out.push_back(make_block(ctx, in[q].ivec, in[q].data, in[q].ndata, &job));
+      std::memcpy(ctx->ring + seg0 + off, in[q].data, static_cast<size_t>(in[q].ndata) * sizeof(float));
+      job.src = reinterpret_cast<const float *>(ctx->dring + seg0 + off);
+      most = std::max(most, std::max(job.ndata, job.ncp));
+      jobs.push_back(job);
+      off += rb;
+      ++q;
+    }
+    const size_t jobs_b = sizeof(SurfacePrep) * jobs.size();
+    std::memcpy(ctx->ring + seg0 + off, jobs.data(), jobs_b);
+    const size_t start = ctx->ring_off;
+    JSI_CUDA(copy_async(L, ctx->dring + seg0 + start, ctx->ring + seg0 + start, off + jobs_b - start,
+                        cudaMemcpyHostToDevice, st));
+    launch_surface_prep(reinterpret_cast<const SurfacePrep *>(ctx->dring + seg0 + off), static_cast<int>(jobs.size()),
+                        most, st);
+    ctx->ring_off = off + al(jobs_b);
   }
-  launch_surface_prep(s.U32, nku, nkv, static_cast<long long>(ncp), s.rat, s.U64, s.V64, s.cpw32, s.cpw64, st);
   JSI_CUDA(cudaGetLastError());
   JSI_CUDA(cudaEventRecord(ctx->upload_ev, st));
-  return s;
+}
+
+SurfaceRec upload_resident(jsi_context *ctx, const int ivec[7], const float *data, int ndata) {
+  std::vector<SurfaceRec> out;
+  upload_resident_many(ctx, {PendingSurface{ivec, data, ndata}}, out);
+  return out[0];
 }
 
 
@@ -1877,6 +1946,7 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
   const int st = guarded(ctx, [&]() {
     lane_init(ctx->main, dev, arena, ctx->budget, &ctx->surfaces);
     JSI_CUDA(cudaMallocHost(reinterpret_cast<void **>(&ctx->ring), kRingSeg * kRingSegs));
+    JSI_CUDA(cudaMalloc(reinterpret_cast<void **>(&ctx->dring), kRingSeg * kRingSegs));
     for (auto &e : ctx->ring_ev) {
       JSI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       JSI_CUDA(cudaEventRecord(e, ctx->main.stream));
@@ -1903,6 +1973,7 @@ int jsi_destroy(jsi_context *ctx) {
     if (e) cudaEventDestroy(e);
   if (ctx->upload_ev) cudaEventDestroy(ctx->upload_ev);
   if (ctx->ring) cudaFreeHost(ctx->ring);
+  if (ctx->dring) cudaFree(ctx->dring);
   lane_free(ctx->main);
   delete ctx;
   return JSI_OK;
@@ -1944,11 +2015,21 @@ int jsi_surface_upload_many(jsi_context *ctx, int n, const int *ivecs, const flo
   int done = 0;
   const int st = guarded(ctx, [&]() {
     JSI_CUDA(cudaSetDevice(ctx->device));
+    std::vector<PendingSurface> in;
+    in.reserve(n);
+    for (int q = 0; q < n; ++q) in.push_back(PendingSurface{ivecs + 7 * q, datas[q], ndatas[q]});
+    std::vector<SurfaceRec> recs;
+    recs.reserve(n);
+    try {
+      upload_resident_many(ctx, in, recs);
+    } catch (...) {
+      for (auto &r : recs) ctx->pool.put(r.block, r.block_bytes);  // none becomes resident
+      throw;
+    }
     for (; done < n; ++done) {
-      SurfaceRec s = upload_resident(ctx, ivecs + 7 * done, datas[done], ndatas[done]);
-      ctx->resident += s.bytes;
+      ctx->resident += recs[done].bytes;
       const int id = ctx->next_id++;
-      ctx->surfaces[id] = s;
+      ctx->surfaces[id] = recs[done];
       out[done] = id;
     }
     return JSI_OK;

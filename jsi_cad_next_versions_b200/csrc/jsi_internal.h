@@ -218,10 +218,19 @@ void launch_dist_head(const SideRound<T> &a, const SideRound<T> &b, const int *m
 // FP32-screen form: FP32 samples from FP64 basis tables; FP64 re-check.
 void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
                            cudaStream_t st, const Batch &bt = Batch{}, const SurfView<float> *vdev = nullptr);
-// Resident surface layout (FP64 knots, FP32/FP64 (x, y, z, w) nets) from the
-// raw float record already on the device.
-void launch_surface_prep(const float *raw, int nku, int nkv, long long ncp, int rat, double *U64, double *V64,
-                         Vec4<float> *cpw32, Vec4<double> *cpw64, cudaStream_t st);
+// Resident surface layout from raw float records staged on the device: the
+// record copied into its block, FP64 knots, FP32/FP64 (x, y, z, w) nets.
+struct SurfacePrep {
+  const float *src;  // staged record
+  float *raw;        // the record in the surface's block
+  double *U64, *V64;
+  Vec4<float> *cpw32;
+  Vec4<double> *cpw64;
+  long long ndata, ncp;
+  int nku, nkv, rat, pad_;
+};
+// jobs: device array of n entries; most = the largest max(ndata, ncp).
+void launch_surface_prep(const SurfacePrep *jobs, int n, long long most, cudaStream_t st);
 // Distance cells straight from the basis tables (no sample grid in HBM):
 // centres and tile ranges of out, bit-identical to launch_samples(_screen) +
 // launch_cells.  TB = basis precision, TC = cell precision.

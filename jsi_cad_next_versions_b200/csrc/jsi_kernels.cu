@@ -37,6 +37,15 @@ template <typename T>
 __device__ __forceinline__ T tmax(T a, T b) {  // std::max
   return (a < b) ? b : a;
 }
+// Single-instruction min / max for the distance cells: they differ from
+// std::min / std::max only in which zero (+0 / -0) they return on a tie and
+// for NaN.  A distance centre is ((lo - 0) + hi) + 0, and the trailing + 0
+// turns a -0 sum into +0, so the choice of zero never reaches a centre, and
+// centres are never -0; coordinates are finite.
+__device__ __forceinline__ float fmn(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double fmn(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float fmx(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmx(double a, double b) { return fmax(a, b); }
 
 __device__ __forceinline__ unsigned long long ordered_bits(float x) { return __float_as_uint(x); }
 __device__ __forceinline__ unsigned long long ordered_bits(double x) {
@@ -2088,21 +2097,21 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
         const Vec4<TC> p1v = S[a * sw + b + 1];
         const Vec4<TC> p2 = S[(a + 1) * sw + b];
         const Vec4<TC> p3 = S[(a + 1) * sw + b + 1];
-        const TC lx = tmin(p0.x, tmin(p1v.x, tmin(p2.x, p3.x)));
-        const TC ly = tmin(p0.y, tmin(p1v.y, tmin(p2.y, p3.y)));
-        const TC lz = tmin(p0.z, tmin(p1v.z, tmin(p2.z, p3.z)));
-        const TC hx = tmax(p0.x, tmax(p1v.x, tmax(p2.x, p3.x)));
-        const TC hy = tmax(p0.y, tmax(p1v.y, tmax(p2.y, p3.y)));
-        const TC hz = tmax(p0.z, tmax(p1v.z, tmax(p2.z, p3.z)));
+        const TC lx = fmn(p0.x, fmn(p1v.x, fmn(p2.x, p3.x)));
+        const TC ly = fmn(p0.y, fmn(p1v.y, fmn(p2.y, p3.y)));
+        const TC lz = fmn(p0.z, fmn(p1v.z, fmn(p2.z, p3.z)));
+        const TC hx = fmx(p0.x, fmx(p1v.x, fmx(p2.x, p3.x)));
+        const TC hy = fmx(p0.y, fmx(p1v.y, fmx(p2.y, p3.y)));
+        const TC hz = fmx(p0.z, fmx(p1v.z, fmx(p2.z, p3.z)));
         cen.x = (lx - TC(0) + hx + TC(0)) / TC(2);
         cen.y = (ly - TC(0) + hy + TC(0)) / TC(2);
         cen.z = (lz - TC(0) + hz + TC(0)) / TC(2);
-        lo[0] = tmin(lo[0], cen.x);
-        lo[1] = tmin(lo[1], cen.y);
-        lo[2] = tmin(lo[2], cen.z);
-        hi[0] = tmax(hi[0], cen.x);
-        hi[1] = tmax(hi[1], cen.y);
-        hi[2] = tmax(hi[2], cen.z);
+        lo[0] = fmn(lo[0], cen.x);
+        lo[1] = fmn(lo[1], cen.y);
+        lo[2] = fmn(lo[2], cen.z);
+        hi[0] = fmx(hi[0], cen.x);
+        hi[1] = fmx(hi[1], cen.y);
+        hi[2] = fmx(hi[2], cen.z);
       }
       out.center[t * te2 + local] = cen;
     }
@@ -2110,8 +2119,8 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        lo[c] = tmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
-        hi[c] = tmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+        lo[c] = fmn(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+        hi[c] = fmx(hi[c], __shfl_xor_sync(kFull, hi[c], o));
       }
     }
     if (lane == 0) {
@@ -2139,6 +2148,7 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
 // per-sample path.
 constexpr int kBandTiles = 32;
 constexpr int kBandCols = kBandTiles * kMaxTile + 1;
+constexpr int kBandThreads = 288;  // one thread per sample column (257) in one pass
 
 template <typename TC>
 constexpr size_t band_smem() {
@@ -2146,14 +2156,19 @@ constexpr size_t band_smem() {
 }
 
 template <typename TB, typename TC, int D>
-__global__ void __launch_bounds__(256) k_cells_band(SurfView<TC> s, const SurfView<TC> *vdev, SideRound<TB> bs,
-                                                    SideRound<TC> out, long long qs) {
+__global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells_band(SurfView<TC> s, const SurfView<TC> *vdev,
+                                                              SideRound<TB> bs, SideRound<TC> out, long long qs) {
   constexpr int kE = kMaxTile + 1;
   constexpr int kP = D + 1;          // u basis values held per thread
   constexpr int kBandRows = D + 3;   // net rows held per thread
   extern __shared__ __align__(16) unsigned char band_raw[];
   Vec4<TC> *S = reinterpret_cast<Vec4<TC> *>(band_raw);  // [kE][kBandCols]
   __shared__ TC snv[kE][kBandRows];
+  // v coefficients of each sample row over the band's net rows, zero outside
+  // the row's degv + 1 window: adding 0 * (finite row sum) to an accumulator
+  // that starts at +0 (and so is never -0) leaves it unchanged, so the padded
+  // sum has the bits of the windowed one.
+  __shared__ TC coef[kE][kBandRows];
   __shared__ int ssv[kE];
   const long long qo = qoff(qs);
   if (vdev) s = *qsh(vdev, qo);
@@ -2195,6 +2210,12 @@ __global__ void __launch_bounds__(256) k_cells_band(SurfView<TC> s, const SurfVi
       nrows = hi - rmin + 1;
     }
     const bool factored = fit && nrows <= kBandRows;
+    if (factored && tid < (nv + 1) * kBandRows) {
+      const int a = tid / kBandRows, R = tid - (tid / kBandRows) * kBandRows;
+      const int R0 = ssv[a] - s.degv - rmin;
+      coef[a][R] = (R >= R0 && R - R0 <= s.degv) ? snv[a][R - R0] : TC(0);
+    }
+    __syncthreads();
     for (int col = tid; col < ncols; col += blockDim.x) {
       const long long lu = lu0 + col;
       if (factored) {
@@ -2250,23 +2271,20 @@ __global__ void __launch_bounds__(256) k_cells_band(SurfView<TC> s, const SurfVi
           rs[R][3] = r3;
         }
         for (int a = 0; a <= nv; ++a) {
-          const int R0 = ssv[a] - s.degv - rmin;
           TC a0 = TC(0), a1 = TC(0), a2 = TC(0), a3 = TC(0);
 #pragma unroll
           for (int R = 0; R < kBandRows; ++R) {
-            if (R >= R0 && R - R0 <= s.degv) {
-              const TC m = snv[a][R - R0];
-              if constexpr (std::is_same<TB, TC>::value) {
-                a0 += m * rs[R][0];
-                a1 += m * rs[R][1];
-                a2 += m * rs[R][2];
-                a3 += m * rs[R][3];
-              } else {
-                a0 = __fmaf_rn(m, rs[R][0], a0);
-                a1 = __fmaf_rn(m, rs[R][1], a1);
-                a2 = __fmaf_rn(m, rs[R][2], a2);
-                a3 = __fmaf_rn(m, rs[R][3], a3);
-              }
+            const TC m = coef[a][R];
+            if constexpr (std::is_same<TB, TC>::value) {
+              a0 += m * rs[R][0];
+              a1 += m * rs[R][1];
+              a2 += m * rs[R][2];
+              if (s.rat) a3 += m * rs[R][3];
+            } else {
+              a0 = __fmaf_rn(m, rs[R][0], a0);
+              a1 = __fmaf_rn(m, rs[R][1], a1);
+              a2 = __fmaf_rn(m, rs[R][2], a2);
+              if (s.rat) a3 = __fmaf_rn(m, rs[R][3], a3);
             }
           }
           Vec4<TC> P{a0, a1, a2, TC(0)};
@@ -2319,21 +2337,21 @@ __global__ void __launch_bounds__(256) k_cells_band(SurfView<TC> s, const SurfVi
           const Vec4<TC> p1v = S[a * kBandCols + c0 + 1];
           const Vec4<TC> p2 = S[(a + 1) * kBandCols + c0];
           const Vec4<TC> p3 = S[(a + 1) * kBandCols + c0 + 1];
-          const TC lx = tmin(p0.x, tmin(p1v.x, tmin(p2.x, p3.x)));
-          const TC ly = tmin(p0.y, tmin(p1v.y, tmin(p2.y, p3.y)));
-          const TC lz = tmin(p0.z, tmin(p1v.z, tmin(p2.z, p3.z)));
-          const TC hx = tmax(p0.x, tmax(p1v.x, tmax(p2.x, p3.x)));
-          const TC hy = tmax(p0.y, tmax(p1v.y, tmax(p2.y, p3.y)));
-          const TC hz = tmax(p0.z, tmax(p1v.z, tmax(p2.z, p3.z)));
+          const TC lx = fmn(p0.x, fmn(p1v.x, fmn(p2.x, p3.x)));
+          const TC ly = fmn(p0.y, fmn(p1v.y, fmn(p2.y, p3.y)));
+          const TC lz = fmn(p0.z, fmn(p1v.z, fmn(p2.z, p3.z)));
+          const TC hx = fmx(p0.x, fmx(p1v.x, fmx(p2.x, p3.x)));
+          const TC hy = fmx(p0.y, fmx(p1v.y, fmx(p2.y, p3.y)));
+          const TC hz = fmx(p0.z, fmx(p1v.z, fmx(p2.z, p3.z)));
           cen.x = (lx - TC(0) + hx + TC(0)) / TC(2);
           cen.y = (ly - TC(0) + hy + TC(0)) / TC(2);
           cen.z = (lz - TC(0) + hz + TC(0)) / TC(2);
-          lo[0] = tmin(lo[0], cen.x);
-          lo[1] = tmin(lo[1], cen.y);
-          lo[2] = tmin(lo[2], cen.z);
-          hi[0] = tmax(hi[0], cen.x);
-          hi[1] = tmax(hi[1], cen.y);
-          hi[2] = tmax(hi[2], cen.z);
+          lo[0] = fmn(lo[0], cen.x);
+          lo[1] = fmn(lo[1], cen.y);
+          lo[2] = fmn(lo[2], cen.z);
+          hi[0] = fmx(hi[0], cen.x);
+          hi[1] = fmx(hi[1], cen.y);
+          hi[2] = fmx(hi[2], cen.z);
         }
         out.center[t * te2 + local] = cen;
       }
@@ -2341,8 +2359,8 @@ __global__ void __launch_bounds__(256) k_cells_band(SurfView<TC> s, const SurfVi
       for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          lo[c] = tmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
-          hi[c] = tmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+          lo[c] = fmn(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+          hi[c] = fmx(hi[c], __shfl_xor_sync(kFull, hi[c], o));
         }
       }
       if (lane == 0) {
@@ -2633,21 +2651,25 @@ __global__ void k_newton_inter(SurfView<double> sa, SurfView<double> sb, const R
 }
 
 // Resident surface layout from the raw EGADS record (knots, xyz net, weights;
-// include/nurbs_data.hpp:1-10): FP64 knot vectors and the (x, y, z, w) nets
-// in FP32 and FP64 (w = 1 when non-rational).  Exact conversions.
-__global__ void k_surface_prep(const float *raw, int nku, int nkv, long long ncp, int rat, double *U64, double *V64,
-                               Vec4<float> *cpw32, Vec4<double> *cpw64) {
-  const long long n = ncp > nku + nkv ? ncp : nku + nkv;
-  const float *cp = raw + nku + nkv;
+// include/nurbs_data.hpp:1-10): the record itself (its first nku + nkv floats
+// are the FP32 knot vectors), FP64 knot vectors and the (x, y, z, w) nets in
+// FP32 and FP64 (w = 1 when non-rational).  Exact conversions.  One block row
+// (blockIdx.y) per surface of the upload.
+__global__ void k_surface_prep(const SurfacePrep *jobs) {
+  const SurfacePrep J = jobs[blockIdx.y];
+  const long long nk = J.nku + J.nkv;
+  const long long n = J.ndata > J.ncp ? J.ndata : J.ncp;
+  const float *cp = J.src + nk;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < n;
        t += static_cast<long long>(gridDim.x) * blockDim.x) {
-    if (t < nku) U64[t] = static_cast<double>(raw[t]);
-    else if (t < nku + nkv) V64[t - nku] = static_cast<double>(raw[t]);
-    if (t < ncp) {
-      const float w = rat ? cp[3 * ncp + t] : 1.0f;
+    if (t < J.ndata) J.raw[t] = J.src[t];
+    if (t < J.nku) J.U64[t] = static_cast<double>(J.src[t]);
+    else if (t < nk) J.V64[t - J.nku] = static_cast<double>(J.src[t]);
+    if (t < J.ncp) {
+      const float w = J.rat ? cp[3 * J.ncp + t] : 1.0f;
       const float x = cp[3 * t], y = cp[3 * t + 1], z = cp[3 * t + 2];
-      cpw32[t] = Vec4<float>{x, y, z, w};
-      cpw64[t] = Vec4<double>{x, y, z, w};
+      J.cpw32[t] = Vec4<float>{x, y, z, w};
+      J.cpw64[t] = Vec4<double>{x, y, z, w};
     }
   }
 }
@@ -2954,11 +2976,11 @@ void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &ba
   k_samples_screen<<<bdim(bgrid((n + 127) / 128, bt, 148 * 32), bt), 128, 0, st>>>(s, vdev, basis_side, out, bt.qs);
 }
 
-void launch_surface_prep(const float *raw, int nku, int nkv, long long ncp, int rat, double *U64, double *V64,
-                         Vec4<float> *cpw32, Vec4<double> *cpw64, cudaStream_t st) {
+void launch_surface_prep(const SurfacePrep *jobs, int n, long long most, cudaStream_t st) {
   counted();
-  const long long n = std::max<long long>(nku + nkv, ncp);
-  k_surface_prep<<<grid_for(n, 256), 256, 0, st>>>(raw, nku, nkv, ncp, rat, U64, V64, cpw32, cpw64);
+  if (n <= 0) return;
+  const int gx = static_cast<int>(std::min<long long>((most + 255) / 256, 64));
+  k_surface_prep<<<dim3(gx > 0 ? gx : 1, n, 1), 256, 0, st>>>(jobs);
 }
 
 template <typename TB, typename TC>
@@ -2977,7 +2999,8 @@ void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const Si
       configured = true;
     }
     const long long units = static_cast<long long>(bs.nreg) * g.tw * ((g.tw + kBandTiles - 1) / kBandTiles);
-    k_cells_band<TB, TC, 3><<<bdim(bgrid(units, bt, 148 * 16), bt), 256, smem, st>>>(s, vdev, bs, out, bt.qs);
+    k_cells_band<TB, TC, 3><<<bdim(bgrid(units, bt, 148 * 16), bt), kBandThreads, smem, st>>>(s, vdev, bs, out,
+                                                                                              bt.qs);
     return;
   }
   const long long warps = static_cast<long long>(bs.nreg) * g.ntiles;
