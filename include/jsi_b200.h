@@ -228,6 +228,10 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
 int jsi_batch_chunk(jsi_context *ctx, int chunk);
 /* Batch items re-run alone after an internal list overflowed (all lanes). */
 int jsi_batch_reruns(jsi_context *ctx, long long *out);
+/* Lockstep batches that repeat a shape, size and lane are captured once as a
+ * CUDA graph and replayed.  enable: 1 on (default), 0 off, -1 unchanged;
+ * replays (may be null) gets the replay count over all lanes. */
+int jsi_batch_graphs(jsi_context *ctx, int enable, long long *replays);
 
 /* --- grid evaluation -----------------------------------------------------
  * Replaces evalWithCuda(int*, float*, int, float, float, float, float, int,

@@ -32,7 +32,7 @@ EXPORTED = [
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
-    "jsi_queue_depth", "jsi_min_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns",
+    "jsi_queue_depth", "jsi_min_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs",
 ]
 
 
@@ -159,6 +159,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_batch_chunk.restype = I
     L.jsi_batch_reruns.argtypes = [P, ctypes.POINTER(LL)]
     L.jsi_batch_reruns.restype = I
+    L.jsi_batch_graphs.argtypes = [P, I, ctypes.POINTER(LL)]
+    L.jsi_batch_graphs.restype = I
     L.jsi_eval_grid_noalloc.argtypes = [P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                         I, P]
     L.jsi_eval_grid_noalloc.restype = I

@@ -255,6 +255,14 @@ class Context:
         lane job)."""
         self._check(self.lib.jsi_batch_chunk(self.handle, int(chunk)))
 
+    def batch_graphs(self, enable: bool | None = None) -> int:
+        """Switch CUDA-graph replay of repeated lockstep batches (None: leave
+        it); returns the number of replays so far."""
+        v = ctypes.c_longlong(0)
+        flag = -1 if enable is None else (1 if enable else 0)
+        self._check(self.lib.jsi_batch_graphs(self.handle, flag, ctypes.byref(v)))
+        return v.value
+
     def batch_reruns(self) -> int:
         """Batch items re-run alone after an internal list overflowed."""
         v = ctypes.c_longlong(0)

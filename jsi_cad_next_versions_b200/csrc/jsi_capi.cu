@@ -258,6 +258,18 @@ struct Lane {
   char *h_pin = nullptr;  // pinned staging of batch heads / records
   size_t h_pin_bytes = 0;
   long long batch_reruns = 0;  // batch items re-run alone after an overflow
+  // Lockstep batches replayed as CUDA graphs, keyed by everything their
+  // launch sequence depends on (see run_distance_batch).
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long nodes = 0;
+    unsigned long long last_use = 0;
+    int seen = 0;
+  };
+  std::map<std::vector<long long>, GraphEntry> graphs;
+  unsigned long long graph_clock = 0;
+  long long graph_replays = 0;
+  bool graphs_on = true;
 };
 
 // One query of a batch: its tasks, the caller's result slot and its status
@@ -306,6 +318,7 @@ struct jsi_context {
   cudaEvent_t ring_ev[kRingSegs] = {};
   cudaEvent_t upload_ev = nullptr;  // recorded after every upload (lanes wait on it)
   int batch_chunk = 64;  // queries per lockstep batch (0: one query per lane job)
+  bool batch_graphs = true;  // replay repeated lockstep batches as CUDA graphs
   std::string kernel_names;
   // worker pool
   std::vector<std::unique_ptr<Lane>> lanes;
@@ -699,6 +712,12 @@ void pull_stats(Lane *ctx) {
   JSI_CUDA(cudaStreamSynchronize(ctx->stream));
   JSI_CUDA(cudaGetLastError());
   if (ctx->timing) resolve_timing(ctx);
+}
+
+unsigned bit_cast_u32(float x) {
+  unsigned u;
+  std::memcpy(&u, &x, sizeof(u));
+  return u;
 }
 
 int bit_width(unsigned long long x) {
@@ -1331,67 +1350,132 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
     std::memcpy(pin + q * hsz, &h, hsz);
     if (kScreen) e = std::max(e, screen_error(sa, sb));
   }
-  JSI_CUDA(cudaMemcpy2DAsync(lay.head, slab, pin, hsz, hsz, n, cudaMemcpyHostToDevice, st));
-  L->h2d_bytes += hsz * n;
-
+  // The bound enters the kernels as an argument: rounded up to a power of
+  // two (still a valid bound, a negligible widening) so that batches of
+  // similar surfaces share one captured graph.
+  if (kScreen && e > 0.0f) {
+    int ex = 0;
+    std::frexp(e, &ex);
+    e = std::ldexp(1.0f, ex);
+  }
   ScreenStats *stats = &lay.head->stats;
   const SurfView<TP> va = view<TP>(s0a), vb = view<TP>(s0b);
   const int R = p.rounds;
-  for (int r = 1; r <= R; ++r) {
-    const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
-    const bool scr = kScreen && r == 1;
-    timed(L, "basis", [&] {
-      launch_basis(va, Rd.A, st, bt, head_view<TP>(lay.head, 0));
-      launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1));
-    });
-    // Work units of the cell build: cells of both sides (exact in round 1,
-    // where every query has one region per side; the refinement rounds'
-    // region counts live on the device).
-    const double cells_units = r == 1 ? double(n) * (double(Rd.A.g.W) * Rd.A.g.W + double(Rd.B.g.W) * Rd.B.g.W) : 0.0;
-    const char *cells_name = r == 1 ? "cells_r1" : "cells";
-    if (!scr) {
-      timed(L, cells_name, [&] {
-        launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0));
-        launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1));
-      }, cells_units);
-      batch_screen<TP>(L, Rd, Rd.A, Rd.B, stats, p.k, false, 0.0f, bt);
-      timed(L, "dist_select", [&] {
-        launch_dist_select(static_cast<const DistCand<TP> *>(Rd.cand), Rd.cand_cap, p.k, Rd.top, stats, st, bt);
+  auto enqueue = [&]() {
+    JSI_CUDA(cudaMemcpy2DAsync(lay.head, slab, pin, hsz, hsz, n, cudaMemcpyHostToDevice, st));
+    L->h2d_bytes += hsz * n;
+
+    for (int r = 1; r <= R; ++r) {
+      const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
+      const bool scr = kScreen && r == 1;
+      timed(L, "basis", [&] {
+        launch_basis(va, Rd.A, st, bt, head_view<TP>(lay.head, 0));
+        launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1));
       });
-    } else if constexpr (kScreen) {
-      timed(L, cells_name, [&] {
-        launch_cells_fused(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
-        launch_cells_fused(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
-      }, cells_units);
-      batch_screen<TC>(L, Rd, Rd.A32, Rd.B32, stats, p.k, true, e, bt);
-      timed(L, "dist_verify", [&] {
-        launch_dist_verify(view<double>(s0a), view<double>(s0b), Rd.A, Rd.B, Rd.map1, Rd.map2,
-                           static_cast<const DistCand<float> *>(Rd.cand), 0, Rd.checked,
-                           st, bt, &lay.head->a64, &lay.head->b64, stats, Rd.cand_cap);
+      // Work units of the cell build: cells of both sides (exact in round 1,
+      // where every query has one region per side; the refinement rounds'
+      // region counts live on the device).
+      const double cells_units = r == 1 ? double(n) * (double(Rd.A.g.W) * Rd.A.g.W + double(Rd.B.g.W) * Rd.B.g.W) : 0.0;
+      const char *cells_name = r == 1 ? "cells_r1" : "cells";
+      if (!scr) {
+        timed(L, cells_name, [&] {
+          launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0));
+          launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1));
+        }, cells_units);
+        batch_screen<TP>(L, Rd, Rd.A, Rd.B, stats, p.k, false, 0.0f, bt);
+        timed(L, "dist_select", [&] {
+          launch_dist_select(static_cast<const DistCand<TP> *>(Rd.cand), Rd.cand_cap, p.k, Rd.top, stats, st, bt);
+        });
+      } else if constexpr (kScreen) {
+        timed(L, cells_name, [&] {
+          launch_cells_fused(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
+          launch_cells_fused(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
+        }, cells_units);
+        batch_screen<TC>(L, Rd, Rd.A32, Rd.B32, stats, p.k, true, e, bt);
+        timed(L, "dist_verify", [&] {
+          launch_dist_verify(view<double>(s0a), view<double>(s0b), Rd.A, Rd.B, Rd.map1, Rd.map2,
+                             static_cast<const DistCand<float> *>(Rd.cand), 0, Rd.checked,
+                             st, bt, &lay.head->a64, &lay.head->b64, stats, Rd.cand_cap);
+        });
+        timed(L, "dist_select", [&] { launch_dist_select(Rd.checked, Rd.cand_cap, p.k, Rd.top, stats, st, bt); });
+      }
+      if (r < R) {
+        timed(L, "dist_next", [&] {
+          launch_dist_next(Rd.top, stats, Rd.A, Rd.B, Rd.map1, Rd.map2, p.nuv_refine, Rd.next1, Rd.next2, Rd.nmap1,
+                           Rd.nmap2, st, bt);
+        });
+      }
+      timed(L, "dist_close", [&] {
+        launch_dist_close(stats, Rd.top, lay.rec, r - 1, Rd.surv_cap, Rd.cand_cap, r == R, st, bt);
       });
-      timed(L, "dist_select", [&] { launch_dist_select(Rd.checked, Rd.cand_cap, p.k, Rd.top, stats, st, bt); });
     }
-    if (r < R) {
-      timed(L, "dist_next", [&] {
-        launch_dist_next(Rd.top, stats, Rd.A, Rd.B, Rd.map1, Rd.map2, p.nuv_refine, Rd.next1, Rd.next2, Rd.nmap1,
-                         Rd.nmap2, st, bt);
+    if (p.newton) {
+      const BatchRound<TP, TC> &Rd = lay.rounds[R - 1];
+      timed(L, "newton", [&] {
+        launch_newton_dist(view<double>(s0a), view<double>(s0b), Rd.A.regions, Rd.B.regions, Rd.map1, Rd.map2,
+                           Rd.A.g.nuv, Rd.B.g.nuv, Rd.top, p.k, lay.head->dom, lay.rec->newton, st, bt,
+                           &lay.head->a64, &lay.head->b64, stats);
       });
     }
-    timed(L, "dist_close", [&] {
-      launch_dist_close(stats, Rd.top, lay.rec, r - 1, Rd.surv_cap, Rd.cand_cap, r == R, st, bt);
-    });
+    JSI_CUDA(cudaGetLastError());
+    JSI_CUDA(cudaMemcpy2DAsync(pin, rsz, lay.rec, slab, rsz, n, cudaMemcpyDeviceToHost, st));
+    L->d2h_bytes += rsz * n;
+  };
+
+  // CUDA graphs: a key's first batch runs eagerly, its second is captured
+  // and later ones replay it.  The key holds what the launch sequence
+  // depends on: form, shape and parameters, batch size, the slab and staging
+  // addresses (the arena rewinds to the same addresses while its blocks stay)
+  // and the rounded bound.  Per-kernel timing always runs eagerly.
+  const std::vector<long long> key = {
+      static_cast<long long>(sizeof(TP)), static_cast<long long>(sizeof(TC)), nuv1, nuv2, p1a, p1b, p.k, p.rounds,
+      p.nuv_refine, p.newton, n, static_cast<long long>(slab), reinterpret_cast<long long>(base),
+      reinterpret_cast<long long>(pin), static_cast<long long>(caps.surv), static_cast<long long>(caps.cand),
+      static_cast<long long>(bit_cast_u32(e))};
+  const bool graphs = !L->timing && L->graphs_on;
+  auto it = graphs ? L->graphs.find(key) : L->graphs.end();
+  if (it != L->graphs.end() && it->second.exec) {
+    JSI_CUDA(cudaGraphLaunch(it->second.exec, st));
+    add_launches(it->second.nodes);
+    L->h2d_bytes += hsz * n;
+    L->d2h_bytes += rsz * n;
+    it->second.last_use = ++L->graph_clock;
+    ++L->graph_replays;
+  } else if (it != L->graphs.end()) {
+    const unsigned long long before = launch_count();
+    cudaGraph_t graph = nullptr;
+    JSI_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue();
+    } catch (...) {
+      cudaStreamEndCapture(st, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    JSI_CUDA(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    JSI_CUDA(ie);
+    it->second.exec = exec;
+    it->second.nodes = launch_count() - before;
+    it->second.last_use = ++L->graph_clock;
+    JSI_CUDA(cudaGraphLaunch(exec, st));
+  } else {
+    enqueue();
+    if (graphs) {
+      if (L->graphs.size() >= 8) {  // keep the 8 most recently used
+        auto lru = L->graphs.begin();
+        for (auto g = L->graphs.begin(); g != L->graphs.end(); ++g)
+          if (g->second.last_use < lru->second.last_use) lru = g;
+        if (lru->second.exec) cudaGraphExecDestroy(lru->second.exec);
+        L->graphs.erase(lru);
+      }
+      auto &ent = L->graphs[key];
+      ent.seen = 1;
+      ent.last_use = ++L->graph_clock;
+    }
   }
-  if (p.newton) {
-    const BatchRound<TP, TC> &Rd = lay.rounds[R - 1];
-    timed(L, "newton", [&] {
-      launch_newton_dist(view<double>(s0a), view<double>(s0b), Rd.A.regions, Rd.B.regions, Rd.map1, Rd.map2,
-                         Rd.A.g.nuv, Rd.B.g.nuv, Rd.top, p.k, lay.head->dom, lay.rec->newton, st, bt,
-                         &lay.head->a64, &lay.head->b64, stats);
-    });
-  }
-  JSI_CUDA(cudaGetLastError());
-  JSI_CUDA(cudaMemcpy2DAsync(pin, rsz, lay.rec, slab, rsz, n, cudaMemcpyDeviceToHost, st));
-  L->d2h_bytes += rsz * n;
   JSI_CUDA(cudaStreamSynchronize(st));
   if (L->timing) resolve_timing(L);
 
@@ -1665,6 +1749,9 @@ void lane_free(Lane &L) {
   L.event_pool.clear();
   if (L.d_stats) cudaFree(L.d_stats);
   if (L.h_stats) cudaFreeHost(L.h_stats);
+  for (auto &g : L.graphs)
+    if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+  L.graphs.clear();
   if (L.h_pin) cudaFreeHost(L.h_pin);
   L.h_pin = nullptr;
   L.h_pin_bytes = 0;
@@ -1881,6 +1968,7 @@ void start_workers(jsi_context *ctx, int n) {
   for (int q = 0; q < n; ++q) {
     auto L = std::make_unique<Lane>();
     lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces, &ctx->lane_held, left);
+    L->graphs_on = ctx->batch_graphs;
     ctx->lanes.push_back(std::move(L));
   }
   for (auto &L : ctx->lanes) ctx->threads.emplace_back(worker_loop, ctx, L.get());
@@ -2263,6 +2351,20 @@ int jsi_queue_depth(jsi_context *ctx, int *queued, int *running) {
 int jsi_batch_chunk(jsi_context *ctx, int chunk) {
   if (!ctx || chunk < 0 || chunk > 65535) return JSI_ERR_INVALID;
   ctx->batch_chunk = chunk;
+  return JSI_OK;
+}
+
+int jsi_batch_graphs(jsi_context *ctx, int enable, long long *replays) {
+  if (!ctx) return JSI_ERR_INVALID;
+  if (enable >= 0) {
+    ctx->batch_graphs = enable != 0;
+    for (auto &L : ctx->lanes) L->graphs_on = ctx->batch_graphs;
+  }
+  if (replays) {
+    long long t = 0;
+    for (auto &L : ctx->lanes) t += L->graph_replays;
+    *replays = t;
+  }
   return JSI_OK;
 }
 

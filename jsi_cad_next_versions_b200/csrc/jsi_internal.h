@@ -163,6 +163,7 @@ __host__ __device__ inline unsigned long long pack_tile_pair(unsigned row, unsig
 // negative slot count -max) are read from each query's ScreenStats, with the
 // host value (or cap) only bounding the grid.
 unsigned long long launch_count();  // kernels launched so far (all contexts)
+void add_launches(unsigned long long n);  // kernels a replayed CUDA graph launched
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt = Batch{},
                   const SurfView<T> *vdev = nullptr);

@@ -2688,6 +2688,7 @@ inline void counted(int n = 1) { g_launches.fetch_add(static_cast<unsigned long 
 }  // namespace
 
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void add_launches(unsigned long long n) { counted(static_cast<int>(n)); }
 
 // ---------------------------------------------------------------------------
 // Launchers

@@ -198,3 +198,25 @@ def test_upload_many_release_reuse():
                 ta = c3.task(c3.upload(A), rect32(A), 96, 1)
                 tb = c3.task(c3.upload(B), rect32(B), 96, 2)
                 assert c3.min_distance(ta, tb, precision="fp64").distance == r.distance
+
+
+@pytest.mark.parametrize("precision", ["fp32_screen", "fp64"])
+def test_batch_graph_replay(precision):
+    """A repeated batch is captured as a CUDA graph on its second run and
+    replayed from the third on: the replays give the eager results."""
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _hard_wave_pairs(6, seed0=1300), 128)
+        ctx.workers(1)
+        try:
+            ctx.batch_graphs(False)
+            eager, _ = ctx.min_distance_batch(tasks, precision=precision, trace=True, newton=True)
+            ctx.batch_graphs(True)
+            runs = [ctx.min_distance_batch(tasks, precision=precision, trace=True, newton=True)[0] for _ in range(4)]
+            replays = ctx.batch_graphs()
+        finally:
+            ctx.workers(0)
+        assert replays >= 2
+        for res in runs:
+            for r, a in zip(res, eager):
+                _same(r, a, newton=True)
