@@ -190,6 +190,49 @@ void jsi_inter_params_default(jsi_inter_params *p);
 int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_inter_params *params,
                   jsi_inter_result *out);
 
+/* --- certified distance interval (bounds mode) ----------------------------
+ * No counterpart in the reference, whose distance is the k-th smallest
+ * distance between cell-box centres (distance_analysis.cu:202-207), not a
+ * bound.  Returns lb <= (true minimum distance between the two rectangles of
+ * the two surfaces) <= ub, rigorously, for non-rational surfaces, by branch
+ * and bound on cell boxes of a grid covering both rectangles:
+ *  - each box is its corner samples' box padded by the bilinear-interpolation
+ *    error bound (du^2 max|S_uu| + dv^2 max|S_vv|) / 8, from the
+ *    second-derivative control nets, and by an evaluation allowance; gaps are
+ *    rounded down;
+ *  - ub starts at the FP64 distance query's Newton pair and drops to the
+ *    closest corner-sample pair of the kept cells each round (surface points,
+ *    distances rounded up, plus the evaluation allowance);
+ *  - pairs whose gap can be below (1 - rel_tol) ub are refined at nuv_refine
+ *    per cell; lb is the smaller of the smallest kept gap and
+ *    (1 - rel_tol) ub, which every dropped pair's gap exceeds.
+ * Rounds stop when ub - lb <= rel_tol * ub or no pair is kept (certified = 1),
+ * after max_rounds, or when a round keeps more than max_pairs pairs.  uv1 /
+ * uv2 / point1 / point2 are the Newton pair (its distance >= ub).
+ * Rational surfaces: JSI_ERR_UNSUPPORTED. */
+typedef struct {
+  int nuv_refine;      /* samples per direction in a refined cell (default 8) */
+  int max_rounds;      /* 1..JSI_MAX_ROUNDS (default 10) */
+  double rel_tol;      /* default 1e-6 */
+  long long max_pairs; /* default 1 << 22 */
+} jsi_bounds_params;
+
+typedef struct {
+  double lb, ub;
+  int certified;
+  int rounds_run;
+  long long kept[JSI_MAX_ROUNDS];       /* cell pairs kept per round */
+  long long pair_tests[JSI_MAX_ROUNDS]; /* cell-pair box tests per round */
+  double lb_round[JSI_MAX_ROUNDS];      /* lower bound after each round */
+  double uv1[2], uv2[2];                /* parameters of the Newton pair */
+  double point1[3], point2[3];
+  float device_ms;
+} jsi_bounds_result;
+
+void jsi_bounds_params_default(jsi_bounds_params *p);
+int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_bounds_params *params,
+                        jsi_bounds_result *out);
+
 /* --- queued and batched queries (the serving engine) ----------------------
  * No counterpart in the reference, whose API runs one query at a time and is
  * not re-entrant (file statics, intersection.cu:36-39).  jsi_workers starts n

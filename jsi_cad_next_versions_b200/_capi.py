@@ -30,7 +30,8 @@ EXPORTED = [
     "jsi_surface_upload", "jsi_surface_upload_many", "jsi_surface_release", "jsi_resident_bytes", "jsi_context_stream",
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_units", "jsi_kernel_names",
     "jsi_dist_params_default",
-    "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_eval_grid", "jsi_eval_grid_f64",
+    "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_bounds_params_default",
+    "jsi_distance_bounds", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
     "jsi_queue_depth", "jsi_min_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs",
 ]
@@ -74,6 +75,19 @@ class InterResult(ctypes.Structure):
                 ("trace_written", ctypes.c_longlong), ("points", ctypes.POINTER(ctypes.c_double)),
                 ("points_cap", ctypes.c_longlong), ("points_written", ctypes.c_longlong),
                 ("points_converged", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+
+
+class BoundsParams(ctypes.Structure):
+    _fields_ = [("nuv_refine", ctypes.c_int), ("max_rounds", ctypes.c_int), ("rel_tol", ctypes.c_double),
+                ("max_pairs", ctypes.c_longlong)]
+
+
+class BoundsResult(ctypes.Structure):
+    _fields_ = [("lb", ctypes.c_double), ("ub", ctypes.c_double), ("certified", ctypes.c_int),
+                ("rounds_run", ctypes.c_int), ("kept", ctypes.c_longlong * MAX_ROUNDS),
+                ("pair_tests", ctypes.c_longlong * MAX_ROUNDS), ("lb_round", ctypes.c_double * MAX_ROUNDS),
+                ("uv1", ctypes.c_double * 2), ("uv2", ctypes.c_double * 2), ("point1", ctypes.c_double * 3),
+                ("point2", ctypes.c_double * 3), ("device_ms", ctypes.c_float)]
 
 
 _lib = None
@@ -155,6 +169,11 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_surface_upload_many.argtypes = [P, I, ctypes.POINTER(I), ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
                                           ctypes.POINTER(I), ctypes.POINTER(I)]
     L.jsi_surface_upload_many.restype = I
+    L.jsi_bounds_params_default.argtypes = [ctypes.POINTER(BoundsParams)]
+    L.jsi_bounds_params_default.restype = None
+    L.jsi_distance_bounds.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(BoundsParams),
+                                      ctypes.POINTER(BoundsResult)]
+    L.jsi_distance_bounds.restype = I
     L.jsi_batch_chunk.argtypes = [P, I]
     L.jsi_batch_chunk.restype = I
     L.jsi_batch_reruns.argtypes = [P, ctypes.POINTER(LL)]

@@ -50,6 +50,23 @@ class DistanceResult:
 
 
 @dataclass
+class DistanceBounds:
+    """Certified interval lb <= min distance <= ub (bounds mode)."""
+    lb: float
+    ub: float
+    certified: bool
+    rounds: int
+    kept: np.ndarray
+    pair_tests: np.ndarray
+    lb_round: np.ndarray
+    uv1: tuple
+    uv2: tuple
+    point1: tuple
+    point2: tuple
+    device_ms: float
+
+
+@dataclass
 class IntersectionResult:
     rounds: int
     counts: np.ndarray
@@ -293,6 +310,20 @@ class Context:
         self._check(self.lib.jsi_min_distance_batch(self.handle, n, ta, tb, ctypes.byref(p), res, status,
                                                     ctypes.byref(ms)))
         return [self._dist_result(res[q], bufs[q], k) for q in range(n)], ms.value
+
+    def distance_bounds(self, a: C.Task, b: C.Task, *, nuv_refine: int = 8, max_rounds: int = 10,
+                        rel_tol: float = 1e-6, max_pairs: int = 1 << 22) -> DistanceBounds:
+        """Rigorous interval for the minimum distance between two non-rational
+        surface rectangles (the FP64 Newton pair as ub, branch and bound on
+        padded cell boxes of a covering grid for lb)."""
+        p = C.BoundsParams(nuv_refine, max_rounds, rel_tol, max_pairs)
+        r = C.BoundsResult()
+        self._check(self.lib.jsi_distance_bounds(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
+                                                 ctypes.byref(r)))
+        n = r.rounds_run
+        return DistanceBounds(r.lb, r.ub, bool(r.certified), n, np.array(r.kept[:n], np.int64),
+                              np.array(r.pair_tests[:n], np.int64), np.array(r.lb_round[:n], np.float64),
+                              tuple(r.uv1), tuple(r.uv2), tuple(r.point1), tuple(r.point2), r.device_ms)
 
     def intersect(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                   halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",

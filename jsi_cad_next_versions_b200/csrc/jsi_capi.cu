@@ -703,6 +703,8 @@ void timed(Lane *ctx, const char *name, Fn &&fn, double units = 0) {
 void reset_stats(Lane *ctx) {
   ScreenStats z{};
   z.tau_bits = 0x7f800000u;
+  z.lb_bits = 0x7ff0000000000000ull;
+  z.ub_bits = 0x7ff0000000000000ull;
   *ctx->h_stats = z;
   JSI_CUDA(copy_async(ctx, ctx->d_stats, ctx->h_stats, sizeof(ScreenStats), cudaMemcpyHostToDevice, ctx->stream));
 }
@@ -1539,6 +1541,59 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
 // ---------------------------------------------------------------------------
 // intersection
 // ---------------------------------------------------------------------------
+// Next round's regions from the round's kept pairs, sorted by (slot, i, j):
+// pair-preserving jobs with (slot, cell) dedup per side on the device
+// (intersection.cu:380-447); cover selects the bounds mode's child grid.
+template <typename T>
+void next_regions(Lane *ctx, const unsigned long long *sorted, long long n, int ij_bits, int slot_bits,
+                  const SideRound<T> &A, const SideRound<T> &B, const int *map1, const int *map2, bool cover,
+                  RegionRec<T> **next1_out, RegionRec<T> **next2_out, int **nmap1_out, int **nmap2_out, int *r1_out,
+                  int *r2_out) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  unsigned long long *key2 = ar.get<unsigned long long>(n), *key2s = ar.get<unsigned long long>(n);
+  int *idx = ar.get<int>(n), *idxs = ar.get<int>(n);
+  unsigned *flag1 = ar.get<unsigned>(n), *ex1 = ar.get<unsigned>(n), *flag2 = ar.get<unsigned>(n),
+           *ex2 = ar.get<unsigned>(n);
+  timed(ctx, "inter_prep", [&] { launch_inter_prep(sorted, n, ij_bits, key2, idx, flag1, st); });
+  size_t tb1 = 0, tb2 = 0, tb3 = 0;
+  JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb1, flag1, ex1, static_cast<int>(n), st));
+  JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key2, key2s, idx, idxs, static_cast<int>(n), 0,
+                                           ij_bits + slot_bits, st));
+  JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, flag2, ex2, static_cast<int>(n), st));
+  const size_t tmax = std::max(tb1, std::max(tb2, tb3));
+  void *tmp = ar.alloc(tmax);
+  size_t tbs = tmax;
+  JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag1, ex1, static_cast<int>(n), st));
+  tbs = tmax;
+  JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tbs, key2, key2s, idx, idxs, static_cast<int>(n), 0,
+                                           ij_bits + slot_bits, st));
+  timed(ctx, "flag_runs", [&] { launch_flag_runs(key2s, n, flag2, st); });
+  tbs = tmax;
+  JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag2, ex2, static_cast<int>(n), st));
+  RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
+  int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
+  timed(ctx, "inter_side1", [&] {
+    launch_inter_side1(sorted, n, ij_bits, flag1, ex1, A, map1, next1, nmap1, st, cover);
+  });
+  timed(ctx, "inter_side2", [&] {
+    launch_inter_side2(key2s, idxs, n, ij_bits, flag2, ex2, B, map2, next2, nmap2, st, cover);
+  });
+  unsigned tail[4];
+  JSI_CUDA(copy_async(ctx, &tail[0], ex1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  JSI_CUDA(copy_async(ctx, &tail[1], flag1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  JSI_CUDA(copy_async(ctx, &tail[2], ex2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  JSI_CUDA(copy_async(ctx, &tail[3], flag2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  JSI_CUDA(cudaStreamSynchronize(st));
+  JSI_CUDA(cudaGetLastError());
+  *r1_out = static_cast<int>(tail[0] + tail[1]);
+  *r2_out = static_cast<int>(tail[2] + tail[3]);
+  *next1_out = next1;
+  *next2_out = next2;
+  *nmap1_out = nmap1;
+  *nmap2_out = nmap2;
+}
+
 template <typename T>
 void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
                       jsi_inter_result *out) {
@@ -1678,37 +1733,10 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
     if (n > p->halve_threshold && nuv > p->min_nuv) nuv /= 2;  // intersection.cu:370
     if (n > (1ll << 31) - 1) fail(JSI_ERR_CAPACITY, "too many pairs for the next round");
     // Pair-preserving jobs and (slot, cell) dedup per side on the device.
-    unsigned long long *key2 = ar.get<unsigned long long>(n), *key2s = ar.get<unsigned long long>(n);
-    int *idx = ar.get<int>(n), *idxs = ar.get<int>(n);
-    unsigned *flag1 = ar.get<unsigned>(n), *ex1 = ar.get<unsigned>(n), *flag2 = ar.get<unsigned>(n),
-             *ex2 = ar.get<unsigned>(n);
-    timed(ctx, "inter_prep", [&] { launch_inter_prep(sorted, n, ij_bits, key2, idx, flag1, st); });
-    size_t tb1 = 0, tb2 = 0, tb3 = 0;
-    JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb1, flag1, ex1, static_cast<int>(n), st));
-    JSI_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key2, key2s, idx, idxs, static_cast<int>(n), 0,
-                                             ij_bits + slot_bits, st));
-    JSI_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, flag2, ex2, static_cast<int>(n), st));
-    void *tmp = ar.alloc(std::max(tb1, std::max(tb2, tb3)));
-    size_t tbs = std::max(tb1, std::max(tb2, tb3));
-    JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag1, ex1, static_cast<int>(n), st));
-    tbs = std::max(tb1, std::max(tb2, tb3));
-    JSI_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tbs, key2, key2s, idx, idxs, static_cast<int>(n), 0,
-                                             ij_bits + slot_bits, st));
-    timed(ctx, "flag_runs", [&] { launch_flag_runs(key2s, n, flag2, st); });
-    tbs = std::max(tb1, std::max(tb2, tb3));
-    JSI_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tbs, flag2, ex2, static_cast<int>(n), st));
-    RegionRec<T> *next1 = ar.get<RegionRec<T>>(n), *next2 = ar.get<RegionRec<T>>(n);
-    int *nmap1 = ar.get<int>(n), *nmap2 = ar.get<int>(n);
-    timed(ctx, "inter_side1", [&] { launch_inter_side1(sorted, n, ij_bits, flag1, ex1, A, map1, next1, nmap1, st); });
-    timed(ctx, "inter_side2", [&] { launch_inter_side2(key2s, idxs, n, ij_bits, flag2, ex2, B, map2, next2, nmap2, st); });
-    unsigned tail[4];
-    JSI_CUDA(copy_async(ctx, &tail[0], ex1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(copy_async(ctx, &tail[1], flag1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(copy_async(ctx, &tail[2], ex2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(copy_async(ctx, &tail[3], flag2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    JSI_CUDA(cudaStreamSynchronize(st));
-    JSI_CUDA(cudaGetLastError());
-    const int r1 = static_cast<int>(tail[0] + tail[1]), r2 = static_cast<int>(tail[2] + tail[3]);
+    RegionRec<T> *next1, *next2;
+    int *nmap1, *nmap2, r1, r2;
+    next_regions<T>(ctx, sorted, n, ij_bits, slot_bits, A, B, map1, map2, false, &next1, &next2, &nmap1, &nmap2, &r1,
+                    &r2);
     A = make_side<T>(ar, make_geom(nuv, p1_of(sa)), r1, true, next1);
     B = make_side<T>(ar, make_geom(nuv, p1_of(sb)), r2, true, next2);
     map1 = nmap1;
@@ -1717,6 +1745,223 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
   }
   out->trace_written = written;
 }
+
+// ---------------------------------------------------------------------------
+// Certified distance interval (bounds mode)
+// ---------------------------------------------------------------------------
+
+// Per coordinate c, max |S_uu[c]| and max |S_vv[c]| over a non-rational surface: the
+// second-derivative control nets (derivative control points, applied twice
+// per direction: Q_i = p (P_{i+1} - P_i) / (U_{i+p+1} - U_{i+1}),
+// R_i = (p - 1)(Q_{i+1} - Q_i) / (U_{i+p+1} - U_{i+2}); a zero knot span
+// gives a zero term) bound the second derivatives by the convex hull
+// property.  Widened by 1e-12 for the double arithmetic.
+void second_derivative_bounds(Lane *L, const SurfaceRec &s, double m2u[3], double m2v[3]) {
+  const int p = s.ivec[1], nu = s.ivec[2], nku = s.ivec[3], q = s.ivec[4], nv = s.ivec[5], nkv = s.ivec[6];
+  const size_t ncp = static_cast<size_t>(nu) * nv;
+  std::vector<float> raw(nku + nkv + 3 * ncp);
+  JSI_CUDA(copy_async(L, raw.data(), s.U32, raw.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+  JSI_CUDA(cudaStreamSynchronize(L->stream));
+  const float *U = raw.data(), *V = U + nku, *P = V + nkv;  // P[(j * nu + i) * 3 + c], u fastest
+  auto line_bound = [](const std::vector<double> &pts, const float *K, int deg, int n, double m[3]) {
+    // pts: n points x 3 along one parameter direction
+    if (deg < 2 || n < 3) return;
+    std::vector<double> Q(3 * (n - 1));
+    for (int i = 0; i < n - 1; ++i) {
+      const double den = static_cast<double>(K[i + deg + 1]) - K[i + 1];
+      for (int c = 0; c < 3; ++c) Q[3 * i + c] = den != 0.0 ? deg * (pts[3 * (i + 1) + c] - pts[3 * i + c]) / den : 0.0;
+    }
+    for (int i = 0; i < n - 2; ++i) {
+      const double den = static_cast<double>(K[i + deg + 1]) - K[i + 2];
+      if (den == 0.0) continue;
+      for (int c = 0; c < 3; ++c) m[c] = std::max(m[c], std::fabs((deg - 1) * (Q[3 * (i + 1) + c] - Q[3 * i + c]) / den));
+    }
+  };
+  double mu[3] = {0.0, 0.0, 0.0}, mv[3] = {0.0, 0.0, 0.0};
+  std::vector<double> line;
+  for (int j = 0; j < nv; ++j) {
+    line.assign(3 * nu, 0.0);
+    for (int i = 0; i < nu; ++i)
+      for (int c = 0; c < 3; ++c) line[3 * i + c] = P[(static_cast<size_t>(j) * nu + i) * 3 + c];
+    line_bound(line, U, p, nu, mu);
+  }
+  for (int i = 0; i < nu; ++i) {
+    line.assign(3 * nv, 0.0);
+    for (int j = 0; j < nv; ++j)
+      for (int c = 0; c < 3; ++c) line[3 * j + c] = P[(static_cast<size_t>(j) * nu + i) * 3 + c];
+    line_bound(line, V, q, nv, mv);
+  }
+  for (int c = 0; c < 3; ++c) {
+    m2u[c] = mu[c] * (1.0 + 1e-12);
+    m2v[c] = mv[c] * (1.0 + 1e-12);
+  }
+}
+
+// Allowance for the FP64 evaluation of a surface point and for the centre /
+// half-span rounding of a cell box: the evaluation's rounding stays below
+// 2^-45 of the largest control-point coordinate (a few dozen roundings of
+// terms bounded by it, the basis being a partition of unity); 2^-40 of it is
+// a 32x margin.
+double eval_allowance(const SurfaceRec &s) {
+  return std::ldexp(std::max(s.cmax[0], std::max(s.cmax[1], s.cmax[2])), -40);
+}
+
+void run_bounds(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_bounds_params *p,
+                jsi_bounds_result *out) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  const SurfaceRec &sa = get_surface(ctx, ta->surface);
+  const SurfaceRec &sb = get_surface(ctx, tb->surface);
+  if (sa.rat || sb.rat) fail(JSI_ERR_UNSUPPORTED, "the bounds mode needs non-rational surfaces");
+  if (sa.zero || sb.zero) fail(JSI_ERR_UNSUPPORTED, "the bounds mode needs surfaces that evaluate");
+  // Upper bound: two surface points from the FP64 query with Newton.
+  jsi_dist_params dp;
+  jsi_dist_params_default(&dp);
+  dp.precision = JSI_PREC_FP64;
+  dp.newton = 1;
+  jsi_dist_result dr;
+  std::memset(&dr, 0, sizeof(dr));
+  run_distance<double, double>(ctx, ta, tb, &dp, &dr);
+  const double ea = eval_allowance(sa), eb = eval_allowance(sb);
+  double ub = dr.newton_distance * (1.0 + 0x1p-50) + std::sqrt(3.0) * 1.000001 * (ea + eb);
+  ub = std::nextafter(ub, INFINITY);
+  out->ub = ub;
+  for (int c = 0; c < 2; ++c) {
+    out->uv1[c] = dr.uv1[c];
+    out->uv2[c] = dr.uv2[c];
+  }
+  for (int c = 0; c < 3; ++c) {
+    out->point1[c] = dr.point1[c];
+    out->point2[c] = dr.point2[c];
+  }
+  // Pairs are kept while their gap can be below the prune level
+  // (1 - rel_tol) ub: a dropped pair's gap exceeds it, so
+  // lb = min(smallest kept gap, prune level) stays a lower bound, and the
+  // kept set empties once the boxes are tighter than the tolerance.  ub (and
+  // with it the prune level) drops each round to the closest corner-sample
+  // pair seen.
+  const double allowance = std::sqrt(3.0) * 1.000001 * (ea + eb);
+  double m2[2][2][3];
+  second_derivative_bounds(ctx, sa, m2[0][0], m2[0][1]);
+  second_derivative_bounds(ctx, sb, m2[1][0], m2[1][1]);
+  const SurfView<double> va = view<double>(sa), vb = view<double>(sb);
+
+  RegionRec<double> roots[2] = {{ta->ustart, ta->vstart, ta->ustop, ta->vstop},
+                                {tb->ustart, tb->vstart, tb->ustop, tb->vstop}};
+  RegionRec<double> *dreg = ar.get<RegionRec<double>>(2);
+  int *dmap = ar.get<int>(2);
+  const int zeros[2] = {0, 0};
+  JSI_CUDA(copy_async(ctx, dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  // Per-coordinate pads: a Vec4 per region in place of the scalar.
+  auto bounds_side = [&](const Geom &g, int nreg, RegionRec<double> *regions) {
+    SideRound<double> S = make_side<double>(ar, g, nreg, true, regions);
+    S.pad = ar.get<double>(static_cast<size_t>(nreg) * 4);
+    return S;
+  };
+  SideRound<double> A = bounds_side(make_geom(ta->nuv, p1_of(sa)), 1, dreg);
+  SideRound<double> B = bounds_side(make_geom(tb->nuv, p1_of(sb)), 1, dreg + 1);
+  const int *map1 = dmap, *map2 = dmap + 1;
+  long long nslots = 1;
+  double lb = 0.0;
+  for (int round = 1; round <= p->max_rounds; ++round) {
+    for (int side = 0; side < 2; ++side) {
+      SideRound<double> &S = side ? B : A;
+      const SurfView<double> &v = side ? vb : va;
+      timed(ctx, "basis", [&] { launch_basis(v, S, st, Batch{}, static_cast<const SurfView<double> *>(nullptr), true); }, 2.0 * S.nreg * S.g.nuv);
+      timed(ctx, "samples", [&] { launch_samples(v, S, false, st); }, double(S.nreg) * S.g.nuv * S.g.nuv);
+      timed(ctx, "pad", [&] { launch_pad_bound(S, m2[side][0], m2[side][1], side ? eb : ea, st); });
+      timed(ctx, "cells", [&] { launch_cells(S, true, st); }, double(S.nreg) * S.g.W * S.g.W);
+    }
+    const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
+    if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+    const int ij_bits = std::max(1, bit_width(static_cast<unsigned long long>(
+                                            std::max(A.g.W * A.g.W, B.g.W * B.g.W) - 1)));
+    const int slot_bits = std::max(1, bit_width(static_cast<unsigned long long>(nslots - 1)));
+    if (2 * ij_bits + slot_bits > 64) fail(JSI_ERR_CAPACITY, "pair key does not fit 64 bits");
+    unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+    const double prune = std::nextafter((1.0 - p->rel_tol) * ub, 0.0);
+    const double ub2 = std::nextafter(prune * prune, INFINITY);
+    reset_stats(ctx);
+    timed(ctx, "bound_cull", [&] {
+      launch_bound_cull(A, B, map1, map2, static_cast<int>(nslots), ub2, surv, tile_pairs, ctx->d_stats, st);
+    });
+    pull_stats(ctx);
+    const unsigned long long nsurv = ctx->h_stats->survivors;
+    unsigned long long key_cap =
+        std::max<unsigned long long>(1ull << 16, std::min<unsigned long long>(nsurv * 64, 1ull << 24));
+    unsigned long long *keys = ar.get<unsigned long long>(key_cap);
+    for (int attempt = 0;; ++attempt) {
+      timed(ctx, "bound_leaf", [&] {
+        launch_bound_leaf(A, B, map1, map2, surv, nsurv, ij_bits, ub2, keys, key_cap, ctx->d_stats, st);
+      });
+      pull_stats(ctx);
+      ScreenStats &hs = *ctx->h_stats;
+      if (hs.candidates <= key_cap) break;
+      if (attempt >= 1) fail(JSI_ERR_CAPACITY, "bounds pair list overflow");
+      key_cap = hs.candidates;
+      keys = ar.get<unsigned long long>(key_cap);
+      hs.candidates = 0;
+      hs.pair_tests = 0;
+      hs.work = 0;
+      hs.lb_bits = 0x7ff0000000000000ull;
+      hs.ub_bits = 0x7ff0000000000000ull;
+      JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+    }
+    const long long n = static_cast<long long>(ctx->h_stats->candidates);
+    double g2;
+    const unsigned long long gb = ctx->h_stats->lb_bits;
+    std::memcpy(&g2, &gb, sizeof(g2));
+    // Every point pair lies in some cell pair; a pair whose gap exceeds ub
+    // cannot hold the minimum, so the smallest kept gap bounds it from below.
+    // (The pair holding the ub points is always kept, so n >= 1.)
+    const double lr = n > 0 ? std::nextafter(std::sqrt(g2), 0.0) : prune;
+    lb = std::max(lb, std::min(lr, prune));
+    double c2;
+    const unsigned long long cb = ctx->h_stats->ub_bits;
+    std::memcpy(&c2, &cb, sizeof(c2));
+    if (n > 0 && c2 < INFINITY) {
+      const double uc = std::nextafter(std::nextafter(std::sqrt(c2), INFINITY) + allowance, INFINITY);
+      ub = std::min(ub, uc);
+    }
+    lb = std::min(lb, ub);
+    out->kept[round - 1] = n;
+    out->pair_tests[round - 1] = static_cast<long long>(ctx->h_stats->pair_tests);
+    out->lb_round[round - 1] = lb;
+    out->rounds_run = round;
+    add_units(ctx, "bound_leaf", static_cast<double>(ctx->h_stats->pair_tests));
+    if (n == 0 || ub - lb <= p->rel_tol * ub) {
+      out->certified = 1;
+      break;
+    }
+    if (round == p->max_rounds || n == 0 || n > p->max_pairs) break;
+    unsigned long long *sorted = keys;
+    if (n > 1) {
+      const int end_bit = 2 * ij_bits + slot_bits;
+      unsigned long long *alt = ar.get<unsigned long long>(n);
+      size_t tmp_bytes = 0;
+      cub::DoubleBuffer<unsigned long long> db(keys, alt);
+      JSI_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
+      void *tmp = ar.alloc(tmp_bytes);
+      timed(ctx, "sort_pairs", [&] {
+        JSI_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, static_cast<int>(n), 0, end_bit, st));
+      });
+      sorted = db.Current();
+    }
+    RegionRec<double> *next1, *next2;
+    int *nmap1, *nmap2, r1, r2;
+    next_regions<double>(ctx, sorted, n, ij_bits, slot_bits, A, B, map1, map2, true, &next1, &next2, &nmap1, &nmap2,
+                         &r1, &r2);
+    A = bounds_side(make_geom(p->nuv_refine, p1_of(sa)), r1, next1);
+    B = bounds_side(make_geom(p->nuv_refine, p1_of(sb)), r2, next2);
+    map1 = nmap1;
+    map2 = nmap2;
+    nslots = n;
+  }
+  out->lb = lb;
+  out->ub = ub;
+}
+
 
 void check_precision(int prec, bool screen_built) {
   if (prec != JSI_PREC_V5_FP32 && prec != JSI_PREC_FP64 && prec != JSI_PREC_FP32_SCREEN)
@@ -2244,6 +2489,42 @@ int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, con
     if (params) p = *params;
     validate_dist(p, a, b);
     exec_distance(&ctx->main, a, b, p, out);
+    return JSI_OK;
+  });
+}
+
+void jsi_bounds_params_default(jsi_bounds_params *p) {
+  if (!p) return;
+  p->nuv_refine = 8;
+  p->max_rounds = 10;
+  p->rel_tol = 1e-6;
+  p->max_pairs = 1ll << 22;
+}
+
+int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_bounds_params *params,
+                        jsi_bounds_result *out) {
+  if (!ctx || !a || !b || !out) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    jsi_bounds_params p;
+    jsi_bounds_params_default(&p);
+    if (params) p = *params;
+    if (p.nuv_refine < 2 || p.nuv_refine > 64) fail(JSI_ERR_INVALID, "nuv_refine = %d", p.nuv_refine);
+    if (p.max_rounds < 1 || p.max_rounds > JSI_MAX_ROUNDS) fail(JSI_ERR_INVALID, "max_rounds = %d", p.max_rounds);
+    if (!(p.rel_tol >= 0.0)) fail(JSI_ERR_INVALID, "rel_tol must be >= 0");
+    if (p.max_pairs < 1) fail(JSI_ERR_INVALID, "max_pairs = %lld", p.max_pairs);
+    check_task<double>(a);
+    check_task<double>(b);
+    std::memset(out, 0, sizeof(*out));
+    Lane *L = &ctx->main;
+    JSI_CUDA(cudaSetDevice(L->device));
+    L->arena.reset();
+    JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
+    run_bounds(L, a, b, &p, out);
+    JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
+    JSI_CUDA(cudaEventSynchronize(L->ev1));
+    JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
+    if (L->timing) resolve_timing(L);
     return JSI_OK;
   });
 }

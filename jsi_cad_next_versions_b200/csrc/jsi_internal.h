@@ -120,6 +120,8 @@ struct ScreenStats {
   unsigned long long nhead;         // tile pairs in the threshold pass's list (batched rounds)
   int nslots;                       // slots of this round (batched rounds)
   int pad2_;
+  unsigned long long lb_bits;       // bounds mode: smallest kept squared box gap (double bits)
+  unsigned long long ub_bits;       // bounds mode: smallest corner-sample squared distance (double bits)
 };
 
 // Lockstep batch of queries that share one shape: query q runs in
@@ -164,9 +166,11 @@ __host__ __device__ inline unsigned long long pack_tile_pair(unsigned row, unsig
 // host value (or cap) only bounding the grid.
 unsigned long long launch_count();  // kernels launched so far (all contexts)
 void add_launches(unsigned long long n);  // kernels a replayed CUDA graph launched
+// cover: sample the covering grid (nuv samples over the whole rectangle, the
+// last on its end) of the bounds mode instead of the reference's grid.
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt = Batch{},
-                  const SurfView<T> *vdev = nullptr);
+                  const SurfView<T> *vdev = nullptr, bool cover = false);
 template <typename T>
 void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st,
                     const Batch &bt = Batch{}, const SurfView<T> *vdev = nullptr);
@@ -276,11 +280,26 @@ void launch_flag_runs(const unsigned long long *sorted, long long n, unsigned *f
 template <typename T>
 void launch_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
                         const unsigned *ex1, const SideRound<T> &cur, const int *map1, RegionRec<T> *next,
-                        int *nmap1, cudaStream_t st);
+                        int *nmap1, cudaStream_t st, bool cover = false);
 template <typename T>
 void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
                         const unsigned *flag2, const unsigned *ex2, const SideRound<T> &cur, const int *map2,
-                        RegionRec<T> *next, int *nmap2, cudaStream_t st);
+                        RegionRec<T> *next, int *nmap2, cudaStream_t st, bool cover = false);
+
+// Bounds mode (certified distance interval), FP64 sides built on the
+// covering grid: rigorous cell padding per region and coordinate, then tile pairs / cell
+// pairs whose box gap (rounded down) can be <= ub, ub2 = ub^2 rounded up; the
+// leaf appends (slot, i, j) keys like the intersection leaf and folds the
+// smallest kept squared gap into stats->lb_bits.
+// sr.pad must hold 4 doubles per region (a Vec4 pad per region, x, y, z).
+void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
+                      cudaStream_t st);
+void launch_bound_cull(const SideRound<double> &a, const SideRound<double> &b, const int *map1, const int *map2,
+                       int nslots, double ub2, unsigned long long *surv, unsigned long long surv_cap,
+                       ScreenStats *stats, cudaStream_t st);
+void launch_bound_leaf(const SideRound<double> &a, const SideRound<double> &b, const int *map1, const int *map2,
+                       const unsigned long long *surv, unsigned long long nsurv, int ij_bits, double ub2,
+                       unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st);
 
 // FP64 Newton refinement.  dom = {u0, u1, v0, v1, s0, s1, t0, t1} (the query
 // rectangles).  Distance: 11 doubles per candidate (d, u, v, s, t, P1, P2);

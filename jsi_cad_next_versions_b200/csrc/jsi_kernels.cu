@@ -215,7 +215,7 @@ __device__ void basis_ders(int span, int p, T u, const T *knots, int nd, T *out,
 
 template <typename T, int MAXP>
 __global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<T> *regions, int nreg,
-                        const int *dnreg, int nuv, int p1max, int *spans, T *basis, long long qs) {
+                        const int *dnreg, int nuv, int p1max, int *spans, T *basis, long long qs, int cover) {
   const long long qo = qoff(qs);
   if (vdev) s = *qsh(vdev, qo);
   if (dnreg) nreg = *qsh(dnreg, qo);
@@ -232,9 +232,11 @@ __global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<
     const T lo = dir ? reg.v0 : reg.u0;
     const T hi = dir ? reg.v1 : reg.u1;
     // ustep = (ustop - ustart) / nuv; u = ustep * idx + ustart
-    // (distance_analysis.cu:92-93, evaluation.cu:366).
-    const T step = (hi - lo) / static_cast<T>(nuv);
-    const T x = step * static_cast<T>(q) + lo;
+    // (distance_analysis.cu:92-93, evaluation.cu:366).  The covering grid of
+    // the bounds mode spaces nuv samples over the whole rectangle instead and
+    // puts the last one on its end.
+    const T step = cover ? (hi - lo) / static_cast<T>(nuv - 1) : (hi - lo) / static_cast<T>(nuv);
+    const T x = (cover && q == nuv - 1) ? hi : step * static_cast<T>(q) + lo;
     const int p = dir ? s.degv : s.degu;
     const int nk = dir ? s.nkv : s.nku;
     const T *knots = dir ? s.V : s.U;
@@ -1452,6 +1454,22 @@ __device__ __forceinline__ RegionRec<T> child_rect(const RegionRec<T> &p, int nu
   return c;
 }
 
+// Child rectangle of a cell on the covering grid (bounds mode): exactly the
+// parameters its corner samples were taken at (k_basis, cover = 1).
+template <typename T>
+__device__ __forceinline__ RegionRec<T> child_rect_cover(const RegionRec<T> &p, int nuv_parent, int bbox) {
+  const T ustep = (p.u1 - p.u0) / static_cast<T>(nuv_parent - 1);
+  const T vstep = (p.v1 - p.v0) / static_cast<T>(nuv_parent - 1);
+  const int w = nuv_parent - 1;
+  const int x = bbox % w, y = bbox / w;
+  RegionRec<T> c;
+  c.u0 = ustep * static_cast<T>(x) + p.u0;
+  c.u1 = x + 1 == w ? p.u1 : ustep * static_cast<T>(x + 1) + p.u0;
+  c.v0 = vstep * static_cast<T>(y) + p.v0;
+  c.v1 = y + 1 == w ? p.v1 : vstep * static_cast<T>(y + 1) + p.v0;
+  return c;
+}
+
 // Pair-preserving refinement jobs with (slot, cell) dedup per side
 // (distance_analysis.cu:399-491): one block.
 template <typename T>
@@ -1787,6 +1805,253 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
   if (lane == 0) atomicAdd(&stats->pair_tests, tests);
 }
 
+// ---- bounds mode (certified distance interval) ------------------------------
+
+// Rigorous padding of a region's cells on the covering grid, per coordinate:
+// over a cell, coordinate c of the surface is within
+// (du^2 max|S_uu[c]| + dv^2 max|S_vv[c]|) / 8 of the bilinear interpolant of
+// the four corners (tensor-product linear interpolation), and that
+// interpolant lies in the corners' box.  du, dv are the region's sample
+// spacings, inflated for the rounding of the sample parameters; m2u / m2v
+// bound |S_uu| / |S_vv| per coordinate over the surface (the
+// second-derivative nets, convex hull); eps covers the evaluation and the
+// centre / half-span rounding.  pad4 holds a Vec4 per region.
+__global__ void k_pad_bound(SideRound<double> sr, Vec4<double> *pad4, Vec4<double> m2u, Vec4<double> m2v,
+                            double eps) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= sr.nreg) return;
+  const RegionRec<double> reg = sr.regions[r];
+  const double n1 = static_cast<double>(sr.g.nuv - 1);
+  const double slack = 1.0 + 0x1p-40;
+  const double du = __dadd_ru(__dmul_ru(__ddiv_ru(fabs(reg.u1 - reg.u0), n1), slack),
+                              0x1p-50 * (fabs(reg.u0) + fabs(reg.u1)));
+  const double dv = __dadd_ru(__dmul_ru(__ddiv_ru(fabs(reg.v1 - reg.v0), n1), slack),
+                              0x1p-50 * (fabs(reg.v0) + fabs(reg.v1)));
+  const double du2 = __dmul_ru(du, du), dv2 = __dmul_ru(dv, dv);
+  auto one = [&](double mu, double mv) {
+    const double e = __dadd_ru(__dmul_ru(du2, mu), __dmul_ru(dv2, mv));
+    return __dadd_ru(__dmul_ru(__dmul_ru(e, 0.125), slack), eps);
+  };
+  pad4[r] = Vec4<double>{one(m2u.x, m2v.x), one(m2u.y, m2v.y), one(m2u.z, m2v.z), 0.0};
+}
+
+// Lower bound of the gap between [c1 - r1, c1 + r1] and [c2 - r2, c2 + r2].
+__device__ __forceinline__ double axis_gap_rd(double c1, double r1, double c2, double r2) {
+  const double d = c1 >= c2 ? __dsub_rd(c1, c2) : __dsub_rd(c2, c1);
+  const double g = __dsub_rd(d, __dadd_ru(r1, r2));
+  return g > 0.0 ? g : 0.0;
+}
+
+__device__ __forceinline__ double gap2_rd(double gx, double gy, double gz) {
+  return __dadd_rd(__dadd_rd(__dmul_rd(gx, gx), __dmul_rd(gy, gy)), __dmul_rd(gz, gz));
+}
+
+// Lower bound of the distance between two cell patches from their corner
+// samples: each patch lies in the convex hull of its four corners widened by
+// its per-coordinate pads, and projecting onto a unit direction never
+// lengthens a distance, so with d the centre-to-centre direction
+//   gap >= (min_j d.q_j - max_i d.p_i - sum_c |d_c| (pad1_c + pad2_c)) / |d|.
+// Near the closest approach d is close to the common normal and the hulls are
+// thin along it, so this bound is second-order in the cell size where the
+// axis-aligned gap is first-order.  The dot products' rounding is covered by
+// subtracting 8 u |d| (max |p| + max |q|) (u = 2^-53) from the numerator.
+__device__ __forceinline__ double proj_gap_rd(const Vec4<double> P[4], const Vec4<double> Q[4], const Vec4<double> &c1,
+                                              const Vec4<double> &c2, const Vec4<double> &p1,
+                                              const Vec4<double> &p2) {
+  const double dx = c2.x - c1.x, dy = c2.y - c1.y, dz = c2.z - c1.z;
+  const double dn = sqrt(dx * dx + dy * dy + dz * dz);
+  if (!(dn > 0.0)) return 0.0;
+  double pmax = -pos_inf<double>(), qmin = pos_inf<double>(), mag = 0.0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    pmax = fmax(pmax, dx * P[i].x + dy * P[i].y + dz * P[i].z);
+    qmin = fmin(qmin, dx * Q[i].x + dy * Q[i].y + dz * Q[i].z);
+    mag = fmax(mag, fmax(fabs(P[i].x) + fabs(P[i].y) + fabs(P[i].z), fabs(Q[i].x) + fabs(Q[i].y) + fabs(Q[i].z)));
+  }
+  const double spread = __dadd_ru(__dadd_ru(__dmul_ru(fabs(dx), __dadd_ru(p1.x, p2.x)),
+                                            __dmul_ru(fabs(dy), __dadd_ru(p1.y, p2.y))),
+                                  __dmul_ru(fabs(dz), __dadd_ru(p1.z, p2.z)));
+  const double slop = __dmul_ru(__dmul_ru(0x1p-50, __dadd_ru(fabs(dx), __dadd_ru(fabs(dy), fabs(dz)))), 2.0 * mag);
+  const double num = __dsub_rd(__dsub_rd(__dsub_rd(qmin, pmax), spread), slop);
+  if (!(num > 0.0)) return 0.0;
+  return __ddiv_rd(num, __dmul_ru(dn, 1.0 + 0x1p-50));
+}
+
+// Squared distance of two points, rounded up.
+__device__ __forceinline__ double dist2_ru(const Vec4<double> &p, const Vec4<double> &q) {
+  const double dx = p.x >= q.x ? __dsub_ru(p.x, q.x) : __dsub_ru(q.x, p.x);
+  const double dy = p.y >= q.y ? __dsub_ru(p.y, q.y) : __dsub_ru(q.y, p.y);
+  const double dz = p.z >= q.z ? __dsub_ru(p.z, q.z) : __dsub_ru(q.z, p.z);
+  return __dadd_ru(__dadd_ru(__dmul_ru(dx, dx), __dmul_ru(dy, dy)), __dmul_ru(dz, dz));
+}
+
+// Tile pairs whose box gap (centre ranges widened by the largest padded half
+// spans) can be <= ub.
+__global__ void k_bound_cull(SideRound<double> a, SideRound<double> b, const int *map1, const int *map2, int nslots,
+                             double ub2, unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats) {
+  const Geom g1 = a.g, g2 = b.g;
+  const long long total = static_cast<long long>(nslots) * g1.ntiles * g2.ntiles;
+  for (long long base = blockIdx.x * static_cast<long long>(blockDim.x); base < total;
+       base += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long e = base + threadIdx.x;
+    bool keep = false;
+    int row = 0, t2 = 0;
+    if (e < total) {
+      row = static_cast<int>(e / g2.ntiles);
+      t2 = static_cast<int>(e - static_cast<long long>(row) * g2.ntiles);
+      const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+      const int r1 = map1[slot], r2 = map2[slot];
+      const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
+      const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
+      const Vec4<double> lo1 = a.tlo[i1], hi1 = a.thi[i1], h1 = a.thmax[i1];
+      const Vec4<double> lo2 = b.tlo[i2], hi2 = b.thi[i2], h2 = b.thmax[i2];
+      const Vec4<double> p1 = reinterpret_cast<const Vec4<double> *>(a.pad)[r1];
+      const Vec4<double> p2 = reinterpret_cast<const Vec4<double> *>(b.pad)[r2];
+      double gg[3];
+      const double L1[3] = {lo1.x, lo1.y, lo1.z}, H1[3] = {hi1.x, hi1.y, hi1.z}, R1[3] = {h1.x, h1.y, h1.z};
+      const double L2[3] = {lo2.x, lo2.y, lo2.z}, H2[3] = {hi2.x, hi2.y, hi2.z}, R2[3] = {h2.x, h2.y, h2.z};
+      const double P1[3] = {p1.x, p1.y, p1.z}, P2[3] = {p2.x, p2.y, p2.z};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double gap = fmax(fmax(__dsub_rd(L2[c], H1[c]), __dsub_rd(L1[c], H2[c])), 0.0);
+        const double reach = __dadd_ru(__dadd_ru(R1[c], P1[c]), __dadd_ru(R2[c], P2[c]));
+        const double g = __dsub_rd(gap, reach);
+        gg[c] = g > 0.0 ? g : 0.0;
+      }
+      keep = gap2_rd(gg[0], gg[1], gg[2]) <= ub2;
+    }
+    const long long pos = warp_append(keep, &stats->survivors);
+    if (pos >= 0 && static_cast<unsigned long long>(pos) < surv_cap)
+      surv[pos] = pack_tile_pair(static_cast<unsigned>(row), static_cast<unsigned>(t2));
+  }
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&stats->tile_pairs, static_cast<unsigned long long>(total));
+}
+
+// Cell pairs of the surviving tile pairs whose padded boxes can be within ub,
+// one warp per tile pair (the layout of k_inter_leaf); each warp folds the
+// smallest kept squared gap of its tile pair into lb_bits, and the smallest
+// squared distance (rounded up) between the kept pairs' first corner
+// samples, which are surface points, into ub_bits.
+__global__ void __launch_bounds__(256) k_bound_leaf(SideRound<double> a, SideRound<double> b, const int *map1,
+                                                    const int *map2, const unsigned long long *surv,
+                                                    unsigned long long nsurv, int ij_bits, double ub2,
+                                                    unsigned long long *keys, unsigned long long key_cap,
+                                                    ScreenStats *stats) {
+  const Geom g1 = a.g, g2 = b.g;
+  const int te1 = g1.te, te2 = g2.te;
+  const int n1 = te1 * te1, n2 = te2 * te2;
+  const int lane = threadIdx.x & 31;
+  unsigned long long tests = 0;
+  const Vec4<double> zero4{0.0, 0.0, 0.0, 0.0};
+  for (;;) {
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(&stats->work, 1ull);
+    w = __shfl_sync(kFull, w, 0);
+    if (w >= nsurv) break;
+    const unsigned long long q = surv[w];
+    const int row = static_cast<int>(q >> 32), t2 = static_cast<int>(q & 0xffffffffull);
+    const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
+    const int r1 = map1[slot], r2 = map2[slot];
+    const long long base1 = (static_cast<long long>(r1) * g1.ntiles + t1) * n1;
+    const long long base2 = (static_cast<long long>(r2) * g2.ntiles + t2) * n2;
+    const Vec4<double> p1 = reinterpret_cast<const Vec4<double> *>(a.pad)[r1];
+    const Vec4<double> p2 = reinterpret_cast<const Vec4<double> *>(b.pad)[r2];
+    const int ty1 = t1 / g1.tw, tx1 = t1 - ty1 * g1.tw, ty2 = t2 / g2.tw, tx2 = t2 - ty2 * g2.tw;
+    const int nv1 = min(te1, g1.W - ty1 * te1), nu1 = min(te1, g1.W - tx1 * te1);
+    const int nv2 = min(te2, g2.W - ty2 * te2), nu2 = min(te2, g2.W - tx2 * te2);
+    const int ja = lane, jb = lane + 32;
+    const int ja_v = ja / te2, ja_u = ja - ja_v * te2, jb_v = jb / te2, jb_u = jb - jb_v * te2;
+    const bool va = ja < n2 && ja_v < nv2 && ja_u < nu2;
+    const bool vb = jb < n2 && jb_v < nv2 && jb_u < nu2;
+    const Vec4<double> c2a = va ? b.center[base2 + ja] : zero4, c2b = vb ? b.center[base2 + jb] : zero4;
+    Vec4<double> r2a = zero4, r2b = zero4;
+    if (va) {
+      r2a = b.half[base2 + ja];
+      r2a.x = __dadd_ru(r2a.x, p2.x);
+      r2a.y = __dadd_ru(r2a.y, p2.y);
+      r2a.z = __dadd_ru(r2a.z, p2.z);
+    }
+    if (vb) {
+      r2b = b.half[base2 + jb];
+      r2b.x = __dadd_ru(r2b.x, p2.x);
+      r2b.y = __dadd_ru(r2b.y, p2.y);
+      r2b.z = __dadd_ru(r2b.z, p2.z);
+    }
+    const unsigned long long cja = static_cast<unsigned long long>((ty2 * te2 + ja_v) * g2.W + tx2 * te2 + ja_u);
+    const unsigned long long cjb = static_cast<unsigned long long>((ty2 * te2 + jb_v) * g2.W + tx2 * te2 + jb_u);
+    const unsigned long long slot_key = static_cast<unsigned long long>(slot) << (2 * ij_bits);
+    // First corner samples of the lane's side-2 cells.
+    const Vec4<double> *S1 = a.samples + static_cast<long long>(r1) * g1.nuv * g1.nuv;
+    const Vec4<double> *S2 = b.samples + static_cast<long long>(r2) * g2.nuv * g2.nuv;
+    // Corner samples (surface points) of the lane's side-2 cells.
+    Vec4<double> Qa[4], Qb[4];
+#pragma unroll
+    for (int cn = 0; cn < 4; ++cn) {
+      const int dv = cn >> 1, du = cn & 1;
+      Qa[cn] = va ? S2[(ty2 * te2 + ja_v + dv) * g2.nuv + tx2 * te2 + ja_u + du] : zero4;
+      Qb[cn] = vb ? S2[(ty2 * te2 + jb_v + dv) * g2.nuv + tx2 * te2 + jb_u + du] : zero4;
+    }
+    const Vec4<double> &q2a = Qa[0], &q2b = Qb[0];
+    double mine = pos_inf<double>(), close = pos_inf<double>();
+    for (int a1 = 0; a1 < nv1; ++a1) {
+      for (int b1 = 0; b1 < nu1; ++b1) {
+        const Vec4<double> c1 = a.center[base1 + a1 * te1 + b1];
+        Vec4<double> r1v = a.half[base1 + a1 * te1 + b1];
+        r1v.x = __dadd_ru(r1v.x, p1.x);
+        r1v.y = __dadd_ru(r1v.y, p1.y);
+        r1v.z = __dadd_ru(r1v.z, p1.z);
+        const double ga = gap2_rd(axis_gap_rd(c1.x, r1v.x, c2a.x, r2a.x), axis_gap_rd(c1.y, r1v.y, c2a.y, r2a.y),
+                                  axis_gap_rd(c1.z, r1v.z, c2a.z, r2a.z));
+        const double gb = gap2_rd(axis_gap_rd(c1.x, r1v.x, c2b.x, r2b.x), axis_gap_rd(c1.y, r1v.y, c2b.y, r2b.y),
+                                  axis_gap_rd(c1.z, r1v.z, c2b.z, r2b.z));
+        bool ha = va && ga <= ub2, hb = vb && gb <= ub2;
+        double ka = ga, kb = gb;
+        if (ha || hb) {
+          Vec4<double> P[4];
+#pragma unroll
+          for (int cn = 0; cn < 4; ++cn)
+            P[cn] = S1[(ty1 * te1 + a1 + (cn >> 1)) * g1.nuv + tx1 * te1 + b1 + (cn & 1)];
+          // Tighter second-order bound (both bounds are valid: keep the larger).
+          if (ha) {
+            const double pg = proj_gap_rd(P, Qa, c1, c2a, p1, p2);
+            ka = fmax(ka, __dmul_rd(pg, pg));
+            ha = ka <= ub2;
+          }
+          if (hb) {
+            const double pg = proj_gap_rd(P, Qb, c1, c2b, p1, p2);
+            kb = fmax(kb, __dmul_rd(pg, pg));
+            hb = kb <= ub2;
+          }
+          if (ha) close = fmin(close, dist2_ru(P[0], q2a));
+          if (hb) close = fmin(close, dist2_ru(P[0], q2b));
+        }
+        if (ha) mine = fmin(mine, ka);
+        if (hb) mine = fmin(mine, kb);
+        if (__any_sync(kFull, ha || hb)) {
+          const unsigned long long ci =
+              static_cast<unsigned long long>((ty1 * te1 + a1) * g1.W + tx1 * te1 + b1) << ij_bits;
+          long long pos = warp_append(ha, &stats->candidates);
+          if (pos >= 0 && static_cast<unsigned long long>(pos) < key_cap) keys[pos] = slot_key | ci | cja;
+          pos = warp_append(hb, &stats->candidates);
+          if (pos >= 0 && static_cast<unsigned long long>(pos) < key_cap) keys[pos] = slot_key | ci | cjb;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mine = fmin(mine, __shfl_xor_sync(kFull, mine, o));
+      close = fmin(close, __shfl_xor_sync(kFull, close, o));
+    }
+    if (lane == 0) {
+      tests += static_cast<unsigned long long>(nv1 * nu1) * (nv2 * nu2);
+      if (mine < pos_inf<double>()) atomicMin(&stats->lb_bits, static_cast<unsigned long long>(__double_as_longlong(mine)));
+      if (close < pos_inf<double>())
+        atomicMin(&stats->ub_bits, static_cast<unsigned long long>(__double_as_longlong(close)));
+    }
+  }
+  if (lane == 0) atomicAdd(&stats->pair_tests, tests);
+}
+
 __global__ void k_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2,
                              int *idx, unsigned *flag1) {
   const unsigned long long mij = (1ull << ij_bits) - 1ull;
@@ -1810,7 +2075,7 @@ __global__ void k_flag_runs(const unsigned long long *sorted, long long n, unsig
 template <typename T>
 __global__ void k_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
                               const unsigned *ex1, SideRound<T> cur, const int *map1, RegionRec<T> *next,
-                              int *nmap1) {
+                              int *nmap1, int cover) {
   const unsigned long long mij = (1ull << ij_bits) - 1ull;
   for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < n;
        q += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -1820,7 +2085,8 @@ __global__ void k_inter_side1(const unsigned long long *keys, long long n, int i
       const unsigned long long k = keys[q];
       const int slot = static_cast<int>(k >> (2 * ij_bits));
       const int i = static_cast<int>((k >> ij_bits) & mij);
-      next[id] = child_rect(cur.regions[map1[slot]], cur.g.nuv, i);
+      next[id] = cover ? child_rect_cover(cur.regions[map1[slot]], cur.g.nuv, i)
+                       : child_rect(cur.regions[map1[slot]], cur.g.nuv, i);
     }
   }
 }
@@ -1829,7 +2095,7 @@ __global__ void k_inter_side1(const unsigned long long *keys, long long n, int i
 template <typename T>
 __global__ void k_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
                               const unsigned *flag2, const unsigned *ex2, SideRound<T> cur, const int *map2,
-                              RegionRec<T> *next, int *nmap2) {
+                              RegionRec<T> *next, int *nmap2, int cover) {
   const unsigned long long mij = (1ull << ij_bits) - 1ull;
   for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -1839,7 +2105,8 @@ __global__ void k_inter_side2(const unsigned long long *key2s, const int *idxs, 
       const unsigned long long k = key2s[p];
       const int slot = static_cast<int>(k >> ij_bits);
       const int j = static_cast<int>(k & mij);
-      next[id] = child_rect(cur.regions[map2[slot]], cur.g.nuv, j);
+      next[id] = cover ? child_rect_cover(cur.regions[map2[slot]], cur.g.nuv, j)
+                       : child_rect(cur.regions[map2[slot]], cur.g.nuv, j);
     }
   }
 }
@@ -2708,17 +2975,17 @@ inline dim3 bdim(int gx, const Batch &bt) { return dim3(static_cast<unsigned>(gx
 
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt,
-                  const SurfView<T> *vdev) {
+                  const SurfView<T> *vdev, bool cover) {
   counted();
   const long long n = static_cast<long long>(sr.nreg) * 2 * sr.g.nuv;
   // Degrees are part of a batch's shape: the host view decides the variant.
   const int maxdeg = s.degu > s.degv ? s.degu : s.degv;
   if (maxdeg < 8)
     k_basis<T, 9><<<bdim(bgrid((n + 127) / 128, bt, 148 * 16), bt), 128, 0, st>>>(
-        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs);
+        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs, cover ? 1 : 0);
   else
     k_basis<T, kMaxDeg + 1><<<bdim(bgrid((n + 63) / 64, bt, 148 * 16), bt), 64, 0, st>>>(
-        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs);
+        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs, cover ? 1 : 0);
 }
 
 template <typename T>
@@ -2943,6 +3210,32 @@ void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *
   k_inter_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats);
 }
 
+void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
+                      cudaStream_t st) {
+  counted();
+  k_pad_bound<<<(sr.nreg + 127) / 128, 128, 0, st>>>(sr, reinterpret_cast<Vec4<double> *>(sr.pad),
+                                                     Vec4<double>{m2u[0], m2u[1], m2u[2], 0.0},
+                                                     Vec4<double>{m2v[0], m2v[1], m2v[2], 0.0}, eps);
+}
+
+void launch_bound_cull(const SideRound<double> &a, const SideRound<double> &b, const int *map1, const int *map2,
+                       int nslots, double ub2, unsigned long long *surv, unsigned long long surv_cap,
+                       ScreenStats *stats, cudaStream_t st) {
+  counted();
+  const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
+  k_bound_cull<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, ub2, surv, surv_cap, stats);
+}
+
+void launch_bound_leaf(const SideRound<double> &a, const SideRound<double> &b, const int *map1, const int *map2,
+                       const unsigned long long *surv, unsigned long long nsurv, int ij_bits, double ub2,
+                       unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st) {
+  counted();
+  if (nsurv == 0) return;
+  const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
+  const int blocks = static_cast<int>((warps + 7) / 8);
+  k_bound_leaf<<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, ub2, keys, key_cap, stats);
+}
+
 void launch_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2, int *idx,
                        unsigned *flag1, cudaStream_t st) {
   counted();
@@ -2957,17 +3250,19 @@ void launch_flag_runs(const unsigned long long *sorted, long long n, unsigned *f
 template <typename T>
 void launch_inter_side1(const unsigned long long *keys, long long n, int ij_bits, const unsigned *flag1,
                         const unsigned *ex1, const SideRound<T> &cur, const int *map1, RegionRec<T> *next,
-                        int *nmap1, cudaStream_t st) {
+                        int *nmap1, cudaStream_t st, bool cover) {
   counted();
-  k_inter_side1<T><<<grid_for(n, 256), 256, 0, st>>>(keys, n, ij_bits, flag1, ex1, cur, map1, next, nmap1);
+  k_inter_side1<T><<<grid_for(n, 256), 256, 0, st>>>(keys, n, ij_bits, flag1, ex1, cur, map1, next, nmap1,
+                                                     cover ? 1 : 0);
 }
 
 template <typename T>
 void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long long n, int ij_bits,
                         const unsigned *flag2, const unsigned *ex2, const SideRound<T> &cur, const int *map2,
-                        RegionRec<T> *next, int *nmap2, cudaStream_t st) {
+                        RegionRec<T> *next, int *nmap2, cudaStream_t st, bool cover) {
   counted();
-  k_inter_side2<T><<<grid_for(n, 256), 256, 0, st>>>(key2s, idxs, n, ij_bits, flag2, ex2, cur, map2, next, nmap2);
+  k_inter_side2<T><<<grid_for(n, 256), 256, 0, st>>>(key2s, idxs, n, ij_bits, flag2, ex2, cur, map2, next, nmap2,
+                                                     cover ? 1 : 0);
 }
 
 void launch_samples_screen(const SurfView<float> &s, const SideRound<double> &basis_side, const SideRound<float> &out,
@@ -3059,7 +3354,7 @@ void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb,
 
 #define JSI_INSTANTIATE(T)                                                                                        \
   template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t, const Batch &,           \
-                                const SurfView<T> *);                                                             \
+                                const SurfView<T> *, bool);                                                       \
   template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t, const Batch &,   \
                                   const SurfView<T> *);                                                           \
   template void launch_pad<T>(const SideRound<T> &, bool, T, T, cudaStream_t);                                    \
@@ -3101,10 +3396,10 @@ void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb,
                                      unsigned long long, ScreenStats *, cudaStream_t);                            \
   template void launch_inter_side1<T>(const unsigned long long *, long long, int, const unsigned *,               \
                                       const unsigned *, const SideRound<T> &, const int *, RegionRec<T> *, int *, \
-                                      cudaStream_t);                                                              \
+                                      cudaStream_t, bool);                                                        \
   template void launch_inter_side2<T>(const unsigned long long *, const int *, long long, int, const unsigned *,  \
                                       const unsigned *, const SideRound<T> &, const int *, RegionRec<T> *, int *, \
-                                      cudaStream_t);
+                                      cudaStream_t, bool);
 
 JSI_INSTANTIATE(float)
 JSI_INSTANTIATE(double)
