@@ -233,6 +233,45 @@ void jsi_bounds_params_default(jsi_bounds_params *p);
 int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_bounds_params *params,
                         jsi_bounds_result *out);
 
+/* --- intersection curves ----------------------------------------------------
+ * No counterpart in the reference, which stops at the per-round overlap
+ * counts (intersection.cu:467-474); the step after it, and the output of
+ * OpenCASCADE's GeomAPI_IntSS that its benchmark compares against
+ * (benchmarks/opencascade_compare.cpp:209-219).  Runs the FP64 intersection
+ * query with Newton points, sampling every refined cell to its far edge
+ * (the reference's grid leaves the last strip of each cell unsampled, which
+ * would leave gaps in the points), then links the converged points:
+ * tangents t = N1 x N2 on the device, then from a seed point a walk to the
+ * nearest unvisited point ahead along the tangent (within link_tol), in both
+ * directions; a walk that returns to its seed closes the curve.  Points the
+ * walk passes (nearer than the chosen next point and along the curve) join
+ * that curve without becoming vertices.
+ * Caller buffers: vertex (vertex_cap x 7: x, y, z, u, v, s, t, in curve
+ * order), curve_start (curve_cap + 1 offsets), curve_closed (curve_cap).
+ * When they are too small the call returns JSI_ERR_CAPACITY with vertices /
+ * curves set to the sizes needed. */
+typedef struct {
+  jsi_inter_params inter; /* the intersection query (precision FP64 is used) */
+  double link_tol;        /* largest step between vertices; 0: 4 x the median size of the final cells */
+} jsi_curve_params;
+
+typedef struct {
+  long long points_found; /* converged intersection points */
+  long long vertices;     /* polyline vertices (written, or needed) */
+  long long curves;       /* polylines with >= 2 vertices (written, or needed) */
+  double link_tol;        /* the tolerance used */
+  double *vertex;
+  long long vertex_cap;
+  long long *curve_start;
+  int *curve_closed;
+  long long curve_cap;
+  float device_ms;
+} jsi_curve_result;
+
+void jsi_curve_params_default(jsi_curve_params *p);
+int jsi_intersection_curves(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_curve_params *params,
+                            jsi_curve_result *out);
+
 /* --- queued and batched queries (the serving engine) ----------------------
  * No counterpart in the reference, whose API runs one query at a time and is
  * not re-entrant (file statics, intersection.cu:36-39).  jsi_workers starts n

@@ -31,7 +31,7 @@ EXPORTED = [
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_units", "jsi_kernel_names",
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_bounds_params_default",
-    "jsi_distance_bounds", "jsi_eval_grid", "jsi_eval_grid_f64",
+    "jsi_distance_bounds", "jsi_curve_params_default", "jsi_intersection_curves", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
     "jsi_queue_depth", "jsi_min_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs",
 ]
@@ -75,6 +75,18 @@ class InterResult(ctypes.Structure):
                 ("trace_written", ctypes.c_longlong), ("points", ctypes.POINTER(ctypes.c_double)),
                 ("points_cap", ctypes.c_longlong), ("points_written", ctypes.c_longlong),
                 ("points_converged", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+
+
+class CurveParams(ctypes.Structure):
+    _fields_ = [("inter", InterParams), ("link_tol", ctypes.c_double)]
+
+
+class CurveResult(ctypes.Structure):
+    _fields_ = [("points_found", ctypes.c_longlong), ("vertices", ctypes.c_longlong), ("curves", ctypes.c_longlong),
+                ("link_tol", ctypes.c_double), ("vertex", ctypes.POINTER(ctypes.c_double)),
+                ("vertex_cap", ctypes.c_longlong), ("curve_start", ctypes.POINTER(ctypes.c_longlong)),
+                ("curve_closed", ctypes.POINTER(ctypes.c_int)), ("curve_cap", ctypes.c_longlong),
+                ("device_ms", ctypes.c_float)]
 
 
 class BoundsParams(ctypes.Structure):
@@ -169,6 +181,11 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_surface_upload_many.argtypes = [P, I, ctypes.POINTER(I), ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
                                           ctypes.POINTER(I), ctypes.POINTER(I)]
     L.jsi_surface_upload_many.restype = I
+    L.jsi_curve_params_default.argtypes = [ctypes.POINTER(CurveParams)]
+    L.jsi_curve_params_default.restype = None
+    L.jsi_intersection_curves.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(CurveParams),
+                                          ctypes.POINTER(CurveResult)]
+    L.jsi_intersection_curves.restype = I
     L.jsi_bounds_params_default.argtypes = [ctypes.POINTER(BoundsParams)]
     L.jsi_bounds_params_default.restype = None
     L.jsi_distance_bounds.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(BoundsParams),

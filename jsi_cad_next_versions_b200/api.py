@@ -50,6 +50,17 @@ class DistanceResult:
 
 
 @dataclass
+class IntersectionCurves:
+    """Polylines through the refined intersection points: curves[k] is an
+    (m, 7) array of (x, y, z, u, v, s, t) in curve order."""
+    points_found: int
+    link_tol: float
+    curves: list
+    closed: list
+    device_ms: float
+
+
+@dataclass
 class DistanceBounds:
     """Certified interval lb <= min distance <= ub (bounds mode)."""
     lb: float
@@ -310,6 +321,31 @@ class Context:
         self._check(self.lib.jsi_min_distance_batch(self.handle, n, ta, tb, ctypes.byref(p), res, status,
                                                     ctypes.byref(ms)))
         return [self._dist_result(res[q], bufs[q], k) for q in range(n)], ms.value
+
+    def intersection_curves(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
+                            halve_threshold: int = 512, min_nuv: int = 4, link_tol: float = 0.0,
+                            vertex_cap: int = 1 << 18, curve_cap: int = 1 << 12) -> IntersectionCurves:
+        """Intersection curves of two surface rectangles (FP64 query, Newton
+        points linked into polylines)."""
+        ip = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, C.PRECISIONS["fp64"], 1)
+        for _ in range(2):
+            p = C.CurveParams(ip, link_tol)
+            verts = np.zeros((vertex_cap, 7), np.float64)
+            starts = np.zeros(curve_cap + 1, np.int64)
+            closed = np.zeros(curve_cap, np.int32)
+            r = C.CurveResult(0, 0, 0, 0.0, verts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), vertex_cap,
+                              starts.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                              closed.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), curve_cap, 0.0)
+            st = self.lib.jsi_intersection_curves(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
+                                                  ctypes.byref(r))
+            if st == -4 and (r.vertices > vertex_cap or r.curves > curve_cap):
+                vertex_cap, curve_cap = max(vertex_cap, r.vertices), max(curve_cap, r.curves)
+                continue
+            self._check(st)
+            n = r.curves
+            curves = [verts[starts[k]:starts[k + 1]].copy() for k in range(n)]
+            return IntersectionCurves(r.points_found, r.link_tol, curves, [bool(x) for x in closed[:n]], r.device_ms)
+        self._check(st)
 
     def distance_bounds(self, a: C.Task, b: C.Task, *, nuv_refine: int = 8, max_rounds: int = 10,
                         rel_tol: float = 1e-6, max_pairs: int = 1 << 22) -> DistanceBounds:

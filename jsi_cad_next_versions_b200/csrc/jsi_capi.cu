@@ -29,6 +29,7 @@
 #include <string>
 #include <thread>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -638,10 +639,11 @@ SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, Regio
 // distance_analysis.cu:88-116 / intersection.cu:175-219).
 template <typename T>
 void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect, bool use_k, T span_u0,
-                T span_v0) {
+                T span_v0, bool cover = false) {
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
-  timed(ctx, "basis", [&] { launch_basis(v, s, st); }, 2.0 * s.nreg * s.g.nuv);
+  timed(ctx, "basis", [&] { launch_basis(v, s, st, Batch{}, static_cast<const SurfView<T> *>(nullptr), cover); },
+        2.0 * s.nreg * s.g.nuv);
   if (!intersect) {
     // Distance: centres straight from the basis tables, no sample grid.
     timed(ctx, "cells", [&] { launch_cells_fused(v, s, s, st); }, double(s.nreg) * s.g.W * s.g.W);
@@ -1594,9 +1596,24 @@ void next_regions(Lane *ctx, const unsigned long long *sorted, long long n, int 
   *nmap2_out = nmap2;
 }
 
+// The final round of an intersection query, for the curve linking.
+template <typename T>
+struct FinalRound {
+  const double *points = nullptr;  // 8 doubles per pair, key order
+  long long n = 0;
+  const RegionRec<T> *reg1 = nullptr, *reg2 = nullptr;
+  const int *map1 = nullptr, *map2 = nullptr;
+  int nuv1 = 0, nuv2 = 0;
+  const unsigned long long *keys = nullptr;
+  int ij_bits = 0;
+};
+
+// cover: sample the covering grid (every refined cell sampled to its far edge)
+// instead of the reference's grid; used by the curve linking, whose points
+// would otherwise skip the last strip of every refined cell.
 template <typename T>
 void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
-                      jsi_inter_result *out) {
+                      jsi_inter_result *out, FinalRound<T> *fin = nullptr, bool cover = false) {
   Arena &ar = ctx->arena;
   cudaStream_t st = ctx->stream;
   const SurfaceRec &sa = get_surface(ctx, ta->surface);
@@ -1628,8 +1645,8 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
   std::vector<unsigned long long> hkeys;
   for (int round = 1; round <= p->rounds; ++round) {
     const int sau = round == 1 ? side_a : 1, sbu = round == 1 ? side_b : 2;
-    build_side(ctx, va, A, true, use_k, span_u[sau], span_v[sau]);
-    build_side(ctx, vb, B, true, use_k, span_u[sbu], span_v[sbu]);
+    build_side(ctx, va, A, true, use_k, span_u[sau], span_v[sau], cover);
+    build_side(ctx, vb, B, true, use_k, span_u[sbu], span_v[sbu], cover);
     if (round == 1) {
       T pads[2];
       JSI_CUDA(copy_async(ctx, &pads[0], A.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
@@ -1703,7 +1720,7 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
     }
     written += n;
     if (round == p->rounds || n == 0) {
-      if (p->points && n > 0 && out->points) {
+      if (p->points && n > 0 && (out->points || fin)) {
         // Intersection points from every final pair (minimum-norm Gauss-Newton).
         double dom[8];
         newton_domain(ta, tb, dom);
@@ -1714,7 +1731,19 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
           launch_newton_inter(view<double>(sa), view<double>(sb), A.regions, B.regions, map1, map2, A.g.nuv, B.g.nuv,
                               sorted, n, ij_bits, ddom, dres, st);
         }, double(n));
-        const long long keep = std::min<long long>(n, out->points_cap);
+        if (fin) {
+          fin->points = dres;
+          fin->n = n;
+          fin->reg1 = A.regions;
+          fin->reg2 = B.regions;
+          fin->map1 = map1;
+          fin->map2 = map2;
+          fin->nuv1 = A.g.nuv;
+          fin->nuv2 = B.g.nuv;
+          fin->keys = sorted;
+          fin->ij_bits = ij_bits;
+        }
+        const long long keep = out->points ? std::min<long long>(n, out->points_cap) : 0;
         if (keep > 0)
           JSI_CUDA(copy_async(ctx, out->points, dres, static_cast<size_t>(keep) * 8 * sizeof(double),
                               cudaMemcpyDeviceToHost, st));
@@ -1735,7 +1764,7 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
     // Pair-preserving jobs and (slot, cell) dedup per side on the device.
     RegionRec<T> *next1, *next2;
     int *nmap1, *nmap2, r1, r2;
-    next_regions<T>(ctx, sorted, n, ij_bits, slot_bits, A, B, map1, map2, false, &next1, &next2, &nmap1, &nmap2, &r1,
+    next_regions<T>(ctx, sorted, n, ij_bits, slot_bits, A, B, map1, map2, cover, &next1, &next2, &nmap1, &nmap2, &r1,
                     &r2);
     A = make_side<T>(ar, make_geom(nuv, p1_of(sa)), r1, true, next1);
     B = make_side<T>(ar, make_geom(nuv, p1_of(sb)), r2, true, next2);
@@ -1961,6 +1990,194 @@ void run_bounds(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_bou
   out->lb = lb;
   out->ub = ub;
 }
+
+// ---------------------------------------------------------------------------
+// Intersection curves: refined points linked into polylines
+// ---------------------------------------------------------------------------
+
+struct CurvePoint {
+  double x[3];
+  double uvst[4];
+  double t[3];  // unit tangent
+};
+
+// Uniform hash grid over the points (cell = link tolerance).
+class PointGrid {
+ public:
+  PointGrid(const std::vector<CurvePoint> &pts, double cell) : pts_(pts), cell_(cell) {
+    for (size_t q = 0; q < pts.size(); ++q) cells_[key(pts[q].x)].push_back(static_cast<int>(q));
+  }
+  template <typename Fn>
+  void near(const double *x, Fn &&fn) const {
+    const long long ix = cellc(x[0]), iy = cellc(x[1]), iz = cellc(x[2]);
+    for (long long a = ix - 1; a <= ix + 1; ++a)
+      for (long long b = iy - 1; b <= iy + 1; ++b)
+        for (long long c = iz - 1; c <= iz + 1; ++c) {
+          auto it = cells_.find(pack(a, b, c));
+          if (it == cells_.end()) continue;
+          for (int q : it->second) fn(q);
+        }
+  }
+
+ private:
+  long long cellc(double v) const { return static_cast<long long>(std::floor(v / cell_)); }
+  static long long pack(long long a, long long b, long long c) {
+    return ((a & 0x1fffff) << 42) | ((b & 0x1fffff) << 21) | (c & 0x1fffff);
+  }
+  long long key(const double *x) const { return pack(cellc(x[0]), cellc(x[1]), cellc(x[2])); }
+  const std::vector<CurvePoint> &pts_;
+  double cell_;
+  std::unordered_map<long long, std::vector<int>> cells_;
+};
+
+double dist3(const double *a, const double *b) {
+  const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+  return std::sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+// Walks from point c along direction d (unit): each step goes to the nearest
+// unvisited point ahead within tol; points nearer than it along the curve
+// (ahead or behind) are absorbed, and so are repeats of a point (closer than
+// 1e-6 tol: several cell pairs refine to the same curve point, and a step
+// onto a repeat would take an arbitrary direction).
+std::vector<int> walk_curve(const std::vector<CurvePoint> &pts, const PointGrid &grid, std::vector<char> &visited,
+                            int c, double d[3], double tol) {
+  std::vector<int> path;
+  for (;;) {
+    int best = -1;
+    double bd = INFINITY;
+    grid.near(pts[c].x, [&](int o) {
+      if (visited[o]) return;
+      const double v[3] = {pts[o].x[0] - pts[c].x[0], pts[o].x[1] - pts[c].x[1], pts[o].x[2] - pts[c].x[2]};
+      const double dist = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      if (dist <= 1e-6 * tol) {
+        visited[o] = 1;  // the same point again
+        return;
+      }
+      if (dist > tol) return;
+      const double along = v[0] * d[0] + v[1] * d[1] + v[2] * d[2];
+      if (along > 0.3 * dist && dist < bd) {
+        bd = dist;
+        best = o;
+      }
+    });
+    if (best < 0) break;
+    grid.near(pts[c].x, [&](int o) {
+      if (visited[o] || o == best) return;
+      const double v[3] = {pts[o].x[0] - pts[c].x[0], pts[o].x[1] - pts[c].x[1], pts[o].x[2] - pts[c].x[2]};
+      const double dist = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      const double along = v[0] * d[0] + v[1] * d[1] + v[2] * d[2];
+      if (dist < bd && std::fabs(along) >= 0.7 * dist) visited[o] = 1;
+    });
+    visited[best] = 1;
+    path.push_back(best);
+    const double v[3] = {pts[best].x[0] - pts[c].x[0], pts[best].x[1] - pts[c].x[1], pts[best].x[2] - pts[c].x[2]};
+    const double s = v[0] * pts[best].t[0] + v[1] * pts[best].t[1] + v[2] * pts[best].t[2] >= 0.0 ? 1.0 : -1.0;
+    for (int k = 0; k < 3; ++k) d[k] = s * pts[best].t[k];
+    c = best;
+  }
+  return path;
+}
+
+void link_curves(const std::vector<CurvePoint> &pts, double tol, std::vector<std::vector<int>> &curves,
+                 std::vector<int> &closed) {
+  if (pts.empty() || !(tol > 0.0)) return;
+  PointGrid grid(pts, tol);
+  std::vector<char> visited(pts.size(), 0);
+  for (size_t s = 0; s < pts.size(); ++s) {
+    if (visited[s]) continue;
+    visited[s] = 1;
+    double d[3] = {pts[s].t[0], pts[s].t[1], pts[s].t[2]};
+    std::vector<int> fwd = walk_curve(pts, grid, visited, static_cast<int>(s), d, tol);
+    const bool loop = fwd.size() >= 3 && dist3(pts[fwd.back()].x, pts[s].x) <= tol;
+    std::vector<int> curve;
+    if (!loop) {
+      double e[3] = {-pts[s].t[0], -pts[s].t[1], -pts[s].t[2]};
+      std::vector<int> bwd = walk_curve(pts, grid, visited, static_cast<int>(s), e, tol);
+      curve.assign(bwd.rbegin(), bwd.rend());
+    }
+    curve.push_back(static_cast<int>(s));
+    curve.insert(curve.end(), fwd.begin(), fwd.end());
+    if (curve.size() >= 2) {
+      curves.push_back(std::move(curve));
+      closed.push_back(loop ? 1 : 0);
+    }
+  }
+}
+
+// The FP64 intersection query with Newton points, tangents on the device,
+// then the links on the host.
+void run_curves(Lane *L, const jsi_task *ta, const jsi_task *tb, const jsi_curve_params *p, jsi_curve_result *out) {
+  jsi_inter_result ir;
+  std::memset(&ir, 0, sizeof(ir));
+  jsi_inter_params ip = p->inter;
+  ip.points = 1;
+  FinalRound<double> fin;
+  run_intersection<double>(L, ta, tb, &ip, &ir, &fin, true);
+  const double *dpts = fin.points;
+  const long long np = fin.n;
+  std::vector<CurvePoint> pts;
+  std::vector<double> scales;
+  if (np > 0 && dpts) {
+    const SurfaceRec &sa = get_surface(L, ta->surface);
+    const SurfaceRec &sb = get_surface(L, tb->surface);
+    double *dtan = L->arena.get<double>(static_cast<size_t>(np) * 5);
+    timed(L, "curve_tangents", [&] {
+      launch_curve_tangents(view<double>(sa), view<double>(sb), fin.reg1, fin.reg2, fin.map1, fin.map2, fin.nuv1,
+                            fin.nuv2, fin.keys, fin.ij_bits, dpts, np, dtan, L->stream);
+    });
+    std::vector<double> hp(static_cast<size_t>(np) * 8), ht(static_cast<size_t>(np) * 5);
+    JSI_CUDA(copy_async(L, hp.data(), dpts, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+    JSI_CUDA(copy_async(L, ht.data(), dtan, ht.size() * sizeof(double), cudaMemcpyDeviceToHost, L->stream));
+    JSI_CUDA(cudaStreamSynchronize(L->stream));
+    for (long long q = 0; q < np; ++q) {
+      const double *x = hp.data() + q * 8, *t = ht.data() + q * 5;
+      const double scale = 1.0 + std::fabs(x[0]) + std::fabs(x[1]) + std::fabs(x[2]);
+      if (!(x[7] <= 1e-9 * scale) || t[3] == 0.0) continue;  // not converged / no tangent
+      CurvePoint cp;
+      for (int k = 0; k < 3; ++k) {
+        cp.x[k] = x[k];
+        cp.t[k] = t[k];
+      }
+      for (int k = 0; k < 4; ++k) cp.uvst[k] = x[3 + k];
+      pts.push_back(cp);
+      scales.push_back(t[4]);
+    }
+  }
+  out->points_found = static_cast<long long>(pts.size());
+  // Default tolerance: 4 x the median size of the cells the points were
+  // refined from (on the covering grid consecutive points come from
+  // neighbouring cells).
+  double tol = p->link_tol;
+  if (!(tol > 0.0) && !scales.empty()) {
+    std::nth_element(scales.begin(), scales.begin() + scales.size() / 2, scales.end());
+    tol = 4.0 * scales[scales.size() / 2];
+  }
+  out->link_tol = tol;
+  std::vector<std::vector<int>> curves;
+  std::vector<int> closed;
+  link_curves(pts, tol, curves, closed);
+  long long nv = 0;
+  for (const auto &cv : curves) nv += static_cast<long long>(cv.size());
+  out->vertices = nv;
+  out->curves = static_cast<long long>(curves.size());
+  if (nv > out->vertex_cap || out->curves > out->curve_cap || (nv > 0 && (!out->vertex || !out->curve_start)))
+    fail(JSI_ERR_CAPACITY, "%lld vertices / %lld curves do not fit the buffers (%lld / %lld)", nv, out->curves,
+         out->vertex_cap, out->curve_cap);
+  long long w = 0;
+  for (size_t k = 0; k < curves.size(); ++k) {
+    out->curve_start[k] = w;
+    if (out->curve_closed) out->curve_closed[k] = closed[k];
+    for (int q : curves[k]) {
+      double *v = out->vertex + w * 7;
+      for (int c = 0; c < 3; ++c) v[c] = pts[q].x[c];
+      for (int c = 0; c < 4; ++c) v[3 + c] = pts[q].uvst[c];
+      ++w;
+    }
+  }
+  if (out->curve_start) out->curve_start[curves.size()] = w;
+}
+
 
 
 void check_precision(int prec, bool screen_built) {
@@ -2489,6 +2706,41 @@ int jsi_min_distance(jsi_context *ctx, const jsi_task *a, const jsi_task *b, con
     if (params) p = *params;
     validate_dist(p, a, b);
     exec_distance(&ctx->main, a, b, p, out);
+    return JSI_OK;
+  });
+}
+
+void jsi_curve_params_default(jsi_curve_params *p) {
+  if (!p) return;
+  jsi_inter_params_default(&p->inter);
+  p->inter.precision = JSI_PREC_FP64;
+  p->inter.points = 1;
+  p->link_tol = 0.0;
+}
+
+int jsi_intersection_curves(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_curve_params *params,
+                            jsi_curve_result *out) {
+  if (!ctx || !a || !b || !out) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    jsi_curve_params p;
+    jsi_curve_params_default(&p);
+    if (params) p = *params;
+    p.inter.precision = JSI_PREC_FP64;
+    validate_inter(p.inter, a, b);
+    if (!(p.link_tol >= 0.0)) fail(JSI_ERR_INVALID, "link_tol must be >= 0");
+    out->points_found = out->vertices = out->curves = 0;
+    out->link_tol = 0.0;
+    out->device_ms = 0.0f;
+    Lane *L = &ctx->main;
+    JSI_CUDA(cudaSetDevice(L->device));
+    L->arena.reset();
+    JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
+    run_curves(L, a, b, &p, out);
+    JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
+    JSI_CUDA(cudaEventSynchronize(L->ev1));
+    JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
+    if (L->timing) resolve_timing(L);
     return JSI_OK;
   });
 }

@@ -291,6 +291,13 @@ void launch_inter_side2(const unsigned long long *key2s, const int *idxs, long l
 // pairs whose box gap (rounded down) can be <= ub, ub2 = ub^2 rounded up; the
 // leaf appends (slot, i, j) keys like the intersection leaf and folds the
 // smallest kept squared gap into stats->lb_bits.
+// Unit tangents and source-cell scales (tx, ty, tz, ok, scale) of the
+// intersection curve at refined points (8 doubles each: x, y, z, u, v, s, t,
+// residual, in the order of the final round's pair keys).
+void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<double> *reg1,
+                           const RegionRec<double> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                           const unsigned long long *keys, int ij_bits, const double *pts, long long n, double *out,
+                           cudaStream_t st);
 // sr.pad must hold 4 doubles per region (a Vec4 pad per region, x, y, z).
 void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
                       cudaStream_t st);

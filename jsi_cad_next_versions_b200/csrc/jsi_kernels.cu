@@ -2941,6 +2941,52 @@ __global__ void k_surface_prep(const SurfacePrep *jobs) {
   }
 }
 
+// Unit tangent of the intersection curve at each refined point: the cross
+// product of the two surface normals (Su x Sv, Ss x St) at the point's
+// parameters; and the size of the point's source cells (the final-round
+// pair it was refined from), |Su| du + |Sv| dv on the larger side, the
+// spacing scale of the points.  out: tx, ty, tz, ok (0 where the normals are
+// parallel or vanish), scale.  pts: 8 doubles per point (x, y, z, u, v, s, t,
+// residual), in the order of the pair keys.
+template <typename TP>
+__global__ void k_curve_tangents(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
+                                 const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                                 const unsigned long long *keys, int ij_bits, const double *pts, long long n,
+                                 double *out) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= n) return;
+  const double *q = pts + e * 8;
+  const unsigned long long key = keys[e];
+  const int slot = static_cast<int>(key >> (2 * ij_bits));
+  const RegionRec<TP> R1 = reg1[map1[slot]], R2 = reg2[map2[slot]];
+  double r1[18], r2[18];
+  point_record(sa, q[3], q[4], r1);
+  point_record(sb, q[5], q[6], r2);
+  auto cross = [](const double *a, const double *b, double *c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  double n1[3], n2[3], t[3];
+  cross(r1 + 3, r1 + 6, n1);
+  cross(r2 + 3, r2 + 6, n2);
+  cross(n1, n2, t);
+  const double tn = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  const double nn = sqrt((n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2]) * (n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]));
+  const bool ok = tn > 1e-12 * nn && tn > 0.0;
+  auto len3 = [](const double *a) { return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); };
+  const double s1 = len3(r1 + 3) * fabs(double(R1.u1) - double(R1.u0)) / nuv1 +
+                    len3(r1 + 6) * fabs(double(R1.v1) - double(R1.v0)) / nuv1;
+  const double s2 = len3(r2 + 3) * fabs(double(R2.u1) - double(R2.u0)) / nuv2 +
+                    len3(r2 + 6) * fabs(double(R2.v1) - double(R2.v0)) / nuv2;
+  double *o = out + e * 5;
+  o[0] = ok ? t[0] / tn : 0.0;
+  o[1] = ok ? t[1] / tn : 0.0;
+  o[2] = ok ? t[2] / tn : 0.0;
+  o[3] = ok ? 1.0 : 0.0;
+  o[4] = fmax(s1, s2);
+}
+
 inline int grid_for(long long n, int block, int max_blocks = 148 * 16) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
@@ -3208,6 +3254,16 @@ void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *
   const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
   const int blocks = static_cast<int>((warps + 7) / 8);
   k_inter_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats);
+}
+
+void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<double> *reg1,
+                           const RegionRec<double> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
+                           const unsigned long long *keys, int ij_bits, const double *pts, long long n, double *out,
+                           cudaStream_t st) {
+  counted();
+  if (n <= 0) return;
+  k_curve_tangents<double><<<static_cast<unsigned>((n + 127) / 128), 128, 0, st>>>(
+      sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, keys, ij_bits, pts, n, out);
 }
 
 void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
