@@ -2415,6 +2415,15 @@ void stop_workers(jsi_context *ctx) {
   ctx->qcv.notify_all();
   for (auto &t : ctx->threads) t.join();
   ctx->threads.clear();
+  // Per-kernel timing totals outlive the lanes (kept on the main lane).
+  for (auto &L : ctx->lanes) {
+    for (auto &kv : L->kernel_ms) {
+      auto &acc = ctx->main.kernel_ms[kv.first];
+      acc.first += kv.second.first;
+      acc.second += kv.second.second;
+    }
+    for (auto &kv : L->kernel_units) ctx->main.kernel_units[kv.first] += kv.second;
+  }
   for (auto &L : ctx->lanes) lane_free(*L);
   ctx->lanes.clear();
   ctx->stopping = false;
@@ -2431,6 +2440,7 @@ void start_workers(jsi_context *ctx, int n) {
     auto L = std::make_unique<Lane>();
     lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces, &ctx->lane_held, left);
     L->graphs_on = ctx->batch_graphs;
+    L->timing = ctx->main.timing;  // per-kernel timing follows the context's setting
     ctx->lanes.push_back(std::move(L));
   }
   for (auto &L : ctx->lanes) ctx->threads.emplace_back(worker_loop, ctx, L.get());

@@ -65,6 +65,10 @@ class SurfaceCache:
         self.rects.append(np.array(surf.rect(), np.float32))
         return len(self.ids) - 1
 
+    def add_many(self, surfs) -> None:
+        self.ids.extend(self.ctx.upload_many(surfs))
+        self.rects.extend(np.array(s.rect(), np.float32) for s in surfs)
+
     def __len__(self):
         return len(self.ids)
 
@@ -220,8 +224,8 @@ def build_cache(ctx, n: int, seed: int = 7) -> SurfaceCache:
     nets 4..64 log-uniform, 30% rational, random-phase height fields)."""
     rng = synth.SplitMix64(seed)
     cache = SurfaceCache(ctx)
-    for q in range(n):
-        cache.add(synth.random_surface(rng, name=f"cache{q}"))
+    for q0 in range(0, n, 1024):
+        cache.add_many([synth.random_surface(rng, name=f"cache{q}") for q in range(q0, min(n, q0 + 1024))])
     return cache
 
 
@@ -236,6 +240,7 @@ def main(argv=None):
     ap.add_argument("--nuv-lo", type=int, default=64)
     ap.add_argument("--nuv-hi", type=int, default=512)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--profile", action="store_true", help="print the per-kernel device time of each run")
     args = ap.parse_args(argv)
     from .api import Context
     with Context(args.device) as ctx:
@@ -247,7 +252,13 @@ def main(argv=None):
                 qs = poisson_queries(args.queries, rate, len(cache), nuv_lo=args.nuv_lo, nuv_hi=args.nuv_hi)
                 loop = ServingLoop(ctx, cache, lanes=args.lanes, budget_bytes=int(args.budget_gb * (1 << 30)),
                                    precision=form)
+                if args.profile:
+                    ctx.kernel_timing(True)
                 st = loop.run(qs)
+                kt = {}
+                if args.profile:
+                    kt = {k: round(v[0], 2) for k, v in sorted(ctx.kernel_times().items(), key=lambda kv: -kv[1][0])[:12]}
+                    ctx.kernel_timing(False)
                 reasons = sorted({q.status for q in qs if q.status != "ok"})[:3]
                 print(json.dumps({
                     "form": form, "offered_rate": rate, "queries": st.queries, "completed": st.completed,
@@ -255,7 +266,8 @@ def main(argv=None):
                     "failed": st.failed, "throughput_qps": st.throughput, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
                     "peak_admitted_gb": st.peak_admitted_bytes / (1 << 30), "peak_inflight": st.peak_inflight,
                     "lanes": args.lanes, "resident_surfaces": len(cache), "resident_mb": ctx.resident_bytes() / 2**20,
-                    "cache_load_s": load_s, "nuv0_range": [args.nuv_lo, args.nuv_hi]}), flush=True)
+                    "cache_load_s": load_s, "nuv0_range": [args.nuv_lo, args.nuv_hi],
+                    **({"kernel_ms": kt} if kt else {})}), flush=True)
         cache.release()
 
 
