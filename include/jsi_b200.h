@@ -310,6 +310,14 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
 int jsi_batch_chunk(jsi_context *ctx, int chunk);
 /* Batch items re-run alone after an internal list overflowed (all lanes). */
 int jsi_batch_reruns(jsi_context *ctx, long long *out);
+/* Autotuner of the lockstep batches: times jsi_min_distance_batch on the n
+ * given queries (all of one shape) for chunk sizes 8, 16, 32, ... up to the
+ * per-lane share of n, with the lanes as configured, and keeps the fastest for
+ * queries of that shape (first-round nuv and degrees of both sides, k,
+ * rounds, precision); later batches of the shape use it.  chunk_out / ms_out
+ * (may be null) get the choice and its batch device time. */
+int jsi_autotune_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
+                       int *chunk_out, float *ms_out);
 /* Lockstep batches that repeat a shape, size and lane are captured once as a
  * CUDA graph and replayed.  enable: 1 on (default), 0 off, -1 unchanged;
  * replays (may be null) gets the replay count over all lanes. */

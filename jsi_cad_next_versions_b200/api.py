@@ -291,6 +291,19 @@ class Context:
         self._check(self.lib.jsi_batch_graphs(self.handle, flag, ctypes.byref(v)))
         return v.value
 
+    def autotune_batch(self, pairs, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
+                       precision: str | int = "v5_fp32", newton: bool = False) -> tuple[int, float]:
+        """Pick the lockstep chunk size for the shape of these queries (all of
+        one shape) by timing them; returns (chunk, batch device ms)."""
+        n = len(pairs)
+        p = self._dist_params(k, rounds, nuv_refine, precision, newton)
+        ta = (C.Task * n)(*[x[0] for x in pairs])
+        tb = (C.Task * n)(*[x[1] for x in pairs])
+        chunk, ms = ctypes.c_int(0), ctypes.c_float(0)
+        self._check(self.lib.jsi_autotune_batch(self.handle, n, ta, tb, ctypes.byref(p), ctypes.byref(chunk),
+                                                ctypes.byref(ms)))
+        return chunk.value, ms.value
+
     def batch_reruns(self) -> int:
         """Batch items re-run alone after an internal list overflowed."""
         v = ctypes.c_longlong(0)

@@ -319,6 +319,9 @@ struct jsi_context {
   cudaEvent_t ring_ev[kRingSegs] = {};
   cudaEvent_t upload_ev = nullptr;  // recorded after every upload (lanes wait on it)
   int batch_chunk = 64;  // queries per lockstep batch (0: one query per lane job)
+  // Chunk sizes chosen by jsi_autotune_batch per shape: first-round nuv and
+  // basis stride of both sides, k, rounds, precision.
+  std::map<std::array<int, 7>, int> tuned_chunk;
   bool batch_graphs = true;  // replay repeated lockstep batches as CUDA graphs
   std::string kernel_names;
   // worker pool
@@ -2911,6 +2914,66 @@ int jsi_batch_graphs(jsi_context *ctx, int enable, long long *replays) {
   return JSI_OK;
 }
 
+int jsi_autotune_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
+                       int *chunk_out, float *ms_out) {
+  if (!ctx || n < 1 || !a || !b) return JSI_ERR_INVALID;
+  if (ctx->lanes.empty()) return record(ctx, JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
+  jsi_dist_params p;
+  jsi_dist_params_default(&p);
+  if (params) p = *params;
+  std::array<int, 4> shape{};
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const int st = guarded(ctx, [&]() {
+      validate_dist(p, &a[0], &b[0]);
+      auto ia = ctx->surfaces.find(a[0].surface), ib = ctx->surfaces.find(b[0].surface);
+      if (ia == ctx->surfaces.end() || ib == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
+      shape = {a[0].nuv, b[0].nuv, p1_of(ia->second), p1_of(ib->second)};
+      for (int q = 1; q < n; ++q) {
+        auto qa = ctx->surfaces.find(a[q].surface), qb = ctx->surfaces.find(b[q].surface);
+        if (qa == ctx->surfaces.end() || qb == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
+        const std::array<int, 4> s2 = {a[q].nuv, b[q].nuv, p1_of(qa->second), p1_of(qb->second)};
+        if (s2 != shape) fail(JSI_ERR_INVALID, "autotune queries differ in shape");
+      }
+      return JSI_OK;
+    });
+    if (st != JSI_OK) return st;
+  }
+  const std::array<int, 7> key = {shape[0], shape[1], shape[2], shape[3], p.k, p.rounds, p.precision};
+  ctx->tuned_chunk.erase(key);
+  const int saved = ctx->batch_chunk;
+  std::vector<jsi_dist_result> out(n);
+  int best = saved > 0 ? saved : 64;
+  float best_ms = INFINITY;
+  // Candidates: powers of two up to the largest per-lane share of the batch.
+  const int nl = static_cast<int>(ctx->lanes.size());
+  const int most = std::max(1, (n + nl - 1) / nl);
+  for (int chunk = 8; chunk <= std::max(8, most); chunk *= 2) {
+    ctx->batch_chunk = chunk;
+    float ms = 0.0f;
+    int st = JSI_OK;
+    for (int rep = 0; rep < 3 && st == JSI_OK; ++rep) {  // one warm run, then the faster of two
+      std::memset(out.data(), 0, sizeof(jsi_dist_result) * out.size());
+      float t = 0.0f;
+      st = jsi_min_distance_batch(ctx, n, a, b, &p, out.data(), nullptr, &t);
+      if (rep == 1 || (rep == 2 && t < ms)) ms = t;
+    }
+    if (st != JSI_OK) {
+      ctx->batch_chunk = saved;
+      return st;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = chunk;
+    }
+  }
+  ctx->batch_chunk = saved;
+  ctx->tuned_chunk[key] = best;
+  if (chunk_out) *chunk_out = best;
+  if (ms_out) *ms_out = best_ms;
+  return JSI_OK;
+}
+
 int jsi_batch_reruns(jsi_context *ctx, long long *out) {
   if (!ctx || !out) return JSI_ERR_INVALID;
   long long t = 0;
@@ -2972,7 +3035,10 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
     const int nl = static_cast<int>(ctx->lanes.size());
     for (auto &g : groups) {
       const int m = static_cast<int>(g.second.size());
-      const int per = std::max(1, std::min(ctx->batch_chunk, (m + nl - 1) / nl));
+      const std::array<int, 7> tk = {g.first[0], g.first[1], g.first[2], g.first[3], p.k, p.rounds, p.precision};
+      auto tit = ctx->tuned_chunk.find(tk);
+      const int chunk = tit != ctx->tuned_chunk.end() ? tit->second : ctx->batch_chunk;
+      const int per = std::max(1, std::min(chunk, (m + nl - 1) / nl));
       for (int s0 = 0; s0 < m; s0 += per) {
         auto job = std::make_shared<Job>();
         job->kind = 2;

@@ -220,3 +220,21 @@ def test_batch_graph_replay(precision):
         for res in runs:
             for r, a in zip(res, eager):
                 _same(r, a, newton=True)
+
+
+def test_autotune_batch():
+    """The autotuner picks a chunk among its candidates for the shape and
+    later batches of that shape use it; results do not change."""
+    import jsi_cad_next_versions_b200 as J
+    with J.Context(0) as ctx:
+        tasks = _upload_pairs(ctx, _hard_wave_pairs(24, seed0=1400), 128)
+        ctx.workers(2)
+        try:
+            before, _ = ctx.min_distance_batch(tasks, precision="fp32_screen", trace=True)
+            chunk, ms = ctx.autotune_batch(tasks, precision="fp32_screen")
+            after, _ = ctx.min_distance_batch(tasks, precision="fp32_screen", trace=True)
+        finally:
+            ctx.workers(0)
+        assert chunk in (8, 16) and ms > 0  # 24 queries over 2 lanes: candidates 8 and 16
+        for r, a in zip(after, before):
+            _same(r, a)
