@@ -2416,10 +2416,12 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
 constexpr int kBandTiles = 32;
 constexpr int kBandCols = kBandTiles * kMaxTile + 1;
 constexpr int kBandThreads = 288;  // one thread per sample column (257) in one pass
+constexpr int kBandNetCols = 96;   // control-net columns a band's net tile holds
+constexpr int kBandNetRows = 6;    // net rows of the tile (D + 3 for D = 3)
 
 template <typename TC>
 constexpr size_t band_smem() {
-  return sizeof(Vec4<TC>) * (kMaxTile + 1) * kBandCols;
+  return sizeof(Vec4<TC>) * ((kMaxTile + 1) * kBandCols + kBandNetRows * kBandNetCols);
 }
 
 template <typename TB, typename TC, int D>
@@ -2428,8 +2430,12 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
   constexpr int kE = kMaxTile + 1;
   constexpr int kP = D + 1;          // u basis values held per thread
   constexpr int kBandRows = D + 3;   // net rows held per thread
+  static_assert(kBandRows <= kBandNetRows, "net tile rows");
   extern __shared__ __align__(16) unsigned char band_raw[];
   Vec4<TC> *S = reinterpret_cast<Vec4<TC> *>(band_raw);  // [kE][kBandCols]
+  // The band's control-net tile: rows rmin.., columns cu0.. of the net.
+  Vec4<TC> *NT = S + kE * kBandCols;                      // [kBandNetRows][kBandNetCols]
+  __shared__ int s_su[2];
   __shared__ TC snv[kE][kBandRows];
   // v coefficients of each sample row over the band's net rows, zero outside
   // the row's degv + 1 window: adding 0 * (finite row sum) to an accumulator
@@ -2465,6 +2471,10 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
         else snv[tid][c] = __double2float_rn(N[c]);
       }
     }
+    // Spans are monotone along the band's sample columns: the first and last
+    // give the net columns the band reads.
+    if (fit && tid == 32) s_su[0] = bs.spans[lu0];
+    if (fit && tid == 64) s_su[1] = bs.spans[lu0 + ncols - 1];
     __syncthreads();
     int rmin = 0, nrows = kBandRows + 1;
     if (fit) {
@@ -2481,6 +2491,18 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
       const int a = tid / kBandRows, R = tid - (tid / kBandRows) * kBandRows;
       const int R0 = ssv[a] - s.degv - rmin;
       coef[a][R] = (R >= R0 && R - R0 <= s.degv) ? snv[a][R - R0] : TC(0);
+    }
+    int cu0 = 0, ncu = kBandNetCols + 1;
+    if (factored) {
+      cu0 = min(s_su[0], s_su[1]) - s.degu;
+      ncu = max(s_su[0], s_su[1]) + 1 - cu0;
+    }
+    const bool tiled = factored && ncu <= kBandNetCols;
+    if (tiled) {
+      for (int e = tid; e < nrows * ncu; e += blockDim.x) {
+        const int R = e / ncu, cc = e - (e / ncu) * ncu;
+        NT[R * kBandNetCols + cc] = s.cpw[static_cast<long long>(s.ncpu) * (rmin + R) + cu0 + cc];
+      }
     }
     __syncthreads();
     for (int col = tid; col < ncols; col += blockDim.x) {
@@ -2501,7 +2523,8 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
         for (int R = 0; R < kBandRows; ++R) {
           TC r0 = TC(0), r1 = TC(0), r2 = TC(0), r3 = TC(0);
           if (R < nrows) {
-            const Vec4<TC> *cp = s.cpw + static_cast<long long>(s.ncpu) * (rmin + R) + (su - s.degu);
+            const Vec4<TC> *cp = tiled ? NT + R * kBandNetCols + (su - s.degu - cu0)
+                                       : s.cpw + static_cast<long long>(s.ncpu) * (rmin + R) + (su - s.degu);
 #pragma unroll
             for (int c = 0; c < kP; ++c) {
               if (c <= s.degu) {
