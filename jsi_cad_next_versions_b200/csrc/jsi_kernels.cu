@@ -2449,7 +2449,10 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
   out = qsh(out, qo);
   const Geom g = out.g;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int te = g.te, te2 = te * te, p1 = g.p1max;
+  // Large grids only (tw >= 16, so te = kMaxTile): the tile edge is a
+  // compile-time constant and cell indices are shifts and masks.
+  constexpr int te = kMaxTile, te2 = kMaxTile * kMaxTile;
+  const int p1 = g.p1max;
   const int nch = (g.tw + kBandTiles - 1) / kBandTiles;
   const long long nunits = static_cast<long long>(nreg_of(bs)) * g.tw * nch;
   for (long long unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
@@ -3363,7 +3366,7 @@ void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const Si
                         const Batch &bt, const SurfView<TC> *vdev) {
   counted();
   const Geom &g = out.g;
-  if (g.tw >= 16 && s.degu <= 3 && s.degv <= 3) {
+  if (g.tw >= 16 && g.te == kMaxTile && s.degu <= 3 && s.degv <= 3) {
     // Large grids of bicubic-or-lower surfaces (degrees are part of a batch's
     // shape): whole bands per block.
     constexpr size_t smem = band_smem<TC>();
