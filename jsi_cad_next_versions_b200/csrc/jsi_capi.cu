@@ -1147,8 +1147,10 @@ SideRound<T> slab_side(SlabPlan &sp, const Geom &g, int nreg, RegionRec<T> *regi
     s.thi = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.ntiles);
   }
   if (super) {
-    s.stlo = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nst);
-    s.sthi = sp.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nst);
+    // Folded by the cell kernels (initialised before them: minima all ones,
+    // maxima zero, see batch_fold_init).
+    s.stmin = sp.get<typename OrdBits<T>::type>(static_cast<size_t>(nreg) * g.nst * 4);
+    s.stmax = sp.get<typename OrdBits<T>::type>(static_cast<size_t>(nreg) * g.nst * 4);
   }
   return s;
 }
@@ -1266,6 +1268,16 @@ BatchLayout<TP, TC> plan_batch(char *base, int nuv1, int nuv2, int p1a, int p1b,
   return L;
 }
 
+// Supertile accumulators of the batch's sides set to their identities before
+// the cell kernels fold into them (one strided memset per array).
+template <typename T>
+void batch_fold_init(const SideRound<T> &S, cudaStream_t st, const Batch &bt) {
+  if (!S.stmin) return;
+  const size_t bytes = static_cast<size_t>(S.nreg) * S.g.nst * 4 * sizeof(typename OrdBits<T>::type);
+  JSI_CUDA(cudaMemset2DAsync(S.stmin, static_cast<size_t>(bt.qs), 0xff, bytes, bt.n, st));
+  JSI_CUDA(cudaMemset2DAsync(S.stmax, static_cast<size_t>(bt.qs), 0x00, bytes, bt.n, st));
+}
+
 // Screening stages of one batched round over sides of precision T.
 template <typename T, typename TP, typename TC>
 void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, const SideRound<T> &Y,
@@ -1273,10 +1285,6 @@ void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, c
   cudaStream_t st = L->stream;
   const int ns = R.max_slots == 1 ? 1 : -R.max_slots;
   if (R.super) {
-    timed(L, "supertiles", [&] {
-      launch_supertiles(X, st, bt);
-      launch_supertiles(Y, st, bt);
-    });
     timed(L, "dist_tau", [&] { launch_dist_tau_st(X, Y, R.map1, R.map2, ns, k, stats, screen, e, st, bt); });
     timed(L, "dist_cull", [&] {
       launch_dist_cull_st(X, Y, R.map1, R.map2, ns, R.st_surv, R.st_cap, stats, screen, e, st, bt);
@@ -1385,6 +1393,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       const double cells_units = r == 1 ? double(n) * (double(Rd.A.g.W) * Rd.A.g.W + double(Rd.B.g.W) * Rd.B.g.W) : 0.0;
       const char *cells_name = r == 1 ? "cells_r1" : "cells";
       if (!scr) {
+        batch_fold_init(Rd.A, st, bt);
+        batch_fold_init(Rd.B, st, bt);
         timed(L, cells_name, [&] {
           launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0));
           launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1));
@@ -1394,6 +1404,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
           launch_dist_select(static_cast<const DistCand<TP> *>(Rd.cand), Rd.cand_cap, p.k, Rd.top, stats, st, bt);
         });
       } else if constexpr (kScreen) {
+        batch_fold_init(Rd.A32, st, bt);
+        batch_fold_init(Rd.B32, st, bt);
         timed(L, cells_name, [&] {
           launch_cells_fused(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
           launch_cells_fused(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);

@@ -43,6 +43,20 @@ struct SurfView {
   const Vec4<T> *cpw;
 };
 
+// Unsigned encodings that order like the float / double they encode
+// (non-negative: bits with the sign bit set; negative: complemented bits), so
+// integer atomicMin / atomicMax compute exact float minima / maxima.
+template <typename T>
+struct OrdBits;
+template <>
+struct OrdBits<float> {
+  using type = unsigned;
+};
+template <>
+struct OrdBits<double> {
+  using type = unsigned long long;
+};
+
 template <typename T>
 struct RegionRec {
   T u0, v0, u1, v1;
@@ -95,6 +109,11 @@ struct SideRound {
   Vec4<T> *stlo;  // supertile bounds [R][nst] (built on demand)
   Vec4<T> *sthi;
   const int *dnreg;  // when set: the region count lives on the device (batched rounds)
+  // When set (batched rounds): supertile bounds folded in by the cell
+  // kernels as encoded [R][nst][4] minima / maxima (OrdBits), used in place
+  // of stlo / sthi.
+  typename OrdBits<T>::type *stmin;
+  typename OrdBits<T>::type *stmax;
 };
 
 // Candidate of the distance screen.

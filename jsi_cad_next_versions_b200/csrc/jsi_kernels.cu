@@ -109,7 +109,50 @@ __device__ __forceinline__ SideRound<T> qsh(SideRound<T> s, long long off) {
   s.stlo = qsh(s.stlo, off);
   s.sthi = qsh(s.sthi, off);
   s.dnreg = qsh(s.dnreg, off);
+  s.stmin = qsh(s.stmin, off);
+  s.stmax = qsh(s.stmax, off);
   return s;
+}
+
+__device__ __forceinline__ unsigned ord_enc(float x) {
+  const unsigned b = __float_as_uint(x);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_dec(unsigned e) {
+  return __uint_as_float((e & 0x80000000u) ? (e & 0x7fffffffu) : ~e);
+}
+__device__ __forceinline__ unsigned long long ord_enc(double x) {
+  const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+  return (b >> 63) ? ~b : (b | (1ull << 63));
+}
+__device__ __forceinline__ double ord_dec(unsigned long long e) {
+  return __longlong_as_double(static_cast<long long>((e >> 63) ? (e & ~(1ull << 63)) : ~e));
+}
+
+// Supertile bounds of entry i: decoded from the folded minima / maxima when
+// the side carries them, else the stored vectors.
+template <typename T>
+__device__ __forceinline__ void st_bounds(const SideRound<T> &s, long long i, Vec4<T> &lo, Vec4<T> &hi) {
+  if (s.stmin) {
+    const typename OrdBits<T>::type *mn = s.stmin + i * 4, *mx = s.stmax + i * 4;
+    lo = Vec4<T>{ord_dec(mn[0]), ord_dec(mn[1]), ord_dec(mn[2]), T(0)};
+    hi = Vec4<T>{ord_dec(mx[0]), ord_dec(mx[1]), ord_dec(mx[2]), T(0)};
+  } else {
+    lo = s.stlo[i];
+    hi = s.sthi[i];
+  }
+}
+
+// Folds a tile's centre range into its supertile's bounds (batched rounds).
+template <typename T>
+__device__ __forceinline__ void fold_supertile(const SideRound<T> &s, int r, int ty, int tx, const T lo[3],
+                                               const T hi[3]) {
+  const long long st = static_cast<long long>(r) * s.g.nst + (ty / kMaxTile) * s.g.stw + tx / kMaxTile;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    atomicMin(s.stmin + st * 4 + c, ord_enc(lo[c]));
+    atomicMax(s.stmax + st * 4 + c, ord_enc(hi[c]));
+  }
 }
 
 // Region count of a side: on the device in batched refinement rounds.
@@ -1115,13 +1158,16 @@ __global__ void k_dist_cull_st(SideRound<T> a, SideRound<T> b, const int *map1, 
   for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
     const int slot = row / g1.nst, s1 = row - slot * g1.nst;
     const long long i1 = static_cast<long long>(map1[slot]) * g1.nst + s1;
-    const Vec4<T> lo1 = a.stlo[i1], hi1 = a.sthi[i1];
+    Vec4<T> lo1, hi1;
+    st_bounds(a, i1, lo1, hi1);
     const long long base2 = static_cast<long long>(map2[slot]) * g2.nst;
     for (int s0 = 0; s0 < g2.nst; s0 += blockDim.x) {
       const int s2 = s0 + threadIdx.x;
       bool keep = false;
       if (s2 < g2.nst) {
-        T lb = tile_lb(lo1, hi1, b.stlo[base2 + s2], b.sthi[base2 + s2]);
+        Vec4<T> lo2, hi2;
+        st_bounds(b, base2 + s2, lo2, hi2);
+        T lb = tile_lb(lo1, hi1, lo2, hi2);
         if constexpr (S) lb = __fmul_rd(lb, 1.0f - 0x1p-19f);
         keep = lb <= tau;
       }
@@ -1197,7 +1243,9 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
           const int t = ty * g1.tw + tx;
           const long long i1 = static_cast<long long>(r1) * g1.ntiles + t;
           const long long j2 = static_cast<long long>(r2) * g2.nst + s2;
-          if (shaved_lb<T, S>(a.tlo[i1], a.thi[i1], b.stlo[j2], b.sthi[j2]) <= tau) s_t1[atomicAdd(&s_n1, 1)] = t;
+          Vec4<T> slo, shi;
+          st_bounds(b, j2, slo, shi);
+          if (shaved_lb<T, S>(a.tlo[i1], a.thi[i1], slo, shi) <= tau) s_t1[atomicAdd(&s_n1, 1)] = t;
         }
       } else {
         const int ty = sy2 * kMaxTile + (l >> 3), tx = sx2 * kMaxTile + (l & 7);
@@ -1205,7 +1253,9 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
           const int t = ty * g2.tw + tx;
           const long long i2 = static_cast<long long>(r2) * g2.ntiles + t;
           const long long j1 = static_cast<long long>(r1) * g1.nst + s1;
-          if (shaved_lb<T, S>(a.stlo[j1], a.sthi[j1], b.tlo[i2], b.thi[i2]) <= tau) s_t2[atomicAdd(&s_n2, 1)] = t;
+          Vec4<T> slo, shi;
+          st_bounds(a, j1, slo, shi);
+          if (shaved_lb<T, S>(slo, shi, b.tlo[i2], b.thi[i2]) <= tau) s_t2[atomicAdd(&s_n2, 1)] = t;
         }
       }
     }
@@ -2393,6 +2443,7 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
     if (lane == 0) {
       out.tlo[t] = Vec4<TC>{lo[0], lo[1], lo[2], TC(0)};
       out.thi[t] = Vec4<TC>{hi[0], hi[1], hi[2], TC(0)};
+      if (out.stmin) fold_supertile(out, r, ty, tx, lo, hi);
     }
     __syncwarp();
   }
@@ -2659,6 +2710,7 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
       if (lane == 0) {
         out.tlo[t] = Vec4<TC>{lo[0], lo[1], lo[2], TC(0)};
         out.thi[t] = Vec4<TC>{hi[0], hi[1], hi[2], TC(0)};
+        if (out.stmin) fold_supertile(out, r, ty, tx, lo, hi);
       }
     }
     __syncthreads();
