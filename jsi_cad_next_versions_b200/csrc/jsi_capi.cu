@@ -433,16 +433,49 @@ void surface_header(SurfaceRec &s, const int ivec[7], const float *data) {
   s.dv = std::min(2, ivec[4]);
   const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
   const float *cp = data + ivec[3] + ivec[6];
-  if (s.rat && ncp > 0) s.wmin = s.wmax = cp[3 * ncp];
+  // Branch-free loops in float (|x| and max are exact, and so is the
+  // conversion to double); the weighted products of two floats are exact in
+  // double.
+  float m[3] = {0.0f, 0.0f, 0.0f};
   for (size_t q = 0; q < ncp; ++q) {
-    const float w = s.rat ? cp[3 * ncp + q] : 1.0f;
-    for (int c = 0; c < 3; ++c) {
-      s.cmax[c] = std::max(s.cmax[c], std::fabs(static_cast<double>(cp[3 * q + c])));
-      s.wcmax[c] = std::max(s.wcmax[c], std::fabs(static_cast<double>(w) * cp[3 * q + c]));
-    }
-    s.wmin = std::min(s.wmin, static_cast<double>(w));
-    s.wmax = std::max(s.wmax, static_cast<double>(w));
+    m[0] = std::max(m[0], std::fabs(cp[3 * q]));
+    m[1] = std::max(m[1], std::fabs(cp[3 * q + 1]));
+    m[2] = std::max(m[2], std::fabs(cp[3 * q + 2]));
   }
+  for (int c = 0; c < 3; ++c) s.cmax[c] = s.wcmax[c] = m[c];
+  s.wmin = s.wmax = 1.0;
+  if (s.rat && ncp > 0) {
+    const float *w = cp + 3 * ncp;
+    float lo = w[0], hi = w[0];
+    double wm[3] = {0.0, 0.0, 0.0};
+    for (size_t q = 0; q < ncp; ++q) {
+      lo = std::min(lo, w[q]);
+      hi = std::max(hi, w[q]);
+      for (int c = 0; c < 3; ++c)
+        wm[c] = std::max(wm[c], std::fabs(static_cast<double>(w[q]) * static_cast<double>(cp[3 * q + c])));
+    }
+    s.wmin = lo;
+    s.wmax = hi;
+    for (int c = 0; c < 3; ++c) s.wcmax[c] = wm[c];
+  }
+}
+
+// Runs fn(q) for q in [0, n) on up to 8 host threads (the upload path's
+// per-surface host work).
+template <typename Fn>
+void parallel_for(size_t n, Fn &&fn) {
+  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>({hw, size_t(8), (n + 63) / 64});
+  if (nt <= 1) {
+    for (size_t q = 0; q < n; ++q) fn(q);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (size_t t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (size_t q = t; q < n; q += nt) fn(q);
+    });
+  for (auto &th : pool) th.join();
 }
 
 SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
@@ -509,10 +542,8 @@ struct PendingSurface {
   int ndata;
 };
 
-SurfaceRec make_block(jsi_context *ctx, const int ivec[7], const float *data, int ndata, SurfacePrep *job) {
-  check_surface(ivec, data, ndata);
-  SurfaceRec s;
-  surface_header(s, ivec, data);
+SurfaceRec make_block(jsi_context *ctx, const SurfaceRec &head, const int ivec[7], int ndata, SurfacePrep *job) {
+  SurfaceRec s = head;
   const int nku = ivec[3], nkv = ivec[6];
   const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
@@ -550,6 +581,19 @@ SurfaceRec make_block(jsi_context *ctx, const int ivec[7], const float *data, in
 void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &in, std::vector<SurfaceRec> &out) {
   Lane *L = &ctx->main;
   cudaStream_t st = L->stream;
+  // Checks and magnitudes of every surface, on host threads.
+  std::vector<SurfaceRec> heads(in.size());
+  std::vector<char> bad(in.size(), 0);
+  parallel_for(in.size(), [&](size_t q) {
+    try {
+      check_surface(in[q].ivec, in[q].data, in[q].ndata);
+      surface_header(heads[q], in[q].ivec, in[q].data);
+    } catch (...) {
+      bad[q] = 1;
+    }
+  });
+  for (size_t q = 0; q < in.size(); ++q)
+    if (bad[q]) check_surface(in[q].ivec, in[q].data, in[q].ndata);  // throws again, on this thread
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   auto next_segment = [&]() {
     JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
@@ -563,7 +607,7 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
     if (rec_b + al(sizeof(SurfacePrep)) > kRingSeg) {
       // Larger than a segment: its own device staging, completed here.
       SurfacePrep job;
-      out.push_back(make_block(ctx, in[q].ivec, in[q].data, in[q].ndata, &job));
+      out.push_back(make_block(ctx, heads[q], in[q].ivec, in[q].ndata, &job));
       char *tmp = nullptr;
       if (cudaMalloc(&tmp, rec_b + al(sizeof(SurfacePrep))) != cudaSuccess) {
         cudaGetLastError();
@@ -585,19 +629,24 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
     const size_t seg0 = static_cast<size_t>(ctx->ring_cur) * kRingSeg;
     size_t off = ctx->ring_off;
     std::vector<SurfacePrep> jobs;
+    std::vector<std::pair<size_t, size_t>> copies;  // (surface, ring offset)
     long long most = 0;
     while (q < in.size()) {
       const size_t rb = al(static_cast<size_t>(in[q].ndata) * sizeof(float));
       if (off + rb + al(sizeof(SurfacePrep) * (jobs.size() + 1)) > kRingSeg) break;
       SurfacePrep job;
-      out.push_back(make_block(ctx, in[q].ivec, in[q].data, in[q].ndata, &job));
-      std::memcpy(ctx->ring + seg0 + off, in[q].data, static_cast<size_t>(in[q].ndata) * sizeof(float));
+      out.push_back(make_block(ctx, heads[q], in[q].ivec, in[q].ndata, &job));
+      copies.push_back({q, off});
       job.src = reinterpret_cast<const float *>(ctx->dring + seg0 + off);
       most = std::max(most, std::max(job.ndata, job.ncp));
       jobs.push_back(job);
       off += rb;
       ++q;
     }
+    parallel_for(copies.size(), [&](size_t e) {
+      const PendingSurface &ps = in[copies[e].first];
+      std::memcpy(ctx->ring + seg0 + copies[e].second, ps.data, static_cast<size_t>(ps.ndata) * sizeof(float));
+    });
     const size_t jobs_b = sizeof(SurfacePrep) * jobs.size();
     std::memcpy(ctx->ring + seg0 + off, jobs.data(), jobs_b);
     const size_t start = ctx->ring_off;
