@@ -72,7 +72,10 @@ UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "cells
 # DRAM traffic per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / its units), for the form it was captured in:
 # profiles/k_cells_band_hardwave_n512.md (FP32 screen, 128 x 511^2 cells).
-MEASURED_TRAFFIC = {("cells_r1", "fp32_screen"): 15.44}
+MEASURED_TRAFFIC = {("cells_r1", "fp32_screen"): 16.17}
+# What one timed "launch" of a kernel name covers.
+LAUNCH_NOTE = {"cells_r1": "the first round's cell build of one batch: one k_cells_band launch per side, "
+                           "back to back on one stream, timed together"}
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 74.4: 148 SMs x 128 lanes x FMA x 1.965 GHz
 NOMINAL_FP64_TFLOPS = NOMINAL_FP32_TFLOPS / 2
 
@@ -97,6 +100,7 @@ def roofline(kernel, kt, form, peaks):
             "frac": gbs / hbm_peak, "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled by units)",
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
             "avg_launch_ms": avg_s * 1e3, "units_per_launch": per_launch_units,
+            "launch": LAUNCH_NOTE.get(kernel, "one kernel launch"),
             "compute": {"achieved": tflops, "peak": fp_peak, "unit": "TFLOP/s", "frac": tflops / fp_peak,
                         "peak_source": "nominal CUDA-core peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz; FP64 half)"}}
 
@@ -338,7 +342,9 @@ def run_ours(args):
         launches = ctx.launch_count() - launches0
         reruns = ctx.batch_reruns() - reruns0
         # Per-kernel breakdown in separate steps (events around every launch
-        # would perturb the timed steps above).
+        # would perturb the timed steps above), on one lane: with several
+        # lanes a launch's events would also span the other lanes' kernels.
+        ctx.workers(1)
         ctx.kernel_timing(True)
         for _ in range(args.steps):
             flush.zero_()
@@ -346,6 +352,7 @@ def run_ours(args):
             step()
         ktimes = ctx.kernel_times()
         ctx.kernel_timing(False)
+        ctx.workers(args.lanes)
         clk.__exit__(None, None, None)
         total_ms = sum(step_ms)
         results[form] = {
