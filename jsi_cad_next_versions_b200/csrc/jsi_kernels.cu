@@ -2467,6 +2467,7 @@ __global__ void __launch_bounds__(128) k_cells_fused(SurfView<TC> s, const SurfV
 constexpr int kBandTiles = 32;
 constexpr int kBandCols = kBandTiles * kMaxTile + 1;
 constexpr int kBandThreads = 288;  // one thread per sample column (257) in one pass
+static_assert(kBandThreads == kBandTiles * kMaxTile + 32, "band cells: 8 warps of cell columns + 1 warp");
 constexpr int kBandNetCols = 96;   // control-net columns a band's net tile holds
 constexpr int kBandNetRows = 6;    // net rows of the tile (D + 3 for D = 3)
 
@@ -2475,8 +2476,206 @@ constexpr size_t band_smem() {
   return sizeof(Vec4<TC>) * ((kMaxTile + 1) * kBandCols + kBandNetRows * kBandNetCols);
 }
 
+// Arithmetic of the factored band evaluation, one helper per step, with the
+// operation sequence of eval_point (TB == TC) or screen_point (TB = double,
+// TC = float) for a net row's u sum, a sample's v accumulation and the
+// rational quotient.
+template <typename TB, typename TC, bool RAT>
+__device__ __forceinline__ void band_row_sum(TC n, const Vec4<TC> &q, TC (&r)[4]) {
+  if constexpr (std::is_same<TB, TC>::value) {
+    if constexpr (!RAT) {
+      r[0] += n * q.x;
+      r[1] += n * q.y;
+      r[2] += n * q.z;
+    } else {
+      const TC nw = n * q.w;
+      r[0] += nw * q.x;
+      r[1] += nw * q.y;
+      r[2] += nw * q.z;
+      r[3] += nw;
+    }
+  } else {
+    float m = n;
+    if constexpr (RAT) {
+      m = __fmul_rn(m, q.w);
+      r[3] = __fadd_rn(r[3], m);
+    }
+    r[0] = __fmaf_rn(m, q.x, r[0]);
+    r[1] = __fmaf_rn(m, q.y, r[1]);
+    r[2] = __fmaf_rn(m, q.z, r[2]);
+  }
+}
+
+template <typename TB, typename TC, bool RAT>
+__device__ __forceinline__ void band_v_acc(TC m, const TC (&rs)[4], TC (&a)[4]) {
+  if constexpr (std::is_same<TB, TC>::value) {
+    a[0] += m * rs[0];
+    a[1] += m * rs[1];
+    a[2] += m * rs[2];
+    if constexpr (RAT) a[3] += m * rs[3];
+  } else {
+    a[0] = __fmaf_rn(m, rs[0], a[0]);
+    a[1] = __fmaf_rn(m, rs[1], a[1]);
+    a[2] = __fmaf_rn(m, rs[2], a[2]);
+    if constexpr (RAT) a[3] = __fmaf_rn(m, rs[3], a[3]);
+  }
+}
+
+template <typename TB, typename TC, bool RAT>
+__device__ __forceinline__ Vec4<TC> band_point(const TC (&a)[4]) {
+  Vec4<TC> P{a[0], a[1], a[2], TC(0)};
+  if constexpr (RAT) {
+    if constexpr (std::is_same<TB, TC>::value) {
+      const TC inv = TC(1) / a[3];
+      P.x = a[0] * inv;
+      P.y = a[1] * inv;
+      P.z = a[2] * inv;
+    } else {
+      const double w = static_cast<double>(a[3]);
+      P.x = __double2float_rn(static_cast<double>(a[0]) / w);
+      P.y = __double2float_rn(static_cast<double>(a[1]) / w);
+      P.z = __double2float_rn(static_cast<double>(a[2]) / w);
+    }
+  }
+  return P;
+}
+
+// One band unit of k_cells_band when both degrees equal D and the band's
+// control-net tile (NR rows, rows past the band's own zero-filled) sits in
+// shared memory.  Every predicate of the general loop is a compile-time
+// constant here.
+//
+// Samples: threads 0..255 own sample columns 0..255 (all rows of the band);
+// the last column (256) goes to warp 8, one lane per sample row, each lane
+// forming the column's row sums itself (the same operations, so the same
+// bits).  Cells: thread c owns cell column c of the chunk (tile c / 8,
+// column c % 8 of it) and walks its te cell rows, carrying the previous
+// sample row's pairwise min/max, so a cell costs two shared loads.  The
+// tile range is an 8-lane reduction.  min/max are exact and, with fminf /
+// fmaxf, independent of order (NaNs are skipped, and the sign of a zero
+// extreme is erased by the centre's trailing + 0, which also keeps every
+// centre off -0), so the centres and ranges carry the general loop's bits.
+template <typename TB, typename TC, int D, int NR, bool RAT>
+__device__ __forceinline__ void band_unit_fast(const SurfView<TC> &s, const SideRound<TB> &bs,
+                                               const SideRound<TC> &out, Vec4<TC> *S, const Vec4<TC> *NT,
+                                               const TC (*coef)[8], int r, int ty, int tx0, int ntx, int nv,
+                                               int ncols, long long lu0, int cu0) {
+  constexpr int kP = D + 1;
+  constexpr int te = kMaxTile, te2 = kMaxTile * kMaxTile;
+  constexpr int kCols = kBandTiles * kMaxTile;  // 256 cell columns, 257 sample columns
+  const Geom g = out.g;
+  const int p1 = g.p1max;
+  const int tid = threadIdx.x;
+  int col, a0, a1;
+  if (tid < kCols) {
+    col = tid;
+    a0 = 0;
+    a1 = nv;
+  } else {
+    col = kCols;
+    a0 = a1 = tid - kCols;
+    if (a0 > nv) col = ncols;  // idle lane
+  }
+  if (col < ncols) {
+    const long long lu = lu0 + col;
+    const int su = bs.spans[lu];
+    const TB *Nb = bs.basis + lu * 3 * p1;
+    TC Nu[kP];
+#pragma unroll
+    for (int c = 0; c < kP; ++c) {
+      if constexpr (std::is_same<TB, TC>::value) Nu[c] = Nb[c];
+      else Nu[c] = __double2float_rn(Nb[c]);
+    }
+    TC rs[NR][4];
+    const Vec4<TC> *cp = NT + (su - D - cu0);
+#pragma unroll
+    for (int R = 0; R < NR; ++R) {
+      TC acc[4] = {TC(0), TC(0), TC(0), TC(0)};
+#pragma unroll
+      for (int c = 0; c < kP; ++c) band_row_sum<TB, TC, RAT>(Nu[c], cp[R * kBandNetCols + c], acc);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) rs[R][k] = acc[k];
+    }
+    for (int a = a0; a <= a1; ++a) {
+      TC m[NR];
+      if constexpr (sizeof(TC) == 4) {
+        const float4 v0 = *reinterpret_cast<const float4 *>(&coef[a][0]);
+        m[0] = v0.x;
+        m[1] = v0.y;
+        m[2] = v0.z;
+        m[3] = v0.w;
+        if constexpr (NR > 4) {
+          const float2 v1 = *reinterpret_cast<const float2 *>(&coef[a][4]);
+          m[4] = v1.x;
+          if constexpr (NR > 5) m[5] = v1.y;
+        }
+      } else {
+#pragma unroll
+        for (int R = 0; R < NR; ++R) m[R] = coef[a][R];
+      }
+      TC acc[4] = {TC(0), TC(0), TC(0), TC(0)};
+#pragma unroll
+      for (int R = 0; R < NR; ++R) band_v_acc<TB, TC, RAT>(m[R], rs[R], acc);
+      S[a * kBandCols + col] = band_point<TB, TC, RAT>(acc);
+    }
+  }
+  __syncthreads();
+  if (tid >= kCols) return;  // warp 8: no cells (a whole warp, so the shuffles below stay converged)
+  const int j = tid >> 3, b = tid & 7;
+  const bool act = j < ntx;
+  TC tlo[3] = {pos_inf<TC>(), pos_inf<TC>(), pos_inf<TC>()};
+  TC thi[3] = {-pos_inf<TC>(), -pos_inf<TC>(), -pos_inf<TC>()};
+  const int tx = tx0 + j;
+  const long long t = static_cast<long long>(r) * g.ntiles + static_cast<long long>(ty) * g.tw + tx;
+  if (act) {
+    const bool colok = b < min(te, g.W - tx * te);
+    Vec4<TC> p = S[tid], q = S[tid + 1];
+    TC pmn[3] = {fmn(p.x, q.x), fmn(p.y, q.y), fmn(p.z, q.z)};
+    TC pmx[3] = {fmx(p.x, q.x), fmx(p.y, q.y), fmx(p.z, q.z)};
+    Vec4<TC> *dst = out.center + t * te2 + b;
+#pragma unroll
+    for (int a = 0; a < te; ++a) {
+      p = S[(a + 1) * kBandCols + tid];
+      q = S[(a + 1) * kBandCols + tid + 1];
+      const TC nmn[3] = {fmn(p.x, q.x), fmn(p.y, q.y), fmn(p.z, q.z)};
+      const TC nmx[3] = {fmx(p.x, q.x), fmx(p.y, q.y), fmx(p.z, q.z)};
+      Vec4<TC> cen{TC(0), TC(0), TC(0), TC(0)};
+      if (a < nv && colok) {
+        TC c3[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const TC lo = fmn(pmn[k], nmn[k]), hi = fmx(pmx[k], nmx[k]);
+          c3[k] = (lo - TC(0) + hi + TC(0)) * TC(0.5);  // = / 2 exactly
+          tlo[k] = fmn(tlo[k], c3[k]);
+          thi[k] = fmx(thi[k], c3[k]);
+        }
+        cen = Vec4<TC>{c3[0], c3[1], c3[2], TC(0)};
+      }
+      dst[a * te] = cen;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        pmn[k] = nmn[k];
+        pmx[k] = nmx[k];
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < te; o <<= 1) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      tlo[k] = fmn(tlo[k], __shfl_xor_sync(kFull, tlo[k], o));
+      thi[k] = fmx(thi[k], __shfl_xor_sync(kFull, thi[k], o));
+    }
+  }
+  if (act && b == 0) {
+    out.tlo[t] = Vec4<TC>{tlo[0], tlo[1], tlo[2], TC(0)};
+    out.thi[t] = Vec4<TC>{thi[0], thi[1], thi[2], TC(0)};
+    if (out.stmin) fold_supertile(out, r, ty, tx, tlo, thi);
+  }
+}
+
 template <typename TB, typename TC, int D>
-__global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells_band(SurfView<TC> s, const SurfView<TC> *vdev,
+__global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 4) k_cells_band(SurfView<TC> s, const SurfView<TC> *vdev,
                                                               SideRound<TB> bs, SideRound<TC> out, long long qs) {
   constexpr int kE = kMaxTile + 1;
   constexpr int kP = D + 1;          // u basis values held per thread
@@ -2492,7 +2691,7 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
   // the row's degv + 1 window: adding 0 * (finite row sum) to an accumulator
   // that starts at +0 (and so is never -0) leaves it unchanged, so the padded
   // sum has the bits of the windowed one.
-  __shared__ TC coef[kE][kBandRows];
+  __shared__ __align__(16) TC coef[kE][8];
   __shared__ int ssv[kE];
   const long long qo = qoff(qs);
   if (vdev) s = *qsh(vdev, qo);
@@ -2505,11 +2704,15 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
   constexpr int te = kMaxTile, te2 = kMaxTile * kMaxTile;
   const int p1 = g.p1max;
   const int nch = (g.tw + kBandTiles - 1) / kBandTiles;
-  const long long nunits = static_cast<long long>(nreg_of(bs)) * g.tw * nch;
-  for (long long unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
-    const int r = static_cast<int>(unit / (static_cast<long long>(g.tw) * nch));
-    const int rest = static_cast<int>(unit - static_cast<long long>(r) * g.tw * nch);
-    const int ty = rest / nch, ch = rest - (rest / nch) * nch;
+  // Units per side: regions x tw x nch, far below 2^31 (32-bit index
+  // arithmetic; a 64-bit division per unit would cost every thread ~100
+  // instructions).
+  const int per_reg = g.tw * nch;
+  const int nunits = nreg_of(bs) * per_reg;
+  for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+    const int r = unit / per_reg;
+    const int rest = unit - r * per_reg;
+    const int ty = rest / nch, ch = rest - ty * nch;
     const int tx0 = ch * kBandTiles, ntx = min(kBandTiles, g.tw - tx0);
     const int nv = min(te, g.W - ty * te);
     const int nuc = min(ntx * te, g.W - tx0 * te);
@@ -2532,11 +2735,9 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
     __syncthreads();
     int rmin = 0, nrows = kBandRows + 1;
     if (fit) {
-      int lo = INT_MAX, hi = INT_MIN;
-      for (int a = 0; a <= nv; ++a) {
-        lo = min(lo, ssv[a]);
-        hi = max(hi, ssv[a]);
-      }
+      // Spans are monotone along the band's sample rows too: the end rows
+      // give the net rows the band reads.
+      const int lo = min(ssv[0], ssv[nv]), hi = max(ssv[0], ssv[nv]);
       rmin = lo - s.degv;
       nrows = hi - rmin + 1;
     }
@@ -2552,13 +2753,34 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 3) k_cells
       ncu = max(s_su[0], s_su[1]) + 1 - cu0;
     }
     const bool tiled = factored && ncu <= kBandNetCols;
+    // Full-degree units take the fast path, over NR = D + 2 or D + 3 net
+    // rows (rows past the band's own are zero-filled).
+    const bool fast = tiled && s.degu == D && s.degv == D;
+    const int nrf = nrows <= D + 2 ? D + 2 : D + 3;
     if (tiled) {
-      for (int e = tid; e < nrows * ncu; e += blockDim.x) {
+      const int nrs = fast ? nrf : nrows;
+      for (int e = tid; e < nrs * ncu; e += blockDim.x) {
         const int R = e / ncu, cc = e - (e / ncu) * ncu;
-        NT[R * kBandNetCols + cc] = s.cpw[static_cast<long long>(s.ncpu) * (rmin + R) + cu0 + cc];
+        NT[R * kBandNetCols + cc] = R < nrows ? s.cpw[static_cast<long long>(s.ncpu) * (rmin + R) + cu0 + cc]
+                                              : Vec4<TC>{TC(0), TC(0), TC(0), TC(0)};
       }
     }
     __syncthreads();
+    if (fast) {
+      if (s.rat) {
+        if (nrf == D + 2)
+          band_unit_fast<TB, TC, D, D + 2, true>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+        else
+          band_unit_fast<TB, TC, D, D + 3, true>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+      } else {
+        if (nrf == D + 2)
+          band_unit_fast<TB, TC, D, D + 2, false>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+        else
+          band_unit_fast<TB, TC, D, D + 3, false>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+      }
+      __syncthreads();
+      continue;
+    }
     for (int col = tid; col < ncols; col += blockDim.x) {
       const long long lu = lu0 + col;
       if (factored) {
