@@ -1179,7 +1179,7 @@ __global__ void k_dist_cull_st(SideRound<T> a, SideRound<T> b, const int *map1, 
 }
 
 // Surviving supertile pairs expanded into their <= 64 x 64 child tile pairs,
-// one block per supertile pair.  Each side's child tiles are first tested
+// one warp per supertile pair.  Each side's child tiles are first tested
 // against the other supertile's box: a tile box lies inside its supertile's
 // box and the rounded gap is monotone, so lb(t1, t2) >= lb(t1, S2) and a tile
 // that fails against the box fails against every tile inside it.  Only the
@@ -1205,9 +1205,15 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
                                                      int cull, unsigned long long *surv, unsigned *surv_lb,
                                                      unsigned long long cap, ScreenStats *stats, float e,
                                                      long long qs) {
+  // One warp per supertile pair, warp-synchronous throughout (no block
+  // barrier inside the loop), so a block keeps four pairs in flight.  The
+  // surviving children of each side, with the data the crossing needs (the
+  // representative centre, or the tile box), sit in the warp's shared lists.
+  constexpr int kW = 4, kC = kMaxTile * kMaxTile;
   __shared__ unsigned sh[256];
-  __shared__ int s_t1[kMaxTile * kMaxTile], s_t2[kMaxTile * kMaxTile];
-  __shared__ int s_n1, s_n2;
+  __shared__ int s_t[kW][2][kC];
+  __shared__ Vec4<T> s_p[kW][2][kC];  // representative centre (cull = 0) or tile lo (cull = 1)
+  __shared__ Vec4<T> s_q[kW][2][kC];  // tile hi (cull = 1)
   const long long qo = qoff(qs);
   a = qsh(a, qo);
   b = qsh(b, qo);
@@ -1220,70 +1226,85 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
   nst_surv = count_of(nst_surv, stats->st_survivors, st_cap);
   const Geom g1 = a.g, g2 = b.g;
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
-  const int tid = threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
   float best = __uint_as_float(0x7f800000u);
-  for (unsigned long long w = blockIdx.x; w < nst_surv; w += gridDim.x) {
+  for (unsigned long long w = static_cast<unsigned long long>(blockIdx.x) * kW + warp; w < nst_surv;
+       w += static_cast<unsigned long long>(gridDim.x) * kW) {
     const unsigned long long q = st_surv[w];
     const int row = static_cast<int>(q >> 32), s2 = static_cast<int>(q & 0xffffffffull);
     const int slot = row / g1.nst, s1 = row - slot * g1.nst;
     const int r1 = map1[slot], r2 = map2[slot];
-    const int sy1 = s1 / g1.stw, sx1 = s1 - sy1 * g1.stw, sy2 = s2 / g2.stw, sx2 = s2 - sy2 * g2.stw;
     const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
     const T tau = thr_compare<T, S>(taub, e);
-    if (tid == 0) {
-      s_n1 = 0;
-      s_n2 = 0;
-    }
-    __syncthreads();
-    if (tid < 2 * kMaxTile * kMaxTile) {
-      const int side = tid >> 6, l = tid & 63;
-      if (side == 0) {
-        const int ty = sy1 * kMaxTile + (l >> 3), tx = sx1 * kMaxTile + (l & 7);
-        if (ty < g1.tw && tx < g1.tw) {
-          const int t = ty * g1.tw + tx;
-          const long long i1 = static_cast<long long>(r1) * g1.ntiles + t;
-          const long long j2 = static_cast<long long>(r2) * g2.nst + s2;
-          Vec4<T> slo, shi;
-          st_bounds(b, j2, slo, shi);
-          if (shaved_lb<T, S>(a.tlo[i1], a.thi[i1], slo, shi) <= tau) s_t1[atomicAdd(&s_n1, 1)] = t;
+    Vec4<T> slo1, shi1, slo2, shi2;
+    st_bounds(a, static_cast<long long>(r1) * g1.nst + s1, slo1, shi1);
+    st_bounds(b, static_cast<long long>(r2) * g2.nst + s2, slo2, shi2);
+    // Children of each side tested against the other supertile's box,
+    // compacted in lane order.
+    int m[2];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const SideRound<T> &X = side ? b : a;
+      const Geom &g = side ? g2 : g1;
+      const int sidx = side ? s2 : s1, r = side ? r2 : r1;
+      const int sy = sidx / g.stw, sx = sidx - sy * g.stw;
+      int base = 0;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int l = lane + 32 * h;
+        const int ty = sy * kMaxTile + (l >> 3), tx = sx * kMaxTile + (l & 7);
+        const bool valid = ty < g.tw && tx < g.tw;
+        const int t = valid ? ty * g.tw + tx : 0;
+        const long long i = static_cast<long long>(r) * g.ntiles + t;
+        Vec4<T> lo{}, hi{};
+        bool ok = false;
+        if (valid) {
+          lo = X.tlo[i];
+          hi = X.thi[i];
+          ok = (side ? shaved_lb<T, S>(slo1, shi1, lo, hi) : shaved_lb<T, S>(lo, hi, slo2, shi2)) <= tau;
         }
-      } else {
-        const int ty = sy2 * kMaxTile + (l >> 3), tx = sx2 * kMaxTile + (l & 7);
-        if (ty < g2.tw && tx < g2.tw) {
-          const int t = ty * g2.tw + tx;
-          const long long i2 = static_cast<long long>(r2) * g2.ntiles + t;
-          const long long j1 = static_cast<long long>(r1) * g1.nst + s1;
-          Vec4<T> slo, shi;
-          st_bounds(a, j1, slo, shi);
-          if (shaved_lb<T, S>(slo, shi, b.tlo[i2], b.thi[i2]) <= tau) s_t2[atomicAdd(&s_n2, 1)] = t;
+        const unsigned mask = __ballot_sync(kFull, ok);
+        if (ok) {
+          const int pos = base + __popc(mask & lt);
+          s_t[warp][side][pos] = t;
+          if (!cull) {
+            s_p[warp][side][pos] = X.center[i * (side ? n2 : n1) + tile_rep(t, g)];
+          } else {
+            s_p[warp][side][pos] = lo;
+            s_q[warp][side][pos] = hi;
+          }
         }
+        base += __popc(mask);
       }
+      m[side] = base;
     }
-    __syncthreads();
-    const int m1 = s_n1, m2 = s_n2, total = m1 * m2;
-    for (int c0 = 0; c0 < total; c0 += blockDim.x) {
-      const int c = c0 + tid;
+    __syncwarp();
+    const int m1 = m[0], m2 = m[1], total = m1 * m2;
+    // c -> (c / m2, c % m2) through a float reciprocal: c < 2^12 and m2 <= 64
+    // keep the rounded quotient within 2^-10 of the true one, whose fraction
+    // lies in [1/128, 1 - 1/128], so the truncation is exact.
+    const float inv = total > 0 ? 1.0f / static_cast<float>(m2) : 0.0f;
+    for (int c0 = 0; c0 < total; c0 += 32) {
+      const int c = c0 + lane;
       bool keep = false;
       T lb = T(0);
-      int t1 = 0, t2 = 0;
+      int i1 = 0, i2 = 0;
       if (c < total) {
-        t1 = s_t1[c / m2];
-        t2 = s_t2[c - (c / m2) * m2];
-        const long long i1 = static_cast<long long>(r1) * g1.ntiles + t1;
-        const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
+        i1 = __float2int_rz((static_cast<float>(c) + 0.5f) * inv);
+        i2 = c - i1 * m2;
         if (!cull) {
-          const Vec4<T> c1 = a.center[i1 * n1 + tile_rep(t1, g1)];
-          const Vec4<T> c2 = b.center[i2 * n2 + tile_rep(t2, g2)];
-          best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+          best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(s_p[warp][0][i1], s_p[warp][1][i2]), e)));
         } else {
-          lb = shaved_lb<T, S>(a.tlo[i1], a.thi[i1], b.tlo[i2], b.thi[i2]);
+          lb = shaved_lb<T, S>(s_p[warp][0][i1], s_q[warp][0][i1], s_p[warp][1][i2], s_q[warp][1][i2]);
           keep = lb <= tau;
         }
       }
       if (cull) {
         const long long pos = warp_append(keep, &stats->survivors);
         if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) {
-          surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + t1), static_cast<unsigned>(t2));
+          surv[pos] = pack_tile_pair(static_cast<unsigned>(slot * g1.ntiles + s_t[warp][0][i1]),
+                                     static_cast<unsigned>(s_t[warp][1][i2]));
           surv_lb[pos] = lb_bits_down(lb);
         }
       }
@@ -1292,10 +1313,10 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
       const unsigned mine = __float_as_uint(best);
       if (__popc(__ballot_sync(kFull, mine < taub)) >= k) {
         const unsigned kth = warp_sorted_at(mine, k - 1);
-        if ((tid & 31) == 0) atomicMin(&stats->tau_bits, kth);
+        if (lane == 0) atomicMin(&stats->tau_bits, kth);
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
   if (!cull && k > 32) fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
 }
@@ -3469,7 +3490,7 @@ void launch_dist_expand(const SideRound<T> &a, const SideRound<T> &b, const int 
                         ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
   if (nst_surv == 0) return;
-  // One 128-thread block per supertile pair (2 x 64 child pre-filter lanes).
+  // 128-thread blocks, one warp per supertile pair.
   const unsigned long long most = nst_surv == kFromDevice ? st_cap : nst_surv;
   const dim3 grid = bdim(bgrid(static_cast<long long>(most < 148ull * 32 ? most : 148ull * 32), bt, 148 * 32), bt);
   if constexpr (std::is_same<T, float>::value) {
