@@ -440,6 +440,7 @@ def run_ours(args):
         "batch_reruns": head["reruns"],
         "screen": {"pair_tests_per_round": [int(x) for x in last.pair_tests],
                    "candidates_per_round": [int(x) for x in last.candidates],
+                   "tile_pairs_per_round": [int(x) for x in last.tile_pairs],
                    "kept_per_round": [int(x) for x in last.npairs]},
         "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
         "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kt.items()},

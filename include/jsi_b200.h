@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define JSI_B200_ABI_VERSION 1
+#define JSI_B200_ABI_VERSION 2
 #define JSI_MAX_ROUNDS 16
 #define JSI_RECORD_SIZE 18 /* ONE_UV_SIZE, include/jsi_cad.hpp:45 */
 
@@ -141,6 +141,7 @@ typedef struct {
   int *trace_pairs;
   long long trace_cap; /* capacity in triples; needs rounds*k */
   float device_ms;     /* device time of the query (CUDA events) */
+  long long tile_pairs[JSI_MAX_ROUNDS]; /* tile pairs that passed the bound screen per round */
 } jsi_dist_result;
 
 void jsi_dist_params_default(jsi_dist_params *p);

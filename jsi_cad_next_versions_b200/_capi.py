@@ -58,7 +58,8 @@ class DistResult(ctypes.Structure):
                 ("point2", ctypes.c_double * 3), ("rounds_run", ctypes.c_int), ("npairs", ctypes.c_int * MAX_ROUNDS),
                 ("kth_d2", ctypes.c_double * MAX_ROUNDS), ("pair_tests", ctypes.c_longlong * MAX_ROUNDS),
                 ("candidates", ctypes.c_longlong * MAX_ROUNDS), ("trace_pairs", ctypes.POINTER(ctypes.c_int)),
-                ("trace_cap", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+                ("trace_cap", ctypes.c_longlong), ("device_ms", ctypes.c_float),
+                ("tile_pairs", ctypes.c_longlong * MAX_ROUNDS)]
 
 
 class InterParams(ctypes.Structure):

@@ -47,6 +47,7 @@ class DistanceResult:
     candidates: np.ndarray
     device_ms: float
     pairs: list = field(default_factory=list)  # per round (n, 3) int32 (slot, i, j) if traced
+    tile_pairs: np.ndarray = None  # tile pairs that passed the bound screen, per round
 
 
 @dataclass
@@ -215,7 +216,8 @@ class Context:
             v5_value=float(np.float32(r.v5_value)), distance=r.distance, newton_distance=r.newton_distance,
             uv1=tuple(r.uv1), uv2=tuple(r.uv2), point1=tuple(r.point1), point2=tuple(r.point2), rounds=n,
             npairs=npairs, kth_d2=np.array(r.kth_d2[:n]), pair_tests=np.array(r.pair_tests[:n], dtype=np.int64),
-            candidates=np.array(r.candidates[:n], dtype=np.int64), device_ms=r.device_ms, pairs=pairs)
+            candidates=np.array(r.candidates[:n], dtype=np.int64), device_ms=r.device_ms, pairs=pairs,
+            tile_pairs=np.array(r.tile_pairs[:n], dtype=np.int64))
 
     def min_distance(self, a: C.Task, b: C.Task, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
                      precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False) -> DistanceResult:

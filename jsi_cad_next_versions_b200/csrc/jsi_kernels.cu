@@ -913,15 +913,29 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
   // Sorted lists are taken in order from a work counter (a bound above tau
   // ends the warp); unsorted lists are split statically and skip such pairs.
   const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
-  unsigned long long wnext = (blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x) >> 5;
+  // Unsorted lists are split statically: warp i owns entries i, i + nwarps,
+  // ... and scans 32 of them at once (one bound per lane, a ballot of those
+  // under tau), then works through the passing ones.
+  unsigned long long chunk = (blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x) >> 5;
+  unsigned pending = 0;
   for (;;) {
     unsigned long long w = 0;
     if (sorted) {
       if (lane == 0) w = atomicAdd(&stats->work, 1ull);
       w = __shfl_sync(kFull, w, 0);
     } else {
-      w = wnext;
-      wnext += nwarps;
+      while (pending == 0 && chunk < nsurv) {
+        const unsigned long long x = chunk + lane * nwarps;
+        const unsigned tb = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
+        const bool pass = x < nsurv && (!surv_lb || __uint_as_float(surv_lb[x]) <=
+                                                        static_cast<float>(thr_compare<float, S>(tb, e)));
+        pending = __ballot_sync(kFull, pass);
+        if (pending == 0) chunk += nwarps * 32;
+      }
+      if (pending == 0) break;
+      w = chunk + static_cast<unsigned long long>(__ffs(pending) - 1) * nwarps;
+      pending &= pending - 1;
+      if (pending == 0) chunk += nwarps * 32;
     }
     if (w >= nsurv) break;
     const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
@@ -988,7 +1002,10 @@ __global__ void __launch_bounds__(256) k_dist_leaf(SideRound<T> a, SideRound<T> 
 // bounds when surv is sorted): one warp per tile pair, each lane keeps the KL
 // smallest d2 of its own pairs in a sorted register list, and the warp merges
 // the 32 lists to the exact k-th smallest d2 of the tile pair (k <= KL), which
-// is a valid upper bound of the global k-th and is folded into tau.
+// is a valid upper bound of the global k-th and is folded into tau.  Only d2
+// <= tau (the threshold when the tile pair starts) enter the lists: with k
+// such values the k-th among them is the tile pair's k-th, and with fewer the
+// tile pair's k-th exceeds tau and its fold would change nothing.
 template <typename T, int KL, bool S>
 __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> b, const int *map1,
                                                    const int *map2, const unsigned long long *surv,
@@ -1026,6 +1043,8 @@ __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> 
     const Vec4<T> c2b = vb ? b.center[base2 + jb] : far4;
     const Vec4<T> c1a = ja < n1 ? a.center[base1 + ja] : far4;
     const Vec4<T> c1b = jb < n1 ? a.center[base1 + jb] : far4;
+    const unsigned taub = *reinterpret_cast<volatile unsigned *>(&stats->tau_bits);
+    const T tau = thr_compare<T, S>(taub, e);
     T L[KL];
 #pragma unroll
     for (int q2 = 0; q2 < KL; ++q2) L[q2] = pos_inf<T>();
@@ -1037,7 +1056,7 @@ __global__ void __launch_bounds__(256) k_dist_head(SideRound<T> a, SideRound<T> 
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const T x = d[h];
-          if (x < L[KL - 1]) {
+          if (x < L[KL - 1] && x <= tau) {
 #pragma unroll
             for (int q2 = KL - 1; q2 >= 1; --q2) L[q2] = (x < L[q2 - 1]) ? L[q2 - 1] : ((x < L[q2]) ? x : L[q2]);
             L[0] = (x < L[0]) ? x : L[0];
