@@ -79,6 +79,15 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id);
  * records; out[q] gets each id (0 for those not uploaded after an error). */
 int jsi_surface_upload_many(jsi_context *ctx, int n, const int *ivecs, const float *const *datas, const int *ndatas,
                             jsi_surface_id *out);
+/* n releases in one call (each as jsi_surface_release; stops at the first
+ * failing id and returns its status). */
+int jsi_surface_release_many(jsi_context *ctx, int n, const jsi_surface_id *ids);
+/* Full parameter domains of n resident surfaces: rects[4q..4q+3] =
+ * (ustart, vstart, ustop, vstop), the values NurbsFace::get_ubegin,
+ * get_vbegin, get_uend, get_vend return (include/nurbs_data.hpp:6-9) and the
+ * reference's examples put into EvalAndConstructTask
+ * (examples/intersection_example.cu:62-65). */
+int jsi_surface_domains(jsi_context *ctx, int n, const jsi_surface_id *ids, float *rects);
 /* Resident surface bytes on the device. */
 int jsi_resident_bytes(const jsi_context *ctx, unsigned long long *out);
 

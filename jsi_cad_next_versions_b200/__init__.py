@@ -6,6 +6,7 @@ orchestration, include/jsi_b200.h); this package is its Python host mirror.
 """
 from .api import (  # noqa: F401
     Context,
+    DistanceBatch,
     DistanceResult,
     EvalAndConstructTask,
     IntersectionResult,
@@ -18,11 +19,12 @@ from .api import (  # noqa: F401
     init_cad,
     intersection,
     minimum_distance,
+    TaskBatch,
 )
 from . import synth  # noqa: F401
 
 __all__ = [
-    "Context", "DistanceResult", "EvalAndConstructTask", "IntersectionResult", "JsiError", "ONE_UV_SIZE",
+    "Context", "DistanceBatch", "DistanceResult", "TaskBatch", "EvalAndConstructTask", "IntersectionResult", "JsiError", "ONE_UV_SIZE",
     "default_global_dist_nuv", "default_global_intersect_nuv", "deinit_cad", "evalWithCuda", "init_cad",
     "intersection", "minimum_distance", "synth",
 ]

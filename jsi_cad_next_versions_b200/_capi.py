@@ -27,7 +27,8 @@ PRECISIONS = {"v5_fp32": PREC_V5_FP32, "fp64": PREC_FP64, "fp32_screen": PREC_FP
 # Every symbol include/jsi_b200.h declares.
 EXPORTED = [
     "jsi_abi_version", "jsi_status_string", "jsi_last_error", "jsi_create", "jsi_destroy",
-    "jsi_surface_upload", "jsi_surface_upload_many", "jsi_surface_release", "jsi_resident_bytes", "jsi_context_stream",
+    "jsi_surface_upload", "jsi_surface_upload_many", "jsi_surface_release", "jsi_surface_release_many",
+    "jsi_surface_domains", "jsi_resident_bytes", "jsi_context_stream",
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_units", "jsi_kernel_names",
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_bounds_params_default",
@@ -179,9 +180,13 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_min_distance_batch.argtypes = [P, I, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),
                                          ctypes.POINTER(DistResult), ctypes.POINTER(I), ctypes.POINTER(ctypes.c_float)]
     L.jsi_min_distance_batch.restype = I
-    L.jsi_surface_upload_many.argtypes = [P, I, ctypes.POINTER(I), ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
-                                          ctypes.POINTER(I), ctypes.POINTER(I)]
+    # datas: the address of an array of n float pointers
+    L.jsi_surface_upload_many.argtypes = [P, I, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.jsi_surface_upload_many.restype = I
+    L.jsi_surface_release_many.argtypes = [P, I, ctypes.c_void_p]
+    L.jsi_surface_release_many.restype = I
+    L.jsi_surface_domains.argtypes = [P, I, ctypes.c_void_p, ctypes.c_void_p]
+    L.jsi_surface_domains.restype = I
     L.jsi_curve_params_default.argtypes = [ctypes.POINTER(CurveParams)]
     L.jsi_curve_params_default.restype = None
     L.jsi_intersection_curves.argtypes = [P, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(CurveParams),

@@ -14,6 +14,7 @@ Errors raise ``JsiError`` carrying the C status; nothing falls back to the CPU.
 from __future__ import annotations
 
 import ctypes
+from collections.abc import Sequence
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -48,6 +49,94 @@ class DistanceResult:
     device_ms: float
     pairs: list = field(default_factory=list)  # per round (n, 3) int32 (slot, i, j) if traced
     tile_pairs: np.ndarray = None  # tile pairs that passed the bound screen, per round
+
+
+def _struct_dtype(st) -> np.dtype:
+    """numpy dtype with the byte layout of a ctypes Structure (pointers as
+    uint64), for zero-copy views of result arrays."""
+    names, formats, offsets = [], [], []
+    for name, ct in st._fields_:
+        if hasattr(ct, "_length_"):
+            f = (np.dtype(ct._type_), (ct._length_,))
+        elif issubclass(ct, ctypes._Pointer):
+            f = np.dtype(np.uint64)
+        else:
+            f = np.dtype(ct)
+        names.append(name)
+        formats.append(f)
+        offsets.append(getattr(st, name).offset)
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": ctypes.sizeof(st)})
+
+
+_DIST_DTYPE = _struct_dtype(C.DistResult)
+
+
+class DistanceBatch(Sequence):
+    """Results of min_distance_batch.  Indexing gives the DistanceResult of
+    one query (built on access); the fields of all queries are also numpy
+    arrays over the C result records (``distance``, ``v5_value``,
+    ``device_ms``, ``newton_distance``, ``rounds``, ``npairs``, ``kth_d2``,
+    ``pair_tests``, ``candidates``, ``tile_pairs``; per-round fields are
+    (n, JSI_MAX_ROUNDS))."""
+
+    def __init__(self, res, bufs, k: int):
+        self._res, self._bufs, self._k = res, bufs, k
+        self.records = np.frombuffer(res, dtype=_DIST_DTYPE, count=len(res))
+
+    def __len__(self) -> int:
+        return len(self._res)
+
+    def __getitem__(self, q):
+        if isinstance(q, slice):
+            return [self[i] for i in range(*q.indices(len(self)))]
+        n = len(self._res)
+        if q < 0:
+            q += n
+        if not 0 <= q < n:
+            raise IndexError(q)
+        return Context._dist_result(self._res[q], self._bufs[q], self._k)
+
+    def __getattr__(self, name):
+        names = {"rounds": "rounds_run"}
+        key = names.get(name, name)
+        if key in _DIST_DTYPE.names and key not in ("trace_pairs", "trace_cap"):
+            return self.records[key]
+        raise AttributeError(name)
+
+
+_TASK_DTYPE = _struct_dtype(C.Task)
+
+
+class TaskBatch:
+    """Query pairs packed once for repeated min_distance_batch calls."""
+
+    def __init__(self, pairs=None):
+        if pairs is None:
+            return
+        self.n = len(pairs)
+        self.a = (C.Task * self.n)(*[x[0] for x in pairs])
+        self.b = (C.Task * self.n)(*[x[1] for x in pairs])
+
+    @classmethod
+    def from_arrays(cls, ids_a, rects_a, nuv_a, ids_b, rects_b, nuv_b, side_a: int = 1, side_b: int = 2):
+        """Tasks from arrays: ids (n,), rects (n, 4) (ustart, vstart, ustop,
+        vstop), nuv scalars or (n,) arrays."""
+        tb = cls()
+        n = len(ids_a)
+        tb.n = n
+        for name, ids, rects, nuv, side in (("a", ids_a, rects_a, nuv_a, side_a), ("b", ids_b, rects_b, nuv_b, side_b)):
+            arr = (C.Task * n)()
+            v = np.frombuffer(arr, dtype=_TASK_DTYPE, count=n)
+            r = np.asarray(rects, np.float32)
+            v["surface"] = ids
+            v["ustart"], v["vstart"], v["ustop"], v["vstop"] = r[:, 0], r[:, 1], r[:, 2], r[:, 3]
+            v["nuv"] = nuv
+            v["side"] = side
+            setattr(tb, name, arr)
+        return tb
+
+    def __len__(self) -> int:
+        return self.n
 
 
 @dataclass
@@ -146,13 +235,25 @@ class Context:
             return []
         iv = np.ascontiguousarray(np.stack([np.asarray(x.ivec, np.int32) for x in surfaces]), dtype=np.int32)
         keep = [np.ascontiguousarray(x.data, dtype=np.float32) for x in surfaces]
-        FP = ctypes.POINTER(ctypes.c_float)
-        ptrs = (FP * n)(*[k.ctypes.data_as(FP) for k in keep])
-        nd = (ctypes.c_int * n)(*[int(k.shape[0]) for k in keep])
-        ids = (ctypes.c_int * n)()
-        self._check(self.lib.jsi_surface_upload_many(self.handle, n, iv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                                     ptrs, nd, ids))
-        return list(ids)
+        ptrs = np.fromiter((k.ctypes.data for k in keep), dtype=np.uintp, count=n)
+        nd = np.fromiter((k.shape[0] for k in keep), dtype=np.int32, count=n)
+        ids = np.zeros(n, np.int32)
+        self._check(self.lib.jsi_surface_upload_many(self.handle, n, iv.ctypes.data, ptrs.ctypes.data, nd.ctypes.data,
+                                                     ids.ctypes.data))
+        return ids.tolist()
+
+    def release_many(self, ids):
+        """Release several surfaces in one call."""
+        a = np.ascontiguousarray(ids, dtype=np.int32)
+        self._check(self.lib.jsi_surface_release_many(self.handle, a.size, a.ctypes.data))
+
+    def surface_domains(self, ids) -> np.ndarray:
+        """(n, 4) float32 full parameter domains (ustart, vstart, ustop, vstop)
+        of resident surfaces."""
+        a = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.zeros((a.size, 4), np.float32)
+        self._check(self.lib.jsi_surface_domains(self.handle, a.size, a.ctypes.data, out.ctypes.data))
+        return out
 
     def release(self, sid: int):
         self._check(self.lib.jsi_surface_release(self.handle, sid))
@@ -316,26 +417,24 @@ class Context:
                            precision: str | int = "v5_fp32", trace: bool = False, newton: bool = False):
         """Distance queries [(task_a, task_b), ...] over the worker lanes
         (lockstep batches per shape, see batch_chunk).
-        Returns (results, device_ms of the whole batch)."""
-        n = len(pairs)
+        ``pairs`` is a list of (task_a, task_b) or a TaskBatch.
+        Returns (DistanceBatch, device_ms of the whole batch)."""
+        tasks = pairs if isinstance(pairs, TaskBatch) else TaskBatch(pairs)
+        n = tasks.n
         p = self._dist_params(k, rounds, nuv_refine, precision, newton)
-        ta = (C.Task * n)(*[x[0] for x in pairs])
-        tb = (C.Task * n)(*[x[1] for x in pairs])
         res = (C.DistResult * n)()
-        bufs = []
-        for q in range(n):
-            if trace:
+        bufs = [None] * n
+        if trace:
+            for q in range(n):
                 buf = np.full(rounds * k * 3, -1, dtype=np.int32)
                 res[q].trace_pairs = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
                 res[q].trace_cap = rounds * k
-                bufs.append(buf)
-            else:
-                bufs.append(None)
+                bufs[q] = buf
         status = (ctypes.c_int * n)()
         ms = ctypes.c_float(0)
-        self._check(self.lib.jsi_min_distance_batch(self.handle, n, ta, tb, ctypes.byref(p), res, status,
+        self._check(self.lib.jsi_min_distance_batch(self.handle, n, tasks.a, tasks.b, ctypes.byref(p), res, status,
                                                     ctypes.byref(ms)))
-        return [self._dist_result(res[q], bufs[q], k) for q in range(n)], ms.value
+        return DistanceBatch(res, bufs, k), ms.value
 
     def intersection_curves(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                             halve_threshold: int = 512, min_nuv: int = 4, link_tol: float = 0.0,

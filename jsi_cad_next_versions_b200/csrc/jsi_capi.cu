@@ -167,6 +167,7 @@ struct SurfaceRec {
   double cmax[3] = {0, 0, 0};   // max |control point coordinate|
   double wcmax[3] = {0, 0, 0};  // max |w * control point coordinate| (rational)
   double wmin = 1, wmax = 1;    // weight range (rational)
+  float dom[4] = {0, 0, 0, 0};  // parameter domain (ustart, vstart, ustop, vstop)
   float *U32 = nullptr, *V32 = nullptr;
   double *U64 = nullptr, *V64 = nullptr;
   Vec4<float> *cpw32 = nullptr;
@@ -431,6 +432,10 @@ void surface_header(SurfaceRec &s, const int ivec[7], const float *data) {
   s.zero = ((!(flags & 1)) && (flags & 12)) || ivec[1] >= kMaxDeg || ivec[4] >= kMaxDeg;
   s.du = std::min(2, ivec[1]);
   s.dv = std::min(2, ivec[4]);
+  s.dom[0] = data[0];
+  s.dom[1] = data[ivec[3]];
+  s.dom[2] = data[ivec[3] - 1];
+  s.dom[3] = data[ivec[3] + ivec[6] - 1];
   const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
   const float *cp = data + ivec[3] + ivec[6];
   // Branch-free loops in float (|x| and max are exact, and so is the
@@ -2631,6 +2636,26 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id) {
   ctx->resident -= it->second.bytes;
   ctx->pool.put(it->second.block, it->second.block_bytes);
   ctx->surfaces.erase(it);
+  return JSI_OK;
+}
+
+int jsi_surface_release_many(jsi_context *ctx, int n, const jsi_surface_id *ids) {
+  if (!ctx || n < 0 || (n > 0 && !ids)) return JSI_ERR_INVALID;
+  for (int q = 0; q < n; ++q) {
+    const int st = jsi_surface_release(ctx, ids[q]);
+    if (st != JSI_OK) return st;
+  }
+  return JSI_OK;
+}
+
+int jsi_surface_domains(jsi_context *ctx, int n, const jsi_surface_id *ids, float *rects) {
+  if (!ctx || n < 0 || (n > 0 && (!ids || !rects))) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (int q = 0; q < n; ++q) {
+    auto it = ctx->surfaces.find(ids[q]);
+    if (it == ctx->surfaces.end()) return record(ctx, JSI_ERR_INVALID, "unknown surface id");
+    std::memcpy(rects + 4 * static_cast<size_t>(q), it->second.dom, sizeof(it->second.dom));
+  }
   return JSI_OK;
 }
 
