@@ -316,6 +316,15 @@ int jsi_queue_depth(jsi_context *ctx, int *queued, int *running);
  * distance_analysis.cu:356). */
 int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
                            const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms);
+/* jsi_min_distance_batch in two halves, so that the caller can stage and
+ * upload the next batch's surfaces while this one runs: submit queues the
+ * batch and returns a ticket at once; a, b, out and status must stay valid
+ * until jsi_wait_distance_batch(ticket) returns.  The batch starts after the
+ * uploads issued before the submit.  device_ms (may be null) is the span
+ * from the submission to the end of the batch's last lane job. */
+int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
+                              const jsi_dist_params *params, jsi_dist_result *out, int *status, jsi_ticket *ticket);
+int jsi_wait_distance_batch(jsi_context *ctx, jsi_ticket ticket, float *device_ms);
 /* Queries per lockstep batch (default 64; 0: every query runs alone). */
 int jsi_batch_chunk(jsi_context *ctx, int chunk);
 /* Batch items re-run alone after an internal list overflowed (all lanes). */

@@ -34,7 +34,7 @@ EXPORTED = [
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_bounds_params_default",
     "jsi_distance_bounds", "jsi_curve_params_default", "jsi_intersection_curves", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
-    "jsi_queue_depth", "jsi_min_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs", "jsi_autotune_batch",
+    "jsi_queue_depth", "jsi_min_distance_batch", "jsi_submit_distance_batch", "jsi_wait_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs", "jsi_autotune_batch",
 ]
 
 
@@ -180,6 +180,11 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_min_distance_batch.argtypes = [P, I, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),
                                          ctypes.POINTER(DistResult), ctypes.POINTER(I), ctypes.POINTER(ctypes.c_float)]
     L.jsi_min_distance_batch.restype = I
+    L.jsi_submit_distance_batch.argtypes = [P, I, ctypes.POINTER(Task), ctypes.POINTER(Task), ctypes.POINTER(DistParams),
+                                            ctypes.POINTER(DistResult), ctypes.POINTER(I), ctypes.POINTER(ctypes.c_longlong)]
+    L.jsi_submit_distance_batch.restype = I
+    L.jsi_wait_distance_batch.argtypes = [P, ctypes.c_longlong, ctypes.POINTER(ctypes.c_float)]
+    L.jsi_wait_distance_batch.restype = I
     # datas: the address of an array of n float pointers
     L.jsi_surface_upload_many.argtypes = [P, I, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.jsi_surface_upload_many.restype = I

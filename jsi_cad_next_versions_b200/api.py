@@ -419,6 +419,15 @@ class Context:
         (lockstep batches per shape, see batch_chunk).
         ``pairs`` is a list of (task_a, task_b) or a TaskBatch.
         Returns (DistanceBatch, device_ms of the whole batch)."""
+        return self.wait_distance_batch(self.submit_distance_batch(pairs, k=k, rounds=rounds, nuv_refine=nuv_refine,
+                                                                   precision=precision, trace=trace, newton=newton))
+
+    def submit_distance_batch(self, pairs, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
+                              precision: str | int = "v5_fp32", trace: bool = False, newton: bool = False):
+        """Queue a batch (as min_distance_batch) and return at once; pass the
+        returned handle to wait_distance_batch.  Uploads issued before the
+        submit are visible to the batch, so the next batch's surfaces can be
+        uploaded while this one runs."""
         tasks = pairs if isinstance(pairs, TaskBatch) else TaskBatch(pairs)
         n = tasks.n
         p = self._dist_params(k, rounds, nuv_refine, precision, newton)
@@ -431,10 +440,17 @@ class Context:
                 res[q].trace_cap = rounds * k
                 bufs[q] = buf
         status = (ctypes.c_int * n)()
+        t = ctypes.c_longlong(0)
+        self._check(self.lib.jsi_submit_distance_batch(self.handle, n, tasks.a, tasks.b, ctypes.byref(p), res, status,
+                                                       ctypes.byref(t)))
+        # everything the C side writes into or reads from stays alive here
+        return {"ticket": t.value, "tasks": tasks, "res": res, "bufs": bufs, "status": status, "k": k}
+
+    def wait_distance_batch(self, handle):
+        """Wait for a submitted batch: (DistanceBatch, device_ms)."""
         ms = ctypes.c_float(0)
-        self._check(self.lib.jsi_min_distance_batch(self.handle, n, tasks.a, tasks.b, ctypes.byref(p), res, status,
-                                                    ctypes.byref(ms)))
-        return DistanceBatch(res, bufs, k), ms.value
+        self._check(self.lib.jsi_wait_distance_batch(self.handle, handle["ticket"], ctypes.byref(ms)))
+        return DistanceBatch(handle["res"], handle["bufs"], handle["k"]), ms.value
 
     def intersection_curves(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                             halve_threshold: int = 512, min_nuv: int = 4, link_tol: float = 0.0,

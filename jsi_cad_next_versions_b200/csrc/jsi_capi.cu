@@ -257,6 +257,10 @@ struct Lane {
   std::map<std::string, std::pair<double, long long>> kernel_ms;
   std::map<std::string, double> kernel_units;  // work units (samples, tile pairs, pair tests, ...)
   const std::map<int, SurfaceRec> *surfaces = nullptr;
+  // Worker lanes: the context mutex that guards the surface table (uploads
+  // and releases on the calling thread change it while lanes run).  Null for
+  // the main lane, whose callers hold it already.
+  std::mutex *surfaces_mu = nullptr;
   char *h_pin = nullptr;  // pinned staging of batch heads / records
   size_t h_pin_bytes = 0;
   long long batch_reruns = 0;  // batch items re-run alone after an overflow
@@ -295,6 +299,32 @@ struct Job {
   int status = JSI_OK;
   std::string error;
   bool done = false;
+  cudaEvent_t end_ev = nullptr;  // recorded on the lane's stream after the job's work
+  Job() = default;
+  Job(const Job &) = delete;
+  Job &operator=(const Job &) = delete;
+  ~Job() {
+    if (end_ev) cudaEventDestroy(end_ev);
+  }
+};
+
+// A distance batch between its submission and its wait: the lane jobs (and
+// tickets of queries run alone), where the results go, and the start event.
+struct PendingBatch {
+  std::vector<long long> tickets;
+  std::vector<std::shared_ptr<Job>> batch_jobs;
+  std::vector<std::shared_ptr<Job>> all_jobs;  // every job, for the device span
+  std::vector<int> solo;  // query index of each ticket of a per-query job (-1: batch job)
+  jsi_dist_result *out = nullptr;
+  int *status = nullptr;
+  int first_err = 0;
+  cudaEvent_t ev0 = nullptr;
+  PendingBatch() = default;
+  PendingBatch(const PendingBatch &) = delete;
+  PendingBatch &operator=(const PendingBatch &) = delete;
+  ~PendingBatch() {
+    if (ev0) cudaEventDestroy(ev0);
+  }
 };
 
 }  // namespace
@@ -332,6 +362,7 @@ struct jsi_context {
   std::condition_variable qcv, dcv;
   std::deque<std::shared_ptr<Job>> queue;
   std::map<long long, std::shared_ptr<Job>> jobs;
+  std::map<long long, std::unique_ptr<PendingBatch>> batches;  // submitted, not yet waited for
   long long next_ticket = 1;
   int busy = 0;
   bool stopping = false;
@@ -525,7 +556,12 @@ SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int n
   return s;
 }
 
+// The returned record stays valid while a job holds the surface: std::map
+// nodes do not move on other insertions, and a surface a queued or running
+// job refers to cannot be released.
 const SurfaceRec &get_surface(Lane *ctx, jsi_surface_id id) {
+  std::unique_lock<std::mutex> lk;
+  if (ctx->surfaces_mu) lk = std::unique_lock<std::mutex>(*ctx->surfaces_mu);
   auto it = ctx->surfaces->find(id);
   if (it == ctx->surfaces->end()) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
   return it->second;
@@ -2466,6 +2502,8 @@ void worker_loop(jsi_context *ctx, Lane *L) {
         exec_intersection(L, &job->a, &job->b, job->ip, &job->ires);
       else
         exec_distance_batch(L, job->items, job->dp);
+      if (!job->end_ev) JSI_CUDA(cudaEventCreate(&job->end_ev));
+      JSI_CUDA(cudaEventRecord(job->end_ev, L->stream));
     });
     release_refs(ctx, *job);
     if (L->arena.held() > ctx->lane_keep) L->arena.trim(ctx->lane_keep);
@@ -2510,6 +2548,7 @@ void start_workers(jsi_context *ctx, int n) {
   for (int q = 0; q < n; ++q) {
     auto L = std::make_unique<Lane>();
     lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces, &ctx->lane_held, left);
+    L->surfaces_mu = &ctx->mu;
     L->graphs_on = ctx->batch_graphs;
     L->timing = ctx->main.timing;  // per-kernel timing follows the context's setting
     ctx->lanes.push_back(std::move(L));
@@ -3070,35 +3109,43 @@ int jsi_batch_reruns(jsi_context *ctx, long long *out) {
   return JSI_OK;
 }
 
-int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
-                           const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms) {
-  if (!ctx || n < 0 || (n > 0 && (!a || !b || !out))) return JSI_ERR_INVALID;
+int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
+                              const jsi_dist_params *params, jsi_dist_result *out, int *status, jsi_ticket *ticket) {
+  if (!ctx || n < 0 || (n > 0 && (!a || !b || !out)) || !ticket) return JSI_ERR_INVALID;
   if (ctx->lanes.empty()) return record(ctx, JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
   jsi_dist_params p;
   jsi_dist_params_default(&p);
   if (params) p = *params;
-  std::vector<jsi_ticket> tickets;
-  std::vector<std::shared_ptr<Job>> batch_jobs;
-  std::vector<int> solo;  // query index of each ticket of a per-query job (-1: batch job)
-  int first_err = JSI_OK;
+  auto pb = std::make_unique<PendingBatch>();
+  pb->out = out;
+  pb->status = status;
+  pb->first_err = JSI_OK;
+  PendingBatch &B = *pb;
   auto set_status = [&](int q, int st) {
     if (status) status[q] = st;
-    if (st != JSI_OK && first_err == JSI_OK) first_err = st;
+    if (st != JSI_OK && B.first_err == JSI_OK) B.first_err = st;
   };
-  // Device span of the batch: every lane waits for a start event on the main
-  // stream; the main stream waits for every lane at the end.
+  // Start of the batch's device span: an event on the main stream after the
+  // uploads issued before this call.  Lane streams are not touched here (a
+  // lane may be capturing a CUDA graph); each job waits for the uploads on
+  // its own lane before it starts.
   {
     std::lock_guard<std::mutex> lk(ctx->mu);
     const int st = guarded(ctx, [&]() {
       JSI_CUDA(cudaSetDevice(ctx->device));
-      JSI_CUDA(cudaEventRecord(ctx->main.ev0, ctx->main.stream));
-      for (auto &L : ctx->lanes) JSI_CUDA(cudaStreamWaitEvent(L->stream, ctx->main.ev0, 0));
+      JSI_CUDA(cudaEventCreate(&B.ev0));
+      JSI_CUDA(cudaEventRecord(B.ev0, ctx->main.stream));
       return JSI_OK;
     });
     if (st != JSI_OK) return st;
   }
   const bool lockstep = ctx->batch_chunk > 0 && p.k >= 1 && p.k <= kBatchK && p.rounds >= 1 &&
                         p.rounds <= kBatchRounds;
+  auto job_of = [&](jsi_ticket t) {
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    auto it = ctx->jobs.find(t);
+    return it != ctx->jobs.end() ? it->second : std::shared_ptr<Job>();
+  };
   if (lockstep) {
     // Group by shape: first-round nuv and basis stride of both sides.
     std::map<std::array<int, 4>, std::vector<int>> groups;
@@ -3148,9 +3195,10 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
           for (int u = s0; u < std::min(m, s0 + per); ++u) set_status(g.second[u], st);
           continue;
         }
-        tickets.push_back(t);
-        solo.push_back(-1);
-        batch_jobs.push_back(job);
+        B.tickets.push_back(t);
+        B.solo.push_back(-1);
+        B.batch_jobs.push_back(job);
+        B.all_jobs.push_back(job);
       }
     }
   } else {
@@ -3161,18 +3209,43 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
         set_status(q, st);
         continue;
       }
-      tickets.push_back(t);
-      solo.push_back(q);
+      B.tickets.push_back(t);
+      B.solo.push_back(q);
+      if (auto j = job_of(t)) B.all_jobs.push_back(j);
     }
   }
+  {
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    *ticket = ctx->next_ticket++;
+    ctx->batches[*ticket] = std::move(pb);
+  }
+  return JSI_OK;
+}
+
+int jsi_wait_distance_batch(jsi_context *ctx, jsi_ticket ticket, float *device_ms) {
+  if (!ctx) return JSI_ERR_INVALID;
+  std::unique_ptr<PendingBatch> pb;
+  {
+    std::lock_guard<std::mutex> lk(ctx->qmu);
+    auto it = ctx->batches.find(ticket);
+    if (it == ctx->batches.end()) return record(ctx, JSI_ERR_INVALID, "unknown batch ticket");
+    pb = std::move(it->second);
+    ctx->batches.erase(it);
+  }
+  PendingBatch &B = *pb;
+  jsi_dist_result *out = B.out;
+  auto set_status = [&](int q, int st) {
+    if (B.status) B.status[q] = st;
+    if (st != JSI_OK && B.first_err == JSI_OK) B.first_err = st;
+  };
   size_t bj = 0;
-  for (size_t w = 0; w < tickets.size(); ++w) {
-    if (solo[w] >= 0) {
-      set_status(solo[w], jsi_wait(ctx, tickets[w], -1, &out[solo[w]], nullptr));
+  for (size_t w = 0; w < B.tickets.size(); ++w) {
+    if (B.solo[w] >= 0) {
+      set_status(B.solo[w], jsi_wait(ctx, B.tickets[w], -1, &out[B.solo[w]], nullptr));
       continue;
     }
-    const int st = jsi_wait(ctx, tickets[w], -1, nullptr, nullptr);
-    Job &job = *batch_jobs[bj++];
+    const int st = jsi_wait(ctx, B.tickets[w], -1, nullptr, nullptr);
+    Job &job = *B.batch_jobs[bj++];
     for (auto &it : job.items) {
       const int q = static_cast<int>(it.out - out);
       const int sq = st != JSI_OK ? st : it.status;
@@ -3183,20 +3256,30 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
       }
     }
   }
+  // Device span: from the start event to the last job's end (each job's end
+  // event is recorded on its lane's stream after its work).
   std::lock_guard<std::mutex> lk(ctx->mu);
   const int st = guarded(ctx, [&]() {
-    for (auto &L : ctx->lanes) {
-      JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
-      JSI_CUDA(cudaStreamWaitEvent(ctx->main.stream, L->ev1, 0));
+    float span = 0.0f;
+    for (auto &j : B.all_jobs) {
+      if (!j->end_ev) continue;
+      JSI_CUDA(cudaEventSynchronize(j->end_ev));
+      float ms = 0.0f;
+      JSI_CUDA(cudaEventElapsedTime(&ms, B.ev0, j->end_ev));
+      span = std::max(span, ms);
     }
-    JSI_CUDA(cudaEventRecord(ctx->main.ev1, ctx->main.stream));
-    JSI_CUDA(cudaEventSynchronize(ctx->main.ev1));
-    float ms = 0.0f;
-    JSI_CUDA(cudaEventElapsedTime(&ms, ctx->main.ev0, ctx->main.ev1));
-    if (device_ms) *device_ms = ms;
+    if (device_ms) *device_ms = span;
     return JSI_OK;
   });
-  return first_err != JSI_OK ? first_err : st;
+  return B.first_err != JSI_OK ? B.first_err : st;
+}
+
+int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
+                           const jsi_dist_params *params, jsi_dist_result *out, int *status, float *device_ms) {
+  jsi_ticket t = 0;
+  const int st = jsi_submit_distance_batch(ctx, n, a, b, params, out, status, &t);
+  if (st != JSI_OK) return st;
+  return jsi_wait_distance_batch(ctx, t, device_ms);
 }
 
 }  // extern "C"

@@ -198,6 +198,31 @@ def test_bulk_domains_tasks_release():
             ctx.surface_domains(ids[:1])
 
 
+def test_submit_wait_overlapping_batches():
+    """Two batches in flight: the second's surfaces are uploaded after the
+    first is submitted; each equals the same batch run synchronously."""
+    import jsi_cad_next_versions_b200 as J
+    first, second = _sine_pairs(5, seed0=1400), _hard_wave_pairs(3, seed0=1500)
+    with J.Context(0) as ctx:
+        ctx.workers(2)
+        try:
+            h = []
+            for pairs, nuv in ((first, 40), (second, 144)):
+                ids = np.asarray(ctx.upload_many([x for pr in pairs for x in pr]), np.int32)
+                dom = ctx.surface_domains(ids)
+                tb = J.TaskBatch.from_arrays(ids[0::2], dom[0::2], nuv, ids[1::2], dom[1::2], nuv)
+                h.append((tb, ctx.submit_distance_batch(tb, precision="fp32_screen", trace=True)))
+            got = [ctx.wait_distance_batch(x)[0] for _, x in reversed(h)][::-1]
+            for (tb, _), g in zip(h, got):
+                ref, _ = ctx.min_distance_batch(tb, precision="fp32_screen", trace=True)
+                for a, b in zip(ref, g):
+                    _same(b, a)
+            with pytest.raises(J.JsiError):
+                ctx.wait_distance_batch(h[0][1])  # already waited for
+        finally:
+            ctx.workers(0)
+
+
 def test_upload_many_release_reuse():
     """Surfaces uploaded in one call, released, and other surfaces uploaded
     into the recycled device blocks: every query sees its own surfaces."""
