@@ -456,6 +456,8 @@ def run_ours(args):
         "screen": {"pair_tests_per_round": [int(x) for x in last.pair_tests],
                    "candidates_per_round": [int(x) for x in last.candidates],
                    "tile_pairs_per_round": [int(x) for x in last.tile_pairs],
+                   "tile_pairs_tested_per_round": [int(x) for x in last.tile_pairs_tested],
+                   "supertile_pairs_per_round": [int(x) for x in last.supertile_pairs],
                    "kept_per_round": [int(x) for x in last.npairs]},
         "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
         "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kt.items()},

@@ -151,6 +151,8 @@ typedef struct {
   long long trace_cap; /* capacity in triples; needs rounds*k */
   float device_ms;     /* device time of the query (CUDA events) */
   long long tile_pairs[JSI_MAX_ROUNDS]; /* tile pairs that passed the bound screen per round */
+  long long tile_pairs_tested[JSI_MAX_ROUNDS]; /* tile pairs whose bound (or representative) was evaluated */
+  long long supertile_pairs[JSI_MAX_ROUNDS];   /* supertile pairs that passed their bound (two-level rounds) */
 } jsi_dist_result;
 
 void jsi_dist_params_default(jsi_dist_params *p);

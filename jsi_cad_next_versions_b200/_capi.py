@@ -60,7 +60,8 @@ class DistResult(ctypes.Structure):
                 ("kth_d2", ctypes.c_double * MAX_ROUNDS), ("pair_tests", ctypes.c_longlong * MAX_ROUNDS),
                 ("candidates", ctypes.c_longlong * MAX_ROUNDS), ("trace_pairs", ctypes.POINTER(ctypes.c_int)),
                 ("trace_cap", ctypes.c_longlong), ("device_ms", ctypes.c_float),
-                ("tile_pairs", ctypes.c_longlong * MAX_ROUNDS)]
+                ("tile_pairs", ctypes.c_longlong * MAX_ROUNDS), ("tile_pairs_tested", ctypes.c_longlong * MAX_ROUNDS),
+                ("supertile_pairs", ctypes.c_longlong * MAX_ROUNDS)]
 
 
 class InterParams(ctypes.Structure):

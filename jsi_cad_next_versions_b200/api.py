@@ -49,6 +49,8 @@ class DistanceResult:
     device_ms: float
     pairs: list = field(default_factory=list)  # per round (n, 3) int32 (slot, i, j) if traced
     tile_pairs: np.ndarray = None  # tile pairs that passed the bound screen, per round
+    tile_pairs_tested: np.ndarray = None  # tile pairs whose bound or representative was evaluated, per round
+    supertile_pairs: np.ndarray = None  # supertile pairs that passed their bound, per round
 
 
 def _struct_dtype(st) -> np.dtype:
@@ -318,7 +320,9 @@ class Context:
             uv1=tuple(r.uv1), uv2=tuple(r.uv2), point1=tuple(r.point1), point2=tuple(r.point2), rounds=n,
             npairs=npairs, kth_d2=np.array(r.kth_d2[:n]), pair_tests=np.array(r.pair_tests[:n], dtype=np.int64),
             candidates=np.array(r.candidates[:n], dtype=np.int64), device_ms=r.device_ms, pairs=pairs,
-            tile_pairs=np.array(r.tile_pairs[:n], dtype=np.int64))
+            tile_pairs=np.array(r.tile_pairs[:n], dtype=np.int64),
+            tile_pairs_tested=np.array(r.tile_pairs_tested[:n], dtype=np.int64),
+            supertile_pairs=np.array(r.supertile_pairs[:n], dtype=np.int64))
 
     def min_distance(self, a: C.Task, b: C.Task, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
                      precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False) -> DistanceResult:

@@ -1126,6 +1126,8 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
     out->pair_tests[round - 1] = tests;
     out->candidates[round - 1] = cands;
     out->tile_pairs[round - 1] = static_cast<long long>(ctx->h_stats->survivors);
+    out->tile_pairs_tested[round - 1] = static_cast<long long>(ctx->h_stats->tile_pairs);
+    out->supertile_pairs[round - 1] = static_cast<long long>(ctx->h_stats->st_survivors);
     if (n > 0) {
       JSI_CUDA(copy_async(ctx, htop.data(), top, sizeof(DistCand<TP>) * n, cudaMemcpyDeviceToHost, st));
       JSI_CUDA(cudaStreamSynchronize(st));
@@ -1610,6 +1612,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       out->pair_tests[round - 1] = rec.tests[round - 1];
       out->candidates[round - 1] = rec.cands[round - 1];
       out->tile_pairs[round - 1] = static_cast<long long>(rec.survivors[round - 1]);
+      out->tile_pairs_tested[round - 1] = static_cast<long long>(rec.examined[round - 1]);
+      out->supertile_pairs[round - 1] = static_cast<long long>(rec.st_kept[round - 1]);
       out->kth_d2[round - 1] = np > 0 ? static_cast<double>(rec.top[round - 1][np - 1].d2) : 0.0;
       if (np > 0 && out->trace_pairs && static_cast<long long>(round) * p.k <= out->trace_cap) {
         for (int e2 = 0; e2 < np; ++e2) {

@@ -166,6 +166,8 @@ struct DistRecord {
   long long tests[kBatchRounds];
   long long cands[kBatchRounds];
   unsigned long long survivors[kBatchRounds];
+  unsigned long long examined[kBatchRounds];  // tile pairs whose bound or representative was evaluated
+  unsigned long long st_kept[kBatchRounds];   // supertile pairs that passed their bound
   int npairs[kBatchRounds];
   int status[kBatchRounds];
   DistCand<TP> top[kBatchRounds][kBatchK];

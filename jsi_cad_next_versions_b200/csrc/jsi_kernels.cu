@@ -810,17 +810,17 @@ __global__ void __launch_bounds__(256) k_dist_tau(SideRound<T> a, SideRound<T> b
   const Geom g1 = a.g, g2 = b.g;
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
   const int nrows = nslots * g1.ntiles;
-  float best = __uint_as_float(0x7f800000u);
+  T best = pos_inf<T>();  // smallest pair d2; thr_bits is monotone, so it is applied once per fold
   for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
     const int slot = row / g1.ntiles, t1 = row - slot * g1.ntiles;
     const Vec4<T> c1 = a.center[(static_cast<long long>(map1[slot]) * g1.ntiles + t1) * n1 + tile_rep(t1, g1)];
     const long long base2 = static_cast<long long>(map2[slot]) * g2.ntiles;
     for (int t2 = threadIdx.x; t2 < g2.ntiles; t2 += blockDim.x) {
       const Vec4<T> c2 = b.center[(base2 + t2) * n2 + tile_rep(t2, g2)];
-      best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+      best = tmin(best, pair_d2<T, S>(c1, c2));
     }
   }
-  fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+  fold_tau(thr_bits<T, S>(best, e), k, &stats->tau_bits, sh);
 }
 
 // Tile pairs whose box-gap bound does not exceed tau survive, with the bound
@@ -1133,6 +1133,46 @@ __device__ __forceinline__ long long super_rep(int r, int st, const Geom &g) {
   return (static_cast<long long>(r) * g.ntiles + t) * (g.te * g.te) + tile_rep(t, g);
 }
 
+// The warp's 32 values sorted ascending across the lanes (bitonic network):
+// lane i receives the i-th smallest.
+template <typename T>
+__device__ __forceinline__ T warp_sort_asc(T v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const T o = __shfl_xor_sync(kFull, v, stride);
+      const bool asc = (lane & size) == 0 || size == 32;
+      const bool low = (lane & stride) == 0;
+      v = (low == asc) ? (o < v ? o : v) : (o < v ? v : o);
+    }
+  }
+  return v;
+}
+
+// Representative cell of a supertile's tile (ry, rx) of an R x R grid of
+// representatives, R clamped to the supertile's own tile counts so that the
+// representatives are distinct tiles (ragged supertiles at the grid's edge).
+__device__ __forceinline__ long long super_rep_at(int r, int st, const Geom &g, int R, int ry, int rx, bool &valid) {
+  const int sy = st / g.stw, sx = st - (st / g.stw) * g.stw;
+  const int nty = min(kMaxTile, g.tw - sy * kMaxTile), ntx = min(kMaxTile, g.tw - sx * kMaxTile);
+  const int Ry = min(R, nty), Rx = min(R, ntx);
+  valid = ry < Ry && rx < Rx;
+  const int ty = (2 * ry + 1) * nty / (2 * Ry), tx = (2 * rx + 1) * ntx / (2 * Rx);
+  const int t = (sy * kMaxTile + min(ty, nty - 1)) * g.tw + sx * kMaxTile + min(tx, ntx - 1);
+  return (static_cast<long long>(r) * g.ntiles + t) * (g.te * g.te) + tile_rep(t, g);
+}
+
+// Threshold seed of the two-level screen.  k <= kStKL: each supertile
+// contributes an R x R grid of representative cells (R = kStR), and each
+// lane keeps the k smallest representative-pair d2 it computes in a sorted
+// register list; every warp folds the exact k-th of its lanes' lists (k
+// distinct cell pairs) into tau.  Larger k: one representative per
+// supertile and the block k-th of thread minima.
+constexpr int kStR = 2;
+constexpr int kStKL = 8;
+
 template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_dist_tau_st(SideRound<T> a, SideRound<T> b, const int *map1,
                                                      const int *map2, int nslots, int k, ScreenStats *stats, float e,
@@ -1147,16 +1187,79 @@ __global__ void __launch_bounds__(256) k_dist_tau_st(SideRound<T> a, SideRound<T
   nslots = nslots_of(nslots, stats);
   const Geom g1 = a.g, g2 = b.g;
   const int nrows = nslots * g1.nst;
-  float best = __uint_as_float(0x7f800000u);
-  for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+  if (k > kStKL) {
+    T best = pos_inf<T>();  // smallest pair d2; thr_bits is monotone, so it is applied once per fold
+    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+      const int slot = row / g1.nst, s1 = row - slot * g1.nst;
+      const Vec4<T> c1 = a.center[super_rep(map1[slot], s1, g1)];
+      for (int s2 = threadIdx.x; s2 < g2.nst; s2 += blockDim.x) {
+        const Vec4<T> c2 = b.center[super_rep(map2[slot], s2, g2)];
+        best = tmin(best, pair_d2<T, S>(c1, c2));
+      }
+    }
+    fold_tau(thr_bits<T, S>(best, e), k, &stats->tau_bits, sh);
+    return;
+  }
+  constexpr int R2 = kStR * kStR;
+  const Vec4<T> far4{pos_inf<T>(), pos_inf<T>(), pos_inf<T>(), T(0)};
+  T L[kStKL];
+#pragma unroll
+  for (int q = 0; q < kStKL; ++q) L[q] = pos_inf<T>();
+  // Supertile pairs (row, s2) over every thread of the query's blocks.
+  const long long npairs = static_cast<long long>(nrows) * g2.nst;
+  for (long long pr = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; pr < npairs;
+       pr += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int row = static_cast<int>(pr / g2.nst), s2 = static_cast<int>(pr - static_cast<long long>(row) * g2.nst);
     const int slot = row / g1.nst, s1 = row - slot * g1.nst;
-    const Vec4<T> c1 = a.center[super_rep(map1[slot], s1, g1)];
-    for (int s2 = threadIdx.x; s2 < g2.nst; s2 += blockDim.x) {
-      const Vec4<T> c2 = b.center[super_rep(map2[slot], s2, g2)];
-      best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(c1, c2), e)));
+    Vec4<T> c1[R2];
+#pragma unroll
+    for (int i = 0; i < R2; ++i) {
+      bool v;
+      const long long idx = super_rep_at(map1[slot], s1, g1, kStR, i / kStR, i % kStR, v);
+      c1[i] = v ? a.center[idx] : far4;
+    }
+#pragma unroll
+    for (int j = 0; j < R2; ++j) {
+      bool v;
+      const long long idx = super_rep_at(map2[slot], s2, g2, kStR, j / kStR, j % kStR, v);
+      if (!v) continue;
+      const Vec4<T> c2 = b.center[idx];
+#pragma unroll
+      for (int i = 0; i < R2; ++i) {
+        const T x = pair_d2<T, S>(c1[i], c2);  // +inf for an absent representative
+        if (x < L[kStKL - 1]) {
+#pragma unroll
+          for (int q = kStKL - 1; q >= 1; --q) L[q] = (x < L[q - 1]) ? L[q - 1] : ((x < L[q]) ? x : L[q]);
+          L[0] = (x < L[0]) ? x : L[0];
+        }
+      }
     }
   }
-  fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+  // Block merge: each warp pops its k smallest (k rounds of warp minimum
+  // over the list heads) into shared memory; warp 0 takes the exact k-th of
+  // the block's 8 x k values (two sorted halves of 32, then the k smallest
+  // of their first 16 each) and folds it.
+  __shared__ T s_top[8 * kStKL];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int r = 0; r < kStKL; ++r) {
+    T m = L[0];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = tmin(m, __shfl_xor_sync(kFull, m, o));
+    const unsigned owner = __ballot_sync(kFull, L[0] == m);
+    if (lane == __ffs(owner) - 1) {
+#pragma unroll
+      for (int q = 0; q < kStKL - 1; ++q) L[q] = L[q + 1];
+      L[kStKL - 1] = pos_inf<T>();
+    }
+    if (lane == 0) s_top[warp * kStKL + r] = r < k ? m : pos_inf<T>();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const T s0 = warp_sort_asc(s_top[lane]), s1 = warp_sort_asc(s_top[lane + 32]);
+    const T y0 = __shfl_sync(kFull, s0, lane & 15), y1 = __shfl_sync(kFull, s1, lane & 15);
+    const T kth = __shfl_sync(kFull, warp_sort_asc(lane < 16 ? y0 : y1), k - 1);
+    if (lane == 0 && kth != pos_inf<T>()) atomicMin(&stats->tau_bits, thr_bits<T, S>(kth, e));
+  }
 }
 
 template <typename T, bool S>
@@ -1247,7 +1350,7 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
   const int n1 = g1.te * g1.te, n2 = g2.te * g2.te;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  float best = __uint_as_float(0x7f800000u);
+  T best = pos_inf<T>();  // smallest pair d2; thr_bits is monotone, so it is applied once per fold
   for (unsigned long long w = static_cast<unsigned long long>(blockIdx.x) * kW + warp; w < nst_surv;
        w += static_cast<unsigned long long>(gridDim.x) * kW) {
     const unsigned long long q = st_surv[w];
@@ -1313,7 +1416,7 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
         i1 = __float2int_rz((static_cast<float>(c) + 0.5f) * inv);
         i2 = c - i1 * m2;
         if (!cull) {
-          best = fminf(best, __uint_as_float(thr_bits<T, S>(pair_d2<T, S>(s_p[warp][0][i1], s_p[warp][1][i2]), e)));
+          best = tmin(best, pair_d2<T, S>(s_p[warp][0][i1], s_p[warp][1][i2]));
         } else {
           lb = shaved_lb<T, S>(s_p[warp][0][i1], s_q[warp][0][i1], s_p[warp][1][i2], s_q[warp][1][i2]);
           keep = lb <= tau;
@@ -1328,8 +1431,9 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
         }
       }
     }
+    if (lane == 0 && total > 0) atomicAdd(&stats->tile_pairs, static_cast<unsigned long long>(total));
     if (!cull && k <= 32) {
-      const unsigned mine = __float_as_uint(best);
+      const unsigned mine = thr_bits<T, S>(best, e);
       if (__popc(__ballot_sync(kFull, mine < taub)) >= k) {
         const unsigned kth = warp_sorted_at(mine, k - 1);
         if (lane == 0) atomicMin(&stats->tau_bits, kth);
@@ -1337,7 +1441,7 @@ __global__ void __launch_bounds__(128) k_dist_expand(SideRound<T> a, SideRound<T
     }
     __syncwarp();
   }
-  if (!cull && k > 32) fold_tau(__float_as_uint(best), k, &stats->tau_bits, sh);
+  if (!cull && k > 32) fold_tau(thr_bits<T, S>(best, e), k, &stats->tau_bits, sh);
 }
 
 // Total order of the top-k (distance_analysis.cu:226-231).
@@ -1649,11 +1753,14 @@ __global__ void k_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRe
   const int n = st == 0 ? stats->nsel : 0;
   if (t < n && t < kBatchK) rec->top[round][t] = top[t];
   const unsigned long long tests = stats->pair_tests, cands = stats->candidates, surv = stats->survivors;
+  const unsigned long long examined = stats->tile_pairs, st_kept = stats->st_survivors;
   __syncwarp();
   if (t == 0) {
     rec->tests[round] = static_cast<long long>(tests);
     rec->cands[round] = static_cast<long long>(cands);
     rec->survivors[round] = surv;
+    rec->examined[round] = examined;
+    rec->st_kept[round] = st_kept;
     rec->npairs[round] = n;
     rec->status[round] = st;
     stats->nslots = n;
