@@ -2703,15 +2703,13 @@ __device__ __forceinline__ Vec4<TC> band_point(const TC (&a)[4]) {
 // extreme is erased by the centre's trailing + 0, which also keeps every
 // centre off -0), so the centres and ranges carry the general loop's bits.
 template <typename TB, typename TC, int D, int NR, bool RAT>
-__device__ __forceinline__ void band_unit_fast(const SurfView<TC> &s, const SideRound<TB> &bs,
-                                               const SideRound<TC> &out, Vec4<TC> *S, const Vec4<TC> *NT,
+__device__ __forceinline__ void band_unit_fast(const SideRound<TC> &out, Vec4<TC> *S, const Vec4<TC> *NT,
                                                const TC (*coef)[8], int r, int ty, int tx0, int ntx, int nv,
-                                               int ncols, long long lu0, int cu0) {
+                                               int ncols, int cu0, int su, const TC (&Nu)[D + 1]) {
   constexpr int kP = D + 1;
   constexpr int te = kMaxTile, te2 = kMaxTile * kMaxTile;
   constexpr int kCols = kBandTiles * kMaxTile;  // 256 cell columns, 257 sample columns
   const Geom g = out.g;
-  const int p1 = g.p1max;
   const int tid = threadIdx.x;
   int col, a0, a1;
   if (tid < kCols) {
@@ -2724,15 +2722,6 @@ __device__ __forceinline__ void band_unit_fast(const SurfView<TC> &s, const Side
     if (a0 > nv) col = ncols;  // idle lane
   }
   if (col < ncols) {
-    const long long lu = lu0 + col;
-    const int su = bs.spans[lu];
-    const TB *Nb = bs.basis + lu * 3 * p1;
-    TC Nu[kP];
-#pragma unroll
-    for (int c = 0; c < kP; ++c) {
-      if constexpr (std::is_same<TB, TC>::value) Nu[c] = Nb[c];
-      else Nu[c] = __double2float_rn(Nb[c]);
-    }
     TC rs[NR][4];
     const Vec4<TC> *cp = NT + (su - D - cu0);
 #pragma unroll
@@ -2832,14 +2821,11 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 4) k_cells
   Vec4<TC> *S = reinterpret_cast<Vec4<TC> *>(band_raw);  // [kE][kBandCols]
   // The band's control-net tile: rows rmin.., columns cu0.. of the net.
   Vec4<TC> *NT = S + kE * kBandCols;                      // [kBandNetRows][kBandNetCols]
-  __shared__ int s_su[2];
-  __shared__ TC snv[kE][kBandRows];
   // v coefficients of each sample row over the band's net rows, zero outside
   // the row's degv + 1 window: adding 0 * (finite row sum) to an accumulator
   // that starts at +0 (and so is never -0) leaves it unchanged, so the padded
   // sum has the bits of the windowed one.
   __shared__ __align__(16) TC coef[kE][8];
-  __shared__ int ssv[kE];
   const long long qo = qoff(qs);
   if (vdev) s = *qsh(vdev, qo);
   bs = qsh(bs, qo);
@@ -2867,43 +2853,49 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 4) k_cells
     const long long lu0 = (static_cast<long long>(r) * 2 + 0) * g.nuv + tx0 * te;
     const long long lv0 = (static_cast<long long>(r) * 2 + 1) * g.nuv + ty * te;
     const bool fit = !s.zero && s.degu <= D && s.degv <= D;
-    if (fit && tid <= nv) {
-      ssv[tid] = bs.spans[lv0 + tid];
-      const TB *N = bs.basis + (lv0 + tid) * 3 * p1;
-      for (int c = 0; c <= s.degv; ++c) {
-        if constexpr (std::is_same<TB, TC>::value) snv[tid][c] = N[c];
-        else snv[tid][c] = __double2float_rn(N[c]);
-      }
-    }
-    // Spans are monotone along the band's sample columns: the first and last
-    // give the net columns the band reads.
-    if (fit && tid == 32) s_su[0] = bs.spans[lu0];
-    if (fit && tid == 64) s_su[1] = bs.spans[lu0 + ncols - 1];
-    __syncthreads();
-    int rmin = 0, nrows = kBandRows + 1;
+    int rmin = 0, nrows = kBandRows + 1, cu0 = 0, ncu = kBandNetCols + 1;
     if (fit) {
-      // Spans are monotone along the band's sample rows too: the end rows
-      // give the net rows the band reads.
-      const int lo = min(ssv[0], ssv[nv]), hi = max(ssv[0], ssv[nv]);
-      rmin = lo - s.degv;
-      nrows = hi - rmin + 1;
+      // Spans are monotone along the band's sample rows and columns: the end
+      // rows and columns give the net rows and columns the band reads.
+      const int v0 = bs.spans[lv0], v1 = bs.spans[lv0 + nv];
+      const int u0 = bs.spans[lu0], u1 = bs.spans[lu0 + ncols - 1];
+      rmin = min(v0, v1) - s.degv;
+      nrows = max(v0, v1) - rmin + 1;
+      cu0 = min(u0, u1) - s.degu;
+      ncu = max(u0, u1) + 1 - cu0;
     }
     const bool factored = fit && nrows <= kBandRows;
-    if (factored && tid < (nv + 1) * kBandRows) {
-      const int a = tid / kBandRows, R = tid - (tid / kBandRows) * kBandRows;
-      const int R0 = ssv[a] - s.degv - rmin;
-      coef[a][R] = (R >= R0 && R - R0 <= s.degv) ? snv[a][R - R0] : TC(0);
-    }
-    int cu0 = 0, ncu = kBandNetCols + 1;
-    if (factored) {
-      cu0 = min(s_su[0], s_su[1]) - s.degu;
-      ncu = max(s_su[0], s_su[1]) + 1 - cu0;
-    }
     const bool tiled = factored && ncu <= kBandNetCols;
     // Full-degree units take the fast path, over NR = D + 2 or D + 3 net
     // rows (rows past the band's own are zero-filled).
     const bool fast = tiled && s.degu == D && s.degv == D;
     const int nrf = nrows <= D + 2 ? D + 2 : D + 3;
+    // The fast path's column inputs (span and u basis of this thread's
+    // sample column; warp 8 shares column 256), loaded ahead of the barrier.
+    const int fcol = tid < kBandCols - 1 ? tid : kBandCols - 1;
+    int fsu = 0;
+    TC fNu[D + 1];
+    if (fast && fcol < ncols) {
+      fsu = bs.spans[lu0 + fcol];
+      const TB *Nb = bs.basis + (lu0 + fcol) * 3 * p1;
+#pragma unroll
+      for (int q = 0; q <= D; ++q) {
+        if constexpr (std::is_same<TB, TC>::value) fNu[q] = Nb[q];
+        else fNu[q] = __double2float_rn(Nb[q]);
+      }
+    }
+    // v coefficients of the band's sample rows over its net rows.
+    if (factored && tid < (nv + 1) * kBandRows) {
+      const int a = tid / kBandRows, R = tid - a * kBandRows;
+      const int q = R - (bs.spans[lv0 + a] - s.degv - rmin);
+      TC m = TC(0);
+      if (q >= 0 && q <= s.degv) {
+        const TB x = bs.basis[(lv0 + a) * 3 * p1 + q];
+        if constexpr (std::is_same<TB, TC>::value) m = x;
+        else m = __double2float_rn(x);
+      }
+      coef[a][R] = m;
+    }
     if (tiled) {
       const int nrs = fast ? nrf : nrows;
       for (int e = tid; e < nrs * ncu; e += blockDim.x) {
@@ -2916,14 +2908,14 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 4) k_cells
     if (fast) {
       if (s.rat) {
         if (nrf == D + 2)
-          band_unit_fast<TB, TC, D, D + 2, true>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+          band_unit_fast<TB, TC, D, D + 2, true>(out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, cu0, fsu, fNu);
         else
-          band_unit_fast<TB, TC, D, D + 3, true>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+          band_unit_fast<TB, TC, D, D + 3, true>(out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, cu0, fsu, fNu);
       } else {
         if (nrf == D + 2)
-          band_unit_fast<TB, TC, D, D + 2, false>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+          band_unit_fast<TB, TC, D, D + 2, false>(out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, cu0, fsu, fNu);
         else
-          band_unit_fast<TB, TC, D, D + 3, false>(s, bs, out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, lu0, cu0);
+          band_unit_fast<TB, TC, D, D + 3, false>(out, S, NT, coef, r, ty, tx0, ntx, nv, ncols, cu0, fsu, fNu);
       }
       __syncthreads();
       continue;
