@@ -735,8 +735,9 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
                 T span_v0, bool cover = false) {
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
-  timed(ctx, "basis", [&] { launch_basis(v, s, st, Batch{}, static_cast<const SurfView<T> *>(nullptr), cover); },
-        2.0 * s.nreg * s.g.nuv);
+  timed(ctx, "basis", [&] {
+    launch_basis(v, s, st, Batch{}, static_cast<const SurfView<T> *>(nullptr), cover, !intersect && !cover);
+  }, 2.0 * s.nreg * s.g.nuv);
   if (!intersect) {
     // Distance: centres straight from the basis tables, no sample grid.
     timed(ctx, "cells", [&] { launch_cells_fused(v, s, s, st); }, double(s.nreg) * s.g.W * s.g.W);
@@ -1114,7 +1115,9 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
         C.center = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.cpr);
         C.tlo = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
         C.thi = ar.get<Vec4<TC>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
-        timed(ctx, "basis", [&] { launch_basis(side ? pb : pa, P, st); }, 2.0 * P.nreg * P.g.nuv);
+        timed(ctx, "basis", [&] {
+          launch_basis(side ? pb : pa, P, st, Batch{}, static_cast<const SurfView<TP> *>(nullptr), false, true);
+        }, 2.0 * P.nreg * P.g.nuv);
         timed(ctx, "cells", [&] { launch_cells_fused(side ? cb : ca, P, C, st); }, double(C.nreg) * C.g.W * C.g.W);
       }
       auto verify = [&](const DistCand<TC> *c, long long m, DistCand<TP> *o) {
@@ -1477,8 +1480,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
       const bool scr = kScreen && r == 1;
       timed(L, "basis", [&] {
-        launch_basis(va, Rd.A, st, bt, head_view<TP>(lay.head, 0));
-        launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1));
+        launch_basis(va, Rd.A, st, bt, head_view<TP>(lay.head, 0), false, true);
+        launch_basis(vb, Rd.B, st, bt, head_view<TP>(lay.head, 1), false, true);
       });
       // Work units of the cell build: cells of both sides (exact in round 1,
       // where every query has one region per side; the refinement rounds'

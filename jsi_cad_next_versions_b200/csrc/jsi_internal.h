@@ -189,9 +189,11 @@ unsigned long long launch_count();  // kernels launched so far (all contexts)
 void add_launches(unsigned long long n);  // kernels a replayed CUDA graph launched
 // cover: sample the covering grid (nuv samples over the whole rectangle, the
 // last on its end) of the bounds mode instead of the reference's grid.
+// values_only: leave the derivative rows zero (the distance path reads the
+// basis values alone).
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt = Batch{},
-                  const SurfView<T> *vdev = nullptr, bool cover = false);
+                  const SurfView<T> *vdev = nullptr, bool cover = false, bool values_only = false);
 template <typename T>
 void launch_samples(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, cudaStream_t st,
                     const Batch &bt = Batch{}, const SurfView<T> *vdev = nullptr);

@@ -258,7 +258,8 @@ __device__ void basis_ders(int span, int p, T u, const T *knots, int nd, T *out,
 
 template <typename T, int MAXP>
 __global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<T> *regions, int nreg,
-                        const int *dnreg, int nuv, int p1max, int *spans, T *basis, long long qs, int cover) {
+                        const int *dnreg, int nuv, int p1max, int *spans, T *basis, long long qs, int cover,
+                        int max_ders) {
   const long long qo = qoff(qs);
   if (vdev) s = *qsh(vdev, qo);
   if (dnreg) nreg = *qsh(dnreg, qo);
@@ -283,7 +284,10 @@ __global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<
     const int p = dir ? s.degv : s.degu;
     const int nk = dir ? s.nkv : s.nku;
     const T *knots = dir ? s.V : s.U;
-    const int nd = dir ? s.dv : s.du;
+    // Derivative rows only where a caller reads them (the intersection's
+    // curvature padding); the distance path reads the values alone, and
+    // the derivative rows stay zero.
+    const int nd = min(dir ? s.dv : s.du, max_ders);
     T *out = basis + t * 3 * p1max;
     if (s.zero) {
       spans[t] = p;
@@ -3460,17 +3464,18 @@ inline dim3 bdim(int gx, const Batch &bt) { return dim3(static_cast<unsigned>(gx
 
 template <typename T>
 void launch_basis(const SurfView<T> &s, const SideRound<T> &sr, cudaStream_t st, const Batch &bt,
-                  const SurfView<T> *vdev, bool cover) {
+                  const SurfView<T> *vdev, bool cover, bool values_only) {
+  const int md = values_only ? 0 : 2;
   counted();
   const long long n = static_cast<long long>(sr.nreg) * 2 * sr.g.nuv;
   // Degrees are part of a batch's shape: the host view decides the variant.
   const int maxdeg = s.degu > s.degv ? s.degu : s.degv;
   if (maxdeg < 8)
     k_basis<T, 9><<<bdim(bgrid((n + 127) / 128, bt, 148 * 16), bt), 128, 0, st>>>(
-        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs, cover ? 1 : 0);
+        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs, cover ? 1 : 0, md);
   else
     k_basis<T, kMaxDeg + 1><<<bdim(bgrid((n + 63) / 64, bt, 148 * 16), bt), 64, 0, st>>>(
-        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs, cover ? 1 : 0);
+        s, vdev, sr.regions, sr.nreg, sr.dnreg, sr.g.nuv, sr.g.p1max, sr.spans, sr.basis, bt.qs, cover ? 1 : 0, md);
 }
 
 template <typename T>
@@ -3849,7 +3854,7 @@ void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb,
 
 #define JSI_INSTANTIATE(T)                                                                                        \
   template void launch_basis<T>(const SurfView<T> &, const SideRound<T> &, cudaStream_t, const Batch &,           \
-                                const SurfView<T> *, bool);                                                       \
+                                const SurfView<T> *, bool, bool);                                                 \
   template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t, const Batch &,   \
                                   const SurfView<T> *);                                                           \
   template void launch_pad<T>(const SideRound<T> &, bool, T, T, cudaStream_t);                                    \
