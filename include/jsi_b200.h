@@ -309,8 +309,8 @@ int jsi_queue_depth(jsi_context *ctx, int *queued, int *running);
 /* n distance queries over the worker lanes; status[q] (may be null) gets each
  * query's status, device_ms (may be null) the device span of the batch
  * (CUDA events).  Returns the first error, else JSI_OK.
- * With k <= 8 and rounds <= 8, queries of one shape (first-round nuv and
- * degrees of both sides) run in lockstep batches of up to jsi_batch_chunk
+ * With k <= 8 and rounds <= 8, queries of one shape (first-round nuv,
+ * degrees and rational flag of both sides) run in lockstep batches of up to jsi_batch_chunk
  * queries per lane: one launch per stage for the whole batch, counts kept on
  * the device, one copy in and one copy out per batch.  Results are the same
  * as the per-query path's; a query whose internal lists overflow is re-run
@@ -334,8 +334,8 @@ int jsi_batch_reruns(jsi_context *ctx, long long *out);
 /* Autotuner of the lockstep batches: times jsi_min_distance_batch on the n
  * given queries (all of one shape) for chunk sizes 8, 16, 32, ... up to the
  * per-lane share of n, with the lanes as configured, and keeps the fastest for
- * queries of that shape (first-round nuv and degrees of both sides, k,
- * rounds, precision); later batches of the shape use it.  chunk_out / ms_out
+ * queries of that shape (first-round nuv, degrees and rational flag of both
+ * sides, k, rounds, precision); later batches of the shape use it.  chunk_out / ms_out
  * (may be null) get the choice and its batch device time. */
 int jsi_autotune_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
                        int *chunk_out, float *ms_out);

@@ -440,6 +440,10 @@ SurfView<double> view<double>(const SurfaceRec &s) {
 
 int p1_of(const SurfaceRec &s) { return std::max(s.ivec[1], s.ivec[4]) + 1; }
 
+// What of a surface decides the kernels of a lockstep batch: both degrees,
+// the rational flag and the zero flag (all queries of a batch share it).
+int shape_of(const SurfaceRec &s) { return s.ivec[1] | (s.ivec[4] << 8) | (s.rat << 16) | (s.zero << 17); }
+
 // Header validation.  Degrees >= 25 and non-flat surfaces with flags bits 2|3
 // are accepted and evaluate to zero records, as the reference does
 // (evaluation.cu:271-272).
@@ -1445,7 +1449,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
   for (int q = 0; q < n; ++q) {
     const SurfaceRec &sa = get_surface(L, items[q].a->surface);
     const SurfaceRec &sb = get_surface(L, items[q].b->surface);
-    if (p1_of(sa) != p1a || p1_of(sb) != p1b || items[q].a->nuv != nuv1 || items[q].b->nuv != nuv2)
+    if (shape_of(sa) != shape_of(s0a) || shape_of(sb) != shape_of(s0b) || items[q].a->nuv != nuv1 ||
+        items[q].b->nuv != nuv2)
       fail(JSI_ERR_INVALID, "batch items differ in shape");
     DistHead<TP> h{};
     h.a64 = view<double>(sa);
@@ -3062,11 +3067,11 @@ int jsi_autotune_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_tas
       validate_dist(p, &a[0], &b[0]);
       auto ia = ctx->surfaces.find(a[0].surface), ib = ctx->surfaces.find(b[0].surface);
       if (ia == ctx->surfaces.end() || ib == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
-      shape = {a[0].nuv, b[0].nuv, p1_of(ia->second), p1_of(ib->second)};
+      shape = {a[0].nuv, b[0].nuv, shape_of(ia->second), shape_of(ib->second)};
       for (int q = 1; q < n; ++q) {
         auto qa = ctx->surfaces.find(a[q].surface), qb = ctx->surfaces.find(b[q].surface);
         if (qa == ctx->surfaces.end() || qb == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
-        const std::array<int, 4> s2 = {a[q].nuv, b[q].nuv, p1_of(qa->second), p1_of(qb->second)};
+        const std::array<int, 4> s2 = {a[q].nuv, b[q].nuv, shape_of(qa->second), shape_of(qb->second)};
         if (s2 != shape) fail(JSI_ERR_INVALID, "autotune queries differ in shape");
       }
       return JSI_OK;
@@ -3154,7 +3159,7 @@ int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const 
     return it != ctx->jobs.end() ? it->second : std::shared_ptr<Job>();
   };
   if (lockstep) {
-    // Group by shape: first-round nuv and basis stride of both sides.
+    // Group by shape: first-round nuv, degrees, rational and zero flags of both sides.
     std::map<std::array<int, 4>, std::vector<int>> groups;
     for (int q = 0; q < n; ++q) {
       std::string err;
@@ -3164,7 +3169,7 @@ int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const 
         std::lock_guard<std::mutex> lk(ctx->mu);
         auto ia = ctx->surfaces.find(a[q].surface), ib = ctx->surfaces.find(b[q].surface);
         if (ia == ctx->surfaces.end() || ib == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
-        key = {a[q].nuv, b[q].nuv, p1_of(ia->second), p1_of(ib->second)};
+        key = {a[q].nuv, b[q].nuv, shape_of(ia->second), shape_of(ib->second)};
       });
       if (st != JSI_OK) {
         set_status(q, st);

@@ -3082,6 +3082,219 @@ __global__ void __launch_bounds__(kBandThreads, sizeof(TC) == 8 ? 2 : 4) k_cells
   }
 }
 
+// Distance cells of large grids, one warp per unit of 4 tiles (32 cell
+// columns, 33 sample columns) of one band of 8 cell rows, every warp on its
+// own: no block barrier anywhere.  The host picks this kernel when the
+// degrees of the whole launch are known and equal (D = 2 or 3) and passes
+// them, and the rational flag, as template arguments.
+//
+// Samples (factored, as in band_unit_fast): lane c owns sample column c
+// (c < 32) and forms the u-direction sums of the band's NR net rows from its
+// u span and basis (control points straight from L1), then every sample of
+// its column in v; the last column (32) goes to lanes 0..nv, one sample
+// row each, each lane forming the column's row sums itself (the same
+// operations, so the same bits).  A unit whose band needs more than D + 3
+// net rows evaluates its samples one by one (eval_point / screen_point,
+// again the same bits).  Cells: as in band_unit_fast, lane c owns cell
+// column c of the unit.
+constexpr int kWT = 4;               // tiles per warp unit
+constexpr int kWC = kWT * kMaxTile;  // cell columns per warp unit (one per lane)
+constexpr int kWS = kWC + 1;         // sample columns per warp unit
+constexpr int kWWarps = 8;           // warps per block
+
+template <typename TC>
+struct BandWarpSmem {
+  Vec4<TC> S[kMaxTile + 1][kWS];
+  TC coef[kMaxTile + 1][8];
+};
+
+template <typename TC>
+constexpr size_t bandw_smem() {
+  return sizeof(BandWarpSmem<TC>) * kWWarps;
+}
+
+// Samples of sample column col, rows a0..a1 (factored).
+template <typename TB, typename TC, int D, int NR, bool RAT>
+__device__ __forceinline__ void bandw_column(BandWarpSmem<TC> &w, const SurfView<TC> &s, const SideRound<TB> &bs,
+                                             long long lu0, int col, int a0, int a1, int rmin, int nrows, int p1) {
+  constexpr int kP = D + 1;
+  const long long lu = lu0 + col;
+  const int su = bs.spans[lu];
+  const TB *Nb = bs.basis + lu * 3 * p1;
+  TC Nu[kP];
+#pragma unroll
+  for (int c = 0; c < kP; ++c) {
+    if constexpr (std::is_same<TB, TC>::value) Nu[c] = Nb[c];
+    else Nu[c] = __double2float_rn(Nb[c]);
+  }
+  TC rs[NR][4];
+#pragma unroll
+  for (int R = 0; R < NR; ++R) {
+    TC acc[4] = {TC(0), TC(0), TC(0), TC(0)};
+    if (R < nrows) {
+      const Vec4<TC> *cp = s.cpw + static_cast<long long>(s.ncpu) * (rmin + R) + (su - D);
+#pragma unroll
+      for (int c = 0; c < kP; ++c) band_row_sum<TB, TC, RAT>(Nu[c], cp[c], acc);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rs[R][k] = acc[k];
+  }
+  for (int a = a0; a <= a1; ++a) {
+    TC m[NR];
+    if constexpr (sizeof(TC) == 4) {
+      const float4 v0 = *reinterpret_cast<const float4 *>(&w.coef[a][0]);
+      m[0] = v0.x;
+      m[1] = v0.y;
+      m[2] = v0.z;
+      m[3] = v0.w;
+      if constexpr (NR > 4) {
+        const float2 v1 = *reinterpret_cast<const float2 *>(&w.coef[a][4]);
+        m[4] = v1.x;
+        if constexpr (NR > 5) m[5] = v1.y;
+      }
+    } else {
+#pragma unroll
+      for (int R = 0; R < NR; ++R) m[R] = w.coef[a][R];
+    }
+    TC acc[4] = {TC(0), TC(0), TC(0), TC(0)};
+#pragma unroll
+    for (int R = 0; R < NR; ++R) band_v_acc<TB, TC, RAT>(m[R], rs[R], acc);
+    w.S[a][col] = band_point<TB, TC, RAT>(acc);
+  }
+}
+
+template <typename TB, typename TC, int D, int NR, bool RAT>
+__device__ __forceinline__ void bandw_samples(BandWarpSmem<TC> &w, const SurfView<TC> &s, const SideRound<TB> &bs,
+                                              long long lu0, long long lv0, int nv, int ncols, int rmin, int nrows,
+                                              int p1, int lane) {
+  // v coefficients of the band's sample rows over its net rows, zero outside
+  // each row's window (see k_cells_band).
+  for (int idx = lane; idx < (nv + 1) * 8; idx += 32) {
+    const int a = idx >> 3, R = idx & 7;
+    TC m = TC(0);
+    if (R < NR) {
+      const int q = R - (bs.spans[lv0 + a] - D - rmin);
+      if (q >= 0 && q <= D) {
+        const TB x = bs.basis[(lv0 + a) * 3 * p1 + q];
+        if constexpr (std::is_same<TB, TC>::value) m = x;
+        else m = __double2float_rn(x);
+      }
+    }
+    w.coef[a][R] = m;
+  }
+  __syncwarp();
+  if (lane < ncols) bandw_column<TB, TC, D, NR, RAT>(w, s, bs, lu0, lane, 0, nv, rmin, nrows, p1);
+  if (ncols > kWC && lane <= nv) bandw_column<TB, TC, D, NR, RAT>(w, s, bs, lu0, kWC, lane, lane, rmin, nrows, p1);
+}
+
+template <typename TB, typename TC, int D, bool RAT>
+__global__ void __launch_bounds__(kWWarps * 32, sizeof(TC) == 8 ? 2 : 4)
+    k_cells_bandw(SurfView<TC> s, const SurfView<TC> *vdev, SideRound<TB> bs, SideRound<TC> out, long long qs) {
+  extern __shared__ __align__(16) unsigned char bandw_raw[];
+  const long long qo = qoff(qs);
+  if (vdev) s = *qsh(vdev, qo);
+  bs = qsh(bs, qo);
+  out = qsh(out, qo);
+  const Geom g = out.g;
+  constexpr int te = kMaxTile, te2 = kMaxTile * kMaxTile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  BandWarpSmem<TC> &w = reinterpret_cast<BandWarpSmem<TC> *>(bandw_raw)[warp];
+  const int p1 = g.p1max;
+  const int nwc = (g.tw + kWT - 1) / kWT;
+  const int per_reg = g.tw * nwc;
+  const int nunits = nreg_of(bs) * per_reg;
+  for (int unit = blockIdx.x * kWWarps + warp; unit < nunits; unit += gridDim.x * kWWarps) {
+    const int r = unit / per_reg;
+    const int rest = unit - r * per_reg;
+    const int ty = rest / nwc, wc = rest - ty * nwc;
+    const int tx0 = wc * kWT, ntx = min(kWT, g.tw - tx0);
+    const int nv = min(te, g.W - ty * te);
+    const int ncols = min(kWC, g.W - tx0 * te) + 1;
+    const long long lu0 = (2LL * r) * g.nuv + tx0 * te;
+    const long long lv0 = (2LL * r + 1) * g.nuv + ty * te;
+    // Spans are monotone along the band's sample rows: the end rows give the
+    // net rows the band reads.
+    const int v0 = bs.spans[lv0], v1 = bs.spans[lv0 + nv];
+    const int rmin = min(v0, v1) - D;
+    const int nrows = max(v0, v1) - rmin + 1;
+    if (nrows <= D + 2) {
+      bandw_samples<TB, TC, D, D + 2, RAT>(w, s, bs, lu0, lv0, nv, ncols, rmin, nrows, p1, lane);
+    } else if (nrows <= D + 3) {
+      bandw_samples<TB, TC, D, D + 3, RAT>(w, s, bs, lu0, lv0, nv, ncols, rmin, nrows, p1, lane);
+    } else {
+      for (int idx = lane; idx < (nv + 1) * ncols; idx += 32) {
+        const int a = idx / ncols, col = idx - (idx / ncols) * ncols;
+        const long long lu = lu0 + col, lv = lv0 + a;
+        const TB *Nu = bs.basis + lu * 3 * p1;
+        const TB *Nv = bs.basis + lv * 3 * p1;
+        Vec4<TC> P;
+        if constexpr (std::is_same<TB, TC>::value) {
+          TC q[3];
+          eval_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv, q);
+          P = Vec4<TC>{q[0], q[1], q[2], TC(0)};
+        } else {
+          P = screen_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv);
+        }
+        w.S[a][col] = P;
+      }
+    }
+    __syncwarp();
+    // Cells: lane c owns cell column c (tile c / 8, column c % 8 of it).
+    const int j = lane >> 3, b = lane & 7;
+    const bool act = j < ntx;
+    TC tlo[3] = {pos_inf<TC>(), pos_inf<TC>(), pos_inf<TC>()};
+    TC thi[3] = {-pos_inf<TC>(), -pos_inf<TC>(), -pos_inf<TC>()};
+    const int tx = tx0 + j;
+    const long long t = static_cast<long long>(r) * g.ntiles + static_cast<long long>(ty) * g.tw + tx;
+    if (act) {
+      const bool colok = b < min(te, g.W - tx * te);
+      Vec4<TC> p = w.S[0][lane], q = w.S[0][lane + 1];
+      TC pmn[3] = {fmn(p.x, q.x), fmn(p.y, q.y), fmn(p.z, q.z)};
+      TC pmx[3] = {fmx(p.x, q.x), fmx(p.y, q.y), fmx(p.z, q.z)};
+      Vec4<TC> *dst = out.center + t * te2 + b;
+#pragma unroll
+      for (int a = 0; a < te; ++a) {
+        p = w.S[a + 1][lane];
+        q = w.S[a + 1][lane + 1];
+        const TC nmn[3] = {fmn(p.x, q.x), fmn(p.y, q.y), fmn(p.z, q.z)};
+        const TC nmx[3] = {fmx(p.x, q.x), fmx(p.y, q.y), fmx(p.z, q.z)};
+        Vec4<TC> cen{TC(0), TC(0), TC(0), TC(0)};
+        if (a < nv && colok) {
+          TC c3[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const TC lo = fmn(pmn[k], nmn[k]), hi = fmx(pmx[k], nmx[k]);
+            c3[k] = (lo - TC(0) + hi + TC(0)) * TC(0.5);  // = / 2 exactly
+            tlo[k] = fmn(tlo[k], c3[k]);
+            thi[k] = fmx(thi[k], c3[k]);
+          }
+          cen = Vec4<TC>{c3[0], c3[1], c3[2], TC(0)};
+        }
+        dst[a * te] = cen;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          pmn[k] = nmn[k];
+          pmx[k] = nmx[k];
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < te; o <<= 1) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        tlo[k] = fmn(tlo[k], __shfl_xor_sync(kFull, tlo[k], o));
+        thi[k] = fmx(thi[k], __shfl_xor_sync(kFull, thi[k], o));
+      }
+    }
+    if (act && b == 0) {
+      out.tlo[t] = Vec4<TC>{tlo[0], tlo[1], tlo[2], TC(0)};
+      out.thi[t] = Vec4<TC>{thi[0], thi[1], thi[2], TC(0)};
+      if (out.stmin) fold_supertile(out, r, ty, tx, tlo, thi);
+    }
+    __syncwarp();
+  }
+}
+
 // FP64 centre of one cell exactly as the FP64 form builds it: P at the four
 // corners from the FP64 basis tables (eval_point), min/max, (lo - 0 + hi + 0)/2.
 __device__ Vec4<double> cell_center64(const SurfView<double> &s, const SideRound<double> &sr, int region, int cell) {
@@ -3779,11 +3992,39 @@ void launch_surface_prep(const SurfacePrep *jobs, int n, long long most, cudaStr
   k_surface_prep<<<dim3(gx > 0 ? gx : 1, n, 1), 256, 0, st>>>(jobs);
 }
 
+template <typename TB, typename TC, int D, bool RAT>
+void launch_bandw(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
+                  const Batch &bt, const SurfView<TC> *vdev) {
+  constexpr size_t smem = bandw_smem<TC>();
+  static bool configured = false;  // once per instantiation
+  if (!configured) {
+    cudaFuncSetAttribute(k_cells_bandw<TB, TC, D, RAT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    configured = true;
+  }
+  const Geom &g = out.g;
+  const long long units = static_cast<long long>(bs.nreg) * g.tw * ((g.tw + kWT - 1) / kWT);
+  k_cells_bandw<TB, TC, D, RAT><<<bdim(bgrid((units + kWWarps - 1) / kWWarps, bt, 148 * 16), bt), kWWarps * 32, smem,
+                                   st>>>(s, vdev, bs, out, bt.qs);
+}
+
 template <typename TB, typename TC>
 void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
                         const Batch &bt, const SurfView<TC> *vdev) {
   counted();
   const Geom &g = out.g;
+  if (g.tw >= 16 && g.te == kMaxTile && !s.zero && s.degu == s.degv && (s.degu == 3 || s.degu == 2)) {
+    // Large grids with equal degrees 2 or 3 (degrees, the rational flag and
+    // the zero flag are part of a batch's shape): warp-independent bands.
+    if (s.degu == 3) {
+      if (s.rat) launch_bandw<TB, TC, 3, true>(s, bs, out, st, bt, vdev);
+      else launch_bandw<TB, TC, 3, false>(s, bs, out, st, bt, vdev);
+    } else {
+      if (s.rat) launch_bandw<TB, TC, 2, true>(s, bs, out, st, bt, vdev);
+      else launch_bandw<TB, TC, 2, false>(s, bs, out, st, bt, vdev);
+    }
+    return;
+  }
   if (g.tw >= 16 && g.te == kMaxTile && s.degu <= 3 && s.degv <= 3) {
     // Large grids of bicubic-or-lower surfaces (degrees are part of a batch's
     // shape): whole bands per block.
