@@ -71,10 +71,10 @@ UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "cells
              "inter_leaf": (9, 0)}
 # DRAM traffic per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch / its units), for the form it was captured in:
-# profiles/k_cells_band_hardwave_n512.md (FP32 screen, 128 x 511^2 cells).
-MEASURED_TRAFFIC = {("cells_r1", "fp32_screen"): 16.17}
+# profiles/k_cells_band_hardwave_n512.md (FP32 screen, 128 x 511^2 cells: 516.8 MB / 33.4M).
+MEASURED_TRAFFIC = {("cells_r1", "fp32_screen"): 15.46}
 # What one timed "launch" of a kernel name covers.
-LAUNCH_NOTE = {"cells_r1": "the first round's cell build of one batch: one k_cells_band launch per side, "
+LAUNCH_NOTE = {"cells_r1": "the first round's cell build of one batch: one k_cells_bandw launch per side, "
                            "back to back on one stream, timed together"}
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 74.4: 148 SMs x 128 lanes x FMA x 1.965 GHz
 NOMINAL_FP64_TFLOPS = NOMINAL_FP32_TFLOPS / 2
@@ -120,6 +120,8 @@ def parse():
                     help="queries per lockstep batch on a lane (0: one query per lane job)")
     ap.add_argument("--e2e-chunks", type=int, default=2,
                     help="end-to-end pass: submitted chunks per step (uploads overlap the previous chunk)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every batch eagerly (no CUDA graph replay), e.g. under a profiler")
     ap.add_argument("--autotune", action="store_true",
                     help="pick each form's chunk with the library's autotuner before timing it")
     return ap.parse_args()
@@ -290,6 +292,8 @@ def run_ours(args):
     ctx = J.Context(local)
     ctx.workers(args.lanes)
     ctx.batch_chunk(args.chunk)
+    if args.no_graphs:
+        ctx.batch_graphs(False)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     pairs = make_pairs(args.batch, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")

@@ -72,3 +72,36 @@ def test_null_arguments_rejected():
     assert lib.jsi_destroy(None) == -1
     assert lib.jsi_min_distance(None, None, None, None, None) == -1
     assert lib.jsi_intersect(None, None, None, None, None) == -1
+
+
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """Every structure the Python mirror passes through the C ABI has the
+    header's size and field offsets (a mismatch would let the library write
+    past the caller's buffers)."""
+    import shutil
+    import subprocess
+    from jsi_cad_next_versions_b200 import _capi as C
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    structs = {"jsi_task": C.Task, "jsi_dist_params": C.DistParams, "jsi_dist_result": C.DistResult,
+               "jsi_inter_params": C.InterParams, "jsi_inter_result": C.InterResult,
+               "jsi_bounds_params": C.BoundsParams, "jsi_bounds_result": C.BoundsResult,
+               "jsi_curve_params": C.CurveParams, "jsi_curve_result": C.CurveResult, "jsi_config": C.Config}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "jsi_b200.h"', "int main(void) {"]
+    for cname, st in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in st._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, fname, val = ln.split()
+        got[(cname, fname)] = int(val)
+    for cname, st in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(st), cname
+        for fname, _ in st._fields_:
+            assert got[(cname, fname)] == getattr(st, fname).offset, (cname, fname)
