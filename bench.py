@@ -121,7 +121,8 @@ def parse():
     ap.add_argument("--e2e-chunks", type=int, default=2,
                     help="end-to-end pass: submitted chunks per step (uploads overlap the previous chunk)")
     ap.add_argument("--no-graphs", action="store_true",
-                    help="launch every batch eagerly (no CUDA graph replay), e.g. under a profiler")
+                    help="launch every batch eagerly (the library's default; kept for older command lines)")
+    ap.add_argument("--graphs", action="store_true", help="replay repeated batches as CUDA graphs")
     ap.add_argument("--autotune", action="store_true",
                     help="pick each form's chunk with the library's autotuner before timing it")
     return ap.parse_args()
@@ -292,8 +293,7 @@ def run_ours(args):
     ctx = J.Context(local)
     ctx.workers(args.lanes)
     ctx.batch_chunk(args.chunk)
-    if args.no_graphs:
-        ctx.batch_graphs(False)
+    ctx.batch_graphs(bool(args.graphs and not args.no_graphs))
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
     pairs = make_pairs(args.batch, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")

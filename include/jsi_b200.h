@@ -339,9 +339,11 @@ int jsi_batch_reruns(jsi_context *ctx, long long *out);
  * (may be null) get the choice and its batch device time. */
 int jsi_autotune_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b, const jsi_dist_params *params,
                        int *chunk_out, float *ms_out);
-/* Lockstep batches that repeat a shape, size and lane are captured once as a
- * CUDA graph and replayed.  enable: 1 on (default), 0 off, -1 unchanged;
- * replays (may be null) gets the replay count over all lanes. */
+/* When on, lockstep batches that repeat a shape, size and lane are captured
+ * once as a CUDA graph and replayed.  enable: 1 on, 0 off (default), -1
+ * unchanged; replays (may be null) gets the replay count over all lanes.
+ * Off by default: with three worker lanes and uploads running beside them a
+ * replay crashed inside cudaGraphLaunch on driver 580. */
 int jsi_batch_graphs(jsi_context *ctx, int enable, long long *replays);
 
 /* --- grid evaluation -----------------------------------------------------

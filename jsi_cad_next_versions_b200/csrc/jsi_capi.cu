@@ -275,7 +275,7 @@ struct Lane {
   std::map<std::vector<long long>, GraphEntry> graphs;
   unsigned long long graph_clock = 0;
   long long graph_replays = 0;
-  bool graphs_on = true;
+  bool graphs_on = false;
 };
 
 // One query of a batch: its tasks, the caller's result slot and its status
@@ -353,7 +353,10 @@ struct jsi_context {
   // Chunk sizes chosen by jsi_autotune_batch per shape: first-round nuv and
   // basis stride of both sides, k, rounds, precision.
   std::map<std::array<int, 7>, int> tuned_chunk;
-  bool batch_graphs = true;  // replay repeated lockstep batches as CUDA graphs
+  // Replay repeated lockstep batches as CUDA graphs (off by default: with
+  // three worker lanes and uploads running beside them, a replay crashed
+  // inside cudaGraphLaunch on this driver).
+  bool batch_graphs = false;
   std::string kernel_names;
   // worker pool
   std::vector<std::unique_ptr<Lane>> lanes;
