@@ -223,6 +223,31 @@ def test_submit_wait_overlapping_batches():
             ctx.workers(0)
 
 
+def test_three_lanes_with_uploads_alongside():
+    """Three worker lanes run submitted batches while the calling thread
+    uploads and releases other surfaces (the surface table changes while
+    lanes look surfaces up); every batch equals the same batch run alone."""
+    import jsi_cad_next_versions_b200 as J
+    pairs = _hard_wave_pairs(9, seed0=1600)
+    extra = [x for pr in _sine_pairs(24, seed0=1700) for x in pr]
+    with J.Context(0) as ctx:
+        ids = np.asarray(ctx.upload_many([x for pr in pairs for x in pr]), np.int32)
+        dom = ctx.surface_domains(ids)
+        tb = J.TaskBatch.from_arrays(ids[0::2], dom[0::2], 144, ids[1::2], dom[1::2], 144)
+        ctx.workers(3)
+        try:
+            ref, _ = ctx.min_distance_batch(tb, precision="fp32_screen", trace=True)
+            for _ in range(3):
+                h = ctx.submit_distance_batch(tb, precision="fp32_screen", trace=True)
+                more = ctx.upload_many(extra)
+                ctx.release_many(more)
+                got, _ = ctx.wait_distance_batch(h)
+                for a, b in zip(ref, got):
+                    _same(b, a)
+        finally:
+            ctx.workers(0)
+
+
 def test_upload_many_release_reuse():
     """Surfaces uploaded in one call, released, and other surfaces uploaded
     into the recycled device blocks: every query sees its own surfaces."""
