@@ -329,6 +329,70 @@ struct PendingBatch {
 
 }  // namespace
 
+namespace {
+
+// A few host threads kept for the upload path's per-surface work (header
+// checks, staging copies), so a parallel loop costs a wake-up rather than
+// thread creation.  run() is called with the context mutex held (one caller
+// at a time); the calling thread takes part.
+class HostPool {
+ public:
+  explicit HostPool(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { loop(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+  void run(size_t n, const std::function<void(size_t)> &fn) {
+    std::unique_lock<std::mutex> lk(mu_);
+    fn_ = &fn;
+    n_ = n;
+    next_.store(0);
+    active_ = th_.size();
+    ++gen_;
+    lk.unlock();
+    cv_.notify_all();
+    work();
+    lk.lock();
+    done_.wait(lk, [&] { return active_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  void work() {
+    for (size_t q; (q = next_.fetch_add(1)) < n_;) (*fn_)(q);
+  }
+  void loop() {
+    unsigned long long seen = 0;
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+      if (stop_) return;
+      seen = gen_;
+      lk.unlock();
+      work();
+      lk.lock();
+      if (--active_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(size_t)> *fn_ = nullptr;
+  size_t n_ = 0;
+  std::atomic<size_t> next_{0};
+  size_t active_ = 0;
+  unsigned long long gen_ = 0;
+  bool stop_ = false;
+};
+
+}  // namespace
+
 struct jsi_context {
   int device = 0;
   Lane main;
@@ -369,6 +433,7 @@ struct jsi_context {
   long long next_ticket = 1;
   int busy = 0;
   bool stopping = false;
+  std::unique_ptr<HostPool> hpool;  // upload path host threads
 };
 
 namespace {
@@ -503,22 +568,14 @@ void surface_header(SurfaceRec &s, const int ivec[7], const float *data) {
   }
 }
 
-// Runs fn(q) for q in [0, n) on up to 8 host threads (the upload path's
-// per-surface host work).
-template <typename Fn>
-void parallel_for(size_t n, Fn &&fn) {
-  const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
-  const size_t nt = std::min<size_t>({hw, size_t(8), (n + 63) / 64});
-  if (nt <= 1) {
-    for (size_t q = 0; q < n; ++q) fn(q);
+// Runs fn(q) for q in [0, n) on the context's host threads (the upload
+// path's per-surface work), or inline without them.
+void parallel_for(HostPool *pool, size_t n, const std::function<void(size_t)> &fn) {
+  if (pool && n > 1) {
+    pool->run(n, fn);
     return;
   }
-  std::vector<std::thread> pool;
-  for (size_t t = 0; t < nt; ++t)
-    pool.emplace_back([&, t] {
-      for (size_t q = t; q < n; q += nt) fn(q);
-    });
-  for (auto &th : pool) th.join();
+  for (size_t q = 0; q < n; ++q) fn(q);
 }
 
 SurfaceRec upload_surface(Lane *ctx, const int ivec[7], const float *data, int ndata, Arena *arena) {
@@ -632,7 +689,7 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
   // Checks and magnitudes of every surface, on host threads.
   std::vector<SurfaceRec> heads(in.size());
   std::vector<char> bad(in.size(), 0);
-  parallel_for(in.size(), [&](size_t q) {
+  parallel_for(ctx->hpool.get(), in.size(), [&](size_t q) {
     try {
       check_surface(in[q].ivec, in[q].data, in[q].ndata);
       surface_header(heads[q], in[q].ivec, in[q].data);
@@ -691,7 +748,7 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
       off += rb;
       ++q;
     }
-    parallel_for(copies.size(), [&](size_t e) {
+    parallel_for(ctx->hpool.get(), copies.size(), [&](size_t e) {
       const PendingSurface &ps = in[copies[e].first];
       std::memcpy(ctx->ring + seg0 + copies[e].second, ps.data, static_cast<size_t>(ps.ndata) * sizeof(float));
     });
@@ -2638,6 +2695,11 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
     }
     JSI_CUDA(cudaEventCreateWithFlags(&ctx->upload_ev, cudaEventDisableTiming));
     JSI_CUDA(cudaEventRecord(ctx->upload_ev, ctx->main.stream));
+    {
+      const int hw = static_cast<int>(std::thread::hardware_concurrency());
+      const int nt = std::min(7, std::max(0, hw - 1));
+      if (nt > 0) ctx->hpool = std::make_unique<HostPool>(nt);
+    }
     return JSI_OK;
   });
   if (st != JSI_OK) {
