@@ -1338,7 +1338,7 @@ BatchCaps batch_caps() {
 constexpr unsigned long long kBatchHeadCap = 2048;        // threshold-pass list
 // Threshold-pass list sizes: round 1 (large grids) and refinement rounds.
 constexpr unsigned kBatchHeadWant = 64;
-constexpr unsigned kBatchHeadWantRefine = 32;
+constexpr unsigned kBatchHeadWantRefine = 16;
 
 // One round's arrays in the slab.  TP sides hold the regions and basis tables
 // (and, in exact rounds, the cells); the FP32 screen's first round keeps its
