@@ -1449,9 +1449,11 @@ void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, c
     timed(L, "dist_cull", [&] {
       launch_dist_cull_st(X, Y, R.map1, R.map2, ns, R.st_surv, R.st_cap, stats, screen, e, st, bt);
     });
+    // The seed of dist_tau (2 x 2 representative tiles per supertile) is
+    // tight enough that the expansion goes straight to its bound pass: a
+    // threshold-tightening pass over the representatives first cost more than
+    // the extra surviving tile pairs it saves.
     timed(L, "dist_expand", [&] {
-      launch_dist_expand(X, Y, R.map1, R.map2, R.st_surv, kFromDevice, R.st_cap, k, 0, R.surv, R.surv_lb, R.surv_cap,
-                         stats, screen, e, st, bt);
       launch_dist_expand(X, Y, R.map1, R.map2, R.st_surv, kFromDevice, R.st_cap, k, 1, R.surv, R.surv_lb, R.surv_cap,
                          stats, screen, e, st, bt);
     });
