@@ -72,6 +72,15 @@ def test_null_arguments_rejected():
     assert lib.jsi_destroy(None) == -1
     assert lib.jsi_min_distance(None, None, None, None, None) == -1
     assert lib.jsi_intersect(None, None, None, None, None) == -1
+    # the bulk, asynchronous and interval entry points
+    assert lib.jsi_surface_upload_many(None, 0, None, None, None, None) == -1
+    assert lib.jsi_surface_release_many(None, 0, None) == -1
+    assert lib.jsi_surface_domains(None, 0, None, None) == -1
+    assert lib.jsi_min_distance_batch(None, 0, None, None, None, None, None, None) == -1
+    assert lib.jsi_submit_distance_batch(None, 0, None, None, None, None, None, None) == -1
+    assert lib.jsi_wait_distance_batch(None, 0, None) == -1
+    assert lib.jsi_distance_bounds(None, None, None, None, None) == -1
+    assert lib.jsi_intersection_curves(None, None, None, None, None) == -1
 
 
 def test_ctypes_layouts_match_the_header(tmp_path):
