@@ -70,8 +70,8 @@ UNIT_WORK = {"samples": (120, 16), "basis": (100, 52), "cells": (36, 32), "cells
              "dist_cull": (14, 0), "dist_leaf": (8, 0), "dist_head": (8, 0), "inter_cull": (14, 0),
              "inter_leaf": (9, 0)}
 # DRAM traffic per unit measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch / its units), for the form it was captured in:
-# profiles/k_cells_band_hardwave_n512.md (FP32 screen, 128 x 511^2 cells: 516.8 MB / 33.4M).
+# of one launch / its units), for the form it was captured in: the band kernel of
+# the FP32 screen over 128 x 511^2 cells wrote and read 516.8 MB, 15.46 B per cell.
 MEASURED_TRAFFIC = {("cells_r1", "fp32_screen"): 15.46}
 # What one timed "launch" of a kernel name covers.
 LAUNCH_NOTE = {"cells_r1": "the first round's cell build of one batch: one k_cells_bandw launch per side, "

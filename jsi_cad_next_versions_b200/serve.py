@@ -125,8 +125,9 @@ class ServingLoop:
         self.budget = budget_bytes
         self.max_inflight = max_inflight or 2 * lanes
         self.precision = precision
-        # The intersection query has no FP32 stage: the
-        # screen form runs it in FP64.
+        # The intersection query has no FP32 stage (every overlapping pair
+        # needs its exact FP64 box and curvature padding): the screen form
+        # runs it in FP64.
         self.inter_precision = inter_precision or ("fp64" if precision == "fp32_screen" else precision)
         self.k = k
         self.inter_rounds = inter_rounds
