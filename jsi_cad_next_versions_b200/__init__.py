@@ -19,12 +19,13 @@ from .api import (  # noqa: F401
     init_cad,
     intersection,
     minimum_distance,
+    SurfaceBatch,
     TaskBatch,
 )
 from . import synth  # noqa: F401
 
 __all__ = [
-    "Context", "DistanceBatch", "DistanceResult", "TaskBatch", "EvalAndConstructTask", "IntersectionResult", "JsiError", "ONE_UV_SIZE",
+    "Context", "DistanceBatch", "DistanceResult", "SurfaceBatch", "TaskBatch", "EvalAndConstructTask", "IntersectionResult", "JsiError", "ONE_UV_SIZE",
     "default_global_dist_nuv", "default_global_intersect_nuv", "deinit_cad", "evalWithCuda", "init_cad",
     "intersection", "minimum_distance", "synth",
 ]

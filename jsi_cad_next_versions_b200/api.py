@@ -141,6 +141,57 @@ class TaskBatch:
         return self.n
 
 
+class SurfaceBatch:
+    """Host surfaces packed once for repeated bulk uploads.
+
+    One contiguous float32 buffer holds every surface's EGADS data, each
+    record starting on a 64-byte boundary, beside the arrays
+    ``jsi_surface_upload_many`` takes: (n, 7) headers, data pointers and
+    lengths. ``batch[a:b]`` is a view of surfaces a..b-1 (no copy), so a
+    caller that uploads the same host set in chunks, again and again, pays no
+    per-surface Python work per upload."""
+
+    _ALIGN = 16  # floats (64 bytes)
+
+    def __init__(self, surfaces=None):
+        if surfaces is None:
+            return
+        n = len(surfaces)
+        iv = [np.asarray(x.ivec, np.int32).reshape(-1) for x in surfaces]
+        if any(v.shape[0] != 7 for v in iv):
+            raise ValueError("every surface header has 7 entries")
+        nd = np.fromiter((np.asarray(x.data).shape[0] for x in surfaces), dtype=np.int64, count=n)
+        stride = -(-nd // self._ALIGN) * self._ALIGN
+        off = np.zeros(n, np.int64)
+        np.cumsum(stride[:-1], out=off[1:])
+        self.data = np.zeros(int(stride.sum()) + self._ALIGN, np.float32)
+        base = (-(self.data.ctypes.data // 4)) % self._ALIGN  # first 64-byte boundary in the buffer
+        off += base
+        for x, o, k in zip(surfaces, off.tolist(), nd.tolist()):
+            self.data[o:o + k] = np.asarray(x.data, np.float32).reshape(-1)
+        self.ivec = np.ascontiguousarray(np.stack(iv), dtype=np.int32) if n else np.zeros((0, 7), np.int32)
+        self.ndata = nd.astype(np.int32)
+        self.offsets = off
+        self.ptrs = (self.data.ctypes.data + 4 * off).astype(np.uintp)
+
+    def __len__(self) -> int:
+        return int(self.ndata.shape[0])
+
+    def __getitem__(self, key):
+        if not isinstance(key, slice) or key.step not in (None, 1):
+            raise TypeError("SurfaceBatch takes contiguous slices")
+        sub = SurfaceBatch()
+        sub.data = self.data
+        sub.ivec, sub.ndata = self.ivec[key], self.ndata[key]
+        sub.offsets, sub.ptrs = self.offsets[key], self.ptrs[key]
+        return sub
+
+    def surface(self, q: int):
+        """(ivec, data) views of surface q."""
+        o = int(self.offsets[q])
+        return self.ivec[q], self.data[o:o + int(self.ndata[q])]
+
+
 @dataclass
 class IntersectionCurves:
     """Polylines through the refined intersection points: curves[k] is an
@@ -231,10 +282,17 @@ class Context:
         return sid.value
 
     def upload_many(self, surfaces) -> list[int]:
-        """Upload several surfaces in one call; returns their ids."""
+        """Upload several surfaces in one call (a sequence of surfaces, or a
+        ``SurfaceBatch`` or slice of one); returns their ids."""
         n = len(surfaces)
         if n == 0:
             return []
+        if isinstance(surfaces, SurfaceBatch):
+            ids = np.zeros(n, np.int32)
+            self._check(self.lib.jsi_surface_upload_many(self.handle, n, surfaces.ivec.ctypes.data,
+                                                         surfaces.ptrs.ctypes.data, surfaces.ndata.ctypes.data,
+                                                         ids.ctypes.data))
+            return ids.tolist()
         iv = np.ascontiguousarray(np.stack([np.asarray(x.ivec, np.int32) for x in surfaces]), dtype=np.int32)
         keep = [np.ascontiguousarray(x.data, dtype=np.float32) for x in surfaces]
         ptrs = np.fromiter((k.ctypes.data for k in keep), dtype=np.uintp, count=n)

@@ -198,6 +198,37 @@ def test_bulk_domains_tasks_release():
             ctx.surface_domains(ids[:1])
 
 
+def test_packed_surface_set_uploads_in_chunks():
+    """A SurfaceBatch uploaded in two slices gives the same domains and the
+    same batch results as the surfaces uploaded one list at a time."""
+    import jsi_cad_next_versions_b200 as J
+    pairs = _hard_wave_pairs(3, seed0=1800) + _sine_pairs(3, seed0=1900)
+    flat = [x for pr in pairs for x in pr]
+    hostset = J.SurfaceBatch(flat)
+    with J.Context(0) as ctx:
+        base = ctx.resident_bytes()
+        ids = np.asarray(ctx.upload_many(hostset[0:6]) + ctx.upload_many(hostset[6:12]), np.int32)
+        ref_ids = np.asarray(ctx.upload_many(flat), np.int32)
+        dom = ctx.surface_domains(ids)
+        assert np.array_equal(dom, ctx.surface_domains(ref_ids))
+        ctx.workers(2)
+        try:
+            for sl, nuv in ((slice(0, 3), 144), (slice(3, 6), 40)):
+                got_ids, want_ids = ids.reshape(-1, 2)[sl], ref_ids.reshape(-1, 2)[sl]
+                d = dom.reshape(-1, 2, 4)[sl]
+                tb = J.TaskBatch.from_arrays(got_ids[:, 0], d[:, 0], nuv, got_ids[:, 1], d[:, 1], nuv)
+                tr = J.TaskBatch.from_arrays(want_ids[:, 0], d[:, 0], nuv, want_ids[:, 1], d[:, 1], nuv)
+                got, _ = ctx.min_distance_batch(tb, precision="fp32_screen", trace=True)
+                want, _ = ctx.min_distance_batch(tr, precision="fp32_screen", trace=True)
+                for a, b in zip(want, got):
+                    _same(b, a)
+        finally:
+            ctx.workers(0)
+        ctx.release_many(ids)
+        ctx.release_many(ref_ids)
+        assert ctx.resident_bytes() == base
+
+
 def test_submit_wait_overlapping_batches():
     """Two batches in flight: the second's surfaces are uploaded after the
     first is submitted; each equals the same batch run synchronously."""
