@@ -396,7 +396,12 @@ class HostPool {
 struct jsi_context {
   int device = 0;
   Lane main;
-  std::mutex mu;  // serialises the main lane and the surface table
+  std::mutex mu;  // serialises the main lane, the upload path and the surface table
+  // The part of the surface table worker lanes touch (surfaces, surface_refs,
+  // upload_ev).  Writers hold it beside mu (mu first); a worker takes it
+  // alone, so a bulk upload staging on host threads under mu does not hold
+  // up the lanes running queries over surfaces already resident.
+  std::mutex surf_mu;
   std::string last_error;
   std::map<int, SurfaceRec> surfaces;
   std::map<int, int> surface_refs;  // queued / running jobs per surface
@@ -762,6 +767,7 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
     ctx->ring_off = off + al(jobs_b);
   }
   JSI_CUDA(cudaGetLastError());
+  std::lock_guard<std::mutex> ls(ctx->surf_mu);
   JSI_CUDA(cudaEventRecord(ctx->upload_ev, st));
 }
 
@@ -2545,7 +2551,7 @@ std::vector<int> job_surfaces(const Job &j) {
 }
 
 void release_refs(jsi_context *ctx, const Job &j) {
-  std::lock_guard<std::mutex> lk(ctx->mu);
+  std::lock_guard<std::mutex> lk(ctx->surf_mu);
   for (int id : job_surfaces(j)) {
     auto it = ctx->surface_refs.find(id);
     if (it != ctx->surface_refs.end() && --it->second <= 0) ctx->surface_refs.erase(it);
@@ -2567,7 +2573,7 @@ void worker_loop(jsi_context *ctx, Lane *L) {
     }
     job->status = run_guarded(job->error, [&] {
       {
-        std::lock_guard<std::mutex> lk(ctx->mu);
+        std::lock_guard<std::mutex> lk(ctx->surf_mu);
         JSI_CUDA(cudaStreamWaitEvent(L->stream, ctx->upload_ev, 0));
       }
       if (job->kind == 0)
@@ -2622,7 +2628,7 @@ void start_workers(jsi_context *ctx, int n) {
   for (int q = 0; q < n; ++q) {
     auto L = std::make_unique<Lane>();
     lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces, &ctx->lane_held, left);
-    L->surfaces_mu = &ctx->mu;
+    L->surfaces_mu = &ctx->surf_mu;
     L->graphs_on = ctx->batch_graphs;
     L->timing = ctx->main.timing;  // per-kernel timing follows the context's setting
     ctx->lanes.push_back(std::move(L));
@@ -2636,6 +2642,7 @@ long long enqueue(jsi_context *ctx, std::shared_ptr<Job> job) {
     const std::vector<int> ids = job_surfaces(*job);
     for (int id : ids)
       if (!ctx->surfaces.count(id)) fail(JSI_ERR_INVALID, "unknown surface id %d", id);
+    std::lock_guard<std::mutex> ls(ctx->surf_mu);
     for (int id : ids) ++ctx->surface_refs[id];
   }
   long long t;
@@ -2736,6 +2743,7 @@ int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, i
     SurfaceRec s = upload_resident(ctx, ivec, data, ndata);
     ctx->resident += s.bytes;
     const int id = ctx->next_id++;
+    std::lock_guard<std::mutex> ls(ctx->surf_mu);
     ctx->surfaces[id] = s;
     *out = id;
     return JSI_OK;
@@ -2745,6 +2753,7 @@ int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, i
 int jsi_surface_release(jsi_context *ctx, jsi_surface_id id) {
   if (!ctx) return JSI_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  std::lock_guard<std::mutex> ls(ctx->surf_mu);
   auto it = ctx->surfaces.find(id);
   if (it == ctx->surfaces.end()) return record(ctx, JSI_ERR_INVALID, "unknown surface id");
   if (ctx->surface_refs.count(id)) return record(ctx, JSI_ERR_INVALID, "surface is used by a queued query");
@@ -2795,6 +2804,7 @@ int jsi_surface_upload_many(jsi_context *ctx, int n, const int *ivecs, const flo
       for (auto &r : recs) ctx->pool.put(r.block, r.block_bytes);  // none becomes resident
       throw;
     }
+    std::lock_guard<std::mutex> ls(ctx->surf_mu);
     for (; done < n; ++done) {
       ctx->resident += recs[done].bytes;
       const int id = ctx->next_id++;
