@@ -2705,8 +2705,12 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
     JSI_CUDA(cudaEventCreateWithFlags(&ctx->upload_ev, cudaEventDisableTiming));
     JSI_CUDA(cudaEventRecord(ctx->upload_ev, ctx->main.stream));
     {
+      // Upload-path host threads beside the caller: up to 7 by default,
+      // JSI_HOST_THREADS (0..63) overrides.
       const int hw = static_cast<int>(std::thread::hardware_concurrency());
-      const int nt = std::min(7, std::max(0, hw - 1));
+      int nt = std::min(7, std::max(0, hw - 1));
+      if (const char *v = std::getenv("JSI_HOST_THREADS"); v && *v)
+        nt = static_cast<int>(std::min(63L, std::max(0L, std::strtol(v, nullptr, 10))));
       if (nt > 0) ctx->hpool = std::make_unique<HostPool>(nt);
     }
     return JSI_OK;
