@@ -3791,15 +3791,19 @@ template <typename T>
 void launch_dist_tau_st(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                         int k, ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
   counted();
-  // k <= kStKL: one block per query, so that its merge takes the exact k-th
-  // of all the query's representative pairs.  Split over several blocks,
-  // each block's own k-th (the smallest of them enters tau) loosens as the
-  // blocks see fewer pairs: for the hard-wave pair at nuv0 = 512, tau grows
-  // 1.25x at 4 blocks, 2.8x at 9 and 6x at 18, and the tile pairs under it
-  // from about 3.7k to 6k, 45k and 234k (past the survivor list's 65,536,
-  // so those queries re-ran alone).  A block covers 4096 supertile pairs
-  // there, 16 per thread.
-  const dim3 grid = k <= kStKL ? bdim(1, bt) : bdim(bgrid(rows_for(nslots, a.g.nst), bt, 148 * 8), bt);
+  // k <= kStKL: a block's merge takes the exact k-th of the pairs it saw,
+  // and the smallest block k-th enters tau, so every block should see many
+  // pairs: a query is split over more blocks only past 64 supertile pairs
+  // per thread (16,384 per block), and up to 16,384 pairs it runs as one
+  // block, whose k-th is the query's exact one.  Split by the batch size
+  // instead, tau loosened as batches shrank: for the hard-wave pair at
+  // nuv0 = 512 (4096 supertile pairs), it grew 1.25x at 4 blocks, 2.8x at 9
+  // and 6x at 18, and the tile pairs under it from about 3.7k to 6k, 45k and
+  // 234k (past the survivor list's 65,536, so those queries re-ran alone).
+  const long long st_pairs = static_cast<long long>(rows_for(nslots, a.g.nst)) * b.g.nst;
+  const long long per_block = 256LL * 64;
+  const dim3 grid = k <= kStKL ? bdim(bgrid((st_pairs + per_block - 1) / per_block, bt, 148 * 8), bt)
+                               : bdim(bgrid(rows_for(nslots, a.g.nst), bt, 148 * 8), bt);
   const int ns = dev_slots(nslots);
   if constexpr (std::is_same<T, float>::value) {
     if (screen) {
