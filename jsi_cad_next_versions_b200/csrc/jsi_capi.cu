@@ -999,8 +999,9 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
     if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
     surv = ar.get<unsigned long long>(tile_pairs);
     surv_lb = ar.get<unsigned>(tile_pairs);
-    timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); },
-          double(tile_pairs));
+    if (dist_tau_folds(B.g, k))
+      timed(ctx, "dist_tau", [&] { launch_dist_tau(A, B, map1, map2, nslots, k, ctx->d_stats, screen, e, st); },
+            double(tile_pairs));
     timed(ctx, "dist_cull", [&] {
       launch_dist_cull(A, B, map1, map2, nslots, surv, surv_lb, tile_pairs, ctx->d_stats, screen, e, st);
     }, double(tile_pairs));
@@ -1464,7 +1465,8 @@ void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, c
                          stats, screen, e, st, bt);
     });
   } else {
-    timed(L, "dist_tau", [&] { launch_dist_tau(X, Y, R.map1, R.map2, ns, k, stats, screen, e, st, bt); });
+    if (dist_tau_folds(Y.g, k))
+      timed(L, "dist_tau", [&] { launch_dist_tau(X, Y, R.map1, R.map2, ns, k, stats, screen, e, st, bt); });
     timed(L, "dist_cull", [&] {
       launch_dist_cull(X, Y, R.map1, R.map2, ns, R.surv, R.surv_lb, R.surv_cap, stats, screen, e, st, bt);
     });

@@ -204,6 +204,12 @@ void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st, const
 template <typename T>
 void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st);
 
+// Whether the single-level threshold seed can fold anything: a block folds
+// the k-th of its 256 threads' minima, and only threads t2 < ntiles of side
+// B see a tile pair, so with fewer than k tiles on that side (4 at nuv 16,
+// where k = 8) no block folds and the launch would change nothing.
+inline bool dist_tau_folds(const Geom &gb, int k) { return k <= 256 && gb.ntiles >= k; }
+
 // screen = true (float only): FP32-screen thresholds with centre-error bound e.
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,

@@ -3727,6 +3727,7 @@ inline int dev_slots(int nslots) { return nslots < 0 ? -1 : nslots; }
 template <typename T>
 void launch_dist_tau(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2, int nslots,
                      int k, ScreenStats *stats, bool screen, float e, cudaStream_t st, const Batch &bt) {
+  if (!dist_tau_folds(b.g, k)) return;
   counted();
   const dim3 grid = bdim(bgrid(rows_for(nslots, a.g.ntiles), bt, 148 * 8), bt);
   const int ns = dev_slots(nslots);
