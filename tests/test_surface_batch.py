@@ -58,3 +58,55 @@ def test_empty_set_and_bad_header():
     bad = synth.Surface(ivec=np.asarray(s.ivec)[:6], data=s.data)
     with pytest.raises(ValueError):
         SurfaceBatch([bad])
+
+
+class _FakeLib:
+    """Stands in for the C library: records what jsi_surface_upload_many
+    receives (read back through the pointers it is given) and hands out ids."""
+
+    def __init__(self):
+        self.calls = []
+        self.next_id = 1
+
+    def jsi_surface_upload_many(self, handle, n, ivecs, datas, ndatas, out):
+        iv = np.ctypeslib.as_array((ctypes.c_int * (7 * n)).from_address(ivecs)).reshape(n, 7).copy()
+        ptrs = np.ctypeslib.as_array((ctypes.c_size_t * n).from_address(datas)).copy()
+        nd = np.ctypeslib.as_array((ctypes.c_int * n).from_address(ndatas)).copy()
+        data = [np.frombuffer((ctypes.c_float * int(nd[q])).from_address(int(ptrs[q])), np.float32).copy()
+                for q in range(n)]
+        self.calls.append((iv, data))
+        ids = (ctypes.c_int * n).from_address(out)
+        for q in range(n):
+            ids[q] = self.next_id
+            self.next_id += 1
+        return 0
+
+    def jsi_last_error(self, handle):
+        return b""
+
+
+def _fake_context():
+    from jsi_cad_next_versions_b200 import Context
+    ctx = object.__new__(Context)
+    ctx.lib = _FakeLib()
+    ctx.handle = None
+    return ctx
+
+
+def test_upload_many_passes_each_slice_to_the_c_call():
+    """Chunked uploads of a packed set hand the C call exactly the surfaces
+    of each slice (headers, lengths and data), the same as a list upload."""
+    surfs = _surfaces()
+    hs = SurfaceBatch(surfs)
+    ctx = _fake_context()
+    ids = ctx.upload_many(hs[0:4]) + ctx.upload_many(hs[4:len(surfs)])
+    assert ids == list(range(1, len(surfs) + 1))
+    ref = _fake_context()
+    ref.upload_many(surfs)
+    got_iv = np.concatenate([c[0] for c in ctx.lib.calls])
+    got_data = [d for c in ctx.lib.calls for d in c[1]]
+    assert np.array_equal(got_iv, ref.lib.calls[0][0])
+    for a, b in zip(got_data, ref.lib.calls[0][1]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert ctx.upload_many(hs[2:2]) == []
+    assert len(ctx.lib.calls) == 2
