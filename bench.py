@@ -404,6 +404,7 @@ def run_ours(args):
     for _ in range(args.warmup):
         e2e_step()
     h0, d0 = ctx.transfer_bytes()
+    rr0 = ctx.batch_reruns()
     e2e_ms = []
     for _ in range(args.steps):
         flush.zero_()
@@ -419,7 +420,8 @@ def run_ours(args):
     h1, d1 = ctx.transfer_bytes()
     e2e = {"value": world * args.batch * args.steps / (sum(e2e_ms) / 1e3), "unit": "queries/s",
            "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps,
-           "form": form, "chunks": -(-args.batch // per)}
+           "form": form, "chunks": -(-args.batch // per),
+           "reruns_per_step": (ctx.batch_reruns() - rr0) / args.steps}
 
     if rank != 0:
         ctx.close()
