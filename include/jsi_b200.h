@@ -366,10 +366,13 @@ int jsi_eval_grid_f64(jsi_context *ctx, const int ivec[7], const float *data, in
  * fixed 32 MiB __device__ array that each GPU loading this code keeps until
  * exit.  Knots, the control net (16 bytes per point) and the nuv*nuv*18 float
  * records, each rounded up to 256 bytes, must fit in it, else
- * JSI_ERR_CAPACITY.  The first call on a device sets up the array's address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All
- * calls share the array: calls whose device work overlaps race; serialise
- * them. */
+ * JSI_ERR_CAPACITY; a malformed header or a data length below what the header
+ * needs gives JSI_ERR_SURFACE before any device work.  Each call uses the CUDA
+ * context current on the calling thread and looks up the array's address in
+ * it (cudaGetSymbolAddress, which allocates nothing).  The copies are
+ * synchronous, on the legacy default stream: no call may run while any thread
+ * of the process is capturing a stream in global capture mode.  All calls
+ * share the array: calls whose device work overlaps race; serialise them. */
 int jsi_eval_grid_noalloc(const int ivec[7], const float *data, int ndata, float ustep, float vstep, float ustart,
                           float vstart, int nuv, float *results);
 

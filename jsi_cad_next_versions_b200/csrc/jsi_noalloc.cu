@@ -19,9 +19,13 @@
 //    JSI_ERR_CAPACITY before touching the device.
 //  * Every GPU on which this library's code is loaded holds the 32 MiB until
 //    the process exits.
-//  * The first call on a device (the current device at the time of the call)
-//    looks up the array's device address with cudaGetSymbolAddress and caches
-//    it per device; that first call should come before any stream capture.
+//  * Every call works on the CUDA context current on the calling thread: it
+//    looks up the array's device address in that context with
+//    cudaGetSymbolAddress (which allocates nothing), so a caller that switches
+//    contexts or resets the device gets the address valid in the new one.
+//  * The copies are synchronous cudaMemcpy calls on the legacy default stream.
+//    No call may run while any thread of the process is capturing a stream in
+//    global capture mode: the copies would invalidate that capture.
 //  * All calls share the one array and it keeps the previous call's contents.
 //    Nothing in it has to start at zero: every knot, control point and record
 //    this call reads is written by this call first (the weight lane of the
@@ -32,7 +36,6 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
-#include <mutex>
 
 #include "jsi_b200.h"
 #include "jsi_internal.h"
@@ -40,28 +43,20 @@
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_setup_mu;
-void *g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
-
 size_t round256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
-// Set-up, once per device, with that device current.
-int scratch_address(int dev, unsigned char **out) {
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return JSI_ERR_CUDA;
-    }
-    g_scratch_addr[dev] = p;
+// Device address of the array in the context current on this thread.
+int scratch_address(unsigned char **out) {
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? JSI_ERR_NO_DEVICE : JSI_ERR_CUDA;
   }
-  *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+  *out = static_cast<unsigned char *>(p);
   return JSI_OK;
 }
 
@@ -71,26 +66,29 @@ extern "C" int jsi_eval_grid_noalloc(const int ivec[7], const float *data, int n
                                      float ustart, float vstart, int nuv, float *results) {
   if (!ivec || !data || !results || nuv < 1) return JSI_ERR_INVALID;
   const int degu = ivec[1], ncpu = ivec[2], nku = ivec[3], degv = ivec[4], ncpv = ivec[5], nkv = ivec[6];
-  if (degu < 0 || degv < 0 || ncpu < degu + 1 || ncpv < degv + 1) return JSI_ERR_SURFACE;
+  // Header and length checks come before any size arithmetic, in 64-bit
+  // signed integers, so that no product below can wrap.
+  if (ndata < 0 || degu < 0 || degv < 0 || ncpu < 1 || ncpv < 1) return JSI_ERR_SURFACE;
+  if (ncpu < degu + 1 || ncpv < degv + 1) return JSI_ERR_SURFACE;
   if (nku != ncpu + degu + 1 || nkv != ncpv + degv + 1) return JSI_ERR_SURFACE;
   const bool rational = (ivec[0] & 2) != 0;
-  const size_t ncp = static_cast<size_t>(ncpu) * ncpv;
-  if (static_cast<size_t>(ndata) < nku + nkv + 3 * ncp + (rational ? ncp : 0)) return JSI_ERR_SURFACE;
+  const long long ncp_ll = static_cast<long long>(ncpu) * ncpv;  // < 2^62
+  const long long need = static_cast<long long>(nku) + nkv + (rational ? 4 : 3) * ncp_ll;
+  if (static_cast<long long>(ndata) < need) return JSI_ERR_SURFACE;
+  // Any of these alone exceeds the array (32 MiB / 16 B points; 4096^2 records).
+  if (ncp_ll > static_cast<long long>(kNoAllocScratchBytes / sizeof(jsi::Vec4<float>)) || nuv > 4096)
+    return JSI_ERR_CAPACITY;
+  const size_t ncp = static_cast<size_t>(ncp_ll);
 
-  const size_t bu = round256(nku * sizeof(float)), bv = round256(nkv * sizeof(float));
+  const size_t bu = round256(static_cast<size_t>(nku) * sizeof(float));
+  const size_t bv = round256(static_cast<size_t>(nkv) * sizeof(float));
   const size_t bc = round256(ncp * sizeof(jsi::Vec4<float>));
   const size_t nrec = static_cast<size_t>(nuv) * nuv * JSI_RECORD_SIZE;
   const size_t br = round256(nrec * sizeof(float));
   if (bu + bv + bc + br > kNoAllocScratchBytes) return JSI_ERR_CAPACITY;
 
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) {
-    cudaGetLastError();
-    return JSI_ERR_NO_DEVICE;
-  }
-  if (dev < 0 || dev >= kMaxDevices) return JSI_ERR_UNSUPPORTED;
   unsigned char *base = nullptr;
-  if (const int st = scratch_address(dev, &base); st != JSI_OK) return st;
+  if (const int st = scratch_address(&base); st != JSI_OK) return st;
 
   float *dU = reinterpret_cast<float *>(base);
   float *dV = reinterpret_cast<float *>(base + bu);

@@ -2,6 +2,7 @@
 binary cache."""
 from __future__ import annotations
 
+import os
 from pathlib import Path
 
 import numpy as np
@@ -9,7 +10,9 @@ import pytest
 
 from jsi_cad_next_versions_b200 import ingest, synth
 
-REF_DATA = Path("/root/reference/JSI_CAD_NEXT_VERSION5/examples/data")
+# The reference checkout (its data files are read where present, else skipped).
+REF_DATA = (Path(os.environ.get("JSI_REFERENCE_ROOT", str(Path(__file__).resolve().parents[2] / "reference")))
+            / "JSI_CAD_NEXT_VERSION5" / "examples" / "data")
 
 
 def test_source_round_trip_is_exact():
