@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define JSI_B200_ABI_VERSION 2
+#define JSI_B200_ABI_VERSION 3
 #define JSI_MAX_ROUNDS 16
 #define JSI_RECORD_SIZE 18 /* ONE_UV_SIZE, include/jsi_cad.hpp:45 */
 
@@ -41,9 +41,13 @@ typedef enum {
  *  FP32_SCREEN  - FP32 evaluation / boxes / screening with every box widened
  *                 by a rigorous rounding-error bound, FP64 knot spans, basis
  *                 and rational division, FP64 re-check of the screened
- *                 candidates; results equal the FP64 form's.  The
- *                 intersection query has no FP32 stage (each surviving pair
- *                 needs its exact FP64 boxes) and runs as FP64. */
+ *                 candidates; results equal the FP64 form's.  Distance: the
+ *                 first round screens in FP32.  Intersection: the first
+ *                 round's samples, curvature terms, cell boxes and overlap
+ *                 screen run in FP32 (the compute_K maxima are made exact by
+ *                 re-evaluating in FP64 only the samples whose FP32 bound
+ *                 reaches the maximum), every candidate pair is re-checked
+ *                 with FP64 boxes, and later rounds run in FP64. */
 typedef enum { JSI_PREC_V5_FP32 = 0, JSI_PREC_FP64 = 1, JSI_PREC_FP32_SCREEN = 2 } jsi_precision;
 
 typedef struct jsi_context jsi_context;
@@ -153,6 +157,16 @@ typedef struct {
   long long tile_pairs[JSI_MAX_ROUNDS]; /* tile pairs that passed the bound screen per round */
   long long tile_pairs_tested[JSI_MAX_ROUNDS]; /* tile pairs whose bound (or representative) was evaluated */
   long long supertile_pairs[JSI_MAX_ROUNDS];   /* supertile pairs that passed their bound (two-level rounds) */
+  /* Optional trace of the first round's screen candidates (caller-owned, may
+   * be null; jsi_min_distance only): the (slot, i, j) triples that passed the
+   * screen, in no particular order, with each pair's FP64 squared centre
+   * distance in cand_d2 (FP64 and FP32_SCREEN forms; V5_FP32: the FP32 value).
+   * Every pair whose d2 is at most the round's k-th value is among them.
+   * cand_written counts all candidates (also those beyond cand_cap). */
+  int *cand_pairs;
+  double *cand_d2;
+  long long cand_cap;
+  long long cand_written;
 } jsi_dist_result;
 
 void jsi_dist_params_default(jsi_dist_params *p);
@@ -196,6 +210,16 @@ typedef struct {
   long long points_written;
   long long points_converged;
   float device_ms;
+  /* FP32_SCREEN only (else 0): the first round's FP32 screen.  screen_written
+   * counts its candidate (slot, i, j) triples (a superset of the FP64 form's
+   * round-1 pairs, which the FP64 re-check then keeps); when screen_pairs is
+   * set (caller-owned) up to screen_cap of them are written there in
+   * (slot, i, j) order.  kmax_rechecked counts the samples whose curvature
+   * terms were re-evaluated in FP64 to get the exact compute_K maxima. */
+  int *screen_pairs;
+  long long screen_cap;
+  long long screen_written;
+  long long kmax_rechecked;
 } jsi_inter_result;
 
 void jsi_inter_params_default(jsi_inter_params *p);

@@ -61,7 +61,9 @@ class DistResult(ctypes.Structure):
                 ("candidates", ctypes.c_longlong * MAX_ROUNDS), ("trace_pairs", ctypes.POINTER(ctypes.c_int)),
                 ("trace_cap", ctypes.c_longlong), ("device_ms", ctypes.c_float),
                 ("tile_pairs", ctypes.c_longlong * MAX_ROUNDS), ("tile_pairs_tested", ctypes.c_longlong * MAX_ROUNDS),
-                ("supertile_pairs", ctypes.c_longlong * MAX_ROUNDS)]
+                ("supertile_pairs", ctypes.c_longlong * MAX_ROUNDS),
+                ("cand_pairs", ctypes.POINTER(ctypes.c_int)), ("cand_d2", ctypes.POINTER(ctypes.c_double)),
+                ("cand_cap", ctypes.c_longlong), ("cand_written", ctypes.c_longlong)]
 
 
 class InterParams(ctypes.Structure):
@@ -77,7 +79,9 @@ class InterResult(ctypes.Structure):
                 ("trace_pairs", ctypes.POINTER(ctypes.c_int)), ("trace_cap", ctypes.c_longlong),
                 ("trace_written", ctypes.c_longlong), ("points", ctypes.POINTER(ctypes.c_double)),
                 ("points_cap", ctypes.c_longlong), ("points_written", ctypes.c_longlong),
-                ("points_converged", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+                ("points_converged", ctypes.c_longlong), ("device_ms", ctypes.c_float),
+                ("screen_pairs", ctypes.POINTER(ctypes.c_int)), ("screen_cap", ctypes.c_longlong),
+                ("screen_written", ctypes.c_longlong), ("kmax_rechecked", ctypes.c_longlong)]
 
 
 class CurveParams(ctypes.Structure):

@@ -51,6 +51,9 @@ class DistanceResult:
     tile_pairs: np.ndarray = None  # tile pairs that passed the bound screen, per round
     tile_pairs_tested: np.ndarray = None  # tile pairs whose bound or representative was evaluated, per round
     supertile_pairs: np.ndarray = None  # supertile pairs that passed their bound, per round
+    # first round's screen candidates (cand_trace=True): (m, 3) int32 (slot, i, j) and their FP64 d2
+    cand_pairs: np.ndarray | None = None
+    cand_d2: np.ndarray | None = None
 
 
 def _struct_dtype(st) -> np.dtype:
@@ -232,6 +235,12 @@ class IntersectionResult:
     pairs: list = field(default_factory=list)  # per round (n, 3) int32 if traced
     points: np.ndarray | None = None  # (n, 8): x, y, z, u, v, s, t, residual
     points_converged: int = 0
+    # FP32_SCREEN: the first round's FP32 candidates (count; (m, 3) (slot, i, j)
+    # in key order when screen_trace=True) and the samples re-evaluated in FP64
+    # for the exact compute_K maxima
+    screen_written: int = 0
+    screen_pairs: np.ndarray | None = None
+    kmax_rechecked: int = 0
 
 
 class Context:
@@ -383,7 +392,8 @@ class Context:
             supertile_pairs=np.array(r.supertile_pairs[:n], dtype=np.int64))
 
     def min_distance(self, a: C.Task, b: C.Task, *, k: int = 8, rounds: int = 4, nuv_refine: int = 16,
-                     precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False) -> DistanceResult:
+                     precision: str | int = "v5_fp32", newton: bool = False, trace: bool = False,
+                     cand_trace: bool = False, cand_cap: int = 1 << 22) -> DistanceResult:
         p = self._dist_params(k, rounds, nuv_refine, precision, newton)
         r = C.DistResult()
         buf = None
@@ -391,9 +401,23 @@ class Context:
             buf = np.full(rounds * k * 3, -1, dtype=np.int32)
             r.trace_pairs = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
             r.trace_cap = rounds * k
+        cbuf = cd2 = None
+        if cand_trace:
+            cbuf = np.full(cand_cap * 3, -1, dtype=np.int32)
+            cd2 = np.full(cand_cap, np.nan, dtype=np.float64)
+            r.cand_pairs = cbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            r.cand_d2 = cd2.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            r.cand_cap = cand_cap
         self._check(self.lib.jsi_min_distance(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
                                               ctypes.byref(r)))
-        return self._dist_result(r, buf, k)
+        res = self._dist_result(r, buf, k)
+        if cand_trace:
+            m = int(r.cand_written)
+            if m > cand_cap:
+                raise JsiError(-4, f"{m} screen candidates exceed cand_cap {cand_cap}")
+            res.cand_pairs = cbuf[:3 * m].reshape(-1, 3).copy()
+            res.cand_d2 = cd2[:m].copy()
+        return res
 
     # -- worker lanes: queued / batched queries ----------------------------
     def workers(self, n: int, lane_bytes: int = 0):
@@ -556,7 +580,8 @@ class Context:
     def intersect(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                   halve_threshold: int = 512, min_nuv: int = 4, precision: str | int = "v5_fp32",
                   trace: bool = False, trace_cap: int = 1 << 24, points: bool = False,
-                  points_cap: int = 1 << 22) -> IntersectionResult:
+                  points_cap: int = 1 << 22, screen_trace: bool = False,
+                  screen_cap: int = 1 << 24) -> IntersectionResult:
         prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         p = C.InterParams(nuv_refine, 1 if use_k else 0, rounds, halve_threshold, min_nuv, prec, 1 if points else 0)
         r = C.InterResult()
@@ -570,9 +595,21 @@ class Context:
             pbuf = np.zeros(points_cap * 8, dtype=np.float64)
             r.points = pbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             r.points_cap = points_cap
+        sbuf = None
+        if screen_trace:
+            sbuf = np.full(screen_cap * 3, -1, dtype=np.int32)
+            r.screen_pairs = sbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            r.screen_cap = screen_cap
         self._check(self.lib.jsi_intersect(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(p),
                                            ctypes.byref(r)))
         res = self._inter_result(r, buf, trace_cap)
+        res.screen_written = int(r.screen_written)
+        res.kmax_rechecked = int(r.kmax_rechecked)
+        if screen_trace:
+            m = int(r.screen_written)
+            if m > screen_cap:
+                raise JsiError(-4, f"{m} screen candidates exceed screen_cap {screen_cap}")
+            res.screen_pairs = sbuf[:3 * m].reshape(-1, 3).copy()
         if points:
             res.points = pbuf[:r.points_written * 8].reshape(-1, 8).copy()
             res.points_converged = int(r.points_converged)

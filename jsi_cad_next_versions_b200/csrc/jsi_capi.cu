@@ -919,20 +919,34 @@ constexpr unsigned long long kMaxTilePairs = 1ull << 27;
 // homogeneous sums (w CP, w), then the FP64 division.  Centres add one FP32
 // and one FP64 rounding of (lo + hi) / 2.  Margins (x1.01) cover the basis
 // sums deviating from 1 by FP64 rounding.
-void centre_error(const SurfaceRec &s, double ec[3]) {
+// gamma_n(u32) + gamma_n(u64) for the n = degu + degv + 6 roundings of
+// either contraction chain of a surface.
+double screen_gamma(const SurfaceRec &s) {
   const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
   const double n = s.ivec[1] + s.ivec[4] + 6;
-  const double g = n * u32 / (1 - n * u32) + n * u64 / (1 - n * u64);
+  return n * u32 / (1 - n * u32) + n * u64 / (1 - n * u64);
+}
+
+// Per-coordinate bound of |P32 - P64| for the samples themselves (before the
+// centre's rounding).
+void sample_error(const SurfaceRec &s, double es[3]) {
+  const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+  const double g = screen_gamma(s);
   for (int c = 0; c < 3; ++c) {
-    double ep;
     if (!s.rat) {
-      ep = g * s.cmax[c] * 1.01;
+      es[c] = g * s.cmax[c] * 1.01;
     } else {
       const double ehx = g * s.wcmax[c] * 1.01, ehw = g * s.wmax * 1.01;
-      ep = (ehx + s.cmax[c] * ehw) / (s.wmin - ehw) + 4 * u64 * s.cmax[c] + u32 * s.cmax[c];
+      es[c] = (ehx + s.cmax[c] * ehw) / (s.wmin - ehw) + 4 * u64 * s.cmax[c] + u32 * s.cmax[c];
     }
-    ec[c] = (ep + (u32 + u64) * (s.cmax[c] + ep)) * 1.01;
   }
+}
+
+void centre_error(const SurfaceRec &s, double ec[3]) {
+  const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+  double ep[3];
+  sample_error(s, ep);
+  for (int c = 0; c < 3; ++c) ec[c] = (ep[c] + (u32 + u64) * (s.cmax[c] + ep[c])) * 1.01;
 }
 
 float screen_error(const SurfaceRec &a, const SurfaceRec &b) {
@@ -954,7 +968,7 @@ float screen_error(const SurfaceRec &a, const SurfaceRec &b) {
 template <typename TC, typename TS, typename Verify>
 int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B, const int *map1,
                       const int *map2, int nslots, int k, bool screen, float e, DistCand<TS> *top, Verify &&verify,
-                      long long *tests, long long *cands) {
+                      long long *tests, long long *cands, jsi_dist_result *trace = nullptr) {
   Arena &ar = ctx->arena;
   cudaStream_t st = ctx->stream;
   const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
@@ -1044,6 +1058,7 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
       JSI_CUDA(cudaMemsetAsync(&ctx->d_stats->work, 0, sizeof(unsigned long long), st));
     }
   }
+  const DistCand<TS> *checked_out = nullptr;  // the screen's candidates with their FP64 d2
   for (int attempt = 0;; ++attempt) {
     timed(ctx, "dist_leaf", [&] {
       launch_dist_leaf(A, B, map1, map2, leaf_surv, leaf_lb, nsurv, nsurv, leaf_lb != nullptr, k, 1, cand, cand_cap,
@@ -1061,6 +1076,7 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
         DistCand<TS> *checked = ar.get<DistCand<TS>>(std::max<unsigned long long>(m, 1));
         timed(ctx, "dist_verify", [&] { verify(cand, static_cast<long long>(m), checked); });
         timed(ctx, "dist_select", [&] { launch_dist_select(checked, m, k, top, ctx->d_stats, st); });
+        checked_out = checked;
       }
     }
     pull_stats(ctx);
@@ -1081,7 +1097,39 @@ int dist_screen_round(Lane *ctx, const SideRound<TC> &A, const SideRound<TC> &B,
   *tests = static_cast<long long>(ctx->h_stats->pair_tests);
   *cands = static_cast<long long>(ctx->h_stats->candidates);
   add_units(ctx, "dist_leaf", static_cast<double>(*tests));
-  return ctx->h_stats->nsel;
+  const int nsel = ctx->h_stats->nsel;
+  if (trace && trace->cand_pairs) {
+    // The screen's candidate set: with the FP64 d2 of each (re-checked for
+    // the FP32 screen), so that a caller can check it holds every pair whose
+    // d2 is at most the k-th value.
+    const long long m = *cands;
+    const long long keep = std::min<long long>(m, trace->cand_cap);
+    if (keep > 0) {
+      std::vector<unsigned char> h;
+      if constexpr (std::is_same<TC, TS>::value) {
+        h.resize(static_cast<size_t>(keep) * sizeof(DistCand<TC>));
+        JSI_CUDA(copy_async(ctx, h.data(), cand, h.size(), cudaMemcpyDeviceToHost, st));
+      } else {
+        h.resize(static_cast<size_t>(keep) * sizeof(DistCand<TS>));
+        JSI_CUDA(copy_async(ctx, h.data(), checked_out, h.size(), cudaMemcpyDeviceToHost, st));
+      }
+      JSI_CUDA(cudaStreamSynchronize(st));
+      for (long long q = 0; q < keep; ++q) {
+        int *tp = trace->cand_pairs + q * 3;
+        double d2;
+        if constexpr (std::is_same<TC, TS>::value) {
+          const DistCand<TC> &c = reinterpret_cast<const DistCand<TC> *>(h.data())[q];
+          tp[0] = c.slot, tp[1] = c.i, tp[2] = c.j, d2 = static_cast<double>(c.d2);
+        } else {
+          const DistCand<TS> &c = reinterpret_cast<const DistCand<TS> *>(h.data())[q];
+          tp[0] = c.slot, tp[1] = c.i, tp[2] = c.j, d2 = static_cast<double>(c.d2);
+        }
+        if (trace->cand_d2) trace->cand_d2[q] = d2;
+      }
+    }
+    trace->cand_written = m;
+  }
+  return nsel;
 }
 
 // Query rectangles as Newton bounds {u0, u1, v0, v1, s0, s1, t0, t1}.
@@ -1174,7 +1222,8 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
     if (!kScreen || round > 1) {
       build_side(ctx, pa, A, false, false, TP(1), TP(1));
       build_side(ctx, pb, B, false, false, TP(1), TP(1));
-      n = dist_screen_round<TP, TP>(ctx, A, B, map1, map2, nslots, k, false, 0.0f, top, NoVerify{}, &tests, &cands);
+      n = dist_screen_round<TP, TP>(ctx, A, B, map1, map2, nslots, k, false, 0.0f, top, NoVerify{}, &tests, &cands,
+                                    round == 1 ? out : nullptr);
     } else if constexpr (kScreen) {
       // FP64 rectangles and basis tables, FP32 samples / cells / tiles.
       SideRound<TC> A32{}, B32{};
@@ -1194,7 +1243,7 @@ void run_distance(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_d
       auto verify = [&](const DistCand<TC> *c, long long m, DistCand<TP> *o) {
         launch_dist_verify(pa, pb, A, B, map1, map2, c, m, o, st);
       };
-      n = dist_screen_round<TC, TP>(ctx, A32, B32, map1, map2, nslots, k, true, e, top, verify, &tests, &cands);
+      n = dist_screen_round<TC, TP>(ctx, A32, B32, map1, map2, nslots, k, true, e, top, verify, &tests, &cands, out);
     }
     out->npairs[round - 1] = n;
     out->pair_tests[round - 1] = tests;
@@ -1785,6 +1834,147 @@ void next_regions(Lane *ctx, const unsigned long long *sorted, long long n, int 
   *nmap2_out = nmap2;
 }
 
+// Per-axis widening w of the intersection's FP32 overlap screen for a pair
+// of surfaces.  The FP64 form keeps (i, j) when, on every axis,
+// fl(|c1 - c2|) < fl((h1 + p1) + (h2 + p2)) over its FP64 centres and half
+// spans; with the exact centres and half spans of the FP64 samples that
+// implies |c1 - c2| < h1 + h2 + p1 + p2 + R64, R64 <= 9 u64 (C1 + C2) +
+// 4 u64 (p1 + p2), C = max |coordinate| (the samples lie in the control
+// net's convex hull: non-negative basis, positive weights).  FP32 samples
+// within e of the FP64 ones move each centre and each half span by at most
+// e, and the FP32 centres / half spans round once more (u32 C').  The FP32
+// screen keeps (i, j) when fl(|c1 - c2|) < fl(fl(h1 + h2) + Q): with
+// Q >= p1 + p2 + 2 (e1 + e2) + 8.2 u32 (C1' + C2') + R64, all times
+// (1 + 4 u32) for the screen's own three roundings, every pair the FP64
+// form keeps passes.  Here Q = ru((p1 + p2)(1 + 2^-20) + w) on the device
+// (iscreen_q) with w = 1.01 (2 (e1 + e2) + 10 u32 (C + e) + 10 u64 C).
+void inter_screen_widen(const SurfaceRec &a, const SurfaceRec &b, float w[3]) {
+  const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+  double ea[3], eb[3];
+  sample_error(a, ea);
+  sample_error(b, eb);
+  for (int c = 0; c < 3; ++c) {
+    const double C = (a.cmax[c] + b.cmax[c]) * 1.01, e = ea[c] + eb[c];
+    const double W = (2 * e + 10 * u32 * (C + e) + 10 * u64 * C) * 1.01;
+    w[c] = std::nextafter(static_cast<float>(W), INFINITY);
+  }
+}
+
+// The first round of the FP32-screen intersection (intersection.cu:175-219,
+// 259-309 with every box and test in FP32, widened): FP64 spans and basis
+// tables; FP32 samples and curvature bounds; the exact FP64 compute_K maxima
+// and paddings; FP32 cells, tile cull and cell-pair screen; FP64 re-check of
+// every candidate.  Returns the FP64 form's overlap keys, unordered.
+void inter_screen_round(Lane *ctx, const SurfaceRec &sa, const SurfaceRec &sb, SideRound<double> &A,
+                        SideRound<double> &B, bool use_k, const double span0[2][2], const int *map1,
+                        const int *map2, int ij_bits, int slot_bits, jsi_inter_result *out,
+                        unsigned long long **keys_out, long long *n_out, long long *tests_out) {
+  Arena &ar = ctx->arena;
+  cudaStream_t st = ctx->stream;
+  if ((sa.rat && !(sa.wmin > 0)) || (sb.rat && !(sb.wmin > 0)))
+    fail(JSI_ERR_UNSUPPORTED, "FP32 screen needs positive weights");
+  float w[3];
+  inter_screen_widen(sa, sb, w);
+  reset_stats(ctx);
+  SideRound<float> S32[2];
+  for (int side = 0; side < 2; ++side) {
+    SideRound<double> &P = side ? B : A;
+    const SurfaceRec &s = side ? sb : sa;
+    SideRound<float> &C = S32[side];
+    C = SideRound<float>{};
+    C.g = P.g;
+    C.nreg = P.nreg;
+    const size_t nsamp = static_cast<size_t>(P.nreg) * P.g.nuv * P.g.nuv;
+    C.samples = ar.get<Vec4<float>>(nsamp);
+    C.center = ar.get<Vec4<float>>(static_cast<size_t>(P.nreg) * P.g.cpr);
+    C.half = ar.get<Vec4<float>>(static_cast<size_t>(P.nreg) * P.g.cpr);
+    C.tlo = ar.get<Vec4<float>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
+    C.thi = ar.get<Vec4<float>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
+    C.thmax = ar.get<Vec4<float>>(static_cast<size_t>(P.nreg) * P.g.ntiles);
+    const SurfView<double> v64 = view<double>(s);
+    timed(ctx, "basis", [&] { launch_basis(v64, P, st, Batch{}, static_cast<const SurfView<double> *>(nullptr)); },
+          2.0 * P.nreg * P.g.nuv);
+    Vec4<float> *khi = use_k ? ar.get<Vec4<float>>(nsamp) : nullptr;
+    unsigned *klo = use_k ? ar.get<unsigned>(static_cast<size_t>(P.nreg) * 3) : nullptr;
+    if (use_k) {
+      JSI_CUDA(cudaMemsetAsync(klo, 0, sizeof(unsigned) * 3 * P.nreg, st));
+      JSI_CUDA(cudaMemsetAsync(P.kmax, 0, sizeof(unsigned long long) * 3 * P.nreg, st));
+    }
+    timed(ctx, "samples", [&] {
+      launch_iscreen_samples(view<float>(s), P, C, use_k, khi, klo, screen_gamma(s) * 1.01, s.cmax, s.wcmax, s.wmax,
+                             st);
+    }, double(nsamp));
+    if (use_k)
+      timed(ctx, "kmax_recheck", [&] { launch_kmax_recheck(v64, P, khi, klo, &ctx->d_stats->rechecked, st); });
+    timed(ctx, "pad", [&] { launch_pad<double>(P, use_k, span0[side][0], span0[side][1], st); });
+    timed(ctx, "cells", [&] { launch_cells<float>(C, true, st); }, double(C.nreg) * C.g.W * C.g.W);
+  }
+  JSI_CUDA(cudaGetLastError());
+  const unsigned long long tile_pairs = static_cast<unsigned long long>(A.g.ntiles) * B.g.ntiles;
+  if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+  unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+  timed(ctx, "inter_cull", [&] {
+    launch_inter_cull_screen(S32[0], S32[1], map1, map2, 1, surv, tile_pairs, ctx->d_stats, w, A.pad, B.pad, st);
+  }, double(tile_pairs));
+  pull_stats(ctx);
+  const unsigned long long nsurv = ctx->h_stats->survivors;
+  unsigned long long key_cap =
+      std::max<unsigned long long>(1ull << 16, std::min<unsigned long long>(nsurv * 64, 1ull << 24));
+  unsigned long long *keys = ar.get<unsigned long long>(key_cap);
+  for (int attempt = 0;; ++attempt) {
+    timed(ctx, "inter_leaf", [&] {
+      launch_inter_leaf_screen(S32[0], S32[1], map1, map2, surv, nsurv, ij_bits, keys, key_cap, ctx->d_stats, w, A.pad,
+                               B.pad, st);
+    });
+    pull_stats(ctx);
+    ScreenStats &hs = *ctx->h_stats;
+    if (hs.candidates <= key_cap) break;
+    if (attempt >= 1) fail(JSI_ERR_CAPACITY, "overlap list overflow");
+    key_cap = hs.candidates;
+    keys = ar.get<unsigned long long>(key_cap);
+    hs.candidates = 0;
+    hs.pair_tests = 0;
+    hs.work = 0;
+    JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+  }
+  const unsigned long long m = ctx->h_stats->candidates;
+  *tests_out = static_cast<long long>(ctx->h_stats->pair_tests);
+  add_units(ctx, "inter_leaf", static_cast<double>(ctx->h_stats->pair_tests));
+  add_units(ctx, "inter_cull", static_cast<double>(tile_pairs));
+  unsigned long long *kept = ar.get<unsigned long long>(std::max<unsigned long long>(m, 1));
+  timed(ctx, "inter_verify", [&] {
+    launch_inter_verify(view<double>(sa), view<double>(sb), A, B, map1, map2, keys, m, ij_bits, kept, m,
+                        ctx->d_stats, st);
+  }, double(m));
+  pull_stats(ctx);
+  out->screen_written = static_cast<long long>(m);
+  out->kmax_rechecked = static_cast<long long>(ctx->h_stats->rechecked);
+  if (out->screen_pairs && m > 0) {
+    // The screen's candidates in (slot, i, j) order, for a superset check.
+    const int end_bit = 2 * ij_bits + slot_bits;
+    unsigned long long *alt = ar.get<unsigned long long>(m);
+    size_t tmp_bytes = 0;
+    cub::DoubleBuffer<unsigned long long> db(keys, alt);
+    JSI_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(m), 0, end_bit, st));
+    void *tmp = ar.alloc(tmp_bytes);
+    JSI_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, static_cast<int>(m), 0, end_bit, st));
+    const long long keep = std::min<long long>(static_cast<long long>(m), out->screen_cap);
+    std::vector<unsigned long long> h(static_cast<size_t>(std::max<long long>(keep, 0)));
+    if (keep > 0)
+      JSI_CUDA(copy_async(ctx, h.data(), db.Current(), keep * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    JSI_CUDA(cudaStreamSynchronize(st));
+    const unsigned long long mij = (1ull << ij_bits) - 1ull;
+    for (long long q = 0; q < keep; ++q) {
+      int *tp = out->screen_pairs + q * 3;
+      tp[0] = static_cast<int>(h[q] >> (2 * ij_bits));
+      tp[1] = static_cast<int>((h[q] >> ij_bits) & mij);
+      tp[2] = static_cast<int>(h[q] & mij);
+    }
+  }
+  *keys_out = kept;
+  *n_out = static_cast<long long>(ctx->h_stats->checked);
+}
+
 // The final round of an intersection query, for the curve linking.
 template <typename T>
 struct FinalRound {
@@ -1800,9 +1990,12 @@ struct FinalRound {
 // cover: sample the covering grid (every refined cell sampled to its far edge)
 // instead of the reference's grid; used by the curve linking, whose points
 // would otherwise skip the last strip of every refined cell.
+// screen (T = double only): the first round runs the FP32 screen
+// (inter_screen_round); its result, and so every later round, equals the
+// FP64 form's.
 template <typename T>
 void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
-                      jsi_inter_result *out, FinalRound<T> *fin = nullptr, bool cover = false) {
+                      jsi_inter_result *out, FinalRound<T> *fin = nullptr, bool cover = false, bool screen = false) {
   Arena &ar = ctx->arena;
   cudaStream_t st = ctx->stream;
   const SurfaceRec &sa = get_surface(ctx, ta->surface);
@@ -1834,8 +2027,23 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
   std::vector<unsigned long long> hkeys;
   for (int round = 1; round <= p->rounds; ++round) {
     const int sau = round == 1 ? side_a : 1, sbu = round == 1 ? side_b : 2;
-    build_side(ctx, va, A, true, use_k, span_u[sau], span_v[sau], cover);
-    build_side(ctx, vb, B, true, use_k, span_u[sbu], span_v[sbu], cover);
+    const bool screen_now = screen && round == 1 && !cover;
+    if (!screen_now) {
+      build_side(ctx, va, A, true, use_k, span_u[sau], span_v[sau], cover);
+      build_side(ctx, vb, B, true, use_k, span_u[sbu], span_v[sbu], cover);
+    }
+    const int ij_bits = std::max(1, bit_width(static_cast<unsigned long long>(
+                                        std::max(A.g.W * A.g.W, B.g.W * B.g.W) - 1)));
+    const int slot_bits = std::max(1, bit_width(static_cast<unsigned long long>(nslots - 1)));
+    if (2 * ij_bits + slot_bits > 64) fail(JSI_ERR_CAPACITY, "pair key does not fit 64 bits");
+    unsigned long long *keys = nullptr;
+    long long n = 0, tests = 0;
+    if (screen_now) {
+      if constexpr (std::is_same<T, double>::value) {
+        const double span0[2][2] = {{span_u[sau], span_v[sau]}, {span_u[sbu], span_v[sbu]}};
+        inter_screen_round(ctx, sa, sb, A, B, use_k, span0, map1, map2, ij_bits, slot_bits, out, &keys, &n, &tests);
+      }
+    }
     if (round == 1) {
       T pads[2];
       JSI_CUDA(copy_async(ctx, &pads[0], A.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
@@ -1844,37 +2052,41 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
       out->pad[0] = static_cast<double>(pads[0]);
       out->pad[1] = static_cast<double>(pads[1]);
     }
-    const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
-    if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
-    const int ij_bits = std::max(1, bit_width(static_cast<unsigned long long>(
-                                            std::max(A.g.W * A.g.W, B.g.W * B.g.W) - 1)));
-    const int slot_bits = std::max(1, bit_width(static_cast<unsigned long long>(nslots - 1)));
-    if (2 * ij_bits + slot_bits > 64) fail(JSI_ERR_CAPACITY, "pair key does not fit 64 bits");
-    unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
-    reset_stats(ctx);
-    timed(ctx, "inter_cull", [&] { launch_inter_cull(A, B, map1, map2, static_cast<int>(nslots), surv, tile_pairs, ctx->d_stats, st); });
-    pull_stats(ctx);
-    const unsigned long long nsurv = ctx->h_stats->survivors;
-    unsigned long long key_cap = std::max<unsigned long long>(1ull << 16, std::min<unsigned long long>(nsurv * 64, 1ull << 24));
-    unsigned long long *keys = ar.get<unsigned long long>(key_cap);
-    for (int attempt = 0;; ++attempt) {
-      timed(ctx, "inter_leaf", [&] { launch_inter_leaf(A, B, map1, map2, surv, nsurv, ij_bits, keys, key_cap, ctx->d_stats, st); });
+    if (!screen_now) {
+      const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
+      if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+      unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
+      reset_stats(ctx);
+      timed(ctx, "inter_cull", [&] {
+        launch_inter_cull(A, B, map1, map2, static_cast<int>(nslots), surv, tile_pairs, ctx->d_stats, st);
+      });
       pull_stats(ctx);
-      ScreenStats &hs = *ctx->h_stats;
-      if (hs.candidates <= key_cap) break;
-      if (attempt >= 1) fail(JSI_ERR_CAPACITY, "overlap list overflow");
-      key_cap = hs.candidates;
+      const unsigned long long nsurv = ctx->h_stats->survivors;
+      unsigned long long key_cap =
+          std::max<unsigned long long>(1ull << 16, std::min<unsigned long long>(nsurv * 64, 1ull << 24));
       keys = ar.get<unsigned long long>(key_cap);
-      hs.candidates = 0;
-      hs.pair_tests = 0;
-      hs.work = 0;
-      JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+      for (int attempt = 0;; ++attempt) {
+        timed(ctx, "inter_leaf", [&] {
+          launch_inter_leaf(A, B, map1, map2, surv, nsurv, ij_bits, keys, key_cap, ctx->d_stats, st);
+        });
+        pull_stats(ctx);
+        ScreenStats &hs = *ctx->h_stats;
+        if (hs.candidates <= key_cap) break;
+        if (attempt >= 1) fail(JSI_ERR_CAPACITY, "overlap list overflow");
+        key_cap = hs.candidates;
+        keys = ar.get<unsigned long long>(key_cap);
+        hs.candidates = 0;
+        hs.pair_tests = 0;
+        hs.work = 0;
+        JSI_CUDA(copy_async(ctx, ctx->d_stats, &hs, sizeof(ScreenStats), cudaMemcpyHostToDevice, st));
+      }
+      n = static_cast<long long>(ctx->h_stats->candidates);
+      tests = static_cast<long long>(ctx->h_stats->pair_tests);
+      add_units(ctx, "inter_leaf", static_cast<double>(tests));
+      add_units(ctx, "inter_cull", static_cast<double>(tile_pairs));
     }
-    const long long n = static_cast<long long>(ctx->h_stats->candidates);
-    add_units(ctx, "inter_leaf", static_cast<double>(ctx->h_stats->pair_tests));
-    add_units(ctx, "inter_cull", static_cast<double>(tile_pairs));
     out->counts[round - 1] = n;
-    out->pair_tests[round - 1] = static_cast<long long>(ctx->h_stats->pair_tests);
+    out->pair_tests[round - 1] = tests;
     out->regions1[round - 1] = A.nreg;
     out->regions2[round - 1] = B.nreg;
     out->rounds_run = round;
@@ -2462,22 +2674,24 @@ void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_
   const long long tc = out->trace_cap;
   double *pts = out->points;
   const long long pc = out->points_cap;
+  int *sp = out->screen_pairs;
+  const long long sc = out->screen_cap;
   std::memset(out, 0, sizeof(*out));
   out->trace_pairs = tp;
   out->trace_cap = tc;
   out->points = pts;
   out->points_cap = pc;
+  out->screen_pairs = sp;
+  out->screen_cap = sc;
   JSI_CUDA(cudaSetDevice(L->device));
   L->arena.reset();
   JSI_CUDA(cudaEventRecord(L->ev0, L->stream));
-  // The intersection query has no FP32 stage: every overlapping pair needs its
-  // exact FP64 boxes (and the FP64 curvature padding of its regions), which
-  // costs what the FP64 evaluation it would replace costs.  FP32_SCREEN
-  // therefore runs the FP64 form.
+  // FP32_SCREEN: the first round screens in FP32 and re-checks in FP64, so
+  // every round's pairs equal the FP64 form's.
   if (p.precision == JSI_PREC_V5_FP32)
     run_intersection<float>(L, a, b, &p, out);
   else
-    run_intersection<double>(L, a, b, &p, out);
+    run_intersection<double>(L, a, b, &p, out, nullptr, false, p.precision == JSI_PREC_FP32_SCREEN);
   JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
   JSI_CUDA(cudaEventSynchronize(L->ev1));
   JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));

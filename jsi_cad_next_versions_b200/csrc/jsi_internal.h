@@ -141,6 +141,8 @@ struct ScreenStats {
   int pad2_;
   unsigned long long lb_bits;       // bounds mode: smallest kept squared box gap (double bits)
   unsigned long long ub_bits;       // bounds mode: smallest corner-sample squared distance (double bits)
+  unsigned long long checked;       // intersection FP32 screen: candidates the FP64 re-check kept
+  unsigned long long rechecked;     // intersection FP32 screen: samples re-evaluated for the exact compute_K maxima
 };
 
 // Lockstep batch of queries that share one shape: query q runs in
@@ -302,6 +304,28 @@ template <typename T>
 void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *map1, const int *map2,
                        const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
                        unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats, cudaStream_t st);
+// FP32 screen of the intersection query (one round): FP32 samples (and, with
+// need_k, curvature terms with rigorous bounds: khi per sample, klo per
+// region) from the FP64 basis tables; exact FP64 curvature maxima from the
+// samples whose bound reaches the maximum (into bs.kmax, count += samples
+// re-evaluated); overlap screen widened per axis by w plus both regions' FP64
+// paddings; FP64 re-check of the candidate keys into out (stats->checked).
+void launch_iscreen_samples(const SurfView<float> &s, const SideRound<double> &bs, const SideRound<float> &out,
+                            bool need_k, Vec4<float> *khi, unsigned *klo, double g, const double cmax[3],
+                            const double wcmax[3], double wmax, cudaStream_t st);
+void launch_kmax_recheck(const SurfView<double> &s, const SideRound<double> &bs, const Vec4<float> *khi,
+                         const unsigned *klo, unsigned long long *count, cudaStream_t st);
+void launch_inter_cull_screen(const SideRound<float> &a, const SideRound<float> &b, const int *map1, const int *map2,
+                              int nslots, unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats,
+                              const float w[3], const double *pad64a, const double *pad64b, cudaStream_t st);
+void launch_inter_leaf_screen(const SideRound<float> &a, const SideRound<float> &b, const int *map1, const int *map2,
+                              const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
+                              unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats,
+                              const float w[3], const double *pad64a, const double *pad64b, cudaStream_t st);
+void launch_inter_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
+                         const SideRound<double> &b, const int *map1, const int *map2, const unsigned long long *keys,
+                         unsigned long long n, int ij_bits, unsigned long long *out, unsigned long long cap,
+                         ScreenStats *stats, cudaStream_t st);
 // Dedup of the next round's regions from sorted (slot, i, j) keys.
 void launch_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2, int *idx,
                        unsigned *flag1, cudaStream_t st);

@@ -1889,12 +1889,23 @@ __global__ void __launch_bounds__(1024) k_dist_pick(const unsigned long long *su
 // Intersection screening
 // ---------------------------------------------------------------------------
 
+// FP32-screen widening of one region pair, per axis: the FP64 paddings of
+// both regions (rounded up through a relative margin of 2^-20) plus the
+// host's bound w of the samples' FP32 error and every rounding on either
+// side; see inter_screen_widen in the host code.
+__device__ __forceinline__ float iscreen_q(double p1, double p2, float w) {
+  return __double2float_ru((p1 + p2) * (1.0 + 0x1p-20) + static_cast<double>(w));
+}
+
 // A tile pair is skipped only when, on some axis, the rounded gap between the
 // centre ranges reaches the rounded sum of the largest padded radii: then no
-// member pair passes the strict test of intersection.cu:60-62.
-template <typename T>
+// member pair passes the strict test of intersection.cu:60-62.  S (the FP32
+// screen, T = float): the radii sum is (h1 + h2) + Q with Q from
+// iscreen_q, and pad64a / pad64b hold the FP64 paddings.
+template <typename T, bool S>
 __global__ void k_inter_cull(SideRound<T> a, SideRound<T> b, const int *map1, const int *map2, int nslots,
-                             unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats) {
+                             unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats,
+                             Vec4<float> wq, const double *pad64a, const double *pad64b) {
   const Geom g1 = a.g, g2 = b.g;
   const long long nrows = static_cast<long long>(nslots) * g1.ntiles;
   const int lanes = blockDim.x;
@@ -1914,10 +1925,18 @@ __global__ void k_inter_cull(SideRound<T> a, SideRound<T> b, const int *map1, co
       const long long i2 = static_cast<long long>(r2) * g2.ntiles + t2;
       const Vec4<T> lo1 = a.tlo[i1], hi1 = a.thi[i1], h1 = a.thmax[i1];
       const Vec4<T> lo2 = b.tlo[i2], hi2 = b.thi[i2], h2 = b.thmax[i2];
-      const T p1 = a.pad[r1], p2 = b.pad[r2];
-      const bool sx = axis_gap(lo1.x, hi1.x, lo2.x, hi2.x) >= (h1.x + p1) + (h2.x + p2);
-      const bool sy = axis_gap(lo1.y, hi1.y, lo2.y, hi2.y) >= (h1.y + p1) + (h2.y + p2);
-      const bool sz = axis_gap(lo1.z, hi1.z, lo2.z, hi2.z) >= (h1.z + p1) + (h2.z + p2);
+      bool sx, sy, sz;
+      if constexpr (S) {
+        const double q1 = pad64a[r1], q2 = pad64b[r2];
+        sx = axis_gap(lo1.x, hi1.x, lo2.x, hi2.x) >= (h1.x + h2.x) + iscreen_q(q1, q2, wq.x);
+        sy = axis_gap(lo1.y, hi1.y, lo2.y, hi2.y) >= (h1.y + h2.y) + iscreen_q(q1, q2, wq.y);
+        sz = axis_gap(lo1.z, hi1.z, lo2.z, hi2.z) >= (h1.z + h2.z) + iscreen_q(q1, q2, wq.z);
+      } else {
+        const T p1 = a.pad[r1], p2 = b.pad[r2];
+        sx = axis_gap(lo1.x, hi1.x, lo2.x, hi2.x) >= (h1.x + p1) + (h2.x + p2);
+        sy = axis_gap(lo1.y, hi1.y, lo2.y, hi2.y) >= (h1.y + p1) + (h2.y + p2);
+        sz = axis_gap(lo1.z, hi1.z, lo2.z, hi2.z) >= (h1.z + p1) + (h2.z + p2);
+      }
       keep = !(sx || sy || sz);
     }
     const long long pos = warp_append(keep, &stats->survivors);
@@ -1930,12 +1949,14 @@ __global__ void k_inter_cull(SideRound<T> a, SideRound<T> b, const int *map1, co
 // Strict per-axis overlap of every cell pair of the surviving tile pairs
 // (intersection.cu:46-63), one warp per tile pair: tile-2 centres and padded
 // radii in registers, tile-1 cells broadcast row by row; hits are appended as
-// (slot, i, j) sort keys.
-template <typename T>
+// (slot, i, j) sort keys.  S (FP32 screen): |c1 - c2| < (h1 + h2) + Q per
+// axis, a superset of the FP64 form's pairs.
+template <typename T, bool S>
 __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T> b, const int *map1,
                                                     const int *map2, const unsigned long long *surv,
                                                     unsigned long long nsurv, int ij_bits, unsigned long long *keys,
-                                                    unsigned long long key_cap, ScreenStats *stats) {
+                                                    unsigned long long key_cap, ScreenStats *stats, Vec4<float> wq,
+                                                    const double *pad64a, const double *pad64b) {
   const Geom g1 = a.g, g2 = b.g;
   const int te1 = g1.te, te2 = g2.te;
   const int n1 = te1 * te1, n2 = te2 * te2;
@@ -1954,7 +1975,18 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
     const int r1 = map1[slot], r2 = map2[slot];
     const long long base1 = (static_cast<long long>(r1) * g1.ntiles + t1) * n1;
     const long long base2 = (static_cast<long long>(r2) * g2.ntiles + t2) * n2;
-    const T p1 = a.pad[r1], p2 = b.pad[r2];
+    // Per-cell radius terms: side 1 adds p1 (FP64 form) or nothing (screen);
+    // side 2 adds p2 (FP64 form) or the pair's widening Q (screen).
+    T p1, p2;
+    if constexpr (S) {
+      const double q1 = pad64a[r1], q2 = pad64b[r2];
+      p1 = T(0);
+      p2 = T(0);
+      wq = Vec4<float>{iscreen_q(q1, q2, wq.x), iscreen_q(q1, q2, wq.y), iscreen_q(q1, q2, wq.z), 0.0f};
+    } else {
+      p1 = a.pad[r1];
+      p2 = b.pad[r2];
+    }
     const int ty1 = t1 / g1.tw, tx1 = t1 - ty1 * g1.tw, ty2 = t2 / g2.tw, tx2 = t2 - ty2 * g2.tw;
     const int nv1 = min(te1, g1.W - ty1 * te1), nu1 = min(te1, g1.W - tx1 * te1);
     const int nv2 = min(te2, g2.W - ty2 * te2), nu2 = min(te2, g2.W - tx2 * te2);
@@ -1967,15 +1999,19 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
     Vec4<T> r2a = neg4, r2b = neg4;
     if (va) {
       r2a = b.half[base2 + ja];
-      r2a.x = r2a.x + p2;  // radius = x_span / 2 + curvature_padding
-      r2a.y = r2a.y + p2;
-      r2a.z = r2a.z + p2;
+      if constexpr (!S) {
+        r2a.x = r2a.x + p2;  // radius = x_span / 2 + curvature_padding
+        r2a.y = r2a.y + p2;
+        r2a.z = r2a.z + p2;
+      }
     }
     if (vb) {
       r2b = b.half[base2 + jb];
-      r2b.x = r2b.x + p2;
-      r2b.y = r2b.y + p2;
-      r2b.z = r2b.z + p2;
+      if constexpr (!S) {
+        r2b.x = r2b.x + p2;
+        r2b.y = r2b.y + p2;
+        r2b.z = r2b.z + p2;
+      }
     }
     const unsigned long long cja = static_cast<unsigned long long>((ty2 * te2 + ja_v) * g2.W + tx2 * te2 + ja_u);
     const unsigned long long cjb = static_cast<unsigned long long>((ty2 * te2 + jb_v) * g2.W + tx2 * te2 + jb_u);
@@ -1984,13 +2020,21 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
       for (int b1 = 0; b1 < nu1; ++b1) {
         const Vec4<T> c1 = a.center[base1 + a1 * te1 + b1];
         Vec4<T> r1 = a.half[base1 + a1 * te1 + b1];
-        r1.x = r1.x + p1;
-        r1.y = r1.y + p1;
-        r1.z = r1.z + p1;
-        const bool ha = fabs(c1.x - c2a.x) < (r1.x + r2a.x) && fabs(c1.y - c2a.y) < (r1.y + r2a.y) &&
-                        fabs(c1.z - c2a.z) < (r1.z + r2a.z);
-        const bool hb = fabs(c1.x - c2b.x) < (r1.x + r2b.x) && fabs(c1.y - c2b.y) < (r1.y + r2b.y) &&
-                        fabs(c1.z - c2b.z) < (r1.z + r2b.z);
+        bool ha, hb;
+        if constexpr (S) {
+          ha = fabs(c1.x - c2a.x) < (r1.x + r2a.x) + wq.x && fabs(c1.y - c2a.y) < (r1.y + r2a.y) + wq.y &&
+               fabs(c1.z - c2a.z) < (r1.z + r2a.z) + wq.z;
+          hb = fabs(c1.x - c2b.x) < (r1.x + r2b.x) + wq.x && fabs(c1.y - c2b.y) < (r1.y + r2b.y) + wq.y &&
+               fabs(c1.z - c2b.z) < (r1.z + r2b.z) + wq.z;
+        } else {
+          r1.x = r1.x + p1;
+          r1.y = r1.y + p1;
+          r1.z = r1.z + p1;
+          ha = fabs(c1.x - c2a.x) < (r1.x + r2a.x) && fabs(c1.y - c2a.y) < (r1.y + r2a.y) &&
+               fabs(c1.z - c2a.z) < (r1.z + r2a.z);
+          hb = fabs(c1.x - c2b.x) < (r1.x + r2b.x) && fabs(c1.y - c2b.y) < (r1.y + r2b.y) &&
+               fabs(c1.z - c2b.z) < (r1.z + r2b.z);
+        }
         if (__any_sync(kFull, ha || hb)) {
           const unsigned long long ci =
               static_cast<unsigned long long>((ty1 * te1 + a1) * g1.W + tx1 * te1 + b1) << ij_bits;
@@ -2379,6 +2423,321 @@ __global__ void k_samples_screen(SurfView<float> s, const SurfView<float> *vdev,
     const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
     out.samples[t] = screen_point(s, basis_side.spans[lu], basis_side.basis + lu * 3 * p1, basis_side.spans[lv],
                                   basis_side.basis + lv * 3 * p1);
+  }
+}
+
+// ---- FP32 screen of the intersection query ---------------------------------
+//
+// Samples, curvature terms, cell boxes and the overlap screen of a round in
+// FP32; everything the FP64 form's decisions depend on is recovered exactly
+// (see k_iscreen_samples, k_kmax_recheck, k_inter_verify).
+
+// |sum of a basis row| bound: sum_c |N_c| over the p+1 non-zero functions of
+// one grid line, in double, for the per-sample error bounds.
+__device__ __forceinline__ double abs_row_sum(const double *N, int p) {
+  double s = 0.0;
+  for (int c = 0; c <= p; ++c) s += fabs(N[c]);
+  return s;
+}
+
+// FP32 samples of one side's regions from the FP64 basis tables (rounded to
+// FP32 and contracted with FMAs against the FP32 control net, as
+// screen_point does; rational sums are divided in FP64).  With need_k the
+// curvature terms of compute_K (common.cu:155-161: max-abs component of Puu,
+// Puv, Pvv) are formed from the same FP32 homogeneous sums, each with a
+// rigorous bound d of its distance to the FP64 form's value:
+//  * every homogeneous sum h_ab = sum_r sum_c N^(a)_c N^(b)_r (w P, w)_rc is
+//    within g * S^(a)_u * S^(b)_v * max|w P| (max w for the weight channel) of
+//    the FP64 form's sum, where S = sum |N| over a basis row and
+//    g = gamma_n(u32) + gamma_n(u64), n = p + q + 6 roundings on either chain;
+//  * rational surfaces propagate those bounds through the quotient rule
+//    (S W = H, Su W = Hu - Wu S, Suu W = Huu - 2 Wu Su - Wuu S, Suv W = Huv -
+//    Wu Sv - Wv Su - Wuv S) with every product of two perturbations kept and
+//    W - eW in the denominators, times 1.01 for the FP64 rounding of both
+//    quotients.
+// khi[t] = (k + d) rounded up per term; klo[3 r + q] = max over the region of
+// (k - d) rounded down (float bits; non-negative values order as unsigned).
+// Samples whose bound cannot be formed (W - eW <= 0, non-finite sums) get an
+// infinite khi, so k_kmax_recheck re-evaluates them.
+struct IScreenConst {
+  double g;         // gamma_n(u32) + gamma_n(u64), with margin
+  double cmax[3];   // max |control point coordinate|
+  double wcmax[3];  // max |w * coordinate| (rational; = cmax otherwise)
+  double wmax;      // max weight (rational)
+};
+
+template <bool NEEDK>
+__global__ void __launch_bounds__(128) k_iscreen_samples(SurfView<float> s, SideRound<double> bs,
+                                                         SideRound<float> out, Vec4<float> *khi, unsigned *klo,
+                                                         IScreenConst cst) {
+  const Geom g = bs.g;
+  const int nuv = g.nuv;
+  const long long per = static_cast<long long>(nuv) * nuv;
+  const long long total = per * bs.nreg;
+  const int p1 = g.p1max;
+  for (long long base = blockIdx.x * static_cast<long long>(blockDim.x); base < total;
+       base += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const long long t = base + threadIdx.x;
+    const bool live = t < total;
+    int r = 0;
+    float lo3[3] = {0.0f, 0.0f, 0.0f};
+    if (live) {
+      r = static_cast<int>(t / per);
+      const int q = static_cast<int>(t - static_cast<long long>(r) * per);
+      const int idx = q % nuv, idy = q / nuv;
+      const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
+      const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
+      const double *Nu = bs.basis + lu * 3 * p1;
+      const double *Nv = bs.basis + lv * 3 * p1;
+      const int spanu = bs.spans[lu], spanv = bs.spans[lv];
+      if (!NEEDK || s.zero) {
+        out.samples[t] = screen_point(s, spanu, Nu, spanv, Nv);
+        if (NEEDK) khi[t] = Vec4<float>{0.0f, 0.0f, 0.0f, 0.0f};
+      } else {
+        // Homogeneous FP32 sums of the six derivative combinations (P, Pu, Pv,
+        // Puu, Puv, Pvv) x (x, y, z, w), u sums per control-net row shared by
+        // the combinations of one u order.
+        float h[6][4];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) h[m][0] = h[m][1] = h[m][2] = h[m][3] = 0.0f;
+        const int cu0 = spanu - s.degu, cv0 = spanv - s.degv;
+        for (int rr = 0; rr <= s.degv; ++rr) {
+          const Vec4<float> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + rr) + cu0;
+          float R[3][4];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) R[a][0] = R[a][1] = R[a][2] = R[a][3] = 0.0f;
+          for (int c = 0; c <= s.degu; ++c) {
+            const Vec4<float> v = cp[c];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              if (a > s.du) break;
+              float n = __double2float_rn(Nu[a * p1 + c]);
+              if (s.rat) {
+                n = __fmul_rn(n, v.w);
+                R[a][3] = __fadd_rn(R[a][3], n);
+              }
+              R[a][0] = __fmaf_rn(n, v.x, R[a][0]);
+              R[a][1] = __fmaf_rn(n, v.y, R[a][1]);
+              R[a][2] = __fmaf_rn(n, v.z, R[a][2]);
+            }
+          }
+          const float m0 = __double2float_rn(Nv[rr]);
+          const float m1 = s.dv >= 1 ? __double2float_rn(Nv[p1 + rr]) : 0.0f;
+          const float m2 = s.dv >= 2 ? __double2float_rn(Nv[2 * p1 + rr]) : 0.0f;
+          // combination m: (u order, v order) = (0,0) (1,0) (0,1) (2,0) (1,1) (0,2)
+#pragma unroll
+          for (int ch = 0; ch < 4; ++ch) {
+            h[0][ch] = __fmaf_rn(m0, R[0][ch], h[0][ch]);
+            h[1][ch] = __fmaf_rn(m0, R[1][ch], h[1][ch]);
+            h[2][ch] = __fmaf_rn(m1, R[0][ch], h[2][ch]);
+            h[3][ch] = __fmaf_rn(m0, R[2][ch], h[3][ch]);
+            h[4][ch] = __fmaf_rn(m1, R[1][ch], h[4][ch]);
+            h[5][ch] = __fmaf_rn(m2, R[0][ch], h[5][ch]);
+          }
+        }
+        // Derivative orders above the degree stay zero (evaluation.cu:283,315).
+        const int ku[6] = {0, 1, 0, 2, 1, 0}, kv[6] = {0, 0, 1, 0, 1, 2};
+        double Su[3], Sv[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          Su[a] = a <= s.du ? abs_row_sum(Nu + a * p1, s.degu) * (1.0 + 1e-12) : 0.0;
+          Sv[a] = a <= s.dv ? abs_row_sum(Nv + a * p1, s.degv) * (1.0 + 1e-12) : 0.0;
+        }
+        double eh[6][4];  // bounds of |h32 - h64|
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          const double mag = cst.g * Su[ku[m]] * Sv[kv[m]];
+          eh[m][0] = mag * cst.wcmax[0];
+          eh[m][1] = mag * cst.wcmax[1];
+          eh[m][2] = mag * cst.wcmax[2];
+          eh[m][3] = mag * cst.wmax;
+        }
+        double S[6][3], e[6][3];
+        bool ok = true;
+        if (!s.rat) {
+#pragma unroll
+          for (int m = 0; m < 6; ++m)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              S[m][c] = static_cast<double>(h[m][c]);
+              e[m][c] = eh[m][c];
+            }
+        } else {
+          const double W = h[0][3], Wu = h[1][3], Wv = h[2][3], Wuu = h[3][3], Wuv = h[4][3], Wvv = h[5][3];
+          const double eW = eh[0][3], eWu = eh[1][3], eWv = eh[2][3], eWuu = eh[3][3], eWuv = eh[4][3],
+                       eWvv = eh[5][3];
+          const double Wl = W - eW;
+          ok = Wl > 0.0;
+          const double inv = 1.0 / W;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double F = h[0][c] * inv;
+            const double Fu = (h[1][c] - Wu * F) * inv;
+            const double Fv = (h[2][c] - Wv * F) * inv;
+            const double Fuu = (h[3][c] - 2.0 * Wu * Fu - Wuu * F) * inv;
+            const double Fuv = (h[4][c] - Wu * Fv - Wv * Fu - Wuv * F) * inv;
+            const double Fvv = (h[5][c] - 2.0 * Wv * Fv - Wvv * F) * inv;
+            S[0][c] = F, S[1][c] = Fu, S[2][c] = Fv, S[3][c] = Fuu, S[4][c] = Fuv, S[5][c] = Fvv;
+            const double eF = (eh[0][c] + fabs(F) * eW) / Wl;
+            const double eFu = (eh[1][c] + fabs(Wu) * eF + fabs(F) * eWu + eWu * eF + fabs(Fu) * eW) / Wl;
+            const double eFv = (eh[2][c] + fabs(Wv) * eF + fabs(F) * eWv + eWv * eF + fabs(Fv) * eW) / Wl;
+            const double eFuu = (eh[3][c] + 2.0 * (fabs(Wu) * eFu + fabs(Fu) * eWu + eWu * eFu) + fabs(Wuu) * eF +
+                                 fabs(F) * eWuu + eWuu * eF + fabs(Fuu) * eW) / Wl;
+            const double eFuv = (eh[4][c] + fabs(Wu) * eFv + fabs(Fv) * eWu + eWu * eFv + fabs(Wv) * eFu +
+                                 fabs(Fu) * eWv + eWv * eFu + fabs(Wuv) * eF + fabs(F) * eWuv + eWuv * eF +
+                                 fabs(Fuv) * eW) / Wl;
+            const double eFvv = (eh[5][c] + 2.0 * (fabs(Wv) * eFv + fabs(Fv) * eWv + eWv * eFv) + fabs(Wvv) * eF +
+                                 fabs(F) * eWvv + eWvv * eF + fabs(Fvv) * eW) / Wl;
+            e[0][c] = eF, e[1][c] = eFu, e[2][c] = eFv, e[3][c] = eFuu, e[4][c] = eFuv, e[5][c] = eFvv;
+          }
+        }
+        Vec4<float> P;
+        if (s.rat) {
+          // P as screen_point forms it: the FP32 sums divided in FP64.
+          const double w = static_cast<double>(h[0][3]);
+          P = Vec4<float>{__double2float_rn(static_cast<double>(h[0][0]) / w),
+                          __double2float_rn(static_cast<double>(h[0][1]) / w),
+                          __double2float_rn(static_cast<double>(h[0][2]) / w), 0.0f};
+        } else {
+          P = Vec4<float>{h[0][0], h[0][1], h[0][2], 0.0f};
+        }
+        out.samples[t] = P;
+        float hi3[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int m = 3 + q;
+          double kv = 0.0, kd = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            kv = fmax(kv, fabs(S[m][c]));
+            kd = fmax(kd, e[m][c]);
+          }
+          kd *= 1.01;
+          const bool fin = ok && isfinite(kv) && isfinite(kd);
+          lo3[q] = fin ? fmaxf(__double2float_rd(kv - kd), 0.0f) : 0.0f;
+          hi3[q] = fin ? __double2float_ru(kv + kd) : pos_inf<float>();
+        }
+        khi[t] = Vec4<float>{hi3[0], hi3[1], hi3[2], 0.0f};
+      }
+    }
+    if (NEEDK) {
+      // Region maxima of the lower bounds: warp maximum when every live lane
+      // shares the region, else per lane.
+      const int r0 = __shfl_sync(kFull, r, 0);
+      const bool uniform = __all_sync(kFull, (!live) || r == r0);
+      if (uniform) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          for (int o = 16; o > 0; o >>= 1) lo3[q] = fmaxf(lo3[q], __shfl_xor_sync(kFull, lo3[q], o));
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+          for (int q = 0; q < 3; ++q) atomicMax(&klo[3 * r0 + q], __float_as_uint(lo3[q]));
+      } else if (live) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) atomicMax(&klo[3 * r + q], __float_as_uint(lo3[q]));
+      }
+    }
+  }
+}
+
+// Exact compute_K maxima from the FP32 bounds: every sample's FP64 term lies
+// in [lo, hi], so the FP64 maximum of a region is at least the largest lo
+// and is reached only at samples with hi >= that.  Those samples are
+// evaluated in FP64 with the FP64 form's code (eval_record), and their terms
+// folded with the same atomic maximum: the result equals the FP64 form's
+// bits.  count gets the number of samples re-evaluated.
+__global__ void k_kmax_recheck(SurfView<double> s, SideRound<double> bs, const Vec4<float> *khi,
+                               const unsigned *klo, unsigned long long *count) {
+  const Geom g = bs.g;
+  const int nuv = g.nuv;
+  const long long per = static_cast<long long>(nuv) * nuv;
+  const long long total = per * bs.nreg;
+  const int p1 = g.p1max;
+  unsigned long long mine = 0;
+  for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(t / per);
+    const Vec4<float> hb = khi[t];
+    const bool cand = hb.x >= __uint_as_float(klo[3 * r]) || hb.y >= __uint_as_float(klo[3 * r + 1]) ||
+                      hb.z >= __uint_as_float(klo[3 * r + 2]);
+    if (!cand) continue;
+    ++mine;
+    const int q = static_cast<int>(t - static_cast<long long>(r) * per);
+    const int idx = q % nuv, idy = q / nuv;
+    const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
+    const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
+    double rec[18];
+    eval_record(s, bs.spans[lu], bs.basis + lu * 3 * p1, bs.spans[lv], bs.basis + lv * 3 * p1, p1, rec);
+    // max-abs component of Puu, Puv, Pvv (common.cu:155-161), as k_samples
+    atomic_max_bits(&bs.kmax[3 * r + 0], tmax(fabs(rec[9]), tmax(fabs(rec[10]), fabs(rec[11]))));
+    atomic_max_bits(&bs.kmax[3 * r + 1], tmax(fabs(rec[12]), tmax(fabs(rec[13]), fabs(rec[14]))));
+    atomic_max_bits(&bs.kmax[3 * r + 2], tmax(fabs(rec[15]), tmax(fabs(rec[16]), fabs(rec[17]))));
+  }
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(kFull, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(count, mine);
+}
+
+// FP64 cell of the intersection query for one (region, cell id): the four
+// corner samples with the FP64 form's code (eval_point; its P equals
+// eval_record's), then centre and half span exactly as k_cells forms them.
+__device__ __forceinline__ void inter_cell64(const SurfView<double> &s, const SideRound<double> &sr, int r, int cell,
+                                             Vec4<double> &cen, Vec4<double> &hal) {
+  const int nuv = sr.g.nuv, W = sr.g.W, p1 = sr.g.p1max;
+  const int iv = cell / W, iu = cell - (cell / W) * W;
+  double P[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int idx = iu + (k & 1), idy = iv + (k >> 1);
+    const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
+    const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
+    eval_point(s, sr.spans[lu], sr.basis + lu * 3 * p1, sr.spans[lv], sr.basis + lv * 3 * p1, P[k]);
+  }
+  double lo[3], hi[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    lo[c] = tmin(P[0][c], tmin(P[1][c], tmin(P[2][c], P[3][c])));
+    hi[c] = tmax(P[0][c], tmax(P[1][c], tmax(P[2][c], P[3][c])));
+  }
+  cen = Vec4<double>{(lo[0] + hi[0]) / 2.0, (lo[1] + hi[1]) / 2.0, (lo[2] + hi[2]) / 2.0, 0.0};
+  hal = Vec4<double>{(hi[0] - lo[0]) / 2.0, (hi[1] - lo[1]) / 2.0, (hi[2] - lo[2]) / 2.0, 0.0};
+}
+
+// FP64 re-check of the FP32 screen's candidate (slot, i, j) keys: the FP64
+// form's boxes and padding, the strict test of intersection.cu:60-62 in the
+// FP64 leaf's operation order.  Kept keys are appended (unordered) to out;
+// stats->checked counts them.
+__global__ void __launch_bounds__(128) k_inter_verify(SurfView<double> sa, SurfView<double> sb,
+                                                      SideRound<double> a, SideRound<double> b, const int *map1,
+                                                      const int *map2, const unsigned long long *keys,
+                                                      unsigned long long n, int ij_bits, unsigned long long *out,
+                                                      unsigned long long cap, ScreenStats *stats) {
+  const unsigned long long mij = (1ull << ij_bits) - 1ull;
+  for (unsigned long long base = blockIdx.x * static_cast<unsigned long long>(blockDim.x); base < n;
+       base += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long q = base + threadIdx.x;
+    bool keep = false;
+    unsigned long long key = 0;
+    if (q < n) {
+      key = keys[q];
+      const int slot = static_cast<int>(key >> (2 * ij_bits));
+      const int i = static_cast<int>((key >> ij_bits) & mij), j = static_cast<int>(key & mij);
+      const int r1 = map1[slot], r2 = map2[slot];
+      Vec4<double> c1, h1, c2, h2;
+      inter_cell64(sa, a, r1, i, c1, h1);
+      inter_cell64(sb, b, r2, j, c2, h2);
+      const double p1 = a.pad[r1], p2 = b.pad[r2];
+      Vec4<double> r1v = h1, r2v = h2;
+      r1v.x = r1v.x + p1;
+      r1v.y = r1v.y + p1;
+      r1v.z = r1v.z + p1;
+      r2v.x = r2v.x + p2;
+      r2v.y = r2v.y + p2;
+      r2v.z = r2v.z + p2;
+      keep = fabs(c1.x - c2.x) < (r1v.x + r2v.x) && fabs(c1.y - c2.y) < (r1v.y + r2v.y) &&
+             fabs(c1.z - c2.z) < (r1v.z + r2v.z);
+    }
+    const long long pos = warp_append(keep, &stats->checked);
+    if (pos >= 0 && static_cast<unsigned long long>(pos) < cap) out[pos] = key;
   }
 }
 
@@ -3912,7 +4271,8 @@ void launch_inter_cull(const SideRound<T> &a, const SideRound<T> &b, const int *
                        unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats, cudaStream_t st) {
   counted();
   const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
-  k_inter_cull<T><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats);
+  k_inter_cull<T, false><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(a, b, map1, map2, nslots, surv, surv_cap, stats,
+                                                                       Vec4<float>{}, nullptr, nullptr);
 }
 
 template <typename T>
@@ -3923,7 +4283,65 @@ void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *
   if (nsurv == 0) return;
   const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
   const int blocks = static_cast<int>((warps + 7) / 8);
-  k_inter_leaf<T><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats);
+  k_inter_leaf<T, false><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats,
+                                                  Vec4<float>{}, nullptr, nullptr);
+}
+
+void launch_inter_cull_screen(const SideRound<float> &a, const SideRound<float> &b, const int *map1, const int *map2,
+                              int nslots, unsigned long long *surv, unsigned long long surv_cap, ScreenStats *stats,
+                              const float w[3], const double *pad64a, const double *pad64b, cudaStream_t st) {
+  counted();
+  const long long n = static_cast<long long>(nslots) * a.g.ntiles * b.g.ntiles;
+  k_inter_cull<float, true><<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(
+      a, b, map1, map2, nslots, surv, surv_cap, stats, Vec4<float>{w[0], w[1], w[2], 0.0f}, pad64a, pad64b);
+}
+
+void launch_inter_leaf_screen(const SideRound<float> &a, const SideRound<float> &b, const int *map1, const int *map2,
+                              const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
+                              unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats,
+                              const float w[3], const double *pad64a, const double *pad64b, cudaStream_t st) {
+  counted();
+  if (nsurv == 0) return;
+  const unsigned long long warps = nsurv < 148ull * 64 ? nsurv : 148ull * 64;
+  const int blocks = static_cast<int>((warps + 7) / 8);
+  k_inter_leaf<float, true><<<blocks, 256, 0, st>>>(a, b, map1, map2, surv, nsurv, ij_bits, keys, key_cap, stats,
+                                                    Vec4<float>{w[0], w[1], w[2], 0.0f}, pad64a, pad64b);
+}
+
+void launch_iscreen_samples(const SurfView<float> &s, const SideRound<double> &bs, const SideRound<float> &out,
+                            bool need_k, Vec4<float> *khi, unsigned *klo, double g, const double cmax[3],
+                            const double wcmax[3], double wmax, cudaStream_t st) {
+  counted();
+  IScreenConst c;
+  c.g = g;
+  for (int q = 0; q < 3; ++q) {
+    c.cmax[q] = cmax[q];
+    c.wcmax[q] = wcmax[q];
+  }
+  c.wmax = wmax;
+  const long long n = static_cast<long long>(bs.nreg) * bs.g.nuv * bs.g.nuv;
+  const int blocks = grid_for(n, 128, 148 * 32);
+  if (need_k)
+    k_iscreen_samples<true><<<blocks, 128, 0, st>>>(s, bs, out, khi, klo, c);
+  else
+    k_iscreen_samples<false><<<blocks, 128, 0, st>>>(s, bs, out, khi, klo, c);
+}
+
+void launch_kmax_recheck(const SurfView<double> &s, const SideRound<double> &bs, const Vec4<float> *khi,
+                         const unsigned *klo, unsigned long long *count, cudaStream_t st) {
+  counted();
+  const long long n = static_cast<long long>(bs.nreg) * bs.g.nuv * bs.g.nuv;
+  k_kmax_recheck<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, bs, khi, klo, count);
+}
+
+void launch_inter_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
+                         const SideRound<double> &b, const int *map1, const int *map2, const unsigned long long *keys,
+                         unsigned long long n, int ij_bits, unsigned long long *out, unsigned long long cap,
+                         ScreenStats *stats, cudaStream_t st) {
+  counted();
+  if (n == 0) return;
+  k_inter_verify<<<grid_for(static_cast<long long>(n), 128, 148 * 32), 128, 0, st>>>(
+      sa, sb, a, b, map1, map2, keys, n, ij_bits, out, cap, stats);
 }
 
 void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<double> *reg1,

@@ -16,7 +16,8 @@ own sources into oracle/_ref/libjsi_v5_ref.so (oracle/Makefile):
 * ref_distance.npz      per-round k-th distances of minimum_distance()
                         (distance_analysis.cu:356-506) obtained by running it with
                         max_layers = 1..rounds, and the round-1 top-k lists
-* ref_inter_synth.npz   per-round counts on the saddle/plane pair at small nuv0
+* ref_inter_synth.npz   per-round counts (and round-1 paddings) on the saddle/plane pair at
+                        nuv0 = 16, 32 and the full-size 256
 * ref_full.json         (--full) the full-size hard-wave distance (nuv0 = 512)
 
 Synthetic surfaces are regenerated by jsi_cad_next_versions_b200.synth; each
@@ -146,10 +147,13 @@ def main(full: bool = False):
     syn = {}
     C, D, _ = synth.intersection_pair_saddle_plane()
     rc, rd = np.array(C.rect(), np.float32), np.array(D.rect(), np.float32)
-    for nuv0 in (16, 32):
+    # nuv0 = 256 is the configuration's full size (4.2e9 first-round box tests).
+    for nuv0 in (16, 32, 256):
         for use_k in (1, 0):
             res = R.intersection(C, D, rc, rd, nuv0, 16, use_k)
             syn[f"n{nuv0}/k{use_k}/counts"] = res["counts"]
+            if res["pads"]:
+                syn[f"n{nuv0}/k{use_k}/pads"] = np.array(res["pads"], np.float32)
     np.savez_compressed(OUT / "ref_inter_synth.npz", **syn)
     (OUT / "ref_inter_synth.json").write_text(json.dumps({"saddle_plane": [digest(C), digest(D)]}, indent=1))
     print(f"synthetic intersection done {time.time() - t0:.1f}s")

@@ -37,7 +37,7 @@ def test_library_is_sm100a_build():
 def test_status_strings_and_abi():
     from jsi_cad_next_versions_b200 import _capi
     lib = _capi.load()
-    assert lib.jsi_abi_version() == 2
+    assert lib.jsi_abi_version() == 3
     assert lib.jsi_status_string(0) == b"ok"
     assert lib.jsi_status_string(-4) == b"capacity exceeded"
 
