@@ -2649,9 +2649,15 @@ void validate_inter(jsi_inter_params &p, const jsi_task *a, const jsi_task *b) {
 void exec_distance(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_dist_params &p, jsi_dist_result *out) {
   int *tp = out->trace_pairs;
   const long long tc = out->trace_cap;
+  int *cp = out->cand_pairs;
+  double *cd = out->cand_d2;
+  const long long cc = out->cand_cap;
   std::memset(out, 0, sizeof(*out));
   out->trace_pairs = tp;
   out->trace_cap = tc;
+  out->cand_pairs = cp;
+  out->cand_d2 = cd;
+  out->cand_cap = cc;
   out->newton_distance = -1.0;
   JSI_CUDA(cudaSetDevice(L->device));
   L->arena.reset();
