@@ -1975,14 +1975,14 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
     const int r1 = map1[slot], r2 = map2[slot];
     const long long base1 = (static_cast<long long>(r1) * g1.ntiles + t1) * n1;
     const long long base2 = (static_cast<long long>(r2) * g2.ntiles + t2) * n2;
-    // Per-cell radius terms: side 1 adds p1 (FP64 form) or nothing (screen);
-    // side 2 adds p2 (FP64 form) or the pair's widening Q (screen).
-    T p1, p2;
+    // Per-cell radius terms: FP64 form, p1 on side 1 and p2 on side 2; FP32
+    // screen, the pair's widening Q per axis (from the kernel argument wq,
+    // which stays unchanged across tile pairs).
+    T p1 = T(0), p2 = T(0);
+    Vec4<float> Q{0.0f, 0.0f, 0.0f, 0.0f};
     if constexpr (S) {
       const double q1 = pad64a[r1], q2 = pad64b[r2];
-      p1 = T(0);
-      p2 = T(0);
-      wq = Vec4<float>{iscreen_q(q1, q2, wq.x), iscreen_q(q1, q2, wq.y), iscreen_q(q1, q2, wq.z), 0.0f};
+      Q = Vec4<float>{iscreen_q(q1, q2, wq.x), iscreen_q(q1, q2, wq.y), iscreen_q(q1, q2, wq.z), 0.0f};
     } else {
       p1 = a.pad[r1];
       p2 = b.pad[r2];
@@ -2022,10 +2022,10 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
         Vec4<T> r1 = a.half[base1 + a1 * te1 + b1];
         bool ha, hb;
         if constexpr (S) {
-          ha = fabs(c1.x - c2a.x) < (r1.x + r2a.x) + wq.x && fabs(c1.y - c2a.y) < (r1.y + r2a.y) + wq.y &&
-               fabs(c1.z - c2a.z) < (r1.z + r2a.z) + wq.z;
-          hb = fabs(c1.x - c2b.x) < (r1.x + r2b.x) + wq.x && fabs(c1.y - c2b.y) < (r1.y + r2b.y) + wq.y &&
-               fabs(c1.z - c2b.z) < (r1.z + r2b.z) + wq.z;
+          ha = fabs(c1.x - c2a.x) < (r1.x + r2a.x) + Q.x && fabs(c1.y - c2a.y) < (r1.y + r2a.y) + Q.y &&
+               fabs(c1.z - c2a.z) < (r1.z + r2a.z) + Q.z;
+          hb = fabs(c1.x - c2b.x) < (r1.x + r2b.x) + Q.x && fabs(c1.y - c2b.y) < (r1.y + r2b.y) + Q.y &&
+               fabs(c1.z - c2b.z) < (r1.z + r2b.z) + Q.z;
         } else {
           r1.x = r1.x + p1;
           r1.y = r1.y + p1;

@@ -69,6 +69,11 @@ def test_saddle_plane_full_size_screen_superset_and_exact(gpu_ctx, use_k):
     assert [_digest(p) for p in f64.pairs] == dig[f"f64/k{use_k}"]["sha256"]
     # the FP32 screen's first-round candidates hold every FP64 pair ...
     assert scr.screen_written >= f64.counts[0]
+    # ... are the same on every run (the widening is a fixed bound per region
+    # pair) and only slightly more
+    again = _inter(gpu_ctx, C, D, 256, use_k, precision="fp32_screen")
+    assert again.screen_written == scr.screen_written
+    assert scr.screen_written <= 1.02 * f64.counts[0] + 256
     assert scr.screen_pairs.shape[0] == scr.screen_written
     assert _contains(scr.screen_pairs, f64.pairs[0])
     # ... and after the FP64 re-check every round equals the FP64 form's
