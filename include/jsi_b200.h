@@ -333,10 +333,13 @@ int jsi_queue_depth(jsi_context *ctx, int *queued, int *running);
 /* n distance queries over the worker lanes; status[q] (may be null) gets each
  * query's status, device_ms (may be null) the device span of the batch
  * (CUDA events).  Returns the first error, else JSI_OK.
- * With k <= 8 and rounds <= 8, queries of one shape (first-round nuv,
- * degrees and rational flag of both sides) run in lockstep batches of up to jsi_batch_chunk
+ * With k <= 8 and rounds <= 8, queries with the same first-round nuv and
+ * zero flags of both sides run in lockstep batches of up to jsi_batch_chunk
  * queries per lane: one launch per stage for the whole batch, counts kept on
- * the device, one copy in and one copy out per batch.  Results are the same
+ * the device, one copy in and one copy out per batch.  Degrees and rational
+ * flags may differ within a batch (each query's surfaces are read from its
+ * slab; such a mixed batch builds its cells with the kernel that takes any
+ * degree).  Results are the same
  * as the per-query path's; a query whose internal lists overflow is re-run
  * alone.  No reference counterpart (V5 runs one query per call,
  * distance_analysis.cu:356). */
@@ -369,6 +372,21 @@ int jsi_autotune_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_tas
  * Off by default: with three worker lanes and uploads running beside them a
  * replay crashed inside cudaGraphLaunch on driver 580. */
 int jsi_batch_graphs(jsi_context *ctx, int enable, long long *replays);
+
+/* --- mixed query batches ---------------------------------------------------
+ * No counterpart in the reference, which runs one query per call.  n queries
+ * of both kinds and any shapes over the worker lanes: kinds[q] = 0 distance
+ * (result in dist_out[q], parameters dp), 1 intersection (inter_out[q],
+ * parameters ip; its caller-owned trace, points and screen buffers are
+ * honoured as by jsi_intersect).  Distance queries run as lockstep batches
+ * grouped by first-round nuv (as jsi_min_distance_batch); intersection
+ * queries run as lane jobs, the largest first-round grids first.  Every
+ * result equals the same query run alone.  status[q] (may be null) gets each
+ * query's status, device_ms (may be null) the device span from the call to
+ * the end of the last job.  Returns the first error, else JSI_OK. */
+int jsi_query_batch(jsi_context *ctx, int n, const int *kinds, const jsi_task *a, const jsi_task *b,
+                    const jsi_dist_params *dp, const jsi_inter_params *ip, jsi_dist_result *dist_out,
+                    jsi_inter_result *inter_out, int *status, float *device_ms);
 
 /* --- grid evaluation -----------------------------------------------------
  * Replaces evalWithCuda(int*, float*, int, float, float, float, float, int,

@@ -538,6 +538,58 @@ class Context:
         self._check(self.lib.jsi_wait_distance_batch(self.handle, handle["ticket"], ctypes.byref(ms)))
         return DistanceBatch(handle["res"], handle["bufs"], handle["k"]), ms.value
 
+    def query_batch(self, queries, *, precision: str | int = "v5_fp32", k: int = 8, rounds: int = 4,
+                    nuv_refine: int = 16, newton: bool = False, use_k: bool = True, inter_rounds: int = 6,
+                    halve_threshold: int = 512, min_nuv: int = 4, points: bool = False, points_cap: int = 1 << 20,
+                    trace: bool = False, trace_cap: int = 1 << 20):
+        """Mixed queries [(kind, task_a, task_b), ...] (kind "distance" or
+        "intersection") in one call over the worker lanes: distance queries in
+        lockstep batches grouped by first-round nuv, intersection queries as
+        lane jobs, largest first.  Returns (results, statuses, device_ms):
+        results[q] is a DistanceResult or an IntersectionResult."""
+        n = len(queries)
+        kinds = (ctypes.c_int * n)(*[0 if q[0] in ("distance", 0) else 1 for q in queries])
+        ta = (C.Task * n)(*[q[1] for q in queries])
+        tb = (C.Task * n)(*[q[2] for q in queries])
+        dp = self._dist_params(k, rounds, nuv_refine, precision, newton)
+        prec = C.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        ip = C.InterParams(nuv_refine, 1 if use_k else 0, inter_rounds, halve_threshold, min_nuv, prec,
+                           1 if points else 0)
+        dres = (C.DistResult * n)()
+        ires = (C.InterResult * n)()
+        pbufs, tbufs = {}, {}
+        for q in range(n):
+            if kinds[q] == 1:
+                if points:
+                    pbufs[q] = np.zeros(points_cap * 8, dtype=np.float64)
+                    ires[q].points = pbufs[q].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+                    ires[q].points_cap = points_cap
+                if trace:
+                    tbufs[q] = np.full(trace_cap * 3, -1, dtype=np.int32)
+                    ires[q].trace_pairs = tbufs[q].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+                    ires[q].trace_cap = trace_cap
+        status = (ctypes.c_int * n)()
+        ms = ctypes.c_float(0)
+        st = self.lib.jsi_query_batch(self.handle, n, kinds, ta, tb, ctypes.byref(dp), ctypes.byref(ip), dres, ires,
+                                      status, ctypes.byref(ms))
+        out = []
+        for q in range(n):
+            if status[q] != 0:
+                out.append(None)
+            elif kinds[q] == 0:
+                out.append(self._dist_result(dres[q], None, k))
+            else:
+                r = self._inter_result(ires[q], tbufs.get(q), trace_cap)
+                if points:
+                    r.points = pbufs[q][:ires[q].points_written * 8].reshape(-1, 8).copy()
+                    r.points_converged = int(ires[q].points_converged)
+                r.screen_written = int(ires[q].screen_written)
+                r.kmax_rechecked = int(ires[q].kmax_rechecked)
+                out.append(r)
+        if st != 0 and all(s == 0 for s in status):
+            self._check(st)
+        return out, list(status), ms.value
+
     def intersection_curves(self, a: C.Task, b: C.Task, *, nuv_refine: int = 16, use_k: bool = True, rounds: int = 6,
                             halve_threshold: int = 512, min_nuv: int = 4, link_tol: float = 0.0,
                             vertex_cap: int = 1 << 18, curve_cap: int = 1 << 12) -> IntersectionCurves:

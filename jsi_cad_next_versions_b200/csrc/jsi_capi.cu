@@ -1553,7 +1553,31 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
   cudaStream_t st = L->stream;
   const SurfaceRec &s0a = get_surface(L, items[0].a->surface);
   const SurfaceRec &s0b = get_surface(L, items[0].b->surface);
-  const int nuv1 = items[0].a->nuv, nuv2 = items[0].b->nuv, p1a = p1_of(s0a), p1b = p1_of(s0b);
+  const int nuv1 = items[0].a->nuv, nuv2 = items[0].b->nuv;
+  // A batch shares the first-round nuv of each side and the zero flags;
+  // degrees and rational flags may differ (a mixed batch): the slabs are laid
+  // out for the largest degrees, the kernels read each query's surface from
+  // its head, and the cell build takes the kernel that handles any degree.
+  int dua = 0, dva = 0, dub = 0, dvb = 0;
+  bool mixed = false;
+  for (int q = 0; q < n; ++q) {
+    const SurfaceRec &sa = get_surface(L, items[q].a->surface);
+    const SurfaceRec &sb = get_surface(L, items[q].b->surface);
+    if (sa.zero != s0a.zero || sb.zero != s0b.zero || items[q].a->nuv != nuv1 || items[q].b->nuv != nuv2)
+      fail(JSI_ERR_INVALID, "batch items differ in first-round nuv or zero flag");
+    mixed = mixed || shape_of(sa) != shape_of(s0a) || shape_of(sb) != shape_of(s0b);
+    dua = std::max(dua, sa.ivec[1]);
+    dva = std::max(dva, sa.ivec[4]);
+    dub = std::max(dub, sb.ivec[1]);
+    dvb = std::max(dvb, sb.ivec[4]);
+  }
+  const int p1a = std::max(dua, dva) + 1, p1b = std::max(dub, dvb) + 1;
+  // Host views: only the kernel variant choice reads them (largest degrees).
+  auto host_view = [&](auto v, int du, int dv) {
+    v.degu = du;
+    v.degv = dv;
+    return v;
+  };
   const BatchCaps caps = batch_caps();
   const BatchLayout<TP, TC> probe = plan_batch<TP, TC>(nullptr, nuv1, nuv2, p1a, p1b, p, caps);
   const size_t slab = (probe.bytes + 255) & ~static_cast<size_t>(255);
@@ -1568,9 +1592,6 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
   for (int q = 0; q < n; ++q) {
     const SurfaceRec &sa = get_surface(L, items[q].a->surface);
     const SurfaceRec &sb = get_surface(L, items[q].b->surface);
-    if (shape_of(sa) != shape_of(s0a) || shape_of(sb) != shape_of(s0b) || items[q].a->nuv != nuv1 ||
-        items[q].b->nuv != nuv2)
-      fail(JSI_ERR_INVALID, "batch items differ in shape");
     DistHead<TP> h{};
     h.a64 = view<double>(sa);
     h.b64 = view<double>(sb);
@@ -1594,7 +1615,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
     e = std::ldexp(1.0f, ex);
   }
   ScreenStats *stats = &lay.head->stats;
-  const SurfView<TP> va = view<TP>(s0a), vb = view<TP>(s0b);
+  const SurfView<TP> va = host_view(view<TP>(s0a), dua, dva), vb = host_view(view<TP>(s0b), dub, dvb);
+  const SurfView<float> va32 = host_view(view<float>(s0a), dua, dva), vb32 = host_view(view<float>(s0b), dub, dvb);
   const int R = p.rounds;
   auto enqueue = [&]() {
     JSI_CUDA(cudaMemcpy2DAsync(lay.head, slab, pin, hsz, hsz, n, cudaMemcpyHostToDevice, st));
@@ -1616,8 +1638,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
         batch_fold_init(Rd.A, st, bt);
         batch_fold_init(Rd.B, st, bt);
         timed(L, cells_name, [&] {
-          launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0));
-          launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1));
+          launch_cells_fused(va, Rd.A, Rd.A, st, bt, head_view<TP>(lay.head, 0), mixed);
+          launch_cells_fused(vb, Rd.B, Rd.B, st, bt, head_view<TP>(lay.head, 1), mixed);
         }, cells_units);
         batch_screen<TP>(L, Rd, Rd.A, Rd.B, stats, p.k, false, 0.0f, bt);
         timed(L, "dist_select", [&] {
@@ -1627,8 +1649,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
         batch_fold_init(Rd.A32, st, bt);
         batch_fold_init(Rd.B32, st, bt);
         timed(L, cells_name, [&] {
-          launch_cells_fused(view<float>(s0a), Rd.A, Rd.A32, st, bt, &lay.head->a32);
-          launch_cells_fused(view<float>(s0b), Rd.B, Rd.B32, st, bt, &lay.head->b32);
+          launch_cells_fused(va32, Rd.A, Rd.A32, st, bt, &lay.head->a32, mixed);
+          launch_cells_fused(vb32, Rd.B, Rd.B32, st, bt, &lay.head->b32, mixed);
         }, cells_units);
         batch_screen<TC>(L, Rd, Rd.A32, Rd.B32, stats, p.k, true, e, bt);
         timed(L, "dist_verify", [&] {
@@ -1670,7 +1692,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       static_cast<long long>(sizeof(TP)), static_cast<long long>(sizeof(TC)), nuv1, nuv2, p1a, p1b, p.k, p.rounds,
       p.nuv_refine, p.newton, n, static_cast<long long>(slab), reinterpret_cast<long long>(base),
       reinterpret_cast<long long>(pin), static_cast<long long>(caps.surv), static_cast<long long>(caps.cand),
-      static_cast<long long>(bit_cast_u32(e))};
+      static_cast<long long>(bit_cast_u32(e)), shape_of(s0a), shape_of(s0b), dua | (dva << 8) | (dub << 16) | (dvb << 24),
+      mixed ? 1 : 0};
   const bool graphs = !L->timing && L->graphs_on;
   auto it = graphs ? L->graphs.find(key) : L->graphs.end();
   if (it != L->graphs.end() && it->second.exec) {
@@ -3462,8 +3485,11 @@ int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const 
     return it != ctx->jobs.end() ? it->second : std::shared_ptr<Job>();
   };
   if (lockstep) {
-    // Group by shape: first-round nuv, degrees, rational and zero flags of both sides.
+    // Group by first-round nuv and zero flags of both sides; degrees and
+    // rational flags may differ within a group (a mixed lockstep batch).
+    // shapes[q] keeps each query's shape key for the autotuner's table.
     std::map<std::array<int, 4>, std::vector<int>> groups;
+    std::vector<std::array<int, 2>> shapes(static_cast<size_t>(n));
     for (int q = 0; q < n; ++q) {
       std::string err;
       std::array<int, 4> key{};
@@ -3472,7 +3498,8 @@ int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const 
         std::lock_guard<std::mutex> lk(ctx->mu);
         auto ia = ctx->surfaces.find(a[q].surface), ib = ctx->surfaces.find(b[q].surface);
         if (ia == ctx->surfaces.end() || ib == ctx->surfaces.end()) fail(JSI_ERR_INVALID, "unknown surface id");
-        key = {a[q].nuv, b[q].nuv, shape_of(ia->second), shape_of(ib->second)};
+        key = {a[q].nuv, b[q].nuv, ia->second.zero, ib->second.zero};
+        shapes[q] = {shape_of(ia->second), shape_of(ib->second)};
       });
       if (st != JSI_OK) {
         set_status(q, st);
@@ -3485,7 +3512,8 @@ int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const 
     const int nl = static_cast<int>(ctx->lanes.size());
     for (auto &g : groups) {
       const int m = static_cast<int>(g.second.size());
-      const std::array<int, 7> tk = {g.first[0], g.first[1], g.first[2], g.first[3], p.k, p.rounds, p.precision};
+      const int q0 = g.second[0];
+      const std::array<int, 7> tk = {g.first[0], g.first[1], shapes[q0][0], shapes[q0][1], p.k, p.rounds, p.precision};
       auto tit = ctx->tuned_chunk.find(tk);
       const int chunk = tit != ctx->tuned_chunk.end() ? tit->second : ctx->batch_chunk;
       const int per = std::max(1, std::min(chunk, (m + nl - 1) / nl));
@@ -3587,6 +3615,115 @@ int jsi_wait_distance_batch(jsi_context *ctx, jsi_ticket ticket, float *device_m
     return JSI_OK;
   });
   return B.first_err != JSI_OK ? B.first_err : st;
+}
+
+int jsi_query_batch(jsi_context *ctx, int n, const int *kinds, const jsi_task *a, const jsi_task *b,
+                    const jsi_dist_params *dp, const jsi_inter_params *ip, jsi_dist_result *dist_out,
+                    jsi_inter_result *inter_out, int *status, float *device_ms) {
+  if (!ctx || n < 0 || (n > 0 && (!kinds || !a || !b))) return JSI_ERR_INVALID;
+  if (ctx->lanes.empty()) return record(ctx, JSI_ERR_INVALID, "no worker lanes (call jsi_workers first)");
+  std::vector<int> di, ii;
+  for (int q = 0; q < n; ++q) {
+    if (kinds[q] == 0) di.push_back(q);
+    else if (kinds[q] == 1) ii.push_back(q);
+    else return record(ctx, JSI_ERR_INVALID, "query kind must be 0 (distance) or 1 (intersection)");
+  }
+  if ((!di.empty() && !dist_out) || (!ii.empty() && !inter_out)) return JSI_ERR_INVALID;
+  int first_err = JSI_OK;
+  auto set_status = [&](int q, int st) {
+    if (status) status[q] = st;
+    if (st != JSI_OK && first_err == JSI_OK) first_err = st;
+  };
+  cudaEvent_t ev0 = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const int st = guarded(ctx, [&]() {
+      JSI_CUDA(cudaSetDevice(ctx->device));
+      JSI_CUDA(cudaEventCreate(&ev0));
+      JSI_CUDA(cudaEventRecord(ev0, ctx->main.stream));
+      return JSI_OK;
+    });
+    if (st != JSI_OK) return st;
+  }
+  // Intersections first, the largest first-round grids first, so that the
+  // long jobs start early and the distance batches fill the lanes last.
+  std::sort(ii.begin(), ii.end(), [&](int x, int y) {
+    const long long wx = 1ll * a[x].nuv * a[x].nuv + 1ll * b[x].nuv * b[x].nuv;
+    const long long wy = 1ll * a[y].nuv * a[y].nuv + 1ll * b[y].nuv * b[y].nuv;
+    return wx != wy ? wx > wy : x < y;
+  });
+  jsi_inter_params ipv;
+  jsi_inter_params_default(&ipv);
+  if (ip) ipv = *ip;
+  std::vector<std::pair<int, jsi_ticket>> itick;
+  std::vector<std::shared_ptr<Job>> ijobs;
+  for (int q : ii) {
+    jsi_ticket t = 0;
+    std::shared_ptr<Job> job;
+    const int st = guarded(ctx, [&]() {
+      validate_inter(ipv, &a[q], &b[q]);
+      job = std::make_shared<Job>();
+      job->kind = 1;
+      job->a = a[q];
+      job->b = b[q];
+      job->ip = ipv;
+      const jsi_inter_result &tpl = inter_out[q];
+      job->ires.trace_pairs = tpl.trace_pairs;
+      job->ires.trace_cap = tpl.trace_cap;
+      job->ires.points = tpl.points;
+      job->ires.points_cap = tpl.points_cap;
+      job->ires.screen_pairs = tpl.screen_pairs;
+      job->ires.screen_cap = tpl.screen_cap;
+      t = enqueue(ctx, job);
+      return JSI_OK;
+    });
+    if (st != JSI_OK) {
+      set_status(q, st);
+      continue;
+    }
+    itick.push_back({q, t});
+    ijobs.push_back(job);
+  }
+  // Distance queries: the lockstep batches of jsi_submit_distance_batch over
+  // compacted copies of their tasks and results.
+  const int nd = static_cast<int>(di.size());
+  std::vector<jsi_task> da(nd), db(nd);
+  std::vector<jsi_dist_result> dres(nd);
+  std::vector<int> dst(nd, JSI_OK);
+  for (int e = 0; e < nd; ++e) {
+    da[e] = a[di[e]];
+    db[e] = b[di[e]];
+    dres[e] = dist_out[di[e]];
+  }
+  jsi_ticket dt = 0;
+  int dsub = JSI_OK;
+  if (nd > 0) dsub = jsi_submit_distance_batch(ctx, nd, da.data(), db.data(), dp, dres.data(), dst.data(), &dt);
+  for (auto &qt : itick) set_status(qt.first, jsi_wait(ctx, qt.second, -1, nullptr, &inter_out[qt.first]));
+  float dms = 0.0f;
+  if (nd > 0) {
+    int dw = dsub;
+    if (dsub == JSI_OK) dw = jsi_wait_distance_batch(ctx, dt, &dms);
+    for (int e = 0; e < nd; ++e) {
+      dist_out[di[e]] = dres[e];
+      set_status(di[e], dsub != JSI_OK ? dsub : dst[e]);
+    }
+    if (dw != JSI_OK && first_err == JSI_OK) first_err = dw;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int st = guarded(ctx, [&]() {
+    float span = dms;  // the distance batch's span starts after ev0
+    for (auto &j : ijobs) {
+      if (!j->end_ev) continue;
+      JSI_CUDA(cudaEventSynchronize(j->end_ev));
+      float ms = 0.0f;
+      JSI_CUDA(cudaEventElapsedTime(&ms, ev0, j->end_ev));
+      span = std::max(span, ms);
+    }
+    if (device_ms) *device_ms = span;
+    return JSI_OK;
+  });
+  cudaEventDestroy(ev0);
+  return first_err != JSI_OK ? first_err : st;
 }
 
 int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,

@@ -270,9 +270,12 @@ void launch_surface_prep(const SurfacePrep *jobs, int n, long long most, cudaStr
 // Distance cells straight from the basis tables (no sample grid in HBM):
 // centres and tile ranges of out, bit-identical to launch_samples(_screen) +
 // launch_cells.  TB = basis precision, TC = cell precision.
+// mixed: the queries of the batch differ in degree or rational flag (s then
+// only carries the largest degrees): the kernel that reads every query's
+// degree and flag from vdev is used.
 template <typename TB, typename TC>
 void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
-                        const Batch &bt = Batch{}, const SurfView<TC> *vdev = nullptr);
+                        const Batch &bt = Batch{}, const SurfView<TC> *vdev = nullptr, bool mixed = false);
 // stats set: the candidate count is read on the device (capped at cap).
 void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
                         const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,

@@ -4441,10 +4441,10 @@ void launch_bandw(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRoun
 
 template <typename TB, typename TC>
 void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const SideRound<TC> &out, cudaStream_t st,
-                        const Batch &bt, const SurfView<TC> *vdev) {
+                        const Batch &bt, const SurfView<TC> *vdev, bool mixed) {
   counted();
   const Geom &g = out.g;
-  if (g.tw >= 16 && g.te == kMaxTile && !s.zero && s.degu == s.degv && (s.degu == 3 || s.degu == 2)) {
+  if (!mixed && g.tw >= 16 && g.te == kMaxTile && !s.zero && s.degu == s.degv && (s.degu == 3 || s.degu == 2)) {
     // Large grids with equal degrees 2 or 3 (degrees, the rational flag and
     // the zero flag are part of a batch's shape): warp-independent bands.
     if (s.degu == 3) {
@@ -4456,7 +4456,7 @@ void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const Si
     }
     return;
   }
-  if (g.tw >= 16 && g.te == kMaxTile && s.degu <= 3 && s.degv <= 3) {
+  if (!mixed && g.tw >= 16 && g.te == kMaxTile && s.degu <= 3 && s.degv <= 3) {
     // Large grids of bicubic-or-lower surfaces (degrees are part of a batch's
     // shape): whole bands per block.
     constexpr size_t smem = band_smem<TC>();
@@ -4481,13 +4481,13 @@ void launch_cells_fused(const SurfView<TC> &s, const SideRound<TB> &bs, const Si
 
 template void launch_cells_fused<float, float>(const SurfView<float> &, const SideRound<float> &,
                                                const SideRound<float> &, cudaStream_t, const Batch &,
-                                               const SurfView<float> *);
+                                               const SurfView<float> *, bool);
 template void launch_cells_fused<double, double>(const SurfView<double> &, const SideRound<double> &,
                                                  const SideRound<double> &, cudaStream_t, const Batch &,
-                                                 const SurfView<double> *);
+                                                 const SurfView<double> *, bool);
 template void launch_cells_fused<double, float>(const SurfView<float> &, const SideRound<double> &,
                                                 const SideRound<float> &, cudaStream_t, const Batch &,
-                                                const SurfView<float> *);
+                                                const SurfView<float> *, bool);
 
 void launch_dist_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
                         const SideRound<double> &b, const int *map1, const int *map2, const DistCand<float> *cand,
