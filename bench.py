@@ -111,6 +111,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, choices=[2, 3, 4], default=2,
+                    help="2: hard-wave distance batch (default); 3: rational saddle / plane intersection at "
+                         "nuv0 = 256; 4: the 4096-pair mixed batch (half distance, half intersection)")
+    ap.add_argument("--queries", type=int, default=4096, help="config 4: pairs in the mixed batch")
     ap.add_argument("--batch", type=int, default=512, help="queries per step")
     ap.add_argument("--nuv0", type=int, default=NUV0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -476,9 +480,398 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Config 3: rational saddle / plane intersection (32 x 32 rational bicubic
+# NURBS, nuv0 = 256, curvature padding on and off, points refined in FP64).
+# Config 4: the mixed batch (4096 seeded pairs: degrees 2-5, nets 4-64, 30%
+# rational, half distance, half intersection, nuv0 64-512) in one call.
+# ---------------------------------------------------------------------------
+
+NOMINAL_FP64_NOTE = "nominal CUDA-core FP64 peak (148 SMs x 64 FP64 lanes x 2 x 1.965 GHz)"
+
+
+def _peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def sample_roofline(ctx, kt, form):
+    """Roofline of the intersection's sample kernel: the algorithmic flops the
+    library counted for the timed launches (full records: every derivative
+    combination within the degrees, FMA = 2) over their event time, against
+    the CUDA-core peak of the form's arithmetic; HBM: 16 / 32 B per sample
+    written (FP32 / FP64 samples)."""
+    ms, launches, units = kt["samples"]
+    flops = ctx.kernel_units("samples:flops")
+    s = ms / 1e3
+    fp64 = form != "v5_fp32" and form != "fp32_screen"
+    peak_f = NOMINAL_FP64_TFLOPS if fp64 else NOMINAL_FP32_TFLOPS
+    peaks = _peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    gbs = units * (32 if fp64 else 16) / s / 1e9 if s > 0 else 0.0
+    tf = flops / s / 1e12 if s > 0 else 0.0
+    return {"bound": "hbm", "kernel": "samples", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+            "frac": gbs / hbm_peak, "traffic": None,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+            "avg_launch_ms": ms / max(launches, 1), "units_per_launch": units / max(launches, 1),
+            "launch": "one sample-kernel launch (one side of one round of one query)",
+            "compute": {"achieved": tf, "peak": peak_f, "unit": "TFLOP/s", "frac": tf / peak_f,
+                        "peak_source": NOMINAL_FP64_NOTE if fp64 else
+                        "nominal CUDA-core FP32 peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)"}}
+
+
+def dominant_roofline(ctx, kt, form, n_queries):
+    dom = max(kt.items(), key=lambda kv: kv[1][0])[0] if kt else None
+    roof = sample_roofline(ctx, kt, form) if "samples" in kt else None
+    return dom, roof
+
+
+def _timed_steps(args, flush, stream, barrier, step):
+    import torch
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+CFG3_WORKLOAD = ("rational saddle / plane intersection: two 32x32 rational bicubic NURBS (w ~ U[0.5, 2]), "
+                 "nuv0=256, 6 rounds from nuv 16 (halved above 512 pairs, min 4), curvature padding on, "
+                 "FP64 Newton points from every final pair")
+
+
+def run_cfg3(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    import jsi_cad_next_versions_b200 as J
+    from jsi_cad_next_versions_b200 import synth
+    ctx = J.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    C, D, _ = synth.intersection_pair_saddle_plane()
+    rc, rd = np.array(C.rect(), np.float32), np.array(D.rect(), np.float32)
+    sc, sd = ctx.upload(C), ctx.upload(D)
+    ta, tb = ctx.task(sc, rc, 256, 1), ctx.task(sd, rd, 256, 2)
+    forms = [f for f in args.forms.split(",") if f]
+    results = {}
+    pts_ref = {}
+    for use_k in (True, False):
+        for form in forms:
+            last = []
+
+            def step():
+                last[:] = [ctx.intersect(ta, tb, use_k=use_k, precision=form, points=True, points_cap=1 << 20)]
+            clk = ClockSampler(local)
+            clk.__enter__()
+            launches0 = ctx.launch_count()
+            times = _timed_steps(args, flush, stream, lambda: torch.cuda.synchronize(), step)
+            launches = (ctx.launch_count() - launches0) / (args.steps + args.warmup)
+            ctx.kernel_timing(True)
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                step()
+            kt = ctx.kernel_times()
+            dom, roof = dominant_roofline(ctx, kt, form, 1)
+            ctx.kernel_timing(False)
+            clk.__exit__(None, None, None)
+            r = last[0]
+            key = f"{form}/k{int(use_k)}"
+            pts_ref[key] = r.points
+            results[key] = {"queries_per_s": 1e3 * args.steps / sum(times), "ms_per_query": sum(times) / args.steps,
+                            "p50_ms": percentile(times, 0.5), "p99_ms": percentile(times, 0.99),
+                            "counts": r.counts.tolist(), "points": int(r.points.shape[0]),
+                            "points_converged": int(r.points_converged), "screen_candidates": r.screen_written,
+                            "kmax_rechecked": r.kmax_rechecked, "gpu_launches": launches, "clocks": clk.summary(),
+                            "dominant_kernel": dom, "roofline": roof,
+                            "kernel_ms": {k: round(v[0] / args.steps, 4)
+                                          for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}}
+    # point error of each form against the FP64 form (same pairs: the same points)
+    for key, pts in pts_ref.items():
+        ref = pts_ref.get("fp64/" + key.split("/")[1])
+        if ref is not None and pts.shape == ref.shape and pts.size:
+            d = np.abs(pts[:, :3] - ref[:, :3]).max() / max(1.0, float(np.abs(ref[:, :3]).max()))
+            results[key]["max_rel_point_err_vs_fp64"] = float(d)
+        elif ref is not None:
+            results[key]["max_rel_point_err_vs_fp64"] = None
+            results[key]["points_differ_from_fp64"] = [int(pts.shape[0]), int(ref.shape[0])]
+    # end to end through the C ABI: both host surfaces uploaded, the query,
+    # the points read back, both released
+    form = forms[0]
+    ctx.release(sc)
+    ctx.release(sd)
+
+    def e2e_step():
+        a, b = ctx.upload_many([C, D])
+        ctx.intersect(ctx.task(a, rc, 256, 1), ctx.task(b, rd, 256, 2), use_k=True, precision=form, points=True,
+                      points_cap=1 << 20)
+        ctx.release_many([a, b])
+    h0, d0 = ctx.transfer_bytes()
+    e2e_t = _timed_steps(args, flush, stream, lambda: torch.cuda.synchronize(), e2e_step)
+    h1, d1 = ctx.transfer_bytes()
+    nrun = args.steps + args.warmup
+    e2e = {"value": 1e3 * args.steps / sum(e2e_t), "unit": "queries/s", "h2d_bytes_per_step": (h1 - h0) // nrun,
+           "d2h_bytes_per_step": (d1 - d0) // nrun, "form": form}
+    head = results[f"{form}/k1"]
+    cpu = None if args.no_cpu_baseline else cpu_baseline_cfg3()
+    line = {
+        "metric": METRIC, "value": head["queries_per_s"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_query"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"fp64": "f64", "v5_fp32": "f32", "fp32_screen": "f32+f64"}[form],
+        "data": "synthetic",
+        "config": {"workload": CFG3_WORKLOAD, "form": form, "queries_per_step": 1, "nuv0": 256,
+                   "l2": "flushed (256 MiB write) between steps", "parallelism": f"dp{world}"},
+        "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"]},
+        "forms": results,
+        "speedup_vs_fp64": head["queries_per_s"] / results["fp64/k1"]["queries_per_s"] if "fp64/k1" in results else None,
+        "e2e": e2e, "roofline": head["roofline"], "cpu_baseline": cpu, "clocks": head["clocks"],
+        "gpu_launches": head["gpu_launches"],
+    }
+    print(json.dumps(line))
+    ctx.close()
+
+
+def cpu_baseline_cfg3():
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    import oracle
+    from jsi_cad_next_versions_b200 import synth
+    if not oracle.Reference.available():
+        return None
+    R = oracle.Reference()
+    C, D, _ = synth.intersection_pair_saddle_plane()
+    rc, rd = np.array(C.rect(), np.float32), np.array(D.rect(), np.float32)
+    t0 = time.perf_counter()
+    res = R.intersection(C, D, rc, rd, 256, 16, 1)
+    el = time.perf_counter() - t0
+    return {"value": 1.0 / el, "unit": "queries/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
+            "sample": f"1 full query through the reference's intersection (nuv0=256, padding on), {el:.2f} s, "
+                      f"counts {res['counts'].tolist()}"}
+
+
+def run_reference_cfg3(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cpu = cpu_baseline_cfg3() if True else None
+    if cpu is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libjsi_v5_ref.so was not built"}))
+        return
+    times = [1.0 / cpu["value"]]
+    for _ in range(max(0, args.steps - 1)):
+        times.append(1.0 / cpu_baseline_cfg3()["value"])
+    value = len(times) / sum(times)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": len(times), "warmup": 0, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": CFG3_WORKLOAD, "queries_per_step": 1, "nuv0": 256, "cores": cpu["cores"]},
+        "cpu_baseline": {**cpu, "value": value}, "e2e": {"value": value, "unit": "queries/s",
+                                                          "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+CFG4_WORKLOAD = ("mixed batch: {n} seeded pairs, degrees 2-5 per direction, nets 4-64 (log-uniform), 30% rational "
+                 "(w ~ U[0.5, 2]), random-phase sinusoid heights (amplitude 0.01-0.2), half distance (k=8, 4 rounds, "
+                 "FP64 Newton closest points) and half intersection (6 rounds, padding on, FP64 Newton points), "
+                 "nuv0 uniform in 64-512 per pair, one query_batch call per step")
+
+
+def run_cfg4(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    import jsi_cad_next_versions_b200 as J
+    from jsi_cad_next_versions_b200 import synth
+    ctx = J.Context(local)
+    ctx.workers(args.lanes)
+    ctx.batch_chunk(args.chunk)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    batch = synth.mixed_batch(args.queries, seed=7 + 1000 * rank)
+    surfaces = [x for a, b, _ in batch for x in (a, b)]
+    ids = ctx.upload_many(surfaces)
+    queries = [(m["kind"], ctx.task(ids[2 * q], np.array(a.rect(), np.float32), m["nuv0"], 1),
+                ctx.task(ids[2 * q + 1], np.array(b.rect(), np.float32), m["nuv0"], 2))
+               for q, (a, b, m) in enumerate(batch)]
+    forms = [f for f in args.forms.split(",") if f and f != "v5_fp32"]
+    points_cap = 4096
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        return reduce_max(x, pg, f"cuda:{local}") if pg else x
+    results = {}
+    outs = {}
+    for form in forms:
+        last = []
+
+        def step():
+            res, status, ms = ctx.query_batch(queries, precision=form, newton=True, points=True,
+                                              points_cap=points_cap)
+            last[:] = [res, status, ms]
+        clk = ClockSampler(local)
+        clk.__enter__()
+        launches0 = ctx.launch_count()
+        times = [max_over_ranks(t) for t in _timed_steps(args, flush, stream, barrier, step)]
+        launches = (ctx.launch_count() - launches0) / (args.steps + args.warmup)
+        ctx.workers(1)
+        ctx.kernel_timing(True)
+        step()
+        kt = ctx.kernel_times()
+        dom, roof = dominant_roofline(ctx, kt, form, len(queries))
+        ctx.kernel_timing(False)
+        ctx.workers(args.lanes)
+        clk.__exit__(None, None, None)
+        res, status, _ = last
+        lat = [r.device_ms for r in res if r is not None]
+        outs[form] = res
+        results[form] = {"queries_per_s": world * len(queries) * args.steps / (sum(times) / 1e3),
+                         "ms_per_step": sum(times) / args.steps, "p50_ms": percentile(lat, 0.5),
+                         "p99_ms": percentile(lat, 0.99), "failed": int(sum(1 for s_ in status if s_ != 0)),
+                         "gpu_launches": launches, "clocks": clk.summary(), "dominant_kernel": dom,
+                         "roofline": roof,
+                         "kernel_ms": {k: round(v[0], 3) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}}
+    # distance / point agreement of the forms (query by query)
+    err = None
+    if "fp64" in outs and forms[0] != "fp64":
+        e = 0.0
+        for a, b in zip(outs[forms[0]], outs["fp64"]):
+            if a is None or b is None:
+                continue
+            if hasattr(a, "kth_d2"):
+                d = abs(a.newton_distance - b.newton_distance) / max(abs(b.newton_distance), 1e-300)
+            else:
+                d = 0.0 if np.array_equal(a.points, b.points) else float(
+                    np.abs(a.points[:, :3] - b.points[:, :3]).max()) if a.points.shape == b.points.shape else 1.0
+            e = max(e, d)
+        err = e
+    # end to end: host surfaces packed once, uploaded per step, the batch,
+    # results read back (distances, up to points_cap points per intersection),
+    # surfaces released
+    form = forms[0]
+    ctx.release_many(ids)
+    hostset = J.SurfaceBatch(surfaces)
+
+    def e2e_step():
+        sid = np.asarray(ctx.upload_many(hostset), np.int32)
+        rects = ctx.surface_domains(sid)
+        qs = [(m["kind"], ctx.task(int(sid[2 * q]), rects[2 * q], m["nuv0"], 1),
+               ctx.task(int(sid[2 * q + 1]), rects[2 * q + 1], m["nuv0"], 2)) for q, (_, _, m) in enumerate(batch)]
+        ctx.query_batch(qs, precision=form, newton=True, points=True, points_cap=points_cap)
+        ctx.release_many(sid)
+    h0, d0 = ctx.transfer_bytes()
+    e2e_t = [max_over_ranks(t) for t in _timed_steps(args, flush, stream, barrier, e2e_step)]
+    h1, d1 = ctx.transfer_bytes()
+    nrun = args.steps + args.warmup
+    e2e = {"value": world * len(queries) * args.steps / (sum(e2e_t) / 1e3), "unit": "queries/s",
+           "h2d_bytes_per_step": (h1 - h0) // nrun, "d2h_bytes_per_step": (d1 - d0) // nrun, "form": form,
+           "points_copied_per_intersection": f"up to {points_cap}"}
+    if rank != 0:
+        ctx.close()
+        if pg:
+            pg.destroy_process_group()
+        return
+    head = results[form]
+    cpu = None if args.no_cpu_baseline else cpu_baseline_cfg4(batch)
+    line = {
+        "metric": METRIC, "value": head["queries_per_s"], "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"fp64": "f64", "fp32_screen": "f32+f64"}[form], "data": "synthetic",
+        "config": {"workload": CFG4_WORKLOAD.format(n=len(queries)), "form": form,
+                   "queries_per_step_per_gpu": len(queries), "lanes": args.lanes, "chunk": args.chunk,
+                   "l2": "flushed (256 MiB write) between steps", "parallelism": f"dp{world}"},
+        "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"],
+                       "note": "per-query device time inside the batch"},
+        "forms": results, "max_rel_err_vs_fp64": err,
+        "speedup_vs_fp64": head["queries_per_s"] / results["fp64"]["queries_per_s"] if "fp64" in results else None,
+        "e2e": e2e, "roofline": head["roofline"], "cpu_baseline": cpu, "clocks": head["clocks"],
+        "gpu_launches": head["gpu_launches"],
+    }
+    print(json.dumps(line))
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def cpu_baseline_cfg4(batch, budget_s: float = 20.0):
+    """The reference on the batch's first queries, alternating kinds, until
+    about budget_s of host time: queries/s = queries run / time."""
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    import oracle
+    if not oracle.Reference.available():
+        return None
+    R = oracle.Reference()
+    t0 = time.perf_counter()
+    done = {"distance": 0, "intersection": 0}
+    for a, b, m in batch:
+        ra, rb = np.array(a.rect(), np.float32), np.array(b.rect(), np.float32)
+        if m["kind"] == "distance":
+            R.minimum_distance(a, b, ra, rb, m["nuv0"], 16, 8, 4)
+        else:
+            R.intersection(a, b, ra, rb, m["nuv0"], 16, 1)
+        done[m["kind"]] += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    n = sum(done.values())
+    return {"value": n / el, "unit": "queries/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
+            "sample": f"the batch's first {n} queries ({done['distance']} distance, {done['intersection']} "
+                      f"intersection) through the reference, {el:.1f} s"}
+
+
+def run_reference_cfg4(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from jsi_cad_next_versions_b200 import synth
+    batch = synth.mixed_batch(args.queries, seed=7)
+    cpu = cpu_baseline_cfg4(batch)
+    if cpu is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libjsi_v5_ref.so was not built"}))
+        return
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "queries/s", "n_gpus": world,
+        "steps": 1, "warmup": 0, "ms_per_step": 1e3 / cpu["value"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": CFG4_WORKLOAD.format(n=args.queries), "cores": cpu["cores"]},
+        "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "queries/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.config == 3:
+        (run_reference_cfg3 if args.impl == "reference" else run_cfg3)(args)
+    elif args.config == 4:
+        (run_reference_cfg4 if args.impl == "reference" else run_cfg4)(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

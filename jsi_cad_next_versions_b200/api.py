@@ -359,6 +359,13 @@ class Context:
             out[n] = (ms.value, cnt.value, units.value)
         return out
 
+    def kernel_units(self, name: str) -> float:
+        """Work units counted under a name since kernel_timing(True) (also
+        the algorithmic flops of a kernel, as "<kernel>:flops")."""
+        units = ctypes.c_double(0)
+        self._check(self.lib.jsi_kernel_units(self.handle, name.encode(), ctypes.byref(units)))
+        return units.value
+
     def launch_count(self) -> int:
         v = ctypes.c_ulonglong(0)
         self._check(self.lib.jsi_launch_count(ctypes.byref(v)))

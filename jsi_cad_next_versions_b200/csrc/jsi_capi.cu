@@ -798,6 +798,22 @@ SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, Regio
   return s;
 }
 
+// Algorithmic flops of one sample of the intersection's sample kernel (FMA =
+// 2 flops): with need_k the full record (every derivative combination within
+// the degrees, evaluation.cu:259-356: rational terms N w, N w P, row sum and
+// v sum, 8 flops per control point and per row; non-rational 6) plus the
+// quotient rule (~60); without, the position alone.
+double record_flops(int degu, int degv, int du, int dv, bool rat, bool need_k) {
+  const double per_cp = rat ? 8.0 : 6.0;
+  const double combo = (degv + 1.0) * (degu + 1.0) * per_cp + (degv + 1.0) * per_cp;
+  if (!need_k) return combo + (rat ? 4.0 : 0.0);
+  const int ku[6] = {0, 1, 0, 2, 1, 0}, kv[6] = {0, 0, 1, 0, 1, 2};
+  double f = 0.0;
+  for (int m = 0; m < 6; ++m)
+    if (ku[m] <= du && kv[m] <= dv) f += combo;
+  return f + (rat ? 60.0 : 0.0);
+}
+
 // Evaluation + cell + tile build of one side (run_evaluation_and_construction_task,
 // distance_analysis.cu:88-116 / intersection.cu:175-219).
 template <typename T>
@@ -815,7 +831,9 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
     return;
   }
   if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
-  timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); }, double(s.nreg) * s.g.nuv * s.g.nuv);
+  const double nsamp = double(s.nreg) * s.g.nuv * s.g.nuv;
+  add_units(ctx, "samples:flops", nsamp * record_flops(v.degu, v.degv, v.du, v.dv, v.rat != 0, need_k));
+  timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); }, nsamp);
   if (intersect) timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
   timed(ctx, "cells", [&] { launch_cells(s, intersect, st); }, double(s.nreg) * s.g.W * s.g.W);
   JSI_CUDA(cudaGetLastError());
@@ -1923,6 +1941,8 @@ void inter_screen_round(Lane *ctx, const SurfaceRec &sa, const SurfaceRec &sb, S
       JSI_CUDA(cudaMemsetAsync(klo, 0, sizeof(unsigned) * 3 * P.nreg, st));
       JSI_CUDA(cudaMemsetAsync(P.kmax, 0, sizeof(unsigned long long) * 3 * P.nreg, st));
     }
+    add_units(ctx, "samples:flops",
+              double(nsamp) * record_flops(s.ivec[1], s.ivec[4], s.du, s.dv, s.rat != 0, use_k));
     timed(ctx, "samples", [&] {
       launch_iscreen_samples(view<float>(s), P, C, use_k, khi, klo, screen_gamma(s) * 1.01, s.cmax, s.wcmax, s.wmax,
                              st);
