@@ -250,8 +250,13 @@ struct Lane {
   ScreenStats *h_stats = nullptr;
   unsigned long long h2d_bytes = 0, d2h_bytes = 0;
   // Optional per-kernel timing: CUDA events recorded on the lane's stream
-  // around every launch, resolved at the next host sync.
-  bool timing = false;
+  // around every launch, resolved at the next host sync.  The lane's thread
+  // writes the timing state while the caller's thread turns timing on or off
+  // and reads the totals, so timing, event_pool, pending, kernel_ms and
+  // kernel_units are only touched under stats_mu (timing itself is atomic so
+  // that the untimed launch path takes no lock).
+  std::mutex stats_mu;
+  std::atomic<bool> timing{false};
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   std::map<std::string, std::pair<double, long long>> kernel_ms;
@@ -274,8 +279,12 @@ struct Lane {
   };
   std::map<std::vector<long long>, GraphEntry> graphs;
   unsigned long long graph_clock = 0;
-  long long graph_replays = 0;
-  bool graphs_on = false;
+  std::atomic<long long> graph_replays{0};
+  std::atomic<bool> graphs_on{false};  // set by the caller's thread, read by the lane's
+  // True while the lane's stream captures a graph: per-kernel timing then
+  // stays off even if the caller turns it on meanwhile (events recorded into
+  // a graph cannot be timed).
+  bool capturing = false;
 };
 
 // One query of a batch: its tasks, the caller's result slot and its status
@@ -839,6 +848,7 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
   JSI_CUDA(cudaGetLastError());
 }
 
+// Callers hold ctx->stats_mu.
 cudaEvent_t take_event(Lane *ctx) {
   if (!ctx->event_pool.empty()) {
     cudaEvent_t e = ctx->event_pool.back();
@@ -852,6 +862,7 @@ cudaEvent_t take_event(Lane *ctx) {
 
 // Resolves recorded kernel timings; call after the stream has synchronised.
 void resolve_timing(Lane *ctx) {
+  std::lock_guard<std::mutex> lk(ctx->stats_mu);
   for (auto &p : ctx->pending) {
     float ms = 0.0f;
     JSI_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
@@ -866,21 +877,29 @@ void resolve_timing(Lane *ctx) {
 
 // Work units of a kernel (for the live roofline); only kept while timing.
 void add_units(Lane *ctx, const char *name, double units) {
-  if (ctx->timing) ctx->kernel_units[name] += units;
+  if (!ctx->timing || ctx->capturing) return;
+  std::lock_guard<std::mutex> lk(ctx->stats_mu);
+  ctx->kernel_units[name] += units;
 }
 
 // Runs one launcher, bracketed by events when timing is on.
 template <typename Fn>
 void timed(Lane *ctx, const char *name, Fn &&fn, double units = 0) {
-  if (!ctx->timing) {
+  if (!ctx->timing || ctx->capturing) {
     fn();
     return;
   }
   add_units(ctx, name, units);
-  cudaEvent_t a = take_event(ctx), b = take_event(ctx);
+  cudaEvent_t a, b;
+  {
+    std::lock_guard<std::mutex> lk(ctx->stats_mu);
+    a = take_event(ctx);
+    b = take_event(ctx);
+  }
   JSI_CUDA(cudaEventRecord(a, ctx->stream));
   fn();
   JSI_CUDA(cudaEventRecord(b, ctx->stream));
+  std::lock_guard<std::mutex> lk(ctx->stats_mu);
   ctx->pending.push_back({name, {a, b}});
 }
 
@@ -897,7 +916,7 @@ void pull_stats(Lane *ctx) {
   JSI_CUDA(copy_async(ctx, ctx->h_stats, ctx->d_stats, sizeof(ScreenStats), cudaMemcpyDeviceToHost, ctx->stream));
   JSI_CUDA(cudaStreamSynchronize(ctx->stream));
   JSI_CUDA(cudaGetLastError());
-  if (ctx->timing) resolve_timing(ctx);
+  resolve_timing(ctx);
 }
 
 unsigned bit_cast_u32(float x) {
@@ -1725,13 +1744,16 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
     const unsigned long long before = launch_count();
     cudaGraph_t graph = nullptr;
     JSI_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    L->capturing = true;
     try {
       enqueue();
     } catch (...) {
+      L->capturing = false;
       cudaStreamEndCapture(st, &graph);
       if (graph) cudaGraphDestroy(graph);
       throw;
     }
+    L->capturing = false;
     JSI_CUDA(cudaStreamEndCapture(st, &graph));
     cudaGraphExec_t exec = nullptr;
     const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
@@ -1757,7 +1779,7 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
     }
   }
   JSI_CUDA(cudaStreamSynchronize(st));
-  if (L->timing) resolve_timing(L);
+  resolve_timing(L);
 
   // Results, in the order and with the meaning run_distance gives them.
   int rerun = 0;
@@ -2714,7 +2736,7 @@ void exec_distance(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_dist
   JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
   JSI_CUDA(cudaEventSynchronize(L->ev1));
   JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
-  if (L->timing) resolve_timing(L);
+  resolve_timing(L);
 }
 
 void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_inter_params &p,
@@ -2744,7 +2766,7 @@ void exec_intersection(Lane *L, const jsi_task *a, const jsi_task *b, const jsi_
   JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
   JSI_CUDA(cudaEventSynchronize(L->ev1));
   JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
-  if (L->timing) resolve_timing(L);
+  resolve_timing(L);
 }
 
 int run_guarded(std::string &err, const std::function<void()> &fn);
@@ -3113,9 +3135,16 @@ int jsi_kernel_timing(jsi_context *ctx, int enable) {
   if (!ctx) return JSI_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->mu);
   auto set = [&](Lane &L) {
+    std::lock_guard<std::mutex> ls(L.stats_mu);
     L.timing = enable != 0;
     L.kernel_ms.clear();
     L.kernel_units.clear();
+    // Events of unresolved launches go back to the pool (re-recording an
+    // event that is still pending on the stream is allowed).
+    for (auto &pe : L.pending) {
+      L.event_pool.push_back(pe.second.first);
+      L.event_pool.push_back(pe.second.second);
+    }
     L.pending.clear();
   };
   set(ctx->main);
@@ -3129,6 +3158,7 @@ int jsi_kernel_time(jsi_context *ctx, const char *name, double *total_ms, long l
   *total_ms = 0.0;
   *launches = 0;
   auto add = [&](Lane &L) {
+    std::lock_guard<std::mutex> ls(L.stats_mu);
     auto it = L.kernel_ms.find(name);
     if (it != L.kernel_ms.end()) {
       *total_ms += it->second.first;
@@ -3145,6 +3175,7 @@ int jsi_kernel_units(jsi_context *ctx, const char *name, double *units) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   *units = 0.0;
   auto add = [&](Lane &L) {
+    std::lock_guard<std::mutex> ls(L.stats_mu);
     auto it = L.kernel_units.find(name);
     if (it != L.kernel_units.end()) *units += it->second;
   };
@@ -3158,8 +3189,10 @@ const char *jsi_kernel_names(jsi_context *ctx) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   std::map<std::string, int> names;
   for (auto &kv : ctx->main.kernel_ms) names[kv.first] = 1;
-  for (auto &L : ctx->lanes)
+  for (auto &L : ctx->lanes) {
+    std::lock_guard<std::mutex> ls(L->stats_mu);
     for (auto &kv : L->kernel_ms) names[kv.first] = 1;
+  }
   ctx->kernel_names.clear();
   for (auto &kv : names) {
     if (!ctx->kernel_names.empty()) ctx->kernel_names += ",";
@@ -3238,7 +3271,7 @@ int jsi_intersection_curves(jsi_context *ctx, const jsi_task *a, const jsi_task 
     JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
     JSI_CUDA(cudaEventSynchronize(L->ev1));
     JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
-    if (L->timing) resolve_timing(L);
+    resolve_timing(L);
     return JSI_OK;
   });
 }
@@ -3274,7 +3307,7 @@ int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, 
     JSI_CUDA(cudaEventRecord(L->ev1, L->stream));
     JSI_CUDA(cudaEventSynchronize(L->ev1));
     JSI_CUDA(cudaEventElapsedTime(&out->device_ms, L->ev0, L->ev1));
-    if (L->timing) resolve_timing(L);
+    resolve_timing(L);
     return JSI_OK;
   });
 }
