@@ -2917,7 +2917,7 @@ void start_workers(jsi_context *ctx, int n) {
     lane_init(*L, ctx->device, std::min(cap, size_t(512) << 20), cap, &ctx->surfaces, &ctx->lane_held, left);
     L->surfaces_mu = &ctx->surf_mu;
     L->graphs_on = ctx->batch_graphs;
-    L->timing = ctx->main.timing;  // per-kernel timing follows the context's setting
+    L->timing = ctx->main.timing.load();  // per-kernel timing follows the context's setting
     ctx->lanes.push_back(std::move(L));
   }
   for (auto &L : ctx->lanes) ctx->threads.emplace_back(worker_loop, ctx, L.get());
