@@ -788,15 +788,20 @@ SurfaceRec upload_resident(jsi_context *ctx, const int ivec[7], const float *dat
 
 
 // Allocates one side's per-round arrays for nreg regions.
+// tables = false (intersection sides that the fused region kernel builds):
+// no spans, basis tables or sample grid.
 template <typename T>
-SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, RegionRec<T> *regions) {
+SideRound<T> make_side(Arena &ar, const Geom &g, int nreg, bool intersect, RegionRec<T> *regions,
+                       bool tables = true) {
   SideRound<T> s{};
   s.g = g;
   s.nreg = nreg;
   s.regions = regions ? regions : ar.get<RegionRec<T>>(nreg);
-  s.spans = ar.get<int>(static_cast<size_t>(nreg) * 2 * g.nuv);
-  s.basis = ar.get<T>(static_cast<size_t>(nreg) * 2 * g.nuv * 3 * g.p1max);
-  s.samples = intersect ? ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv) : nullptr;
+  if (tables) {
+    s.spans = ar.get<int>(static_cast<size_t>(nreg) * 2 * g.nuv);
+    s.basis = ar.get<T>(static_cast<size_t>(nreg) * 2 * g.nuv * 3 * g.p1max);
+  }
+  s.samples = intersect && tables ? ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.nuv * g.nuv) : nullptr;
   s.kmax = ar.get<unsigned long long>(static_cast<size_t>(nreg) * 3);
   s.pad = ar.get<T>(nreg);
   s.center = ar.get<Vec4<T>>(static_cast<size_t>(nreg) * g.cpr);
@@ -830,18 +835,25 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
                 T span_v0, bool cover = false) {
   cudaStream_t st = ctx->stream;
   const bool need_k = intersect && use_k;
-  timed(ctx, "basis", [&] {
-    launch_basis(v, s, st, Batch{}, static_cast<const SurfView<T> *>(nullptr), cover, !intersect && !cover);
-  }, 2.0 * s.nreg * s.g.nuv);
+  if (!intersect || s.samples)
+    timed(ctx, "basis", [&] {
+      launch_basis(v, s, st, Batch{}, static_cast<const SurfView<T> *>(nullptr), cover, !intersect && !cover);
+    }, 2.0 * s.nreg * s.g.nuv);
   if (!intersect) {
     // Distance: centres straight from the basis tables, no sample grid.
     timed(ctx, "cells", [&] { launch_cells_fused(v, s, s, st); }, double(s.nreg) * s.g.W * s.g.W);
     JSI_CUDA(cudaGetLastError());
     return;
   }
-  if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
   const double nsamp = double(s.nreg) * s.g.nuv * s.g.nuv;
   add_units(ctx, "samples:flops", nsamp * record_flops(v.degu, v.degv, v.du, v.dv, v.rat != 0, need_k));
+  if (!s.samples) {
+    // Small regions without tables: one fused launch per side.
+    timed(ctx, "region_cells", [&] { launch_region_cells(v, s, need_k, span_u0, span_v0, cover, st); }, nsamp);
+    JSI_CUDA(cudaGetLastError());
+    return;
+  }
+  if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
   timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); }, nsamp);
   if (intersect) timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
   timed(ctx, "cells", [&] { launch_cells(s, intersect, st); }, double(s.nreg) * s.g.W * s.g.W);
@@ -2232,8 +2244,11 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
     int *nmap1, *nmap2, r1, r2;
     next_regions<T>(ctx, sorted, n, ij_bits, slot_bits, A, B, map1, map2, cover, &next1, &next2, &nmap1, &nmap2, &r1,
                     &r2);
-    A = make_side<T>(ar, make_geom(nuv, p1_of(sa)), r1, true, next1);
-    B = make_side<T>(ar, make_geom(nuv, p1_of(sb)), r2, true, next2);
+    // Refinement rounds of small regions run the fused region kernel (no
+    // basis tables or sample grid).
+    const Geom g1 = make_geom(nuv, p1_of(sa)), g2 = make_geom(nuv, p1_of(sb));
+    A = make_side<T>(ar, g1, r1, true, next1, !(g1.nuv <= kRegNuv && g1.p1max <= kRegP1));
+    B = make_side<T>(ar, g2, r2, true, next2, !(g2.nuv <= kRegNuv && g2.p1max <= kRegP1));
     map1 = nmap1;
     map2 = nmap2;
     nslots = n;

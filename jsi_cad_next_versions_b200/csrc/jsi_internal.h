@@ -203,6 +203,19 @@ template <typename T>
 void launch_pad(const SideRound<T> &sr, bool use_k, T span_u0, T span_v0, cudaStream_t st);
 template <typename T>
 void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st, const Batch &bt = Batch{});
+// Limits of the fused region kernel: samples per direction and basis stride
+// (degree + 1).
+constexpr int kRegNuv = 16;
+constexpr int kRegP1 = 9;
+// Intersection sides of small regions (nuv <= 16, degree <= 8): basis,
+// samples, compute_K padding, cells and tile ranges of every region in one
+// launch, bit-identical to launch_basis + launch_samples + launch_pad +
+// launch_cells (the basis tables and sample grid are not written).
+template <typename T>
+bool region_cells_fits(const SideRound<T> &sr);
+template <typename T>
+void launch_region_cells(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, T span_u0, T span_v0, bool cover,
+                         cudaStream_t st);
 template <typename T>
 void launch_records(const SurfView<T> &s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out, cudaStream_t st);
 

@@ -621,6 +621,152 @@ __global__ void k_cells(SideRound<T> sr, int intersect, long long qs) {
   }
 }
 
+// Intersection cells of small regions in one pass (refinement rounds, nuv <=
+// kRegNuv): one block per region computes the region's knot spans and basis
+// lines (k_basis), its samples and compute_K terms (k_samples), its padding
+// (k_pad) and its cells and tile ranges (k_cells) in shared memory, with the
+// same functions and operation order as those kernels, so centres, half
+// spans, paddings and tile ranges carry the same bits; nothing but the
+// cells, tile ranges and padding goes to HBM.
+template <typename T>
+__global__ void __launch_bounds__(256) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
+                                                      T span_v0, int cover) {
+  __shared__ T sb[2][kRegNuv][3][kRegP1];
+  __shared__ int ssp[2][kRegNuv];
+  __shared__ Vec4<T> smp[kRegNuv * kRegNuv];
+  __shared__ Vec4<T> scen[kRegNuv * kRegNuv], shal[kRegNuv * kRegNuv];
+  __shared__ unsigned long long skm[3];
+  const Geom g = sr.g;
+  const int nuv = g.nuv, te2 = g.te * g.te, tid = threadIdx.x;
+  for (int r = blockIdx.x; r < sr.nreg; r += gridDim.x) {
+    const RegionRec<T> reg = sr.regions[r];
+    if (tid < 3) skm[tid] = 0ull;
+    // basis lines: u lines 0..nuv-1, v lines nuv..2 nuv-1 (k_basis)
+    if (tid < 2 * nuv) {
+      const int dir = tid >= nuv, q = tid - dir * nuv;
+      const T lo = dir ? reg.v0 : reg.u0;
+      const T hi = dir ? reg.v1 : reg.u1;
+      const T step = cover ? (hi - lo) / static_cast<T>(nuv - 1) : (hi - lo) / static_cast<T>(nuv);
+      const T x = (cover && q == nuv - 1) ? hi : step * static_cast<T>(q) + lo;
+      const int p = dir ? s.degv : s.degu;
+      T *out = &sb[dir][q][0][0];
+      if (s.zero) {
+        ssp[dir][q] = p;
+        for (int j = 0; j < 3 * kRegP1; ++j) out[j] = T(0);
+      } else {
+        const int span = find_span(dir ? s.nkv : s.nku, p, x, dir ? s.V : s.U);
+        ssp[dir][q] = span;
+        for (int j = 0; j < 3 * kRegP1; ++j) out[j] = T(0);
+        basis_ders<T, kRegP1>(span, p, x, dir ? s.V : s.U, min(dir ? s.dv : s.du, 2), out, kRegP1);
+      }
+      // the global tables are not written: nothing downstream reads them
+    }
+    __syncthreads();
+    // samples and compute_K terms (k_samples; max is exact and order-free)
+    T kuu = T(0), kuv = T(0), kvv = T(0);
+    for (int t = tid; t < nuv * nuv; t += blockDim.x) {
+      const int idx = t % nuv, idy = t / nuv;
+      Vec4<T> P;
+      if (need_k) {
+        T rec[18];
+        eval_record(s, ssp[0][idx], &sb[0][idx][0][0], ssp[1][idy], &sb[1][idy][0][0], kRegP1, rec);
+        P = Vec4<T>{rec[0], rec[1], rec[2], T(0)};
+        kuu = tmax(kuu, tmax(fabs(rec[9]), tmax(fabs(rec[10]), fabs(rec[11]))));
+        kuv = tmax(kuv, tmax(fabs(rec[12]), tmax(fabs(rec[13]), fabs(rec[14]))));
+        kvv = tmax(kvv, tmax(fabs(rec[15]), tmax(fabs(rec[16]), fabs(rec[17]))));
+      } else {
+        T q3[3];
+        eval_point(s, ssp[0][idx], &sb[0][idx][0][0], ssp[1][idy], &sb[1][idy][0][0], q3);
+        P = Vec4<T>{q3[0], q3[1], q3[2], T(0)};
+      }
+      smp[t] = P;
+    }
+    if (need_k) {
+      atomic_max_bits(&skm[0], kuu);
+      atomic_max_bits(&skm[1], kuv);
+      atomic_max_bits(&skm[2], kvv);
+    }
+    __syncthreads();
+    // padding (k_pad)
+    if (tid == 0) {
+      T pad = T(0);
+      if (need_k) {
+        const T muu = from_ordered<T>(skm[0]), muv = from_ordered<T>(skm[1]), mvv = from_ordered<T>(skm[2]);
+        const int side = nuv > 1 ? nuv - 1 : 1;
+        const T ss = static_cast<T>(side * side);
+        const T raw = (muu / ss + T(2) * muv / ss + mvv / ss) / T(8);
+        const T us = fabs(reg.u1 - reg.u0) / span_u0;
+        const T vs = fabs(reg.v1 - reg.v0) / span_v0;
+        const T ps = tmax(us, vs);
+        pad = raw * ps * ps;
+        if (!isfinite(pad) || pad < T(0)) pad = T(0);
+        sr.kmax[3 * r + 0] = skm[0];
+        sr.kmax[3 * r + 1] = skm[1];
+        sr.kmax[3 * r + 2] = skm[2];
+      }
+      sr.pad[r] = pad;
+    }
+    // cells, tile-major (k_cells): thread per padded cell slot
+    const int ncell = g.ntiles * te2;
+    for (int c = tid; c < ncell; c += blockDim.x) {
+      const int tile = c / te2, local = c - tile * te2;
+      const int ty = tile / g.tw, tx = tile - ty * g.tw;
+      const int a = local / g.te, b = local - (local / g.te) * g.te;
+      const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
+      Vec4<T> cen{T(0), T(0), T(0), T(0)}, hal{T(0), T(0), T(0), T(0)};
+      if (a < nv && b < nu) {
+        const int iv = ty * g.te + a, iu = tx * g.te + b;
+        const Vec4<T> p0 = smp[iv * nuv + iu], q1 = smp[iv * nuv + iu + 1];
+        const Vec4<T> p2 = smp[(iv + 1) * nuv + iu], p3 = smp[(iv + 1) * nuv + iu + 1];
+        const T lx = tmin(p0.x, tmin(q1.x, tmin(p2.x, p3.x)));
+        const T ly = tmin(p0.y, tmin(q1.y, tmin(p2.y, p3.y)));
+        const T lz = tmin(p0.z, tmin(q1.z, tmin(p2.z, p3.z)));
+        const T hx = tmax(p0.x, tmax(q1.x, tmax(p2.x, p3.x)));
+        const T hy = tmax(p0.y, tmax(q1.y, tmax(p2.y, p3.y)));
+        const T hz = tmax(p0.z, tmax(q1.z, tmax(p2.z, p3.z)));
+        cen.x = (lx + hx) / T(2);
+        cen.y = (ly + hy) / T(2);
+        cen.z = (lz + hz) / T(2);
+        hal.x = (hx - lx) / T(2);
+        hal.y = (hy - ly) / T(2);
+        hal.z = (hz - lz) / T(2);
+      }
+      const long long o = static_cast<long long>(r) * g.cpr + c;
+      sr.center[o] = cen;
+      sr.half[o] = hal;
+      scen[c] = cen;
+      shal[c] = hal;
+    }
+    __syncthreads();
+    // tile ranges of the centres and largest half spans (valid cells only)
+    if (tid < g.ntiles) {
+      const int ty = tid / g.tw, tx = tid - ty * g.tw;
+      const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
+      T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
+      T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
+      T hm[3] = {T(0), T(0), T(0)};
+      for (int a = 0; a < nv; ++a)
+        for (int b = 0; b < nu; ++b) {
+          const Vec4<T> cen = scen[tid * te2 + a * g.te + b], hal = shal[tid * te2 + a * g.te + b];
+          lo[0] = tmin(lo[0], cen.x);
+          lo[1] = tmin(lo[1], cen.y);
+          lo[2] = tmin(lo[2], cen.z);
+          hi[0] = tmax(hi[0], cen.x);
+          hi[1] = tmax(hi[1], cen.y);
+          hi[2] = tmax(hi[2], cen.z);
+          hm[0] = tmax(hm[0], hal.x);
+          hm[1] = tmax(hm[1], hal.y);
+          hm[2] = tmax(hm[2], hal.z);
+        }
+      const long long t = static_cast<long long>(r) * g.ntiles + tid;
+      sr.tlo[t] = Vec4<T>{lo[0], lo[1], lo[2], T(0)};
+      sr.thi[t] = Vec4<T>{hi[0], hi[1], hi[2], T(0)};
+      sr.thmax[t] = Vec4<T>{hm[0], hm[1], hm[2], T(0)};
+    }
+    __syncthreads();
+  }
+}
+
 template <typename T>
 __global__ void k_records(SurfView<T> s, T ustep, T vstep, T ustart, T vstart, int nuv, T *out) {
   // Full-record grid for the evalWithCuda entry point; basis per sample.
@@ -3723,6 +3869,67 @@ __device__ void point_record(const SurfView<double> &s, double u, double v, doub
   eval_record(s, spanu, Nu, spanv, Nv, kMaxDeg + 1, rec);
 }
 
+// P, Pu, Pv of one point: the first 9 values of point_record, bit for bit
+// (the same basis functions and first derivatives, which A2.3 forms
+// independently of the higher orders; the same contractions; the first-order
+// steps of the quotient rule), without the second-order work.  MAXP bounds
+// degree + 1.
+template <int MAXP>
+__device__ void point_record1_impl(const SurfView<double> &s, double u, double v, double rec[9]) {
+  double Nu[3 * MAXP], Nv[3 * MAXP];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) rec[q] = 0.0;
+  if (s.zero) return;
+  const int spanu = find_span(s.nku, s.degu, u, s.U);
+  basis_ders<double, MAXP>(spanu, s.degu, u, s.U, min(s.du, 1), Nu, MAXP);
+  const int spanv = find_span(s.nkv, s.degv, v, s.V);
+  basis_ders<double, MAXP>(spanv, s.degv, v, s.V, min(s.dv, 1), Nv, MAXP);
+  const int cu0 = spanu - s.degu, cv0 = spanv - s.degv;
+  const int ku[3] = {0, 1, 0}, lv[3] = {0, 0, 1};
+  if (!s.rat) {
+    for (int m = 0; m < 3; ++m) {
+      if (ku[m] > s.du || lv[m] > s.dv) continue;
+      double acc[3];
+      contract3(s, cu0, cv0, Nu + ku[m] * MAXP, Nv + lv[m] * MAXP, acc);
+      rec[3 * m] = acc[0];
+      rec[3 * m + 1] = acc[1];
+      rec[3 * m + 2] = acc[2];
+    }
+    return;
+  }
+  double h[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) h[q] = 0.0;
+  for (int m = 0; m < 3; ++m) {
+    if (ku[m] > s.du || lv[m] > s.dv) continue;
+    double acc[4];
+    contract4(s, cu0, cv0, Nu + ku[m] * MAXP, Nv + lv[m] * MAXP, acc);
+    h[4 * m] = acc[0];
+    h[4 * m + 1] = acc[1];
+    h[4 * m + 2] = acc[2];
+    h[4 * m + 3] = acc[3];
+  }
+  // quotient2's first-order part
+  const double inv = 1.0 / h[3];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) h[q] *= inv;
+  const double ws = -h[7], wt = -h[11];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    h[4 + c] += ws * h[c];
+    h[8 + c] += wt * h[c];
+  }
+  for (int m = 0; m < 3; ++m)
+    for (int c = 0; c < 3; ++c) rec[3 * m + c] = h[4 * m + c];
+}
+
+__device__ void point_record1(const SurfView<double> &s, double u, double v, double rec[9]) {
+  if (s.degu < 9 && s.degv < 9)
+    point_record1_impl<9>(s, u, v, rec);
+  else
+    point_record1_impl<kMaxDeg + 1>(s, u, v, rec);
+}
+
 __device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 __device__ __forceinline__ double clampd(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
@@ -3873,10 +4080,10 @@ __global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const Su
 // unknowns): step = -J^T (J J^T)^-1 D.  out: x, y, z, u, v, s, t, residual.
 __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> &sb, const double dom[8], double x[4],
                              double out[8]) {
-  double r1[18], r2[18], D[3];
+  double r1[9], r2[9], D[3];
   for (int it = 0; it < 40; ++it) {
-    point_record(sa, x[0], x[1], r1);
-    point_record(sb, x[2], x[3], r2);
+    point_record1(sa, x[0], x[1], r1);
+    point_record1(sb, x[2], x[3], r2);
     for (int c = 0; c < 3; ++c) D[c] = r1[c] - r2[c];
     const double J[3][4] = {{r1[3], r1[6], -r2[3], -r2[6]},
                             {r1[4], r1[7], -r2[4], -r2[7]},
@@ -3898,8 +4105,8 @@ __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> 
     }
     if (dmax <= 1e-15) break;
   }
-  point_record(sa, x[0], x[1], r1);
-  point_record(sb, x[2], x[3], r2);
+  point_record1(sa, x[0], x[1], r1);
+  point_record1(sb, x[2], x[3], r2);
   for (int c = 0; c < 3; ++c) {
     D[c] = r1[c] - r2[c];
     out[c] = 0.5 * (r1[c] + r2[c]);
@@ -4069,6 +4276,20 @@ void launch_cells(const SideRound<T> &sr, bool intersect, cudaStream_t st, const
   counted();
   const long long warps = static_cast<long long>(sr.nreg) * sr.g.ntiles;
   k_cells<T><<<bdim(bgrid((warps + 7) / 8, bt, 148 * 32), bt), 256, 0, st>>>(sr, intersect ? 1 : 0, bt.qs);
+}
+
+template <typename T>
+bool region_cells_fits(const SideRound<T> &sr) {
+  return sr.g.nuv <= kRegNuv && sr.g.p1max <= kRegP1;
+}
+
+template <typename T>
+void launch_region_cells(const SurfView<T> &s, const SideRound<T> &sr, bool need_k, T span_u0, T span_v0, bool cover,
+                         cudaStream_t st) {
+  counted();
+  if (sr.nreg <= 0) return;
+  const int blocks = sr.nreg < 148 * 16 ? sr.nreg : 148 * 16;
+  k_region_cells<T><<<blocks, 256, 0, st>>>(s, sr, need_k ? 1 : 0, span_u0, span_v0, cover ? 1 : 0);
 }
 
 template <typename T>
@@ -4530,6 +4751,8 @@ void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb,
   template void launch_samples<T>(const SurfView<T> &, const SideRound<T> &, bool, cudaStream_t, const Batch &,   \
                                   const SurfView<T> *);                                                           \
   template void launch_pad<T>(const SideRound<T> &, bool, T, T, cudaStream_t);                                    \
+  template bool region_cells_fits<T>(const SideRound<T> &);                                                       \
+  template void launch_region_cells<T>(const SurfView<T> &, const SideRound<T> &, bool, T, T, bool, cudaStream_t); \
   template void launch_cells<T>(const SideRound<T> &, bool, cudaStream_t, const Batch &);                         \
   template void launch_records<T>(const SurfView<T> &, T, T, T, T, int, T *, cudaStream_t);                       \
   template void launch_dist_tau<T>(const SideRound<T> &, const SideRound<T> &, const int *, const int *, int, int, \
