@@ -354,6 +354,9 @@ int jsi_min_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi
 int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const jsi_task *b,
                               const jsi_dist_params *params, jsi_dist_result *out, int *status, jsi_ticket *ticket);
 int jsi_wait_distance_batch(jsi_context *ctx, jsi_ticket ticket, float *device_ms);
+/* Whether every lane job of a submitted distance batch has finished (*done =
+ * 1; jsi_wait_distance_batch then returns without blocking), without waiting. */
+int jsi_poll_distance_batch(jsi_context *ctx, jsi_ticket ticket, int *done);
 /* Queries per lockstep batch (default 64; 0: every query runs alone). */
 int jsi_batch_chunk(jsi_context *ctx, int chunk);
 /* Batch items re-run alone after an internal list overflowed (all lanes). */

@@ -35,7 +35,7 @@ EXPORTED = [
     "jsi_distance_bounds", "jsi_curve_params_default", "jsi_intersection_curves", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
     "jsi_queue_depth", "jsi_min_distance_batch", "jsi_submit_distance_batch", "jsi_wait_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs", "jsi_autotune_batch",
-    "jsi_query_batch",
+    "jsi_query_batch", "jsi_poll_distance_batch",
 ]
 
 
@@ -221,6 +221,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
                                   ctypes.POINTER(DistParams), ctypes.POINTER(InterParams), ctypes.POINTER(DistResult),
                                   ctypes.POINTER(InterResult), ctypes.POINTER(I), ctypes.POINTER(ctypes.c_float)]
     L.jsi_query_batch.restype = I
+    L.jsi_poll_distance_batch.argtypes = [P, ctypes.c_longlong, ctypes.POINTER(I)]
+    L.jsi_poll_distance_batch.restype = I
     L.jsi_eval_grid_noalloc.argtypes = [P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                         I, P]
     L.jsi_eval_grid_noalloc.restype = I

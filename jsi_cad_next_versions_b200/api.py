@@ -539,6 +539,12 @@ class Context:
         # everything the C side writes into or reads from stays alive here
         return {"ticket": t.value, "tasks": tasks, "res": res, "bufs": bufs, "status": status, "k": k}
 
+    def poll_distance_batch(self, handle) -> bool:
+        """True when every lane job of a submitted batch has finished."""
+        d = ctypes.c_int(0)
+        self._check(self.lib.jsi_poll_distance_batch(self.handle, handle["ticket"], ctypes.byref(d)))
+        return bool(d.value)
+
     def wait_distance_batch(self, handle):
         """Wait for a submitted batch: (DistanceBatch, device_ms)."""
         ms = ctypes.c_float(0)

@@ -3633,6 +3633,18 @@ int jsi_submit_distance_batch(jsi_context *ctx, int n, const jsi_task *a, const 
   return JSI_OK;
 }
 
+int jsi_poll_distance_batch(jsi_context *ctx, jsi_ticket ticket, int *done) {
+  if (!ctx || !done) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->qmu);
+  auto it = ctx->batches.find(ticket);
+  if (it == ctx->batches.end()) return record(ctx, JSI_ERR_INVALID, "unknown batch ticket");
+  int all = 1;
+  for (auto &j : it->second->all_jobs)
+    if (!j->done) all = 0;
+  *done = all;
+  return JSI_OK;
+}
+
 int jsi_wait_distance_batch(jsi_context *ctx, jsi_ticket ticket, float *device_ms) {
   if (!ctx) return JSI_ERR_INVALID;
   std::unique_ptr<PendingBatch> pb;
