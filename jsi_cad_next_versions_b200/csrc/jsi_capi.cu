@@ -697,22 +697,70 @@ SurfaceRec make_block(jsi_context *ctx, const SurfaceRec &head, const int ivec[7
   return s;
 }
 
+// surface_header and the copy of the record into the staging ring in one
+// pass over the caller's data: knots copied, then every control point (and
+// weight) copied while its magnitudes are folded in.  The results equal
+// surface_header's (max and |x| are exact; the weighted products of two
+// floats are exact in double).
+void stage_surface(SurfaceRec &s, const int ivec[7], const float *data, int ndata, float *dst) {
+  std::memcpy(s.ivec, ivec, sizeof(s.ivec));
+  const int flags = ivec[0];
+  s.rat = (flags & 2) ? 1 : 0;
+  s.zero = ((!(flags & 1)) && (flags & 12)) || ivec[1] >= kMaxDeg || ivec[4] >= kMaxDeg;
+  s.du = std::min(2, ivec[1]);
+  s.dv = std::min(2, ivec[4]);
+  s.dom[0] = data[0];
+  s.dom[1] = data[ivec[3]];
+  s.dom[2] = data[ivec[3] - 1];
+  s.dom[3] = data[ivec[3] + ivec[6] - 1];
+  const size_t nk = static_cast<size_t>(ivec[3]) + ivec[6];
+  const size_t ncp = static_cast<size_t>(ivec[2]) * ivec[5];
+  std::memcpy(dst, data, nk * sizeof(float));
+  const float *cp = data + nk;
+  float *dcp = dst + nk;
+  float m[3] = {0.0f, 0.0f, 0.0f};
+  for (size_t q = 0; q < ncp; ++q) {
+    const float x = cp[3 * q], y = cp[3 * q + 1], z = cp[3 * q + 2];
+    dcp[3 * q] = x;
+    dcp[3 * q + 1] = y;
+    dcp[3 * q + 2] = z;
+    m[0] = std::max(m[0], std::fabs(x));
+    m[1] = std::max(m[1], std::fabs(y));
+    m[2] = std::max(m[2], std::fabs(z));
+  }
+  for (int c = 0; c < 3; ++c) s.cmax[c] = s.wcmax[c] = m[c];
+  s.wmin = s.wmax = 1.0;
+  size_t done = nk + 3 * ncp;
+  if (s.rat && ncp > 0) {
+    const float *w = cp + 3 * ncp;
+    float *dw = dcp + 3 * ncp;
+    float lo = w[0], hi = w[0];
+    double wm[3] = {0.0, 0.0, 0.0};
+    for (size_t q = 0; q < ncp; ++q) {
+      const float wq = w[q];
+      dw[q] = wq;
+      lo = std::min(lo, wq);
+      hi = std::max(hi, wq);
+      for (int c = 0; c < 3; ++c)
+        wm[c] = std::max(wm[c], std::fabs(static_cast<double>(wq) * static_cast<double>(cp[3 * q + c])));
+    }
+    s.wmin = lo;
+    s.wmax = hi;
+    for (int c = 0; c < 3; ++c) s.wcmax[c] = wm[c];
+    done += ncp;
+  }
+  // the rest of the record (nothing the header describes) as given
+  if (static_cast<size_t>(ndata) > done)
+    std::memcpy(dst + done, data + done, (static_cast<size_t>(ndata) - done) * sizeof(float));
+}
+
 void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &in, std::vector<SurfaceRec> &out) {
   Lane *L = &ctx->main;
   cudaStream_t st = L->stream;
-  // Checks and magnitudes of every surface, on host threads.
+  // Header checks (ivec and ndata only) first, so that a bad surface fails
+  // the call before anything is staged.
+  for (size_t q = 0; q < in.size(); ++q) check_surface(in[q].ivec, in[q].data, in[q].ndata);
   std::vector<SurfaceRec> heads(in.size());
-  std::vector<char> bad(in.size(), 0);
-  parallel_for(ctx->hpool.get(), in.size(), [&](size_t q) {
-    try {
-      check_surface(in[q].ivec, in[q].data, in[q].ndata);
-      surface_header(heads[q], in[q].ivec, in[q].data);
-    } catch (...) {
-      bad[q] = 1;
-    }
-  });
-  for (size_t q = 0; q < in.size(); ++q)
-    if (bad[q]) check_surface(in[q].ivec, in[q].data, in[q].ndata);  // throws again, on this thread
   auto al = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
   auto next_segment = [&]() {
     JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
@@ -725,6 +773,7 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
     const size_t rec_b = al(static_cast<size_t>(in[q].ndata) * sizeof(float));
     if (rec_b + al(sizeof(SurfacePrep)) > kRingSeg) {
       // Larger than a segment: its own device staging, completed here.
+      surface_header(heads[q], in[q].ivec, in[q].data);
       SurfacePrep job;
       out.push_back(make_block(ctx, heads[q], in[q].ivec, in[q].ndata, &job));
       char *tmp = nullptr;
@@ -743,29 +792,32 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
       ++q;
       continue;
     }
-    // Pack as many records as fit in the rest of the segment, then the jobs.
+    // Plan the segment: as many records as fit in the rest of it, then the
+    // jobs; the copies (with the header pass fused in) run on host threads.
     if (ctx->ring_off + rec_b + al(sizeof(SurfacePrep)) > kRingSeg) next_segment();
     const size_t seg0 = static_cast<size_t>(ctx->ring_cur) * kRingSeg;
     size_t off = ctx->ring_off;
-    std::vector<SurfacePrep> jobs;
     std::vector<std::pair<size_t, size_t>> copies;  // (surface, ring offset)
-    long long most = 0;
     while (q < in.size()) {
       const size_t rb = al(static_cast<size_t>(in[q].ndata) * sizeof(float));
-      if (off + rb + al(sizeof(SurfacePrep) * (jobs.size() + 1)) > kRingSeg) break;
-      SurfacePrep job;
-      out.push_back(make_block(ctx, heads[q], in[q].ivec, in[q].ndata, &job));
+      if (off + rb + al(sizeof(SurfacePrep) * (copies.size() + 1)) > kRingSeg) break;
       copies.push_back({q, off});
-      job.src = reinterpret_cast<const float *>(ctx->dring + seg0 + off);
-      most = std::max(most, std::max(job.ndata, job.ncp));
-      jobs.push_back(job);
       off += rb;
       ++q;
     }
     parallel_for(ctx->hpool.get(), copies.size(), [&](size_t e) {
-      const PendingSurface &ps = in[copies[e].first];
-      std::memcpy(ctx->ring + seg0 + copies[e].second, ps.data, static_cast<size_t>(ps.ndata) * sizeof(float));
+      const size_t sq = copies[e].first;
+      const PendingSurface &ps = in[sq];
+      stage_surface(heads[sq], ps.ivec, ps.data, ps.ndata, reinterpret_cast<float *>(ctx->ring + seg0 + copies[e].second));
     });
+    std::vector<SurfacePrep> jobs(copies.size());
+    long long most = 0;
+    for (size_t e = 0; e < copies.size(); ++e) {
+      const size_t sq = copies[e].first;
+      out.push_back(make_block(ctx, heads[sq], in[sq].ivec, in[sq].ndata, &jobs[e]));
+      jobs[e].src = reinterpret_cast<const float *>(ctx->dring + seg0 + copies[e].second);
+      most = std::max(most, std::max(jobs[e].ndata, jobs[e].ncp));
+    }
     const size_t jobs_b = sizeof(SurfacePrep) * jobs.size();
     std::memcpy(ctx->ring + seg0 + off, jobs.data(), jobs_b);
     const size_t start = ctx->ring_off;
