@@ -372,6 +372,23 @@ def run_ours(args):
         ref_values[form] = last.v5_value if form == "v5_fp32" else last.distance
         results[form]["distances"] = step_distances
 
+    # ---------------- the plain per-query FP64 path --------------------------
+    # One query per call (jsi_min_distance: no batching, the host reads each
+    # round's counts), on a bounded sample of the same queries.
+    nq = min(24, len(tasks))
+    for ta, tb in tasks[:2]:
+        ctx.min_distance(ta, tb, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision="fp64")
+    flush.zero_()
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for ta, tb in tasks[:nq]:
+        ctx.min_distance(ta, tb, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision="fp64")
+    p1.record(stream)
+    torch.cuda.synchronize()
+    fp64_per_query = nq / (p0.elapsed_time(p1) / 1e3)
+
     # ---------------- end to end through the C ABI, host buffers -----------
     form = forms[0]
     h0, d0 = ctx.transfer_bytes()
@@ -470,6 +487,8 @@ def run_ours(args):
                   for f, r in results.items()},
         "rel_err_vs_fp64": rel_err,
         "speedup_vs_fp64": (head["value"] / results["fp64"]["value"]) if "fp64" in results else None,
+        "fp64_per_query_qps": fp64_per_query,
+        "speedup_vs_fp64_per_query": head["value"] / fp64_per_query,
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": head["clocks"],
         "gpu_launches": head["gpu_launches"],
         "batch_reruns": head["reruns"],
