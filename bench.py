@@ -779,6 +779,8 @@ def run_cfg4(args):
         results[form] = {"queries_per_s": world * len(queries) * args.steps / (sum(times) / 1e3),
                          "ms_per_step": sum(times) / args.steps, "p50_ms": percentile(lat, 0.5),
                          "p99_ms": percentile(lat, 0.99), "failed": int(sum(1 for s_ in status if s_ != 0)),
+                         "failed_status": sorted({int(s_) for s_ in status if s_ != 0}),
+                         "failed_queries": [q for q, s_ in enumerate(status) if s_ != 0][:8],
                          "gpu_launches": launches, "clocks": clk.summary(), "dominant_kernel": dom,
                          "roofline": roof,
                          "kernel_ms": {k: round(v[0], 3) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}}

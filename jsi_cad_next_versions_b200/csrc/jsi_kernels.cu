@@ -622,93 +622,140 @@ __global__ void k_cells(SideRound<T> sr, int intersect, long long qs) {
 }
 
 // Intersection cells of small regions in one pass (refinement rounds, nuv <=
-// kRegNuv): one block per region computes the region's knot spans and basis
-// lines (k_basis), its samples and compute_K terms (k_samples), its padding
-// (k_pad) and its cells and tile ranges (k_cells) in shared memory, with the
-// same functions and operation order as those kernels, so centres, half
-// spans, paddings and tile ranges carry the same bits; nothing but the
-// cells, tile ranges and padding goes to HBM.
+// kRegNuv): a block of kRegThreads threads takes rpb regions at a time (rpb =
+// kRegThreads / nuv^2, at most kRegMaxRpb, so that the block's threads stay
+// busy at nuv 4 and 8) and computes, in shared memory, the regions' knot spans
+// and basis lines (as k_basis), samples and compute_K terms (as k_samples),
+// paddings (as k_pad), and cells and tile ranges (as k_cells), with the same
+// functions and operation order, so centres, half spans and paddings carry
+// the same bits.  Tile ranges are folded with order-preserving integer
+// atomics (exact minima / maxima).  Nothing but the cells, tile ranges and
+// paddings goes to HBM.
+constexpr int kRegThreads = 256;
+constexpr int kRegMaxRpb = 16;
+
+__host__ __device__ inline int region_cells_rpb(int nuv) {
+  int r = kRegThreads / (nuv * nuv);
+  if (r < 1) r = 1;
+  if (r > kRegMaxRpb) r = kRegMaxRpb;
+  return r;
+}
+
+__host__ __device__ inline size_t al16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
+
+// Shared-memory layout of one block: basis [rpb][2 nuv][3 p1], spans
+// [rpb][2 nuv], samples [rpb][nuv^2], region maxima [rpb][3], tile folds
+// [rpb][ntiles][9].
 template <typename T>
-__global__ void __launch_bounds__(256) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
-                                                      T span_v0, int cover) {
-  __shared__ T sb[2][kRegNuv][3][kRegP1];
-  __shared__ int ssp[2][kRegNuv];
-  __shared__ Vec4<T> smp[kRegNuv * kRegNuv];
-  __shared__ Vec4<T> scen[kRegNuv * kRegNuv], shal[kRegNuv * kRegNuv];
-  __shared__ unsigned long long skm[3];
+__host__ __device__ inline size_t region_cells_smem(const Geom &g, int rpb, size_t *offs) {
+  using U = typename OrdBits<T>::type;
+  size_t o = 0;
+  offs[0] = o;
+  o = al16(o + sizeof(T) * rpb * 2 * g.nuv * 3 * g.p1max);
+  offs[1] = o;
+  o = al16(o + sizeof(int) * rpb * 2 * g.nuv);
+  offs[2] = o;
+  o = al16(o + sizeof(Vec4<T>) * rpb * g.nuv * g.nuv);
+  offs[3] = o;
+  o = al16(o + sizeof(unsigned long long) * rpb * 3);
+  offs[4] = o;
+  o = al16(o + sizeof(U) * rpb * g.ntiles * 9);
+  return o;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRegThreads) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
+                                                              T span_v0, int cover) {
+  using U = typename OrdBits<T>::type;
+  extern __shared__ __align__(16) unsigned char rc_raw[];
   const Geom g = sr.g;
-  const int nuv = g.nuv, te2 = g.te * g.te, tid = threadIdx.x;
-  for (int r = blockIdx.x; r < sr.nreg; r += gridDim.x) {
-    const RegionRec<T> reg = sr.regions[r];
-    if (tid < 3) skm[tid] = 0ull;
-    // basis lines: u lines 0..nuv-1, v lines nuv..2 nuv-1 (k_basis)
-    if (tid < 2 * nuv) {
-      const int dir = tid >= nuv, q = tid - dir * nuv;
+  const int nuv = g.nuv, p1 = g.p1max, te2 = g.te * g.te, nl = 2 * nuv, ns = nuv * nuv;
+  const int ncell = g.ntiles * te2, rpb = region_cells_rpb(nuv), tid = threadIdx.x, nth = blockDim.x;
+  size_t offs[5];
+  region_cells_smem<T>(g, rpb, offs);
+  T *sb = reinterpret_cast<T *>(rc_raw + offs[0]);
+  int *ssp = reinterpret_cast<int *>(rc_raw + offs[1]);
+  Vec4<T> *smp = reinterpret_cast<Vec4<T> *>(rc_raw + offs[2]);
+  unsigned long long *skm = reinterpret_cast<unsigned long long *>(rc_raw + offs[3]);
+  U *stl = reinterpret_cast<U *>(rc_raw + offs[4]);
+  const U lo_id = ~U(0), hi_id = U(0), hm_id = ord_enc(T(0));
+  for (int r0 = blockIdx.x * rpb; r0 < sr.nreg; r0 += gridDim.x * rpb) {
+    const int nr = min(rpb, sr.nreg - r0);
+    for (int t = tid; t < nr * 3; t += nth) skm[t] = 0ull;
+    for (int t = tid; t < nr * g.ntiles; t += nth) {
+      U *f = stl + static_cast<long long>(t) * 9;
+      f[0] = f[1] = f[2] = lo_id;
+      f[3] = f[4] = f[5] = hi_id;
+      f[6] = f[7] = f[8] = hm_id;
+    }
+    // basis lines of every region: u lines 0..nuv-1, v lines nuv..2 nuv-1
+    for (int t = tid; t < nr * nl; t += nth) {
+      const int k = t / nl, line = t - k * nl;
+      const RegionRec<T> reg = sr.regions[r0 + k];
+      const int dir = line >= nuv, q = line - dir * nuv;
       const T lo = dir ? reg.v0 : reg.u0;
       const T hi = dir ? reg.v1 : reg.u1;
       const T step = cover ? (hi - lo) / static_cast<T>(nuv - 1) : (hi - lo) / static_cast<T>(nuv);
       const T x = (cover && q == nuv - 1) ? hi : step * static_cast<T>(q) + lo;
       const int p = dir ? s.degv : s.degu;
-      T *out = &sb[dir][q][0][0];
+      T *out = sb + static_cast<long long>(t) * 3 * p1;
+      for (int j = 0; j < 3 * p1; ++j) out[j] = T(0);
       if (s.zero) {
-        ssp[dir][q] = p;
-        for (int j = 0; j < 3 * kRegP1; ++j) out[j] = T(0);
+        ssp[t] = p;
       } else {
         const int span = find_span(dir ? s.nkv : s.nku, p, x, dir ? s.V : s.U);
-        ssp[dir][q] = span;
-        for (int j = 0; j < 3 * kRegP1; ++j) out[j] = T(0);
-        basis_ders<T, kRegP1>(span, p, x, dir ? s.V : s.U, min(dir ? s.dv : s.du, 2), out, kRegP1);
+        ssp[t] = span;
+        basis_ders<T, kRegP1>(span, p, x, dir ? s.V : s.U, min(dir ? s.dv : s.du, 2), out, p1);
       }
-      // the global tables are not written: nothing downstream reads them
     }
     __syncthreads();
-    // samples and compute_K terms (k_samples; max is exact and order-free)
-    T kuu = T(0), kuv = T(0), kvv = T(0);
-    for (int t = tid; t < nuv * nuv; t += blockDim.x) {
-      const int idx = t % nuv, idy = t / nuv;
+    // samples and compute_K terms (max is exact and order-free)
+    for (int t = tid; t < nr * ns; t += nth) {
+      const int k = t / ns, qq = t - k * ns;
+      const int idx = qq % nuv, idy = qq / nuv;
+      const int lu = k * nl + idx, lv = k * nl + nuv + idy;
+      const T *Nu = sb + static_cast<long long>(lu) * 3 * p1, *Nv = sb + static_cast<long long>(lv) * 3 * p1;
       Vec4<T> P;
       if (need_k) {
         T rec[18];
-        eval_record(s, ssp[0][idx], &sb[0][idx][0][0], ssp[1][idy], &sb[1][idy][0][0], kRegP1, rec);
+        eval_record(s, ssp[lu], Nu, ssp[lv], Nv, p1, rec);
         P = Vec4<T>{rec[0], rec[1], rec[2], T(0)};
-        kuu = tmax(kuu, tmax(fabs(rec[9]), tmax(fabs(rec[10]), fabs(rec[11]))));
-        kuv = tmax(kuv, tmax(fabs(rec[12]), tmax(fabs(rec[13]), fabs(rec[14]))));
-        kvv = tmax(kvv, tmax(fabs(rec[15]), tmax(fabs(rec[16]), fabs(rec[17]))));
+        atomic_max_bits(&skm[3 * k + 0], tmax(fabs(rec[9]), tmax(fabs(rec[10]), fabs(rec[11]))));
+        atomic_max_bits(&skm[3 * k + 1], tmax(fabs(rec[12]), tmax(fabs(rec[13]), fabs(rec[14]))));
+        atomic_max_bits(&skm[3 * k + 2], tmax(fabs(rec[15]), tmax(fabs(rec[16]), fabs(rec[17]))));
       } else {
         T q3[3];
-        eval_point(s, ssp[0][idx], &sb[0][idx][0][0], ssp[1][idy], &sb[1][idy][0][0], q3);
+        eval_point(s, ssp[lu], Nu, ssp[lv], Nv, q3);
         P = Vec4<T>{q3[0], q3[1], q3[2], T(0)};
       }
       smp[t] = P;
     }
-    if (need_k) {
-      atomic_max_bits(&skm[0], kuu);
-      atomic_max_bits(&skm[1], kuv);
-      atomic_max_bits(&skm[2], kvv);
-    }
     __syncthreads();
-    // padding (k_pad)
-    if (tid == 0) {
+    // paddings (k_pad)
+    for (int k = tid; k < nr; k += nth) {
+      const int r = r0 + k;
       T pad = T(0);
       if (need_k) {
-        const T muu = from_ordered<T>(skm[0]), muv = from_ordered<T>(skm[1]), mvv = from_ordered<T>(skm[2]);
+        const T muu = from_ordered<T>(skm[3 * k]), muv = from_ordered<T>(skm[3 * k + 1]),
+                mvv = from_ordered<T>(skm[3 * k + 2]);
         const int side = nuv > 1 ? nuv - 1 : 1;
         const T ss = static_cast<T>(side * side);
         const T raw = (muu / ss + T(2) * muv / ss + mvv / ss) / T(8);
+        const RegionRec<T> reg = sr.regions[r];
         const T us = fabs(reg.u1 - reg.u0) / span_u0;
         const T vs = fabs(reg.v1 - reg.v0) / span_v0;
         const T ps = tmax(us, vs);
         pad = raw * ps * ps;
         if (!isfinite(pad) || pad < T(0)) pad = T(0);
-        sr.kmax[3 * r + 0] = skm[0];
-        sr.kmax[3 * r + 1] = skm[1];
-        sr.kmax[3 * r + 2] = skm[2];
+        sr.kmax[3 * r + 0] = skm[3 * k];
+        sr.kmax[3 * r + 1] = skm[3 * k + 1];
+        sr.kmax[3 * r + 2] = skm[3 * k + 2];
       }
       sr.pad[r] = pad;
     }
-    // cells, tile-major (k_cells): thread per padded cell slot
-    const int ncell = g.ntiles * te2;
-    for (int c = tid; c < ncell; c += blockDim.x) {
+    // cells, tile-major (k_cells), folded into the tile ranges
+    for (int t = tid; t < nr * ncell; t += nth) {
+      const int k = t / ncell, c = t - k * ncell;
       const int tile = c / te2, local = c - tile * te2;
       const int ty = tile / g.tw, tx = tile - ty * g.tw;
       const int a = local / g.te, b = local - (local / g.te) * g.te;
@@ -716,8 +763,9 @@ __global__ void __launch_bounds__(256) k_region_cells(SurfView<T> s, SideRound<T
       Vec4<T> cen{T(0), T(0), T(0), T(0)}, hal{T(0), T(0), T(0), T(0)};
       if (a < nv && b < nu) {
         const int iv = ty * g.te + a, iu = tx * g.te + b;
-        const Vec4<T> p0 = smp[iv * nuv + iu], q1 = smp[iv * nuv + iu + 1];
-        const Vec4<T> p2 = smp[(iv + 1) * nuv + iu], p3 = smp[(iv + 1) * nuv + iu + 1];
+        const Vec4<T> *S = smp + static_cast<long long>(k) * ns;
+        const Vec4<T> p0 = S[iv * nuv + iu], q1 = S[iv * nuv + iu + 1];
+        const Vec4<T> p2 = S[(iv + 1) * nuv + iu], p3 = S[(iv + 1) * nuv + iu + 1];
         const T lx = tmin(p0.x, tmin(q1.x, tmin(p2.x, p3.x)));
         const T ly = tmin(p0.y, tmin(q1.y, tmin(p2.y, p3.y)));
         const T lz = tmin(p0.z, tmin(q1.z, tmin(p2.z, p3.z)));
@@ -730,38 +778,28 @@ __global__ void __launch_bounds__(256) k_region_cells(SurfView<T> s, SideRound<T
         hal.x = (hx - lx) / T(2);
         hal.y = (hy - ly) / T(2);
         hal.z = (hz - lz) / T(2);
+        U *f = stl + (static_cast<long long>(k) * g.ntiles + tile) * 9;
+        atomicMin(f + 0, ord_enc(cen.x));
+        atomicMin(f + 1, ord_enc(cen.y));
+        atomicMin(f + 2, ord_enc(cen.z));
+        atomicMax(f + 3, ord_enc(cen.x));
+        atomicMax(f + 4, ord_enc(cen.y));
+        atomicMax(f + 5, ord_enc(cen.z));
+        atomicMax(f + 6, ord_enc(hal.x));
+        atomicMax(f + 7, ord_enc(hal.y));
+        atomicMax(f + 8, ord_enc(hal.z));
       }
-      const long long o = static_cast<long long>(r) * g.cpr + c;
+      const long long o = static_cast<long long>(r0 + k) * g.cpr + c;
       sr.center[o] = cen;
       sr.half[o] = hal;
-      scen[c] = cen;
-      shal[c] = hal;
     }
     __syncthreads();
-    // tile ranges of the centres and largest half spans (valid cells only)
-    if (tid < g.ntiles) {
-      const int ty = tid / g.tw, tx = tid - ty * g.tw;
-      const int nv = min(g.te, g.W - ty * g.te), nu = min(g.te, g.W - tx * g.te);
-      T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
-      T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
-      T hm[3] = {T(0), T(0), T(0)};
-      for (int a = 0; a < nv; ++a)
-        for (int b = 0; b < nu; ++b) {
-          const Vec4<T> cen = scen[tid * te2 + a * g.te + b], hal = shal[tid * te2 + a * g.te + b];
-          lo[0] = tmin(lo[0], cen.x);
-          lo[1] = tmin(lo[1], cen.y);
-          lo[2] = tmin(lo[2], cen.z);
-          hi[0] = tmax(hi[0], cen.x);
-          hi[1] = tmax(hi[1], cen.y);
-          hi[2] = tmax(hi[2], cen.z);
-          hm[0] = tmax(hm[0], hal.x);
-          hm[1] = tmax(hm[1], hal.y);
-          hm[2] = tmax(hm[2], hal.z);
-        }
-      const long long t = static_cast<long long>(r) * g.ntiles + tid;
-      sr.tlo[t] = Vec4<T>{lo[0], lo[1], lo[2], T(0)};
-      sr.thi[t] = Vec4<T>{hi[0], hi[1], hi[2], T(0)};
-      sr.thmax[t] = Vec4<T>{hm[0], hm[1], hm[2], T(0)};
+    for (int t = tid; t < nr * g.ntiles; t += nth) {
+      const U *f = stl + static_cast<long long>(t) * 9;
+      const long long o = static_cast<long long>(r0) * g.ntiles + t;
+      sr.tlo[o] = Vec4<T>{ord_dec(f[0]), ord_dec(f[1]), ord_dec(f[2]), T(0)};
+      sr.thi[o] = Vec4<T>{ord_dec(f[3]), ord_dec(f[4]), ord_dec(f[5]), T(0)};
+      sr.thmax[o] = Vec4<T>{ord_dec(f[6]), ord_dec(f[7]), ord_dec(f[8]), T(0)};
     }
     __syncthreads();
   }
@@ -4288,8 +4326,12 @@ void launch_region_cells(const SurfView<T> &s, const SideRound<T> &sr, bool need
                          cudaStream_t st) {
   counted();
   if (sr.nreg <= 0) return;
-  const int blocks = sr.nreg < 148 * 16 ? sr.nreg : 148 * 16;
-  k_region_cells<T><<<blocks, 256, 0, st>>>(s, sr, need_k ? 1 : 0, span_u0, span_v0, cover ? 1 : 0);
+  const int rpb = region_cells_rpb(sr.g.nuv);
+  size_t offs[5];
+  const size_t smem = region_cells_smem<T>(sr.g, rpb, offs);
+  const long long groups = (sr.nreg + rpb - 1) / rpb;
+  const int blocks = static_cast<int>(groups < 148 * 16 ? groups : 148 * 16);
+  k_region_cells<T><<<blocks, kRegThreads, smem, st>>>(s, sr, need_k ? 1 : 0, span_u0, span_v0, cover ? 1 : 0);
 }
 
 template <typename T>

@@ -79,7 +79,11 @@ def test_query_batch_equals_alone(lanes_ctx, precision):
                 alone = ctx.intersect(ta, tb, precision=precision, points=True, trace=True)
                 assert np.array_equal(res[q].counts, alone.counts), q
                 for r in range(alone.rounds):
-                    assert np.array_equal(res[q].pairs[r], alone.pairs[r]), (q, r)
+                    # a round beyond a trace buffer's capacity is not traced
+                    # (the batch's buffers are smaller than the alone run's)
+                    if res[q].pairs[r] is not None:
+                        assert np.array_equal(res[q].pairs[r], alone.pairs[r]), (q, r)
+                assert res[q].pairs[0] is not None, q
                 m = min(cap, alone.points.shape[0])
                 assert res[q].points.shape[0] == m, q
                 assert np.array_equal(res[q].points.view(np.uint64), alone.points[:m].view(np.uint64)), q
