@@ -4119,6 +4119,7 @@ __global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const Su
 __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> &sb, const double dom[8], double x[4],
                              double out[8]) {
   double r1[9], r2[9], D[3];
+  double prev = INFINITY;
   for (int it = 0; it < 40; ++it) {
     point_record1(sa, x[0], x[1], r1);
     point_record1(sb, x[2], x[3], r2);
@@ -4141,7 +4142,9 @@ __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> 
       dmax = fmax(dmax, fabs(nx - x[q]));
       x[q] = nx;
     }
-    if (dmax <= 1e-15) break;
+    // converged, or the steps stopped shrinking at rounding level
+    if (dmax <= 1e-15 || (dmax <= 1e-12 && dmax > 0.5 * prev)) break;
+    prev = dmax;
   }
   point_record1(sa, x[0], x[1], r1);
   point_record1(sb, x[2], x[3], r2);

@@ -724,6 +724,7 @@ void lm_distance(const Surface<double> &sa, const Surface<double> &sb, const dou
 void gn_point(const Surface<double> &sa, const Surface<double> &sb, const double dom[8], double x[4],
               double out[8]) {
   double r1[18], r2[18], D[3];
+  double prev = INFINITY;
   for (int it = 0; it < 40; ++it) {
     record_at(sa, x[0], x[1], r1);
     record_at(sb, x[2], x[3], r2);
@@ -747,7 +748,9 @@ void gn_point(const Surface<double> &sa, const Surface<double> &sb, const double
       dmax = std::max(dmax, std::fabs(nx - x[q]));
       x[q] = nx;
     }
-    if (dmax <= 1e-15) break;
+    // converged, or the steps stopped shrinking at rounding level
+    if (dmax <= 1e-15 || (dmax <= 1e-12 && dmax > 0.5 * prev)) break;
+    prev = dmax;
   }
   record_at(sa, x[0], x[1], r1);
   record_at(sb, x[2], x[3], r2);
