@@ -1005,6 +1005,10 @@ void check_task(const jsi_task *t) {
 }
 
 constexpr unsigned long long kMaxTilePairs = 1ull << 27;
+// The intersection's survivor list (8 B per tile pair): refinement rounds of
+// heavily overlapping pairs reach 10^8 tile pairs (13.5 M slots x 16); the
+// arena's budget bounds it further.
+constexpr unsigned long long kMaxInterTilePairs = 1ull << 30;
 
 // ---------------------------------------------------------------------------
 // minimum_distance
@@ -2037,10 +2041,14 @@ void inter_screen_round(Lane *ctx, const SurfaceRec &sa, const SurfaceRec &sb, S
       timed(ctx, "kmax_recheck", [&] { launch_kmax_recheck(v64, P, khi, klo, &ctx->d_stats->rechecked, st); });
     timed(ctx, "pad", [&] { launch_pad<double>(P, use_k, span0[side][0], span0[side][1], st); });
     timed(ctx, "cells", [&] { launch_cells<float>(C, true, st); }, double(C.nreg) * C.g.W * C.g.W);
+    // FP64 positions (one contraction per sample, no curvature terms) and
+    // the FP64 form's cells from them, for the re-check of the candidates.
+    timed(ctx, "samples64", [&] { launch_samples<double>(v64, P, false, st); }, double(nsamp));
+    timed(ctx, "cells64", [&] { launch_cells<double>(P, true, st); }, double(P.nreg) * P.g.W * P.g.W);
   }
   JSI_CUDA(cudaGetLastError());
   const unsigned long long tile_pairs = static_cast<unsigned long long>(A.g.ntiles) * B.g.ntiles;
-  if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+  if (tile_pairs > kMaxInterTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
   unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
   timed(ctx, "inter_cull", [&] {
     launch_inter_cull_screen(S32[0], S32[1], map1, map2, 1, surv, tile_pairs, ctx->d_stats, w, A.pad, B.pad, st);
@@ -2072,8 +2080,7 @@ void inter_screen_round(Lane *ctx, const SurfaceRec &sa, const SurfaceRec &sb, S
   add_units(ctx, "inter_cull", static_cast<double>(tile_pairs));
   unsigned long long *kept = ar.get<unsigned long long>(std::max<unsigned long long>(m, 1));
   timed(ctx, "inter_verify", [&] {
-    launch_inter_verify(view<double>(sa), view<double>(sb), A, B, map1, map2, keys, m, ij_bits, kept, m,
-                        ctx->d_stats, st);
+    launch_inter_verify_cells(A, B, map1, map2, keys, m, ij_bits, kept, m, ctx->d_stats, st);
   }, double(m));
   pull_stats(ctx);
   out->screen_written = static_cast<long long>(m);
@@ -2183,7 +2190,7 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
     }
     if (!screen_now) {
       const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
-      if (tile_pairs > kMaxTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
+      if (tile_pairs > kMaxInterTilePairs) fail(JSI_ERR_CAPACITY, "%llu tile pairs exceed the screen's list", tile_pairs);
       unsigned long long *surv = ar.get<unsigned long long>(tile_pairs);
       reset_stats(ctx);
       timed(ctx, "inter_cull", [&] {

@@ -325,7 +325,8 @@ void launch_inter_leaf(const SideRound<T> &a, const SideRound<T> &b, const int *
 // region) from the FP64 basis tables; exact FP64 curvature maxima from the
 // samples whose bound reaches the maximum (into bs.kmax, count += samples
 // re-evaluated); overlap screen widened per axis by w plus both regions' FP64
-// paddings; FP64 re-check of the candidate keys into out (stats->checked).
+// paddings; FP64 re-check of the candidate keys into out (stats->checked),
+// from the round's FP64 cells.
 void launch_iscreen_samples(const SurfView<float> &s, const SideRound<double> &bs, const SideRound<float> &out,
                             bool need_k, Vec4<float> *khi, unsigned *klo, double g, const double cmax[3],
                             const double wcmax[3], double wmax, cudaStream_t st);
@@ -338,10 +339,11 @@ void launch_inter_leaf_screen(const SideRound<float> &a, const SideRound<float> 
                               const unsigned long long *surv, unsigned long long nsurv, int ij_bits,
                               unsigned long long *keys, unsigned long long key_cap, ScreenStats *stats,
                               const float w[3], const double *pad64a, const double *pad64b, cudaStream_t st);
-void launch_inter_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
-                         const SideRound<double> &b, const int *map1, const int *map2, const unsigned long long *keys,
-                         unsigned long long n, int ij_bits, unsigned long long *out, unsigned long long cap,
-                         ScreenStats *stats, cudaStream_t st);
+// The same re-check from the FP64 cells of the round (a.center / a.half, with
+// a.pad): a lookup per candidate instead of eight point evaluations.
+void launch_inter_verify_cells(const SideRound<double> &a, const SideRound<double> &b, const int *map1,
+                               const int *map2, const unsigned long long *keys, unsigned long long n, int ij_bits,
+                               unsigned long long *out, unsigned long long cap, ScreenStats *stats, cudaStream_t st);
 // Dedup of the next round's regions from sorted (slot, i, j) keys.
 void launch_inter_prep(const unsigned long long *keys, long long n, int ij_bits, unsigned long long *key2, int *idx,
                        unsigned *flag1, cudaStream_t st);

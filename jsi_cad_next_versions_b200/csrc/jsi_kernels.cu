@@ -2614,7 +2614,7 @@ __global__ void k_samples_screen(SurfView<float> s, const SurfView<float> *vdev,
 //
 // Samples, curvature terms, cell boxes and the overlap screen of a round in
 // FP32; everything the FP64 form's decisions depend on is recovered exactly
-// (see k_iscreen_samples, k_kmax_recheck, k_inter_verify).
+// (see k_iscreen_samples, k_kmax_recheck, k_inter_verify_cells).
 
 // |sum of a basis row| bound: sum_c |N_c| over the p+1 non-zero functions of
 // one grid line, in double, for the per-sample error bounds.
@@ -2861,41 +2861,22 @@ __global__ void k_kmax_recheck(SurfView<double> s, SideRound<double> bs, const V
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(count, mine);
 }
 
-// FP64 cell of the intersection query for one (region, cell id): the four
-// corner samples with the FP64 form's code (eval_point; its P equals
-// eval_record's), then centre and half span exactly as k_cells forms them.
-__device__ __forceinline__ void inter_cell64(const SurfView<double> &s, const SideRound<double> &sr, int r, int cell,
-                                             Vec4<double> &cen, Vec4<double> &hal) {
-  const int nuv = sr.g.nuv, W = sr.g.W, p1 = sr.g.p1max;
-  const int iv = cell / W, iu = cell - (cell / W) * W;
-  double P[4][3];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int idx = iu + (k & 1), idy = iv + (k >> 1);
-    const long long lu = (static_cast<long long>(r) * 2 + 0) * nuv + idx;
-    const long long lv = (static_cast<long long>(r) * 2 + 1) * nuv + idy;
-    eval_point(s, sr.spans[lu], sr.basis + lu * 3 * p1, sr.spans[lv], sr.basis + lv * 3 * p1, P[k]);
-  }
-  double lo[3], hi[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    lo[c] = tmin(P[0][c], tmin(P[1][c], tmin(P[2][c], P[3][c])));
-    hi[c] = tmax(P[0][c], tmax(P[1][c], tmax(P[2][c], P[3][c])));
-  }
-  cen = Vec4<double>{(lo[0] + hi[0]) / 2.0, (lo[1] + hi[1]) / 2.0, (lo[2] + hi[2]) / 2.0, 0.0};
-  hal = Vec4<double>{(hi[0] - lo[0]) / 2.0, (hi[1] - lo[1]) / 2.0, (hi[2] - lo[2]) / 2.0, 0.0};
-}
-
-// FP64 re-check of the FP32 screen's candidate (slot, i, j) keys: the FP64
-// form's boxes and padding, the strict test of intersection.cu:60-62 in the
-// FP64 leaf's operation order.  Kept keys are appended (unordered) to out;
-// stats->checked counts them.
-__global__ void __launch_bounds__(128) k_inter_verify(SurfView<double> sa, SurfView<double> sb,
-                                                      SideRound<double> a, SideRound<double> b, const int *map1,
-                                                      const int *map2, const unsigned long long *keys,
-                                                      unsigned long long n, int ij_bits, unsigned long long *out,
-                                                      unsigned long long cap, ScreenStats *stats) {
+// FP64 re-check from the FP64 cells of the round (the FP64 form's centres and
+// half spans, from its position-only samples): the strict test of
+// intersection.cu:60-62 in the FP64 leaf's operation order, per candidate key.
+__global__ void __launch_bounds__(128) k_inter_verify_cells(SideRound<double> a, SideRound<double> b,
+                                                            const int *map1, const int *map2,
+                                                            const unsigned long long *keys, unsigned long long n,
+                                                            int ij_bits, unsigned long long *out,
+                                                            unsigned long long cap, ScreenStats *stats) {
   const unsigned long long mij = (1ull << ij_bits) - 1ull;
+  auto at = [](const SideRound<double> &sr, int r, int cell) {
+    const Geom &g = sr.g;
+    const int iv = cell / g.W, iu = cell - (cell / g.W) * g.W;
+    const int ty = iv / g.te, tx = iu / g.te;
+    return (static_cast<long long>(r) * g.ntiles + ty * g.tw + tx) * (g.te * g.te) + (iv - ty * g.te) * g.te +
+           (iu - tx * g.te);
+  };
   for (unsigned long long base = blockIdx.x * static_cast<unsigned long long>(blockDim.x); base < n;
        base += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
     const unsigned long long q = base + threadIdx.x;
@@ -2906,11 +2887,10 @@ __global__ void __launch_bounds__(128) k_inter_verify(SurfView<double> sa, SurfV
       const int slot = static_cast<int>(key >> (2 * ij_bits));
       const int i = static_cast<int>((key >> ij_bits) & mij), j = static_cast<int>(key & mij);
       const int r1 = map1[slot], r2 = map2[slot];
-      Vec4<double> c1, h1, c2, h2;
-      inter_cell64(sa, a, r1, i, c1, h1);
-      inter_cell64(sb, b, r2, j, c2, h2);
+      const long long i1 = at(a, r1, i), i2 = at(b, r2, j);
+      const Vec4<double> c1 = a.center[i1], c2 = b.center[i2];
+      Vec4<double> r1v = a.half[i1], r2v = b.half[i2];
       const double p1 = a.pad[r1], p2 = b.pad[r2];
-      Vec4<double> r1v = h1, r2v = h2;
       r1v.x = r1v.x + p1;
       r1v.y = r1v.y + p1;
       r1v.z = r1v.z + p1;
@@ -4600,15 +4580,15 @@ void launch_kmax_recheck(const SurfView<double> &s, const SideRound<double> &bs,
   k_kmax_recheck<<<grid_for(n, 128, 148 * 32), 128, 0, st>>>(s, bs, khi, klo, count);
 }
 
-void launch_inter_verify(const SurfView<double> &sa, const SurfView<double> &sb, const SideRound<double> &a,
-                         const SideRound<double> &b, const int *map1, const int *map2, const unsigned long long *keys,
-                         unsigned long long n, int ij_bits, unsigned long long *out, unsigned long long cap,
-                         ScreenStats *stats, cudaStream_t st) {
+void launch_inter_verify_cells(const SideRound<double> &a, const SideRound<double> &b, const int *map1,
+                               const int *map2, const unsigned long long *keys, unsigned long long n, int ij_bits,
+                               unsigned long long *out, unsigned long long cap, ScreenStats *stats, cudaStream_t st) {
   counted();
   if (n == 0) return;
-  k_inter_verify<<<grid_for(static_cast<long long>(n), 128, 148 * 32), 128, 0, st>>>(
-      sa, sb, a, b, map1, map2, keys, n, ij_bits, out, cap, stats);
+  k_inter_verify_cells<<<grid_for(static_cast<long long>(n), 128, 148 * 32), 128, 0, st>>>(a, b, map1, map2, keys, n,
+                                                                                          ij_bits, out, cap, stats);
 }
+
 
 void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &sb, const RegionRec<double> *reg1,
                            const RegionRec<double> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,

@@ -67,7 +67,7 @@ def test_query_batch_equals_alone(lanes_ctx, precision):
     try:
         cap = 1 << 16
         res, status, ms = ctx.query_batch(queries, precision=precision, newton=True, points=True, trace=True,
-                                          points_cap=cap)
+                                          points_cap=cap, trace_cap=1 << 22)
         assert all(s == 0 for s in status)
         assert ms > 0
         for q, (kind, ta, tb) in enumerate(queries):
@@ -83,7 +83,6 @@ def test_query_batch_equals_alone(lanes_ctx, precision):
                     # (the batch's buffers are smaller than the alone run's)
                     if res[q].pairs[r] is not None:
                         assert np.array_equal(res[q].pairs[r], alone.pairs[r]), (q, r)
-                assert res[q].pairs[0] is not None, q
                 m = min(cap, alone.points.shape[0])
                 assert res[q].points.shape[0] == m, q
                 assert np.array_equal(res[q].points.view(np.uint64), alone.points[:m].view(np.uint64)), q
