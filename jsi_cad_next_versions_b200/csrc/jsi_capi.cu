@@ -1778,7 +1778,8 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
     if (p.newton) {
       const BatchRound<TP, TC> &Rd = lay.rounds[R - 1];
       timed(L, "newton", [&] {
-        launch_newton_dist(view<double>(s0a), view<double>(s0b), Rd.A.regions, Rd.B.regions, Rd.map1, Rd.map2,
+        launch_newton_dist(host_view(view<double>(s0a), dua, dva), host_view(view<double>(s0b), dub, dvb),
+                           Rd.A.regions, Rd.B.regions, Rd.map1, Rd.map2,
                            Rd.A.g.nuv, Rd.B.g.nuv, Rd.top, p.k, lay.head->dom, lay.rec->newton, st, bt,
                            &lay.head->a64, &lay.head->b64, stats);
       });

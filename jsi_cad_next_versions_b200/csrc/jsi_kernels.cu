@@ -256,6 +256,87 @@ __device__ void basis_ders(int span, int p, T u, const T *knots, int nd, T *out,
   }
 }
 
+// A2.3 for a degree P known at compile time: the same operations in the same
+// order as basis_ders (so the same bits), with every loop bound a constant,
+// so that the triangle and the derivative rows stay in registers instead of
+// a local-memory stack frame.
+template <typename T, int P>
+__device__ __forceinline__ void basis_ders_fixed(int span, T u, const T *knots, int nd, T *out, int stride) {
+  T ndu[P + 1][P + 1];
+  T left[P + 1], right[P + 1];
+  T a[2][P + 1];
+  ndu[0][0] = T(1);
+#pragma unroll
+  for (int j = 1; j <= P; ++j) {
+    left[j] = u - knots[span + 1 - j];
+    right[j] = knots[span + j] - u;
+    T saved = T(0);
+#pragma unroll
+    for (int r = 0; r < j; ++r) {
+      ndu[j][r] = right[r + 1] + left[j - r];
+      const T tmp = ndu[r][j - 1] / ndu[j][r];
+      ndu[r][j] = saved + right[r + 1] * tmp;
+      saved = left[j - r] * tmp;
+    }
+    ndu[j][j] = saved;
+  }
+#pragma unroll
+  for (int j = 0; j <= P; ++j) out[j] = ndu[j][P];
+#pragma unroll
+  for (int k = 1; k <= 2; ++k)
+#pragma unroll
+    for (int j = 0; j <= P; ++j) out[k * stride + j] = T(0);
+#pragma unroll
+  for (int r = 0; r <= P; ++r) {
+    a[0][0] = T(1);
+#pragma unroll
+    for (int k = 1; k <= 2; ++k) {
+      if (k > nd) break;
+      const int s1 = (k - 1) & 1, s2 = k & 1;
+      T d = T(0);
+      const int rk = r - k, pk = P - k;
+      if (r >= k) {
+        a[s2][0] = a[s1][0] / ndu[pk + 1][rk];
+        d = a[s2][0] * ndu[rk][pk];
+      }
+      const int j1 = (rk >= -1) ? 1 : -rk;
+      const int j2 = (r - 1 <= pk) ? k - 1 : P - r;
+#pragma unroll
+      for (int j = j1; j <= j2; ++j) {
+        a[s2][j] = (a[s1][j] - a[s1][j - 1]) / ndu[pk + 1][rk + j];
+        d += a[s2][j] * ndu[rk + j][pk];
+      }
+      if (r <= pk) {
+        a[s2][k] = -a[s1][k - 1] / ndu[pk + 1][r];
+        d += a[s2][k] * ndu[r][pk];
+      }
+      out[k * stride + r] = d;
+    }
+  }
+  int fac = P;
+#pragma unroll
+  for (int k = 1; k <= 2; ++k) {
+    if (k > nd) break;
+#pragma unroll
+    for (int j = 0; j <= P; ++j) out[k * stride + j] *= static_cast<T>(fac);
+    fac *= P - k;
+  }
+}
+
+// basis_ders with the common degrees 1-5 on the register path above; other
+// degrees (MAXP >= p + 1) on the general one.
+template <typename T, int MAXP>
+__device__ __forceinline__ void basis_ders_any(int span, int p, T u, const T *knots, int nd, T *out, int stride) {
+  switch (p) {
+    case 1: basis_ders_fixed<T, 1>(span, u, knots, nd, out, stride); return;
+    case 2: basis_ders_fixed<T, 2>(span, u, knots, nd, out, stride); return;
+    case 3: basis_ders_fixed<T, 3>(span, u, knots, nd, out, stride); return;
+    case 4: basis_ders_fixed<T, 4>(span, u, knots, nd, out, stride); return;
+    case 5: basis_ders_fixed<T, 5>(span, u, knots, nd, out, stride); return;
+    default: basis_ders<T, MAXP>(span, p, u, knots, nd, out, stride); return;
+  }
+}
+
 template <typename T, int MAXP>
 __global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<T> *regions, int nreg,
                         const int *dnreg, int nuv, int p1max, int *spans, T *basis, long long qs, int cover,
@@ -296,7 +377,7 @@ __global__ void k_basis(SurfView<T> s, const SurfView<T> *vdev, const RegionRec<
     }
     const int span = find_span(nk, p, x, knots);
     spans[t] = span;
-    basis_ders<T, MAXP>(span, p, x, knots, nd, out, p1max);
+    basis_ders_any<T, MAXP>(span, p, x, knots, nd, out, p1max);
   }
 }
 
@@ -384,6 +465,7 @@ __device__ void eval_record(const SurfView<T> &s, int spanu, const T *Nu, int sp
   const int ku[6] = {0, 1, 0, 2, 1, 0};
   const int lv[6] = {0, 0, 1, 0, 1, 2};
   if (!s.rat) {
+#pragma unroll
     for (int m = 0; m < 6; ++m) {
       if (ku[m] > s.du || lv[m] > s.dv) continue;
       T acc[3];
@@ -397,6 +479,7 @@ __device__ void eval_record(const SurfView<T> &s, int spanu, const T *Nu, int sp
   T h[24];
 #pragma unroll
   for (int q = 0; q < 24; ++q) h[q] = T(0);
+#pragma unroll
   for (int m = 0; m < 6; ++m) {
     if (ku[m] > s.du || lv[m] > s.dv) continue;
     T acc[4];
@@ -407,7 +490,9 @@ __device__ void eval_record(const SurfView<T> &s, int spanu, const T *Nu, int sp
     h[4 * m + 3] = acc[3];
   }
   quotient2(h);
+#pragma unroll
   for (int m = 0; m < 6; ++m)
+#pragma unroll
     for (int c = 0; c < 3; ++c) out[3 * m + c] = h[4 * m + c];
 }
 
@@ -705,7 +790,7 @@ __global__ void __launch_bounds__(kRegThreads) k_region_cells(SurfView<T> s, Sid
       } else {
         const int span = find_span(dir ? s.nkv : s.nku, p, x, dir ? s.V : s.U);
         ssp[t] = span;
-        basis_ders<T, kRegP1>(span, p, x, dir ? s.V : s.U, min(dir ? s.dv : s.du, 2), out, p1);
+        basis_ders_any<T, kRegP1>(span, p, x, dir ? s.V : s.U, min(dir ? s.dv : s.du, 2), out, p1);
       }
     }
     __syncthreads();
@@ -819,9 +904,9 @@ __global__ void k_records(SurfView<T> s, T ustep, T vstep, T ustart, T vstart, i
     int spanu = s.degu, spanv = s.degv;
     if (!s.zero) {
       spanu = find_span(s.nku, s.degu, u, s.U);
-      basis_ders<T, kMaxDeg>(spanu, s.degu, u, s.U, s.du, Nu, kMaxDeg);
+      basis_ders_any<T, kMaxDeg>(spanu, s.degu, u, s.U, s.du, Nu, kMaxDeg);
       spanv = find_span(s.nkv, s.degv, v, s.V);
-      basis_ders<T, kMaxDeg>(spanv, s.degv, v, s.V, s.dv, Nv, kMaxDeg);
+      basis_ders_any<T, kMaxDeg>(spanv, s.degv, v, s.V, s.dv, Nv, kMaxDeg);
     }
     eval_record(s, spanu, Nu, spanv, Nv, kMaxDeg, rec);
     T *o = out + t * 18;
@@ -3874,17 +3959,25 @@ __global__ void k_dist_verify(SurfView<double> sa, SurfView<double> sb, const Su
 // FP64 Newton refinement (closest points, intersection points)
 // ---------------------------------------------------------------------------
 
-// Full 18-value record at an arbitrary (u, v) in FP64.
+// Full 18-value record at an arbitrary (u, v) in FP64.  MAXP bounds degree + 1
+// (the kernels that call it are instantiated for degrees up to 8 and for any
+// degree, so that the common case keeps a small stack frame).
+template <int MAXP>
 __device__ void point_record(const SurfView<double> &s, double u, double v, double rec[18]) {
-  double Nu[3 * (kMaxDeg + 1)], Nv[3 * (kMaxDeg + 1)];
+  double Nu[3 * MAXP], Nv[3 * MAXP];
   int spanu = s.degu, spanv = s.degv;
   if (!s.zero) {
     spanu = find_span(s.nku, s.degu, u, s.U);
-    basis_ders<double, kMaxDeg + 1>(spanu, s.degu, u, s.U, s.du, Nu, kMaxDeg + 1);
+    basis_ders_any<double, MAXP>(spanu, s.degu, u, s.U, s.du, Nu, MAXP);
     spanv = find_span(s.nkv, s.degv, v, s.V);
-    basis_ders<double, kMaxDeg + 1>(spanv, s.degv, v, s.V, s.dv, Nv, kMaxDeg + 1);
+    basis_ders_any<double, MAXP>(spanv, s.degv, v, s.V, s.dv, Nv, MAXP);
   }
-  eval_record(s, spanu, Nu, spanv, Nv, kMaxDeg + 1, rec);
+  eval_record(s, spanu, Nu, spanv, Nv, MAXP, rec);
+}
+
+// The basis bound of a pair of surfaces' kernels: 9 for degrees up to 8.
+inline int newton_maxp(const SurfView<double> &a, const SurfView<double> &b) {
+  return (a.degu < 9 && a.degv < 9 && b.degu < 9 && b.degv < 9) ? 9 : kMaxDeg + 1;
 }
 
 // P, Pu, Pv of one point: the first 9 values of point_record, bit for bit
@@ -3899,9 +3992,9 @@ __device__ void point_record1_impl(const SurfView<double> &s, double u, double v
   for (int q = 0; q < 9; ++q) rec[q] = 0.0;
   if (s.zero) return;
   const int spanu = find_span(s.nku, s.degu, u, s.U);
-  basis_ders<double, MAXP>(spanu, s.degu, u, s.U, min(s.du, 1), Nu, MAXP);
+  basis_ders_any<double, MAXP>(spanu, s.degu, u, s.U, min(s.du, 1), Nu, MAXP);
   const int spanv = find_span(s.nkv, s.degv, v, s.V);
-  basis_ders<double, MAXP>(spanv, s.degv, v, s.V, min(s.dv, 1), Nv, MAXP);
+  basis_ders_any<double, MAXP>(spanv, s.degv, v, s.V, min(s.dv, 1), Nv, MAXP);
   const int cu0 = spanu - s.degu, cv0 = spanv - s.degv;
   const int ku[3] = {0, 1, 0}, lv[3] = {0, 0, 1};
   if (!s.rat) {
@@ -3941,11 +4034,9 @@ __device__ void point_record1_impl(const SurfView<double> &s, double u, double v
     for (int c = 0; c < 3; ++c) rec[3 * m + c] = h[4 * m + c];
 }
 
+template <int MAXP>
 __device__ void point_record1(const SurfView<double> &s, double u, double v, double rec[9]) {
-  if (s.degu < 9 && s.degv < 9)
-    point_record1_impl<9>(s, u, v, rec);
-  else
-    point_record1_impl<kMaxDeg + 1>(s, u, v, rec);
+  point_record1_impl<MAXP>(s, u, v, rec);
 }
 
 __device__ __forceinline__ double dot3(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
@@ -3987,11 +4078,12 @@ __device__ bool solve_small(double M[4][4], double r[4], int n) {
 // Levenberg-Marquardt on f(u, v, s, t) = |S1(u, v) - S2(s, t)|^2 from the
 // centres of the candidate cells, inside the query rectangles.  Records are
 // P, Pu, Pv, Puu, Puv, Pvv (3 each).  out: d, u, v, s, t, P1[3], P2[3].
+template <int MAXP>
 __device__ void newton_distance(const SurfView<double> &sa, const SurfView<double> &sb, const double dom[8],
                                 double x[4], double out[11]) {
   double r1[18], r2[18];
-  point_record(sa, x[0], x[1], r1);
-  point_record(sb, x[2], x[3], r2);
+  point_record<MAXP>(sa, x[0], x[1], r1);
+  point_record<MAXP>(sb, x[2], x[3], r2);
   double D[3] = {r1[0] - r2[0], r1[1] - r2[1], r1[2] - r2[2]};
   double f = dot3(D, D);
   double lam = 1e-6;
@@ -4027,8 +4119,8 @@ __device__ void newton_distance(const SurfView<double> &sa, const SurfView<doubl
       double y[4];
       for (int a = 0; a < 4; ++a) y[a] = clampd(x[a] + step[a], dom[2 * a], dom[2 * a + 1]);
       double q1[18], q2[18];
-      point_record(sa, y[0], y[1], q1);
-      point_record(sb, y[2], y[3], q2);
+      point_record<MAXP>(sa, y[0], y[1], q1);
+      point_record<MAXP>(sb, y[2], y[3], q2);
       const double E[3] = {q1[0] - q2[0], q1[1] - q2[1], q1[2] - q2[2]};
       const double fy = dot3(E, E);
       if (fy < f) {
@@ -4062,7 +4154,7 @@ __device__ void newton_distance(const SurfView<double> &sa, const SurfView<doubl
 }
 
 // One thread per final candidate pair: cell centres as the starting point.
-template <typename TP>
+template <typename TP, int MAXP>
 __global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const SurfView<double> *va,
                               const SurfView<double> *vb, const RegionRec<TP> *reg1, const RegionRec<TP> *reg2,
                               const int *map1, const int *map2, int nuv1, int nuv2, const DistCand<TP> *top, int n,
@@ -4090,19 +4182,20 @@ __global__ void k_newton_dist(SurfView<double> sa, SurfView<double> sb, const Su
   double d[8];
   for (int q = 0; q < 8; ++q) d[q] = dom[q];
   double o[11];
-  newton_distance(sa, sb, d, x, o);
+  newton_distance<MAXP>(sa, sb, d, x, o);
   for (int q = 0; q < 11; ++q) out[e * 11 + q] = o[q];
 }
 
 // Minimum-norm Gauss-Newton on S1(u, v) - S2(s, t) = 0 (3 equations, 4
 // unknowns): step = -J^T (J J^T)^-1 D.  out: x, y, z, u, v, s, t, residual.
+template <int MAXP>
 __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> &sb, const double dom[8], double x[4],
                              double out[8]) {
   double r1[9], r2[9], D[3];
   double prev = INFINITY;
   for (int it = 0; it < 40; ++it) {
-    point_record1(sa, x[0], x[1], r1);
-    point_record1(sb, x[2], x[3], r2);
+    point_record1<MAXP>(sa, x[0], x[1], r1);
+    point_record1<MAXP>(sb, x[2], x[3], r2);
     for (int c = 0; c < 3; ++c) D[c] = r1[c] - r2[c];
     const double J[3][4] = {{r1[3], r1[6], -r2[3], -r2[6]},
                             {r1[4], r1[7], -r2[4], -r2[7]},
@@ -4126,8 +4219,8 @@ __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> 
     if (dmax <= 1e-15 || (dmax <= 1e-12 && dmax > 0.5 * prev)) break;
     prev = dmax;
   }
-  point_record1(sa, x[0], x[1], r1);
-  point_record1(sb, x[2], x[3], r2);
+  point_record1<MAXP>(sa, x[0], x[1], r1);
+  point_record1<MAXP>(sb, x[2], x[3], r2);
   for (int c = 0; c < 3; ++c) {
     D[c] = r1[c] - r2[c];
     out[c] = 0.5 * (r1[c] + r2[c]);
@@ -4136,7 +4229,7 @@ __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> 
   out[7] = sqrt(dot3(D, D));
 }
 
-template <typename TP>
+template <typename TP, int MAXP>
 __global__ void k_newton_inter(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
                                const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
                                const unsigned long long *keys, long long n, int ij_bits, const double *dom,
@@ -4156,7 +4249,7 @@ __global__ void k_newton_inter(SurfView<double> sa, SurfView<double> sb, const R
   double d[8];
   for (int q = 0; q < 8; ++q) d[q] = dom[q];
   double o[8];
-  newton_point(sa, sb, d, x, o);
+  newton_point<MAXP>(sa, sb, d, x, o);
   for (int q = 0; q < 8; ++q) out[e * 8 + q] = o[q];
 }
 
@@ -4191,7 +4284,7 @@ __global__ void k_surface_prep(const SurfacePrep *jobs) {
 // spacing scale of the points.  out: tx, ty, tz, ok (0 where the normals are
 // parallel or vanish), scale.  pts: 8 doubles per point (x, y, z, u, v, s, t,
 // residual), in the order of the pair keys.
-template <typename TP>
+template <typename TP, int MAXP>
 __global__ void k_curve_tangents(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
                                  const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
                                  const unsigned long long *keys, int ij_bits, const double *pts, long long n,
@@ -4203,8 +4296,8 @@ __global__ void k_curve_tangents(SurfView<double> sa, SurfView<double> sb, const
   const int slot = static_cast<int>(key >> (2 * ij_bits));
   const RegionRec<TP> R1 = reg1[map1[slot]], R2 = reg2[map2[slot]];
   double r1[18], r2[18];
-  point_record(sa, q[3], q[4], r1);
-  point_record(sb, q[5], q[6], r2);
+  point_record<MAXP>(sa, q[3], q[4], r1);
+  point_record<MAXP>(sb, q[5], q[6], r2);
   auto cross = [](const double *a, const double *b, double *c) {
     c[0] = a[1] * b[2] - a[2] * b[1];
     c[1] = a[2] * b[0] - a[0] * b[2];
@@ -4596,8 +4689,13 @@ void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &s
                            cudaStream_t st) {
   counted();
   if (n <= 0) return;
-  k_curve_tangents<double><<<static_cast<unsigned>((n + 127) / 128), 128, 0, st>>>(
-      sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, keys, ij_bits, pts, n, out);
+  const unsigned grid = static_cast<unsigned>((n + 127) / 128);
+  if (newton_maxp(sa, sb) == 9)
+    k_curve_tangents<double, 9><<<grid, 128, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, keys, ij_bits, pts,
+                                                      n, out);
+  else
+    k_curve_tangents<double, kMaxDeg + 1><<<grid, 128, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, keys,
+                                                                ij_bits, pts, n, out);
 }
 
 void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
@@ -4755,8 +4853,14 @@ void launch_newton_dist(const SurfView<double> &sa, const SurfView<double> &sb, 
                         const ScreenStats *stats) {
   counted();
   if (n <= 0) return;
-  k_newton_dist<TP><<<bdim((n + 63) / 64, bt), 64, 0, st>>>(sa, sb, va, vb, reg1, reg2, map1, map2, nuv1, nuv2, top, n,
-                                                            stats, dom, out, bt.qs);
+  // sa / sb carry the largest degrees of a batch (the queries' own views
+  // come from va / vb).
+  if (newton_maxp(sa, sb) == 9)
+    k_newton_dist<TP, 9><<<bdim((n + 63) / 64, bt), 64, 0, st>>>(sa, sb, va, vb, reg1, reg2, map1, map2, nuv1, nuv2,
+                                                                 top, n, stats, dom, out, bt.qs);
+  else
+    k_newton_dist<TP, kMaxDeg + 1><<<bdim((n + 63) / 64, bt), 64, 0, st>>>(sa, sb, va, vb, reg1, reg2, map1, map2,
+                                                                           nuv1, nuv2, top, n, stats, dom, out, bt.qs);
 }
 
 template <typename TP>
@@ -4766,8 +4870,12 @@ void launch_newton_inter(const SurfView<double> &sa, const SurfView<double> &sb,
                          cudaStream_t st) {
   counted();
   if (n <= 0) return;
-  k_newton_inter<TP><<<static_cast<unsigned>((n + 63) / 64), 64, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2,
-                                                                          keys, n, ij_bits, dom, out);
+  const unsigned grid = static_cast<unsigned>((n + 63) / 64);
+  if (newton_maxp(sa, sb) == 9)
+    k_newton_inter<TP, 9><<<grid, 64, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, keys, n, ij_bits, dom, out);
+  else
+    k_newton_inter<TP, kMaxDeg + 1><<<grid, 64, 0, st>>>(sa, sb, reg1, reg2, map1, map2, nuv1, nuv2, keys, n, ij_bits,
+                                                         dom, out);
 }
 
 #define JSI_INSTANTIATE(T)                                                                                        \
