@@ -464,15 +464,56 @@ __device__ void eval_record(const SurfView<T> &s, int spanu, const T *Nu, int sp
   // (k, l) = derivative order in (u, v); record slots P, Pu, Pv, Puu, Puv, Pvv.
   const int ku[6] = {0, 1, 0, 2, 1, 0};
   const int lv[6] = {0, 0, 1, 0, 1, 2};
+  // Factored over the control-net window: each net row is read once and its
+  // u sums for the orders 0..du are formed once, then every derivative
+  // combination takes its v step.  Each combination's sum is the same
+  // operation sequence as contract3 / contract4 (the u sum over the columns
+  // in order, then acc += N_v[r] * row in row order), so the bits are those
+  // of the per-combination contraction.
+  const int nch = s.rat ? 4 : 3;
+  T acc[6][4];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) acc[m][0] = acc[m][1] = acc[m][2] = acc[m][3] = T(0);
+  for (int r = 0; r <= s.degv; ++r) {
+    const Vec4<T> *cp = s.cpw + static_cast<long long>(s.ncpu) * (cv0 + r) + cu0;
+    T row[3][4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) row[k][0] = row[k][1] = row[k][2] = row[k][3] = T(0);
+    for (int c = 0; c <= s.degu; ++c) {
+      const Vec4<T> q = cp[c];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k > s.du) break;
+        if (s.rat) {
+          const T nw = Nu[k * p1 + c] * q.w;
+          row[k][0] += nw * q.x;
+          row[k][1] += nw * q.y;
+          row[k][2] += nw * q.z;
+          row[k][3] += nw;
+        } else {
+          const T n = Nu[k * p1 + c];
+          row[k][0] += n * q.x;
+          row[k][1] += n * q.y;
+          row[k][2] += n * q.z;
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      if (ku[m] > s.du || lv[m] > s.dv) continue;
+      const T mv = Nv[lv[m] * p1 + r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c < nch) acc[m][c] += mv * row[ku[m]][c];
+    }
+  }
   if (!s.rat) {
 #pragma unroll
     for (int m = 0; m < 6; ++m) {
       if (ku[m] > s.du || lv[m] > s.dv) continue;
-      T acc[3];
-      contract3(s, cu0, cv0, Nu + ku[m] * p1, Nv + lv[m] * p1, acc);
-      out[3 * m] = acc[0];
-      out[3 * m + 1] = acc[1];
-      out[3 * m + 2] = acc[2];
+      out[3 * m] = acc[m][0];
+      out[3 * m + 1] = acc[m][1];
+      out[3 * m + 2] = acc[m][2];
     }
     return;
   }
@@ -482,12 +523,10 @@ __device__ void eval_record(const SurfView<T> &s, int spanu, const T *Nu, int sp
 #pragma unroll
   for (int m = 0; m < 6; ++m) {
     if (ku[m] > s.du || lv[m] > s.dv) continue;
-    T acc[4];
-    contract4(s, cu0, cv0, Nu + ku[m] * p1, Nv + lv[m] * p1, acc);
-    h[4 * m] = acc[0];
-    h[4 * m + 1] = acc[1];
-    h[4 * m + 2] = acc[2];
-    h[4 * m + 3] = acc[3];
+    h[4 * m] = acc[m][0];
+    h[4 * m + 1] = acc[m][1];
+    h[4 * m + 2] = acc[m][2];
+    h[4 * m + 3] = acc[m][3];
   }
   quotient2(h);
 #pragma unroll
