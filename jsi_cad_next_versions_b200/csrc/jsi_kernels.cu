@@ -3749,10 +3749,20 @@ constexpr int kWC = kWT * kMaxTile;  // cell columns per warp unit (one per lane
 constexpr int kWS = kWC + 1;         // sample columns per warp unit
 constexpr int kWWarps = 8;           // warps per block
 
+// A warp unit's samples as three coordinate planes (12 B per FP32 sample
+// through shared memory instead of a padded 16 B vector).
 template <typename TC>
 struct BandWarpSmem {
-  Vec4<TC> S[kMaxTile + 1][kWS];
+  TC Sx[kMaxTile + 1][kWS], Sy[kMaxTile + 1][kWS], Sz[kMaxTile + 1][kWS];
   TC coef[kMaxTile + 1][8];
+  __device__ __forceinline__ void put(int a, int col, const Vec4<TC> &P) {
+    Sx[a][col] = P.x;
+    Sy[a][col] = P.y;
+    Sz[a][col] = P.z;
+  }
+  __device__ __forceinline__ Vec4<TC> get(int a, int col) const {
+    return Vec4<TC>{Sx[a][col], Sy[a][col], Sz[a][col], TC(0)};
+  }
 };
 
 template <typename TC>
@@ -3806,7 +3816,7 @@ __device__ __forceinline__ void bandw_column(BandWarpSmem<TC> &w, const SurfView
     TC acc[4] = {TC(0), TC(0), TC(0), TC(0)};
 #pragma unroll
     for (int R = 0; R < NR; ++R) band_v_acc<TB, TC, RAT>(m[R], rs[R], acc);
-    w.S[a][col] = band_point<TB, TC, RAT>(acc);
+    w.put(a, col, band_point<TB, TC, RAT>(acc));
   }
 }
 
@@ -3882,7 +3892,7 @@ __global__ void __launch_bounds__(kWWarps * 32, sizeof(TC) == 8 ? 2 : 4)
         } else {
           P = screen_point(s, bs.spans[lu], Nu, bs.spans[lv], Nv);
         }
-        w.S[a][col] = P;
+        w.put(a, col, P);
       }
     }
     __syncwarp();
@@ -3895,14 +3905,14 @@ __global__ void __launch_bounds__(kWWarps * 32, sizeof(TC) == 8 ? 2 : 4)
     const long long t = static_cast<long long>(r) * g.ntiles + static_cast<long long>(ty) * g.tw + tx;
     if (act) {
       const bool colok = b < min(te, g.W - tx * te);
-      Vec4<TC> p = w.S[0][lane], q = w.S[0][lane + 1];
+      Vec4<TC> p = w.get(0, lane), q = w.get(0, lane + 1);
       TC pmn[3] = {fmn(p.x, q.x), fmn(p.y, q.y), fmn(p.z, q.z)};
       TC pmx[3] = {fmx(p.x, q.x), fmx(p.y, q.y), fmx(p.z, q.z)};
       Vec4<TC> *dst = out.center + t * te2 + b;
 #pragma unroll
       for (int a = 0; a < te; ++a) {
-        p = w.S[a + 1][lane];
-        q = w.S[a + 1][lane + 1];
+        p = w.get(a + 1, lane);
+        q = w.get(a + 1, lane + 1);
         const TC nmn[3] = {fmn(p.x, q.x), fmn(p.y, q.y), fmn(p.z, q.z)};
         const TC nmx[3] = {fmx(p.x, q.x), fmx(p.y, q.y), fmx(p.z, q.z)};
         Vec4<TC> cen{TC(0), TC(0), TC(0), TC(0)};
