@@ -248,6 +248,10 @@ struct Lane {
   Arena arena;
   ScreenStats *d_stats = nullptr;
   ScreenStats *h_stats = nullptr;
+  // Pinned words for the few scalars read back per round (dedup tail counts,
+  // curvature pads): queued behind the kernels and drained by one sync,
+  // instead of one staged pageable copy each.
+  unsigned long long *h_small = nullptr;
   unsigned long long h2d_bytes = 0, d2h_bytes = 0;
   // Optional per-kernel timing: CUDA events recorded on the lane's stream
   // around every launch, resolved at the next host sync.  The lane's thread
@@ -1951,7 +1955,7 @@ void next_regions(Lane *ctx, const unsigned long long *sorted, long long n, int 
   timed(ctx, "inter_side2", [&] {
     launch_inter_side2(key2s, idxs, n, ij_bits, flag2, ex2, B, map2, next2, nmap2, st, cover);
   });
-  unsigned tail[4];
+  unsigned *tail = reinterpret_cast<unsigned *>(ctx->h_small);
   JSI_CUDA(copy_async(ctx, &tail[0], ex1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   JSI_CUDA(copy_async(ctx, &tail[1], flag1 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   JSI_CUDA(copy_async(ctx, &tail[2], ex2 + n - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -2182,7 +2186,7 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
       }
     }
     if (round == 1) {
-      T pads[2];
+      T *pads = reinterpret_cast<T *>(ctx->h_small);
       JSI_CUDA(copy_async(ctx, &pads[0], A.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
       JSI_CUDA(copy_async(ctx, &pads[1], B.pad, sizeof(T), cudaMemcpyDeviceToHost, st));
       JSI_CUDA(cudaStreamSynchronize(st));
@@ -2739,6 +2743,7 @@ void lane_init(Lane &L, int device, size_t block, size_t budget, const std::map<
   JSI_CUDA(cudaEventCreate(&L.ev1));
   JSI_CUDA(cudaMalloc(&L.d_stats, sizeof(ScreenStats)));
   JSI_CUDA(cudaMallocHost(&L.h_stats, sizeof(ScreenStats)));
+  JSI_CUDA(cudaMallocHost(&L.h_small, 8 * sizeof(unsigned long long)));
 }
 
 void lane_free(Lane &L) {
@@ -2752,6 +2757,8 @@ void lane_free(Lane &L) {
   L.event_pool.clear();
   if (L.d_stats) cudaFree(L.d_stats);
   if (L.h_stats) cudaFreeHost(L.h_stats);
+  if (L.h_small) cudaFreeHost(L.h_small);
+  L.h_small = nullptr;
   for (auto &g : L.graphs)
     if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
   L.graphs.clear();

@@ -3750,11 +3750,14 @@ constexpr int kWS = kWC + 1;         // sample columns per warp unit
 constexpr int kWWarps = 8;           // warps per block
 
 // A warp unit's samples as three coordinate planes (12 B per FP32 sample
-// through shared memory instead of a padded 16 B vector).
+// through shared memory instead of a padded 16 B vector).  The v coefficient
+// rows come first and the struct is 16-byte aligned: bandw_column reads each
+// row as a float4 + float2, so every row, in every warp's copy, starts on a
+// 16-byte boundary.
 template <typename TC>
-struct BandWarpSmem {
+struct alignas(16) BandWarpSmem {
+  alignas(16) TC coef[kMaxTile + 1][8];
   TC Sx[kMaxTile + 1][kWS], Sy[kMaxTile + 1][kWS], Sz[kMaxTile + 1][kWS];
-  TC coef[kMaxTile + 1][8];
   __device__ __forceinline__ void put(int a, int col, const Vec4<TC> &P) {
     Sx[a][col] = P.x;
     Sy[a][col] = P.y;
@@ -3764,6 +3767,10 @@ struct BandWarpSmem {
     return Vec4<TC>{Sx[a][col], Sy[a][col], Sz[a][col], TC(0)};
   }
 };
+
+static_assert(sizeof(BandWarpSmem<float>) % 16 == 0 && sizeof(BandWarpSmem<double>) % 16 == 0,
+              "per-warp band staging must keep 16-byte row alignment");
+static_assert((8 * sizeof(float)) % 16 == 0, "coefficient rows must be 16-byte multiples");
 
 template <typename TC>
 constexpr size_t bandw_smem() {
