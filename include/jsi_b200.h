@@ -245,7 +245,10 @@ int jsi_intersect(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const 
  * Rounds stop when ub - lb <= rel_tol * ub or no pair is kept (certified = 1),
  * after max_rounds, or when a round keeps more than max_pairs pairs.  uv1 /
  * uv2 / point1 / point2 are the Newton pair (its distance >= ub).
- * Rational surfaces: JSI_ERR_UNSUPPORTED. */
+ * Rational surfaces (positive weights) take the second-derivative bound of
+ * the quotient A / w (jsi_surface_curvature_bounds) and an evaluation
+ * allowance scaled by 1 / min w; a non-positive weight gives
+ * JSI_ERR_UNSUPPORTED. */
 typedef struct {
   int nuv_refine;      /* samples per direction in a refined cell (default 8) */
   int max_rounds;      /* 1..JSI_MAX_ROUNDS (default 10) */
@@ -266,6 +269,15 @@ typedef struct {
 } jsi_bounds_result;
 
 void jsi_bounds_params_default(jsi_bounds_params *p);
+/* Host only (no device work, no context): per coordinate c, upper bounds
+ * m2u[c] >= max |S_uu[c]| and m2v[c] >= max |S_vv[c]| over the whole surface
+ * (the record as jsi_surface_upload takes it), the pads of the bounds mode.
+ * Non-rational: the second-derivative control nets.  Rational: the same nets
+ * of the homogeneous net (w (P - m), w), m the net's bounding-box centre,
+ * combined through S_uu = (A_uu - 2 w_u S_u - w_uu (S - m)) / w with
+ * |S - m| <= the net's half range and w >= min w.  JSI_ERR_SURFACE for a bad
+ * header or length, JSI_ERR_UNSUPPORTED for a non-positive weight. */
+int jsi_surface_curvature_bounds(const int *ivec, const float *data, int ndata, double *m2u, double *m2v);
 int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_bounds_params *params,
                         jsi_bounds_result *out);
 

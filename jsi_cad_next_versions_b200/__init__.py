@@ -6,6 +6,7 @@ orchestration, include/jsi_b200.h); this package is its Python host mirror.
 """
 from .api import (  # noqa: F401
     Context,
+    curvature_bounds,
     DistanceBatch,
     DistanceResult,
     EvalAndConstructTask,
@@ -26,6 +27,6 @@ from . import synth  # noqa: F401
 
 __all__ = [
     "Context", "DistanceBatch", "DistanceResult", "SurfaceBatch", "TaskBatch", "EvalAndConstructTask", "IntersectionResult", "JsiError", "ONE_UV_SIZE",
-    "default_global_dist_nuv", "default_global_intersect_nuv", "deinit_cad", "evalWithCuda", "init_cad",
+    "curvature_bounds", "default_global_dist_nuv", "default_global_intersect_nuv", "deinit_cad", "evalWithCuda", "init_cad",
     "intersection", "minimum_distance", "synth",
 ]

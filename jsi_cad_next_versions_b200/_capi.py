@@ -32,7 +32,7 @@ EXPORTED = [
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_units", "jsi_kernel_names",
     "jsi_dist_params_default",
     "jsi_min_distance", "jsi_inter_params_default", "jsi_intersect", "jsi_bounds_params_default",
-    "jsi_distance_bounds", "jsi_curve_params_default", "jsi_intersection_curves", "jsi_eval_grid", "jsi_eval_grid_f64",
+    "jsi_distance_bounds", "jsi_surface_curvature_bounds", "jsi_curve_params_default", "jsi_intersection_curves", "jsi_eval_grid", "jsi_eval_grid_f64",
     "jsi_eval_grid_noalloc", "jsi_workers", "jsi_submit_distance", "jsi_submit_intersect", "jsi_wait",
     "jsi_queue_depth", "jsi_min_distance_batch", "jsi_submit_distance_batch", "jsi_wait_distance_batch", "jsi_batch_chunk", "jsi_batch_reruns", "jsi_batch_graphs", "jsi_autotune_batch",
     "jsi_query_batch", "jsi_poll_distance_batch",
@@ -226,6 +226,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_eval_grid_noalloc.argtypes = [P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                         I, P]
     L.jsi_eval_grid_noalloc.restype = I
+    L.jsi_surface_curvature_bounds.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.jsi_surface_curvature_bounds.restype = I
     if path is None:
         _lib = L
     return L

@@ -2324,51 +2324,114 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
 // Certified distance interval (bounds mode)
 // ---------------------------------------------------------------------------
 
-// Per coordinate c, max |S_uu[c]| and max |S_vv[c]| over a non-rational surface: the
-// second-derivative control nets (derivative control points, applied twice
-// per direction: Q_i = p (P_{i+1} - P_i) / (U_{i+p+1} - U_{i+1}),
-// R_i = (p - 1)(Q_{i+1} - Q_i) / (U_{i+p+1} - U_{i+2}); a zero knot span
-// gives a zero term) bound the second derivatives by the convex hull
-// property.  Widened by 1e-12 for the double arithmetic.
-void second_derivative_bounds(Lane *L, const SurfaceRec &s, double m2u[3], double m2v[3]) {
-  const int p = s.ivec[1], nu = s.ivec[2], nku = s.ivec[3], q = s.ivec[4], nv = s.ivec[5], nkv = s.ivec[6];
+// Per coordinate c, bounds on |S_uu[c]| and |S_vv[c]| over a surface, from
+// the raw record (knots U, knots V, control points, weights if rational).
+//
+// Non-rational: the second-derivative control nets (derivative control
+// points applied twice per direction: Q_i = p (P_{i+1} - P_i) /
+// (U_{i+p+1} - U_{i+1}), R_i = (p - 1)(Q_{i+1} - Q_i) / (U_{i+p+1} -
+// U_{i+2}); a zero knot span gives a zero term) bound the second
+// derivatives by the convex hull property.
+//
+// Rational (positive weights): S = A / w with A = sum N_i N_j w_ij (P_ij - m)
+// + m w, m the centre of the control net's bounding box.  Differentiating
+// (S - m) w = A' twice along u gives
+//   S_u  = (A'_u - w_u (S - m)) / w,
+//   S_uu = (A'_uu - 2 w_u S_u - w_uu (S - m)) / w,
+// and with |S - m| <= h (the net's half range: S lies in the net's convex
+// hull), w >= min w_ij, and the derivative nets of the homogeneous net
+// (w (P - m), w) bounding A'_u, A'_uu, w_u, w_uu, every term is bounded.
+// Each net entry carries a magnitude (the same recurrence on absolute
+// values), and 1e-14 of it (about 45 units in the last place) covers the
+// double rounding of the differences; the results are widened by 1e-12.
+void second_derivative_bounds_host(const int ivec[7], const float *data, double m2u[3], double m2v[3]) {
+  const int p = ivec[1], nu = ivec[2], nku = ivec[3], q = ivec[4], nv = ivec[5], nkv = ivec[6];
+  const bool rat = (ivec[0] & 2) != 0;
   const size_t ncp = static_cast<size_t>(nu) * nv;
-  std::vector<float> raw(nku + nkv + 3 * ncp);
-  JSI_CUDA(copy_async(L, raw.data(), s.U32, raw.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
-  JSI_CUDA(cudaStreamSynchronize(L->stream));
-  const float *U = raw.data(), *V = U + nku, *P = V + nkv;  // P[(j * nu + i) * 3 + c], u fastest
-  auto line_bound = [](const std::vector<double> &pts, const float *K, int deg, int n, double m[3]) {
-    // pts: n points x 3 along one parameter direction
-    if (deg < 2 || n < 3) return;
-    std::vector<double> Q(3 * (n - 1));
+  const float *U = data, *V = U + nku, *P = V + nkv;  // P[(j * nu + i) * 3 + c], u fastest
+  const float *W = rat ? P + 3 * ncp : nullptr;
+  constexpr int kC = 4;
+  double mid[3] = {0.0, 0.0, 0.0}, half[3] = {0.0, 0.0, 0.0}, wmin = 1.0;
+  if (rat) {
+    for (int c = 0; c < 3; ++c) {
+      float lo = P[c], hi = P[c];
+      for (size_t k = 0; k < ncp; ++k) {
+        lo = std::min(lo, P[3 * k + c]);
+        hi = std::max(hi, P[3 * k + c]);
+      }
+      mid[c] = 0.5 * (static_cast<double>(lo) + static_cast<double>(hi));  // exact
+      half[c] = 0.5 * (static_cast<double>(hi) - static_cast<double>(lo));  // exact
+    }
+    wmin = W[0];
+    for (size_t k = 0; k < ncp; ++k) wmin = std::min(wmin, static_cast<double>(W[k]));
+  }
+  // One homogeneous net entry (w (P - m), w) and its magnitude.
+  auto entry = [&](size_t k, double h[kC], double a[kC]) {
+    const double w = rat ? static_cast<double>(W[k]) : 1.0;
+    for (int c = 0; c < 3; ++c) {
+      h[c] = rat ? w * (static_cast<double>(P[3 * k + c]) - mid[c]) : static_cast<double>(P[3 * k + c]);
+      a[c] = std::fabs(h[c]);
+    }
+    h[3] = w;
+    a[3] = std::fabs(w);
+  };
+  // m1 / m2: max |first / second derivative net entry| + its rounding slack.
+  auto line_bound = [](const std::vector<double> &h, const std::vector<double> &a, const float *K, int deg, int n,
+                       double m1[kC], double m2[kC]) {
+    if (deg < 1 || n < 2) return;
+    std::vector<double> Q(kC * (n - 1)), QA(kC * (n - 1));
     for (int i = 0; i < n - 1; ++i) {
       const double den = static_cast<double>(K[i + deg + 1]) - K[i + 1];
-      for (int c = 0; c < 3; ++c) Q[3 * i + c] = den != 0.0 ? deg * (pts[3 * (i + 1) + c] - pts[3 * i + c]) / den : 0.0;
+      for (int c = 0; c < kC; ++c) {
+        Q[kC * i + c] = den != 0.0 ? deg * (h[kC * (i + 1) + c] - h[kC * i + c]) / den : 0.0;
+        QA[kC * i + c] = den != 0.0 ? deg * (a[kC * (i + 1) + c] + a[kC * i + c]) / std::fabs(den) : 0.0;
+        m1[c] = std::max(m1[c], std::fabs(Q[kC * i + c]) + 1e-14 * QA[kC * i + c]);
+      }
     }
+    if (deg < 2 || n < 3) return;
     for (int i = 0; i < n - 2; ++i) {
       const double den = static_cast<double>(K[i + deg + 1]) - K[i + 2];
       if (den == 0.0) continue;
-      for (int c = 0; c < 3; ++c) m[c] = std::max(m[c], std::fabs((deg - 1) * (Q[3 * (i + 1) + c] - Q[3 * i + c]) / den));
+      for (int c = 0; c < kC; ++c) {
+        const double r = (deg - 1) * (Q[kC * (i + 1) + c] - Q[kC * i + c]) / den;
+        const double ra = (deg - 1) * (QA[kC * (i + 1) + c] + QA[kC * i + c]) / std::fabs(den);
+        m2[c] = std::max(m2[c], std::fabs(r) + 1e-14 * ra);
+      }
     }
   };
-  double mu[3] = {0.0, 0.0, 0.0}, mv[3] = {0.0, 0.0, 0.0};
-  std::vector<double> line;
+  double m1u[kC] = {0, 0, 0, 0}, m2u_[kC] = {0, 0, 0, 0}, m1v[kC] = {0, 0, 0, 0}, m2v_[kC] = {0, 0, 0, 0};
+  std::vector<double> h, a;
   for (int j = 0; j < nv; ++j) {
-    line.assign(3 * nu, 0.0);
-    for (int i = 0; i < nu; ++i)
-      for (int c = 0; c < 3; ++c) line[3 * i + c] = P[(static_cast<size_t>(j) * nu + i) * 3 + c];
-    line_bound(line, U, p, nu, mu);
+    h.assign(kC * nu, 0.0);
+    a.assign(kC * nu, 0.0);
+    for (int i = 0; i < nu; ++i) entry(static_cast<size_t>(j) * nu + i, &h[kC * i], &a[kC * i]);
+    line_bound(h, a, U, p, nu, m1u, m2u_);
   }
   for (int i = 0; i < nu; ++i) {
-    line.assign(3 * nv, 0.0);
-    for (int j = 0; j < nv; ++j)
-      for (int c = 0; c < 3; ++c) line[3 * j + c] = P[(static_cast<size_t>(j) * nu + i) * 3 + c];
-    line_bound(line, V, q, nv, mv);
+    h.assign(kC * nv, 0.0);
+    a.assign(kC * nv, 0.0);
+    for (int j = 0; j < nv; ++j) entry(static_cast<size_t>(j) * nu + i, &h[kC * j], &a[kC * j]);
+    line_bound(h, a, V, q, nv, m1v, m2v_);
   }
   for (int c = 0; c < 3; ++c) {
-    m2u[c] = mu[c] * (1.0 + 1e-12);
-    m2v[c] = mv[c] * (1.0 + 1e-12);
+    double bu = m2u_[c], bv = m2v_[c];
+    if (rat) {
+      const double s1u = (m1u[c] + m1u[3] * half[c]) / wmin, s1v = (m1v[c] + m1v[3] * half[c]) / wmin;
+      bu = (m2u_[c] + 2.0 * m1u[3] * s1u + m2u_[3] * half[c]) / wmin;
+      bv = (m2v_[c] + 2.0 * m1v[3] * s1v + m2v_[3] * half[c]) / wmin;
+    }
+    m2u[c] = bu * (1.0 + 1e-12);
+    m2v[c] = bv * (1.0 + 1e-12);
   }
+}
+
+// The same bounds for a resident surface (its raw record read back).
+void second_derivative_bounds(Lane *L, const SurfaceRec &s, double m2u[3], double m2v[3]) {
+  const size_t ncp = static_cast<size_t>(s.ivec[2]) * s.ivec[5];
+  std::vector<float> raw(static_cast<size_t>(s.ivec[3]) + s.ivec[6] + (s.rat ? 4 : 3) * ncp);
+  JSI_CUDA(copy_async(L, raw.data(), s.U32, raw.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
+  JSI_CUDA(cudaStreamSynchronize(L->stream));
+  second_derivative_bounds_host(s.ivec, raw.data(), m2u, m2v);
 }
 
 // Allowance for the FP64 evaluation of a surface point and for the centre /
@@ -2377,6 +2440,14 @@ void second_derivative_bounds(Lane *L, const SurfaceRec &s, double m2u[3], doubl
 // terms bounded by it, the basis being a partition of unity); 2^-40 of it is
 // a 32x margin.
 double eval_allowance(const SurfaceRec &s) {
+  if (s.rat) {
+    // Rational: the homogeneous sums' rounding stays below 2^-45 of
+    // max |w P| (coordinates) and of max w (weight); the quotient's error is
+    // at most (e_A + |S| e_w) / w with w >= min w and |S| <= max |P|.
+    const double c = std::max(s.cmax[0], std::max(s.cmax[1], s.cmax[2]));
+    const double m = std::max(s.wcmax[0], std::max(s.wcmax[1], s.wcmax[2])) + c * s.wmax;
+    return std::ldexp(m / s.wmin, -40);
+  }
   return std::ldexp(std::max(s.cmax[0], std::max(s.cmax[1], s.cmax[2])), -40);
 }
 
@@ -2386,7 +2457,8 @@ void run_bounds(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_bou
   cudaStream_t st = ctx->stream;
   const SurfaceRec &sa = get_surface(ctx, ta->surface);
   const SurfaceRec &sb = get_surface(ctx, tb->surface);
-  if (sa.rat || sb.rat) fail(JSI_ERR_UNSUPPORTED, "the bounds mode needs non-rational surfaces");
+  if ((sa.rat && !(sa.wmin > 0)) || (sb.rat && !(sb.wmin > 0)))
+    fail(JSI_ERR_UNSUPPORTED, "the bounds mode needs positive weights");
   if (sa.zero || sb.zero) fail(JSI_ERR_UNSUPPORTED, "the bounds mode needs surfaces that evaluate");
   // Upper bound: two surface points from the FP64 query with Newton.
   jsi_dist_params dp;
@@ -3364,6 +3436,22 @@ void jsi_bounds_params_default(jsi_bounds_params *p) {
   p->max_rounds = 10;
   p->rel_tol = 1e-6;
   p->max_pairs = 1ll << 22;
+}
+
+int jsi_surface_curvature_bounds(const int *ivec, const float *data, int ndata, double *m2u, double *m2v) {
+  if (!ivec || !data || !m2u || !m2v) return JSI_ERR_INVALID;
+  try {
+    check_surface(ivec, data, ndata);
+    SurfaceRec s;
+    surface_header(s, ivec, data);
+    if (s.rat && !(s.wmin > 0)) return JSI_ERR_UNSUPPORTED;
+    second_derivative_bounds_host(ivec, data, m2u, m2v);
+    return JSI_OK;
+  } catch (const StatusError &e) {
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    return JSI_ERR_NOMEM;
+  }
 }
 
 int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_bounds_params *params,

@@ -66,17 +66,23 @@ def test_bounds_sine_pair(gpu_ctx, orc, seeds):
     assert abs(fp64.newton_distance - r.ub) <= 1e-9 * r.ub
 
 
-def test_bounds_random_surfaces(gpu_ctx, orc):
-    rng = synth.SplitMix64(515)
+@pytest.mark.parametrize("want_rational", [False, True])
+def test_bounds_random_surfaces(gpu_ctx, orc, want_rational):
+    """Random pairs of degree 1-5; the rational case takes pairs with at
+    least one rational surface (the quotient-rule curvature bound and the
+    weight-scaled evaluation allowance)."""
+    rng = synth.SplitMix64(515 if not want_rational else 616)
     done = 0
     while done < 3:
         A, B = synth.random_surface(rng), synth.random_surface(rng)
-        if int(A.ivec[0]) & 2 or int(B.ivec[0]) & 2:
-            continue  # rational: not supported by the bounds mode
+        rat = bool(int(A.ivec[0]) & 2 or int(B.ivec[0]) & 2)
+        if rat != want_rational:
+            continue
         ta, tb = _tasks(gpu_ctx, A, B, 32)
         r = gpu_ctx.distance_bounds(ta, tb, max_rounds=8)
         assert 0.0 <= r.lb <= r.ub
         assert r.lb <= _dense_min(orc, A, B, n=64)
+        assert np.all(np.diff(r.lb_round) >= 0)
         done += 1
 
 
@@ -90,9 +96,44 @@ def test_bounds_hard_wave_full_size(gpu_ctx):
     assert np.all(np.diff(r.lb_round) >= 0)
 
 
-def test_bounds_rejects_rational(gpu_ctx):
-    import jsi_cad_next_versions_b200 as J
+def test_bounds_rational_saddle_plane(gpu_ctx, orc):
+    """The rational intersection pair: the surfaces cross, so the minimum
+    distance is 0 and the interval must close onto it from above."""
     C, D, _ = synth.intersection_pair_saddle_plane()
-    ta, tb = _tasks(gpu_ctx, C, D, 16)
+    ta, tb = _tasks(gpu_ctx, C, D, 32)
+    r = gpu_ctx.distance_bounds(ta, tb, max_rounds=4)
+    assert 0.0 <= r.lb <= r.ub
+    assert r.lb <= _dense_min(orc, C, D, n=64)
+    assert r.ub < 1e-3
+
+
+def test_bounds_rational_separated_pair(gpu_ctx, orc):
+    """A rational sine pair (seeded weights in [0.5, 2] on both nets) held
+    apart: the interval certifies and brackets the dense sample minimum."""
+    A0, B0, _ = synth.distance_pair_sine()
+    out = []
+    for k, s in enumerate((A0, B0)):
+        cp, _ = s.control_net()
+        w = synth.SplitMix64(900 + k).uniform(cp.shape[0] * cp.shape[1], 0.5, 2.0)
+        out.append(synth.make_surface(cp.astype(np.float64), int(s.ivec[1]), int(s.ivec[4]),
+                                      weights=w.reshape(cp.shape[0], cp.shape[1])))
+    A, B = out
+    ta, tb = _tasks(gpu_ctx, A, B, 64)
+    r = gpu_ctx.distance_bounds(ta, tb, rel_tol=1e-6)
+    dense = _dense_min(orc, A, B)
+    assert 0.0 < r.lb <= r.ub
+    assert r.lb <= dense
+    assert r.ub <= dense * (1 + 1e-9) + 1e-12
+    assert r.certified, (r.lb, r.ub, r.kept)
+
+
+def test_bounds_rejects_nonpositive_weight(gpu_ctx):
+    import jsi_cad_next_versions_b200 as J
+    A0, _, _ = synth.distance_pair_sine()
+    cp, _ = A0.control_net()
+    w = np.ones(cp.shape[:2])
+    w[1, 1] = 0.0
+    A = synth.make_surface(cp.astype(np.float64), int(A0.ivec[1]), int(A0.ivec[4]), weights=w)
+    ta, tb = _tasks(gpu_ctx, A, A0, 16)
     with pytest.raises(J.JsiError):
         gpu_ctx.distance_bounds(ta, tb)
