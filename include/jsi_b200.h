@@ -270,14 +270,21 @@ typedef struct {
 
 void jsi_bounds_params_default(jsi_bounds_params *p);
 /* Host only (no device work, no context): per coordinate c, upper bounds
- * m2u[c] >= max |S_uu[c]| and m2v[c] >= max |S_vv[c]| over the whole surface
- * (the record as jsi_surface_upload takes it), the pads of the bounds mode.
- * Non-rational: the second-derivative control nets.  Rational: the same nets
- * of the homogeneous net (w (P - m), w), m the net's bounding-box centre,
- * combined through S_uu = (A_uu - 2 w_u S_u - w_uu (S - m)) / w with
- * |S - m| <= the net's half range and w >= min w.  JSI_ERR_SURFACE for a bad
- * header or length, JSI_ERR_UNSUPPORTED for a non-positive weight. */
-int jsi_surface_curvature_bounds(const int *ivec, const float *data, int ndata, double *m2u, double *m2v);
+ * m2u[c] >= |S_uu[c]| and m2v[c] >= |S_vv[c]| (the record as
+ * jsi_surface_upload takes it), the pads of the bounds mode.  rect = NULL:
+ * over the whole surface.  rect = {u0, v0, u1, v1}: over that parameter
+ * rectangle, as the bounds mode pads a region, the largest of the per-knot-
+ * span bounds (each from that span's own control points) over the spans it
+ * touches.  Non-rational: the second-derivative control nets.  Rational: the
+ * same nets of the homogeneous net (w (P - m), w), m the net's bounding-box
+ * centre, combined through S_uu = (A_uu - 2 w_u S_u - w_uu (S - m)) / w with
+ * |S - m| <= the net's half range and w >= min w.  Within a span the bound
+ * holds everywhere; across a knot where the surface is only C0 S_uu does not
+ * exist there (the bounds mode cuts its rectangles at such knots).
+ * JSI_ERR_SURFACE for a bad header or length, JSI_ERR_UNSUPPORTED for a
+ * non-positive weight. */
+int jsi_surface_curvature_bounds(const int *ivec, const float *data, int ndata, const double *rect, double *m2u,
+                                 double *m2v);
 int jsi_distance_bounds(jsi_context *ctx, const jsi_task *a, const jsi_task *b, const jsi_bounds_params *params,
                         jsi_bounds_result *out);
 

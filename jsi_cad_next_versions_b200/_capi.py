@@ -226,7 +226,8 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_eval_grid_noalloc.argtypes = [P, P, I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                         I, P]
     L.jsi_eval_grid_noalloc.restype = I
-    L.jsi_surface_curvature_bounds.argtypes = [P, P, I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.jsi_surface_curvature_bounds.argtypes = [P, P, I, P, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_double)]
     L.jsi_surface_curvature_bounds.restype = I
     if path is None:
         _lib = L

@@ -711,16 +711,18 @@ class Context:
         return out
 
 
-def curvature_bounds(surface=None, *, ivec=None, data=None) -> tuple[np.ndarray, np.ndarray]:
+def curvature_bounds(surface=None, *, ivec=None, data=None, rect=None) -> tuple[np.ndarray, np.ndarray]:
     """Per-coordinate bounds (m2u, m2v) on |S_uu| and |S_vv| over the whole
-    surface, the pads of the bounds mode (host only: no device, no context)."""
+    surface, or over the parameter rectangle ``rect`` = (u0, v0, u1, v1) as
+    the bounds mode pads a region (host only: no device, no context)."""
     if surface is not None:
         ivec, data = surface.ivec, surface.data
     iv = np.ascontiguousarray(ivec, dtype=np.int32)
     da = np.ascontiguousarray(data, dtype=np.float32)
     mu = np.zeros(3, np.float64)
     mv = np.zeros(3, np.float64)
-    st = C.load().jsi_surface_curvature_bounds(_p(iv), _p(da), int(da.shape[0]),
+    rc = None if rect is None else np.ascontiguousarray(rect, dtype=np.float64)
+    st = C.load().jsi_surface_curvature_bounds(_p(iv), _p(da), int(da.shape[0]), None if rc is None else _p(rc),
                                                mu.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                mv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     if st != C.JSI_OK:

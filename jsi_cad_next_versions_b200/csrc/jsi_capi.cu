@@ -2344,26 +2344,37 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
 // Each net entry carries a magnitude (the same recurrence on absolute
 // values), and 1e-14 of it (about 45 units in the last place) covers the
 // double rounding of the differences; the results are widened by 1e-12.
-void second_derivative_bounds_host(const int ivec[7], const float *data, double m2u[3], double m2v[3]) {
+//
+// Over control points i0..i1 (u) x j0..j1 (v) only, the bounds hold on the
+// knot spans those points alone define: a span (su, sv) takes
+// [su - p, su] x [sv - q, sv] (on it the u derivative nets that do not vanish
+// are Q_{su-p..su-1} and R_{su-p..su-2}, which read only those points, and
+// S lies in their convex hull).
+void second_derivative_bounds_range(const int ivec[7], const float *data, int i0, int i1, int j0, int j1,
+                                    double m2u[3], double m2v[3]) {
   const int p = ivec[1], nu = ivec[2], nku = ivec[3], q = ivec[4], nv = ivec[5], nkv = ivec[6];
   const bool rat = (ivec[0] & 2) != 0;
   const size_t ncp = static_cast<size_t>(nu) * nv;
   const float *U = data, *V = U + nku, *P = V + nkv;  // P[(j * nu + i) * 3 + c], u fastest
   const float *W = rat ? P + 3 * ncp : nullptr;
+  const int lu = i1 - i0 + 1, lv = j1 - j0 + 1;
+  auto at = [&](int i, int j) { return static_cast<size_t>(j0 + j) * nu + (i0 + i); };
   constexpr int kC = 4;
   double mid[3] = {0.0, 0.0, 0.0}, half[3] = {0.0, 0.0, 0.0}, wmin = 1.0;
   if (rat) {
     for (int c = 0; c < 3; ++c) {
-      float lo = P[c], hi = P[c];
-      for (size_t k = 0; k < ncp; ++k) {
-        lo = std::min(lo, P[3 * k + c]);
-        hi = std::max(hi, P[3 * k + c]);
-      }
+      float lo = P[3 * at(0, 0) + c], hi = lo;
+      for (int j = 0; j < lv; ++j)
+        for (int i = 0; i < lu; ++i) {
+          lo = std::min(lo, P[3 * at(i, j) + c]);
+          hi = std::max(hi, P[3 * at(i, j) + c]);
+        }
       mid[c] = 0.5 * (static_cast<double>(lo) + static_cast<double>(hi));  // exact
       half[c] = 0.5 * (static_cast<double>(hi) - static_cast<double>(lo));  // exact
     }
-    wmin = W[0];
-    for (size_t k = 0; k < ncp; ++k) wmin = std::min(wmin, static_cast<double>(W[k]));
+    wmin = W[at(0, 0)];
+    for (int j = 0; j < lv; ++j)
+      for (int i = 0; i < lu; ++i) wmin = std::min(wmin, static_cast<double>(W[at(i, j)]));
   }
   // One homogeneous net entry (w (P - m), w) and its magnitude.
   auto entry = [&](size_t k, double h[kC], double a[kC]) {
@@ -2401,17 +2412,17 @@ void second_derivative_bounds_host(const int ivec[7], const float *data, double 
   };
   double m1u[kC] = {0, 0, 0, 0}, m2u_[kC] = {0, 0, 0, 0}, m1v[kC] = {0, 0, 0, 0}, m2v_[kC] = {0, 0, 0, 0};
   std::vector<double> h, a;
-  for (int j = 0; j < nv; ++j) {
-    h.assign(kC * nu, 0.0);
-    a.assign(kC * nu, 0.0);
-    for (int i = 0; i < nu; ++i) entry(static_cast<size_t>(j) * nu + i, &h[kC * i], &a[kC * i]);
-    line_bound(h, a, U, p, nu, m1u, m2u_);
+  for (int j = 0; j < lv; ++j) {
+    h.assign(kC * lu, 0.0);
+    a.assign(kC * lu, 0.0);
+    for (int i = 0; i < lu; ++i) entry(at(i, j), &h[kC * i], &a[kC * i]);
+    line_bound(h, a, U + i0, p, lu, m1u, m2u_);
   }
-  for (int i = 0; i < nu; ++i) {
-    h.assign(kC * nv, 0.0);
-    a.assign(kC * nv, 0.0);
-    for (int j = 0; j < nv; ++j) entry(static_cast<size_t>(j) * nu + i, &h[kC * j], &a[kC * j]);
-    line_bound(h, a, V, q, nv, m1v, m2v_);
+  for (int i = 0; i < lu; ++i) {
+    h.assign(kC * lv, 0.0);
+    a.assign(kC * lv, 0.0);
+    for (int j = 0; j < lv; ++j) entry(at(i, j), &h[kC * j], &a[kC * j]);
+    line_bound(h, a, V + j0, q, lv, m1v, m2v_);
   }
   for (int c = 0; c < 3; ++c) {
     double bu = m2u_[c], bv = m2v_[c];
@@ -2425,13 +2436,62 @@ void second_derivative_bounds_host(const int ivec[7], const float *data, double 
   }
 }
 
-// The same bounds for a resident surface (its raw record read back).
-void second_derivative_bounds(Lane *L, const SurfaceRec &s, double m2u[3], double m2v[3]) {
+void second_derivative_bounds_host(const int ivec[7], const float *data, double m2u[3], double m2v[3]) {
+  second_derivative_bounds_range(ivec, data, 0, ivec[2] - 1, 0, ivec[5] - 1, m2u, m2v);
+}
+
+// A resident surface's raw record read back.
+std::vector<float> raw_record(Lane *L, const SurfaceRec &s) {
   const size_t ncp = static_cast<size_t>(s.ivec[2]) * s.ivec[5];
   std::vector<float> raw(static_cast<size_t>(s.ivec[3]) + s.ivec[6] + (s.rat ? 4 : 3) * ncp);
   JSI_CUDA(copy_async(L, raw.data(), s.U32, raw.size() * sizeof(float), cudaMemcpyDeviceToHost, L->stream));
   JSI_CUDA(cudaStreamSynchronize(L->stream));
-  second_derivative_bounds_host(s.ivec, raw.data(), m2u, m2v);
+  return raw;
+}
+
+// Per knot span (su, sv), su in [p, ncpu - 1], sv in [q, ncpv - 1]: the
+// bounds over that span's own control points, as two Vec4 rows (m2u, m2v)
+// at index (sv - q) * (ncpu - p) + (su - p); zero for an empty span.
+std::vector<Vec4<double>> span_curvature_table(const int ivec[7], const float *data) {
+  const int p = ivec[1], nu = ivec[2], nku = ivec[3], q = ivec[4], nv = ivec[5];
+  const float *U = data, *V = data + nku;
+  const int nsu = nu - p, nsv = nv - q;
+  if (static_cast<long long>(nsu) * nsv > (1ll << 20)) fail(JSI_ERR_CAPACITY, "%d x %d knot spans", nsu, nsv);
+  std::vector<Vec4<double>> tab(2 * static_cast<size_t>(nsu) * nsv, Vec4<double>{0, 0, 0, 0});
+  for (int sv = q; sv < nv; ++sv)
+    for (int su = p; su < nu; ++su) {
+      if (!(U[su + 1] > U[su]) || !(V[sv + 1] > V[sv])) continue;
+      double mu[3], mv[3];
+      second_derivative_bounds_range(ivec, data, su - p, su, sv - q, sv, mu, mv);
+      const size_t k = 2 * (static_cast<size_t>(sv - q) * nsu + (su - p));
+      tab[k] = Vec4<double>{mu[0], mu[1], mu[2], 0.0};
+      tab[k + 1] = Vec4<double>{mv[0], mv[1], mv[2], 0.0};
+    }
+  return tab;
+}
+
+// Breakpoints of one parameter direction of a task rectangle [a, b] for the
+// bounds mode's first round: every distinct interior knot where the surface
+// may be only C0 (multiplicity >= the degree; every knot at degree 1), so
+// that no cell straddles a kink, plus every g-th other knot, g chosen to
+// keep the pieces near 16.
+std::vector<double> knot_pieces(const float *K, int nk, int deg, double a, double b) {
+  std::vector<std::pair<double, int>> in;  // distinct interior knots and their multiplicities
+  for (int k = 0; k < nk; ++k) {
+    const double x = K[k];
+    if (!(x > a && x < b)) continue;
+    if (!in.empty() && in.back().first == x) ++in.back().second;
+    else in.push_back({x, 1});
+  }
+  const size_t g = std::max<size_t>(1, (in.size() + 1 + 15) / 16);
+  std::vector<double> cuts{a};
+  for (size_t k = 0; k < in.size(); ++k)
+    if (in[k].second >= std::max(deg, 1) || (k + 1) % g == 0) cuts.push_back(in[k].first);
+  cuts.push_back(b);
+  std::sort(cuts.begin(), cuts.end());
+  cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+  if (cuts.size() - 1 > 64) fail(JSI_ERR_UNSUPPORTED, "more than 64 C0 pieces in one direction");
+  return cuts;
 }
 
 // Allowance for the FP64 evaluation of a surface point and for the centre /
@@ -2487,28 +2547,54 @@ void run_bounds(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_bou
   // with it the prune level) drops each round to the closest corner-sample
   // pair seen.
   const double allowance = std::sqrt(3.0) * 1.000001 * (ea + eb);
-  double m2[2][2][3];
-  second_derivative_bounds(ctx, sa, m2[0][0], m2[0][1]);
-  second_derivative_bounds(ctx, sb, m2[1][0], m2[1][1]);
+  // Curvature bounds per knot span (each span's own control points), looked
+  // up per region by the pad kernel.
+  const std::vector<float> rawa = raw_record(ctx, sa), rawb = raw_record(ctx, sb);
+  const std::vector<Vec4<double>> taba = span_curvature_table(sa.ivec, rawa.data());
+  const std::vector<Vec4<double>> tabb = span_curvature_table(sb.ivec, rawb.data());
+  Vec4<double> *dtab[2] = {ar.get<Vec4<double>>(taba.size()), ar.get<Vec4<double>>(tabb.size())};
+  JSI_CUDA(copy_async(ctx, dtab[0], taba.data(), taba.size() * sizeof(Vec4<double>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dtab[1], tabb.data(), tabb.size() * sizeof(Vec4<double>), cudaMemcpyHostToDevice, st));
   const SurfView<double> va = view<double>(sa), vb = view<double>(sb);
 
-  RegionRec<double> roots[2] = {{ta->ustart, ta->vstart, ta->ustop, ta->vstop},
-                                {tb->ustart, tb->vstart, tb->ustop, tb->vstop}};
-  RegionRec<double> *dreg = ar.get<RegionRec<double>>(2);
-  int *dmap = ar.get<int>(2);
-  const int zeros[2] = {0, 0};
-  JSI_CUDA(copy_async(ctx, dreg, roots, sizeof(roots), cudaMemcpyHostToDevice, st));
-  JSI_CUDA(copy_async(ctx, dmap, zeros, sizeof(zeros), cudaMemcpyHostToDevice, st));
+  // First round: each rectangle cut at its knots into pieces (every C0 knot,
+  // the others thinned to about 16 pieces per direction), the first-round
+  // width shared out over the pieces, and every piece of one side paired with
+  // every piece of the other.  No cell then straddles a kink, and each
+  // piece's pads come from its own spans.
+  auto pieces = [&](const std::vector<float> &raw, const SurfaceRec &s, const jsi_task *t,
+                    std::vector<RegionRec<double>> &out) {
+    const float *U = raw.data(), *V = U + s.ivec[3];
+    const std::vector<double> cu = knot_pieces(U, s.ivec[3], s.ivec[1], t->ustart, t->ustop);
+    const std::vector<double> cv = knot_pieces(V, s.ivec[6], s.ivec[4], t->vstart, t->vstop);
+    for (size_t j = 0; j + 1 < cv.size(); ++j)
+      for (size_t i = 0; i + 1 < cu.size(); ++i) out.push_back({cu[i], cv[j], cu[i + 1], cv[j + 1]});
+    const int np = static_cast<int>(std::max(cu.size(), cv.size()) - 1);
+    return std::max(3, (t->nuv - 1 + np - 1) / np + 1);
+  };
+  std::vector<RegionRec<double>> ra, rb;
+  const int nuva = pieces(rawa, sa, ta, ra), nuvb = pieces(rawb, sb, tb, rb);
+  const long long na = static_cast<long long>(ra.size()), nb = static_cast<long long>(rb.size());
+  long long nslots = na * nb;
+  std::vector<int> hmap(2 * nslots);
+  for (long long k = 0; k < nslots; ++k) {
+    hmap[k] = static_cast<int>(k / nb);
+    hmap[nslots + k] = static_cast<int>(k % nb);
+  }
+  RegionRec<double> *dreg = ar.get<RegionRec<double>>(na + nb);
+  int *dmap = ar.get<int>(2 * nslots);
+  JSI_CUDA(copy_async(ctx, dreg, ra.data(), na * sizeof(RegionRec<double>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dreg + na, rb.data(), nb * sizeof(RegionRec<double>), cudaMemcpyHostToDevice, st));
+  JSI_CUDA(copy_async(ctx, dmap, hmap.data(), hmap.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   // Per-coordinate pads: a Vec4 per region in place of the scalar.
   auto bounds_side = [&](const Geom &g, int nreg, RegionRec<double> *regions) {
     SideRound<double> S = make_side<double>(ar, g, nreg, true, regions);
     S.pad = ar.get<double>(static_cast<size_t>(nreg) * 4);
     return S;
   };
-  SideRound<double> A = bounds_side(make_geom(ta->nuv, p1_of(sa)), 1, dreg);
-  SideRound<double> B = bounds_side(make_geom(tb->nuv, p1_of(sb)), 1, dreg + 1);
-  const int *map1 = dmap, *map2 = dmap + 1;
-  long long nslots = 1;
+  SideRound<double> A = bounds_side(make_geom(nuva, p1_of(sa)), static_cast<int>(na), dreg);
+  SideRound<double> B = bounds_side(make_geom(nuvb, p1_of(sb)), static_cast<int>(nb), dreg + na);
+  const int *map1 = dmap, *map2 = dmap + nslots;
   double lb = 0.0;
   for (int round = 1; round <= p->max_rounds; ++round) {
     for (int side = 0; side < 2; ++side) {
@@ -2516,7 +2602,7 @@ void run_bounds(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_bou
       const SurfView<double> &v = side ? vb : va;
       timed(ctx, "basis", [&] { launch_basis(v, S, st, Batch{}, static_cast<const SurfView<double> *>(nullptr), true); }, 2.0 * S.nreg * S.g.nuv);
       timed(ctx, "samples", [&] { launch_samples(v, S, false, st); }, double(S.nreg) * S.g.nuv * S.g.nuv);
-      timed(ctx, "pad", [&] { launch_pad_bound(S, m2[side][0], m2[side][1], side ? eb : ea, st); });
+      timed(ctx, "pad", [&] { launch_pad_bound(S, v, dtab[side], side ? eb : ea, st); });
       timed(ctx, "cells", [&] { launch_cells(S, true, st); }, double(S.nreg) * S.g.W * S.g.W);
     }
     const unsigned long long tile_pairs = static_cast<unsigned long long>(nslots) * A.g.ntiles * B.g.ntiles;
@@ -3438,14 +3524,45 @@ void jsi_bounds_params_default(jsi_bounds_params *p) {
   p->max_pairs = 1ll << 22;
 }
 
-int jsi_surface_curvature_bounds(const int *ivec, const float *data, int ndata, double *m2u, double *m2v) {
+int jsi_surface_curvature_bounds(const int *ivec, const float *data, int ndata, const double *rect, double *m2u,
+                                 double *m2v) {
   if (!ivec || !data || !m2u || !m2v) return JSI_ERR_INVALID;
   try {
     check_surface(ivec, data, ndata);
     SurfaceRec s;
     surface_header(s, ivec, data);
     if (s.rat && !(s.wmin > 0)) return JSI_ERR_UNSUPPORTED;
-    second_derivative_bounds_host(ivec, data, m2u, m2v);
+    if (!rect) {
+      second_derivative_bounds_host(ivec, data, m2u, m2v);
+      return JSI_OK;
+    }
+    // The bounds mode's per-region rule: the largest per-span bound over the
+    // spans the rectangle touches, its upper ends looked up just below.
+    const int p = ivec[1], q = ivec[4], nsu = ivec[2] - p;
+    const std::vector<Vec4<double>> tab = span_curvature_table(ivec, data);
+    std::vector<double> U(data, data + ivec[3]), V(data + ivec[3], data + ivec[3] + ivec[6]);
+    auto span = [](const std::vector<double> &K, int deg, double u) {
+      const int n = static_cast<int>(K.size()) - deg - 1;
+      if (u <= K[deg]) return deg;
+      if (u >= K[n]) return n - 1;
+      int k = deg;
+      while (k + 1 < n && K[k + 1] <= u) ++k;
+      return k;
+    };
+    const double ulo = std::min(rect[0], rect[2]), uhi = std::max(rect[0], rect[2]);
+    const double vlo = std::min(rect[1], rect[3]), vhi = std::max(rect[1], rect[3]);
+    const int su0 = span(U, p, ulo), su1 = span(U, p, uhi > ulo ? std::nextafter(uhi, ulo) : uhi);
+    const int sv0 = span(V, q, vlo), sv1 = span(V, q, vhi > vlo ? std::nextafter(vhi, vlo) : vhi);
+    for (int c = 0; c < 3; ++c) m2u[c] = m2v[c] = 0.0;
+    for (int sv = sv0; sv <= sv1; ++sv)
+      for (int su = su0; su <= su1; ++su) {
+        const size_t k = 2 * (static_cast<size_t>(sv - q) * nsu + (su - p));
+        const double a[3] = {tab[k].x, tab[k].y, tab[k].z}, b[3] = {tab[k + 1].x, tab[k + 1].y, tab[k + 1].z};
+        for (int c = 0; c < 3; ++c) {
+          m2u[c] = std::max(m2u[c], a[c]);
+          m2v[c] = std::max(m2v[c], b[c]);
+        }
+      }
     return JSI_OK;
   } catch (const StatusError &e) {
     return e.status;

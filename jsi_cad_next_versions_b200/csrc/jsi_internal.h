@@ -370,7 +370,9 @@ void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &s
                            const unsigned long long *keys, int ij_bits, const double *pts, long long n, double *out,
                            cudaStream_t st);
 // sr.pad must hold 4 doubles per region (a Vec4 pad per region, x, y, z).
-void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
+// Per-region pads of the bounds mode from a per-knot-span table of
+// curvature bounds (two Vec4 per span: m2u, m2v).
+void launch_pad_bound(const SideRound<double> &sr, const SurfView<double> &v, const Vec4<double> *tab, double eps,
                       cudaStream_t st);
 void launch_bound_cull(const SideRound<double> &a, const SideRound<double> &b, const int *map1, const int *map2,
                        int nslots, double ub2, unsigned long long *surv, unsigned long long surv_cap,

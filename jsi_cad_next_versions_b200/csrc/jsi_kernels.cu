@@ -2369,7 +2369,7 @@ __global__ void __launch_bounds__(256) k_inter_leaf(SideRound<T> a, SideRound<T>
 // bound |S_uu| / |S_vv| per coordinate over the surface (the
 // second-derivative nets, convex hull); eps covers the evaluation and the
 // centre / half-span rounding.  pad4 holds a Vec4 per region.
-__global__ void k_pad_bound(SideRound<double> sr, Vec4<double> *pad4, Vec4<double> m2u, Vec4<double> m2v,
+__global__ void k_pad_bound(SideRound<double> sr, Vec4<double> *pad4, SurfView<double> v, const Vec4<double> *tab,
                             double eps) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= sr.nreg) return;
@@ -2381,11 +2381,27 @@ __global__ void k_pad_bound(SideRound<double> sr, Vec4<double> *pad4, Vec4<doubl
   const double dv = __dadd_ru(__dmul_ru(__ddiv_ru(fabs(reg.v1 - reg.v0), n1), slack),
                               0x1p-50 * (fabs(reg.v0) + fabs(reg.v1)));
   const double du2 = __dmul_ru(du, du), dv2 = __dmul_ru(dv, dv);
-  auto one = [&](double mu, double mv) {
-    const double e = __dadd_ru(__dmul_ru(du2, mu), __dmul_ru(dv2, mv));
+  // The largest span bounds over every knot span the region touches.  The
+  // upper end is looked up just below itself: a region that ends on a knot
+  // lies in the closed span before it, where that span's polynomial bound
+  // holds.
+  const int p = v.degu, q = v.degv, nsu = v.ncpu - p;
+  const double ulo = fmin(reg.u0, reg.u1), uhi = fmax(reg.u0, reg.u1);
+  const double vlo = fmin(reg.v0, reg.v1), vhi = fmax(reg.v0, reg.v1);
+  const int su0 = find_span(v.nku, p, ulo, v.U), su1 = find_span(v.nku, p, uhi > ulo ? nextafter(uhi, ulo) : uhi, v.U);
+  const int sv0 = find_span(v.nkv, q, vlo, v.V), sv1 = find_span(v.nkv, q, vhi > vlo ? nextafter(vhi, vlo) : vhi, v.V);
+  Vec4<double> mu{0, 0, 0, 0}, mv{0, 0, 0, 0};
+  for (int sv = sv0; sv <= sv1; ++sv)
+    for (int su = su0; su <= su1; ++su) {
+      const Vec4<double> a = tab[2 * ((sv - q) * nsu + (su - p))], b = tab[2 * ((sv - q) * nsu + (su - p)) + 1];
+      mu = Vec4<double>{fmax(mu.x, a.x), fmax(mu.y, a.y), fmax(mu.z, a.z), 0.0};
+      mv = Vec4<double>{fmax(mv.x, b.x), fmax(mv.y, b.y), fmax(mv.z, b.z), 0.0};
+    }
+  auto one = [&](double m_u, double m_v) {
+    const double e = __dadd_ru(__dmul_ru(du2, m_u), __dmul_ru(dv2, m_v));
     return __dadd_ru(__dmul_ru(__dmul_ru(e, 0.125), slack), eps);
   };
-  pad4[r] = Vec4<double>{one(m2u.x, m2v.x), one(m2u.y, m2v.y), one(m2u.z, m2v.z), 0.0};
+  pad4[r] = Vec4<double>{one(mu.x, mv.x), one(mu.y, mv.y), one(mu.z, mv.z), 0.0};
 }
 
 // Lower bound of the gap between [c1 - r1, c1 + r1] and [c2 - r2, c2 + r2].
@@ -4754,12 +4770,10 @@ void launch_curve_tangents(const SurfView<double> &sa, const SurfView<double> &s
                                                                 ij_bits, pts, n, out);
 }
 
-void launch_pad_bound(const SideRound<double> &sr, const double m2u[3], const double m2v[3], double eps,
+void launch_pad_bound(const SideRound<double> &sr, const SurfView<double> &v, const Vec4<double> *tab, double eps,
                       cudaStream_t st) {
   counted();
-  k_pad_bound<<<(sr.nreg + 127) / 128, 128, 0, st>>>(sr, reinterpret_cast<Vec4<double> *>(sr.pad),
-                                                     Vec4<double>{m2u[0], m2u[1], m2u[2], 0.0},
-                                                     Vec4<double>{m2v[0], m2v[1], m2v[2], 0.0}, eps);
+  k_pad_bound<<<(sr.nreg + 127) / 128, 128, 0, st>>>(sr, reinterpret_cast<Vec4<double> *>(sr.pad), v, tab, eps);
 }
 
 void launch_bound_cull(const SideRound<double> &a, const SideRound<double> &b, const int *map1, const int *map2,
