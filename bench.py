@@ -549,8 +549,40 @@ def sample_roofline(ctx, kt, form):
                         "nominal CUDA-core FP32 peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)"}}
 
 
+def region_roofline(ctx, kt, form):
+    """Roofline of the refinement rounds' fused region kernel
+    (k_region_cells): HBM bytes the library counted for the timed launches
+    (region records, pads, every cell's centre and half span, three bound
+    vectors per tile; the control net stays in L2) and the algorithmic flops
+    of its samples (full records, FMA = 2), over their event time.  The
+    refinement rounds run in FP64 in the FP64 and FP32-screen forms."""
+    ms, launches, units = kt["region_cells"]
+    flops = ctx.kernel_units("region_cells:flops")
+    nbytes = ctx.kernel_units("region_cells:bytes")
+    s = ms / 1e3
+    fp64 = form != "v5_fp32"
+    peak_f = NOMINAL_FP64_TFLOPS if fp64 else NOMINAL_FP32_TFLOPS
+    peaks = _peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    gbs = nbytes / s / 1e9 if s > 0 else 0.0
+    tf = flops / s / 1e12 if s > 0 else 0.0
+    return {"bound": "hbm", "kernel": "region_cells", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+            "frac": gbs / hbm_peak, "traffic": None,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+            "avg_launch_ms": ms / max(launches, 1), "units_per_launch": units / max(launches, 1),
+            "unit_name": "samples", "bytes_per_launch": nbytes / max(launches, 1),
+            "launch": "one fused region-kernel launch (one side of one refinement round of one query)",
+            "compute": {"achieved": tf, "peak": peak_f, "unit": "TFLOP/s", "frac": tf / peak_f,
+                        "peak_source": NOMINAL_FP64_NOTE if fp64 else
+                        "nominal CUDA-core FP32 peak (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)"}}
+
+
 def dominant_roofline(ctx, kt, form, n_queries):
+    """The dominant kernel's roofline when it is the region kernel or the
+    sample kernel (the intersection's evaluation), else the sample kernel's."""
     dom = max(kt.items(), key=lambda kv: kv[1][0])[0] if kt else None
+    if dom == "region_cells" and ctx.kernel_units("region_cells:bytes") > 0:
+        return dom, region_roofline(ctx, kt, form)
     roof = sample_roofline(ctx, kt, form) if "samples" in kt else None
     return dom, roof
 

@@ -32,6 +32,14 @@ def _p(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _shrink_points(buf: np.ndarray, written: int) -> np.ndarray:
+    """The first ``written`` 8-double point records of a point buffer, in
+    place: the buffer is shrunk (a realloc, which for a large block remaps
+    its pages without copying them) instead of the records being copied."""
+    buf.resize(written * 8, refcheck=False)
+    return buf.reshape(-1, 8)
+
+
 @dataclass
 class DistanceResult:
     v5_value: float
@@ -574,7 +582,7 @@ class Context:
         for q in range(n):
             if kinds[q] == 1:
                 if points:
-                    pbufs[q] = np.zeros(points_cap * 8, dtype=np.float64)
+                    pbufs[q] = np.empty(points_cap * 8, dtype=np.float64)
                     ires[q].points = pbufs[q].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
                     ires[q].points_cap = points_cap
                 if trace:
@@ -594,7 +602,7 @@ class Context:
             else:
                 r = self._inter_result(ires[q], tbufs.get(q), trace_cap)
                 if points:
-                    r.points = pbufs[q][:ires[q].points_written * 8].reshape(-1, 8).copy()
+                    r.points = _shrink_points(pbufs.pop(q), int(ires[q].points_written))
                     r.points_converged = int(ires[q].points_converged)
                 r.screen_written = int(ires[q].screen_written)
                 r.kmax_rechecked = int(ires[q].kmax_rechecked)
@@ -657,7 +665,7 @@ class Context:
             r.trace_cap = trace_cap
         pbuf = None
         if points:
-            pbuf = np.zeros(points_cap * 8, dtype=np.float64)
+            pbuf = np.empty(points_cap * 8, dtype=np.float64)
             r.points = pbuf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             r.points_cap = points_cap
         sbuf = None
@@ -676,7 +684,7 @@ class Context:
                 raise JsiError(-4, f"{m} screen candidates exceed screen_cap {screen_cap}")
             res.screen_pairs = sbuf[:3 * m].reshape(-1, 3).copy()
         if points:
-            res.points = pbuf[:r.points_written * 8].reshape(-1, 8).copy()
+            res.points = _shrink_points(pbuf, int(r.points_written))
             res.points_converged = int(r.points_converged)
         return res
 

@@ -884,6 +884,8 @@ double record_flops(int degu, int degv, int du, int dv, bool rat, bool need_k) {
   return f + (rat ? 60.0 : 0.0);
 }
 
+void add_units(Lane *ctx, const char *name, double units);
+
 // Evaluation + cell + tile build of one side (run_evaluation_and_construction_task,
 // distance_analysis.cu:88-116 / intersection.cu:175-219).
 template <typename T>
@@ -902,13 +904,21 @@ void build_side(Lane *ctx, const SurfView<T> &v, SideRound<T> &s, bool intersect
     return;
   }
   const double nsamp = double(s.nreg) * s.g.nuv * s.g.nuv;
-  add_units(ctx, "samples:flops", nsamp * record_flops(v.degu, v.degv, v.du, v.dv, v.rat != 0, need_k));
+  const double sample_flops = nsamp * record_flops(v.degu, v.degv, v.du, v.dv, v.rat != 0, need_k);
   if (!s.samples) {
-    // Small regions without tables: one fused launch per side.
+    // Small regions without tables: one fused launch per side.  Its HBM
+    // bytes: region records and the pads / curvature maxima per region, the
+    // centre and half span of every cell and three bound vectors per tile
+    // (the control net is L2-resident).
+    add_units(ctx, "region_cells:flops", sample_flops);
+    add_units(ctx, "region_cells:bytes",
+              double(s.nreg) * (sizeof(RegionRec<T>) + sizeof(T) + 3 * sizeof(unsigned long long) +
+                                double(s.g.W) * s.g.W * 2 * sizeof(Vec4<T>) + double(s.g.ntiles) * 3 * sizeof(Vec4<T>)));
     timed(ctx, "region_cells", [&] { launch_region_cells(v, s, need_k, span_u0, span_v0, cover, st); }, nsamp);
     JSI_CUDA(cudaGetLastError());
     return;
   }
+  add_units(ctx, "samples:flops", sample_flops);
   if (need_k) JSI_CUDA(cudaMemsetAsync(s.kmax, 0, sizeof(unsigned long long) * 3 * s.nreg, st));
   timed(ctx, "samples", [&] { launch_samples(v, s, need_k, st); }, nsamp);
   if (intersect) timed(ctx, "pad", [&] { launch_pad(s, need_k, span_u0, span_v0, st); });
