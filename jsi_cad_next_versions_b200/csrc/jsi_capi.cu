@@ -237,6 +237,8 @@ constexpr size_t kRingSeg = size_t(8) << 20;
 
 namespace {
 
+class HostPool;
+
 // One execution lane: a CUDA stream with its own device arena, stats record,
 // transfer counters and optional kernel timing.  The context owns a main lane
 // for synchronous calls and worker lanes for queued and batched queries, whose
@@ -270,7 +272,10 @@ struct Lane {
   // and releases on the calling thread change it while lanes run).  Null for
   // the main lane, whose callers hold it already.
   std::mutex *surfaces_mu = nullptr;
-  char *h_pin = nullptr;  // pinned staging of batch heads / records
+  char *h_pin = nullptr;  // pinned staging of batch heads / records / points
+  // The context's host threads (main lane only: its callers hold the context
+  // mutex, as the upload path that shares them does); null on worker lanes.
+  HostPool *hpool = nullptr;
   size_t h_pin_bytes = 0;
   long long batch_reruns = 0;  // batch items re-run alone after an overflow
   // Lockstep batches replayed as CUDA graphs, keyed by everything their
@@ -1741,7 +1746,10 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
     JSI_CUDA(cudaMemcpy2DAsync(lay.head, slab, pin, hsz, hsz, n, cudaMemcpyHostToDevice, st));
     L->h2d_bytes += hsz * n;
 
-    for (int r = 1; r <= R; ++r) {
+    // Refinement rounds at nuv <= kRefineNuv run as one fused launch
+    // (k_dist_refine: every round of a query in one block).
+    const bool fused = R >= 2 && p.nuv_refine <= kRefineNuv && p.k <= kBatchK;
+    for (int r = 1; r <= (fused ? 1 : R); ++r) {
       const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
       const bool scr = kScreen && r == 1;
       timed(L, "basis", [&] {
@@ -1787,6 +1795,22 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       }
       timed(L, "dist_close", [&] {
         launch_dist_close(stats, Rd.top, lay.rec, r - 1, Rd.surv_cap, Rd.cand_cap, r == R, st, bt);
+      });
+    }
+    if (fused) {
+      RefineArgs<TP> ra{};
+      for (int r = 2; r <= R; ++r) {
+        const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
+        ra.r[r - 1] = RefineRound<TP>{Rd.A.regions, Rd.B.regions, Rd.map1,  Rd.map2,
+                                      Rd.top,       Rd.next1,     Rd.next2, Rd.nmap1, Rd.nmap2};
+      }
+      ra.first = 2;
+      ra.last = R;
+      ra.nuv = p.nuv_refine;
+      ra.k = p.k;
+      timed(L, "refine", [&] {
+        launch_dist_refine<TP>(va, vb, head_view<TP>(lay.head, 0), head_view<TP>(lay.head, 1), stats, lay.rec, ra,
+                               st, bt);
       });
     }
     if (p.newton) {
@@ -2144,6 +2168,32 @@ struct FinalRound {
 // screen (T = double only): the first round runs the FP32 screen
 // (inter_screen_round); its result, and so every later round, equals the
 // FP64 form's.
+// Intersection points to the caller: one DMA into the lane's pinned staging,
+// then the copy into the caller's (pageable, often freshly mapped) buffer
+// split over the host threads, each chunk counting its converged points
+// (residual <= 1e-9 (1 + |x| + |y| + |z|)) on the way.  Returns that count.
+long long deliver_points(Lane *ctx, const double *dres, double *dst, long long keep, cudaStream_t st) {
+  const size_t bytes = static_cast<size_t>(keep) * 8 * sizeof(double);
+  const double *pin = reinterpret_cast<const double *>(lane_pinned(ctx, bytes));
+  JSI_CUDA(copy_async(ctx, const_cast<double *>(pin), dres, bytes, cudaMemcpyDeviceToHost, st));
+  JSI_CUDA(cudaStreamSynchronize(st));
+  constexpr long long kChunk = 8192;  // points (512 KiB) per host task
+  const size_t nchunk = static_cast<size_t>((keep + kChunk - 1) / kChunk);
+  std::atomic<long long> conv{0};
+  parallel_for(ctx->hpool, nchunk, [&](size_t c) {
+    const long long q0 = static_cast<long long>(c) * kChunk, q1 = std::min(keep, q0 + kChunk);
+    std::memcpy(dst + q0 * 8, pin + q0 * 8, static_cast<size_t>(q1 - q0) * 8 * sizeof(double));
+    long long m = 0;
+    for (long long q = q0; q < q1; ++q) {
+      const double *pt = pin + q * 8;
+      const double scale = 1.0 + std::fabs(pt[0]) + std::fabs(pt[1]) + std::fabs(pt[2]);
+      if (pt[7] <= 1e-9 * scale) ++m;
+    }
+    conv += m;
+  });
+  return conv.load();
+}
+
 template <typename T>
 void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const jsi_inter_params *p,
                       jsi_inter_result *out, FinalRound<T> *fin = nullptr, bool cover = false, bool screen = false) {
@@ -2296,18 +2346,9 @@ void run_intersection(Lane *ctx, const jsi_task *ta, const jsi_task *tb, const j
           fin->ij_bits = ij_bits;
         }
         const long long keep = out->points ? std::min<long long>(n, out->points_cap) : 0;
-        if (keep > 0)
-          JSI_CUDA(copy_async(ctx, out->points, dres, static_cast<size_t>(keep) * 8 * sizeof(double),
-                              cudaMemcpyDeviceToHost, st));
-        JSI_CUDA(cudaStreamSynchronize(st));
         out->points_written = keep;
-        long long conv = 0;
-        for (long long q = 0; q < keep; ++q) {
-          const double *pt = out->points + q * 8;
-          const double scale = 1.0 + std::fabs(pt[0]) + std::fabs(pt[1]) + std::fabs(pt[2]);
-          if (pt[7] <= 1e-9 * scale) ++conv;
-        }
-        out->points_converged = conv;
+        out->points_converged = keep > 0 ? deliver_points(ctx, dres, out->points, keep, st) : 0;
+        if (keep == 0) JSI_CUDA(cudaStreamSynchronize(st));
       }
       break;
     }
@@ -3249,6 +3290,7 @@ int jsi_create(const jsi_config *cfg, jsi_context **out) {
       if (const char *v = std::getenv("JSI_HOST_THREADS"); v && *v)
         nt = static_cast<int>(std::min(63L, std::max(0L, std::strtol(v, nullptr, 10))));
       if (nt > 0) ctx->hpool = std::make_unique<HostPool>(nt);
+      ctx->main.hpool = ctx->hpool.get();
     }
     return JSI_OK;
   });

@@ -309,6 +309,35 @@ template <typename TP>
 void launch_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRecord<TP> *rec, int round,
                        unsigned long long surv_cap, unsigned long long cand_cap, bool last, cudaStream_t st,
                        const Batch &bt);
+
+// The refinement rounds of a batched distance query in one launch (one block
+// of kRefineThreads per query, every round of the query inside it): the
+// round's regions evaluated into shared memory (basis, samples, cell centres
+// and tile ranges, the same operations as k_basis + k_cells_fused), the
+// exact k smallest (d2, slot, i, j) over the slots' cell pairs with tile
+// pairs pruned by their box gap against the k-th of the closest tile pairs,
+// the next round's regions with (slot, cell) dedup (k_dist_next) and the
+// round's record (k_dist_close).  Needs nuv <= kRefineNuv and k <= kBatchK.
+constexpr int kRefineNuv = 16;
+constexpr int kRefineThreads = 256;
+template <typename T>
+struct RefineRound {
+  const RegionRec<T> *reg1, *reg2;  // this round's regions (side A / B)
+  const int *map1, *map2;           // slot -> region
+  DistCand<T> *top;                 // the round's kept pairs
+  RegionRec<T> *next1, *next2;      // the next round's regions (null in the last round)
+  int *nmap1, *nmap2;
+};
+template <typename T>
+struct RefineArgs {
+  RefineRound<T> r[kBatchRounds];  // indexed by round - 1
+  int first, last;                 // rounds first..last (1-based, first >= 2)
+  int nuv, k;
+};
+template <typename T>
+void launch_dist_refine(const SurfView<T> &sa, const SurfView<T> &sb, const SurfView<T> *va, const SurfView<T> *vb,
+                        ScreenStats *stats, DistRecord<T> *rec, const RefineArgs<T> &args, cudaStream_t st,
+                        const Batch &bt);
 void launch_dist_pick(const unsigned long long *surv, const unsigned *surv_lb, unsigned long long surv_cap,
                       unsigned long long *head, unsigned long long head_cap, unsigned want, ScreenStats *stats,
                       cudaStream_t st, const Batch &bt);

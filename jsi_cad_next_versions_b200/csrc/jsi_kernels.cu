@@ -2091,6 +2091,444 @@ __global__ void k_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRe
   }
 }
 
+// ---- batched distance: every refinement round of a query in one block -------
+//
+// One block of kRefineThreads per query runs rounds first..last back to back
+// (a round needs only the query's own previous round).  Per round:
+//  * the regions of both sides (at most kBatchK each) are evaluated into
+//    shared memory: basis and span of each sample row and column as k_basis
+//    computes them (values only), every sample by eval_point (the factored
+//    cell kernels produce the same bits), every cell centre from its four
+//    corners as k_cells_fused forms it, and the centre range of each 8 x 8
+//    tile;
+//  * the exact k smallest pairs under the order (d2, slot, i, j) over every
+//    slot's cell pairs: each lane keeps its own kBatchK smallest in sorted
+//    registers (the k smallest overall are among the kBatchK smallest of the
+//    lane that examined them).  The block first examines the kRefineWarps
+//    tile pairs with the smallest box gaps and merges to their exact k-th,
+//    tau; a tile pair whose gap exceeds tau holds no pair of the k smallest
+//    (every pair's d2 is at least its tile pair's rounded gap), the others
+//    are examined, and a final merge gives the k smallest;
+//  * the next round's regions with (slot, cell) dedup per side, as
+//    k_dist_next, and the round's record and counters, as k_dist_close
+//    (tests = cell pairs examined, cands = lane-list entries, survivors =
+//    tile pairs examined, examined = tile pairs bounded).
+constexpr int kRefCells = (kRefineNuv - 1) * (kRefineNuv - 1);
+constexpr int kRefRegs = 2 * kBatchK;
+constexpr int kRefTe = 8;                                   // tile edge (cells)
+constexpr int kRefTiles = ((kRefineNuv - 1 + kRefTe - 1) / kRefTe) * ((kRefineNuv - 1 + kRefTe - 1) / kRefTe);
+constexpr int kRefPairs = kBatchK * kRefTiles * kRefTiles;  // tile pairs of a round at most
+constexpr int kRefineWarps = kRefineThreads / 32;
+constexpr int kRefMerge = kRefineWarps * kBatchK;
+static_assert(kRefCells <= 256 && kBatchK <= 256, "cell and slot indices are packed in 8 bits each");
+static_assert(kRefPairs <= kRefineThreads && kRefineNuv * kRefineNuv <= kRefineThreads, "one item per thread");
+static_assert((kRefPairs & (kRefPairs - 1)) == 0, "bitonic sort of the tile pairs");
+
+template <typename T, int MAXP>
+struct RefineSmem {
+  T cen[3][kRefRegs * kRefCells];   // cell centres, planes x / y / z; side B regions after side A's
+  T tb[kRefRegs * kRefTiles][6];    // tile centre ranges: lo xyz, hi xyz
+  T smp[3][kRefineNuv * kRefineNuv];
+  // basis of the sample columns (0) and rows (1): the values, then the two
+  // derivative rows that the basis routine zeroes (stride MAXP)
+  T nb[2][kRefineNuv][3 * MAXP];
+  T tplb[kRefPairs];                // box-gap bound of each tile pair
+  unsigned long long tpk[kRefPairs];  // (bound rounded down to float bits) << 32 | tile pair, sorted
+  unsigned long long mob[kRefMerge];
+  int mkey[kRefMerge];
+  unsigned long long tob[kBatchK];  // the k smallest: ordered d2 bits and packed (slot, i, j)
+  int tkey[kBatchK];
+  int sp[2][kRefineNuv];
+  int map1[kBatchK], map2[kBatchK];
+  unsigned long long tests, cands, surv;
+  int n;
+};
+
+template <typename T, int MAXP>
+constexpr size_t refine_smem() {
+  return sizeof(RefineSmem<T, MAXP>);
+}
+
+constexpr unsigned long long kRefPadOb = ~0ull;
+constexpr int kRefPadKey = INT_MAX;
+
+__device__ __forceinline__ bool ref_less(unsigned long long ao, int ak, unsigned long long bo, int bk) {
+  return ao < bo || (ao == bo && ak < bk);
+}
+
+// Sorted insert into a lane's list of the kBatchK smallest entries.
+__device__ __forceinline__ void ref_insert(unsigned long long (&lo)[kBatchK], int (&lk)[kBatchK],
+                                           unsigned long long o, int key) {
+  if (!ref_less(o, key, lo[kBatchK - 1], lk[kBatchK - 1])) return;
+  lo[kBatchK - 1] = o;
+  lk[kBatchK - 1] = key;
+#pragma unroll
+  for (int j = kBatchK - 1; j > 0; --j) {
+    if (ref_less(lo[j], lk[j], lo[j - 1], lk[j - 1])) {
+      const unsigned long long to = lo[j];
+      lo[j] = lo[j - 1];
+      lo[j - 1] = to;
+      const int tk = lk[j];
+      lk[j] = lk[j - 1];
+      lk[j - 1] = tk;
+    }
+  }
+}
+
+// The k smallest entries of all lane lists of the block into sm.tob / tkey
+// and their count into sm.n (every thread calls it; the lists are kept).
+template <typename SM>
+__device__ void ref_merge(SM &sm, const unsigned long long (&lo)[kBatchK], const int (&lk)[kBatchK], int k) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long co[kBatchK];
+  int ck[kBatchK];
+#pragma unroll
+  for (int j = 0; j < kBatchK; ++j) {
+    co[j] = lo[j];
+    ck[j] = lk[j];
+  }
+  // Each warp's k smallest, one per step: the lane holding the warp's
+  // smallest head drops it.  Entries are unique, padding aside, and padding
+  // only ever goes to later, unused positions.
+  for (int it = 0; it < kBatchK; ++it) {
+    unsigned long long bo = co[0];
+    int bk = ck[0], bl = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long oo = __shfl_xor_sync(kFull, bo, o);
+      const int ok = __shfl_xor_sync(kFull, bk, o);
+      const int ol = __shfl_xor_sync(kFull, bl, o);
+      if (ref_less(oo, ok, bo, bk) || (oo == bo && ok == bk && ol < bl)) {
+        bo = oo;
+        bk = ok;
+        bl = ol;
+      }
+    }
+    if (lane == 0) {
+      sm.mob[w * kBatchK + it] = it < k ? bo : kRefPadOb;
+      sm.mkey[w * kBatchK + it] = it < k ? bk : kRefPadKey;
+    }
+    if (lane == bl) {
+#pragma unroll
+      for (int j = 0; j < kBatchK - 1; ++j) {
+        co[j] = co[j + 1];
+        ck[j] = ck[j + 1];
+      }
+      co[kBatchK - 1] = kRefPadOb;
+      ck[kBatchK - 1] = kRefPadKey;
+    }
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t < kRefMerge) {
+    const unsigned long long o = sm.mob[t];
+    const int kk = sm.mkey[t];
+    if (!(o == kRefPadOb && kk == kRefPadKey)) {
+      int rank = 0;
+      for (int e = 0; e < kRefMerge; ++e) rank += ref_less(sm.mob[e], sm.mkey[e], o, kk) ? 1 : 0;
+      if (rank < k) {
+        sm.tob[rank] = o;
+        sm.tkey[rank] = kk;
+      }
+    }
+  }
+  if (t == 0) {
+    int cnt = 0;
+    for (int e = 0; e < kRefMerge; ++e) cnt += (sm.mob[e] == kRefPadOb && sm.mkey[e] == kRefPadKey) ? 0 : 1;
+    sm.n = cnt < k ? cnt : k;
+  }
+  __syncthreads();
+}
+
+// One region of one side into shared-memory slot `ri`: basis rows, samples,
+// cell centres, tile ranges.  Every thread calls it.
+template <typename T, int MAXP, typename SM>
+__device__ void ref_region(SM &sm, const SurfView<T> &s, const RegionRec<T> &reg, int nuv, int ri) {
+  const int t = threadIdx.x, W = nuv - 1, tw = (W + kRefTe - 1) / kRefTe;
+  if (t < 2 * nuv) {
+    // u = ((ustop - ustart) / nuv) * idx + ustart, as k_basis (no cover)
+    const int dir = t >= nuv ? 1 : 0, q = dir ? t - nuv : t;
+    const T lo = dir ? reg.v0 : reg.u0, hi = dir ? reg.v1 : reg.u1;
+    const T step = (hi - lo) / static_cast<T>(nuv);
+    const T x = step * static_cast<T>(q) + lo;
+    const int p = dir ? s.degv : s.degu;
+    T *out = sm.nb[dir][q];
+    if (s.zero) {
+      sm.sp[dir][q] = p;
+      for (int j = 0; j < 3 * MAXP; ++j) out[j] = T(0);
+    } else {
+      const int span = find_span(dir ? s.nkv : s.nku, p, x, dir ? s.V : s.U);
+      sm.sp[dir][q] = span;
+      basis_ders_any<T, MAXP>(span, p, x, dir ? s.V : s.U, 0, out, MAXP);
+    }
+  }
+  __syncthreads();
+  if (t < nuv * nuv) {
+    const int a = t / nuv, b = t - a * nuv;
+    T P[3];
+    eval_point(s, sm.sp[0][b], sm.nb[0][b], sm.sp[1][a], sm.nb[1][a], P);
+    sm.smp[0][t] = P[0];
+    sm.smp[1][t] = P[1];
+    sm.smp[2][t] = P[2];
+  }
+  __syncthreads();
+  if (t < W * W) {
+    const int a = t / W, b = t - a * W;
+    const int i0 = a * nuv + b, i1 = i0 + 1, i2 = i0 + nuv, i3 = i2 + 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T *S = sm.smp[c];
+      const T l = fmn(S[i0], fmn(S[i1], fmn(S[i2], S[i3])));
+      const T h = fmx(S[i0], fmx(S[i1], fmx(S[i2], S[i3])));
+      sm.cen[c][ri * kRefCells + t] = (l - T(0) + h + T(0)) / T(2);
+    }
+  }
+  __syncthreads();
+  const int w = t >> 5, lane = t & 31;
+  if (w < tw * tw) {
+    const int ty = w / tw, tx = w - (w / tw) * tw;
+    T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
+    T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
+    for (int l = lane; l < kRefTe * kRefTe; l += 32) {
+      const int a = ty * kRefTe + (l >> 3), b = tx * kRefTe + (l & 7);
+      if (a < W && b < W) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T v = sm.cen[c][ri * kRefCells + a * W + b];
+          lo[c] = fmn(lo[c], v);
+          hi[c] = fmx(hi[c], v);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        lo[c] = fmn(lo[c], __shfl_xor_sync(kFull, lo[c], o));
+        hi[c] = fmx(hi[c], __shfl_xor_sync(kFull, hi[c], o));
+      }
+    }
+    if (lane == 0) {
+      T *d = sm.tb[ri * kRefTiles + w];
+      d[0] = lo[0];
+      d[1] = lo[1];
+      d[2] = lo[2];
+      d[3] = hi[0];
+      d[4] = hi[1];
+      d[5] = hi[2];
+    }
+  }
+}
+
+// All cell pairs of tile pair tp (slot-major, then tile 1, then tile 2),
+// one warp: the lane's two tile-2 cells against every tile-1 cell.  Pairs
+// with ordered d2 above tau_ob are not entered.
+template <typename T, typename SM>
+__device__ __forceinline__ void ref_tile_pair(const SM &sm, int tp, int W, unsigned long long tau_ob,
+                                              unsigned long long (&lo)[kBatchK], int (&lk)[kBatchK],
+                                              unsigned long long &tests, unsigned long long &ins) {
+  const int lane = threadIdx.x & 31, tw = (W + kRefTe - 1) / kRefTe, nt = tw * tw;
+  const int slot = tp / (nt * nt), rem = tp - slot * nt * nt, t1 = rem / nt, t2 = rem - (rem / nt) * nt;
+  const int r1 = sm.map1[slot], r2 = kBatchK + sm.map2[slot];
+  const int ty1 = t1 / tw, tx1 = t1 - ty1 * tw, ty2 = t2 / tw, tx2 = t2 - ty2 * tw;
+  const int nv1 = min(kRefTe, W - ty1 * kRefTe), nu1 = min(kRefTe, W - tx1 * kRefTe);
+  const int nv2 = min(kRefTe, W - ty2 * kRefTe), nu2 = min(kRefTe, W - tx2 * kRefTe);
+  Vec4<T> c2[2];
+  int ci2[2];
+  bool v2[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int l2 = lane + 32 * h, a2 = l2 >> 3, b2 = l2 & 7;
+    v2[h] = a2 < nv2 && b2 < nu2;
+    ci2[h] = (ty2 * kRefTe + a2) * W + tx2 * kRefTe + b2;
+    const int o = r2 * kRefCells + (v2[h] ? ci2[h] : 0);
+    c2[h] = Vec4<T>{sm.cen[0][o], sm.cen[1][o], sm.cen[2][o], T(0)};
+  }
+  unsigned long long n = 0;
+  for (int a1 = 0; a1 < nv1; ++a1) {
+    for (int b1 = 0; b1 < nu1; ++b1) {
+      const int ci1 = (ty1 * kRefTe + a1) * W + tx1 * kRefTe + b1;
+      const int o = r1 * kRefCells + ci1;
+      const Vec4<T> c1{sm.cen[0][o], sm.cen[1][o], sm.cen[2][o], T(0)};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (!v2[h]) continue;
+        const unsigned long long ob = ordered_bits(center_d2(c1, c2[h]));
+        ++n;
+        if (ob <= tau_ob) {
+          const int key = (slot << 16) | (ci1 << 8) | ci2[h];
+          if (ref_less(ob, key, lo[kBatchK - 1], lk[kBatchK - 1])) {
+            ref_insert(lo, lk, ob, key);
+            ++ins;
+          }
+        }
+      }
+    }
+  }
+  tests += n;
+}
+
+template <typename T, int MAXP>
+__global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, SurfView<T> sb, const SurfView<T> *va,
+                                                                 const SurfView<T> *vb, ScreenStats *stats,
+                                                                 DistRecord<T> *rec, RefineArgs<T> args,
+                                                                 long long qs) {
+  extern __shared__ __align__(16) unsigned char refine_raw[];
+  RefineSmem<T, MAXP> &sm = *reinterpret_cast<RefineSmem<T, MAXP> *>(refine_raw);
+  const long long qo = qoff(qs);
+  if (va) sa = *qsh(va, qo);
+  if (vb) sb = *qsh(vb, qo);
+  stats = qsh(stats, qo);
+  rec = qsh(rec, qo);
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int nuv = args.nuv, W = nuv - 1, tw = (W + kRefTe - 1) / kRefTe, nt = tw * tw, k = args.k;
+  for (int round = args.first; round <= args.last; ++round) {
+    const RefineRound<T> R = args.r[round - 1];
+    const RegionRec<T> *reg1 = qsh(R.reg1, qo), *reg2 = qsh(R.reg2, qo);
+    const int *map1 = qsh(R.map1, qo), *map2 = qsh(R.map2, qo);
+    const int last = round == args.last;
+    // Counts from the previous round (its close and next).
+    const int st = stats->status;
+    const int nslots = st == 0 ? min(stats->nslots, kBatchK) : 0;
+    const int nreg1 = nslots > 0 ? min(stats->nreg1, kBatchK) : 0;
+    const int nreg2 = nslots > 0 ? min(stats->nreg2, kBatchK) : 0;
+    if (t == 0) {
+      sm.tests = 0;
+      sm.cands = 0;
+      sm.surv = 0;
+    }
+    if (t < kBatchK) {
+      // region indices of the slots, kept inside the evaluated regions
+      sm.map1[t] = t < nslots ? min(max(map1[t], 0), max(nreg1 - 1, 0)) : 0;
+      sm.map2[t] = t < nslots ? min(max(map2[t], 0), max(nreg2 - 1, 0)) : 0;
+    }
+    for (int r = 0; r < nreg1; ++r) ref_region<T, MAXP>(sm, sa, reg1[r], nuv, r);
+    for (int r = 0; r < nreg2; ++r) ref_region<T, MAXP>(sm, sb, reg2[r], nuv, kBatchK + r);
+    __syncthreads();
+    // Tile-pair bounds, sorted by their float round-down (ties by index).
+    const int npairs = nslots * nt * nt;
+    if (t < kRefPairs) {
+      unsigned long long key = ~0ull;
+      if (t < npairs) {
+        const int slot = t / (nt * nt), rem = t - slot * nt * nt, t1 = rem / nt, t2 = rem - (rem / nt) * nt;
+        const T *b1 = sm.tb[sm.map1[slot] * kRefTiles + t1];
+        const T *b2 = sm.tb[(kBatchK + sm.map2[slot]) * kRefTiles + t2];
+        const T lb = tile_lb(Vec4<T>{b1[0], b1[1], b1[2], T(0)}, Vec4<T>{b1[3], b1[4], b1[5], T(0)},
+                             Vec4<T>{b2[0], b2[1], b2[2], T(0)}, Vec4<T>{b2[3], b2[4], b2[5], T(0)});
+        sm.tplb[t] = lb;
+        key = (static_cast<unsigned long long>(lb_bits_down(lb)) << 32) | static_cast<unsigned>(t);
+      }
+      sm.tpk[t] = key;
+    }
+    for (int size = 2; size <= kRefPairs; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        __syncthreads();
+        if (t < kRefPairs) {
+          const int j = t ^ stride;
+          if (j > t) {
+            const bool up = (t & size) == 0;
+            const unsigned long long x = sm.tpk[t], y = sm.tpk[j];
+            if ((x > y) == up) {
+              sm.tpk[t] = y;
+              sm.tpk[j] = x;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    unsigned long long lo[kBatchK];
+    int lk[kBatchK];
+#pragma unroll
+    for (int j = 0; j < kBatchK; ++j) {
+      lo[j] = kRefPadOb;
+      lk[j] = kRefPadKey;
+    }
+    unsigned long long tests = 0, ins = 0, surv = 0;
+    // The kRefineWarps tile pairs with the smallest bounds, one per warp,
+    // then their exact k-th as the threshold.
+    const int head = min(npairs, kRefineWarps);
+    if (w < head) {
+      ref_tile_pair<T>(sm, static_cast<int>(sm.tpk[w] & 0xffffffffull), W, kRefPadOb, lo, lk, tests, ins);
+      ++surv;
+    }
+    ref_merge(sm, lo, lk, k);
+    const unsigned long long tau_ob = sm.n == k ? sm.tob[k - 1] : kRefPadOb;
+    const T tau = from_ordered<T>(tau_ob);
+    for (int e = head + w; e < npairs; e += kRefineWarps) {
+      const unsigned long long key = sm.tpk[e];
+      // key's bound is rounded down, so a key above tau means every later
+      // tile pair's bound is above it too
+      if (tau_ob != kRefPadOb && static_cast<T>(__uint_as_float(static_cast<unsigned>(key >> 32))) > tau) break;
+      const int tp = static_cast<int>(key & 0xffffffffull);
+      if (tau_ob != kRefPadOb && ordered_bits(sm.tplb[tp]) > tau_ob) continue;
+      ref_tile_pair<T>(sm, tp, W, tau_ob, lo, lk, tests, ins);
+      ++surv;
+    }
+    if (lane == 0) atomicAdd(&sm.surv, surv);
+    // tests / ins are per lane
+    atomicAdd(&sm.tests, tests);
+    atomicAdd(&sm.cands, ins);
+    ref_merge(sm, lo, lk, k);
+    const int n = sm.n;
+    DistCand<T> *top = qsh(R.top, qo);
+    if (t < n) {
+      const int key = sm.tkey[t];
+      const DistCand<T> c{from_ordered<T>(sm.tob[t]), key >> 16, (key >> 8) & 255, key & 255};
+      top[t] = c;
+      rec->top[round - 1][t] = c;
+    }
+    if (t == 0) {
+      if (R.next1 && n > 0) {
+        // Pair-preserving jobs with (slot, cell) dedup per side, in the
+        // order of the kept pairs (k_dist_next).
+        RegionRec<T> *next1 = qsh(R.next1, qo), *next2 = qsh(R.next2, qo);
+        int *nmap1 = qsh(R.nmap1, qo), *nmap2 = qsh(R.nmap2, qo);
+        int c1 = 0, c2 = 0;
+        for (int e = 0; e < n; ++e) {
+          const int ke = sm.tkey[e], se = ke >> 16, ie = (ke >> 8) & 255, je = ke & 255;
+          int u1 = -1, u2 = -1;
+          for (int q = 0; q < e; ++q) {
+            const int kq = sm.tkey[q], sq = kq >> 16;
+            if (u1 < 0 && sq == se && ((kq >> 8) & 255) == ie) u1 = nmap1[q];
+            if (u2 < 0 && sq == se && (kq & 255) == je) u2 = nmap2[q];
+          }
+          if (u1 < 0) {
+            u1 = c1++;
+            next1[u1] = child_rect(reg1[sm.map1[se]], nuv, ie);
+          }
+          if (u2 < 0) {
+            u2 = c2++;
+            next2[u2] = child_rect(reg2[sm.map2[se]], nuv, je);
+          }
+          nmap1[e] = u1;
+          nmap2[e] = u2;
+        }
+        stats->nreg1 = c1;
+        stats->nreg2 = c2;
+      }
+      rec->tests[round - 1] = static_cast<long long>(sm.tests);
+      rec->cands[round - 1] = static_cast<long long>(sm.cands);
+      rec->survivors[round - 1] = sm.surv;
+      rec->examined[round - 1] = static_cast<unsigned long long>(npairs);
+      rec->st_kept[round - 1] = 0;
+      rec->npairs[round - 1] = n;
+      rec->status[round - 1] = st;
+      stats->nsel = n;
+      stats->nslots = n;
+      stats->tile_pairs = static_cast<unsigned long long>(npairs);
+      stats->survivors = sm.surv;
+      stats->pair_tests = sm.tests;
+      stats->candidates = sm.cands;
+      if (!last) {
+        stats->status = 0;
+        stats->tau_bits = 0x7f800000u;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Block-wide search over 4096 counts for the bin where the running total
 // reaches want: *bin and the count still needed inside it (1024 threads).
 __device__ void find_crossing(const unsigned *hist, unsigned want, unsigned *s_warp, int *s_bin, unsigned *s_need) {
@@ -5020,5 +5458,33 @@ template void launch_newton_inter<double>(const SurfView<double> &, const SurfVi
                                           const RegionRec<double> *, const RegionRec<double> *, const int *,
                                           const int *, int, int, const unsigned long long *, long long, int,
                                           const double *, double *, cudaStream_t);
+
+template <typename T, int MAXP>
+void launch_dist_refine_p(const SurfView<T> &sa, const SurfView<T> &sb, const SurfView<T> *va, const SurfView<T> *vb,
+                          ScreenStats *stats, DistRecord<T> *rec, const RefineArgs<T> &args, cudaStream_t st,
+                          const Batch &bt) {
+  constexpr size_t smem = refine_smem<T, MAXP>();
+  cudaFuncSetAttribute(k_dist_refine<T, MAXP>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  counted();
+  k_dist_refine<T, MAXP><<<bdim(1, bt), kRefineThreads, smem, st>>>(sa, sb, va, vb, stats, rec, args, bt.qs);
+}
+
+template <typename T>
+void launch_dist_refine(const SurfView<T> &sa, const SurfView<T> &sb, const SurfView<T> *va, const SurfView<T> *vb,
+                        ScreenStats *stats, DistRecord<T> *rec, const RefineArgs<T> &args, cudaStream_t st,
+                        const Batch &bt) {
+  const int deg = std::max(std::max(sa.degu, sa.degv), std::max(sb.degu, sb.degv));
+  if (deg <= 8)
+    launch_dist_refine_p<T, 9>(sa, sb, va, vb, stats, rec, args, st, bt);
+  else
+    launch_dist_refine_p<T, kMaxDeg + 1>(sa, sb, va, vb, stats, rec, args, st, bt);
+}
+
+template void launch_dist_refine<float>(const SurfView<float> &, const SurfView<float> &, const SurfView<float> *,
+                                        const SurfView<float> *, ScreenStats *, DistRecord<float> *,
+                                        const RefineArgs<float> &, cudaStream_t, const Batch &);
+template void launch_dist_refine<double>(const SurfView<double> &, const SurfView<double> &, const SurfView<double> *,
+                                         const SurfView<double> *, ScreenStats *, DistRecord<double> *,
+                                         const RefineArgs<double> &, cudaStream_t, const Batch &);
 
 }  // namespace jsi
