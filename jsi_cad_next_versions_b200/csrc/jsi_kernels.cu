@@ -2128,17 +2128,15 @@ template <typename T, int MAXP>
 struct RefineSmem {
   T cen[3][kRefRegs * kRefCells];   // cell centres, planes x / y / z; side B regions after side A's
   T tb[kRefRegs * kRefTiles][6];    // tile centre ranges: lo xyz, hi xyz
-  T smp[3][kRefineNuv * kRefineNuv];
-  // basis of the sample columns (0) and rows (1): the values, then the two
-  // derivative rows that the basis routine zeroes (stride MAXP)
-  T nb[2][kRefineNuv][3 * MAXP];
+  T smp[3][kBatchK * kRefineNuv * kRefineNuv];  // one side's samples
+  T nb[kBatchK][2][kRefineNuv][MAXP];            // basis values of sample columns (0) and rows (1)
   T tplb[kRefPairs];                // box-gap bound of each tile pair
   unsigned long long tpk[kRefPairs];  // (bound rounded down to float bits) << 32 | tile pair, sorted
   unsigned long long mob[kRefMerge];
   int mkey[kRefMerge];
   unsigned long long tob[kBatchK];  // the k smallest: ordered d2 bits and packed (slot, i, j)
   int tkey[kBatchK];
-  int sp[2][kRefineNuv];
+  int sp[kBatchK][2][kRefineNuv];
   int map1[kBatchK], map2[kBatchK];
   unsigned long long tests, cands, surv;
   int n;
@@ -2240,64 +2238,74 @@ __device__ void ref_merge(SM &sm, const unsigned long long (&lo)[kBatchK], const
   __syncthreads();
 }
 
-// One region of one side into shared-memory slot `ri`: basis rows, samples,
-// cell centres, tile ranges.  Every thread calls it.
+// Every region of one side into shared-memory slots off..off + nreg - 1, in
+// four block-wide phases (basis rows, samples, cell centres, tile ranges),
+// each spread over all threads.  Every thread calls it.
 template <typename T, int MAXP, typename SM>
-__device__ void ref_region(SM &sm, const SurfView<T> &s, const RegionRec<T> &reg, int nuv, int ri) {
-  const int t = threadIdx.x, W = nuv - 1, tw = (W + kRefTe - 1) / kRefTe;
-  if (t < 2 * nuv) {
+__device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs, int nreg, int nuv, int off) {
+  const int t = threadIdx.x, W = nuv - 1, tw = (W + kRefTe - 1) / kRefTe, nt = tw * tw;
+  const int nl = 2 * nuv, ns = nuv * nuv, nc = W * W;
+  for (int idx = t; idx < nreg * nl; idx += kRefineThreads) {
     // u = ((ustop - ustart) / nuv) * idx + ustart, as k_basis (no cover)
-    const int dir = t >= nuv ? 1 : 0, q = dir ? t - nuv : t;
+    const int r = idx / nl, rem = idx - r * nl, dir = rem >= nuv ? 1 : 0, q = dir ? rem - nuv : rem;
+    const RegionRec<T> reg = regs[r];
     const T lo = dir ? reg.v0 : reg.u0, hi = dir ? reg.v1 : reg.u1;
     const T step = (hi - lo) / static_cast<T>(nuv);
     const T x = step * static_cast<T>(q) + lo;
     const int p = dir ? s.degv : s.degu;
-    T *out = sm.nb[dir][q];
+    T *out = sm.nb[r][dir][q];
     if (s.zero) {
-      sm.sp[dir][q] = p;
-      for (int j = 0; j < 3 * MAXP; ++j) out[j] = T(0);
+      sm.sp[r][dir][q] = p;
+      for (int j = 0; j < MAXP; ++j) out[j] = T(0);
     } else {
+      // the basis routine also zeroes two derivative rows (stride MAXP)
+      T tmp[3 * MAXP];
       const int span = find_span(dir ? s.nkv : s.nku, p, x, dir ? s.V : s.U);
-      sm.sp[dir][q] = span;
-      basis_ders_any<T, MAXP>(span, p, x, dir ? s.V : s.U, 0, out, MAXP);
+      sm.sp[r][dir][q] = span;
+      basis_ders_any<T, MAXP>(span, p, x, dir ? s.V : s.U, 0, tmp, MAXP);
+      for (int j = 0; j <= p; ++j) out[j] = tmp[j];
     }
   }
   __syncthreads();
-  if (t < nuv * nuv) {
-    const int a = t / nuv, b = t - a * nuv;
+  for (int idx = t; idx < nreg * ns; idx += kRefineThreads) {
+    const int r = idx / ns, l = idx - r * ns, a = l / nuv, b = l - (l / nuv) * nuv;
     T P[3];
-    eval_point(s, sm.sp[0][b], sm.nb[0][b], sm.sp[1][a], sm.nb[1][a], P);
-    sm.smp[0][t] = P[0];
-    sm.smp[1][t] = P[1];
-    sm.smp[2][t] = P[2];
+    eval_point(s, sm.sp[r][0][b], sm.nb[r][0][b], sm.sp[r][1][a], sm.nb[r][1][a], P);
+    sm.smp[0][idx] = P[0];
+    sm.smp[1][idx] = P[1];
+    sm.smp[2][idx] = P[2];
   }
   __syncthreads();
-  if (t < W * W) {
-    const int a = t / W, b = t - a * W;
-    const int i0 = a * nuv + b, i1 = i0 + 1, i2 = i0 + nuv, i3 = i2 + 1;
+  for (int idx = t; idx < nreg * nc; idx += kRefineThreads) {
+    const int r = idx / nc, l = idx - r * nc, a = l / W, b = l - (l / W) * W;
+    const int i0 = r * ns + a * nuv + b, i1 = i0 + 1, i2 = i0 + nuv, i3 = i2 + 1;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const T *S = sm.smp[c];
-      const T l = fmn(S[i0], fmn(S[i1], fmn(S[i2], S[i3])));
-      const T h = fmx(S[i0], fmx(S[i1], fmx(S[i2], S[i3])));
-      sm.cen[c][ri * kRefCells + t] = (l - T(0) + h + T(0)) / T(2);
+      const T lo = fmn(S[i0], fmn(S[i1], fmn(S[i2], S[i3])));
+      const T hi = fmx(S[i0], fmx(S[i1], fmx(S[i2], S[i3])));
+      sm.cen[c][(off + r) * kRefCells + l] = (lo - T(0) + hi + T(0)) / T(2);
     }
   }
   __syncthreads();
   const int w = t >> 5, lane = t & 31;
-  if (w < tw * tw) {
-    const int ty = w / tw, tx = w - (w / tw) * tw;
+  for (int tt = w; tt < nreg * nt; tt += kRefineWarps) {
+    const int r = tt / nt, tile = tt - r * nt, ty = tile / tw, tx = tile - (tile / tw) * tw;
+    const T *C0 = sm.cen[0] + (off + r) * kRefCells;
+    const T *C1 = sm.cen[1] + (off + r) * kRefCells;
+    const T *C2 = sm.cen[2] + (off + r) * kRefCells;
     T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
     T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
     for (int l = lane; l < kRefTe * kRefTe; l += 32) {
       const int a = ty * kRefTe + (l >> 3), b = tx * kRefTe + (l & 7);
       if (a < W && b < W) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T v = sm.cen[c][ri * kRefCells + a * W + b];
-          lo[c] = fmn(lo[c], v);
-          hi[c] = fmx(hi[c], v);
-        }
+        const int o = a * W + b;
+        lo[0] = fmn(lo[0], C0[o]);
+        lo[1] = fmn(lo[1], C1[o]);
+        lo[2] = fmn(lo[2], C2[o]);
+        hi[0] = fmx(hi[0], C0[o]);
+        hi[1] = fmx(hi[1], C1[o]);
+        hi[2] = fmx(hi[2], C2[o]);
       }
     }
 #pragma unroll
@@ -2309,7 +2317,7 @@ __device__ void ref_region(SM &sm, const SurfView<T> &s, const RegionRec<T> &reg
       }
     }
     if (lane == 0) {
-      T *d = sm.tb[ri * kRefTiles + w];
+      T *d = sm.tb[(off + r) * kRefTiles + tile];
       d[0] = lo[0];
       d[1] = lo[1];
       d[2] = lo[2];
@@ -2402,8 +2410,9 @@ __global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, 
       sm.map1[t] = t < nslots ? min(max(map1[t], 0), max(nreg1 - 1, 0)) : 0;
       sm.map2[t] = t < nslots ? min(max(map2[t], 0), max(nreg2 - 1, 0)) : 0;
     }
-    for (int r = 0; r < nreg1; ++r) ref_region<T, MAXP>(sm, sa, reg1[r], nuv, r);
-    for (int r = 0; r < nreg2; ++r) ref_region<T, MAXP>(sm, sb, reg2[r], nuv, kBatchK + r);
+    ref_side<T, MAXP>(sm, sa, reg1, nreg1, nuv, 0);
+    __syncthreads();
+    ref_side<T, MAXP>(sm, sb, reg2, nreg2, nuv, kBatchK);
     __syncthreads();
     // Tile-pair bounds, sorted by their float round-down (ties by index).
     const int npairs = nslots * nt * nt;
