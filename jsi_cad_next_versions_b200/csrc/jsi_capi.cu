@@ -1801,8 +1801,9 @@ int run_distance_batch(Lane *L, std::vector<BatchItem> &items, const jsi_dist_pa
       RefineArgs<TP> ra{};
       for (int r = 2; r <= R; ++r) {
         const BatchRound<TP, TC> &Rd = lay.rounds[r - 1];
-        ra.r[r - 1] = RefineRound<TP>{Rd.A.regions, Rd.B.regions, Rd.map1,  Rd.map2,
-                                      Rd.top,       Rd.next1,     Rd.next2, Rd.nmap1, Rd.nmap2};
+        // the round's centre arrays hold k x cpr >= k x (nuv - 1)^2 entries
+        ra.r[r - 1] = RefineRound<TP>{Rd.A.regions, Rd.B.regions, Rd.map1,  Rd.map2,  Rd.top,
+                                      Rd.next1,     Rd.next2,     Rd.nmap1, Rd.nmap2, Rd.A.center, Rd.B.center};
       }
       ra.first = 2;
       ra.last = R;

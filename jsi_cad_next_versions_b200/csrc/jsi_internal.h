@@ -327,6 +327,7 @@ struct RefineRound {
   DistCand<T> *top;                 // the round's kept pairs
   RegionRec<T> *next1, *next2;      // the next round's regions (null in the last round)
   int *nmap1, *nmap2;
+  Vec4<T> *cen1, *cen2;             // the round's cell centres, (nuv - 1)^2 per region
 };
 template <typename T>
 struct RefineArgs {

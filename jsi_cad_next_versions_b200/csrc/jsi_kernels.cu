@@ -2095,51 +2095,59 @@ __global__ void k_dist_close(ScreenStats *stats, const DistCand<TP> *top, DistRe
 //
 // One block of kRefineThreads per query runs rounds first..last back to back
 // (a round needs only the query's own previous round).  Per round:
-//  * the regions of both sides (at most kBatchK each) are evaluated into
-//    shared memory: basis and span of each sample row and column as k_basis
-//    computes them (values only), every sample by eval_point (the factored
-//    cell kernels produce the same bits), every cell centre from its four
-//    corners as k_cells_fused forms it, and the centre range of each 8 x 8
+//  * the regions of both sides (at most kBatchK each) are evaluated: basis
+//    and span of each sample row and column as k_basis computes them (values
+//    only) and every sample by eval_point (the factored cell kernels produce
+//    the same bits) in shared memory, every cell centre from its four
+//    corners as k_cells_fused forms it into the round's centre arrays in the
+//    query's slab (L1 / L2-resident), and the centre range of each 4 x 4
 //    tile;
 //  * the exact k smallest pairs under the order (d2, slot, i, j) over every
 //    slot's cell pairs: each lane keeps its own kBatchK smallest in sorted
 //    registers (the k smallest overall are among the kBatchK smallest of the
-//    lane that examined them).  The block first examines the kRefineWarps
-//    tile pairs with the smallest box gaps and merges to their exact k-th,
-//    tau; a tile pair whose gap exceeds tau holds no pair of the k smallest
-//    (every pair's d2 is at least its tile pair's rounded gap), the others
-//    are examined, and a final merge gives the k smallest;
+//    lane that examined them).  Every tile pair gets its box-gap bound; each
+//    slot's tile pair with the smallest bound is examined first (a warp per
+//    slot) and they are merged to their exact k-th, tau; a tile pair whose
+//    bound exceeds tau
+//    holds no pair of the k smallest (every pair's d2 is at least its tile
+//    pair's rounded gap), the others are examined, and a final merge gives
+//    the k smallest.  Tiles of 4 x 4 cells keep the examined pairs near the
+//    pairs that matter when the two patches run nearly parallel;
 //  * the next round's regions with (slot, cell) dedup per side, as
 //    k_dist_next, and the round's record and counters, as k_dist_close
 //    (tests = cell pairs examined, cands = lane-list entries, survivors =
 //    tile pairs examined, examined = tile pairs bounded).
 constexpr int kRefCells = (kRefineNuv - 1) * (kRefineNuv - 1);
 constexpr int kRefRegs = 2 * kBatchK;
-constexpr int kRefTe = 8;                                   // tile edge (cells)
-constexpr int kRefTiles = ((kRefineNuv - 1 + kRefTe - 1) / kRefTe) * ((kRefineNuv - 1 + kRefTe - 1) / kRefTe);
+constexpr int kRefTe = 4;                                   // tile edge (cells)
+constexpr int kRefTw = (kRefineNuv - 1 + kRefTe - 1) / kRefTe;
+constexpr int kRefTiles = kRefTw * kRefTw;
 constexpr int kRefPairs = kBatchK * kRefTiles * kRefTiles;  // tile pairs of a round at most
 constexpr int kRefineWarps = kRefineThreads / 32;
 constexpr int kRefMerge = kRefineWarps * kBatchK;
+constexpr int kRefRows = 6;  // control-net rows a sample column's u sums hold in registers
 static_assert(kRefCells <= 256 && kBatchK <= 256, "cell and slot indices are packed in 8 bits each");
-static_assert(kRefPairs <= kRefineThreads && kRefineNuv * kRefineNuv <= kRefineThreads, "one item per thread");
-static_assert((kRefPairs & (kRefPairs - 1)) == 0, "bitonic sort of the tile pairs");
+static_assert(kRefineNuv * kRefineNuv <= kRefineThreads, "one basis line per thread");
+static_assert(kRefTe * kRefTe == 16, "a half warp per tile");
+static_assert(kRefineWarps >= kBatchK, "a warp per slot picks the slot's first tile pair");
 
 template <typename T, int MAXP>
 struct RefineSmem {
-  T cen[3][kRefRegs * kRefCells];   // cell centres, planes x / y / z; side B regions after side A's
   T tb[kRefRegs * kRefTiles][6];    // tile centre ranges: lo xyz, hi xyz
   T smp[3][kBatchK * kRefineNuv * kRefineNuv];  // one side's samples
   T nb[kBatchK][2][kRefineNuv][MAXP];            // basis values of sample columns (0) and rows (1)
   T tplb[kRefPairs];                // box-gap bound of each tile pair
-  unsigned long long tpk[kRefPairs];  // (bound rounded down to float bits) << 32 | tile pair, sorted
+  unsigned short tpl[kRefPairs];    // tile pairs left to examine after the head
+  unsigned headmask[kRefPairs / 32];
   unsigned long long mob[kRefMerge];
   int mkey[kRefMerge];
   unsigned long long tob[kBatchK];  // the k smallest: ordered d2 bits and packed (slot, i, j)
   int tkey[kBatchK];
+  int head[kRefineWarps];
   int sp[kBatchK][2][kRefineNuv];
   int map1[kBatchK], map2[kBatchK];
   unsigned long long tests, cands, surv;
-  int n;
+  int n, ntpl;
 };
 
 template <typename T, int MAXP>
@@ -2186,27 +2194,26 @@ __device__ void ref_merge(SM &sm, const unsigned long long (&lo)[kBatchK], const
     ck[j] = lk[j];
   }
   // Each warp's k smallest, one per step: the lane holding the warp's
-  // smallest head drops it.  Entries are unique, padding aside, and padding
-  // only ever goes to later, unused positions.
+  // smallest head drops it.
   for (int it = 0; it < kBatchK; ++it) {
     unsigned long long bo = co[0];
-    int bk = ck[0], bl = lane;
+    int bk = ck[0];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const unsigned long long oo = __shfl_xor_sync(kFull, bo, o);
       const int ok = __shfl_xor_sync(kFull, bk, o);
-      const int ol = __shfl_xor_sync(kFull, bl, o);
-      if (ref_less(oo, ok, bo, bk) || (oo == bo && ok == bk && ol < bl)) {
+      if (ref_less(oo, ok, bo, bk)) {
         bo = oo;
         bk = ok;
-        bl = ol;
       }
     }
     if (lane == 0) {
       sm.mob[w * kBatchK + it] = it < k ? bo : kRefPadOb;
       sm.mkey[w * kBatchK + it] = it < k ? bk : kRefPadKey;
     }
-    if (lane == bl) {
+    // The lane holding the warp's smallest drops it (entries are unique;
+    // lanes whose head is padding equal to it drop padding).
+    if (co[0] == bo && ck[0] == bk) {
 #pragma unroll
       for (int j = 0; j < kBatchK - 1; ++j) {
         co[j] = co[j + 1];
@@ -2238,11 +2245,13 @@ __device__ void ref_merge(SM &sm, const unsigned long long (&lo)[kBatchK], const
   __syncthreads();
 }
 
+
 // Every region of one side into shared-memory slots off..off + nreg - 1, in
 // four block-wide phases (basis rows, samples, cell centres, tile ranges),
 // each spread over all threads.  Every thread calls it.
 template <typename T, int MAXP, typename SM>
-__device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs, int nreg, int nuv, int off) {
+__device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs, int nreg, int nuv, int off,
+                         Vec4<T> *cen) {
   const int t = threadIdx.x, W = nuv - 1, tw = (W + kRefTe - 1) / kRefTe, nt = tw * tw;
   const int nl = 2 * nuv, ns = nuv * nuv, nc = W * W;
   for (int idx = t; idx < nreg * nl; idx += kRefineThreads) {
@@ -2267,56 +2276,128 @@ __device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs,
     }
   }
   __syncthreads();
-  for (int idx = t; idx < nreg * ns; idx += kRefineThreads) {
-    const int r = idx / ns, l = idx - r * ns, a = l / nuv, b = l - (l / nuv) * nuv;
-    T P[3];
-    eval_point(s, sm.sp[r][0][b], sm.nb[r][0][b], sm.sp[r][1][a], sm.nb[r][1][a], P);
-    sm.smp[0][idx] = P[0];
-    sm.smp[1][idx] = P[1];
-    sm.smp[2][idx] = P[2];
+  // Samples, a thread per (region, sample column): the u sums of the
+  // control-net rows the column's samples need, in registers, then each
+  // sample's v combination.  Every u sum and v accumulation is the operation
+  // sequence of eval_point (contract3 / contract4 and the quotient), so the
+  // samples carry its bits; a column needing more than kRefRows net rows
+  // evaluates its samples one by one.
+  for (int idx = t; idx < nreg * nuv; idx += kRefineThreads) {
+    const int r = idx / nuv, b = idx - r * nuv;
+    int rmin = sm.sp[r][1][0], rmax = rmin;
+    for (int a = 1; a < nuv; ++a) {
+      rmin = min(rmin, sm.sp[r][1][a]);
+      rmax = max(rmax, sm.sp[r][1][a]);
+    }
+    rmin -= s.degv;
+    const int nrows = rmax - rmin + 1;
+    if (s.zero || nrows > kRefRows) {
+      for (int a = 0; a < nuv; ++a) {
+        T P[3];
+        eval_point(s, sm.sp[r][0][b], sm.nb[r][0][b], sm.sp[r][1][a], sm.nb[r][1][a], P);
+        sm.smp[0][r * ns + a * nuv + b] = P[0];
+        sm.smp[1][r * ns + a * nuv + b] = P[1];
+        sm.smp[2][r * ns + a * nuv + b] = P[2];
+      }
+      continue;
+    }
+    const T *Nu = sm.nb[r][0][b];
+    const int cu0 = sm.sp[r][0][b] - s.degu;
+    T rs[kRefRows][4];
+#pragma unroll
+    for (int R = 0; R < kRefRows; ++R) {
+      T r0 = T(0), r1 = T(0), r2 = T(0), r3 = T(0);
+      if (R < nrows) {
+        const Vec4<T> *cp = s.cpw + static_cast<long long>(s.ncpu) * (rmin + R) + cu0;
+        if (!s.rat) {
+          for (int c = 0; c <= s.degu; ++c) {
+            const Vec4<T> q = cp[c];
+            const T n = Nu[c];
+            r0 += n * q.x;
+            r1 += n * q.y;
+            r2 += n * q.z;
+          }
+        } else {
+          for (int c = 0; c <= s.degu; ++c) {
+            const Vec4<T> q = cp[c];
+            const T nw = Nu[c] * q.w;
+            r0 += nw * q.x;
+            r1 += nw * q.y;
+            r2 += nw * q.z;
+            r3 += nw;
+          }
+        }
+      }
+      rs[R][0] = r0;
+      rs[R][1] = r1;
+      rs[R][2] = r2;
+      rs[R][3] = r3;
+    }
+    for (int a = 0; a < nuv; ++a) {
+      const T *Nv = sm.nb[r][1][a];
+      const int R0 = sm.sp[r][1][a] - s.degv - rmin;
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll
+      for (int R = 0; R < kRefRows; ++R) {
+        const int rr = R - R0;
+        if (rr >= 0 && rr <= s.degv) {
+          const T m = Nv[rr];
+          a0 += m * rs[R][0];
+          a1 += m * rs[R][1];
+          a2 += m * rs[R][2];
+          a3 += m * rs[R][3];
+        }
+      }
+      if (s.rat) {
+        const T inv = T(1) / a3;
+        a0 = a0 * inv;
+        a1 = a1 * inv;
+        a2 = a2 * inv;
+      }
+      sm.smp[0][r * ns + a * nuv + b] = a0;
+      sm.smp[1][r * ns + a * nuv + b] = a1;
+      sm.smp[2][r * ns + a * nuv + b] = a2;
+    }
   }
   __syncthreads();
   for (int idx = t; idx < nreg * nc; idx += kRefineThreads) {
     const int r = idx / nc, l = idx - r * nc, a = l / W, b = l - (l / W) * W;
     const int i0 = r * ns + a * nuv + b, i1 = i0 + 1, i2 = i0 + nuv, i3 = i2 + 1;
+    T m[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const T *S = sm.smp[c];
       const T lo = fmn(S[i0], fmn(S[i1], fmn(S[i2], S[i3])));
       const T hi = fmx(S[i0], fmx(S[i1], fmx(S[i2], S[i3])));
-      sm.cen[c][(off + r) * kRefCells + l] = (lo - T(0) + hi + T(0)) / T(2);
+      m[c] = (lo - T(0) + hi + T(0)) / T(2);
     }
+    cen[r * nc + l] = Vec4<T>{m[0], m[1], m[2], T(0)};
   }
   __syncthreads();
-  const int w = t >> 5, lane = t & 31;
-  for (int tt = w; tt < nreg * nt; tt += kRefineWarps) {
-    const int r = tt / nt, tile = tt - r * nt, ty = tile / tw, tx = tile - (tile / tw) * tw;
-    const T *C0 = sm.cen[0] + (off + r) * kRefCells;
-    const T *C1 = sm.cen[1] + (off + r) * kRefCells;
-    const T *C2 = sm.cen[2] + (off + r) * kRefCells;
+  // Tile ranges: a half warp per 4 x 4 tile, one cell per lane.
+  const int lane = t & 31, half = lane >> 4, hl = lane & 15;
+  for (int base = 2 * (t >> 5); base < nreg * nt; base += 2 * kRefineWarps) {
+    const int tt = base + half;
+    const bool ok = tt < nreg * nt;
+    const int r = ok ? tt / nt : 0, tile = ok ? tt - r * nt : 0, ty = tile / tw, tx = tile - (tile / tw) * tw;
+    const int a = ty * kRefTe + (hl >> 2), b = tx * kRefTe + (hl & 3);
     T lo[3] = {pos_inf<T>(), pos_inf<T>(), pos_inf<T>()};
     T hi[3] = {-pos_inf<T>(), -pos_inf<T>(), -pos_inf<T>()};
-    for (int l = lane; l < kRefTe * kRefTe; l += 32) {
-      const int a = ty * kRefTe + (l >> 3), b = tx * kRefTe + (l & 7);
-      if (a < W && b < W) {
-        const int o = a * W + b;
-        lo[0] = fmn(lo[0], C0[o]);
-        lo[1] = fmn(lo[1], C1[o]);
-        lo[2] = fmn(lo[2], C2[o]);
-        hi[0] = fmx(hi[0], C0[o]);
-        hi[1] = fmx(hi[1], C1[o]);
-        hi[2] = fmx(hi[2], C2[o]);
-      }
+    if (ok && a < W && b < W) {
+      const Vec4<T> v = cen[r * nc + a * W + b];
+      lo[0] = hi[0] = v.x;
+      lo[1] = hi[1] = v.y;
+      lo[2] = hi[2] = v.z;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 8; o > 0; o >>= 1) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         lo[c] = fmn(lo[c], __shfl_xor_sync(kFull, lo[c], o));
         hi[c] = fmx(hi[c], __shfl_xor_sync(kFull, hi[c], o));
       }
     }
-    if (lane == 0) {
+    if (ok && hl == 0) {
       T *d = sm.tb[(off + r) * kRefTiles + tile];
       d[0] = lo[0];
       d[1] = lo[1];
@@ -2329,47 +2410,35 @@ __device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs,
 }
 
 // All cell pairs of tile pair tp (slot-major, then tile 1, then tile 2),
-// one warp: the lane's two tile-2 cells against every tile-1 cell.  Pairs
-// with ordered d2 above tau_ob are not entered.
+// one warp: lane l takes tile-2 cell l % 16 against tile-1 cells
+// 8 (l / 16) .. 8 (l / 16) + 7.  Pairs with ordered d2 above tau_ob are not
+// entered.
 template <typename T, typename SM>
-__device__ __forceinline__ void ref_tile_pair(const SM &sm, int tp, int W, unsigned long long tau_ob,
-                                              unsigned long long (&lo)[kBatchK], int (&lk)[kBatchK],
-                                              unsigned long long &tests, unsigned long long &ins) {
+__device__ __forceinline__ void ref_tile_pair(const SM &sm, const Vec4<T> *cen1, const Vec4<T> *cen2, int tp, int W,
+                                              unsigned long long tau_ob, unsigned long long (&lo)[kBatchK],
+                                              int (&lk)[kBatchK], unsigned long long &tests,
+                                              unsigned long long &ins) {
   const int lane = threadIdx.x & 31, tw = (W + kRefTe - 1) / kRefTe, nt = tw * tw;
   const int slot = tp / (nt * nt), rem = tp - slot * nt * nt, t1 = rem / nt, t2 = rem - (rem / nt) * nt;
-  const int r1 = sm.map1[slot], r2 = kBatchK + sm.map2[slot];
+  const Vec4<T> *C1 = cen1 + sm.map1[slot] * W * W, *C2 = cen2 + sm.map2[slot] * W * W;
   const int ty1 = t1 / tw, tx1 = t1 - ty1 * tw, ty2 = t2 / tw, tx2 = t2 - ty2 * tw;
-  const int nv1 = min(kRefTe, W - ty1 * kRefTe), nu1 = min(kRefTe, W - tx1 * kRefTe);
-  const int nv2 = min(kRefTe, W - ty2 * kRefTe), nu2 = min(kRefTe, W - tx2 * kRefTe);
-  Vec4<T> c2[2];
-  int ci2[2];
-  bool v2[2];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int l2 = lane + 32 * h, a2 = l2 >> 3, b2 = l2 & 7;
-    v2[h] = a2 < nv2 && b2 < nu2;
-    ci2[h] = (ty2 * kRefTe + a2) * W + tx2 * kRefTe + b2;
-    const int o = r2 * kRefCells + (v2[h] ? ci2[h] : 0);
-    c2[h] = Vec4<T>{sm.cen[0][o], sm.cen[1][o], sm.cen[2][o], T(0)};
-  }
+  const int l2 = lane & 15, a2 = ty2 * kRefTe + (l2 >> 2), b2 = tx2 * kRefTe + (l2 & 3);
+  if (a2 >= W || b2 >= W) return;
+  const int ci2 = a2 * W + b2;
+  const Vec4<T> c2 = C2[ci2];
   unsigned long long n = 0;
-  for (int a1 = 0; a1 < nv1; ++a1) {
-    for (int b1 = 0; b1 < nu1; ++b1) {
-      const int ci1 = (ty1 * kRefTe + a1) * W + tx1 * kRefTe + b1;
-      const int o = r1 * kRefCells + ci1;
-      const Vec4<T> c1{sm.cen[0][o], sm.cen[1][o], sm.cen[2][o], T(0)};
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (!v2[h]) continue;
-        const unsigned long long ob = ordered_bits(center_d2(c1, c2[h]));
-        ++n;
-        if (ob <= tau_ob) {
-          const int key = (slot << 16) | (ci1 << 8) | ci2[h];
-          if (ref_less(ob, key, lo[kBatchK - 1], lk[kBatchK - 1])) {
-            ref_insert(lo, lk, ob, key);
-            ++ins;
-          }
-        }
+#pragma unroll 4
+  for (int q = 0; q < 8; ++q) {
+    const int l1 = 8 * (lane >> 4) + q, a1 = ty1 * kRefTe + (l1 >> 2), b1 = tx1 * kRefTe + (l1 & 3);
+    if (a1 >= W || b1 >= W) continue;
+    const int ci1 = a1 * W + b1;
+    const unsigned long long ob = ordered_bits(center_d2(C1[ci1], c2));
+    ++n;
+    if (ob <= tau_ob) {
+      const int key = (slot << 16) | (ci1 << 8) | ci2;
+      if (ref_less(ob, key, lo[kBatchK - 1], lk[kBatchK - 1])) {
+        ref_insert(lo, lk, ob, key);
+        ++ins;
       }
     }
   }
@@ -2394,6 +2463,7 @@ __global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, 
     const RefineRound<T> R = args.r[round - 1];
     const RegionRec<T> *reg1 = qsh(R.reg1, qo), *reg2 = qsh(R.reg2, qo);
     const int *map1 = qsh(R.map1, qo), *map2 = qsh(R.map2, qo);
+    Vec4<T> *cen1 = qsh(R.cen1, qo), *cen2 = qsh(R.cen2, qo);
     const int last = round == args.last;
     // Counts from the previous round (its close and next).
     const int st = stats->status;
@@ -2410,42 +2480,13 @@ __global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, 
       sm.map1[t] = t < nslots ? min(max(map1[t], 0), max(nreg1 - 1, 0)) : 0;
       sm.map2[t] = t < nslots ? min(max(map2[t], 0), max(nreg2 - 1, 0)) : 0;
     }
-    ref_side<T, MAXP>(sm, sa, reg1, nreg1, nuv, 0);
+    ref_side<T, MAXP>(sm, sa, reg1, nreg1, nuv, 0, cen1);
     __syncthreads();
-    ref_side<T, MAXP>(sm, sb, reg2, nreg2, nuv, kBatchK);
+    ref_side<T, MAXP>(sm, sb, reg2, nreg2, nuv, kBatchK, cen2);
     __syncthreads();
-    // Tile-pair bounds, sorted by their float round-down (ties by index).
-    const int npairs = nslots * nt * nt;
-    if (t < kRefPairs) {
-      unsigned long long key = ~0ull;
-      if (t < npairs) {
-        const int slot = t / (nt * nt), rem = t - slot * nt * nt, t1 = rem / nt, t2 = rem - (rem / nt) * nt;
-        const T *b1 = sm.tb[sm.map1[slot] * kRefTiles + t1];
-        const T *b2 = sm.tb[(kBatchK + sm.map2[slot]) * kRefTiles + t2];
-        const T lb = tile_lb(Vec4<T>{b1[0], b1[1], b1[2], T(0)}, Vec4<T>{b1[3], b1[4], b1[5], T(0)},
-                             Vec4<T>{b2[0], b2[1], b2[2], T(0)}, Vec4<T>{b2[3], b2[4], b2[5], T(0)});
-        sm.tplb[t] = lb;
-        key = (static_cast<unsigned long long>(lb_bits_down(lb)) << 32) | static_cast<unsigned>(t);
-      }
-      sm.tpk[t] = key;
-    }
-    for (int size = 2; size <= kRefPairs; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        __syncthreads();
-        if (t < kRefPairs) {
-          const int j = t ^ stride;
-          if (j > t) {
-            const bool up = (t & size) == 0;
-            const unsigned long long x = sm.tpk[t], y = sm.tpk[j];
-            if ((x > y) == up) {
-              sm.tpk[t] = y;
-              sm.tpk[j] = x;
-            }
-          }
-        }
-      }
-    }
-    __syncthreads();
+    // Warp w bounds slot w's tile pairs and examines the one with the
+    // smallest bound (ties by index); the k-th of those pairs is tau.
+    const int npairs = nslots * nt * nt, per = nt * nt;
     unsigned long long lo[kBatchK];
     int lk[kBatchK];
 #pragma unroll
@@ -2453,29 +2494,58 @@ __global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, 
       lo[j] = kRefPadOb;
       lk[j] = kRefPadKey;
     }
+    if (t < kRefPairs / 32) sm.headmask[t] = 0u;
+    if (t == 0) sm.ntpl = 0;
+    __syncthreads();
     unsigned long long tests = 0, ins = 0, surv = 0;
-    // The kRefineWarps tile pairs with the smallest bounds, one per warp,
-    // then their exact k-th as the threshold.
-    const int head = min(npairs, kRefineWarps);
-    if (w < head) {
-      ref_tile_pair<T>(sm, static_cast<int>(sm.tpk[w] & 0xffffffffull), W, kRefPadOb, lo, lk, tests, ins);
+    if (w < nslots) {
+      unsigned long long bo = kRefPadOb;
+      int bk = kRefPadKey;
+      const T *tb1 = sm.tb[sm.map1[w] * kRefTiles];
+      const T *tb2 = sm.tb[(kBatchK + sm.map2[w]) * kRefTiles];
+      for (int q = lane; q < per; q += 32) {
+        const int t1 = q / nt, t2 = q - (q / nt) * nt, tp = w * per + q;
+        const T *b1 = tb1 + 6 * t1, *b2 = tb2 + 6 * t2;
+        const T lb = tile_lb(Vec4<T>{b1[0], b1[1], b1[2], T(0)}, Vec4<T>{b1[3], b1[4], b1[5], T(0)},
+                             Vec4<T>{b2[0], b2[1], b2[2], T(0)}, Vec4<T>{b2[3], b2[4], b2[5], T(0)});
+        sm.tplb[tp] = lb;
+        const unsigned long long ob = ordered_bits(lb);
+        if (ref_less(ob, tp, bo, bk)) {
+          bo = ob;
+          bk = tp;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long oo = __shfl_xor_sync(kFull, bo, o);
+        const int ok = __shfl_xor_sync(kFull, bk, o);
+        if (ref_less(oo, ok, bo, bk)) {
+          bo = oo;
+          bk = ok;
+        }
+      }
+      if (lane == 0) atomicOr(&sm.headmask[bk >> 5], 1u << (bk & 31));
+      ref_tile_pair<T>(sm, cen1, cen2, bk, W, kRefPadOb, lo, lk, tests, ins);
       ++surv;
     }
     ref_merge(sm, lo, lk, k);
     const unsigned long long tau_ob = sm.n == k ? sm.tob[k - 1] : kRefPadOb;
-    const T tau = from_ordered<T>(tau_ob);
-    for (int e = head + w; e < npairs; e += kRefineWarps) {
-      const unsigned long long key = sm.tpk[e];
-      // key's bound is rounded down, so a key above tau means every later
-      // tile pair's bound is above it too
-      if (tau_ob != kRefPadOb && static_cast<T>(__uint_as_float(static_cast<unsigned>(key >> 32))) > tau) break;
-      const int tp = static_cast<int>(key & 0xffffffffull);
-      if (tau_ob != kRefPadOb && ordered_bits(sm.tplb[tp]) > tau_ob) continue;
-      ref_tile_pair<T>(sm, tp, W, tau_ob, lo, lk, tests, ins);
+    // The other tile pairs whose bound is at most tau, compacted, then one
+    // per warp.
+    for (int tp = t; tp < npairs; tp += kRefineThreads) {
+      if ((sm.headmask[tp >> 5] >> (tp & 31)) & 1u) continue;
+      if (ordered_bits(sm.tplb[tp]) > tau_ob) continue;
+      const int pos = atomicAdd(&sm.ntpl, 1);
+      sm.tpl[pos] = static_cast<unsigned short>(tp);
+    }
+    __syncthreads();
+    const int ntpl = sm.ntpl;
+    for (int e = w; e < ntpl; e += kRefineWarps) {
+      ref_tile_pair<T>(sm, cen1, cen2, sm.tpl[e], W, tau_ob, lo, lk, tests, ins);
       ++surv;
     }
+    // tests / ins are per lane, surv per warp
     if (lane == 0) atomicAdd(&sm.surv, surv);
-    // tests / ins are per lane
     atomicAdd(&sm.tests, tests);
     atomicAdd(&sm.cands, ins);
     ref_merge(sm, lo, lk, k);
@@ -2494,13 +2564,14 @@ __global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, 
         RegionRec<T> *next1 = qsh(R.next1, qo), *next2 = qsh(R.next2, qo);
         int *nmap1 = qsh(R.nmap1, qo), *nmap2 = qsh(R.nmap2, qo);
         int c1 = 0, c2 = 0;
+        int m1[kBatchK], m2[kBatchK];  // this round's maps, kept on chip while they are built
         for (int e = 0; e < n; ++e) {
           const int ke = sm.tkey[e], se = ke >> 16, ie = (ke >> 8) & 255, je = ke & 255;
           int u1 = -1, u2 = -1;
           for (int q = 0; q < e; ++q) {
             const int kq = sm.tkey[q], sq = kq >> 16;
-            if (u1 < 0 && sq == se && ((kq >> 8) & 255) == ie) u1 = nmap1[q];
-            if (u2 < 0 && sq == se && (kq & 255) == je) u2 = nmap2[q];
+            if (u1 < 0 && sq == se && ((kq >> 8) & 255) == ie) u1 = m1[q];
+            if (u2 < 0 && sq == se && (kq & 255) == je) u2 = m2[q];
           }
           if (u1 < 0) {
             u1 = c1++;
@@ -2510,6 +2581,8 @@ __global__ void __launch_bounds__(kRefineThreads) k_dist_refine(SurfView<T> sa, 
             u2 = c2++;
             next2[u2] = child_rect(reg2[sm.map2[se]], nuv, je);
           }
+          m1[e] = u1;
+          m2[e] = u2;
           nmap1[e] = u1;
           nmap2[e] = u2;
         }
