@@ -2276,23 +2276,30 @@ __device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs,
     }
   }
   __syncthreads();
-  // Samples, a thread per (region, sample column): the u sums of the
-  // control-net rows the column's samples need, in registers, then each
-  // sample's v combination.  Every u sum and v accumulation is the operation
+  // Samples, a thread per (region, sample column, part of its rows): the u
+  // sums of the control-net rows those samples need, in registers, then
+  // each sample's v combination.  Every u sum and v accumulation is the operation
   // sequence of eval_point (contract3 / contract4 and the quotient), so the
   // samples carry its bits; a column needing more than kRefRows net rows
   // evaluates its samples one by one.
-  for (int idx = t; idx < nreg * nuv; idx += kRefineThreads) {
-    const int r = idx / nuv, b = idx - r * nuv;
-    int rmin = sm.sp[r][1][0], rmax = rmin;
-    for (int a = 1; a < nuv; ++a) {
+  // A column's sample rows are split over `split` threads so that every
+  // thread has work (each forms the u sums its own rows need).
+  const int ncol = max(nreg * nuv, 1);
+  const int split = max(1, min(nuv, kRefineThreads / ncol)), rows_per = (nuv + split - 1) / split;
+  for (int idx = t; idx < ncol * split && nreg > 0; idx += kRefineThreads) {
+    const int col = idx / split, part = idx - col * split;
+    const int r = col / nuv, b = col - r * nuv;
+    const int a_begin = part * rows_per, a_end = min(nuv, a_begin + rows_per);
+    if (a_begin >= a_end) continue;
+    int rmin = sm.sp[r][1][a_begin], rmax = rmin;
+    for (int a = a_begin + 1; a < a_end; ++a) {
       rmin = min(rmin, sm.sp[r][1][a]);
       rmax = max(rmax, sm.sp[r][1][a]);
     }
     rmin -= s.degv;
     const int nrows = rmax - rmin + 1;
     if (s.zero || nrows > kRefRows) {
-      for (int a = 0; a < nuv; ++a) {
+      for (int a = a_begin; a < a_end; ++a) {
         T P[3];
         eval_point(s, sm.sp[r][0][b], sm.nb[r][0][b], sm.sp[r][1][a], sm.nb[r][1][a], P);
         sm.smp[0][r * ns + a * nuv + b] = P[0];
@@ -2333,7 +2340,7 @@ __device__ void ref_side(SM &sm, const SurfView<T> &s, const RegionRec<T> *regs,
       rs[R][2] = r2;
       rs[R][3] = r3;
     }
-    for (int a = 0; a < nuv; ++a) {
+    for (int a = a_begin; a < a_end; ++a) {
       const T *Nv = sm.nb[r][1][a];
       const int R0 = sm.sp[r][1][a] - s.degv - rmin;
       T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
