@@ -124,6 +124,9 @@ def parse():
                     help="queries per lockstep batch on a lane (0: one query per lane job)")
     ap.add_argument("--e2e-chunks", type=int, default=2,
                     help="end-to-end pass: submitted chunks per step (uploads overlap the previous chunk)")
+    ap.add_argument("--e2e-host", choices=("pinned", "pageable"), default="pinned",
+                    help="end-to-end pass: host surfaces in page-locked memory from the context "
+                         "(uploaded by DMA straight from it) or in ordinary memory (staged)")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every batch eagerly (the library's default; kept for older command lines)")
     ap.add_argument("--graphs", action="store_true", help="replay repeated batches as CUDA graphs")
@@ -398,7 +401,8 @@ def run_ours(args):
 
     # The host surfaces as one packed set (what a caller holding a model's
     # faces in memory passes); packing is done once, like building them.
-    hostset = J.SurfaceBatch([x for pr in pairs for x in pr])
+    hostset = J.SurfaceBatch([x for pr in pairs for x in pr],
+                             alloc=ctx.host_array if args.e2e_host == "pinned" else None)
 
     e2e_result = []
     per = max(1, -(-args.batch // max(1, args.e2e_chunks)))  # queries per submitted chunk
@@ -448,6 +452,8 @@ def run_ours(args):
     e2e = {"value": world * args.batch * args.steps / (e2e_total / 1e3), "unit": "queries/s",
            "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps,
            "form": form, "chunks_per_step": -(-args.batch // per),
+           "host_memory": ("page-locked (Context.host_array): uploaded by DMA straight from it"
+                           if args.e2e_host == "pinned" else "pageable: staged into pinned memory"),
            "timing": f"{args.steps} steps as one continuous stream (chunks pipelined across steps); "
                      "the device working set per step (~4 GB of cells) exceeds L2",
            "reruns_per_step": (ctx.batch_reruns() - rr0) / args.steps}

@@ -79,6 +79,15 @@ int jsi_abi_version(void);
  * context's pool without synchronising. */
 int jsi_surface_upload(jsi_context *ctx, const int ivec[7], const float *data, int ndata, jsi_surface_id *out);
 int jsi_surface_release(jsi_context *ctx, jsi_surface_id id);
+/* Page-locked host memory owned by the context (freed by jsi_host_free or
+ * jsi_destroy).  Surface records that lie in one such block, in increasing
+ * address order, 16-byte aligned and not overlapping, are uploaded by
+ * jsi_surface_upload_many with one DMA per staging segment straight from it
+ * instead of being copied into the pinned staging first; the call still
+ * returns only after those copies have completed. */
+int jsi_host_alloc(jsi_context *ctx, unsigned long long bytes, void **ptr);
+int jsi_host_free(jsi_context *ctx, void *ptr);
+
 /* n surfaces in one call: ivecs = n x 7 headers, datas[q] / ndatas[q] the
  * records; out[q] gets each id (0 for those not uploaded after an error). */
 int jsi_surface_upload_many(jsi_context *ctx, int n, const int *ivecs, const float *const *datas, const int *ndatas,

@@ -27,7 +27,7 @@ PRECISIONS = {"v5_fp32": PREC_V5_FP32, "fp64": PREC_FP64, "fp32_screen": PREC_FP
 # Every symbol include/jsi_b200.h declares.
 EXPORTED = [
     "jsi_abi_version", "jsi_status_string", "jsi_last_error", "jsi_create", "jsi_destroy",
-    "jsi_surface_upload", "jsi_surface_upload_many", "jsi_surface_release", "jsi_surface_release_many",
+    "jsi_surface_upload", "jsi_surface_upload_many", "jsi_host_alloc", "jsi_host_free", "jsi_surface_release", "jsi_surface_release_many",
     "jsi_surface_domains", "jsi_resident_bytes", "jsi_context_stream",
     "jsi_transfer_bytes", "jsi_launch_count", "jsi_kernel_timing", "jsi_kernel_time", "jsi_kernel_units", "jsi_kernel_names",
     "jsi_dist_params_default",
@@ -136,6 +136,10 @@ def load(path: Path | str | None = None) -> ctypes.CDLL:
     L.jsi_destroy.restype = I
     L.jsi_surface_upload.argtypes = [P, P, P, I, ctypes.POINTER(I)]
     L.jsi_surface_upload.restype = I
+    L.jsi_host_alloc.argtypes = [P, ctypes.c_ulonglong, ctypes.POINTER(P)]
+    L.jsi_host_alloc.restype = I
+    L.jsi_host_free.argtypes = [P, P]
+    L.jsi_host_free.restype = I
     L.jsi_surface_release.argtypes = [P, I]
     L.jsi_surface_release.restype = I
     L.jsi_resident_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_ulonglong)]

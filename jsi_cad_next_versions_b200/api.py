@@ -164,7 +164,10 @@ class SurfaceBatch:
 
     _ALIGN = 16  # floats (64 bytes)
 
-    def __init__(self, surfaces=None):
+    def __init__(self, surfaces=None, alloc=None):
+        """``alloc(n)``, when given, supplies the float32 buffer (for example
+        ``Context.host_array``: page-locked memory, which the bulk upload then
+        reads by DMA without a staging copy)."""
         if surfaces is None:
             return
         n = len(surfaces)
@@ -175,7 +178,12 @@ class SurfaceBatch:
         stride = -(-nd // self._ALIGN) * self._ALIGN
         off = np.zeros(n, np.int64)
         np.cumsum(stride[:-1], out=off[1:])
-        self.data = np.zeros(int(stride.sum()) + self._ALIGN, np.float32)
+        total = int(stride.sum()) + self._ALIGN
+        if alloc is None:
+            self.data = np.zeros(total, np.float32)
+        else:
+            self.data = alloc(total)
+            self.data[:] = 0.0
         base = (-(self.data.ctypes.data // 4)) % self._ALIGN  # first 64-byte boundary in the buffer
         off += base
         for x, o, k in zip(surfaces, off.tolist(), nd.tolist()):
@@ -269,6 +277,29 @@ class Context:
         if getattr(self, "handle", None):
             self.lib.jsi_destroy(self.handle)
             self.handle = None
+            getattr(self, "_host_blocks", {}).clear()
+
+    def host_array(self, n: int, dtype=np.float32) -> np.ndarray:
+        """A host array of n elements in page-locked memory owned by the
+        context (``jsi_host_alloc``): surface records packed in it are
+        uploaded by DMA straight from it.  It stays valid until
+        ``host_free`` or ``close``."""
+        nbytes = int(n) * np.dtype(dtype).itemsize
+        p = ctypes.c_void_p()
+        self._check(self.lib.jsi_host_alloc(self.handle, nbytes, ctypes.byref(p)))
+        buf = (ctypes.c_char * nbytes).from_address(p.value)
+        arr = np.frombuffer(buf, dtype=dtype, count=int(n))
+        if not hasattr(self, "_host_blocks"):
+            self._host_blocks = {}
+        self._host_blocks[p.value] = buf
+        return arr
+
+    def host_free(self, arr: np.ndarray):
+        """Frees an array from ``host_array`` (the array must not be used
+        afterwards)."""
+        ptr = arr.__array_interface__["data"][0]
+        self._check(self.lib.jsi_host_free(self.handle, ctypes.c_void_p(ptr)))
+        getattr(self, "_host_blocks", {}).pop(ptr, None)
 
     def __enter__(self):
         return self

@@ -15,6 +15,7 @@
 #include <array>
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <chrono>
 #include <condition_variable>
@@ -457,6 +458,9 @@ struct jsi_context {
   int busy = 0;
   bool stopping = false;
   std::unique_ptr<HostPool> hpool;  // upload path host threads
+  // Page-locked host blocks handed out by jsi_host_alloc (base -> bytes):
+  // surface records inside one are uploaded by DMA straight from it.
+  std::map<uintptr_t, size_t> host_blocks;
 };
 
 namespace {
@@ -777,7 +781,80 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
     ctx->ring_off = 0;
     JSI_CUDA(cudaEventSynchronize(ctx->ring_ev[ctx->ring_cur]));
   };
-  size_t q = 0;
+  // Records that lie, in order and without overlap, inside one block of
+  // jsi_host_alloc go to the device ring by DMA straight from there: one copy
+  // per ring segment of the span they cover, no staging copy on the host (the
+  // header pass still reads them).  The call returns after those copies have
+  // completed, so the caller may change the records afterwards, as with the
+  // staged path.
+  bool direct = !in.empty() && !ctx->host_blocks.empty();
+  if (direct) {
+    const uintptr_t p0 = reinterpret_cast<uintptr_t>(in[0].data);
+    auto it = ctx->host_blocks.upper_bound(p0);
+    if (it == ctx->host_blocks.begin()) {
+      direct = false;
+    } else {
+      --it;
+      const uintptr_t lo = it->first, hi = it->first + it->second;
+      uintptr_t prev = lo;
+      for (size_t e = 0; e < in.size() && direct; ++e) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(in[e].data);
+        const uintptr_t b = a + static_cast<size_t>(in[e].ndata) * sizeof(float);
+        direct = a >= prev && b <= hi && (a & 15) == 0;
+        prev = b;
+      }
+    }
+  }
+  if (direct) {
+    size_t q = 0;
+    while (q < in.size()) {
+      // Records [q, q1) whose span and jobs fit in the rest of the segment.
+      const uintptr_t base = reinterpret_cast<uintptr_t>(in[q].data);
+      auto span_to = [&](size_t e) {
+        return reinterpret_cast<uintptr_t>(in[e].data) + static_cast<size_t>(in[e].ndata) * sizeof(float) - base;
+      };
+      if (ctx->ring_off + al(span_to(q)) + al(sizeof(SurfacePrep)) > kRingSeg && ctx->ring_off > 0) next_segment();
+      if (al(span_to(q)) + al(sizeof(SurfacePrep)) > kRingSeg) {
+        direct = false;  // a record larger than a segment: the staged path takes the rest
+        break;
+      }
+      size_t q1 = q + 1;
+      while (q1 < in.size() &&
+             ctx->ring_off + al(span_to(q1)) + al(sizeof(SurfacePrep) * (q1 - q + 1)) <= kRingSeg)
+        ++q1;
+      const size_t seg0 = static_cast<size_t>(ctx->ring_cur) * kRingSeg;
+      const size_t off = ctx->ring_off, span = span_to(q1 - 1), joff = off + al(span);
+      parallel_for(ctx->hpool.get(), q1 - q,
+                   [&](size_t e) { surface_header(heads[q + e], in[q + e].ivec, in[q + e].data); });
+      std::vector<SurfacePrep> jobs(q1 - q);
+      long long most = 0;
+      for (size_t e = q; e < q1; ++e) {
+        out.push_back(make_block(ctx, heads[e], in[e].ivec, in[e].ndata, &jobs[e - q]));
+        jobs[e - q].src = reinterpret_cast<const float *>(ctx->dring + seg0 + off +
+                                                          (reinterpret_cast<uintptr_t>(in[e].data) - base));
+        most = std::max(most, std::max(jobs[e - q].ndata, jobs[e - q].ncp));
+      }
+      const size_t jobs_b = sizeof(SurfacePrep) * jobs.size();
+      std::memcpy(ctx->ring + seg0 + joff, jobs.data(), jobs_b);
+      JSI_CUDA(copy_async(L, ctx->dring + seg0 + off, in[q].data, span, cudaMemcpyHostToDevice, st));
+      JSI_CUDA(copy_async(L, ctx->dring + seg0 + joff, ctx->ring + seg0 + joff, jobs_b, cudaMemcpyHostToDevice, st));
+      launch_surface_prep(reinterpret_cast<const SurfacePrep *>(ctx->dring + seg0 + joff),
+                          static_cast<int>(jobs.size()), most, st);
+      ctx->ring_off = joff + al(jobs_b);
+      q = q1;
+    }
+    if (direct) {
+      JSI_CUDA(cudaGetLastError());
+      // the caller's records are read by the copies queued above
+      JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
+      JSI_CUDA(cudaEventSynchronize(ctx->ring_ev[ctx->ring_cur]));
+      std::lock_guard<std::mutex> ls(ctx->surf_mu);
+      JSI_CUDA(cudaEventRecord(ctx->upload_ev, st));
+      return;
+    }
+    // fall through: the staged path uploads the records from out.size() on
+  }
+  size_t q = out.size();
   while (q < in.size()) {
     const size_t rec_b = al(static_cast<size_t>(in[q].ndata) * sizeof(float));
     if (rec_b + al(sizeof(SurfacePrep)) > kRingSeg) {
@@ -3314,8 +3391,38 @@ int jsi_destroy(jsi_context *ctx) {
   if (ctx->upload_ev) cudaEventDestroy(ctx->upload_ev);
   if (ctx->ring) cudaFreeHost(ctx->ring);
   if (ctx->dring) cudaFree(ctx->dring);
+  for (auto &b : ctx->host_blocks) cudaFreeHost(reinterpret_cast<void *>(b.first));
+  ctx->host_blocks.clear();
   lane_free(ctx->main);
   delete ctx;
+  return JSI_OK;
+}
+
+int jsi_host_alloc(jsi_context *ctx, unsigned long long bytes, void **ptr) {
+  if (!ctx || !ptr || bytes == 0) return JSI_ERR_INVALID;
+  *ptr = nullptr;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return guarded(ctx, [&]() {
+    JSI_CUDA(cudaSetDevice(ctx->device));
+    void *p = nullptr;
+    if (cudaMallocHost(&p, static_cast<size_t>(bytes)) != cudaSuccess) {
+      cudaGetLastError();
+      fail(JSI_ERR_NOMEM, "cudaMallocHost of %llu bytes failed", bytes);
+    }
+    ctx->host_blocks[reinterpret_cast<uintptr_t>(p)] = static_cast<size_t>(bytes);
+    *ptr = p;
+    return JSI_OK;
+  });
+}
+
+int jsi_host_free(jsi_context *ctx, void *ptr) {
+  if (!ctx || !ptr) return JSI_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->host_blocks.find(reinterpret_cast<uintptr_t>(ptr));
+  if (it == ctx->host_blocks.end()) return record(ctx, JSI_ERR_INVALID, "not a block of jsi_host_alloc");
+  // Uploads complete their copies from these blocks before returning.
+  cudaFreeHost(ptr);
+  ctx->host_blocks.erase(it);
   return JSI_OK;
 }
 

@@ -229,6 +229,54 @@ def test_packed_surface_set_uploads_in_chunks():
         assert ctx.resident_bytes() == base
 
 
+def test_pinned_surface_set_uploads_by_dma():
+    """A SurfaceBatch in the context's page-locked memory (uploaded by DMA
+    straight from it, spanning several staging segments) gives the same
+    resident surfaces as the same set in ordinary memory: same domains and
+    the same batch results.  A slice taken out of order (records not in
+    increasing address order) goes through the staged path."""
+    import jsi_cad_next_versions_b200 as J
+    pairs = _hard_wave_pairs(100, seed0=2100)  # 200 records x ~49 KB: more than one 8 MB segment
+    flat = [x for pr in pairs for x in pr]
+    with J.Context(0) as ctx:
+        pinned = J.SurfaceBatch(flat, alloc=ctx.host_array)
+        plain = J.SurfaceBatch(flat)
+        ids = np.asarray(ctx.upload_many(pinned), np.int32)
+        ref_ids = np.asarray(ctx.upload_many(plain), np.int32)
+        dom = ctx.surface_domains(ids)
+        assert np.array_equal(dom, ctx.surface_domains(ref_ids))
+        # the same records again, after the pinned buffer was changed and restored
+        keep = pinned.data.copy()
+        pinned.data[:] = 0.0
+        pinned.data[:] = keep
+        ids2 = np.asarray(ctx.upload_many(pinned[10:30]), np.int32)
+        assert np.array_equal(ctx.surface_domains(ids2), dom[10:30])
+        # records of the pinned block in decreasing address order: staged path
+        from types import SimpleNamespace
+        rev = [SimpleNamespace(ivec=pinned.surface(q)[0], data=pinned.surface(q)[1]) for q in range(9, -1, -1)]
+        ids3 = np.asarray(ctx.upload_many(rev), np.int32)
+        assert np.array_equal(ctx.surface_domains(ids3), dom[9::-1])
+        ctx.workers(2)
+        try:
+            sl = slice(0, 16)
+            got_ids, want_ids = ids.reshape(-1, 2)[sl], ref_ids.reshape(-1, 2)[sl]
+            d = dom.reshape(-1, 2, 4)[sl]
+            tb = J.TaskBatch.from_arrays(got_ids[:, 0], d[:, 0], 160, got_ids[:, 1], d[:, 1], 160)
+            tr = J.TaskBatch.from_arrays(want_ids[:, 0], d[:, 0], 160, want_ids[:, 1], d[:, 1], 160)
+            for form in ("fp32_screen", "v5_fp32"):
+                got, _ = ctx.min_distance_batch(tb, precision=form, trace=True)
+                want, _ = ctx.min_distance_batch(tr, precision=form, trace=True)
+                for a, b in zip(want, got):
+                    _same(b, a)
+        finally:
+            ctx.workers(0)
+        ctx.release_many(ids)
+        ctx.release_many(ids2)
+        ctx.release_many(ids3)
+        ctx.release_many(ref_ids)
+        ctx.host_free(pinned.data)
+
+
 def test_submit_wait_overlapping_batches():
     """Two batches in flight: the second's surfaces are uploaded after the
     first is submitted; each equals the same batch run synchronously."""
