@@ -83,8 +83,10 @@ int jsi_surface_release(jsi_context *ctx, jsi_surface_id id);
  * jsi_destroy).  Surface records that lie in one such block, in increasing
  * address order, 16-byte aligned and not overlapping, are uploaded by
  * jsi_surface_upload_many with one DMA per staging segment straight from it
- * instead of being copied into the pinned staging first; the call still
- * returns only after those copies have completed. */
+ * instead of being copied into the pinned staging first.  Those copies are
+ * asynchronous: the caller keeps the uploaded records unchanged until the
+ * upload has completed on the device (any query result that uses the
+ * surfaces, or jsi_host_free, which waits for it). */
 int jsi_host_alloc(jsi_context *ctx, unsigned long long bytes, void **ptr);
 int jsi_host_free(jsi_context *ctx, void *ptr);
 

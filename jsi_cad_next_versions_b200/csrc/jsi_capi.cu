@@ -784,9 +784,9 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
   // Records that lie, in order and without overlap, inside one block of
   // jsi_host_alloc go to the device ring by DMA straight from there: one copy
   // per ring segment of the span they cover, no staging copy on the host (the
-  // header pass still reads them).  The call returns after those copies have
-  // completed, so the caller may change the records afterwards, as with the
-  // staged path.
+  // header pass still reads them).  The copies are asynchronous: the caller
+  // keeps those records unchanged until the upload has completed on the
+  // device (jsi_host_free waits for it).
   bool direct = !in.empty() && !ctx->host_blocks.empty();
   if (direct) {
     const uintptr_t p0 = reinterpret_cast<uintptr_t>(in[0].data);
@@ -845,9 +845,6 @@ void upload_resident_many(jsi_context *ctx, const std::vector<PendingSurface> &i
     }
     if (direct) {
       JSI_CUDA(cudaGetLastError());
-      // the caller's records are read by the copies queued above
-      JSI_CUDA(cudaEventRecord(ctx->ring_ev[ctx->ring_cur], st));
-      JSI_CUDA(cudaEventSynchronize(ctx->ring_ev[ctx->ring_cur]));
       std::lock_guard<std::mutex> ls(ctx->surf_mu);
       JSI_CUDA(cudaEventRecord(ctx->upload_ev, st));
       return;
@@ -3420,7 +3417,8 @@ int jsi_host_free(jsi_context *ctx, void *ptr) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   auto it = ctx->host_blocks.find(reinterpret_cast<uintptr_t>(ptr));
   if (it == ctx->host_blocks.end()) return record(ctx, JSI_ERR_INVALID, "not a block of jsi_host_alloc");
-  // Uploads complete their copies from these blocks before returning.
+  // Uploads copy from these blocks asynchronously on the main stream.
+  if (ctx->main.stream) cudaStreamSynchronize(ctx->main.stream);
   cudaFreeHost(ptr);
   ctx->host_blocks.erase(it);
   return JSI_OK;
