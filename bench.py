@@ -226,14 +226,16 @@ def cpu_baseline(nuv0: int):
     if not oracle.Reference.available():
         return None
     R = oracle.Reference()
-    A, B, _ = synth.distance_pair_hard_wave()
+    sa, sb = shard_seeds(1, 0)[0]
+    A, B, _ = synth.distance_pair_hard_wave(seed_a=sa, seed_b=sb)
     ra, rb = np.array(A.rect(), np.float32), np.array(B.rect(), np.float32)
     t0 = time.perf_counter()
     v = R.minimum_distance(A, B, ra, rb, nuv0, NUV_REFINE, K, ROUNDS)
     el = time.perf_counter() - t0
     return {"value": 1.0 / el, "unit": "queries/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
-            "sample": f"1 full query (hard-wave seeds 3/4, nuv0={nuv0}) through the reference's minimum_distance, "
-                      f"{el:.2f} s, result {float(v):.9g}"}
+            "sample": f"1 full query (hard-wave seeds {sa}/{sb}, the first query of the GPU batch, nuv0={nuv0}) "
+                      f"through the reference's minimum_distance, {el:.2f} s",
+            "result": float(v)}
 
 
 def run_reference(args):
@@ -251,16 +253,19 @@ def run_reference(args):
         return
     from jsi_cad_next_versions_b200 import synth
     R = oracle.Reference()
-    A, B, _ = synth.distance_pair_hard_wave()
+    # The first query of the GPU arm's batch (rank 0's first seed pair).
+    sa, sb = shard_seeds(1, 0)[0]
+    A, B, _ = synth.distance_pair_hard_wave(seed_a=sa, seed_b=sb)
     ra, rb = np.array(A.rect(), np.float32), np.array(B.rect(), np.float32)
     # Each step is one full query (a bounded sample of the batch); the CPU has
     # no device warm-up, so one untimed query suffices.
     for _ in range(min(args.warmup, 1)):
         R.minimum_distance(A, B, ra, rb, args.nuv0, NUV_REFINE, K, ROUNDS)
     times = []
+    v = None
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        R.minimum_distance(A, B, ra, rb, args.nuv0, NUV_REFINE, K, ROUNDS)
+        v = R.minimum_distance(A, B, ra, rb, args.nuv0, NUV_REFINE, K, ROUNDS)
         times.append(time.perf_counter() - t0)
     total = sum(times)
     value = args.steps / total
@@ -269,10 +274,13 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "queries_per_step": 1, "nuv0": args.nuv0, "cores": int(os.environ["OMP_NUM_THREADS"])},
+        "config": {"workload": WORKLOAD, "queries_per_step": 1, "nuv0": args.nuv0, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                   "query": f"hard-wave seeds {sa}/{sb}: the first query of the GPU arm's batch"},
+        "result": None if v is None else float(v),
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
-                         "kind": "reference", "sample": "one full query per step through minimum_distance"},
+                         "kind": "reference",
+                         "sample": f"one full query per step (hard-wave seeds {sa}/{sb}) through minimum_distance"},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -321,12 +329,14 @@ def run_ours(args):
               ctx.task(b, np.array(B.rect(), np.float32), args.nuv0, 2)) for (a, b), (A, B) in zip(ids, pairs)]
     packed = J.TaskBatch(tasks)  # the query descriptors, packed once like the resident surfaces
     ref_values = {}
+    first_query = {}  # the query the reference arm and the CPU baseline time
     for form in forms:
         step_distances = []
 
         def step():
             res, _ = ctx.min_distance_batch(packed, k=K, rounds=ROUNDS, nuv_refine=NUV_REFINE, precision=form)
             step_distances[:] = res.distance.tolist()
+            first_query[form] = {"v5_value": float(res.v5_value[0]), "distance": float(res.distance[0])}
             return res.device_ms.tolist(), res[-1]
         # Clocks are sampled from the warm-up on (all of it runs under load):
         # the timed steps alone are shorter than nvidia-smi's start-up.
@@ -491,6 +501,8 @@ def run_ours(args):
         "forms": {f: {"queries_per_s": r["value"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
                       "result": ref_values[f], **({"tuned_chunk": r["tuned_chunk"]} if r["tuned_chunk"] else {})}
                   for f, r in results.items()},
+        "first_query": {"seeds": list(shard_seeds(1, 0)[0]), "by_form": first_query,
+                        "reference_result": cpu.get("result") if cpu else None},
         "rel_err_vs_fp64": rel_err,
         "speedup_vs_fp64": (head["value"] / results["fp64"]["value"]) if "fp64" in results else None,
         "fp64_per_query_qps": fp64_per_query,
