@@ -4828,8 +4828,11 @@ __device__ void newton_point(const SurfView<double> &sa, const SurfView<double> 
   out[7] = sqrt(dot3(D, D));
 }
 
+// 64-thread blocks, 8 per SM (at most 128 registers a thread, no spills):
+// the iteration is a chain of dependent FP64 steps, so warps in flight set
+// its speed (165 registers gave 12 warps per SM).
 template <typename TP, int MAXP>
-__global__ void k_newton_inter(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
+__global__ void __launch_bounds__(64, 8) k_newton_inter(SurfView<double> sa, SurfView<double> sb, const RegionRec<TP> *reg1,
                                const RegionRec<TP> *reg2, const int *map1, const int *map2, int nuv1, int nuv2,
                                const unsigned long long *keys, long long n, int ij_bits, const double *dom,
                                double *out) {
