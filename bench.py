@@ -685,9 +685,28 @@ def run_cfg3(args):
         elif ref is not None:
             results[key]["max_rel_point_err_vs_fp64"] = None
             results[key]["points_differ_from_fp64"] = [int(pts.shape[0]), int(ref.shape[0])]
+    # Queries in flight: 16 independent copies of the query (padding on, the
+    # headline form, points from every final pair) in one query_batch call on
+    # 4 worker lanes, so one query's host round trips overlap another's kernels.
+    form = forms[0]
+    n_inflight, inflight_lanes = 16, 4
+    ctx.workers(inflight_lanes)
+    inflight_q = [("intersection", ta, tb)] * n_inflight
+    inflight_last = []
+
+    def inflight_step():
+        inflight_last[:] = [ctx.query_batch(inflight_q, precision=form, newton=True, points=True,
+                                            points_cap=1 << 20)]
+    inflight_t = _timed_steps(args, flush, stream, lambda: torch.cuda.synchronize(), inflight_step)
+    ires, ist, _ = inflight_last[0]
+    inflight = {"queries": n_inflight, "lanes": inflight_lanes, "form": form,
+                "queries_per_s": 1e3 * n_inflight * args.steps / sum(inflight_t),
+                "failed": int(sum(1 for x in ist if x != 0)),
+                "same_counts_as_alone": all(r is not None and r.counts.tolist() == results[f"{form}/k1"]["counts"]
+                                            for r in ires)}
+    ctx.workers(0)
     # end to end through the C ABI: both host surfaces uploaded, the query,
     # the points read back, both released
-    form = forms[0]
     ctx.release(sc)
     ctx.release(sd)
 
@@ -715,7 +734,7 @@ def run_cfg3(args):
         "forms": results,
         "speedup_vs_fp64": head["queries_per_s"] / results["fp64/k1"]["queries_per_s"] if "fp64/k1" in results else None,
         "e2e": e2e, "roofline": head["roofline"], "cpu_baseline": cpu, "clocks": head["clocks"],
-        "gpu_launches": head["gpu_launches"],
+        "gpu_launches": head["gpu_launches"], "in_flight": inflight,
     }
     print(json.dumps(line))
     ctx.close()
