@@ -1731,12 +1731,16 @@ void batch_screen(Lane *L, const BatchRound<TP, TC> &R, const SideRound<T> &X, c
 
 char *lane_pinned(Lane *L, size_t bytes) {
   if (L->h_pin_bytes < bytes) {
+    // At least double: every regrowth frees page-locked memory, which waits
+    // for the whole device (the other lanes' work included), so a lane whose
+    // jobs grow step by step regrows a logarithmic number of times.
+    const size_t want = std::max(bytes, std::max<size_t>(2 * L->h_pin_bytes, size_t(1) << 20));
     JSI_CUDA(cudaStreamSynchronize(L->stream));
     if (L->h_pin) JSI_CUDA(cudaFreeHost(L->h_pin));
     L->h_pin = nullptr;
     L->h_pin_bytes = 0;
-    JSI_CUDA(cudaMallocHost(reinterpret_cast<void **>(&L->h_pin), bytes));
-    L->h_pin_bytes = bytes;
+    JSI_CUDA(cudaMallocHost(reinterpret_cast<void **>(&L->h_pin), want));
+    L->h_pin_bytes = want;
   }
   return L->h_pin;
 }

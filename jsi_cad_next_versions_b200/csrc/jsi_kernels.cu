@@ -787,8 +787,11 @@ __host__ __device__ inline size_t region_cells_smem(const Geom &g, int rpb, size
   return o;
 }
 
+// Three blocks per SM (at most 85 registers a thread; the FP64 instance
+// spills a few words): the kernel waits on block barriers and shared-memory
+// loads, so more blocks in flight shorten it (126 registers gave two).
 template <typename T>
-__global__ void __launch_bounds__(kRegThreads) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
+__global__ void __launch_bounds__(kRegThreads, 3) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
                                                               T span_v0, int cover) {
   using U = typename OrdBits<T>::type;
   extern __shared__ __align__(16) unsigned char rc_raw[];
