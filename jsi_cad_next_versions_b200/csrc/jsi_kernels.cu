@@ -787,11 +787,12 @@ __host__ __device__ inline size_t region_cells_smem(const Geom &g, int rpb, size
   return o;
 }
 
-// Three blocks per SM (at most 85 registers a thread; the FP64 instance
-// spills a few words): the kernel waits on block barriers and shared-memory
-// loads, so more blocks in flight shorten it (126 registers gave two).
+// FP64: three blocks per SM (at most 85 registers a thread, a few words
+// spilled) instead of the two that 126 registers gave; the kernel waits on
+// block barriers and shared-memory loads, so more blocks in flight shorten it.
+// FP32: four blocks (64 registers, no spills).
 template <typename T>
-__global__ void __launch_bounds__(kRegThreads, 3) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
+__global__ void __launch_bounds__(kRegThreads, sizeof(T) == 8 ? 3 : 4) k_region_cells(SurfView<T> s, SideRound<T> sr, int need_k, T span_u0,
                                                               T span_v0, int cover) {
   using U = typename OrdBits<T>::type;
   extern __shared__ __align__(16) unsigned char rc_raw[];
